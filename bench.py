@@ -1,0 +1,404 @@
+#!/usr/bin/env python
+"""Benchmark of the two hot paths on B200 -- prints ONE JSON line.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Headline workload (a "step"): one FP64 DGEMM C(3527x9583) += A(3527x6581) *
+B(6581x9583), row-major, ld = row length (the reference README's DGEMM,
+README.md:11-17), inputs resident in HBM.  value = 2*m*n*k / step time, summed
+over ranks.  With N > 1 (torchrun, one process per GPU) every rank runs an
+independent replica: the paths run on one GPU and have no exchange step.
+
+Also reported in the same line:
+  * e2e       -- the same metric through the C ABI's host-pointer call
+                 (cfgmm_matmul_anyway_full) on pinned host buffers, the H2D copy
+                 of A, B, C and the D2H copy of C inside the timed region;
+  * roofline  -- achieved FP64 TFLOP/s of the DGEMM kernel (CUDA events on its
+                 stream) over the FP64 tensor-core peak measured in the same run;
+  * cpu_baseline -- the oracle (a C++ restatement of the reference's Rust
+                 loops; the reference itself cannot be built here) on the host
+                 cores, on a bounded row sample of the same DGEMM (rank 0, N=1);
+  * aodmao2rho -- the masked AO-DM-AO contraction on the taxol-sized geometric
+                 workload (2228 AOs, 16384 points in blocks of 64, 3 DMs, tile
+                 density 0.3) in FP64: effective masked GFLOP/s.
+
+--impl reference times the oracle port on the host cores on the same config and
+metric (rank 0 only; other ranks exit without work).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import importlib
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "rho GFLOP/s & DGEMM TFLOP/s, split-prec vs FP64 at <=1e-12 rel err; p99 latency"
+M, N, K = 3527, 9583, 6581
+# README.md:11-17: 530 ms on a Ryzen 7945HX for this DGEMM -> 2mnk / 0.53 s.
+PUBLISHED_TFLOPS = 2.0 * M * N * K / 0.530 / 1e12
+WORKLOAD = ("FP64 DGEMM C(3527x9583) += A(3527x6581) B(6581x9583), NN, row-major, "
+            "ld = row length, A,B ~ U(-1,1)")
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------
+# process group (one rank per GPU)
+# ---------------------------------------------------------------------------
+class Ranks:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.dist = None
+
+    def init(self, backend: str):
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.dist:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist:
+            self.dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+def peaks_lib():
+    L = ctypes.CDLL(os.path.join(ROOT, "cfgable-matmul_b200", "libcfgmm_peaks.so"))
+    for name in ("cfgmm_peak_dmma_tflops", "cfgmm_peak_dfma_tflops"):
+        getattr(L, name).argtypes = [ctypes.c_int, ctypes.c_int]
+        getattr(L, name).restype = ctypes.c_double
+    return L
+
+
+def profile_traffic(name: str):
+    """DRAM bytes per launch recorded from an ncu capture in profiles/<name>.md
+    (a line 'traffic_bytes_per_launch: <int>'), or None."""
+    path = os.path.join(ROOT, "profiles", name + ".md")
+    try:
+        m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+def oracle_mod():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    oracle.build()
+    return oracle
+
+
+def cpu_dgemm_sample(target_s: float = 10.0) -> dict:
+    """Times the oracle on a row sample of the DGEMM with every host thread,
+    growing the sample until it takes about target_s seconds."""
+    oracle = oracle_mod()
+    rng = np.random.default_rng(0)
+    b = rng.uniform(-1, 1, (K, N))
+    rows = 14
+    while True:
+        a = rng.uniform(-1, 1, (rows, K))
+        c = np.zeros((rows, N))
+        t0 = time.perf_counter()
+        oracle.matmul_anyway_full(c, a, b, rows, N, K, K, N, N, False, False)
+        dt = time.perf_counter() - t0
+        if dt >= target_s / 4 or rows >= M:
+            break
+        rows = min(M, max(rows * 2, int(rows * target_s / 4 / max(dt, 1e-3))))
+    # one more run at the final size so the figure is a steady-state one
+    t0 = time.perf_counter()
+    oracle.matmul_anyway_full(c, a, b, rows, N, K, K, N, N, False, False)
+    dt = time.perf_counter() - t0
+    return {"value": 2.0 * rows * N * K / dt / 1e12, "unit": "TFLOP/s",
+            "cores": oracle.max_threads(), "kind": "port",
+            "sample": f"{rows} of the 3527 rows of A (C[{rows}x9583] += A[{rows}x6581] B), "
+                      f"{dt:.2f} s"}
+
+
+# ---------------------------------------------------------------------------
+# the reference arm
+# ---------------------------------------------------------------------------
+def run_reference(args, ranks: Ranks):
+    if ranks.rank != 0:
+        return
+    oracle = oracle_mod()
+    rng = np.random.default_rng(0)
+    b = rng.uniform(-1, 1, (K, N))
+    rows = 28
+    a = rng.uniform(-1, 1, (rows, K))
+    c = np.zeros((rows, N))
+    # size each step to about 5 s of host work
+    t0 = time.perf_counter()
+    oracle.matmul_anyway_full(c, a, b, rows, N, K, K, N, N, False, False)
+    dt = time.perf_counter() - t0
+    rows = int(min(M, max(14, rows * 5.0 / max(dt, 1e-3))))
+    a = rng.uniform(-1, 1, (rows, K))
+    c = np.zeros((rows, N))
+    for _ in range(args.warmup):
+        oracle.matmul_anyway_full(c, a, b, rows, N, K, K, N, N, False, False)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.matmul_anyway_full(c, a, b, rows, N, K, K, N, N, False, False)
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    value = 2.0 * rows * N * K * args.steps / tot / 1e12
+    sample = f"{rows} of the 3527 rows of A per step (C[{rows}x9583] += A[{rows}x6581] B)"
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "TFLOP/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": value / PUBLISHED_TFLOPS, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "m": M, "n": N, "k": K, "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": oracle.max_threads(),
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": "C++ restatement of the reference's Rust loops (impl_matmul.rs:155-248); the Rust "
+                "reference cannot be built in this image (no Rust toolchain)",
+    }
+    print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, ranks: Ranks):
+    import torch
+    cm = importlib.import_module("cfgable-matmul_b200")
+    wl = importlib.import_module("cfgable-matmul_b200.workloads")
+    torch.cuda.set_device(ranks.local)
+    dev = torch.device("cuda", ranks.local)
+    stream = torch.cuda.current_stream()
+    lib = cm.lib()
+
+    def dgemm_dev(c, a, b):
+        rc = lib.cfgmm_matmul_dev(c.data_ptr(), a.data_ptr(), b.data_ptr(), M, N, K, K, N, N, 0,
+                                  0, cm.PREC_FP64, stream.cuda_stream)
+        if rc != 0:
+            cm._raise(rc)
+
+    # ---- peak of the FP64 tensor pipe, measured here (burst) ----
+    pk = peaks_lib()
+    dmma_peak = max(pk.cfgmm_peak_dmma_tflops(20000, 2), pk.cfgmm_peak_dmma_tflops(20000, 4))
+    dfma_peak = pk.cfgmm_peak_dfma_tflops(20000, 4)
+
+    g = torch.Generator(device=dev).manual_seed(1234 + ranks.rank)
+    a = torch.rand(M, K, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+    b = torch.rand(K, N, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+    c = torch.zeros(M, N, dtype=torch.float64, device=dev)
+
+    for _ in range(args.warmup):
+        dgemm_dev(c, a, b)
+    torch.cuda.synchronize()
+    clocks = Clocks(ranks.local)
+    clocks.start()
+    ranks.barrier()
+    torch.cuda.synchronize()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    evs[0].record(stream)
+    for i in range(args.steps):
+        dgemm_dev(c, a, b)
+        evs[i + 1].record(stream)
+    torch.cuda.synchronize()
+    ranks.barrier()
+    clk = clocks.stop()
+    per = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
+    total_ms = ranks.max(sum(per))
+    flops = 2.0 * M * N * K
+    value = ranks.world * flops * args.steps / (total_ms * 1e-3) / 1e12
+    kernel_ms = sum(per) / len(per)
+    achieved = flops / (kernel_ms * 1e-3) / 1e12
+    traffic = profile_traffic("dgemm_fp64_3527x9583x6581")
+
+    # ---- end to end through the C ABI host-pointer call, pinned buffers ----
+    ha = torch.empty(M, K, dtype=torch.float64).pin_memory()
+    hb = torch.empty(K, N, dtype=torch.float64).pin_memory()
+    hc = torch.zeros(M, N, dtype=torch.float64).pin_memory()
+    ha.copy_(a.cpu())
+    hb.copy_(b.cpu())
+    del a, b, c
+    torch.cuda.empty_cache()
+
+    def e2e_step():
+        rc = lib.cfgmm_matmul_anyway_full(hc.data_ptr(), hc.numel(), ha.data_ptr(), ha.numel(),
+                                          hb.data_ptr(), hb.numel(), M, N, K, K, N, N, 0, 0)
+        if rc != 0:
+            cm._raise(rc)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    ranks.barrier()
+    e2e_times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_total = ranks.max(sum(e2e_times))
+    e2e_value = ranks.world * flops * args.steps / e2e_total / 1e12
+    lib.cfgmm_release_workspace()
+    del ha, hb, hc
+
+    # ---- masked AO-DM-AO, taxol-sized geometric workload, FP64 ----
+    p = wl.geometric(seed=0)
+    ao = torch.from_numpy(p.ao).to(dev)
+    dms = torch.from_numpy(p.dms).to(dev)
+    tab = torch.from_numpy(p.tab).to(dev)
+    rho = torch.zeros(p.nset, p.ngrid, dtype=torch.float64, device=dev)
+
+    def aodm_step():
+        rc = lib.cfgmm_aodmao2rho_dev(rho.data_ptr(), dms.data_ptr(), ao.data_ptr(), ao.data_ptr(),
+                                      p.nao, p.ngrid, p.nao, p.ngrid, p.nset, tab.data_ptr(),
+                                      p.nblk, p.blksize, cm.PREC_FP64, stream.cuda_stream)
+        if rc != 0:
+            cm._raise(rc)
+
+    for _ in range(args.warmup):
+        aodm_step()
+    torch.cuda.synchronize()
+    ranks.barrier()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    ev[0].record(stream)
+    for i in range(args.steps):
+        aodm_step()
+        ev[i + 1].record(stream)
+    torch.cuda.synchronize()
+    aper = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
+    atot = ranks.max(sum(aper))
+    aflops = p.flops()
+    aodm = {"workload": p.name + f", blocks of {p.blksize}, tile density {p.density():.3f}",
+            "precision": "fp64", "value": ranks.world * aflops * args.steps / (atot * 1e-3) / 1e9,
+            "unit": "GFLOP/s", "ms_per_step": atot / args.steps,
+            "flops_per_step": aflops, "flops": "sum_s sum_b (2|I_b|^2 + 2|I_b|)|b| (masked)",
+            "frac_of_dmma_peak": (aflops / (atot / args.steps * 1e-3) / 1e12) / dmma_peak,
+            "launches_per_step": 3}
+
+    cpu = cpu_dgemm_sample() if (ranks.rank == 0 and ranks.world == 1 and not args.no_cpu) else None
+    out = {
+        "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": ranks.world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": value / PUBLISHED_TFLOPS,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "m": M, "n": N, "k": K,
+                   "parallelism": f"{ranks.world} independent replica(s), one per GPU",
+                   "l2": "inputs larger than L2 (961 MB of A, B, C per step)",
+                   "vs_baseline_ref": "README.md:11-17, 530 ms on Ryzen 7945HX"},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": dmma_peak,
+                     "unit": "TFLOP/s", "frac": achieved / dmma_peak, "traffic": traffic,
+                     "kernel": "dgemm_fp64_kernel<false,false>",
+                     "peak_source": "measured in this run: FP64 DMMA m16n8k4 register loop on "
+                                    "every SM (burst); FP64 FMA pipe measured "
+                                    f"{dfma_peak:.2f} TFLOP/s"},
+        "e2e": {"value": e2e_value, "unit": "TFLOP/s",
+                "h2d_bytes_per_step": 8 * (M * K + K * N + M * N),
+                "d2h_bytes_per_step": 8 * M * N,
+                "path": "cfgmm_matmul_anyway_full on pinned host buffers (synchronous)"},
+        "gpu_launches": args.steps,
+        "clocks": clk,
+        "aodmao2rho": aodm,
+    }
+    if cpu:
+        out["cpu_baseline"] = cpu
+    if ranks.rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    args = ap.parse_args()
+    ranks = Ranks()
+    if args.impl == "reference":
+        run_reference(args, ranks)
+        return
+    ranks.init("nccl")
+    try:
+        run_ours(args, ranks)
+    finally:
+        ranks.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,258 @@
+"""cfgable-matmul on B200: Python front end of libcfgmm.so.
+
+The functions mirror the reference crate's public API for its two hot paths --
+same names, argument order and meaning -- and call the C ABI declared in
+include/cfgmm.h through ctypes:
+
+=====================================  ============================================
+this module                            reference (paths relative to the crate root)
+=====================================  ============================================
+``MatmulLoops(...).matmul_loop_parallel_mnk_pack_a``  src/impl_matmul.rs:155-231
+``MatmulLoops(...).matmul_loop_macro_mb``             README.md:22-31
+``matmul_anyway_full``                                src/impl_matmul.rs:234-248
+``MatmulLoops(...).aodmao2rho_loop_parallel``         src/impl_aodmao2rho.rs:171-244
+``aodmao2rho_anyway``                                 src/impl_aodmao2rho.rs:247-261
+=====================================  ============================================
+
+Arguments are numpy arrays (host memory; the call is synchronous, like the
+reference) or CUDA torch tensors (device memory; the work is enqueued on the
+current torch stream).  Outputs are accumulated into.  Where the reference
+panics, these functions raise: ``ValueError`` for an argument the reference
+would reject by a panic, ``NotImplementedError`` for its ``unimplemented!``,
+``RuntimeError`` for a CUDA failure.  There is no CPU fallback: without the
+compiled library or a CUDA device every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = [
+    "MatmulLoops", "matmul_anyway_full", "aodmao2rho_anyway", "matmul_ex", "aodmao2rho_ex",
+    "PREC_FP64", "PREC_OZAKI_INT8", "CfgmmError", "lib", "library_path",
+]
+
+PREC_FP64 = 0
+PREC_OZAKI_INT8 = 1
+
+OK = 0
+ERR_INVALID_ARGUMENT = -1
+ERR_UNIMPLEMENTED = -2
+ERR_CUDA = -3
+ERR_NO_DEVICE = -4
+ERR_OUT_OF_MEMORY = -5
+ERR_TIMEOUT = -6
+ERR_BUSY = -7
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+library_path = os.path.join(_HERE, "libcfgmm.so")
+_lib = None
+
+
+class CfgmmError(RuntimeError):
+    """A CUDA-side failure reported by libcfgmm (status, message)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"libcfgmm status {status}: {message}")
+        self.status = status
+
+
+def lib() -> ctypes.CDLL:
+    """Loads libcfgmm.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(library_path):
+            raise ImportError(f"{library_path} is missing: run `python cfgable-matmul_b200/build.py`")
+        L = ctypes.CDLL(library_path)
+        P, S, U8, I = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint8, ctypes.c_int
+        gemm_host = [P, S, P, S, P, S, S, S, S, S, S, S, U8, U8]
+        for name in ("cfgmm_matmul_loop_parallel_mnk_pack_a", "cfgmm_matmul_anyway_full",
+                     "cfgmm_matmul_loop_macro_mb"):
+            getattr(L, name).argtypes = gemm_host
+            getattr(L, name).restype = I
+        L.cfgmm_matmul_ex.argtypes = gemm_host + [I]
+        L.cfgmm_matmul_ex.restype = I
+        L.cfgmm_matmul_dev.argtypes = [P, P, P, S, S, S, S, S, S, U8, U8, I, P]
+        L.cfgmm_matmul_dev.restype = I
+        aodm_host = [P, S, P, S, P, S, P, S, S, S, S, S, S, P, S, S]
+        L.cfgmm_aodmao2rho_anyway.argtypes = aodm_host
+        L.cfgmm_aodmao2rho_anyway.restype = I
+        L.cfgmm_aodmao2rho_loop_parallel.argtypes = aodm_host + [S]
+        L.cfgmm_aodmao2rho_loop_parallel.restype = I
+        L.cfgmm_aodmao2rho_ex.argtypes = aodm_host + [S, I]
+        L.cfgmm_aodmao2rho_ex.restype = I
+        L.cfgmm_aodmao2rho_dev.argtypes = [P, P, P, P, S, S, S, S, S, P, S, S, I, P]
+        L.cfgmm_aodmao2rho_dev.restype = I
+        L.cfgmm_status_string.argtypes = [I]
+        L.cfgmm_status_string.restype = ctypes.c_char_p
+        L.cfgmm_last_error.restype = ctypes.c_char_p
+        L.cfgmm_version.restype = I
+        L.cfgmm_release_workspace.restype = I
+        _lib = L
+    return _lib
+
+
+def _raise(rc: int) -> None:
+    if rc == OK:
+        return
+    msg = lib().cfgmm_last_error().decode(errors="replace") or lib().cfgmm_status_string(rc).decode()
+    if rc == ERR_INVALID_ARGUMENT:
+        raise ValueError(msg)
+    if rc == ERR_UNIMPLEMENTED:
+        raise NotImplementedError(msg)
+    raise CfgmmError(rc, msg)
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _host(x, dtype, writable=False):
+    """(pointer, length) of a C-contiguous numpy array of `dtype`."""
+    if not isinstance(x, np.ndarray):
+        raise TypeError("expected a numpy array or a CUDA torch tensor")
+    if x.dtype != dtype:
+        raise TypeError(f"expected dtype {np.dtype(dtype).name}, got {x.dtype}")
+    if not x.flags.c_contiguous:
+        raise ValueError("arrays must be C-contiguous (a Rust slice is contiguous)")
+    if writable and not x.flags.writeable:
+        raise ValueError("output array is read-only")
+    return x.ctypes.data, x.size
+
+
+def _dev(x, dtype_name):
+    if not x.is_cuda or not x.is_contiguous():
+        raise ValueError("device tensors must be contiguous CUDA tensors")
+    if str(x.dtype) != dtype_name:
+        raise TypeError(f"expected {dtype_name}, got {x.dtype}")
+    return x.data_ptr()
+
+
+def _stream_ptr():
+    import torch
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _as_tab(tab):
+    if isinstance(tab, np.ndarray) and tab.dtype == np.bool_:
+        return tab.view(np.uint8)
+    if _is_torch(tab) and str(tab.dtype) == "torch.bool":
+        return tab.view(dtype=__import__("torch").uint8)
+    return tab
+
+
+def matmul_ex(c, a, b, m, n, k, lda, ldb, ldc, transa, transb, precision=PREC_FP64) -> None:
+    """C += op(A) op(B) with an explicit arithmetic (PREC_FP64 / PREC_OZAKI_INT8)."""
+    if _is_torch(c):
+        rc = lib().cfgmm_matmul_dev(_dev(c, "torch.float64"), _dev(a, "torch.float64"),
+                                    _dev(b, "torch.float64"), m, n, k, lda, ldb, ldc,
+                                    int(bool(transa)), int(bool(transb)), precision, _stream_ptr())
+        return _raise(rc)
+    pc, lc = _host(c, np.float64, True)
+    pa, la = _host(a, np.float64)
+    pb, lb = _host(b, np.float64)
+    _raise(lib().cfgmm_matmul_ex(pc, lc, pa, la, pb, lb, m, n, k, lda, ldb, ldc,
+                                 int(bool(transa)), int(bool(transb)), precision))
+
+
+def matmul_anyway_full(c, a, b, m, n, k, lda, ldb, ldc, transa, transb) -> None:
+    """C[i*ldc+j] += sum_p opA(i,p) opB(p,j) (src/impl_matmul.rs:234-248)."""
+    if _is_torch(c):
+        return matmul_ex(c, a, b, m, n, k, lda, ldb, ldc, transa, transb)
+    pc, lc = _host(c, np.float64, True)
+    pa, la = _host(a, np.float64)
+    pb, lb = _host(b, np.float64)
+    _raise(lib().cfgmm_matmul_anyway_full(pc, lc, pa, la, pb, lb, m, n, k, lda, ldb, ldc,
+                                          int(bool(transa)), int(bool(transb))))
+
+
+def aodmao2rho_ex(rhos, dms, ao_lhs, ao_rhs, strides, shape, nset, tab, ldtab, blksize=48,
+                  precision=PREC_FP64) -> None:
+    """The masked AO-DM-AO contraction with an explicit BLKSIZE and arithmetic."""
+    stride_ao, stride_grid = strides
+    nao, ngrid = shape
+    tab = _as_tab(tab)
+    if _is_torch(rhos):
+        rc = lib().cfgmm_aodmao2rho_dev(
+            _dev(rhos, "torch.float64"), _dev(dms, "torch.float64"), _dev(ao_lhs, "torch.float64"),
+            _dev(ao_rhs, "torch.float64"), stride_ao, stride_grid, nao, ngrid, nset,
+            _dev(tab, "torch.uint8"), ldtab, blksize, precision, _stream_ptr())
+        return _raise(rc)
+    pr, lr = _host(rhos, np.float64, True)
+    pd, ld = _host(dms, np.float64)
+    pl, ll = _host(ao_lhs, np.float64)
+    pq, lq = _host(ao_rhs, np.float64)
+    pt, lt = _host(tab, np.uint8)
+    _raise(lib().cfgmm_aodmao2rho_ex(pr, lr, pd, ld, pl, ll, pq, lq, stride_ao, stride_grid, nao,
+                                     ngrid, nset, pt, lt, ldtab, blksize, precision))
+
+
+def aodmao2rho_anyway(rhos, dms, ao_lhs, ao_rhs, strides, shape, nset, tab, ldtab) -> None:
+    """rho[s,g] += sum_{u,v} ao_lhs[u,g] D_s[u,v] ao_rhs[v,g] over the AOs active in
+    g's block of 48 points (src/impl_aodmao2rho.rs:247-261)."""
+    if _is_torch(rhos):
+        return aodmao2rho_ex(rhos, dms, ao_lhs, ao_rhs, strides, shape, nset, tab, ldtab, 48)
+    stride_ao, stride_grid = strides
+    nao, ngrid = shape
+    pr, lr = _host(rhos, np.float64, True)
+    pd, ld = _host(dms, np.float64)
+    pl, ll = _host(ao_lhs, np.float64)
+    pq, lq = _host(ao_rhs, np.float64)
+    pt, lt = _host(_as_tab(tab), np.uint8)
+    _raise(lib().cfgmm_aodmao2rho_anyway(pr, lr, pd, ld, pl, ll, pq, lq, stride_ao, stride_grid,
+                                         nao, ngrid, nset, pt, lt, ldtab))
+
+
+class MatmulLoops:
+    """Mirror of ``MatmulLoops<T, MC, KC, NC, MR, NR_LANE, LANE>`` (src/structs.rs:15).
+
+    The const generics select CPU cache and register blocking in the
+    reference; on the GPU the library picks its own tiles, so they are kept
+    only for signature compatibility.  ``dtype`` must be float64: the
+    reference implements the micro-kernel for f64 only (src/structs.rs:19-20).
+    """
+
+    def __init__(self, dtype=np.float64, MC=252, KC=512, NC=240, MR=14, NR_LANE=2, LANE=8, MB=None):
+        if np.dtype(dtype) != np.float64:
+            raise TypeError("MatmulLoops is implemented for f64 only")
+        self.tuning = dict(MC=MC, KC=KC, NC=NC, MR=MR, NR_LANE=NR_LANE, LANE=LANE, MB=MB)
+
+    def matmul_loop_parallel_mnk_pack_a(self, c, a, b, m, n, k, lda, ldb, ldc, transa, transb):
+        """src/impl_matmul.rs:155-231"""
+        if _is_torch(c):
+            return matmul_ex(c, a, b, m, n, k, lda, ldb, ldc, transa, transb)
+        pc, lc = _host(c, np.float64, True)
+        pa, la = _host(a, np.float64)
+        pb, lb = _host(b, np.float64)
+        _raise(lib().cfgmm_matmul_loop_parallel_mnk_pack_a(pc, lc, pa, la, pb, lb, m, n, k, lda,
+                                                           ldb, ldc, int(bool(transa)),
+                                                           int(bool(transb))))
+
+    def matmul_loop_macro_mb(self, c, a, b, m, n, k, lda, ldb, ldc, transa, transb):
+        """README.md:22-31 (documented there, absent from the crate's sources)."""
+        if _is_torch(c):
+            return matmul_ex(c, a, b, m, n, k, lda, ldb, ldc, transa, transb)
+        pc, lc = _host(c, np.float64, True)
+        pa, la = _host(a, np.float64)
+        pb, lb = _host(b, np.float64)
+        _raise(lib().cfgmm_matmul_loop_macro_mb(pc, lc, pa, la, pb, lb, m, n, k, lda, ldb, ldc,
+                                                int(bool(transa)), int(bool(transb))))
+
+    def aodmao2rho_loop_parallel(self, rhos, dms, ao_lhs, ao_rhs, strides, shape, nset, tab,
+                                 ldtab, BLKSIZE=48):
+        """src/impl_aodmao2rho.rs:171-244; BLKSIZE is the const generic."""
+        if _is_torch(rhos):
+            return aodmao2rho_ex(rhos, dms, ao_lhs, ao_rhs, strides, shape, nset, tab, ldtab,
+                                 BLKSIZE)
+        stride_ao, stride_grid = strides
+        nao, ngrid = shape
+        pr, lr = _host(rhos, np.float64, True)
+        pd, ld = _host(dms, np.float64)
+        pl, ll = _host(ao_lhs, np.float64)
+        pq, lq = _host(ao_rhs, np.float64)
+        pt, lt = _host(_as_tab(tab), np.uint8)
+        _raise(lib().cfgmm_aodmao2rho_loop_parallel(pr, lr, pd, ld, pl, ll, pq, lq, stride_ao,
+                                                    stride_grid, nao, ngrid, nset, pt, lt, ldtab,
+                                                    BLKSIZE))

@@ -1,0 +1,410 @@
+// abi.cu -- the extern "C" boundary of libcfgmm.so (declared in include/cfgmm.h).
+//
+// Host-side duties only: argument validation that reproduces the reference's
+// panics as status codes, per-device workspaces and streams, host<->device
+// staging for the host-pointer entry points, and dispatch to the kernels.
+// Validation happens before any CUDA call, so a rejected call never touches a
+// device or an output buffer.
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/cfgmm.h"
+#include "aodmao2rho_fp64.cuh"
+#include "dgemm_fp64.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int status, const std::string& msg) {
+  g_last_error = msg;
+  return status;
+}
+
+int cuda_fail(cudaError_t err, const char* where) {
+  g_last_error = std::string(where) + ": " + cudaGetErrorName(err) + " (" +
+                 cudaGetErrorString(err) + ")";
+  if (err == cudaErrorMemoryAllocation) return CFGMM_ERR_OUT_OF_MEMORY;
+  if (err == cudaErrorNoDevice || err == cudaErrorInsufficientDriver) return CFGMM_ERR_NO_DEVICE;
+  return CFGMM_ERR_CUDA;
+}
+
+#define CFGMM_CUDA(call)                                   \
+  do {                                                     \
+    cudaError_t e_ = (call);                               \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);    \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// extents: number of elements a Rust slice must hold for the index range read
+// or written (0 when nothing is accessed).
+// ---------------------------------------------------------------------------
+bool mul_ok(size_t a, size_t b, size_t* out) { return !__builtin_mul_overflow(a, b, out); }
+bool add_ok(size_t a, size_t b, size_t* out) { return !__builtin_add_overflow(a, b, out); }
+
+// rows x cols with row stride ld: (rows-1)*ld + cols
+bool extent2(size_t rows, size_t cols, size_t ld, size_t* out) {
+  if (rows == 0 || cols == 0) { *out = 0; return true; }
+  size_t t;
+  return mul_ok(rows - 1, ld, &t) && add_ok(t, cols, out);
+}
+
+// Kernels index with 32-bit ints and round sizes up to their tiles.
+bool fits_int(size_t v) { return v <= size_t(INT_MAX) - 4096; }
+
+// ---------------------------------------------------------------------------
+// per-device state for the host-pointer entry points
+// ---------------------------------------------------------------------------
+struct DeviceState {
+  std::mutex mu;
+  cudaStream_t stream = nullptr;
+  void* buf = nullptr;
+  size_t cap = 0;
+};
+
+std::mutex g_devices_mu;
+std::vector<std::unique_ptr<DeviceState>> g_devices;
+
+int current_device(int* dev) {
+  int n = 0;
+  cudaError_t err = cudaGetDeviceCount(&n);
+  if (err != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return fail(CFGMM_ERR_NO_DEVICE, "no CUDA device is visible");
+  }
+  CFGMM_CUDA(cudaGetDevice(dev));
+  return CFGMM_OK;
+}
+
+DeviceState* device_state(int dev) {
+  std::lock_guard<std::mutex> lk(g_devices_mu);
+  if (g_devices.size() <= size_t(dev)) g_devices.resize(dev + 1);
+  if (!g_devices[dev]) g_devices[dev].reset(new DeviceState);
+  return g_devices[dev].get();
+}
+
+// Grows the device's staging buffer to at least `bytes` (caller holds st->mu).
+int reserve(DeviceState* st, size_t bytes) {
+  if (!st->stream) CFGMM_CUDA(cudaStreamCreateWithFlags(&st->stream, cudaStreamNonBlocking));
+  if (st->cap >= bytes) return CFGMM_OK;
+  if (st->buf) {
+    CFGMM_CUDA(cudaFree(st->buf));
+    st->buf = nullptr;
+    st->cap = 0;
+  }
+  CFGMM_CUDA(cudaMalloc(&st->buf, bytes));
+  st->cap = bytes;
+  return CFGMM_OK;
+}
+
+size_t align256(size_t v) { return (v + 255) / 256 * 256; }
+
+// ---------------------------------------------------------------------------
+// DGEMM
+// ---------------------------------------------------------------------------
+struct GemmExtents {
+  size_t a, b, c;
+};
+
+int check_gemm(const double* c, size_t c_len, const double* a, size_t a_len, const double* b,
+               size_t b_len, size_t m, size_t n, size_t k, size_t lda, size_t ldb, size_t ldc,
+               bool ta, bool tb, GemmExtents* ex) {
+  if (m == 0 || n == 0 || k == 0) {
+    *ex = {0, 0, 0};
+    return CFGMM_OK;
+  }
+  if (!fits_int(m) || !fits_int(n) || !fits_int(k))
+    return fail(CFGMM_ERR_INVALID_ARGUMENT, "m, n and k must each be below 2^31");
+  if (ldc < n)
+    return fail(CFGMM_ERR_INVALID_ARGUMENT, "ldc < n: rows of C would overlap");
+  bool ok = (ta ? extent2(k, m, lda, &ex->a) : extent2(m, k, lda, &ex->a)) &&
+            (tb ? extent2(n, k, ldb, &ex->b) : extent2(k, n, ldb, &ex->b)) &&
+            extent2(m, n, ldc, &ex->c);
+  if (!ok) return fail(CFGMM_ERR_INVALID_ARGUMENT, "index range overflows usize");
+  if (a_len < ex->a || b_len < ex->b || c_len < ex->c) {
+    char msg[256];
+    std::snprintf(msg, sizeof(msg),
+                  "slice too short (a %zu < %zu, b %zu < %zu or c %zu < %zu): the reference "
+                  "panics here",
+                  a_len, ex->a, b_len, ex->b, c_len, ex->c);
+    return fail(CFGMM_ERR_INVALID_ARGUMENT, msg);
+  }
+  if (!a || !b || !c) return fail(CFGMM_ERR_INVALID_ARGUMENT, "null pointer");
+  return CFGMM_OK;
+}
+
+int check_precision(int precision) {
+  if (precision == CFGMM_PREC_FP64) return CFGMM_OK;
+  if (precision == CFGMM_PREC_OZAKI_INT8)
+    return fail(CFGMM_ERR_UNIMPLEMENTED, "CFGMM_PREC_OZAKI_INT8 is not available in this build");
+  return fail(CFGMM_ERR_INVALID_ARGUMENT, "unknown precision");
+}
+
+int gemm_host(double* c, size_t c_len, const double* a, size_t a_len, const double* b,
+              size_t b_len, size_t m, size_t n, size_t k, size_t lda, size_t ldb, size_t ldc,
+              uint8_t transa, uint8_t transb, int precision) {
+  g_last_error.clear();
+  GemmExtents ex;
+  int rc = check_gemm(c, c_len, a, a_len, b, b_len, m, n, k, lda, ldb, ldc, transa != 0,
+                      transb != 0, &ex);
+  if (rc != CFGMM_OK) return rc;
+  if ((rc = check_precision(precision)) != CFGMM_OK) return rc;
+  if (ex.c == 0) return CFGMM_OK;
+  int dev;
+  if ((rc = current_device(&dev)) != CFGMM_OK) return rc;
+  DeviceState* st = device_state(dev);
+  std::lock_guard<std::mutex> lk(st->mu);
+  const size_t oa = 0, ob = align256(ex.a * 8), oc = ob + align256(ex.b * 8);
+  if ((rc = reserve(st, oc + ex.c * 8)) != CFGMM_OK) return rc;
+  char* base = static_cast<char*>(st->buf);
+  double* da = reinterpret_cast<double*>(base + oa);
+  double* db = reinterpret_cast<double*>(base + ob);
+  double* dc = reinterpret_cast<double*>(base + oc);
+  CFGMM_CUDA(cudaMemcpyAsync(da, a, ex.a * 8, cudaMemcpyHostToDevice, st->stream));
+  CFGMM_CUDA(cudaMemcpyAsync(db, b, ex.b * 8, cudaMemcpyHostToDevice, st->stream));
+  CFGMM_CUDA(cudaMemcpyAsync(dc, c, ex.c * 8, cudaMemcpyHostToDevice, st->stream));
+  CFGMM_CUDA(cfgmm::dgemm_fp64(dc, da, db, int(m), int(n), int(k), lda, ldb, ldc, transa != 0,
+                               transb != 0, st->stream));
+  CFGMM_CUDA(cudaMemcpyAsync(c, dc, ex.c * 8, cudaMemcpyDeviceToHost, st->stream));
+  CFGMM_CUDA(cudaStreamSynchronize(st->stream));
+  return CFGMM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// AO-DM-AO
+// ---------------------------------------------------------------------------
+struct AodmExtents {
+  size_t rhos, dms, ao, tab;
+};
+
+int check_aodm(const double* rhos, size_t rhos_len, const double* dms, size_t dms_len,
+               const double* ao_lhs, size_t ao_lhs_len, const double* ao_rhs, size_t ao_rhs_len,
+               size_t stride_ao, size_t stride_grid, size_t nao, size_t ngrid, size_t nset,
+               const uint8_t* tab, size_t tab_len, size_t ldtab, size_t blksize,
+               AodmExtents* ex) {
+  if (blksize == 0)
+    return fail(CFGMM_ERR_INVALID_ARGUMENT, "BLKSIZE must be at least 1");
+  if (nao == 0 || ngrid == 0 || nset == 0) {
+    *ex = {0, 0, 0, 0};
+    return CFGMM_OK;
+  }
+  if (!fits_int(nao) || !fits_int(ngrid) || !fits_int(nset) || !fits_int(blksize))
+    return fail(CFGMM_ERR_INVALID_ARGUMENT, "nao, ngrid, nset and BLKSIZE must be below 2^31");
+  if (stride_grid < ngrid)
+    return fail(CFGMM_ERR_INVALID_ARGUMENT, "stride_grid < ngrid: rows of rho would overlap");
+  const size_t nblk = (ngrid + blksize - 1) / blksize;
+  size_t dm_stride, t;
+  bool ok = extent2(nset, ngrid, stride_grid, &ex->rhos) && extent2(nao, ngrid, stride_grid, &ex->ao) &&
+            extent2(nao, nblk, ldtab, &ex->tab) && mul_ok(stride_ao, stride_ao, &dm_stride) &&
+            extent2(nao, nao, stride_ao, &t) && mul_ok(nset - 1, dm_stride, &ex->dms) &&
+            add_ok(ex->dms, t, &ex->dms);
+  if (!ok) return fail(CFGMM_ERR_INVALID_ARGUMENT, "index range overflows usize");
+  if (rhos_len < ex->rhos || dms_len < ex->dms || ao_lhs_len < ex->ao || ao_rhs_len < ex->ao ||
+      tab_len < ex->tab) {
+    char msg[320];
+    std::snprintf(msg, sizeof(msg),
+                  "slice too short (rhos %zu/%zu, dms %zu/%zu, ao_lhs %zu/%zu, ao_rhs %zu/%zu, "
+                  "tab %zu/%zu): the reference panics here",
+                  rhos_len, ex->rhos, dms_len, ex->dms, ao_lhs_len, ex->ao, ao_rhs_len, ex->ao,
+                  tab_len, ex->tab);
+    return fail(CFGMM_ERR_INVALID_ARGUMENT, msg);
+  }
+  if (!rhos || !dms || !ao_lhs || !ao_rhs || !tab)
+    return fail(CFGMM_ERR_INVALID_ARGUMENT, "null pointer");
+  return CFGMM_OK;
+}
+
+int aodm_host(double* rhos, size_t rhos_len, const double* dms, size_t dms_len,
+              const double* ao_lhs, size_t ao_lhs_len, const double* ao_rhs, size_t ao_rhs_len,
+              size_t stride_ao, size_t stride_grid, size_t nao, size_t ngrid, size_t nset,
+              const uint8_t* tab, size_t tab_len, size_t ldtab, size_t blksize, int precision) {
+  g_last_error.clear();
+  AodmExtents ex;
+  int rc = check_aodm(rhos, rhos_len, dms, dms_len, ao_lhs, ao_lhs_len, ao_rhs, ao_rhs_len,
+                      stride_ao, stride_grid, nao, ngrid, nset, tab, tab_len, ldtab, blksize, &ex);
+  if (rc != CFGMM_OK) return rc;
+  if ((rc = check_precision(precision)) != CFGMM_OK) return rc;
+  if (ex.rhos == 0) return CFGMM_OK;
+  int dev;
+  if ((rc = current_device(&dev)) != CFGMM_OK) return rc;
+  DeviceState* st = device_state(dev);
+  std::lock_guard<std::mutex> lk(st->mu);
+  // ao_lhs and ao_rhs are usually the same table (rho = phi^T D phi): stage once.
+  const bool same_ao = ao_lhs == ao_rhs;
+  const size_t o_dms = 0;
+  const size_t o_lhs = o_dms + align256(ex.dms * 8);
+  const size_t o_rhs = o_lhs + align256(ex.ao * 8);
+  const size_t o_tab = o_rhs + (same_ao ? 0 : align256(ex.ao * 8));
+  const size_t o_rho = o_tab + align256(ex.tab);
+  const size_t o_ws = o_rho + align256(ex.rhos * 8);
+  const size_t ws = cfgmm::aodmao2rho_fp64_workspace(nao, ngrid, nset, blksize);
+  if ((rc = reserve(st, o_ws + ws)) != CFGMM_OK) return rc;
+  char* base = static_cast<char*>(st->buf);
+  double* d_dms = reinterpret_cast<double*>(base + o_dms);
+  double* d_lhs = reinterpret_cast<double*>(base + o_lhs);
+  double* d_rhs = reinterpret_cast<double*>(base + o_rhs);
+  uint8_t* d_tab = reinterpret_cast<uint8_t*>(base + o_tab);
+  double* d_rho = reinterpret_cast<double*>(base + o_rho);
+  CFGMM_CUDA(cudaMemcpyAsync(d_dms, dms, ex.dms * 8, cudaMemcpyHostToDevice, st->stream));
+  CFGMM_CUDA(cudaMemcpyAsync(d_lhs, ao_lhs, ex.ao * 8, cudaMemcpyHostToDevice, st->stream));
+  if (!same_ao)
+    CFGMM_CUDA(cudaMemcpyAsync(d_rhs, ao_rhs, ex.ao * 8, cudaMemcpyHostToDevice, st->stream));
+  CFGMM_CUDA(cudaMemcpyAsync(d_tab, tab, ex.tab, cudaMemcpyHostToDevice, st->stream));
+  CFGMM_CUDA(cudaMemcpyAsync(d_rho, rhos, ex.rhos * 8, cudaMemcpyHostToDevice, st->stream));
+  CFGMM_CUDA(cfgmm::aodmao2rho_fp64(d_rho, d_dms, d_lhs, same_ao ? d_lhs : d_rhs, stride_ao,
+                                    stride_grid, int(nao), int(ngrid), int(nset), d_tab, ldtab,
+                                    int(blksize), base + o_ws, st->stream));
+  CFGMM_CUDA(cudaMemcpyAsync(rhos, d_rho, ex.rhos * 8, cudaMemcpyDeviceToHost, st->stream));
+  CFGMM_CUDA(cudaStreamSynchronize(st->stream));
+  return CFGMM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cfgmm_status_string(int status) {
+  switch (status) {
+    case CFGMM_OK: return "success";
+    case CFGMM_ERR_INVALID_ARGUMENT: return "invalid argument (the reference would panic)";
+    case CFGMM_ERR_UNIMPLEMENTED: return "not implemented (the reference's unimplemented!)";
+    case CFGMM_ERR_CUDA: return "CUDA runtime error";
+    case CFGMM_ERR_NO_DEVICE: return "no CUDA device";
+    case CFGMM_ERR_OUT_OF_MEMORY: return "device out of memory";
+    case CFGMM_ERR_TIMEOUT: return "device-side wait timed out";
+    case CFGMM_ERR_BUSY: return "busy: request refused";
+    default: return "unknown status";
+  }
+}
+
+const char* cfgmm_last_error(void) { return g_last_error.c_str(); }
+
+int cfgmm_version(void) { return 100; }
+
+int cfgmm_matmul_loop_parallel_mnk_pack_a(double* c, size_t c_len, const double* a, size_t a_len,
+                                          const double* b, size_t b_len, size_t m, size_t n,
+                                          size_t k, size_t lda, size_t ldb, size_t ldc,
+                                          uint8_t transa, uint8_t transb) {
+  return gemm_host(c, c_len, a, a_len, b, b_len, m, n, k, lda, ldb, ldc, transa, transb,
+                   CFGMM_PREC_FP64);
+}
+
+int cfgmm_matmul_anyway_full(double* c, size_t c_len, const double* a, size_t a_len,
+                             const double* b, size_t b_len, size_t m, size_t n, size_t k,
+                             size_t lda, size_t ldb, size_t ldc, uint8_t transa, uint8_t transb) {
+  return gemm_host(c, c_len, a, a_len, b, b_len, m, n, k, lda, ldb, ldc, transa, transb,
+                   CFGMM_PREC_FP64);
+}
+
+int cfgmm_matmul_loop_macro_mb(double* c, size_t c_len, const double* a, size_t a_len,
+                               const double* b, size_t b_len, size_t m, size_t n, size_t k,
+                               size_t lda, size_t ldb, size_t ldc, uint8_t transa,
+                               uint8_t transb) {
+  return gemm_host(c, c_len, a, a_len, b, b_len, m, n, k, lda, ldb, ldc, transa, transb,
+                   CFGMM_PREC_FP64);
+}
+
+int cfgmm_matmul_ex(double* c, size_t c_len, const double* a, size_t a_len, const double* b,
+                    size_t b_len, size_t m, size_t n, size_t k, size_t lda, size_t ldb,
+                    size_t ldc, uint8_t transa, uint8_t transb, int precision) {
+  return gemm_host(c, c_len, a, a_len, b, b_len, m, n, k, lda, ldb, ldc, transa, transb,
+                   precision);
+}
+
+int cfgmm_matmul_dev(double* c, const double* a, const double* b, size_t m, size_t n, size_t k,
+                     size_t lda, size_t ldb, size_t ldc, uint8_t transa, uint8_t transb,
+                     int precision, void* stream) {
+  g_last_error.clear();
+  GemmExtents ex;
+  int rc = check_gemm(c, SIZE_MAX, a, SIZE_MAX, b, SIZE_MAX, m, n, k, lda, ldb, ldc, transa != 0,
+                      transb != 0, &ex);
+  if (rc != CFGMM_OK) return rc;
+  if ((rc = check_precision(precision)) != CFGMM_OK) return rc;
+  if (ex.c == 0) return CFGMM_OK;
+  int dev;
+  if ((rc = current_device(&dev)) != CFGMM_OK) return rc;
+  CFGMM_CUDA(cfgmm::dgemm_fp64(c, a, b, int(m), int(n), int(k), lda, ldb, ldc, transa != 0,
+                               transb != 0, static_cast<cudaStream_t>(stream)));
+  return CFGMM_OK;
+}
+
+int cfgmm_aodmao2rho_loop_parallel(double* rhos, size_t rhos_len, const double* dms,
+                                   size_t dms_len, const double* ao_lhs, size_t ao_lhs_len,
+                                   const double* ao_rhs, size_t ao_rhs_len, size_t stride_ao,
+                                   size_t stride_grid, size_t nao, size_t ngrid, size_t nset,
+                                   const uint8_t* tab, size_t tab_len, size_t ldtab,
+                                   size_t blksize) {
+  return aodm_host(rhos, rhos_len, dms, dms_len, ao_lhs, ao_lhs_len, ao_rhs, ao_rhs_len,
+                   stride_ao, stride_grid, nao, ngrid, nset, tab, tab_len, ldtab, blksize,
+                   CFGMM_PREC_FP64);
+}
+
+int cfgmm_aodmao2rho_anyway(double* rhos, size_t rhos_len, const double* dms, size_t dms_len,
+                            const double* ao_lhs, size_t ao_lhs_len, const double* ao_rhs,
+                            size_t ao_rhs_len, size_t stride_ao, size_t stride_grid, size_t nao,
+                            size_t ngrid, size_t nset, const uint8_t* tab, size_t tab_len,
+                            size_t ldtab) {
+  return aodm_host(rhos, rhos_len, dms, dms_len, ao_lhs, ao_lhs_len, ao_rhs, ao_rhs_len,
+                   stride_ao, stride_grid, nao, ngrid, nset, tab, tab_len, ldtab, 48,
+                   CFGMM_PREC_FP64);
+}
+
+int cfgmm_aodmao2rho_ex(double* rhos, size_t rhos_len, const double* dms, size_t dms_len,
+                        const double* ao_lhs, size_t ao_lhs_len, const double* ao_rhs,
+                        size_t ao_rhs_len, size_t stride_ao, size_t stride_grid, size_t nao,
+                        size_t ngrid, size_t nset, const uint8_t* tab, size_t tab_len,
+                        size_t ldtab, size_t blksize, int precision) {
+  return aodm_host(rhos, rhos_len, dms, dms_len, ao_lhs, ao_lhs_len, ao_rhs, ao_rhs_len,
+                   stride_ao, stride_grid, nao, ngrid, nset, tab, tab_len, ldtab, blksize,
+                   precision);
+}
+
+int cfgmm_aodmao2rho_dev(double* rhos, const double* dms, const double* ao_lhs,
+                         const double* ao_rhs, size_t stride_ao, size_t stride_grid, size_t nao,
+                         size_t ngrid, size_t nset, const uint8_t* tab, size_t ldtab,
+                         size_t blksize, int precision, void* stream) {
+  g_last_error.clear();
+  AodmExtents ex;
+  int rc = check_aodm(rhos, SIZE_MAX, dms, SIZE_MAX, ao_lhs, SIZE_MAX, ao_rhs, SIZE_MAX,
+                      stride_ao, stride_grid, nao, ngrid, nset, tab, SIZE_MAX, ldtab, blksize, &ex);
+  if (rc != CFGMM_OK) return rc;
+  if ((rc = check_precision(precision)) != CFGMM_OK) return rc;
+  if (ex.rhos == 0) return CFGMM_OK;
+  int dev;
+  if ((rc = current_device(&dev)) != CFGMM_OK) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // Stream-ordered scratch: safe against concurrent calls on other streams.
+  void* ws = nullptr;
+  const size_t bytes = cfgmm::aodmao2rho_fp64_workspace(nao, ngrid, nset, blksize);
+  CFGMM_CUDA(cudaMallocAsync(&ws, bytes, s));
+  cudaError_t err = cfgmm::aodmao2rho_fp64(rhos, dms, ao_lhs, ao_rhs, stride_ao, stride_grid,
+                                           int(nao), int(ngrid), int(nset), tab, ldtab,
+                                           int(blksize), ws, s);
+  cudaError_t err2 = cudaFreeAsync(ws, s);
+  if (err != cudaSuccess) return cuda_fail(err, "aodmao2rho_fp64");
+  if (err2 != cudaSuccess) return cuda_fail(err2, "cudaFreeAsync");
+  return CFGMM_OK;
+}
+
+int cfgmm_release_workspace(void) {
+  g_last_error.clear();
+  int dev;
+  int rc = current_device(&dev);
+  if (rc != CFGMM_OK) return rc;
+  DeviceState* st = device_state(dev);
+  std::lock_guard<std::mutex> lk(st->mu);
+  if (st->buf) CFGMM_CUDA(cudaFree(st->buf));
+  st->buf = nullptr;
+  st->cap = 0;
+  return CFGMM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,348 @@
+// aodmao2rho_fp64.cu -- masked AO-DM-AO contraction in FP64 on the FP64 tensor cores.
+//
+//   rho[s][g] += sum_{u in I(b)} ao_lhs[u][g] * sum_{v in I(b)} D_s[u][v] * ao_rhs[v][g],
+//   b = g / BLK,  I(b) = { u < nao : tab[u*ldtab + b] != 0 } in ascending order.
+//
+// Semantics follow MatmulLoops::aodmao2rho_loop_parallel
+// (src/impl_aodmao2rho.rs:171-244): the per-block active lists are exactly the
+// reference's compaction (get_indices_from_non0tab, impl_matmul_non0tab.rs:
+// 118-129, applied per block in impl_aodmao2rho.rs:126-133), a block with an
+// empty list is skipped, masked (AO, block) entries never contribute whatever
+// ao_lhs / ao_rhs hold there, and rho is accumulated into.
+//
+// Design:
+//   1. aodm_block_lists: one CTA per grid block builds I(b) on the device
+//      (ballot + popc prefix sums); no host round trip.
+//   2. aodm_fp64_kernel: one CTA per work item (block b, 64-point grid tile,
+//      64-row tile of I(b)) and group of up to 4 density matrices.  It forms
+//      X = D_s[I,I] * ao_rhs[I, tile] on the FP64 tensor cores (DMMA
+//      m16n8k4) with the gather done by 8-byte cp.async straight from the
+//      compacted index list -- no packed copy of D ever reaches HBM -- and
+//      then reduces phi_lhs (.) X over the 64 rows in registers, warp
+//      shuffles and shared memory, so X never leaves the SM.  The ao_rhs
+//      tile is shared by all density matrices of the group.
+//   3. aodm_reduce: adds the per-row-tile partial sums of each grid tile in a
+//      fixed order, so results are deterministic run to run (unlike the
+//      reference, whose lock order varies).
+#include "common.cuh"
+#include "aodmao2rho_fp64.cuh"
+
+namespace cfgmm {
+namespace {
+
+constexpr int TU = 64;   // compacted rows (u) per work item
+constexpr int TG = 64;   // grid points per work item
+constexpr int TK = 32;   // compacted v per pipeline stage
+constexpr int STAGES = 3;
+constexpr int THREADS = 256;
+
+// ---------------------------------------------------------------------------
+// 1. active lists: lists[b*nao + i] = i-th active AO of block b, counts[b]
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+aodm_block_lists(const uint8_t* __restrict__ tab, size_t ldtab, int nao, int nblk,
+                 int* __restrict__ lists, int* __restrict__ counts) {
+  const int b = blockIdx.x;
+  if (b >= nblk) return;
+  __shared__ int warp_tot[8];
+  __shared__ int base_s;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) base_s = 0;
+  __syncthreads();
+  int* out = lists + size_t(b) * nao;
+  for (int u0 = 0; u0 < nao; u0 += 256) {
+    const int u = u0 + tid;
+    const bool on = (u < nao) && tab[size_t(u) * ldtab + b] != 0;
+    const unsigned bal = __ballot_sync(0xffffffffu, on);
+    if (lane == 0) warp_tot[warp] = __popc(bal);
+    __syncthreads();
+    int before = base_s;
+    for (int w = 0; w < warp; ++w) before += warp_tot[w];
+    if (on) out[before + __popc(bal & ((1u << lane) - 1u))] = u;
+    __syncthreads();
+    if (tid == 0) {
+      int t = 0;
+      for (int w = 0; w < 8; ++w) t += warp_tot[w];
+      base_s += t;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) counts[b] = base_s;
+}
+
+// ---------------------------------------------------------------------------
+// 2. main kernel
+// ---------------------------------------------------------------------------
+struct AodmArgs {
+  const double* dms;
+  const double* ao_lhs;
+  const double* ao_rhs;
+  const int* lists;
+  const int* counts;
+  double* partial;  // [item][nset][TG]
+  size_t stride_ao, stride_grid, dm_stride;  // dm_stride = stride_ao^2
+  int nao, ngrid, nset, blk, gsub;           // gsub = grid tiles per block
+  int max_utiles;                            // row tiles per (block, grid tile) slot
+};
+
+template <int NS>
+__global__ void __launch_bounds__(THREADS, 1) aodm_fp64_kernel(AodmArgs p) {
+  extern __shared__ __align__(128) double smem[];
+  constexpr int D_TILE = TU * TK;  // one D tile per set
+  constexpr int P_TILE = TG * TK;  // ao_rhs tile, stored [g][k]
+  constexpr int STAGE = NS * D_TILE + P_TILE;
+
+  const int item = blockIdx.x;
+  const int set0 = blockIdx.y * NS;
+  const int utile = item % p.max_utiles;
+  const int bg = item / p.max_utiles;  // (block, grid tile)
+  const int b = bg / p.gsub, gt = bg % p.gsub;
+  const int nb = p.counts[b];
+  const int u0 = utile * TU;
+  if (u0 >= nb) return;
+  const int ns = min(NS, p.nset - set0);
+
+  const int g0 = b * p.blk + gt * TG;
+  const int gend = min(min((b + 1) * p.blk, p.ngrid), g0 + TG);
+  const int gw = gend - g0;
+  const int mu = min(TU, nb - u0);
+  const int* I = p.lists + size_t(b) * p.nao;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 2, wn = warp & 3;  // 2 x 4 warps; warp tile 32 (u) x 16 (g)
+  const int g = lane >> 2, q = lane & 3;
+
+  // D gather map: thread owns column c_d = tid % 32 and rows tid/32 + 8i.
+  const int c_d = tid & 31;
+  const int r_d0 = tid >> 5;
+  int urow[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int r = r_d0 + 8 * i;
+    urow[i] = (r < mu) ? I[u0 + r] : -1;
+  }
+  // ao_rhs gather map: thread owns grid column j_p = tid % 64 and k rows tid/64 + 4i.
+  const int j_p = tid & 63;
+  const int c_p0 = tid >> 6;
+  const bool jok = j_p < gw;
+
+  const int kchunks = (nb + TK - 1) / TK;
+  auto issue = [&](int kc) {
+    double* st = smem + (kc % STAGES) * STAGE;
+    const int k0 = kc * TK;
+    const int kw = min(TK, nb - k0);
+    const bool cok = c_d < kw;
+    const int vcol = cok ? I[k0 + c_d] : 0;
+    for (int s = 0; s < NS; ++s) {
+      double* Ds = st + s * D_TILE;
+      const bool sok = s < ns;
+      const double* dm = p.dms + size_t(set0 + (sok ? s : 0)) * p.dm_stride;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int r = r_d0 + 8 * i;
+        const bool ok = sok && cok && urow[i] >= 0;
+        const double* src = ok ? dm + size_t(urow[i]) * p.stride_ao + vcol : p.dms;
+        cp_async_8(Ds + swz<TK>(r, c_d), src, ok);
+      }
+    }
+    double* Ps = st + NS * D_TILE;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int c = c_p0 + 4 * i;
+      const bool ok = jok && c < kw;
+      const double* src = ok ? p.ao_rhs + size_t(I[k0 + c]) * p.stride_grid + (g0 + j_p) : p.ao_rhs;
+      cp_async_8(Ps + swz<TK>(j_p, c), src, ok);
+    }
+  };
+
+  double acc[NS][2][2][4];
+#pragma unroll
+  for (int s = 0; s < NS; ++s)
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[s][i][j][e] = 0.0;
+
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < kchunks) issue(s);
+    cp_async_commit();
+  }
+  for (int kc = 0; kc < kchunks; ++kc) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    if (kc + STAGES - 1 < kchunks) issue(kc + STAGES - 1);
+    cp_async_commit();
+
+    const double* st = smem + (kc % STAGES) * STAGE;
+    const double* Ps = st + NS * D_TILE;
+#pragma unroll
+    for (int kk = 0; kk < TK; kk += 8) {
+      double2 bv[2];
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt)
+        bv[nt] = *reinterpret_cast<const double2*>(Ps + swz<TK>(wn * 16 + nt * 8 + g, kk + 2 * q));
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const double* Ds = st + s * D_TILE;
+        double2 av[2][2];
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+          const int r = wm * 32 + mt * 16 + g;
+          av[mt][0] = *reinterpret_cast<const double2*>(Ds + swz<TK>(r, kk + 2 * q));
+          av[mt][1] = *reinterpret_cast<const double2*>(Ds + swz<TK>(r + 8, kk + 2 * q));
+        }
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+          for (int nt = 0; nt < 2; ++nt) {
+            dmma_16x8x4(acc[s][mt][nt], av[mt][0].x, av[mt][1].x, bv[nt].x);
+            dmma_16x8x4(acc[s][mt][nt], av[mt][0].y, av[mt][1].y, bv[nt].y);
+          }
+      }
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();  // stage buffers are reused below
+
+  // Epilogue: rho_part[s][j] = sum_r ao_lhs[I[u0+r]][g0+j] * X[s][r][j].
+  // Thread rows: r = wm*32 + mt*16 + g + 8h; columns j = wn*16 + nt*8 + 2q + e.
+  double lhs[2][2][2][2];  // [mt][h][nt][e]
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = wm * 32 + mt * 16 + g + 8 * h;
+      const bool rok = r < mu;
+      const double* row = rok ? p.ao_lhs + size_t(I[u0 + r]) * p.stride_grid : nullptr;
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int j = wn * 16 + nt * 8 + 2 * q + e;
+          lhs[mt][h][nt][e] = (rok && j < gw) ? row[g0 + j] : 0.0;
+        }
+    }
+  double* red = smem;  // [NS][2 (wm)][TG]
+#pragma unroll
+  for (int s = 0; s < NS; ++s)
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        double v = 0.0;
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) v = fma(acc[s][mt][nt][2 * h + e], lhs[mt][h][nt][e], v);
+        v += __shfl_xor_sync(0xffffffffu, v, 4);
+        v += __shfl_xor_sync(0xffffffffu, v, 8);
+        v += __shfl_xor_sync(0xffffffffu, v, 16);
+        if (g == 0) red[(s * 2 + wm) * TG + wn * 16 + nt * 8 + 2 * q + e] = v;
+      }
+  __syncthreads();
+  for (int t = tid; t < ns * TG; t += THREADS) {
+    const int s = t / TG, j = t % TG;
+    p.partial[(size_t(item) * p.nset + set0 + s) * TG + j] =
+        red[(s * 2 + 0) * TG + j] + red[(s * 2 + 1) * TG + j];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 3. deterministic reduction of the row-tile partials into rho
+// ---------------------------------------------------------------------------
+__global__ void aodm_reduce(double* __restrict__ rhos, const double* __restrict__ partial,
+                            const int* __restrict__ counts, size_t stride_grid, int ngrid,
+                            int nset, int blk, int gsub, int max_utiles, int nbg) {
+  const int bg = blockIdx.x;
+  if (bg >= nbg) return;
+  const int b = bg / gsub, gt = bg % gsub;
+  const int nt = (counts[b] + TU - 1) / TU;
+  if (nt == 0) return;  // fully masked block: rho untouched, as in the reference
+  const int g0 = b * blk + gt * TG;
+  const int gend = min(min((b + 1) * blk, ngrid), g0 + TG);
+  for (int t = threadIdx.x; t < nset * TG; t += blockDim.x) {
+    const int s = t / TG, j = t % TG;
+    if (g0 + j >= gend) continue;
+    double v = 0.0;
+    for (int u = 0; u < nt; ++u) v += partial[((size_t(bg) * max_utiles + u) * nset + s) * TG + j];
+    double* r = rhos + size_t(s) * stride_grid + g0 + j;
+    *r = v + *r;
+  }
+}
+
+template <int NS>
+cudaError_t launch_main(const AodmArgs& a, int nitems, int ngroups, cudaStream_t stream) {
+  constexpr size_t smem = size_t(STAGES) * (NS * TU * TK + TG * TK) * sizeof(double);
+  static_assert(NS * 2 * TG <= STAGES * (NS * TU * TK + TG * TK), "reduction buffer fits");
+  cudaError_t err = cudaFuncSetAttribute(aodm_fp64_kernel<NS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (err != cudaSuccess) return err;
+  aodm_fp64_kernel<NS><<<dim3(nitems, ngroups), THREADS, smem, stream>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t aodmao2rho_fp64_workspace(size_t nao, size_t ngrid, size_t nset, size_t blk) {
+  const size_t nblk = (ngrid + blk - 1) / blk;
+  const size_t gsub = (blk + TG - 1) / TG;
+  const size_t max_utiles = (nao + TU - 1) / TU;
+  size_t bytes = 0;
+  bytes += ((nblk * nao * sizeof(int)) + 255) / 256 * 256;        // lists
+  bytes += ((nblk * sizeof(int)) + 255) / 256 * 256;              // counts
+  bytes += nblk * gsub * max_utiles * nset * TG * sizeof(double);  // partials
+  return bytes;
+}
+
+cudaError_t aodmao2rho_fp64(double* rhos, const double* dms, const double* ao_lhs,
+                            const double* ao_rhs, size_t stride_ao, size_t stride_grid, int nao,
+                            int ngrid, int nset, const uint8_t* tab, size_t ldtab, int blk,
+                            void* workspace, cudaStream_t stream) {
+  if (nao <= 0 || ngrid <= 0 || nset <= 0) return cudaSuccess;
+  const int nblk = (ngrid + blk - 1) / blk;
+  const int gsub = (blk + TG - 1) / TG;
+  const int max_utiles = (nao + TU - 1) / TU;
+  char* ws = static_cast<char*>(workspace);
+  int* lists = reinterpret_cast<int*>(ws);
+  ws += ((size_t(nblk) * nao * sizeof(int)) + 255) / 256 * 256;
+  int* counts = reinterpret_cast<int*>(ws);
+  ws += ((size_t(nblk) * sizeof(int)) + 255) / 256 * 256;
+  double* partial = reinterpret_cast<double*>(ws);
+
+  aodm_block_lists<<<nblk, 256, 0, stream>>>(tab, ldtab, nao, nblk, lists, counts);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return err;
+
+  AodmArgs a;
+  a.dms = dms;
+  a.ao_lhs = ao_lhs;
+  a.ao_rhs = ao_rhs;
+  a.lists = lists;
+  a.counts = counts;
+  a.partial = partial;
+  a.stride_ao = stride_ao;
+  a.stride_grid = stride_grid;
+  a.dm_stride = stride_ao * stride_ao;
+  a.nao = nao;
+  a.ngrid = ngrid;
+  a.nset = nset;
+  a.blk = blk;
+  a.gsub = gsub;
+  a.max_utiles = max_utiles;
+  const int nbg = nblk * gsub;
+  const int nitems = nbg * max_utiles;
+  // Sets are processed in groups sharing one ao_rhs tile: 3 at a time (the
+  // register budget of the FP64 accumulators), the remainder in one group.
+  if (nset == 1) err = launch_main<1>(a, nitems, 1, stream);
+  else if (nset == 2) err = launch_main<2>(a, nitems, 1, stream);
+  else err = launch_main<3>(a, nitems, (nset + 2) / 3, stream);
+  if (err != cudaSuccess) return err;
+  aodm_reduce<<<nbg, 128, 0, stream>>>(rhos, partial, counts, stride_grid, ngrid, nset, blk, gsub,
+                                       max_utiles, nbg);
+  return cudaGetLastError();
+}
+
+}  // namespace cfgmm

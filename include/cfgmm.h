@@ -1,0 +1,154 @@
+/*
+ * cfgmm.h -- C ABI of libcfgmm.so, a B200 (sm_100a) implementation of the two
+ * data-parallel hot paths of cfgable-matmul:
+ *
+ *   1. the row-major blocked DGEMM   C += op(A) * op(B)
+ *   2. the non0tab-masked AO-DM-AO density contraction
+ *        rho[s][g] += sum_{u,v active in g's block} ao_lhs[u][g] * D_s[u][v] * ao_rhs[v][g]
+ *
+ * Every entry point keeps the argument order and meaning of the Rust function
+ * it replaces (cited per declaration, paths relative to the reference crate
+ * root).  A Rust `&[T]` / `&mut [T]` slice is passed as (pointer, length); a
+ * Rust `bool` is one byte holding 0 or 1, and `&[bool]` is `const uint8_t*`
+ * (any nonzero byte counts as true).  `usize` is `size_t`.
+ *
+ * Semantics shared by every entry point:
+ *   - Outputs are ACCUMULATED into (C += ..., rho += ...), exactly as in the
+ *     reference (impl_matmul.rs:31-46, impl_aodmao2rho.rs:77-92); the caller
+ *     zero-fills when it wants a plain product.
+ *   - Host-pointer entry points are synchronous and blocking, like the
+ *     reference's calls: inputs are copied to the current CUDA device, the
+ *     kernels run, the output is copied back, and the call returns.
+ *   - `_dev` entry points take device pointers and a cudaStream_t (passed as
+ *     void*, NULL = the legacy default stream) and only enqueue work; they do
+ *     not synchronize.
+ *   - Where the reference panics (a slice shorter than the index range it
+ *     reads or writes, `unimplemented!`, a failed `assert!`), the call returns
+ *     a negative status instead and touches no output.
+ *   - Zero-sized problems (m, n or k == 0; nao, ngrid or nset == 0) are valid
+ *     and leave the output unchanged, as in the reference.
+ *   - Calls are thread-safe: per-device workspaces are guarded internally.
+ *   - There is no CPU fallback.  Without a usable CUDA device a call returns
+ *     CFGMM_ERR_NO_DEVICE.
+ */
+#ifndef CFGMM_H
+#define CFGMM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define CFGMM_OK                    0
+#define CFGMM_ERR_INVALID_ARGUMENT (-1) /* reference would panic: slice too short, bad BLKSIZE, null */
+#define CFGMM_ERR_UNIMPLEMENTED    (-2) /* reference `unimplemented!` (masked GEMM with transb) */
+#define CFGMM_ERR_CUDA             (-3) /* CUDA runtime error; see cfgmm_last_error() */
+#define CFGMM_ERR_NO_DEVICE        (-4) /* no CUDA device visible */
+#define CFGMM_ERR_OUT_OF_MEMORY    (-5) /* device allocation failed */
+#define CFGMM_ERR_TIMEOUT          (-6) /* a bounded device-side wait gave up */
+#define CFGMM_ERR_BUSY             (-7) /* serving queue full / request refused by the HBM budget */
+
+/* ---- arithmetic of a call ---------------------------------------------- */
+#define CFGMM_PREC_FP64        0 /* FP64 tensor-core (DMMA) kernels */
+#define CFGMM_PREC_OZAKI_INT8  1 /* Ozaki-style INT8 split-precision kernels (tcgen05) */
+
+/* Short English description of a status code. */
+const char* cfgmm_status_string(int status);
+/* Detail of the last error raised on the calling thread ("" when none). */
+const char* cfgmm_last_error(void);
+/* Library version, major * 10000 + minor * 100 + patch. */
+int cfgmm_version(void);
+
+/* ======================================================================== */
+/* 1. DGEMM  C[i*ldc + j] += sum_p opA(i,p) * opB(p,j)                      */
+/*    opA(i,p) = transa ? a[p*lda + i] : a[i*lda + p]                       */
+/*    opB(p,j) = transb ? b[j*ldb + p] : b[p*ldb + j]                       */
+/* ======================================================================== */
+
+/* Replaces MatmulLoops::<T,MC,KC,NC,MR,NR_LANE,LANE>::matmul_loop_parallel_mnk_pack_a
+ * (src/impl_matmul.rs:155-167 signature, 155-231 body).  The CPU const
+ * generics have no meaning on the GPU: tiles are chosen by the library. */
+int cfgmm_matmul_loop_parallel_mnk_pack_a(double* c, size_t c_len, const double* a, size_t a_len,
+                                          const double* b, size_t b_len, size_t m, size_t n,
+                                          size_t k, size_t lda, size_t ldb, size_t ldc,
+                                          uint8_t transa, uint8_t transb);
+
+/* Replaces matmul_anyway_full (src/impl_matmul.rs:234-248): the same call with
+ * the reference's fixed Zen4 tuning; here identical to the entry point above. */
+int cfgmm_matmul_anyway_full(double* c, size_t c_len, const double* a, size_t a_len,
+                             const double* b, size_t b_len, size_t m, size_t n, size_t k,
+                             size_t lda, size_t ldb, size_t ldc, uint8_t transa, uint8_t transb);
+
+/* Replaces MatmulLoops::<f64,MC,KC,NC,MR,NR_LANE,LANE,MB>::matmul_loop_macro_mb as
+ * README.md:22-31 documents it (the function is named there but absent from
+ * the crate's sources).  Same semantics as matmul_loop_parallel_mnk_pack_a. */
+int cfgmm_matmul_loop_macro_mb(double* c, size_t c_len, const double* a, size_t a_len,
+                               const double* b, size_t b_len, size_t m, size_t n, size_t k,
+                               size_t lda, size_t ldb, size_t ldc, uint8_t transa,
+                               uint8_t transb);
+
+/* Host-pointer DGEMM with an explicit arithmetic (CFGMM_PREC_*).  With
+ * CFGMM_PREC_FP64 this is cfgmm_matmul_anyway_full. */
+int cfgmm_matmul_ex(double* c, size_t c_len, const double* a, size_t a_len, const double* b,
+                    size_t b_len, size_t m, size_t n, size_t k, size_t lda, size_t ldb,
+                    size_t ldc, uint8_t transa, uint8_t transb, int precision);
+
+/* Device-pointer DGEMM, enqueued on `stream` (cudaStream_t).  Same index
+ * semantics as above; the caller guarantees the extents. */
+int cfgmm_matmul_dev(double* c, const double* a, const double* b, size_t m, size_t n, size_t k,
+                     size_t lda, size_t ldb, size_t ldc, uint8_t transa, uint8_t transb,
+                     int precision, void* stream);
+
+/* ======================================================================== */
+/* 2. Masked AO-DM-AO contraction                                           */
+/*    rhos[s*stride_grid + g] += sum_{u,v: tab[u*ldtab + g/BLK] && tab[v*ldtab + g/BLK]}
+ *        ao_lhs[u*stride_grid + g] * dms[s*stride_ao^2 + u*stride_ao + v] * ao_rhs[v*stride_grid + g]
+ *    for s < nset, g < ngrid; strides = [stride_ao, stride_grid], shape = [nao, ngrid].
+ *    Masked (AO, block) entries are skipped whatever ao_lhs/ao_rhs hold there
+ *    (impl_aodmao2rho.rs:128-151).                                         */
+/* ======================================================================== */
+
+/* Replaces MatmulLoops::aodmao2rho_loop_parallel::<BLKSIZE>
+ * (src/impl_aodmao2rho.rs:171-181 signature, 171-244 body); BLKSIZE is the
+ * `blksize` argument.  Any blksize >= 1 is accepted (the reference's own
+ * constraints, BLKSIZE % 16 == 0 and NC % BLKSIZE == 0, stem from its CPU
+ * tiling and do not apply). */
+int cfgmm_aodmao2rho_loop_parallel(double* rhos, size_t rhos_len, const double* dms,
+                                   size_t dms_len, const double* ao_lhs, size_t ao_lhs_len,
+                                   const double* ao_rhs, size_t ao_rhs_len, size_t stride_ao,
+                                   size_t stride_grid, size_t nao, size_t ngrid, size_t nset,
+                                   const uint8_t* tab, size_t tab_len, size_t ldtab,
+                                   size_t blksize);
+
+/* Replaces aodmao2rho_anyway (src/impl_aodmao2rho.rs:247-261): BLKSIZE 48. */
+int cfgmm_aodmao2rho_anyway(double* rhos, size_t rhos_len, const double* dms, size_t dms_len,
+                            const double* ao_lhs, size_t ao_lhs_len, const double* ao_rhs,
+                            size_t ao_rhs_len, size_t stride_ao, size_t stride_grid, size_t nao,
+                            size_t ngrid, size_t nset, const uint8_t* tab, size_t tab_len,
+                            size_t ldtab);
+
+/* Host-pointer contraction with an explicit arithmetic (CFGMM_PREC_*). */
+int cfgmm_aodmao2rho_ex(double* rhos, size_t rhos_len, const double* dms, size_t dms_len,
+                        const double* ao_lhs, size_t ao_lhs_len, const double* ao_rhs,
+                        size_t ao_rhs_len, size_t stride_ao, size_t stride_grid, size_t nao,
+                        size_t ngrid, size_t nset, const uint8_t* tab, size_t tab_len,
+                        size_t ldtab, size_t blksize, int precision);
+
+/* Device-pointer contraction enqueued on `stream`; `tab` is a device pointer. */
+int cfgmm_aodmao2rho_dev(double* rhos, const double* dms, const double* ao_lhs,
+                         const double* ao_rhs, size_t stride_ao, size_t stride_grid, size_t nao,
+                         size_t ngrid, size_t nset, const uint8_t* tab, size_t ldtab,
+                         size_t blksize, int precision, void* stream);
+
+/* Releases the calling device's cached workspaces (they are otherwise kept
+ * and reused across calls until process exit). */
+int cfgmm_release_workspace(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CFGMM_H */

@@ -1,0 +1,128 @@
+"""CPU tests of the C-ABI boundary (libcfgmm.so): it loads, it exports every
+symbol include/*.h declares, and it rejects -- before touching any device --
+every call the reference would panic on.  No compute call is made here."""
+import ctypes
+import glob
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, has_cuda
+
+
+def _declared_symbols():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"\b(cfgmm_\w+)\s*\(", text))
+    return sorted(names)
+
+
+def test_library_builds_and_loads(cm):
+    lib = cm.lib()
+    assert os.path.exists(cm.library_path)
+    assert lib.cfgmm_version() >= 100
+
+
+def test_every_declared_symbol_is_exported(cm):
+    names = _declared_symbols()
+    assert len(names) >= 13
+    lib = ctypes.CDLL(cm.library_path)
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_status_strings(cm):
+    lib = cm.lib()
+    for rc in range(0, -8, -1):
+        assert lib.cfgmm_status_string(rc)
+    assert b"unknown" in lib.cfgmm_status_string(-99)
+
+
+def _gemm_args(m=4, n=5, k=6):
+    a = np.ones((m, k))
+    b = np.ones((k, n))
+    c = np.zeros((m, n))
+    return c, a, b
+
+
+def test_gemm_short_slice_is_rejected(cm):
+    c, a, b = _gemm_args()
+    with pytest.raises(ValueError, match="slice too short"):
+        cm.matmul_anyway_full(c, a[:3], b, 4, 5, 6, 6, 5, 5, False, False)
+    with pytest.raises(ValueError, match="slice too short"):
+        cm.matmul_anyway_full(c, a, b, 4, 5, 6, 7, 5, 5, False, False)  # lda 7 overruns A
+    with pytest.raises(ValueError, match="slice too short"):
+        cm.matmul_anyway_full(c[:2], a, b, 4, 5, 6, 6, 5, 5, False, False)
+    with pytest.raises(ValueError):
+        cm.matmul_anyway_full(c, a, b, 4, 5, 6, 6, 5, 4, False, False)  # ldc < n
+    assert np.all(c == 0)
+
+
+def test_gemm_zero_sizes_are_noops(cm):
+    # The reference's task loops are empty for m, n or k == 0: nothing is
+    # touched and no device is needed.
+    c, a, b = _gemm_args()
+    for m, n, k in ((0, 5, 6), (4, 0, 6), (4, 5, 0)):
+        cm.matmul_anyway_full(c, a, b, m, n, k, 6, 5, 5, False, False)
+    assert np.all(c == 0)
+
+
+def test_unknown_precision(cm):
+    c, a, b = _gemm_args()
+    with pytest.raises(ValueError, match="precision"):
+        cm.matmul_ex(c, a, b, 4, 5, 6, 6, 5, 5, False, False, precision=7)
+
+
+def _aodm_args(nao=10, ngrid=100, nset=2, blk=48):
+    nblk = -(-ngrid // blk)
+    rho = np.zeros((nset, ngrid))
+    dms = np.ones((nset, nao, nao))
+    ao = np.ones((nao, ngrid))
+    tab = np.ones((nao, nblk), np.uint8)
+    return rho, dms, ao, tab, nblk
+
+
+def test_aodm_validation(cm):
+    rho, dms, ao, tab, nblk = _aodm_args()
+    with pytest.raises(ValueError, match="slice too short"):
+        cm.aodmao2rho_anyway(rho, dms[:1], ao, ao, (10, 100), (10, 100), 2, tab, nblk)
+    with pytest.raises(ValueError, match="slice too short"):
+        cm.aodmao2rho_anyway(rho, dms, ao, ao, (10, 100), (10, 100), 2, tab[:5], nblk)
+    with pytest.raises(ValueError, match="slice too short"):
+        cm.aodmao2rho_anyway(rho[:1], dms, ao, ao, (10, 100), (10, 100), 2, tab, nblk)
+    with pytest.raises(ValueError, match="BLKSIZE"):
+        cm.aodmao2rho_ex(rho, dms, ao, ao, (10, 100), (10, 100), 2, tab, nblk, blksize=0)
+    with pytest.raises(ValueError, match="stride_grid"):
+        cm.aodmao2rho_anyway(rho, dms, ao, ao, (10, 50), (10, 100), 2, tab, nblk)
+    assert np.all(rho == 0)
+
+
+def test_aodm_zero_sizes_are_noops(cm):
+    rho, dms, ao, tab, nblk = _aodm_args()
+    cm.aodmao2rho_anyway(rho, dms, ao, ao, (10, 100), (0, 100), 2, tab, nblk)
+    cm.aodmao2rho_anyway(rho, dms, ao, ao, (10, 100), (10, 0), 2, tab, nblk)
+    cm.aodmao2rho_anyway(rho, dms, ao, ao, (10, 100), (10, 100), 0, tab, nblk)
+    assert np.all(rho == 0)
+
+
+def test_bool_mask_is_accepted(cm):
+    rho, dms, ao, tab, nblk = _aodm_args()
+    with pytest.raises(ValueError, match="slice too short"):
+        cm.aodmao2rho_anyway(rho, dms, ao, ao, (10, 100), (10, 100), 2, tab.astype(bool)[:3], nblk)
+
+
+@pytest.mark.skipif(has_cuda(), reason="checks the no-device path")
+def test_no_cpu_fallback_without_device(cm):
+    """A valid call on a machine without a GPU must fail loudly, not compute on the CPU."""
+    c, a, b = _gemm_args()
+    with pytest.raises(cm.CfgmmError) as e:
+        cm.matmul_anyway_full(c, a, b, 4, 5, 6, 6, 5, 5, False, False)
+    assert e.value.status == -4
+    rho, dms, ao, tab, nblk = _aodm_args()
+    with pytest.raises(cm.CfgmmError):
+        cm.aodmao2rho_anyway(rho, dms, ao, ao, (10, 100), (10, 100), 2, tab, nblk)
+    assert np.all(c == 0) and np.all(rho == 0)
