@@ -269,6 +269,12 @@ int aodm_host(double* rhos, size_t rhos_len, const double* dms, size_t dms_len,
 
 }  // namespace
 
+namespace cfgmm {
+// Lets entry points defined in other translation units report a detail
+// message through cfgmm_last_error().
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace cfgmm
+
 extern "C" {
 
 const char* cfgmm_status_string(int status) {

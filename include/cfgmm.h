@@ -143,6 +143,25 @@ int cfgmm_aodmao2rho_dev(double* rhos, const double* dms, const double* ao_lhs,
                          size_t ngrid, size_t nset, const uint8_t* tab, size_t ldtab,
                          size_t blksize, int precision, void* stream);
 
+/* No counterpart in the reference: an addition for callers that cannot
+ * allocate device memory -- a host that has given all of the GPU's memory to
+ * its own pool or arena, or code that must not call cudaMalloc/cudaFree (which
+ * can synchronise the whole device) inside a time-critical loop.
+ * Same arguments and result as cfgmm_aodmao2rho_dev with CFGMM_PREC_FP64, but
+ * the scratch it needs (per-block active AO lists, per-row-tile partial sums)
+ * lives in one fixed array of CFGMM_NOALLOC_SCRATCH_BYTES inside the library's
+ * device image, which every GPU that loads the library holds until exit; the
+ * call itself allocates nothing.  A problem whose scratch does not fit is
+ * refused with CFGMM_ERR_INVALID_ARGUMENT (the message gives the size it
+ * needs).  The first call on a device looks up that device's copy of the
+ * array; make that first call before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU race and must be ordered by the caller. */
+#define CFGMM_NOALLOC_SCRATCH_BYTES (32u << 20)
+int cfgmm_aodmao2rho_dev_noalloc(double* rhos, const double* dms, const double* ao_lhs,
+                                 const double* ao_rhs, size_t stride_ao, size_t stride_grid,
+                                 size_t nao, size_t ngrid, size_t nset, const uint8_t* tab,
+                                 size_t ldtab, size_t blksize, void* stream);
+
 /* Releases the calling device's cached workspaces (they are otherwise kept
  * and reused across calls until process exit). */
 int cfgmm_release_workspace(void);
