@@ -349,7 +349,7 @@ def run_ours(args, ranks: Ranks):
             "unit": "GFLOP/s", "ms_per_step": atot / args.steps,
             "flops_per_step": aflops, "flops": "sum_s sum_b (2|I_b|^2 + 2|I_b|)|b| (masked)",
             "frac_of_dmma_peak": (aflops / (atot / args.steps * 1e-3) / 1e12) / dmma_peak,
-            "launches_per_step": 3}
+            "launches_per_step": 4}
 
     cpu = cpu_dgemm_sample() if (ranks.rank == 0 and ranks.world == 1 and not args.no_cpu) else None
     out = {
@@ -381,6 +381,40 @@ def run_ours(args, ranks: Ranks):
         print(json.dumps(out), flush=True)
 
 
+def run_profile_case(args):
+    """Runs one kernel on one case `--reps` times and exits: the target of the
+    ncu captures summarised under profiles/ (prints nothing but a status line)."""
+    import torch
+    cm = importlib.import_module("cfgable-matmul_b200")
+    wl = importlib.import_module("cfgable-matmul_b200.workloads")
+    lib = cm.lib()
+    stream = torch.cuda.current_stream()
+    if args.profile == "dgemm":
+        m, n, k = args.m, args.n, args.k
+        g = torch.Generator(device="cuda").manual_seed(0)
+        a = torch.rand(m, k, dtype=torch.float64, device="cuda", generator=g)
+        b = torch.rand(k, n, dtype=torch.float64, device="cuda", generator=g)
+        c = torch.zeros(m, n, dtype=torch.float64, device="cuda")
+        for _ in range(args.reps):
+            rc = lib.cfgmm_matmul_dev(c.data_ptr(), a.data_ptr(), b.data_ptr(), m, n, k, k, n, n,
+                                      0, 0, cm.PREC_FP64, stream.cuda_stream)
+            assert rc == 0, rc
+    else:
+        p = wl.geometric(seed=0)
+        ao = torch.from_numpy(p.ao).cuda()
+        dms = torch.from_numpy(p.dms).cuda()
+        tab = torch.from_numpy(p.tab).cuda()
+        rho = torch.zeros(p.nset, p.ngrid, dtype=torch.float64, device="cuda")
+        for _ in range(args.reps):
+            rc = lib.cfgmm_aodmao2rho_dev(rho.data_ptr(), dms.data_ptr(), ao.data_ptr(),
+                                          ao.data_ptr(), p.nao, p.ngrid, p.nao, p.ngrid, p.nset,
+                                          tab.data_ptr(), p.nblk, p.blksize, cm.PREC_FP64,
+                                          stream.cuda_stream)
+            assert rc == 0, rc
+    torch.cuda.synchronize()
+    print(f"profile case {args.profile} done", flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -388,7 +422,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--profile", choices=["dgemm", "aodm"], default=None,
+                    help="run one kernel on one case (ncu target) and exit")
+    ap.add_argument("--m", type=int, default=4096)
+    ap.add_argument("--n", type=int, default=4096)
+    ap.add_argument("--k", type=int, default=4096)
+    ap.add_argument("--reps", type=int, default=3)
     args = ap.parse_args()
+    if args.profile:
+        run_profile_case(args)
+        return
     ranks = Ranks()
     if args.impl == "reference":
         run_reference(args, ranks)

@@ -13,15 +13,20 @@
 // Design:
 //   1. aodm_block_lists: one CTA per grid block builds I(b) on the device
 //      (ballot + popc prefix sums); no host round trip.
-//   2. aodm_fp64_kernel: one CTA per work item (block b, 64-point grid tile,
-//      64-row tile of I(b)) and group of up to 4 density matrices.  It forms
+//   2. aodm_build_items: one CTA turns the per-block counts into a compact
+//      work list (block b, 64-point grid tile, 64-row tile of I(b)) and resets
+//      the work counters.
+//   3. aodm_fp64_kernel: a persistent kernel, one CTA per SM and group of up
+//      to 3 density matrices, that draws work items from the list.  It forms
 //      X = D_s[I,I] * ao_rhs[I, tile] on the FP64 tensor cores (DMMA
 //      m16n8k4) with the gather done by 8-byte cp.async straight from the
 //      compacted index list -- no packed copy of D ever reaches HBM -- and
 //      then reduces phi_lhs (.) X over the 64 rows in registers, warp
 //      shuffles and shared memory, so X never leaves the SM.  The ao_rhs
 //      tile is shared by all density matrices of the group.
-//   3. aodm_reduce: adds the per-row-tile partial sums of each grid tile in a
+//      The active list of the current block is staged in shared memory, so
+//      the gather addresses never wait on global loads.
+//   4. aodm_reduce: adds the per-row-tile partial sums of each grid tile in a
 //      fixed order, so results are deterministic run to run (unlike the
 //      reference, whose lock order varies).
 #include "common.cuh"
@@ -35,6 +40,7 @@ constexpr int TG = 64;   // grid points per work item
 constexpr int TK = 32;   // compacted v per pipeline stage
 constexpr int STAGES = 3;
 constexpr int THREADS = 256;
+constexpr int LIST_CAP = 8192;  // active-list entries staged in shared memory
 
 // ---------------------------------------------------------------------------
 // 1. active lists: lists[b*nao + i] = i-th active AO of block b, counts[b]
@@ -71,7 +77,48 @@ aodm_block_lists(const uint8_t* __restrict__ tab, size_t ldtab, int nao, int nbl
 }
 
 // ---------------------------------------------------------------------------
-// 2. main kernel
+// 2. work list: items[i] = (b * gsub + gt, utile) for every row tile of every
+//    non-empty (block, grid tile), in block order; counters[g] = 0.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024)
+aodm_build_items(const int* __restrict__ counts, int nblk, int gsub, int2* __restrict__ items,
+                 int* __restrict__ counters, int ncounters) {
+  __shared__ int warp_tot[32];
+  __shared__ int base_s;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) base_s = 0;
+  for (int i = tid; i <= ncounters; i += 1024) counters[i] = 0;  // [ncounters] = total
+  __syncthreads();
+  for (int b0 = 0; b0 < nblk; b0 += 1024) {
+    const int b = b0 + tid;
+    const int nt = (b < nblk) ? (counts[b] + TU - 1) / TU : 0;
+    const int mine = nt * gsub;
+    // block-wide exclusive scan of `mine`
+    int incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    int before = base_s;
+    for (int w = 0; w < warp; ++w) before += warp_tot[w];
+    before += incl - mine;
+    for (int j = 0; j < mine; ++j) items[before + j] = make_int2(b * gsub + j / nt, j % nt);
+    __syncthreads();
+    if (tid == 0) {
+      int t = 0;
+      for (int w = 0; w < 32; ++w) t += warp_tot[w];
+      base_s += t;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) counters[ncounters] = base_s;
+}
+
+// ---------------------------------------------------------------------------
+// 3. main kernel
 // ---------------------------------------------------------------------------
 struct AodmArgs {
   const double* dms;
@@ -79,7 +126,10 @@ struct AodmArgs {
   const double* ao_rhs;
   const int* lists;
   const int* counts;
-  double* partial;  // [item][nset][TG]
+  const int2* items;  // work list (bg, utile)
+  int* counters;      // [ngroups] work counters, then the item total
+  int ngroups;
+  double* partial;  // [bg * max_utiles + utile][nset][TG]
   size_t stride_ao, stride_grid, dm_stride;  // dm_stride = stride_ao^2
   int nao, ngrid, nset, blk, gsub;           // gsub = grid tiles per block
   int max_utiles;                            // row tiles per (block, grid tile) slot
@@ -91,162 +141,185 @@ __global__ void __launch_bounds__(THREADS, 1) aodm_fp64_kernel(AodmArgs p) {
   constexpr int D_TILE = TU * TK;  // one D tile per set
   constexpr int P_TILE = TG * TK;  // ao_rhs tile, stored [g][k]
   constexpr int STAGE = NS * D_TILE + P_TILE;
+  int* list_s = reinterpret_cast<int*>(smem + STAGES * STAGE);  // LIST_CAP entries
+  __shared__ int item_s, blk_s;
 
-  const int item = blockIdx.x;
   const int set0 = blockIdx.y * NS;
-  const int utile = item % p.max_utiles;
-  const int bg = item / p.max_utiles;  // (block, grid tile)
-  const int b = bg / p.gsub, gt = bg % p.gsub;
-  const int nb = p.counts[b];
-  const int u0 = utile * TU;
-  if (u0 >= nb) return;
   const int ns = min(NS, p.nset - set0);
-
-  const int g0 = b * p.blk + gt * TG;
-  const int gend = min(min((b + 1) * p.blk, p.ngrid), g0 + TG);
-  const int gw = gend - g0;
-  const int mu = min(TU, nb - u0);
-  const int* I = p.lists + size_t(b) * p.nao;
+  const int total = p.counters[p.ngroups];
+  int* counter = p.counters + blockIdx.y;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 2, wn = warp & 3;  // 2 x 4 warps; warp tile 32 (u) x 16 (g)
   const int g = lane >> 2, q = lane & 3;
+  const int c_d = tid & 31, r_d0 = tid >> 5;  // D gather: column c_d, rows r_d0 + 8i
+  const int j_p = tid & 63, c_p0 = tid >> 6;  // ao_rhs gather: point j_p, k rows c_p0 + 4i
 
-  // D gather map: thread owns column c_d = tid % 32 and rows tid/32 + 8i.
-  const int c_d = tid & 31;
-  const int r_d0 = tid >> 5;
-  int urow[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int r = r_d0 + 8 * i;
-    urow[i] = (r < mu) ? I[u0 + r] : -1;
-  }
-  // ao_rhs gather map: thread owns grid column j_p = tid % 64 and k rows tid/64 + 4i.
-  const int j_p = tid & 63;
-  const int c_p0 = tid >> 6;
-  const bool jok = j_p < gw;
-
-  const int kchunks = (nb + TK - 1) / TK;
-  auto issue = [&](int kc) {
-    double* st = smem + (kc % STAGES) * STAGE;
-    const int k0 = kc * TK;
-    const int kw = min(TK, nb - k0);
-    const bool cok = c_d < kw;
-    const int vcol = cok ? I[k0 + c_d] : 0;
-    for (int s = 0; s < NS; ++s) {
-      double* Ds = st + s * D_TILE;
-      const bool sok = s < ns;
-      const double* dm = p.dms + size_t(set0 + (sok ? s : 0)) * p.dm_stride;
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int r = r_d0 + 8 * i;
-        const bool ok = sok && cok && urow[i] >= 0;
-        const double* src = ok ? dm + size_t(urow[i]) * p.stride_ao + vcol : p.dms;
-        cp_async_8(Ds + swz<TK>(r, c_d), src, ok);
-      }
+  if (tid == 0) blk_s = -1;
+  for (;;) {
+    if (tid == 0) item_s = atomicAdd(counter, 1);
+    __syncthreads();  // also orders this item's smem use after the previous one's
+    const int it = item_s;
+    if (it >= total) break;
+    const int2 w = p.items[it];
+    const int bg = w.x, utile = w.y;
+    const int b = bg / p.gsub, gt = bg % p.gsub;
+    const int nb = p.counts[b];
+    const int* Ig = p.lists + size_t(b) * p.nao;
+    const bool staged = nb <= LIST_CAP;
+    if (staged && blk_s != b) {  // stage the active list of block b once
+      for (int i = tid; i < nb; i += THREADS) list_s[i] = Ig[i];
+      __syncthreads();
+      if (tid == 0) blk_s = b;
     }
-    double* Ps = st + NS * D_TILE;
+    const int* I = staged ? list_s : Ig;
+    const int u0 = utile * TU;
+    const int g0 = b * p.blk + gt * TG;
+    const int gw = min(min((b + 1) * p.blk, p.ngrid), g0 + TG) - g0;
+    const int mu = min(TU, nb - u0);
+    const bool jok = j_p < gw;
+
+    int urow[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      const int c = c_p0 + 4 * i;
-      const bool ok = jok && c < kw;
-      const double* src = ok ? p.ao_rhs + size_t(I[k0 + c]) * p.stride_grid + (g0 + j_p) : p.ao_rhs;
-      cp_async_8(Ps + swz<TK>(j_p, c), src, ok);
+      const int r = r_d0 + 8 * i;
+      urow[i] = (r < mu) ? I[u0 + r] : -1;
     }
-  };
 
-  double acc[NS][2][2][4];
-#pragma unroll
-  for (int s = 0; s < NS; ++s)
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-      for (int j = 0; j < 2; ++j)
-#pragma unroll
-        for (int e = 0; e < 4; ++e) acc[s][i][j][e] = 0.0;
-
-#pragma unroll
-  for (int s = 0; s < STAGES - 1; ++s) {
-    if (s < kchunks) issue(s);
-    cp_async_commit();
-  }
-  for (int kc = 0; kc < kchunks; ++kc) {
-    cp_async_wait<STAGES - 2>();
-    __syncthreads();
-    if (kc + STAGES - 1 < kchunks) issue(kc + STAGES - 1);
-    cp_async_commit();
-
-    const double* st = smem + (kc % STAGES) * STAGE;
-    const double* Ps = st + NS * D_TILE;
-#pragma unroll
-    for (int kk = 0; kk < TK; kk += 8) {
-      double2 bv[2];
-#pragma unroll
-      for (int nt = 0; nt < 2; ++nt)
-        bv[nt] = *reinterpret_cast<const double2*>(Ps + swz<TK>(wn * 16 + nt * 8 + g, kk + 2 * q));
+    const int kchunks = (nb + TK - 1) / TK;
+    auto issue = [&](int kc) {
+      double* st = smem + (kc % STAGES) * STAGE;
+      const int k0 = kc * TK;
+      const int kw = min(TK, nb - k0);
+      const bool cok = c_d < kw;
+      const int vcol = cok ? I[k0 + c_d] : 0;
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
-        const double* Ds = st + s * D_TILE;
-        double2 av[2][2];
+        double* Ds = st + s * D_TILE;
+        const bool sok = s < ns;
+        const double* dm = p.dms + size_t(set0 + (sok ? s : 0)) * p.dm_stride;
 #pragma unroll
-        for (int mt = 0; mt < 2; ++mt) {
-          const int r = wm * 32 + mt * 16 + g;
-          av[mt][0] = *reinterpret_cast<const double2*>(Ds + swz<TK>(r, kk + 2 * q));
-          av[mt][1] = *reinterpret_cast<const double2*>(Ds + swz<TK>(r + 8, kk + 2 * q));
+        for (int i = 0; i < 8; ++i) {
+          const int r = r_d0 + 8 * i;
+          const bool ok = sok && cok && urow[i] >= 0;
+          const double* src = ok ? dm + size_t(urow[i]) * p.stride_ao + vcol : p.dms;
+          cp_async_8(Ds + swz<TK>(r, c_d), src, ok);
         }
+      }
+      double* Ps = st + NS * D_TILE;
 #pragma unroll
-        for (int mt = 0; mt < 2; ++mt)
+      for (int i = 0; i < 8; ++i) {
+        const int c = c_p0 + 4 * i;
+        const bool ok = jok && c < kw;
+        const double* src =
+            ok ? p.ao_rhs + size_t(I[k0 + c]) * p.stride_grid + (g0 + j_p) : p.ao_rhs;
+        cp_async_8(Ps + swz<TK>(j_p, c), src, ok);
+      }
+    };
+
+    double acc[NS][2][2][4];
 #pragma unroll
-          for (int nt = 0; nt < 2; ++nt) {
-            dmma_16x8x4(acc[s][mt][nt], av[mt][0].x, av[mt][1].x, bv[nt].x);
-            dmma_16x8x4(acc[s][mt][nt], av[mt][0].y, av[mt][1].y, bv[nt].y);
+    for (int s = 0; s < NS; ++s)
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) acc[s][i][j][e] = 0.0;
+
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) {
+      if (s < kchunks) issue(s);
+      cp_async_commit();
+    }
+    for (int kc = 0; kc < kchunks; ++kc) {
+      cp_async_wait<STAGES - 2>();
+      __syncthreads();
+      if (kc + STAGES - 1 < kchunks) issue(kc + STAGES - 1);
+      cp_async_commit();
+
+      const double* st = smem + (kc % STAGES) * STAGE;
+      const double* Ps = st + NS * D_TILE;
+#pragma unroll
+      for (int kk = 0; kk < TK; kk += 8) {
+        double2 bv[2];
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt)
+          bv[nt] = *reinterpret_cast<const double2*>(Ps + swz<TK>(wn * 16 + nt * 8 + g, kk + 2 * q));
+        double2 av[NS][2][2];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          const double* Ds = st + s * D_TILE;
+#pragma unroll
+          for (int mt = 0; mt < 2; ++mt) {
+            const int r = wm * 32 + mt * 16 + g;
+            av[s][mt][0] = *reinterpret_cast<const double2*>(Ds + swz<TK>(r, kk + 2 * q));
+            av[s][mt][1] = *reinterpret_cast<const double2*>(Ds + swz<TK>(r + 8, kk + 2 * q));
           }
+        }
+        // k-slot .x of every tile of every set, then .y: dependent DMMAs on one
+        // accumulator are 4*NS instructions apart.
+#pragma unroll
+        for (int s = 0; s < NS; ++s)
+#pragma unroll
+          for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt)
+              dmma_16x8x4(acc[s][mt][nt], av[s][mt][0].x, av[s][mt][1].x, bv[nt].x);
+#pragma unroll
+        for (int s = 0; s < NS; ++s)
+#pragma unroll
+          for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt)
+              dmma_16x8x4(acc[s][mt][nt], av[s][mt][0].y, av[s][mt][1].y, bv[nt].y);
       }
     }
-  }
-  cp_async_wait<0>();
-  __syncthreads();  // stage buffers are reused below
+    cp_async_wait<0>();
+    __syncthreads();  // stage buffers are reused below
 
-  // Epilogue: rho_part[s][j] = sum_r ao_lhs[I[u0+r]][g0+j] * X[s][r][j].
-  // Thread rows: r = wm*32 + mt*16 + g + 8h; columns j = wn*16 + nt*8 + 2q + e.
-  double lhs[2][2][2][2];  // [mt][h][nt][e]
+    // Epilogue: rho_part[s][j] = sum_r ao_lhs[I[u0+r]][g0+j] * X[s][r][j].
+    // Thread rows: r = wm*32 + mt*16 + g + 8h; columns j = wn*16 + nt*8 + 2q + e.
+    double lhs[2][2][2][2];  // [mt][h][nt][e]
 #pragma unroll
-  for (int mt = 0; mt < 2; ++mt)
+    for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int r = wm * 32 + mt * 16 + g + 8 * h;
-      const bool rok = r < mu;
-      const double* row = rok ? p.ao_lhs + size_t(I[u0 + r]) * p.stride_grid : nullptr;
+      for (int h = 0; h < 2; ++h) {
+        const int r = wm * 32 + mt * 16 + g + 8 * h;
+        const bool rok = r < mu;
+        const double* row = rok ? p.ao_lhs + size_t(I[u0 + r]) * p.stride_grid : nullptr;
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int j = wn * 16 + nt * 8 + 2 * q + e;
+            lhs[mt][h][nt][e] = (rok && j < gw) ? row[g0 + j] : 0.0;
+          }
+      }
+    double* red = smem;  // [NS][2 (wm)][TG]
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
 #pragma unroll
       for (int nt = 0; nt < 2; ++nt)
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
-          const int j = wn * 16 + nt * 8 + 2 * q + e;
-          lhs[mt][h][nt][e] = (rok && j < gw) ? row[g0 + j] : 0.0;
+          double v = 0.0;
+#pragma unroll
+          for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) v = fma(acc[s][mt][nt][2 * h + e], lhs[mt][h][nt][e], v);
+          v += __shfl_xor_sync(0xffffffffu, v, 4);
+          v += __shfl_xor_sync(0xffffffffu, v, 8);
+          v += __shfl_xor_sync(0xffffffffu, v, 16);
+          if (g == 0) red[(s * 2 + wm) * TG + wn * 16 + nt * 8 + 2 * q + e] = v;
         }
+    __syncthreads();
+    const size_t slot = size_t(bg) * p.max_utiles + utile;
+    for (int t = tid; t < ns * TG; t += THREADS) {
+      const int s = t / TG, j = t % TG;
+      p.partial[(slot * p.nset + set0 + s) * TG + j] = red[(s * 2 + 0) * TG + j] + red[(s * 2 + 1) * TG + j];
     }
-  double* red = smem;  // [NS][2 (wm)][TG]
-#pragma unroll
-  for (int s = 0; s < NS; ++s)
-#pragma unroll
-    for (int nt = 0; nt < 2; ++nt)
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        double v = 0.0;
-#pragma unroll
-        for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-          for (int h = 0; h < 2; ++h) v = fma(acc[s][mt][nt][2 * h + e], lhs[mt][h][nt][e], v);
-        v += __shfl_xor_sync(0xffffffffu, v, 4);
-        v += __shfl_xor_sync(0xffffffffu, v, 8);
-        v += __shfl_xor_sync(0xffffffffu, v, 16);
-        if (g == 0) red[(s * 2 + wm) * TG + wn * 16 + nt * 8 + 2 * q + e] = v;
-      }
-  __syncthreads();
-  for (int t = tid; t < ns * TG; t += THREADS) {
-    const int s = t / TG, j = t % TG;
-    p.partial[(size_t(item) * p.nset + set0 + s) * TG + j] =
-        red[(s * 2 + 0) * TG + j] + red[(s * 2 + 1) * TG + j];
+    // the __syncthreads at the top of the loop protects `red` and the stages
   }
 }
 
@@ -274,27 +347,48 @@ __global__ void aodm_reduce(double* __restrict__ rhos, const double* __restrict_
 }
 
 template <int NS>
-cudaError_t launch_main(const AodmArgs& a, int nitems, int ngroups, cudaStream_t stream) {
-  constexpr size_t smem = size_t(STAGES) * (NS * TU * TK + TG * TK) * sizeof(double);
+cudaError_t launch_main(const AodmArgs& a, int ngroups, cudaStream_t stream) {
+  constexpr size_t smem = size_t(STAGES) * (NS * TU * TK + TG * TK) * sizeof(double) +
+                          size_t(LIST_CAP) * sizeof(int);
   static_assert(NS * 2 * TG <= STAGES * (NS * TU * TK + TG * TK), "reduction buffer fits");
+  static_assert(smem <= 227 * 1024, "shared memory budget");
   cudaError_t err = cudaFuncSetAttribute(aodm_fp64_kernel<NS>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (err != cudaSuccess) return err;
-  aodm_fp64_kernel<NS><<<dim3(nitems, ngroups), THREADS, smem, stream>>>(a);
+  int dev = 0, nsm = 0;
+  if ((err = cudaGetDevice(&dev)) != cudaSuccess) return err;
+  if ((err = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+    return err;
+  aodm_fp64_kernel<NS><<<dim3(nsm, ngroups), THREADS, smem, stream>>>(a);
   return cudaGetLastError();
 }
 
 }  // namespace
 
-size_t aodmao2rho_fp64_workspace(size_t nao, size_t ngrid, size_t nset, size_t blk) {
+namespace {
+struct Layout {
+  size_t lists, counts, items, counters, partial, total;
+};
+
+Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk) {
   const size_t nblk = (ngrid + blk - 1) / blk;
   const size_t gsub = (blk + TG - 1) / TG;
   const size_t max_utiles = (nao + TU - 1) / TU;
-  size_t bytes = 0;
-  bytes += ((nblk * nao * sizeof(int)) + 255) / 256 * 256;        // lists
-  bytes += ((nblk * sizeof(int)) + 255) / 256 * 256;              // counts
-  bytes += nblk * gsub * max_utiles * nset * TG * sizeof(double);  // partials
-  return bytes;
+  const size_t ngroups = (nset + 2) / 3;
+  auto a256 = [](size_t v) { return (v + 255) / 256 * 256; };
+  Layout L;
+  L.lists = 0;
+  L.counts = L.lists + a256(nblk * nao * sizeof(int));
+  L.items = L.counts + a256(nblk * sizeof(int));
+  L.counters = L.items + a256(nblk * gsub * max_utiles * sizeof(int2));
+  L.partial = L.counters + a256((ngroups + 1) * sizeof(int));
+  L.total = L.partial + nblk * gsub * max_utiles * nset * TG * sizeof(double);
+  return L;
+}
+}  // namespace
+
+size_t aodmao2rho_fp64_workspace(size_t nao, size_t ngrid, size_t nset, size_t blk) {
+  return layout(nao, ngrid, nset, blk).total;
 }
 
 cudaError_t aodmao2rho_fp64(double* rhos, const double* dms, const double* ao_lhs,
@@ -305,16 +399,20 @@ cudaError_t aodmao2rho_fp64(double* rhos, const double* dms, const double* ao_lh
   const int nblk = (ngrid + blk - 1) / blk;
   const int gsub = (blk + TG - 1) / TG;
   const int max_utiles = (nao + TU - 1) / TU;
+  const int ngroups = (nset + 2) / 3;
+  const Layout L = layout(nao, ngrid, nset, blk);
   char* ws = static_cast<char*>(workspace);
-  int* lists = reinterpret_cast<int*>(ws);
-  ws += ((size_t(nblk) * nao * sizeof(int)) + 255) / 256 * 256;
-  int* counts = reinterpret_cast<int*>(ws);
-  ws += ((size_t(nblk) * sizeof(int)) + 255) / 256 * 256;
-  double* partial = reinterpret_cast<double*>(ws);
+  int* lists = reinterpret_cast<int*>(ws + L.lists);
+  int* counts = reinterpret_cast<int*>(ws + L.counts);
+  int2* items = reinterpret_cast<int2*>(ws + L.items);
+  int* counters = reinterpret_cast<int*>(ws + L.counters);
+  double* partial = reinterpret_cast<double*>(ws + L.partial);
 
   aodm_block_lists<<<nblk, 256, 0, stream>>>(tab, ldtab, nao, nblk, lists, counts);
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) return err;
+  aodm_build_items<<<1, 1024, 0, stream>>>(counts, nblk, gsub, items, counters, ngroups);
+  if ((err = cudaGetLastError()) != cudaSuccess) return err;
 
   AodmArgs a;
   a.dms = dms;
@@ -322,6 +420,9 @@ cudaError_t aodmao2rho_fp64(double* rhos, const double* dms, const double* ao_lh
   a.ao_rhs = ao_rhs;
   a.lists = lists;
   a.counts = counts;
+  a.items = items;
+  a.counters = counters;
+  a.ngroups = ngroups;
   a.partial = partial;
   a.stride_ao = stride_ao;
   a.stride_grid = stride_grid;
@@ -332,14 +433,13 @@ cudaError_t aodmao2rho_fp64(double* rhos, const double* dms, const double* ao_lh
   a.blk = blk;
   a.gsub = gsub;
   a.max_utiles = max_utiles;
-  const int nbg = nblk * gsub;
-  const int nitems = nbg * max_utiles;
   // Sets are processed in groups sharing one ao_rhs tile: 3 at a time (the
   // register budget of the FP64 accumulators), the remainder in one group.
-  if (nset == 1) err = launch_main<1>(a, nitems, 1, stream);
-  else if (nset == 2) err = launch_main<2>(a, nitems, 1, stream);
-  else err = launch_main<3>(a, nitems, (nset + 2) / 3, stream);
+  if (nset == 1) err = launch_main<1>(a, 1, stream);
+  else if (nset == 2) err = launch_main<2>(a, 1, stream);
+  else err = launch_main<3>(a, ngroups, stream);
   if (err != cudaSuccess) return err;
+  const int nbg = nblk * gsub;
   aodm_reduce<<<nbg, 128, 0, stream>>>(rhos, partial, counts, stride_grid, ngrid, nset, blk, gsub,
                                        max_utiles, nbg);
   return cudaGetLastError();

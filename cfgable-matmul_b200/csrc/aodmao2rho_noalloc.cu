@@ -18,8 +18,9 @@
 //
 // All calls share the one array and it keeps whatever the previous call left
 // in it.  Nothing in it needs to start at zero: the list kernel writes every
-// count and list entry the later kernels read, and the main kernel writes
-// every partial sum the reduction reads.  Two calls whose work overlaps on the
+// count and list entry the later kernels read, the work-list kernel writes the
+// work items and resets the work counters before the main kernel draws from
+// them, and the main kernel writes every partial sum the reduction reads.  Two calls whose work overlaps on the
 // GPU (different streams, or different host threads without ordering) race on
 // the array and may return wrong results; the caller must order them.
 #include <cuda_runtime.h>

@@ -44,13 +44,30 @@ __device__ __forceinline__ void dmma_16x8x4(double (&d)[4], double a0, double a1
       : "d"(a0), "d"(a1), "d"(b0));
 }
 
+// FP64 tensor-core MMA, D(16x8) += A(16x8) * B(8x8), row.col fragments:
+//   a0 = A[g][q], a1 = A[g+8][q], a2 = A[g][q+4], a3 = A[g+8][q+4],
+//   b0 = B[q][g], b1 = B[q+4][g], d as in dmma_16x8x4.
+__device__ __forceinline__ void dmma_16x8x8(double (&d)[4], double a0, double a1, double a2,
+                                            double a3, double b0, double b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
+}
+
 // Offset (in doubles) of element (row, col) of a shared-memory tile whose rows
 // hold `kRowDoubles` doubles (a multiple of 16), with the 16-byte chunks of
-// each row XOR-swizzled by (row & 7).  Fragment loads of 8 consecutive rows at
-// the same column pair then hit distinct bank groups.
+// each row XOR-swizzled.  A 16-byte fragment load of a warp (lane = 4g + q
+// reads row r0 + g, chunk c0 + q, r0 % 8 == 0) is served in four phases of 8
+// lanes = rows {2p, 2p+1}; the XOR key ((r&1)<<2 | (r>>1)&3) sends those two
+// rows to disjoint halves of the 8 bank groups, so every phase is one
+// conflict-free wavefront.
+__device__ __forceinline__ int swz_key(int row) { return ((row & 1) << 2) | ((row >> 1) & 3); }
+
 template <int kRowDoubles>
 __device__ __forceinline__ int swz(int row, int col) {
-  return row * kRowDoubles + ((((col >> 1) ^ (row & 7))) << 1) + (col & 1);
+  return row * kRowDoubles + (((col >> 1) ^ swz_key(row)) << 1) + (col & 1);
 }
 
 }  // namespace cfgmm

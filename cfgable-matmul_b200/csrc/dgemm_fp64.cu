@@ -8,60 +8,93 @@
 // Design (B200-first, not a translation of the CPU loops):
 //   * FP64 has no tcgen05 kind, so the math is the FP64 tensor-core MMA
 //     (DMMA, mma.sync m16n8k4 f64), fed from shared memory.
-//   * CTA tile 128x128, K step 16, 8 warps in a 2x4 grid (warp tile 64x32,
-//     4x4 MMA tiles, 64 FP64 accumulators per thread), 4-stage cp.async ring.
+//   * CTA tile 128x128, K step 32, 8 warps in a 2x4 grid (warp tile 64x32,
+//     4x4 m16n8k8 DMMA tiles, 64 FP64 accumulators per thread), 3-stage
+//     cp.async ring (192 KB shared memory, one CTA per SM).
 //   * Every operand tile is stored "K-contiguous" in shared memory
 //     (As[m][k], Bs[n][k]) whatever transa/transb are: the global->shared
 //     copies do the transposition, with the thread->element map chosen so that
 //     global reads stay coalesced for each transpose case.
 //   * 8-byte cp.async keeps any lda/ldb (odd ld, as in the 3527x6581x9583
 //     workload) and any base alignment legal; out-of-range elements are
-//     zero-filled, so edge tiles need no separate path.
+//     zero-filled, so edge tiles need no separate path.  Each thread's copy
+//     pointers are computed once and bumped per K step, and the copies of the
+//     next stage are spread between the DMMA groups of the current one, so
+//     the tensor pipe keeps issuing while they go out.
 //   * The k index inside each 8-wide group is permuted (thread q of a quad
-//     holds k = 2q and 2q+1), so each fragment load is one 16-byte
-//     shared-memory load; the same permutation is applied to A and B, which
-//     leaves the sum unchanged up to FP64 rounding order.
+//     holds k = 2q and 2q+1 as MMA k-slots q and q+4), so each fragment load
+//     is one 16-byte shared-memory load; the same permutation is applied to A
+//     and B, which leaves the sum unchanged up to FP64 rounding order.
 #include "common.cuh"
 #include "dgemm_fp64.cuh"
 
 namespace cfgmm {
 namespace {
 
-constexpr int BM = 128, BN = 128, BK = 16, STAGES = 4, THREADS = 256, GROUP_M = 8;
+constexpr int BM = 128, BN = 128, BK = 32, STAGES = 3, THREADS = 256, GROUP_M = 8;
 constexpr int TILE_DOUBLES = BM * BK;  // As or Bs per stage (BM == BN)
 constexpr size_t SMEM_BYTES = size_t(STAGES) * 2 * TILE_DOUBLES * sizeof(double);
+constexpr int CPT = TILE_DOUBLES / THREADS;  // copies per thread per operand tile (16)
 
-// Copies one BMxBK tile of op(X) (X = A, or B viewed as its transpose) into
-// shared memory as S[r][k], r < 128 rows of op(X) ("m" for A, "n" for B).
-//   kRowsContig: X's rows are the 128-dim (element (r,k) at x[r*ld + k], k
-//   contiguous); otherwise element (r,k) is at x[k*ld + r], r contiguous.
+// One thread's share of the copies of one 128 x BK operand tile into shared
+// memory as S[r][k] (r = row of op(X): m for A, n for B).
+//   kRowsContig: element (r,k) at x[r*ld + k] (k contiguous).  The thread copies
+//     k = tid % 32 of rows tid/32 + 8i: a warp reads 256 contiguous bytes.
+//   otherwise:   element (r,k) at x[k*ld + r] (r contiguous).  The thread copies
+//     r = tid % 128 of k = tid/128 + 2i: a warp reads 256 contiguous bytes.
 template <bool kRowsContig>
-__device__ __forceinline__ void load_tile(double* S, const double* x, size_t ld, int r0, int k0,
-                                          int rmax, int kmax, int tid) {
-  if (kRowsContig) {
-    // 16 threads sweep the 16 contiguous k of one row: 128-byte segments.
-    const int k = tid & 15;
-    const int rb = tid >> 4;
+struct TileCopier {
+  const double* src;     // element i = 0 of the current K step
+  size_t step_i;         // distance between consecutive elements i
+  size_t step_k;         // advance per K step
+  int dst0;              // shared offset of element 0 within a stage
+  unsigned row_ok;       // bit i: element i's row is inside the matrix
+  int kpos;              // k of element 0 relative to the K step
+  int key;               // swizzle key of the thread's row (kRowsContig = false)
+
+  __device__ __forceinline__ void init(const double* x, size_t ld, int r0, int rmax, int tid) {
+    if (kRowsContig) {
+      const int k = tid & 31, rb = tid >> 5;
+      src = x + size_t(r0 + rb) * ld + k;
+      step_i = 8 * ld;
+      step_k = BK;
+      dst0 = swz<BK>(rb, k);
+      row_ok = 0;
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int r = rb + 16 * i;
-      const bool ok = (r0 + r < rmax) && (k0 + k < kmax);
-      const double* src = ok ? x + size_t(r0 + r) * ld + (k0 + k) : x;
-      cp_async_8(S + swz<BK>(r, k), src, ok);
-    }
-  } else {
-    // 128 threads sweep the 128 contiguous r of one k: 1-KB segments.
-    const int r = tid & 127;
-    const int kb = tid >> 7;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int k = kb + 2 * i;
-      const bool ok = (r0 + r < rmax) && (k0 + k < kmax);
-      const double* src = ok ? x + size_t(k0 + k) * ld + (r0 + r) : x;
-      cp_async_8(S + swz<BK>(r, k), src, ok);
+      for (int i = 0; i < CPT; ++i) row_ok |= unsigned(r0 + rb + 8 * i < rmax) << i;
+      kpos = k;
+    } else {
+      const int r = tid & 127, kb = tid >> 7;
+      src = x + size_t(kb) * ld + (r0 + r);
+      step_i = 2 * ld;
+      step_k = size_t(BK) * ld;
+      key = swz_key(r);
+      dst0 = r * BK + kb;
+      row_ok = (r0 + r < rmax) ? 0xffffu : 0u;
+      kpos = kb;
     }
   }
-}
+
+  // Issues elements [i0, i0 + n) of K step `kt` into stage buffer S.
+  template <int i0, int n>
+  __device__ __forceinline__ void issue(double* S, int kt, int kmax) const {
+    const double* base = src + size_t(kt) * step_k;
+    const int krem = kmax - kt * BK - kpos;  // element ok while its k offset < krem
+#pragma unroll
+    for (int i = i0; i < i0 + n; ++i) {
+      bool ok;
+      int dst;
+      if (kRowsContig) {
+        ok = ((row_ok >> i) & 1u) && krem > 0;
+        dst = dst0 + i * 8 * BK;  // rows +8i keep the same swizzle key
+      } else {
+        ok = row_ok && 2 * i < krem;
+        dst = dst0 + ((i ^ key) << 1);  // k = kb + 2i: chunk i, half kb
+      }
+      cp_async_8(S + dst, ok ? base + size_t(i) * step_i : src, ok);
+    }
+  }
+};
 
 template <bool TA, bool TB>
 __global__ void __launch_bounds__(THREADS, 1)
@@ -89,6 +122,13 @@ dgemm_fp64_kernel(double* __restrict__ c, const double* __restrict__ a,
   const int n0 = (in_group / gsz) * BN;
   const int ktiles = (k + BK - 1) / BK;
 
+  // A: rows m, k contiguous unless transposed.  B: rows n, k contiguous only
+  // when transposed (b[j*ldb + p]).
+  TileCopier<!TA> ca;
+  TileCopier<TB> cb;
+  ca.init(a, lda, m0, m, tid);
+  cb.init(b, ldb, n0, n, tid);
+
   double acc[4][4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
@@ -97,25 +137,22 @@ dgemm_fp64_kernel(double* __restrict__ c, const double* __restrict__ a,
 #pragma unroll
       for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
 
-  // A: rows m, k contiguous unless transposed.  B: rows n, k contiguous only
-  // when transposed (b[j*ldb + p]).
-  auto issue = [&](int kt) {
-    const int st = kt % STAGES;
-    load_tile<!TA>(As + st * TILE_DOUBLES, a, lda, m0, kt * BK, m, k, tid);
-    load_tile<TB>(Bs + st * TILE_DOUBLES, b, ldb, n0, kt * BK, n, k, tid);
-  };
-
 #pragma unroll
   for (int s = 0; s < STAGES - 1; ++s) {
-    if (s < ktiles) issue(s);
+    if (s < ktiles) {
+      ca.issue<0, CPT>(As + s * TILE_DOUBLES, s, k);
+      cb.issue<0, CPT>(Bs + s * TILE_DOUBLES, s, k);
+    }
     cp_async_commit();
   }
 
   for (int kt = 0; kt < ktiles; ++kt) {
     cp_async_wait<STAGES - 2>();
     __syncthreads();
-    if (kt + STAGES - 1 < ktiles) issue(kt + STAGES - 1);
-    cp_async_commit();
+    const int nk = kt + STAGES - 1;  // K step whose copies go out during this one
+    const bool pre = nk < ktiles;
+    double* An = As + (nk % STAGES) * TILE_DOUBLES;
+    double* Bn = Bs + (nk % STAGES) * TILE_DOUBLES;
 
     const double* A_s = As + (kt % STAGES) * TILE_DOUBLES;
     const double* B_s = Bs + (kt % STAGES) * TILE_DOUBLES;
@@ -136,11 +173,18 @@ dgemm_fp64_kernel(double* __restrict__ c, const double* __restrict__ a,
 #pragma unroll
       for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
-          dmma_16x8x4(acc[mt][nt], av[mt][0].x, av[mt][1].x, bv[nt].x);
-          dmma_16x8x4(acc[mt][nt], av[mt][0].y, av[mt][1].y, bv[nt].y);
-        }
+        for (int nt = 0; nt < 4; ++nt)
+          dmma_16x8x8(acc[mt][nt], av[mt][0].x, av[mt][1].x, av[mt][0].y, av[mt][1].y, bv[nt].x,
+                      bv[nt].y);
+      // a quarter of the next stage's copies after each group of 16 DMMAs
+      if (pre) {
+        if (kk == 0) ca.template issue<0, CPT / 2>(An, nk, k);
+        if (kk == 8) ca.template issue<CPT / 2, CPT / 2>(An, nk, k);
+        if (kk == 16) cb.template issue<0, CPT / 2>(Bn, nk, k);
+        if (kk == 24) cb.template issue<CPT / 2, CPT / 2>(Bn, nk, k);
+      }
     }
+    cp_async_commit();
   }
   cp_async_wait<0>();
 

@@ -12,6 +12,7 @@ namespace {
 
 constexpr int kChains = 8;  // independent accumulators per warp
 
+template <int kChains>
 __global__ void __launch_bounds__(256) dmma_loop(double* out, int iters, double seed) {
   const int lane = threadIdx.x & 31;
   double a0 = seed + lane * 1e-3, a1 = seed - lane * 1e-3, b0 = 1.0 + lane * 1e-6;
@@ -84,7 +85,26 @@ double cfgmm_peak_dmma_tflops(int iters, int ctas_per_sm) {
   if (cudaMalloc(&out, 8) != cudaSuccess) return -1.0;
   const int grid = sm_count() * ctas_per_sm;
   const double flops = double(grid) * 8 /*warps*/ * iters * kChains * 2.0 * 16 * 8 * 4;
-  double r = time_kernel([&] { dmma_loop<<<grid, 256>>>(out, iters, 0.5); }, flops);
+  double r = time_kernel([&] { dmma_loop<kChains><<<grid, 256>>>(out, iters, 0.5); }, flops);
+  cudaFree(out);
+  return r;
+}
+
+// DMMA throughput with `chains` (4, 8 or 16) independent accumulators per warp,
+// `warps` (1..8) warps per CTA and `ctas_per_sm` CTAs per SM: how much
+// parallelism the FP64 tensor pipe needs.
+double cfgmm_peak_dmma_sweep(int iters, int ctas_per_sm, int warps, int chains) {
+  double* out = nullptr;
+  if (warps < 1 || warps > 8 || cudaMalloc(&out, 8) != cudaSuccess) return -1.0;
+  const int grid = sm_count() * ctas_per_sm;
+  const double flops = double(grid) * warps * iters * chains * 2.0 * 16 * 8 * 4;
+  double r = -1.0;
+  if (chains == 4)
+    r = time_kernel([&] { dmma_loop<4><<<grid, 32 * warps>>>(out, iters, 0.5); }, flops);
+  else if (chains == 8)
+    r = time_kernel([&] { dmma_loop<8><<<grid, 32 * warps>>>(out, iters, 0.5); }, flops);
+  else if (chains == 16)
+    r = time_kernel([&] { dmma_loop<16><<<grid, 32 * warps>>>(out, iters, 0.5); }, flops);
   cudaFree(out);
   return r;
 }
