@@ -19,6 +19,8 @@
 #include "../../include/cfgmm.h"
 #include "aodmao2rho_fp64.cuh"
 #include "dgemm_fp64.cuh"
+#include "gemm_i8.cuh"
+#include "ozaki.cuh"
 
 namespace {
 
@@ -142,10 +144,27 @@ int check_gemm(const double* c, size_t c_len, const double* a, size_t a_len, con
 }
 
 int check_precision(int precision) {
-  if (precision == CFGMM_PREC_FP64) return CFGMM_OK;
-  if (precision == CFGMM_PREC_OZAKI_INT8)
-    return fail(CFGMM_ERR_UNIMPLEMENTED, "CFGMM_PREC_OZAKI_INT8 is not available in this build");
+  if (precision == CFGMM_PREC_FP64 || precision == CFGMM_PREC_OZAKI_INT8) return CFGMM_OK;
   return fail(CFGMM_ERR_INVALID_ARGUMENT, "unknown precision");
+}
+
+int check_split_gemm(size_t k) {
+  if (k > size_t(cfgmm::kOzakiMaxK))
+    return fail(CFGMM_ERR_UNIMPLEMENTED,
+                "CFGMM_PREC_OZAKI_INT8 supports k <= 65536 (exact INT32 accumulation)");
+  return CFGMM_OK;
+}
+
+// Reads the sticky error word of the tcgen05 kernels after a synchronised call.
+int check_device_waits() {
+  int code = 0;
+  CFGMM_CUDA(cfgmm::gemm_i8_read_error(&code));
+  if (code != 0) {
+    char msg[128];
+    std::snprintf(msg, sizeof(msg), "a tensor-core pipeline wait timed out (code %d)", code);
+    return fail(CFGMM_ERR_TIMEOUT, msg);
+  }
+  return CFGMM_OK;
 }
 
 int gemm_host(double* c, size_t c_len, const double* a, size_t a_len, const double* b,
@@ -158,12 +177,17 @@ int gemm_host(double* c, size_t c_len, const double* a, size_t a_len, const doub
   if (rc != CFGMM_OK) return rc;
   if ((rc = check_precision(precision)) != CFGMM_OK) return rc;
   if (ex.c == 0) return CFGMM_OK;
+  const bool split = precision == CFGMM_PREC_OZAKI_INT8;
+  if (split && (rc = check_split_gemm(k)) != CFGMM_OK) return rc;
   int dev;
   if ((rc = current_device(&dev)) != CFGMM_OK) return rc;
   DeviceState* st = device_state(dev);
   std::lock_guard<std::mutex> lk(st->mu);
+  const int nmod = split ? cfgmm::ozaki_default_moduli(int(k)) : 0;
   const size_t oa = 0, ob = align256(ex.a * 8), oc = ob + align256(ex.b * 8);
-  if ((rc = reserve(st, oc + ex.c * 8)) != CFGMM_OK) return rc;
+  const size_t ows = oc + align256(ex.c * 8);
+  const size_t wsb = split ? cfgmm::ozaki_dgemm_workspace(int(m), int(n), int(k), nmod) : 0;
+  if ((rc = reserve(st, ows + wsb)) != CFGMM_OK) return rc;
   char* base = static_cast<char*>(st->buf);
   double* da = reinterpret_cast<double*>(base + oa);
   double* db = reinterpret_cast<double*>(base + ob);
@@ -171,10 +195,17 @@ int gemm_host(double* c, size_t c_len, const double* a, size_t a_len, const doub
   CFGMM_CUDA(cudaMemcpyAsync(da, a, ex.a * 8, cudaMemcpyHostToDevice, st->stream));
   CFGMM_CUDA(cudaMemcpyAsync(db, b, ex.b * 8, cudaMemcpyHostToDevice, st->stream));
   CFGMM_CUDA(cudaMemcpyAsync(dc, c, ex.c * 8, cudaMemcpyHostToDevice, st->stream));
-  CFGMM_CUDA(cfgmm::dgemm_fp64(dc, da, db, int(m), int(n), int(k), lda, ldb, ldc, transa != 0,
-                               transb != 0, st->stream));
+  if (split) {
+    CFGMM_CUDA(cfgmm::gemm_i8_reset_error(st->stream));
+    CFGMM_CUDA(cfgmm::ozaki_dgemm(dc, da, db, int(m), int(n), int(k), lda, ldb, ldc, transa != 0,
+                                  transb != 0, nmod, base + ows, st->stream));
+  } else {
+    CFGMM_CUDA(cfgmm::dgemm_fp64(dc, da, db, int(m), int(n), int(k), lda, ldb, ldc, transa != 0,
+                                 transb != 0, st->stream));
+  }
   CFGMM_CUDA(cudaMemcpyAsync(c, dc, ex.c * 8, cudaMemcpyDeviceToHost, st->stream));
   CFGMM_CUDA(cudaStreamSynchronize(st->stream));
+  if (split) return check_device_waits();
   return CFGMM_OK;
 }
 
@@ -232,6 +263,8 @@ int aodm_host(double* rhos, size_t rhos_len, const double* dms, size_t dms_len,
                       stride_ao, stride_grid, nao, ngrid, nset, tab, tab_len, ldtab, blksize, &ex);
   if (rc != CFGMM_OK) return rc;
   if ((rc = check_precision(precision)) != CFGMM_OK) return rc;
+  if (precision != CFGMM_PREC_FP64)
+    return fail(CFGMM_ERR_UNIMPLEMENTED, "split precision for the AO-DM-AO contraction");
   if (ex.rhos == 0) return CFGMM_OK;
   int dev;
   if ((rc = current_device(&dev)) != CFGMM_OK) return rc;
@@ -337,8 +370,21 @@ int cfgmm_matmul_dev(double* c, const double* a, const double* b, size_t m, size
   if (ex.c == 0) return CFGMM_OK;
   int dev;
   if ((rc = current_device(&dev)) != CFGMM_OK) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (precision == CFGMM_PREC_OZAKI_INT8) {
+    if ((rc = check_split_gemm(k)) != CFGMM_OK) return rc;
+    const int nmod = cfgmm::ozaki_default_moduli(int(k));
+    void* ws = nullptr;
+    CFGMM_CUDA(cudaMallocAsync(&ws, cfgmm::ozaki_dgemm_workspace(int(m), int(n), int(k), nmod), s));
+    cudaError_t err = cfgmm::ozaki_dgemm(c, a, b, int(m), int(n), int(k), lda, ldb, ldc,
+                                         transa != 0, transb != 0, nmod, ws, s);
+    cudaError_t err2 = cudaFreeAsync(ws, s);
+    if (err != cudaSuccess) return cuda_fail(err, "ozaki_dgemm");
+    if (err2 != cudaSuccess) return cuda_fail(err2, "cudaFreeAsync");
+    return CFGMM_OK;
+  }
   CFGMM_CUDA(cfgmm::dgemm_fp64(c, a, b, int(m), int(n), int(k), lda, ldb, ldc, transa != 0,
-                               transb != 0, static_cast<cudaStream_t>(stream)));
+                               transb != 0, s));
   return CFGMM_OK;
 }
 
@@ -383,6 +429,8 @@ int cfgmm_aodmao2rho_dev(double* rhos, const double* dms, const double* ao_lhs,
                       stride_ao, stride_grid, nao, ngrid, nset, tab, SIZE_MAX, ldtab, blksize, &ex);
   if (rc != CFGMM_OK) return rc;
   if ((rc = check_precision(precision)) != CFGMM_OK) return rc;
+  if (precision != CFGMM_PREC_FP64)
+    return fail(CFGMM_ERR_UNIMPLEMENTED, "split precision for the AO-DM-AO contraction");
   if (ex.rhos == 0) return CFGMM_OK;
   int dev;
   if ((rc = current_device(&dev)) != CFGMM_OK) return rc;

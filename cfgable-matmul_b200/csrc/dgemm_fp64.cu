@@ -140,8 +140,8 @@ dgemm_fp64_kernel(double* __restrict__ c, const double* __restrict__ a,
 #pragma unroll
   for (int s = 0; s < STAGES - 1; ++s) {
     if (s < ktiles) {
-      ca.issue<0, CPT>(As + s * TILE_DOUBLES, s, k);
-      cb.issue<0, CPT>(Bs + s * TILE_DOUBLES, s, k);
+      ca.template issue<0, CPT>(As + s * TILE_DOUBLES, s, k);
+      cb.template issue<0, CPT>(Bs + s * TILE_DOUBLES, s, k);
     }
     cp_async_commit();
   }

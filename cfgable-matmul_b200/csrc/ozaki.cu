@@ -1,0 +1,457 @@
+// ozaki.cu -- FP64 GEMM emulated on the INT8 tensor cores by the Ozaki
+// scheme in its Chinese-remainder form ("Ozaki scheme II": Ozaki, Uchino and
+// Imamura, 2024/2025), restated here from the mathematics:
+//
+//   1. scaling: row i of op(A) is multiplied by 2^e_i and column j of op(B)
+//      by 2^f_j and rounded to integers A', B' with |A'| <= 2^alpha,
+//      |B'| <= 2^beta, where k 2^(alpha+beta) <= M/8 and M = prod m_l;
+//   2. residues: A'_l = A' mods m_l, B'_l = B' mods m_l (int8) for N pairwise
+//      coprime moduli m_l <= 256;
+//   3. N exact INT8 GEMMs C_l = A'_l B'_l (INT32 in TMEM, gemm_i8.cu), each
+//      reduced to r_l = C_l mods m_l in its epilogue;
+//   4. reconstruction: C' = A'B' is the unique integer with |C'| < M/2 and
+//      C' = r_l (mod m_l): C' = sum_l r_l w_l - q M with the CRT weights w_l and
+//      q = round(sum_l r_l w_l / M).  Evaluated in FP64 with each w_l and M
+//      split at 2^T into a high part (exact products and sums, < 2^53) and a
+//      low part, so C' comes out with one rounding; C = C' 2^-(e_i + f_j).
+//
+// The only error is the rounding of A and B to alpha / beta bits relative to
+// their row / column maxima; the number of moduli sets alpha and beta.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <mutex>
+
+#include "gemm_i8.cuh"
+#include "ozaki.cuh"
+
+namespace cfgmm {
+
+// Pairwise coprime moduli, largest first (256 = 2^8, 255 = 3*5*17,
+// 253 = 11*23, 247 = 13*19, 217 = 7*31, the rest prime).
+static const int kModuli[kMaxModuli] = {256, 255, 253, 251, 247, 241, 239, 233,
+                                        229, 227, 223, 217, 211, 199, 197, 193};
+
+namespace {
+
+using u128 = unsigned __int128;
+
+int bit_length(u128 v) {
+  int n = 0;
+  while (v) {
+    ++n;
+    v >>= 1;
+  }
+  return n;
+}
+
+long long mod_inverse(long long a, long long m) {  // a^-1 mod m, gcd(a, m) = 1
+  long long t = 0, nt = 1, r = m, nr = a % m;
+  while (nr) {
+    const long long qq = r / nr;
+    long long tmp = t - qq * nt;
+    t = nt;
+    nt = tmp;
+    tmp = r - qq * nr;
+    r = nr;
+    nr = tmp;
+  }
+  return t < 0 ? t + m : t;
+}
+
+int ceil_log2(long long v) {
+  int n = 0;
+  while ((1LL << n) < v) ++n;
+  return n;
+}
+
+}  // namespace
+
+OzakiPlan ozaki_plan(int k, int nmod, int min_bits) {
+  OzakiPlan p{};
+  if (nmod <= 0) {
+    // smallest N whose operand precision reaches min_bits
+    for (nmod = 2; nmod < kMaxModuli; ++nmod) {
+      OzakiPlan t = ozaki_plan(k, nmod, min_bits);
+      if (t.alpha >= min_bits && t.beta >= min_bits) break;
+    }
+  }
+  if (nmod > kMaxModuli) nmod = kMaxModuli;
+  p.nmod = nmod;
+  u128 M = 1;
+  for (int l = 0; l < nmod; ++l) M *= u128(kModuli[l]);
+  const int logM = bit_length(M) - 1;  // floor(log2 M)
+  const int P = logM - 3 - ceil_log2(k > 1 ? k : 2);
+  p.alpha = P / 2;
+  p.beta = P - p.alpha;
+  // split point T: sum_l |r_l| hi_l + |q| H < 2^53 with |r_l| <= 128, |q| <= 128 N
+  const int T = std::max(0, logM + 1 + 7 + ceil_log2(nmod + 1) + 1 - 52);
+  p.two_T = std::ldexp(1.0, T);
+  const u128 lo_mask = (T >= 128) ? ~u128(0) : ((u128(1) << T) - 1);
+  const double Md = double(M);
+  for (int l = 0; l < nmod; ++l) {
+    const long long m = kModuli[l];
+    const u128 Ml = M / u128(m);
+    const long long inv = mod_inverse(static_cast<long long>(Ml % u128(m)), m);
+    const u128 w = Ml * u128(inv);  // < M
+    p.mod[l] = int(m);
+    p.inv_f[l] = 1.0f / float(m);
+    p.inv_d[l] = 1.0 / double(m);
+    p.w_frac[l] = double(w) / Md;
+    p.w_hi[l] = double(w >> T);
+    p.w_lo[l] = double(w & lo_mask);
+  }
+  p.M_hi = double(M >> T);
+  p.M_lo = double(M & lo_mask);
+  return p;
+}
+
+namespace {
+
+constexpr int kNonFinite = INT_MAX;  // exponent sentinel of a row holding Inf/NaN
+
+// ---------------------------------------------------------------------------
+// exponents: e[r] = bits - E_r with max_p |x(r,p)| < 2^E_r  (0 for a zero row)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int scale_exponent(double amax, int bits) {
+  if (!(amax <= 1.7976931348623157e308)) return kNonFinite;  // Inf or NaN
+  if (amax == 0.0) return 0;
+  int E;
+  frexp(amax, &E);  // amax = f 2^E, f in [0.5, 1): amax < 2^E
+  return bits - E;
+}
+
+// element (r, p) at x[r*ld + p]: one CTA per row
+__global__ void __launch_bounds__(256)
+exps_rows(const double* __restrict__ x, size_t ld, int rows, int k, int bits, int* __restrict__ e) {
+  const int r = blockIdx.x;
+  if (r >= rows) return;
+  const double* row = x + size_t(r) * ld;
+  double mx = 0.0;
+  bool bad = false;
+  for (int p = threadIdx.x; p < k; p += 256) {
+    const double v = fabs(row[p]);
+    bad |= !(v <= 1.7976931348623157e308);
+    mx = fmax(mx, v);
+  }
+  __shared__ double red[8];
+  __shared__ int badw[8];
+  for (int o = 16; o > 0; o >>= 1) {
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    bad |= __shfl_xor_sync(0xffffffffu, int(bad), o) != 0;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[threadIdx.x >> 5] = mx;
+    badw[threadIdx.x >> 5] = bad;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    int b = 0;
+    for (int w = 0; w < 8; ++w) {
+      m = fmax(m, red[w]);
+      b |= badw[w];
+    }
+    e[r] = b ? kNonFinite : scale_exponent(m, bits);
+  }
+}
+
+// element (r, p) at x[p*ld + r]: one thread per r, coalesced over r
+__global__ void __launch_bounds__(256)
+exps_cols(const double* __restrict__ x, size_t ld, int rows, int k, int bits, int* __restrict__ e) {
+  const int r = blockIdx.x * 256 + threadIdx.x;
+  if (r >= rows) return;
+  double mx = 0.0;
+  bool bad = false;
+  for (int p = 0; p < k; ++p) {
+    const double v = fabs(x[size_t(p) * ld + r]);
+    bad |= !(v <= 1.7976931348623157e308);
+    mx = fmax(mx, v);
+  }
+  e[r] = bad ? kNonFinite : scale_exponent(mx, bits);
+}
+
+// ---------------------------------------------------------------------------
+// residues: Y[l][r][p] = rint(x(r,p) 2^e[r]) mods m_l  (int8), p < k
+// ---------------------------------------------------------------------------
+struct ResidueArgs {
+  int nmod;
+  int mod[kMaxModuli];
+  double inv[kMaxModuli];
+};
+
+__device__ __forceinline__ int8_t mods(double v, int m, double inv) {
+  const double q = rint(v * inv);
+  double r = fma(-double(m), q, v);  // exact: |m q| < 2^53
+  const int hi = (m - 1) >> 1, lo = -(m >> 1);
+  if (r > hi) r -= m;
+  else if (r < lo) r += m;
+  return int8_t(int(r));
+}
+
+__device__ __forceinline__ double scaled_int(double x, int e) {
+  return (e == kNonFinite) ? 0.0 : rint(ldexp(x, e));
+}
+
+__device__ __forceinline__ void write_residues(const ResidueArgs& a, int8_t* Y, size_t plane,
+                                               size_t off, const double (&v)[4]) {
+  // modulus 256: the low byte of the two's-complement integer
+  {
+    char4 c;
+    c.x = int8_t(static_cast<long long>(v[0]));
+    c.y = int8_t(static_cast<long long>(v[1]));
+    c.z = int8_t(static_cast<long long>(v[2]));
+    c.w = int8_t(static_cast<long long>(v[3]));
+    *reinterpret_cast<char4*>(Y + off) = c;
+  }
+  for (int l = 1; l < a.nmod; ++l) {
+    const int m = a.mod[l];
+    const double inv = a.inv[l];
+    char4 c;
+    c.x = mods(v[0], m, inv);
+    c.y = mods(v[1], m, inv);
+    c.z = mods(v[2], m, inv);
+    c.w = mods(v[3], m, inv);
+    *reinterpret_cast<char4*>(Y + size_t(l) * plane + off) = c;
+  }
+}
+
+// element (r, p) at x[r*ld + p]: CTA per row, thread per 4 consecutive p
+__global__ void __launch_bounds__(256)
+residues_rows(const double* __restrict__ x, size_t ld, int rows, int k, size_t kpad,
+              const int* __restrict__ e, int8_t* __restrict__ Y, ResidueArgs a) {
+  const int r = blockIdx.x;
+  if (r >= rows) return;
+  const int er = e[r];
+  const double* row = x + size_t(r) * ld;
+  const size_t plane = size_t(rows) * kpad;
+  for (int p = 4 * threadIdx.x; p < k; p += 4 * 256) {
+    double v[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) v[j] = (p + j < k) ? scaled_int(row[p + j], er) : 0.0;
+    write_residues(a, Y, plane, size_t(r) * kpad + p, v);
+  }
+}
+
+// element (r, p) at x[p*ld + r]: 32 (r) x 64 (p) tiles transposed through shared memory
+__global__ void __launch_bounds__(256)
+residues_cols(const double* __restrict__ x, size_t ld, int rows, int k, size_t kpad,
+              const int* __restrict__ e, int8_t* __restrict__ Y, ResidueArgs a) {
+  __shared__ double tile[64][33];
+  const int r0 = blockIdx.x * 32, p0 = blockIdx.y * 64;
+  const int tr = threadIdx.x & 31, tp = threadIdx.x >> 5;  // 8 rows of p per pass
+  for (int pp = tp; pp < 64; pp += 8) {
+    const int p = p0 + pp, r = r0 + tr;
+    tile[pp][tr] = (p < k && r < rows) ? x[size_t(p) * ld + r] : 0.0;
+  }
+  __syncthreads();
+  const size_t plane = size_t(rows) * kpad;
+  // 32 rows x 16 groups of 4 p = 512 units, 2 per thread
+  for (int u = threadIdx.x; u < 512; u += 256) {
+    const int rr = u >> 4, pg = (u & 15) * 4;
+    const int r = r0 + rr, p = p0 + pg;
+    if (r >= rows || p >= k) continue;
+    const int er = e[r];
+    double v[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) v[j] = (p + j < k) ? scaled_int(tile[pg + j][rr], er) : 0.0;
+    write_residues(a, Y, plane, size_t(r) * kpad + p, v);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// reconstruction: C[i][j] += 2^-(e_i + f_j) * CRT(r_0..r_{N-1})
+// ---------------------------------------------------------------------------
+struct ReconArgs {
+  int nmod;
+  double w_frac[kMaxModuli], w_hi[kMaxModuli], w_lo[kMaxModuli];
+  double M_hi, M_lo, two_T;
+};
+
+__global__ void __launch_bounds__(256)
+reconstruct(double* __restrict__ c, size_t ldc, int m, int n, const int8_t* __restrict__ R,
+            size_t ldr, const int* __restrict__ ea, const int* __restrict__ eb, ReconArgs a) {
+  const int bpr = (n + 1023) / 1024;  // CTAs per row of C
+  const int i = blockIdx.x / bpr;
+  const int j0 = ((blockIdx.x % bpr) * 256 + threadIdx.x) * 4;
+  if (j0 >= n || i >= m) return;
+  const size_t plane = size_t(m) * ldr;
+  const int8_t* Ri = R + size_t(i) * ldr + j0;
+  double t[4] = {0, 0, 0, 0}, X[4] = {0, 0, 0, 0}, Y[4] = {0, 0, 0, 0};
+  for (int l = 0; l < a.nmod; ++l) {
+    const char4 r4 = *reinterpret_cast<const char4*>(Ri + size_t(l) * plane);
+    const double rv[4] = {double(r4.x), double(r4.y), double(r4.z), double(r4.w)};
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      t[u] = fma(rv[u], a.w_frac[l], t[u]);
+      X[u] = fma(rv[u], a.w_hi[l], X[u]);  // exact: every partial sum < 2^53
+      Y[u] = fma(rv[u], a.w_lo[l], Y[u]);
+    }
+  }
+  const int ei = ea[i];
+  double* ci = c + size_t(i) * ldc;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int j = j0 + u;
+    if (j >= n) break;
+    const int fj = eb[j];
+    const double q = rint(t[u]);
+    const double hi = fma(-q, a.M_hi, X[u]);  // exact
+    const double lo = fma(-q, a.M_lo, Y[u]);
+    const double cp = fma(hi, a.two_T, lo);   // C' with one rounding
+    const double val = (ei == kNonFinite || fj == kNonFinite) ? __longlong_as_double(0x7ff8000000000000LL)
+                                                              : ldexp(cp, -(ei + fj));
+    ci[j] += val;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// tensor maps
+// ---------------------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  });
+  return fn;
+}
+
+bool make_plane_map(CUtensorMap* map, void* base, int k, int rows, int nplanes, size_t kpad,
+                    int box_rows) {
+  auto enc = encode_fn();
+  if (!enc) return false;
+  cuuint64_t dims[3] = {cuuint64_t(k), cuuint64_t(rows), cuuint64_t(nplanes)};
+  cuuint64_t strides[2] = {cuuint64_t(kpad), cuuint64_t(rows) * kpad};
+  cuuint32_t box[3] = {128, cuuint32_t(box_rows), 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+size_t a256(size_t v) { return (v + 255) / 256 * 256; }
+
+struct DgemmLayout {
+  size_t kpad, ldr, a_res, b_res, r, ea, eb, total;
+};
+
+DgemmLayout dgemm_layout(int m, int n, int k, int nmod) {
+  DgemmLayout L;
+  L.kpad = (size_t(k) + 127) / 128 * 128;
+  L.ldr = (size_t(n) + 15) / 16 * 16;
+  L.a_res = 0;
+  L.b_res = L.a_res + a256(size_t(nmod) * m * L.kpad);
+  L.r = L.b_res + a256(size_t(nmod) * n * L.kpad);
+  L.ea = L.r + a256(size_t(nmod) * m * L.ldr);
+  L.eb = L.ea + a256(size_t(m) * sizeof(int));
+  L.total = L.eb + a256(size_t(n) * sizeof(int));
+  return L;
+}
+
+ResidueArgs residue_args(const OzakiPlan& p) {
+  ResidueArgs a{};
+  a.nmod = p.nmod;
+  for (int l = 0; l < p.nmod; ++l) {
+    a.mod[l] = p.mod[l];
+    a.inv[l] = p.inv_d[l];
+  }
+  return a;
+}
+
+// Scales, rounds and splits op(X) into residue planes Y[nmod][rows][kpad].
+cudaError_t prepare(const double* x, size_t ld, bool rows_contig, int rows, int k, size_t kpad,
+                    int bits, int* e, int8_t* Y, const ResidueArgs& ra, cudaStream_t s) {
+  if (rows_contig) {
+    exps_rows<<<rows, 256, 0, s>>>(x, ld, rows, k, bits, e);
+    residues_rows<<<rows, 256, 0, s>>>(x, ld, rows, k, kpad, e, Y, ra);
+  } else {
+    exps_cols<<<(rows + 255) / 256, 256, 0, s>>>(x, ld, rows, k, bits, e);
+    dim3 grid((rows + 31) / 32, (k + 63) / 64);
+    residues_cols<<<grid, 256, 0, s>>>(x, ld, rows, k, kpad, e, Y, ra);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+int ozaki_default_moduli(int k) {
+  const char* env = std::getenv("CFGMM_OZAKI_MODULI");
+  if (env) {
+    const int v = std::atoi(env);
+    if (v >= 2 && v <= kMaxModuli) return v;
+  }
+  return ozaki_plan(k, 0, kOzakiMinBits).nmod;
+}
+
+size_t ozaki_dgemm_workspace(int m, int n, int k, int nmod) {
+  return dgemm_layout(m, n, k, nmod).total;
+}
+
+cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int n, int k,
+                        size_t lda, size_t ldb, size_t ldc, bool transa, bool transb, int nmod,
+                        void* workspace, cudaStream_t stream) {
+  if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
+  if (k > kOzakiMaxK) return cudaErrorInvalidValue;
+  const OzakiPlan plan = ozaki_plan(k, nmod, 0);
+  const DgemmLayout L = dgemm_layout(m, n, k, plan.nmod);
+  char* ws = static_cast<char*>(workspace);
+  int8_t* a_res = reinterpret_cast<int8_t*>(ws + L.a_res);
+  int8_t* b_res = reinterpret_cast<int8_t*>(ws + L.b_res);
+  int8_t* r = reinterpret_cast<int8_t*>(ws + L.r);
+  int* ea = reinterpret_cast<int*>(ws + L.ea);
+  int* eb = reinterpret_cast<int*>(ws + L.eb);
+  const ResidueArgs ra = residue_args(plan);
+  // op(A) rows are i (k contiguous unless transa); op(B) "rows" are j
+  // (k contiguous only when transb).
+  cudaError_t err = prepare(a, lda, !transa, m, k, L.kpad, plan.alpha, ea, a_res, ra, stream);
+  if (err != cudaSuccess) return err;
+  err = prepare(b, ldb, transb, n, k, L.kpad, plan.beta, eb, b_res, ra, stream);
+  if (err != cudaSuccess) return err;
+
+  CUtensorMap tmA, tmB;
+  if (!make_plane_map(&tmA, a_res, k, m, plan.nmod, L.kpad, gemm_i8_tile_rows_a()) ||
+      !make_plane_map(&tmB, b_res, k, n, plan.nmod, L.kpad, gemm_i8_tile_rows_b()))
+    return cudaErrorInvalidValue;
+  GemmI8Args g{};
+  g.rows_a = m;
+  g.rows_b = n;
+  g.k = k;
+  g.nmod = plan.nmod;
+  g.out = r;
+  g.ldr = L.ldr;
+  for (int l = 0; l < plan.nmod; ++l) {
+    g.mod[l] = plan.mod[l];
+    g.inv[l] = plan.inv_f[l];
+  }
+  if ((err = gemm_i8_mod(tmA, tmB, g, stream)) != cudaSuccess) return err;
+
+  ReconArgs rc{};
+  rc.nmod = plan.nmod;
+  for (int l = 0; l < plan.nmod; ++l) {
+    rc.w_frac[l] = plan.w_frac[l];
+    rc.w_hi[l] = plan.w_hi[l];
+    rc.w_lo[l] = plan.w_lo[l];
+  }
+  rc.M_hi = plan.M_hi;
+  rc.M_lo = plan.M_lo;
+  rc.two_T = plan.two_T;
+  const long long rgrid = (long long)((n + 1023) / 1024) * m;
+  if (rgrid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+  reconstruct<<<unsigned(rgrid), 256, 0, stream>>>(c, ldc, m, n, r, L.ldr, ea, eb, rc);
+  return cudaGetLastError();
+}
+
+}  // namespace cfgmm

@@ -1,0 +1,45 @@
+// ozaki.cuh -- internal interface of the Ozaki-scheme split-precision paths.
+#pragma once
+#include <cstddef>
+#include <cuda_runtime.h>
+
+#include "gemm_i8.cuh"
+
+namespace cfgmm {
+
+// Exact INT32 accumulation needs k * 128 * 128 < 2^31; the epilogue's
+// float-quotient reduction is exact (after two corrections) for |acc| < 2^30.
+constexpr int kOzakiMaxK = 65536;
+// Default operand precision (bits kept relative to each row / column max).
+constexpr int kOzakiMinBits = 45;
+
+struct OzakiPlan {
+  int nmod;             // number of moduli N
+  int alpha, beta;      // bits of the scaled integer operands A', B'
+  int mod[kMaxModuli];  // moduli, 256 first
+  float inv_f[kMaxModuli];
+  double inv_d[kMaxModuli];
+  // CRT weights w_l (sum_l r_l w_l = C' mod M), split at 2^T:
+  double w_frac[kMaxModuli];  // w_l / M
+  double w_hi[kMaxModuli];    // w_l >> T (exact)
+  double w_lo[kMaxModuli];    // w_l mod 2^T (rounded)
+  double M_hi, M_lo, two_T;   // M >> T, M mod 2^T, 2^T
+};
+
+// Plan for contraction length k with `nmod` moduli (<= 0: the fewest moduli
+// that keep min_bits bits of both operands).
+OzakiPlan ozaki_plan(int k, int nmod, int min_bits);
+
+// Moduli used for contraction length k (environment CFGMM_OZAKI_MODULI
+// overrides, 2..16).
+int ozaki_default_moduli(int k);
+
+size_t ozaki_dgemm_workspace(int m, int n, int k, int nmod);
+
+// C[i*ldc+j] += sum_p opA(i,p) opB(p,j) by INT8 tensor-core emulation; device
+// pointers; workspace of ozaki_dgemm_workspace bytes (256-byte aligned).
+cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int n, int k,
+                        size_t lda, size_t ldb, size_t ldc, bool transa, bool transb, int nmod,
+                        void* workspace, cudaStream_t stream);
+
+}  // namespace cfgmm

@@ -8,6 +8,8 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 
+#include "../tcgen05.cuh"
+
 namespace {
 
 constexpr int kChains = 8;  // independent accumulators per warp
@@ -75,9 +77,67 @@ int sm_count() {
   return n;
 }
 
+__device__ int g_peak_err;
+
+// tcgen05.mma kind::i8, M=128 N=256 K=32, issued back to back by one thread
+// on operands resident in shared memory (zeros), accumulating in TMEM.
+__global__ void __launch_bounds__(128, 1) i8_mma_loop(int iters) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                             ~uintptr_t(1023));
+  uint8_t* sA = smem;                // 128 x 128 B
+  uint8_t* sB = smem + 16384;        // 256 x 128 B
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 49152);
+  uint32_t* slot = reinterpret_cast<uint32_t*>(smem + 49160);
+  for (int i = threadIdx.x; i < 49152 / 16; i += blockDim.x)
+    reinterpret_cast<uint4*>(smem)[i] = make_uint4(0, 0, 0, 0);
+  if (threadIdx.x == 0) {
+    cfgmm::tc::mbar_init(bar, 1);
+    cfgmm::tc::mbar_fence_init();
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (threadIdx.x < 32) {
+    cfgmm::tc::tmem_alloc(slot, 256);
+    cfgmm::tc::tmem_relinquish();
+  }
+  cfgmm::tc::fence_before_sync();
+  __syncthreads();
+  cfgmm::tc::fence_after_sync();
+  const uint32_t tmem = *slot;
+  if (threadIdx.x == 0) {
+    const uint32_t idesc = cfgmm::tc::idesc_i8(128, 256);
+    const uint32_t a0 = cfgmm::tc::smem_u32(sA), b0 = cfgmm::tc::smem_u32(sB);
+    for (int it = 0; it < iters; ++it)
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks)
+        cfgmm::tc::mma_i8(tmem, cfgmm::tc::smem_desc_k128(a0 + 32 * ks),
+                          cfgmm::tc::smem_desc_k128(b0 + 32 * ks), idesc, it > 0 || ks > 0);
+    cfgmm::tc::mma_commit(bar);
+    cfgmm::tc::mbar_wait(bar, 0, &g_peak_err, 1, true);
+  }
+  cfgmm::tc::fence_before_sync();
+  __syncthreads();
+  cfgmm::tc::fence_after_sync();
+  if (threadIdx.x < 32) cfgmm::tc::tmem_dealloc(tmem, 256);
+}
+
 }  // namespace
 
 extern "C" {
+
+// INT8 tensor-core (tcgen05.mma kind::i8) throughput in TOP/s; < 0 on error.
+double cfgmm_peak_i8_tops(int iters) {
+  const int smem = 49152 + 1024 + 64;
+  if (cudaFuncSetAttribute(i8_mma_loop, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+      cudaSuccess)
+    return -1.0;
+  const int grid = sm_count();
+  const double ops = double(grid) * iters * 4 * 2.0 * 128 * 256 * 32;
+  double r = time_kernel([&] { i8_mma_loop<<<grid, 128, smem>>>(iters); }, ops);
+  int code = 0;
+  cudaMemcpyFromSymbol(&code, g_peak_err, sizeof(int));
+  return code ? -2.0 : r;
+}
 
 // FP64 tensor-core (DMMA m16n8k4) throughput in TFLOP/s; < 0 on error.
 double cfgmm_peak_dmma_tflops(int iters, int ctas_per_sm) {

@@ -1,0 +1,115 @@
+"""GPU tests of the split-precision DGEMM (Ozaki scheme on INT8 tcgen05 tensor
+cores) through the C ABI.  Bar: within 1e-12 normwise of FP64 (the oracle, or
+the reference tests' dense comparator); the reference has no such path, so
+the FP64 oracle is the only judge of accuracy here."""
+import numpy as np
+import pytest
+
+from conftest import check_gemm_summary, load_golden, normwise
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def split(cm, c, a, b, m, n, k, lda, ldb, ldc, ta, tb):
+    cm.matmul_ex(c, a, b, m, n, k, lda, ldb, ldc, ta, tb, precision=cm.PREC_OZAKI_INT8)
+
+
+@pytest.mark.parametrize("ta", [False, True])
+@pytest.mark.parametrize("tb", [False, True])
+@pytest.mark.parametrize("shape", [(1, 1, 1), (7, 300, 33), (129, 257, 128), (200, 300, 500),
+                                   (300, 513, 1000)])
+def test_split_vs_oracle(cm, oracle, ta, tb, shape):
+    m, n, k = shape
+    rng = np.random.default_rng(m + 3 * n + 7 * k)
+    a = rng.uniform(-1, 1, (k, m) if ta else (m, k))
+    b = rng.uniform(-1, 1, (n, k) if tb else (k, n))
+    c0 = rng.uniform(-1, 1, (m, n))
+    c, ref = c0.copy(), c0.copy()
+    split(cm, c, a, b, m, n, k, a.shape[1], b.shape[1], n, ta, tb)
+    oracle.matmul_anyway_full(ref, a, b, m, n, k, a.shape[1], b.shape[1], n, ta, tb)
+    assert normwise(c, ref) < TOL
+
+
+@pytest.mark.parametrize("name", ["matmul_nn", "matmul_nt", "matmul_tn", "matmul_tt"])
+def test_split_golden(cm, wl, name):
+    g = load_golden(name)
+    m, n, k, ta, tb = int(g["m"]), int(g["n"]), int(g["k"]), bool(g["transa"]), bool(g["transb"])
+    a, b, lda, ldb = wl.ref_matmul_inputs(m, n, k, ta, tb)
+    c = np.zeros((m, n))
+    split(cm, c, a, b, m, n, k, lda, ldb, n, ta, tb)
+    check_gemm_summary(c, g, TOL)
+
+
+def test_split_wide_dynamic_range(cm, oracle):
+    """Rows and columns spanning 2^-300 .. 2^300: the per-row / per-column
+    power-of-two scaling must keep each one's own precision."""
+    rng = np.random.default_rng(1)
+    m, n, k = 64, 80, 96
+    a = rng.uniform(-1, 1, (m, k)) * np.ldexp(1.0, rng.integers(-300, 300, m))[:, None]
+    b = rng.uniform(-1, 1, (k, n)) * np.ldexp(1.0, rng.integers(-300, 300, n))[None, :]
+    c = np.zeros((m, n))
+    ref = np.zeros((m, n))
+    split(cm, c, a, b, m, n, k, k, n, n, False, False)
+    oracle.matmul_anyway_full(ref, a, b, m, n, k, k, n, n, False, False)
+    scale = np.abs(a).max(axis=1)[:, None] * np.abs(b).max(axis=0)[None, :] * k
+    assert np.max(np.abs(c - ref) / scale) < 1e-14
+
+
+def test_split_nonfinite_rows_propagate(cm):
+    m, n, k = 20, 30, 40
+    a = np.ones((m, k))
+    b = np.ones((k, n))
+    a[3, 5] = np.nan
+    b[7, 11] = np.inf
+    c = np.zeros((m, n))
+    split(cm, c, a, b, m, n, k, k, n, n, False, False)
+    assert np.all(np.isnan(c[3, :])) and np.all(np.isnan(c[:, 11]))
+    mask = np.ones((m, n), bool)
+    mask[3, :] = False
+    mask[:, 11] = False
+    assert np.allclose(c[mask], k)
+
+
+def test_split_repeatable(cm, wl):
+    a, b, lda, ldb = wl.dgemm_uniform(300, 400, 500, seed=4)
+    c1 = np.zeros((300, 400))
+    c2 = np.zeros((300, 400))
+    split(cm, c1, a, b, 300, 400, 500, lda, ldb, 400, False, False)
+    split(cm, c2, a, b, 300, 400, 500, lda, ldb, 400, False, False)
+    assert np.array_equal(c1, c2)
+
+
+def test_split_k_limit(cm):
+    c = np.zeros((2, 2))
+    a = np.zeros((2, 70000))
+    b = np.zeros((70000, 2))
+    with pytest.raises(NotImplementedError):
+        split(cm, c, a, b, 2, 2, 70000, 70000, 2, 2, False, False)
+
+
+def test_split_device_pointers(cm):
+    import torch
+    m, n, k = 257, 300, 700
+    g = torch.Generator(device="cuda").manual_seed(3)
+    a = torch.rand(m, k, dtype=torch.float64, device="cuda", generator=g) - 0.5
+    b = torch.rand(k, n, dtype=torch.float64, device="cuda", generator=g) - 0.5
+    c = torch.zeros(m, n, dtype=torch.float64, device="cuda")
+    cm.matmul_ex(c, a, b, m, n, k, k, n, n, False, False, precision=cm.PREC_OZAKI_INT8)
+    torch.cuda.synchronize()
+    assert normwise(c.cpu().numpy(), a.cpu().numpy() @ b.cpu().numpy()) < TOL
+
+
+@pytest.mark.parametrize("ta,tb", [(False, False), (True, True)])
+def test_split_full_size_sampled(cm, wl, ta, tb):
+    m, n, k = 3527, 9583, 6581
+    a, b, lda, ldb = wl.dgemm_uniform(m, n, k, ta, tb, seed=12)
+    c = np.zeros((m, n))
+    split(cm, c, a, b, m, n, k, lda, ldb, n, ta, tb)
+    rng = np.random.default_rng(5)
+    i = rng.integers(0, m, 2048)
+    j = rng.integers(0, n, 2048)
+    A = a.T if ta else a
+    B = b.T if tb else b
+    ref = np.einsum("sk,ks->s", A[i, :], B[:, j])
+    assert normwise(c[i, j], ref) < TOL
