@@ -146,6 +146,8 @@ def peaks_lib():
     for name in ("cfgmm_peak_dmma_tflops", "cfgmm_peak_dfma_tflops"):
         getattr(L, name).argtypes = [ctypes.c_int, ctypes.c_int]
         getattr(L, name).restype = ctypes.c_double
+    L.cfgmm_peak_i8_tops.argtypes = [ctypes.c_int]
+    L.cfgmm_peak_i8_tops.restype = ctypes.c_double
     return L
 
 
@@ -241,6 +243,39 @@ def run_reference(args, ranks: Ranks):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+class Timed:
+    """K steps of one device-pointer DGEMM call, with the CUDA events the
+    library records at its phase boundaries (cfgmm_matmul_dev_timed)."""
+
+    def __init__(self, lib, stream, nphase_events, steps):
+        import torch
+        self.lib, self.stream = lib, stream
+        self.ev = [[torch.cuda.Event(enable_timing=True) for _ in range(nphase_events)]
+                   for _ in range(steps)]
+        for row in self.ev:  # materialise the underlying cudaEvent_t handles
+            for e in row:
+                e.record(stream)
+        torch.cuda.synchronize()
+        self.handles = [(ctypes.c_void_p * nphase_events)(*[e.cuda_event for e in row])
+                        for row in self.ev]
+
+    def step(self, i, c, a, b, precision):
+        h = self.handles[i]
+        rc = self.lib.cfgmm_matmul_dev_timed(c.data_ptr(), a.data_ptr(), b.data_ptr(), M, N, K,
+                                             K, N, N, 0, 0, precision, self.stream.cuda_stream,
+                                             ctypes.cast(h, ctypes.POINTER(ctypes.c_void_p)),
+                                             len(h))
+        if rc != 0:
+            raise RuntimeError(f"cfgmm_matmul_dev_timed returned {rc}: "
+                               f"{self.lib.cfgmm_last_error().decode()}")
+
+    def total_ms(self, steps):
+        return self.ev[0][0].elapsed_time(self.ev[steps - 1][-1])
+
+    def phase_ms(self, steps, i0, i1):
+        return [self.ev[s][i0].elapsed_time(self.ev[s][i1]) for s in range(steps)]
+
+
 def run_ours(args, ranks: Ranks):
     import torch
     cm = importlib.import_module("cfgable-matmul_b200")
@@ -249,45 +284,64 @@ def run_ours(args, ranks: Ranks):
     dev = torch.device("cuda", ranks.local)
     stream = torch.cuda.current_stream()
     lib = cm.lib()
+    FP64, SPLIT = cm.PREC_FP64, cm.PREC_OZAKI_INT8
+    nmod = lib.cfgmm_split_moduli(K)
+    flops = 2.0 * M * N * K
 
-    def dgemm_dev(c, a, b):
-        rc = lib.cfgmm_matmul_dev(c.data_ptr(), a.data_ptr(), b.data_ptr(), M, N, K, K, N, N, 0,
-                                  0, cm.PREC_FP64, stream.cuda_stream)
-        if rc != 0:
-            cm._raise(rc)
-
-    # ---- peak of the FP64 tensor pipe, measured here (burst) ----
+    # ---- measured peaks (roofline denominators), burst ----
     pk = peaks_lib()
     dmma_peak = max(pk.cfgmm_peak_dmma_tflops(20000, 2), pk.cfgmm_peak_dmma_tflops(20000, 4))
     dfma_peak = pk.cfgmm_peak_dfma_tflops(20000, 4)
+    i8_peak = pk.cfgmm_peak_i8_tops(20000)
 
     g = torch.Generator(device=dev).manual_seed(1234 + ranks.rank)
     a = torch.rand(M, K, dtype=torch.float64, device=dev, generator=g) * 2 - 1
     b = torch.rand(K, N, dtype=torch.float64, device=dev, generator=g) * 2 - 1
     c = torch.zeros(M, N, dtype=torch.float64, device=dev)
 
-    for _ in range(args.warmup):
-        dgemm_dev(c, a, b)
-    torch.cuda.synchronize()
     clocks = Clocks(ranks.local)
     clocks.start()
-    ranks.barrier()
+
+    def timed_run(precision, nev):
+        t = Timed(lib, stream, nev, args.steps)
+        for i in range(args.warmup):
+            t.step(i % args.steps, c, a, b, precision)
+        torch.cuda.synchronize()
+        ranks.barrier()
+        torch.cuda.synchronize()
+        for i in range(args.steps):
+            t.step(i, c, a, b, precision)
+        torch.cuda.synchronize()
+        ranks.barrier()
+        return t
+
+    # ---- FP64 DGEMM ----
+    t64 = timed_run(FP64, 2)
+    fp64_ms = ranks.max(t64.total_ms(args.steps))
+    fp64_kernel_ms = sum(t64.phase_ms(args.steps, 0, 1)) / args.steps
+    # ---- split-precision DGEMM (the headline) ----
+    tsp = timed_run(SPLIT, 4)
+    split_ms = ranks.max(tsp.total_ms(args.steps))
+    prep_ms = sum(tsp.phase_ms(args.steps, 0, 1)) / args.steps
+    gemm_ms = sum(tsp.phase_ms(args.steps, 1, 2)) / args.steps
+    recon_ms = sum(tsp.phase_ms(args.steps, 2, 3)) / args.steps
+    rc = lib.cfgmm_device_check()
+    if rc != 0:
+        raise RuntimeError("device check after the split DGEMM: " + lib.cfgmm_last_error().decode())
+
+    # ---- accuracy of the split result against FP64, this run's inputs ----
+    c64 = torch.zeros(M, N, dtype=torch.float64, device=dev)
+    csp = torch.zeros(M, N, dtype=torch.float64, device=dev)
+    cm.matmul_ex(c64, a, b, M, N, K, K, N, N, False, False, precision=FP64)
+    cm.matmul_ex(csp, a, b, M, N, K, K, N, N, False, False, precision=SPLIT)
     torch.cuda.synchronize()
-    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
-    evs[0].record(stream)
-    for i in range(args.steps):
-        dgemm_dev(c, a, b)
-        evs[i + 1].record(stream)
-    torch.cuda.synchronize()
-    ranks.barrier()
-    clk = clocks.stop()
-    per = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
-    total_ms = ranks.max(sum(per))
-    flops = 2.0 * M * N * K
-    value = ranks.world * flops * args.steps / (total_ms * 1e-3) / 1e12
-    kernel_ms = sum(per) / len(per)
-    achieved = flops / (kernel_ms * 1e-3) / 1e12
-    traffic = profile_traffic("dgemm_fp64_3527x9583x6581")
+    split_err = float((csp - c64).abs().max() / c64.abs().max())
+    rs = np.random.default_rng(7)
+    si, sj = rs.integers(0, M, 256), rs.integers(0, N, 256)
+    an, bn = a.cpu().numpy(), b.cpu().numpy()
+    exact = np.einsum("sk,ks->s", an[si, :], bn[:, sj])
+    fp64_err = float(np.abs(c64.cpu().numpy()[si, sj] - exact).max() / np.abs(exact).max())
+    del c64, csp
 
     # ---- end to end through the C ABI host-pointer call, pinned buffers ----
     ha = torch.empty(M, K, dtype=torch.float64).pin_memory()
@@ -298,22 +352,24 @@ def run_ours(args, ranks: Ranks):
     del a, b, c
     torch.cuda.empty_cache()
 
-    def e2e_step():
-        rc = lib.cfgmm_matmul_anyway_full(hc.data_ptr(), hc.numel(), ha.data_ptr(), ha.numel(),
-                                          hb.data_ptr(), hb.numel(), M, N, K, K, N, N, 0, 0)
-        if rc != 0:
-            cm._raise(rc)
+    def e2e(precision):
+        def step():
+            rc = lib.cfgmm_matmul_ex(hc.data_ptr(), hc.numel(), ha.data_ptr(), ha.numel(),
+                                     hb.data_ptr(), hb.numel(), M, N, K, K, N, N, 0, 0, precision)
+            if rc != 0:
+                cm._raise(rc)
+        for _ in range(max(1, args.warmup)):
+            step()
+        ranks.barrier()
+        ts = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            step()
+            ts.append(time.perf_counter() - t0)
+        return ranks.world * flops * args.steps / ranks.max(sum(ts)) / 1e12
 
-    for _ in range(max(1, args.warmup)):
-        e2e_step()
-    ranks.barrier()
-    e2e_times = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        e2e_step()
-        e2e_times.append(time.perf_counter() - t0)
-    e2e_total = ranks.max(sum(e2e_times))
-    e2e_value = ranks.world * flops * args.steps / e2e_total / 1e12
+    e2e_split = e2e(SPLIT)
+    e2e_fp64 = e2e(FP64)
     lib.cfgmm_release_workspace()
     del ha, hb, hc
 
@@ -327,7 +383,7 @@ def run_ours(args, ranks: Ranks):
     def aodm_step():
         rc = lib.cfgmm_aodmao2rho_dev(rho.data_ptr(), dms.data_ptr(), ao.data_ptr(), ao.data_ptr(),
                                       p.nao, p.ngrid, p.nao, p.ngrid, p.nset, tab.data_ptr(),
-                                      p.nblk, p.blksize, cm.PREC_FP64, stream.cuda_stream)
+                                      p.nblk, p.blksize, FP64, stream.cuda_stream)
         if rc != 0:
             cm._raise(rc)
 
@@ -341,37 +397,56 @@ def run_ours(args, ranks: Ranks):
         aodm_step()
         ev[i + 1].record(stream)
     torch.cuda.synchronize()
-    aper = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
-    atot = ranks.max(sum(aper))
+    atot = ranks.max(ev[0].elapsed_time(ev[-1]))
     aflops = p.flops()
+    clk = clocks.stop()
     aodm = {"workload": p.name + f", blocks of {p.blksize}, tile density {p.density():.3f}",
             "precision": "fp64", "value": ranks.world * aflops * args.steps / (atot * 1e-3) / 1e9,
-            "unit": "GFLOP/s", "ms_per_step": atot / args.steps,
-            "flops_per_step": aflops, "flops": "sum_s sum_b (2|I_b|^2 + 2|I_b|)|b| (masked)",
+            "unit": "GFLOP/s", "ms_per_step": atot / args.steps, "flops_per_step": aflops,
+            "flops": "sum_s sum_b (2|I_b|^2 + 2|I_b|)|b| (masked)",
             "frac_of_dmma_peak": (aflops / (atot / args.steps * 1e-3) / 1e12) / dmma_peak,
             "launches_per_step": 4}
 
     cpu = cpu_dgemm_sample() if (ranks.rank == 0 and ranks.world == 1 and not args.no_cpu) else None
+    value = ranks.world * flops * args.steps / (split_ms * 1e-3) / 1e12
+    i8_achieved = nmod * flops / (gemm_ms * 1e-3) / 1e12
     out = {
         "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": ranks.world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": split_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": value / PUBLISHED_TFLOPS,
-        "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "m": M, "n": N, "k": K,
+        "dtype": "i8 tensor cores + f64 reconstruction (Ozaki split precision)",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD + ", split precision", "m": M, "n": N, "k": K,
+                   "moduli": nmod, "error_vs_fp64": split_err, "error_bar": 1e-12,
                    "parallelism": f"{ranks.world} independent replica(s), one per GPU",
                    "l2": "inputs larger than L2 (961 MB of A, B, C per step)",
-                   "vs_baseline_ref": "README.md:11-17, 530 ms on Ryzen 7945HX"},
-        "roofline": {"bound": "tensor", "achieved": achieved, "peak": dmma_peak,
-                     "unit": "TFLOP/s", "frac": achieved / dmma_peak, "traffic": traffic,
-                     "kernel": "dgemm_fp64_kernel<false,false>",
-                     "peak_source": "measured in this run: FP64 DMMA m16n8k4 register loop on "
-                                    "every SM (burst); FP64 FMA pipe measured "
-                                    f"{dfma_peak:.2f} TFLOP/s"},
-        "e2e": {"value": e2e_value, "unit": "TFLOP/s",
+                   "vs_baseline_ref": "README.md:11-17, 530 ms on Ryzen 7945HX (FP64)"},
+        "roofline": {"bound": "tensor", "achieved": i8_achieved, "peak": i8_peak,
+                     "unit": "TOP/s (INT8)", "frac": i8_achieved / i8_peak,
+                     "traffic": profile_traffic("gemm_i8_mod_3527x9583x6581"),
+                     "kernel": "gemm_i8_mod_kernel", "kernel_ms": gemm_ms,
+                     "work": f"{nmod} x 2mnk INT8 ops per launch",
+                     "peak_source": "measured in this run: tcgen05.mma kind::i8 128x256x32 loop "
+                                    "on every SM (burst)"},
+        "split_phases_ms": {"prepare": prep_ms, "int8_gemm": gemm_ms, "reconstruct": recon_ms},
+        "fp64": {"value": ranks.world * flops * args.steps / (fp64_ms * 1e-3) / 1e12,
+                 "unit": "TFLOP/s", "ms_per_step": fp64_ms / args.steps,
+                 "error_vs_exact_sampled": fp64_err,
+                 "roofline": {"bound": "tensor", "achieved": flops / (fp64_kernel_ms * 1e-3) / 1e12,
+                              "peak": dmma_peak, "unit": "TFLOP/s",
+                              "frac": flops / (fp64_kernel_ms * 1e-3) / 1e12 / dmma_peak,
+                              "traffic": profile_traffic("dgemm_fp64_3527x9583x6581"),
+                              "kernel": "dgemm_fp64_kernel<false,false>",
+                              "peak_source": "measured in this run: DMMA m16n8k4 register loop "
+                                             f"(burst); FP64 FMA pipe {dfma_peak:.2f} TFLOP/s"},
+                 "e2e": e2e_fp64},
+        "speedup_split_vs_fp64": fp64_ms / split_ms,
+        "e2e": {"value": e2e_split, "unit": "TFLOP/s",
                 "h2d_bytes_per_step": 8 * (M * K + K * N + M * N),
                 "d2h_bytes_per_step": 8 * M * N,
-                "path": "cfgmm_matmul_anyway_full on pinned host buffers (synchronous)"},
-        "gpu_launches": args.steps,
+                "path": "cfgmm_matmul_ex(CFGMM_PREC_OZAKI_INT8) on pinned host buffers "
+                        "(synchronous)"},
+        "gpu_launches": 6 * args.steps,
         "clocks": clk,
         "aodmao2rho": aodm,
     }
@@ -389,15 +464,16 @@ def run_profile_case(args):
     wl = importlib.import_module("cfgable-matmul_b200.workloads")
     lib = cm.lib()
     stream = torch.cuda.current_stream()
-    if args.profile == "dgemm":
+    if args.profile in ("dgemm", "split"):
         m, n, k = args.m, args.n, args.k
+        prec = cm.PREC_FP64 if args.profile == "dgemm" else cm.PREC_OZAKI_INT8
         g = torch.Generator(device="cuda").manual_seed(0)
         a = torch.rand(m, k, dtype=torch.float64, device="cuda", generator=g)
         b = torch.rand(k, n, dtype=torch.float64, device="cuda", generator=g)
         c = torch.zeros(m, n, dtype=torch.float64, device="cuda")
         for _ in range(args.reps):
             rc = lib.cfgmm_matmul_dev(c.data_ptr(), a.data_ptr(), b.data_ptr(), m, n, k, k, n, n,
-                                      0, 0, cm.PREC_FP64, stream.cuda_stream)
+                                      0, 0, prec, stream.cuda_stream)
             assert rc == 0, rc
     else:
         p = wl.geometric(seed=0)
@@ -418,11 +494,11 @@ def run_profile_case(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
-    ap.add_argument("--profile", choices=["dgemm", "aodm"], default=None,
+    ap.add_argument("--profile", choices=["dgemm", "split", "aodm"], default=None,
                     help="run one kernel on one case (ncu target) and exit")
     ap.add_argument("--m", type=int, default=4096)
     ap.add_argument("--n", type=int, default=4096)

@@ -76,6 +76,12 @@ def lib() -> ctypes.CDLL:
         L.cfgmm_matmul_ex.restype = I
         L.cfgmm_matmul_dev.argtypes = [P, P, P, S, S, S, S, S, S, U8, U8, I, P]
         L.cfgmm_matmul_dev.restype = I
+        L.cfgmm_matmul_dev_timed.argtypes = [P, P, P, S, S, S, S, S, S, U8, U8, I, P,
+                                             ctypes.POINTER(P), I]
+        L.cfgmm_matmul_dev_timed.restype = I
+        L.cfgmm_split_moduli.argtypes = [S]
+        L.cfgmm_split_moduli.restype = I
+        L.cfgmm_device_check.restype = I
         aodm_host = [P, S, P, S, P, S, P, S, S, S, S, S, S, P, S, S]
         L.cfgmm_aodmao2rho_anyway.argtypes = aodm_host
         L.cfgmm_aodmao2rho_anyway.restype = I

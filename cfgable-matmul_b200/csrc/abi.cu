@@ -75,6 +75,24 @@ struct DeviceState {
 std::mutex g_devices_mu;
 std::vector<std::unique_ptr<DeviceState>> g_devices;
 
+// Once per device and process: keep memory freed with cudaFreeAsync in the
+// device's default pool, so the stream-ordered scratch of repeated _dev calls
+// is reused instead of being returned to the driver at every synchronisation.
+void init_device_once(int dev) {
+  static std::mutex mu;
+  static std::vector<bool> done;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.size() <= size_t(dev)) done.resize(dev + 1, false);
+  if (done[dev]) return;
+  done[dev] = true;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
+}
+
 int current_device(int* dev) {
   int n = 0;
   cudaError_t err = cudaGetDeviceCount(&n);
@@ -83,6 +101,7 @@ int current_device(int* dev) {
     return fail(CFGMM_ERR_NO_DEVICE, "no CUDA device is visible");
   }
   CFGMM_CUDA(cudaGetDevice(dev));
+  init_device_once(*dev);
   return CFGMM_OK;
 }
 
@@ -386,6 +405,54 @@ int cfgmm_matmul_dev(double* c, const double* a, const double* b, size_t m, size
   CFGMM_CUDA(cfgmm::dgemm_fp64(c, a, b, int(m), int(n), int(k), lda, ldb, ldc, transa != 0,
                                transb != 0, s));
   return CFGMM_OK;
+}
+
+int cfgmm_matmul_dev_timed(double* c, const double* a, const double* b, size_t m, size_t n,
+                           size_t k, size_t lda, size_t ldb, size_t ldc, uint8_t transa,
+                           uint8_t transb, int precision, void* stream, void* const* events,
+                           int nevents) {
+  g_last_error.clear();
+  const int need = precision == CFGMM_PREC_OZAKI_INT8 ? 4 : 2;
+  if (!events || nevents != need)
+    return fail(CFGMM_ERR_INVALID_ARGUMENT, "events: 2 for FP64, 4 for OZAKI_INT8");
+  GemmExtents ex;
+  int rc = check_gemm(c, SIZE_MAX, a, SIZE_MAX, b, SIZE_MAX, m, n, k, lda, ldb, ldc, transa != 0,
+                      transb != 0, &ex);
+  if (rc != CFGMM_OK) return rc;
+  if ((rc = check_precision(precision)) != CFGMM_OK) return rc;
+  if (ex.c == 0) return CFGMM_OK;
+  int dev;
+  if ((rc = current_device(&dev)) != CFGMM_OK) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const cudaEvent_t* ev = reinterpret_cast<const cudaEvent_t*>(events);
+  if (precision == CFGMM_PREC_OZAKI_INT8) {
+    if ((rc = check_split_gemm(k)) != CFGMM_OK) return rc;
+    const int nmod = cfgmm::ozaki_default_moduli(int(k));
+    void* ws = nullptr;
+    CFGMM_CUDA(cudaMallocAsync(&ws, cfgmm::ozaki_dgemm_workspace(int(m), int(n), int(k), nmod), s));
+    cudaError_t err = cfgmm::ozaki_dgemm(c, a, b, int(m), int(n), int(k), lda, ldb, ldc,
+                                         transa != 0, transb != 0, nmod, ws, s, ev);
+    cudaError_t err2 = cudaFreeAsync(ws, s);
+    if (err != cudaSuccess) return cuda_fail(err, "ozaki_dgemm");
+    if (err2 != cudaSuccess) return cuda_fail(err2, "cudaFreeAsync");
+    return CFGMM_OK;
+  }
+  CFGMM_CUDA(cudaEventRecord(ev[0], s));
+  CFGMM_CUDA(cfgmm::dgemm_fp64(c, a, b, int(m), int(n), int(k), lda, ldb, ldc, transa != 0,
+                               transb != 0, s));
+  CFGMM_CUDA(cudaEventRecord(ev[1], s));
+  return CFGMM_OK;
+}
+
+int cfgmm_split_moduli(size_t k) { return cfgmm::ozaki_default_moduli(int(k > 65536 ? 65536 : k)); }
+
+int cfgmm_device_check(void) {
+  g_last_error.clear();
+  int dev;
+  int rc = current_device(&dev);
+  if (rc != CFGMM_OK) return rc;
+  CFGMM_CUDA(cudaDeviceSynchronize());
+  return check_device_waits();
 }
 
 int cfgmm_aodmao2rho_loop_parallel(double* rhos, size_t rhos_len, const double* dms,

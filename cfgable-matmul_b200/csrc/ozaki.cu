@@ -88,8 +88,9 @@ OzakiPlan ozaki_plan(int k, int nmod, int min_bits) {
   for (int l = 0; l < nmod; ++l) M *= u128(kModuli[l]);
   const int logM = bit_length(M) - 1;  // floor(log2 M)
   const int P = logM - 3 - ceil_log2(k > 1 ? k : 2);
-  p.alpha = P / 2;
-  p.beta = P - p.alpha;
+  // at most 52 bits each: the FP32 residue computation is exact up to 2^52
+  p.alpha = std::min(P / 2, kOzakiMaxBits);
+  p.beta = std::min(P - P / 2, kOzakiMaxBits);
   // split point T: sum_l |r_l| hi_l + |q| H < 2^53 with |r_l| <= 128, |q| <= 128 N
   const int T = std::max(0, logM + 1 + 7 + ceil_log2(nmod + 1) + 1 - 52);
   p.two_T = std::ldexp(1.0, T);
@@ -118,81 +119,86 @@ constexpr int kNonFinite = INT_MAX;  // exponent sentinel of a row holding Inf/N
 
 // ---------------------------------------------------------------------------
 // exponents: e[r] = bits - E_r with max_p |x(r,p)| < 2^E_r  (0 for a zero row)
+// Computed in two steps: Emax[r] = max over chunks of the binary exponent of
+// the chunk maximum (INT_MAX for Inf/NaN, INT_MIN for all-zero), then e[r].
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int scale_exponent(double amax, int bits) {
-  if (!(amax <= 1.7976931348623157e308)) return kNonFinite;  // Inf or NaN
-  if (amax == 0.0) return 0;
+__device__ __forceinline__ int exponent_of(double amax) {
+  if (!(amax <= 1.7976931348623157e308)) return INT_MAX;  // Inf or NaN
+  if (amax == 0.0) return INT_MIN;
   int E;
   frexp(amax, &E);  // amax = f 2^E, f in [0.5, 1): amax < 2^E
-  return bits - E;
+  return E;
+}
+
+__global__ void fill_int(int* __restrict__ v, int n, int value) {
+  const int i = blockIdx.x * 256 + threadIdx.x;
+  if (i < n) v[i] = value;
 }
 
 // element (r, p) at x[r*ld + p]: one CTA per row
 __global__ void __launch_bounds__(256)
-exps_rows(const double* __restrict__ x, size_t ld, int rows, int k, int bits, int* __restrict__ e) {
+emax_rows(const double* __restrict__ x, size_t ld, int rows, int k, int* __restrict__ emax) {
   const int r = blockIdx.x;
   if (r >= rows) return;
   const double* row = x + size_t(r) * ld;
-  double mx = 0.0;
-  bool bad = false;
-  for (int p = threadIdx.x; p < k; p += 256) {
-    const double v = fabs(row[p]);
-    bad |= !(v <= 1.7976931348623157e308);
-    mx = fmax(mx, v);
-  }
-  __shared__ double red[8];
-  __shared__ int badw[8];
-  for (int o = 16; o > 0; o >>= 1) {
-    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    bad |= __shfl_xor_sync(0xffffffffu, int(bad), o) != 0;
-  }
-  if ((threadIdx.x & 31) == 0) {
-    red[threadIdx.x >> 5] = mx;
-    badw[threadIdx.x >> 5] = bad;
-  }
+  int E = INT_MIN;
+  for (int p = threadIdx.x; p < k; p += 256) E = max(E, exponent_of(fabs(row[p])));
+  for (int o = 16; o > 0; o >>= 1) E = max(E, __shfl_xor_sync(0xffffffffu, E, o));
+  __shared__ int red[8];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = E;
   __syncthreads();
   if (threadIdx.x == 0) {
-    double m = 0.0;
-    int b = 0;
-    for (int w = 0; w < 8; ++w) {
-      m = fmax(m, red[w]);
-      b |= badw[w];
-    }
-    e[r] = b ? kNonFinite : scale_exponent(m, bits);
+    for (int w = 1; w < 8; ++w) E = max(E, red[w]);
+    emax[r] = max(E, red[0]);
   }
 }
 
-// element (r, p) at x[p*ld + r]: one thread per r, coalesced over r
+// element (r, p) at x[p*ld + r]: thread per r (coalesced), CTA rows of p chunks
+constexpr int kColChunk = 128;
 __global__ void __launch_bounds__(256)
-exps_cols(const double* __restrict__ x, size_t ld, int rows, int k, int bits, int* __restrict__ e) {
+emax_cols(const double* __restrict__ x, size_t ld, int rows, int k, int* __restrict__ emax) {
   const int r = blockIdx.x * 256 + threadIdx.x;
+  const int p0 = blockIdx.y * kColChunk;
   if (r >= rows) return;
+  const int p1 = min(k, p0 + kColChunk);
   double mx = 0.0;
   bool bad = false;
-  for (int p = 0; p < k; ++p) {
+  for (int p = p0; p < p1; ++p) {
     const double v = fabs(x[size_t(p) * ld + r]);
     bad |= !(v <= 1.7976931348623157e308);
     mx = fmax(mx, v);
   }
-  e[r] = bad ? kNonFinite : scale_exponent(mx, bits);
+  atomicMax(&emax[r], bad ? INT_MAX : exponent_of(mx));
+}
+
+__global__ void finalize_exps(const int* __restrict__ emax, int rows, int bits, int* __restrict__ e) {
+  const int r = blockIdx.x * 256 + threadIdx.x;
+  if (r >= rows) return;
+  const int E = emax[r];
+  e[r] = (E == INT_MAX) ? kNonFinite : (E == INT_MIN ? 0 : bits - E);
 }
 
 // ---------------------------------------------------------------------------
 // residues: Y[l][r][p] = rint(x(r,p) 2^e[r]) mods m_l  (int8), p < k
+// The integer v (|v| <= 2^52) is split into 14-bit chunks
+// v = d3 2^42 + d2 2^28 + d1 2^14 + d0 (d3 signed, |d3| <= 2^10; d0..d2 in
+// [0, 2^14)); with symmetric c_t = 2^(14t) mods m (|c_t| <= 127) the sum
+// s = d3 c3 + d2 c2 + d1 c1 + d0 is exact in FP32 (|s| < 2^23) and congruent to
+// v, so v mods m follows from one FP32 quotient and one correction.
 // ---------------------------------------------------------------------------
 struct ResidueArgs {
   int nmod;
   int mod[kMaxModuli];
-  double inv[kMaxModuli];
+  float inv[kMaxModuli];
+  float c14[kMaxModuli], c28[kMaxModuli], c42[kMaxModuli];
 };
 
-__device__ __forceinline__ int8_t mods(double v, int m, double inv) {
-  const double q = rint(v * inv);
-  double r = fma(-double(m), q, v);  // exact: |m q| < 2^53
-  const int hi = (m - 1) >> 1, lo = -(m >> 1);
+__device__ __forceinline__ int8_t mods_f(float s, float m, float inv, float hi, float lo) {
+  const float q = rintf(s * inv);
+  float r = fmaf(-m, q, s);  // exact: |r| <= 1.5 m
   if (r > hi) r -= m;
   else if (r < lo) r += m;
-  return int8_t(int(r));
+  return int8_t(__float2int_rn(r));
 }
 
 __device__ __forceinline__ double scaled_int(double x, int e) {
@@ -201,24 +207,30 @@ __device__ __forceinline__ double scaled_int(double x, int e) {
 
 __device__ __forceinline__ void write_residues(const ResidueArgs& a, int8_t* Y, size_t plane,
                                                size_t off, const double (&v)[4]) {
-  // modulus 256: the low byte of the two's-complement integer
-  {
-    char4 c;
-    c.x = int8_t(static_cast<long long>(v[0]));
-    c.y = int8_t(static_cast<long long>(v[1]));
-    c.z = int8_t(static_cast<long long>(v[2]));
-    c.w = int8_t(static_cast<long long>(v[3]));
-    *reinterpret_cast<char4*>(Y + off) = c;
+  float d0[4], d1[4], d2[4], d3[4];
+  char4 b256;
+  int8_t* b = reinterpret_cast<int8_t*>(&b256);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const long long iv = static_cast<long long>(v[j]);
+    b[j] = int8_t(iv);  // modulus 256: the low byte of the two's complement
+    d3[j] = float(iv >> 42);
+    d2[j] = float(int((iv >> 28) & 0x3fff));
+    d1[j] = float(int((iv >> 14) & 0x3fff));
+    d0[j] = float(int(iv & 0x3fff));
   }
+  *reinterpret_cast<char4*>(Y + off) = b256;
   for (int l = 1; l < a.nmod; ++l) {
-    const int m = a.mod[l];
-    const double inv = a.inv[l];
-    char4 c;
-    c.x = mods(v[0], m, inv);
-    c.y = mods(v[1], m, inv);
-    c.z = mods(v[2], m, inv);
-    c.w = mods(v[3], m, inv);
-    *reinterpret_cast<char4*>(Y + size_t(l) * plane + off) = c;
+    const float m = float(a.mod[l]), inv = a.inv[l];
+    const float hi = float((a.mod[l] - 1) >> 1), lo = -float(a.mod[l] >> 1);
+    char4 out;
+    int8_t* o = reinterpret_cast<int8_t*>(&out);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float s = fmaf(d3[j], a.c42[l], fmaf(d2[j], a.c28[l], fmaf(d1[j], a.c14[l], d0[j])));
+      o[j] = mods_f(s, m, inv, hi, lo);
+    }
+    *reinterpret_cast<char4*>(Y + size_t(l) * plane + off) = out;
   }
 }
 
@@ -345,7 +357,7 @@ bool make_plane_map(CUtensorMap* map, void* base, int k, int rows, int nplanes, 
 size_t a256(size_t v) { return (v + 255) / 256 * 256; }
 
 struct DgemmLayout {
-  size_t kpad, ldr, a_res, b_res, r, ea, eb, total;
+  size_t kpad, ldr, a_res, b_res, r, ea, eb, emax, total;
 };
 
 DgemmLayout dgemm_layout(int m, int n, int k, int nmod) {
@@ -357,8 +369,16 @@ DgemmLayout dgemm_layout(int m, int n, int k, int nmod) {
   L.r = L.b_res + a256(size_t(nmod) * n * L.kpad);
   L.ea = L.r + a256(size_t(nmod) * m * L.ldr);
   L.eb = L.ea + a256(size_t(m) * sizeof(int));
-  L.total = L.eb + a256(size_t(n) * sizeof(int));
+  L.emax = L.eb + a256(size_t(n) * sizeof(int));
+  L.total = L.emax + a256(size_t(std::max(m, n)) * sizeof(int));
   return L;
+}
+
+int mods_host(long long v, int m) {  // symmetric residue
+  long long r = v % m;
+  if (r < 0) r += m;
+  if (r > (m - 1) / 2) r -= m;
+  return int(r);
 }
 
 ResidueArgs residue_args(const OzakiPlan& p) {
@@ -366,19 +386,30 @@ ResidueArgs residue_args(const OzakiPlan& p) {
   a.nmod = p.nmod;
   for (int l = 0; l < p.nmod; ++l) {
     a.mod[l] = p.mod[l];
-    a.inv[l] = p.inv_d[l];
+    a.inv[l] = p.inv_f[l];
+    a.c14[l] = float(mods_host(1LL << 14, p.mod[l]));
+    a.c28[l] = float(mods_host(1LL << 28, p.mod[l]));
+    a.c42[l] = float(mods_host(1LL << 42, p.mod[l]));
   }
   return a;
 }
 
-// Scales, rounds and splits op(X) into residue planes Y[nmod][rows][kpad].
+// Scales, rounds and splits op(X) into residue planes Y[nmod][rows][kpad];
+// `emax` is scratch for rows ints.
 cudaError_t prepare(const double* x, size_t ld, bool rows_contig, int rows, int k, size_t kpad,
-                    int bits, int* e, int8_t* Y, const ResidueArgs& ra, cudaStream_t s) {
+                    int bits, int* emax, int* e, int8_t* Y, const ResidueArgs& ra,
+                    cudaStream_t s) {
+  const int rb = (rows + 255) / 256;
   if (rows_contig) {
-    exps_rows<<<rows, 256, 0, s>>>(x, ld, rows, k, bits, e);
+    emax_rows<<<rows, 256, 0, s>>>(x, ld, rows, k, emax);
+  } else {
+    fill_int<<<rb, 256, 0, s>>>(emax, rows, INT_MIN);
+    emax_cols<<<dim3(rb, (k + kColChunk - 1) / kColChunk), 256, 0, s>>>(x, ld, rows, k, emax);
+  }
+  finalize_exps<<<rb, 256, 0, s>>>(emax, rows, bits, e);
+  if (rows_contig) {
     residues_rows<<<rows, 256, 0, s>>>(x, ld, rows, k, kpad, e, Y, ra);
   } else {
-    exps_cols<<<(rows + 255) / 256, 256, 0, s>>>(x, ld, rows, k, bits, e);
     dim3 grid((rows + 31) / 32, (k + 63) / 64);
     residues_cols<<<grid, 256, 0, s>>>(x, ld, rows, k, kpad, e, Y, ra);
   }
@@ -402,8 +433,9 @@ size_t ozaki_dgemm_workspace(int m, int n, int k, int nmod) {
 
 cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int n, int k,
                         size_t lda, size_t ldb, size_t ldc, bool transa, bool transb, int nmod,
-                        void* workspace, cudaStream_t stream) {
+                        void* workspace, cudaStream_t stream, const cudaEvent_t* events) {
   if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
+  auto mark = [&](int i) { if (events) cudaEventRecord(events[i], stream); };
   if (k > kOzakiMaxK) return cudaErrorInvalidValue;
   const OzakiPlan plan = ozaki_plan(k, nmod, 0);
   const DgemmLayout L = dgemm_layout(m, n, k, plan.nmod);
@@ -414,13 +446,17 @@ cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int 
   int* ea = reinterpret_cast<int*>(ws + L.ea);
   int* eb = reinterpret_cast<int*>(ws + L.eb);
   const ResidueArgs ra = residue_args(plan);
+  mark(0);
   // op(A) rows are i (k contiguous unless transa); op(B) "rows" are j
   // (k contiguous only when transb).
-  cudaError_t err = prepare(a, lda, !transa, m, k, L.kpad, plan.alpha, ea, a_res, ra, stream);
+  int* emax = reinterpret_cast<int*>(ws + L.emax);
+  cudaError_t err =
+      prepare(a, lda, !transa, m, k, L.kpad, plan.alpha, emax, ea, a_res, ra, stream);
   if (err != cudaSuccess) return err;
-  err = prepare(b, ldb, transb, n, k, L.kpad, plan.beta, eb, b_res, ra, stream);
+  err = prepare(b, ldb, transb, n, k, L.kpad, plan.beta, emax, eb, b_res, ra, stream);
   if (err != cudaSuccess) return err;
 
+  mark(1);
   CUtensorMap tmA, tmB;
   if (!make_plane_map(&tmA, a_res, k, m, plan.nmod, L.kpad, gemm_i8_tile_rows_a()) ||
       !make_plane_map(&tmB, b_res, k, n, plan.nmod, L.kpad, gemm_i8_tile_rows_b()))
@@ -437,6 +473,7 @@ cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int 
     g.inv[l] = plan.inv_f[l];
   }
   if ((err = gemm_i8_mod(tmA, tmB, g, stream)) != cudaSuccess) return err;
+  mark(2);
 
   ReconArgs rc{};
   rc.nmod = plan.nmod;
@@ -451,6 +488,7 @@ cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int 
   const long long rgrid = (long long)((n + 1023) / 1024) * m;
   if (rgrid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
   reconstruct<<<unsigned(rgrid), 256, 0, stream>>>(c, ldc, m, n, r, L.ldr, ea, eb, rc);
+  mark(3);
   return cudaGetLastError();
 }
 

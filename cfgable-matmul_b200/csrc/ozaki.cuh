@@ -11,7 +11,9 @@ namespace cfgmm {
 // float-quotient reduction is exact (after two corrections) for |acc| < 2^30.
 constexpr int kOzakiMaxK = 65536;
 // Default operand precision (bits kept relative to each row / column max).
-constexpr int kOzakiMinBits = 45;
+constexpr int kOzakiMinBits = 46;
+// Upper bound of the operand precision (exactness of the residue arithmetic).
+constexpr int kOzakiMaxBits = 52;
 
 struct OzakiPlan {
   int nmod;             // number of moduli N
@@ -38,8 +40,11 @@ size_t ozaki_dgemm_workspace(int m, int n, int k, int nmod);
 
 // C[i*ldc+j] += sum_p opA(i,p) opB(p,j) by INT8 tensor-core emulation; device
 // pointers; workspace of ozaki_dgemm_workspace bytes (256-byte aligned).
+// `events` (optional, 4 entries) are recorded before the residue preparation
+// and after the preparation, the INT8 GEMM and the reconstruction.
 cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int n, int k,
                         size_t lda, size_t ldb, size_t ldc, bool transa, bool transb, int nmod,
-                        void* workspace, cudaStream_t stream);
+                        void* workspace, cudaStream_t stream,
+                        const cudaEvent_t* events = nullptr);
 
 }  // namespace cfgmm

@@ -102,6 +102,28 @@ int cfgmm_matmul_dev(double* c, const double* a, const double* b, size_t m, size
                      size_t lda, size_t ldb, size_t ldc, uint8_t transa, uint8_t transb,
                      int precision, void* stream);
 
+/* No counterpart in the reference: benchmark instrumentation.  The device-
+ * pointer DGEMM with CUDA events (cudaEvent_t, passed as void*) recorded on
+ * `stream` at its phase boundaries: FP64 -- events[0] before and events[1]
+ * after the GEMM kernel (nevents = 2); OZAKI_INT8 -- before the residue
+ * preparation, after it, after the INT8 GEMM, after the reconstruction
+ * (nevents = 4). */
+int cfgmm_matmul_dev_timed(double* c, const double* a, const double* b, size_t m, size_t n,
+                           size_t k, size_t lda, size_t ldb, size_t ldc, uint8_t transa,
+                           uint8_t transb, int precision, void* stream, void* const* events,
+                           int nevents);
+
+/* No counterpart in the reference: the number of INT8 moduli (GEMM passes)
+ * the split-precision path uses for contraction length k.  The environment
+ * variable CFGMM_OZAKI_MODULI (2..16) overrides the default, which keeps at
+ * least 46 bits of every operand relative to its row / column maximum. */
+int cfgmm_split_moduli(size_t k);
+
+/* No counterpart in the reference: synchronises the current device and
+ * reports CFGMM_ERR_TIMEOUT if a tensor-core pipeline wait of an earlier
+ * asynchronous (_dev) call gave up; CFGMM_OK otherwise. */
+int cfgmm_device_check(void);
+
 /* ======================================================================== */
 /* 2. Masked AO-DM-AO contraction                                           */
 /*    rhos[s*stride_grid + g] += sum_{u,v: tab[u*ldtab + g/BLK] && tab[v*ldtab + g/BLK]}
