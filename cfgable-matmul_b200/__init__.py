@@ -10,6 +10,8 @@ this module                            reference (paths relative to the crate ro
 ``MatmulLoops(...).matmul_loop_parallel_mnk_pack_a``  src/impl_matmul.rs:155-231
 ``MatmulLoops(...).matmul_loop_macro_mb``             README.md:22-31
 ``matmul_anyway_full``                                src/impl_matmul.rs:234-248
+``MatmulLoops(...).matmul_loop_parallel_mnk_pack_a_non0tab``  src/impl_matmul_non0tab.rs:210-306
+``matmul_anyway_full_non0tab``                        src/impl_matmul_non0tab.rs:308-326
 ``MatmulLoops(...).aodmao2rho_loop_parallel``         src/impl_aodmao2rho.rs:171-244
 ``aodmao2rho_anyway``                                 src/impl_aodmao2rho.rs:247-261
 =====================================  ============================================
@@ -31,6 +33,7 @@ import numpy as np
 
 __all__ = [
     "MatmulLoops", "matmul_anyway_full", "aodmao2rho_anyway", "matmul_ex", "aodmao2rho_ex",
+    "matmul_anyway_full_non0tab", "matmul_non0tab_ex",
     "PREC_FP64", "PREC_OZAKI_INT8", "CfgmmError", "lib", "library_path",
 ]
 
@@ -76,6 +79,15 @@ def lib() -> ctypes.CDLL:
         L.cfgmm_matmul_ex.restype = I
         L.cfgmm_matmul_dev.argtypes = [P, P, P, S, S, S, S, S, S, U8, U8, I, P]
         L.cfgmm_matmul_dev.restype = I
+        mask_host = gemm_host + [P, S, S]
+        L.cfgmm_matmul_anyway_full_non0tab.argtypes = mask_host
+        L.cfgmm_matmul_anyway_full_non0tab.restype = I
+        L.cfgmm_matmul_loop_parallel_mnk_pack_a_non0tab.argtypes = mask_host + [S]
+        L.cfgmm_matmul_loop_parallel_mnk_pack_a_non0tab.restype = I
+        L.cfgmm_matmul_non0tab_ex.argtypes = mask_host + [S, I]
+        L.cfgmm_matmul_non0tab_ex.restype = I
+        L.cfgmm_matmul_non0tab_dev.argtypes = [P, P, P, S, S, S, S, S, S, U8, U8, P, S, S, I, P]
+        L.cfgmm_matmul_non0tab_dev.restype = I
         L.cfgmm_matmul_dev_timed.argtypes = [P, P, P, S, S, S, S, S, S, U8, U8, I, P,
                                              ctypes.POINTER(P), I]
         L.cfgmm_matmul_dev_timed.restype = I
@@ -174,6 +186,40 @@ def matmul_anyway_full(c, a, b, m, n, k, lda, ldb, ldc, transa, transb) -> None:
                                           int(bool(transa)), int(bool(transb))))
 
 
+def matmul_non0tab_ex(c, a, b, m, n, k, lda, ldb, ldc, transa, transb, tab, ldtab, blksize=48,
+                      precision=PREC_FP64) -> None:
+    """Masked GEMM C[i,j] += sum_{p: tab[p, j/BLK]} opA(i,p) B[p,j] with an explicit
+    BLKSIZE and arithmetic; transb raises NotImplementedError as the reference panics."""
+    tab = _as_tab(tab)
+    if _is_torch(c):
+        rc = lib().cfgmm_matmul_non0tab_dev(
+            _dev(c, "torch.float64"), _dev(a, "torch.float64"), _dev(b, "torch.float64"), m, n, k,
+            lda, ldb, ldc, int(bool(transa)), int(bool(transb)), _dev(tab, "torch.uint8"), ldtab,
+            blksize, precision, _stream_ptr())
+        return _raise(rc)
+    pc, lc = _host(c, np.float64, True)
+    pa, la = _host(a, np.float64)
+    pb, lb = _host(b, np.float64)
+    pt, lt = _host(tab, np.uint8)
+    _raise(lib().cfgmm_matmul_non0tab_ex(pc, lc, pa, la, pb, lb, m, n, k, lda, ldb, ldc,
+                                         int(bool(transa)), int(bool(transb)), pt, lt, ldtab,
+                                         blksize, precision))
+
+
+def matmul_anyway_full_non0tab(c, a, b, m, n, k, lda, ldb, ldc, transa, transb, tab,
+                               ldtab) -> None:
+    """Masked GEMM with BLKSIZE 48 (src/impl_matmul_non0tab.rs:308-326)."""
+    if _is_torch(c):
+        return matmul_non0tab_ex(c, a, b, m, n, k, lda, ldb, ldc, transa, transb, tab, ldtab, 48)
+    pc, lc = _host(c, np.float64, True)
+    pa, la = _host(a, np.float64)
+    pb, lb = _host(b, np.float64)
+    pt, lt = _host(_as_tab(tab), np.uint8)
+    _raise(lib().cfgmm_matmul_anyway_full_non0tab(pc, lc, pa, la, pb, lb, m, n, k, lda, ldb, ldc,
+                                                  int(bool(transa)), int(bool(transb)), pt, lt,
+                                                  ldtab))
+
+
 def aodmao2rho_ex(rhos, dms, ao_lhs, ao_rhs, strides, shape, nset, tab, ldtab, blksize=48,
                   precision=PREC_FP64) -> None:
     """The masked AO-DM-AO contraction with an explicit BLKSIZE and arithmetic."""
@@ -245,6 +291,20 @@ class MatmulLoops:
         pb, lb = _host(b, np.float64)
         _raise(lib().cfgmm_matmul_loop_macro_mb(pc, lc, pa, la, pb, lb, m, n, k, lda, ldb, ldc,
                                                 int(bool(transa)), int(bool(transb))))
+
+    def matmul_loop_parallel_mnk_pack_a_non0tab(self, c, a, b, m, n, k, lda, ldb, ldc, transa,
+                                                transb, tab, ldtab, BLKSIZE=48):
+        """src/impl_matmul_non0tab.rs:210-306; BLKSIZE is the const generic."""
+        if _is_torch(c):
+            return matmul_non0tab_ex(c, a, b, m, n, k, lda, ldb, ldc, transa, transb, tab, ldtab,
+                                     BLKSIZE)
+        pc, lc = _host(c, np.float64, True)
+        pa, la = _host(a, np.float64)
+        pb, lb = _host(b, np.float64)
+        pt, lt = _host(_as_tab(tab), np.uint8)
+        _raise(lib().cfgmm_matmul_loop_parallel_mnk_pack_a_non0tab(
+            pc, lc, pa, la, pb, lb, m, n, k, lda, ldb, ldc, int(bool(transa)), int(bool(transb)),
+            pt, lt, ldtab, BLKSIZE))
 
     def aodmao2rho_loop_parallel(self, rhos, dms, ao_lhs, ao_rhs, strides, shape, nset, tab,
                                  ldtab, BLKSIZE=48):

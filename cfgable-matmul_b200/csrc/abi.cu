@@ -186,13 +186,46 @@ int check_device_waits() {
   return CFGMM_OK;
 }
 
+// Mask of the masked GEMM: tab[p * ldtab + j / blk] for p < k, j < n.
+struct GemmMask {
+  const uint8_t* tab;  // null: plain GEMM
+  size_t tab_len, ldtab, blk;
+};
+
+int check_mask(const GemmMask& mk, size_t n, size_t k, uint8_t transb, size_t* tab_extent) {
+  *tab_extent = 0;
+  if (!mk.tab && mk.tab_len == 0 && mk.blk == 0) return CFGMM_OK;  // plain GEMM
+  // impl_matmul_non0tab.rs:228-230: transb panics before anything else
+  if (transb)
+    return fail(CFGMM_ERR_UNIMPLEMENTED,
+                "transb=true is not implemented for the masked GEMM (as in the reference)");
+  if (mk.blk == 0) return fail(CFGMM_ERR_INVALID_ARGUMENT, "BLKSIZE must be at least 1");
+  if (n == 0 || k == 0) return CFGMM_OK;
+  if (!fits_int(mk.blk)) return fail(CFGMM_ERR_INVALID_ARGUMENT, "BLKSIZE must be below 2^31");
+  if (!extent2(k, (n + mk.blk - 1) / mk.blk, mk.ldtab, tab_extent))
+    return fail(CFGMM_ERR_INVALID_ARGUMENT, "index range overflows usize");
+  if (mk.tab_len < *tab_extent) {
+    char msg[160];
+    std::snprintf(msg, sizeof(msg), "slice too short (tab %zu < %zu): the reference panics here",
+                  mk.tab_len, *tab_extent);
+    return fail(CFGMM_ERR_INVALID_ARGUMENT, msg);
+  }
+  if (!mk.tab) return fail(CFGMM_ERR_INVALID_ARGUMENT, "null pointer");
+  return CFGMM_OK;
+}
+
 int gemm_host(double* c, size_t c_len, const double* a, size_t a_len, const double* b,
               size_t b_len, size_t m, size_t n, size_t k, size_t lda, size_t ldb, size_t ldc,
-              uint8_t transa, uint8_t transb, int precision) {
+              uint8_t transa, uint8_t transb, int precision,
+              GemmMask mk = GemmMask{nullptr, 0, 0, 0}) {
   g_last_error.clear();
+  const bool masked = mk.tab || mk.tab_len || mk.blk;
+  size_t tab_ext = 0;
+  int rc = check_mask(mk, n, k, transb, &tab_ext);
+  if (rc != CFGMM_OK) return rc;
   GemmExtents ex;
-  int rc = check_gemm(c, c_len, a, a_len, b, b_len, m, n, k, lda, ldb, ldc, transa != 0,
-                      transb != 0, &ex);
+  rc = check_gemm(c, c_len, a, a_len, b, b_len, m, n, k, lda, ldb, ldc, transa != 0,
+                  transb != 0, &ex);
   if (rc != CFGMM_OK) return rc;
   if ((rc = check_precision(precision)) != CFGMM_OK) return rc;
   if (ex.c == 0) return CFGMM_OK;
@@ -204,20 +237,27 @@ int gemm_host(double* c, size_t c_len, const double* a, size_t a_len, const doub
   std::lock_guard<std::mutex> lk(st->mu);
   const int nmod = split ? cfgmm::ozaki_default_moduli(int(k)) : 0;
   const size_t oa = 0, ob = align256(ex.a * 8), oc = ob + align256(ex.b * 8);
-  const size_t ows = oc + align256(ex.c * 8);
+  const size_t ot = oc + align256(ex.c * 8);
+  const size_t ows = ot + align256(tab_ext);
   const size_t wsb = split ? cfgmm::ozaki_dgemm_workspace(int(m), int(n), int(k), nmod) : 0;
   if ((rc = reserve(st, ows + wsb)) != CFGMM_OK) return rc;
   char* base = static_cast<char*>(st->buf);
   double* da = reinterpret_cast<double*>(base + oa);
   double* db = reinterpret_cast<double*>(base + ob);
   double* dc = reinterpret_cast<double*>(base + oc);
+  uint8_t* dt = masked ? reinterpret_cast<uint8_t*>(base + ot) : nullptr;
   CFGMM_CUDA(cudaMemcpyAsync(da, a, ex.a * 8, cudaMemcpyHostToDevice, st->stream));
   CFGMM_CUDA(cudaMemcpyAsync(db, b, ex.b * 8, cudaMemcpyHostToDevice, st->stream));
   CFGMM_CUDA(cudaMemcpyAsync(dc, c, ex.c * 8, cudaMemcpyHostToDevice, st->stream));
+  if (masked) CFGMM_CUDA(cudaMemcpyAsync(dt, mk.tab, tab_ext, cudaMemcpyHostToDevice, st->stream));
   if (split) {
     CFGMM_CUDA(cfgmm::gemm_i8_reset_error(st->stream));
     CFGMM_CUDA(cfgmm::ozaki_dgemm(dc, da, db, int(m), int(n), int(k), lda, ldb, ldc, transa != 0,
-                                  transb != 0, nmod, base + ows, st->stream));
+                                  transb != 0, nmod, base + ows, st->stream, nullptr, dt,
+                                  mk.ldtab, int(mk.blk)));
+  } else if (masked) {
+    CFGMM_CUDA(cfgmm::dgemm_fp64_non0tab(dc, da, db, int(m), int(n), int(k), lda, ldb, ldc,
+                                         transa != 0, dt, mk.ldtab, int(mk.blk), st->stream));
   } else {
     CFGMM_CUDA(cfgmm::dgemm_fp64(dc, da, db, int(m), int(n), int(k), lda, ldb, ldc, transa != 0,
                                  transb != 0, st->stream));
@@ -404,6 +444,69 @@ int cfgmm_matmul_dev(double* c, const double* a, const double* b, size_t m, size
   }
   CFGMM_CUDA(cfgmm::dgemm_fp64(c, a, b, int(m), int(n), int(k), lda, ldb, ldc, transa != 0,
                                transb != 0, s));
+  return CFGMM_OK;
+}
+
+int cfgmm_matmul_anyway_full_non0tab(double* c, size_t c_len, const double* a, size_t a_len,
+                                     const double* b, size_t b_len, size_t m, size_t n, size_t k,
+                                     size_t lda, size_t ldb, size_t ldc, uint8_t transa,
+                                     uint8_t transb, const uint8_t* tab, size_t tab_len,
+                                     size_t ldtab) {
+  return gemm_host(c, c_len, a, a_len, b, b_len, m, n, k, lda, ldb, ldc, transa, transb,
+                   CFGMM_PREC_FP64, GemmMask{tab, tab_len, ldtab, 48});
+}
+
+int cfgmm_matmul_loop_parallel_mnk_pack_a_non0tab(double* c, size_t c_len, const double* a,
+                                                  size_t a_len, const double* b, size_t b_len,
+                                                  size_t m, size_t n, size_t k, size_t lda,
+                                                  size_t ldb, size_t ldc, uint8_t transa,
+                                                  uint8_t transb, const uint8_t* tab,
+                                                  size_t tab_len, size_t ldtab, size_t blksize) {
+  return gemm_host(c, c_len, a, a_len, b, b_len, m, n, k, lda, ldb, ldc, transa, transb,
+                   CFGMM_PREC_FP64, GemmMask{tab, tab_len, ldtab, blksize});
+}
+
+int cfgmm_matmul_non0tab_ex(double* c, size_t c_len, const double* a, size_t a_len,
+                            const double* b, size_t b_len, size_t m, size_t n, size_t k,
+                            size_t lda, size_t ldb, size_t ldc, uint8_t transa, uint8_t transb,
+                            const uint8_t* tab, size_t tab_len, size_t ldtab, size_t blksize,
+                            int precision) {
+  return gemm_host(c, c_len, a, a_len, b, b_len, m, n, k, lda, ldb, ldc, transa, transb,
+                   precision, GemmMask{tab, tab_len, ldtab, blksize});
+}
+
+int cfgmm_matmul_non0tab_dev(double* c, const double* a, const double* b, size_t m, size_t n,
+                             size_t k, size_t lda, size_t ldb, size_t ldc, uint8_t transa,
+                             uint8_t transb, const uint8_t* tab, size_t ldtab, size_t blksize,
+                             int precision, void* stream) {
+  g_last_error.clear();
+  size_t tab_ext = 0;
+  int rc = check_mask(GemmMask{tab, SIZE_MAX, ldtab, blksize}, n, k, transb, &tab_ext);
+  if (rc != CFGMM_OK) return rc;
+  GemmExtents ex;
+  rc = check_gemm(c, SIZE_MAX, a, SIZE_MAX, b, SIZE_MAX, m, n, k, lda, ldb, ldc, transa != 0,
+                  false, &ex);
+  if (rc != CFGMM_OK) return rc;
+  if ((rc = check_precision(precision)) != CFGMM_OK) return rc;
+  if (ex.c == 0) return CFGMM_OK;
+  int dev;
+  if ((rc = current_device(&dev)) != CFGMM_OK) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (precision == CFGMM_PREC_OZAKI_INT8) {
+    if ((rc = check_split_gemm(k)) != CFGMM_OK) return rc;
+    const int nmod = cfgmm::ozaki_default_moduli(int(k));
+    void* ws = nullptr;
+    CFGMM_CUDA(cudaMallocAsync(&ws, cfgmm::ozaki_dgemm_workspace(int(m), int(n), int(k), nmod), s));
+    cudaError_t err = cfgmm::ozaki_dgemm(c, a, b, int(m), int(n), int(k), lda, ldb, ldc,
+                                         transa != 0, false, nmod, ws, s, nullptr, tab, ldtab,
+                                         int(blksize));
+    cudaError_t err2 = cudaFreeAsync(ws, s);
+    if (err != cudaSuccess) return cuda_fail(err, "ozaki_dgemm (masked)");
+    if (err2 != cudaSuccess) return cuda_fail(err2, "cudaFreeAsync");
+    return CFGMM_OK;
+  }
+  CFGMM_CUDA(cfgmm::dgemm_fp64_non0tab(c, a, b, int(m), int(n), int(k), lda, ldb, ldc,
+                                       transa != 0, tab, ldtab, int(blksize), s));
   return CFGMM_OK;
 }
 

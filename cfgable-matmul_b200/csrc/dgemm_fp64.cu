@@ -42,6 +42,14 @@ constexpr int CPT = TILE_DOUBLES / THREADS;  // copies per thread per operand ti
 //     k = tid % 32 of rows tid/32 + 8i: a warp reads 256 contiguous bytes.
 //   otherwise:   element (r,k) at x[k*ld + r] (r contiguous).  The thread copies
 //     r = tid % 128 of k = tid/128 + 2i: a warp reads 256 contiguous bytes.
+// Column mask of the masked GEMM (impl_matmul_non0tab.rs:196-207): element
+// (p, j) of B takes part only when tab[p * ldtab + j / blk] != 0.
+struct ColMask {
+  const uint8_t* tab;  // null: no mask
+  size_t ldtab;
+  int blk;
+};
+
 template <bool kRowsContig>
 struct TileCopier {
   const double* src;     // element i = 0 of the current K step
@@ -51,8 +59,13 @@ struct TileCopier {
   unsigned row_ok;       // bit i: element i's row is inside the matrix
   int kpos;              // k of element 0 relative to the K step
   int key;               // swizzle key of the thread's row (kRowsContig = false)
+  const uint8_t* mcol;   // mask column of the thread's row (masked B only), else null
+  size_t mstride;        // mask row stride (ldtab)
 
-  __device__ __forceinline__ void init(const double* x, size_t ld, int r0, int rmax, int tid) {
+  __device__ __forceinline__ void init(const double* x, size_t ld, int r0, int rmax, int tid,
+                                       ColMask mask = ColMask{nullptr, 0, 1}) {
+    mcol = nullptr;
+    mstride = 0;
     if (kRowsContig) {
       const int k = tid & 31, rb = tid >> 5;
       src = x + size_t(r0 + rb) * ld + k;
@@ -72,6 +85,10 @@ struct TileCopier {
       dst0 = r * BK + kb;
       row_ok = (r0 + r < rmax) ? 0xffffu : 0u;
       kpos = kb;
+      if (mask.tab && r0 + r < rmax) {
+        mcol = mask.tab + (r0 + r) / mask.blk + size_t(kb) * mask.ldtab;
+        mstride = mask.ldtab;
+      }
     }
   }
 
@@ -90,6 +107,7 @@ struct TileCopier {
       } else {
         ok = row_ok && 2 * i < krem;
         dst = dst0 + ((i ^ key) << 1);  // k = kb + 2i: chunk i, half kb
+        if (mcol && ok) ok = mcol[(size_t(kt) * BK + 2 * i) * mstride] != 0;
       }
       cp_async_8(S + dst, ok ? base + size_t(i) * step_i : src, ok);
     }
@@ -100,7 +118,7 @@ template <bool TA, bool TB>
 __global__ void __launch_bounds__(THREADS, 1)
 dgemm_fp64_kernel(double* __restrict__ c, const double* __restrict__ a,
                   const double* __restrict__ b, int m, int n, int k, size_t lda, size_t ldb,
-                  size_t ldc) {
+                  size_t ldc, ColMask mask) {
   extern __shared__ __align__(128) double smem[];
   double* As = smem;
   double* Bs = smem + STAGES * TILE_DOUBLES;
@@ -127,7 +145,7 @@ dgemm_fp64_kernel(double* __restrict__ c, const double* __restrict__ a,
   TileCopier<!TA> ca;
   TileCopier<TB> cb;
   ca.init(a, lda, m0, m, tid);
-  cb.init(b, ldb, n0, n, tid);
+  cb.init(b, ldb, n0, n, tid, mask);  // the mask only applies to a non-transposed B
 
   double acc[4][4][4];
 #pragma unroll
@@ -207,14 +225,14 @@ dgemm_fp64_kernel(double* __restrict__ c, const double* __restrict__ a,
 
 template <bool TA, bool TB>
 cudaError_t launch_t(double* c, const double* a, const double* b, int m, int n, int k,
-                     size_t lda, size_t ldb, size_t ldc, cudaStream_t stream) {
+                     size_t lda, size_t ldb, size_t ldc, ColMask mask, cudaStream_t stream) {
   auto kern = dgemm_fp64_kernel<TA, TB>;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          int(SMEM_BYTES));
   if (err != cudaSuccess) return err;
   const long long tiles = (long long)((m + BM - 1) / BM) * ((n + BN - 1) / BN);
   if (tiles > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-  kern<<<unsigned(tiles), THREADS, SMEM_BYTES, stream>>>(c, a, b, m, n, k, lda, ldb, ldc);
+  kern<<<unsigned(tiles), THREADS, SMEM_BYTES, stream>>>(c, a, b, m, n, k, lda, ldb, ldc, mask);
   return cudaGetLastError();
 }
 
@@ -224,10 +242,23 @@ cudaError_t dgemm_fp64(double* c, const double* a, const double* b, int m, int n
                        size_t lda, size_t ldb, size_t ldc, bool transa, bool transb,
                        cudaStream_t stream) {
   if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
-  if (!transa && !transb) return launch_t<false, false>(c, a, b, m, n, k, lda, ldb, ldc, stream);
-  if (!transa && transb) return launch_t<false, true>(c, a, b, m, n, k, lda, ldb, ldc, stream);
-  if (transa && !transb) return launch_t<true, false>(c, a, b, m, n, k, lda, ldb, ldc, stream);
-  return launch_t<true, true>(c, a, b, m, n, k, lda, ldb, ldc, stream);
+  const ColMask none{nullptr, 0, 1};
+  if (!transa && !transb)
+    return launch_t<false, false>(c, a, b, m, n, k, lda, ldb, ldc, none, stream);
+  if (!transa && transb)
+    return launch_t<false, true>(c, a, b, m, n, k, lda, ldb, ldc, none, stream);
+  if (transa && !transb)
+    return launch_t<true, false>(c, a, b, m, n, k, lda, ldb, ldc, none, stream);
+  return launch_t<true, true>(c, a, b, m, n, k, lda, ldb, ldc, none, stream);
+}
+
+cudaError_t dgemm_fp64_non0tab(double* c, const double* a, const double* b, int m, int n, int k,
+                               size_t lda, size_t ldb, size_t ldc, bool transa,
+                               const uint8_t* tab, size_t ldtab, int blk, cudaStream_t stream) {
+  if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
+  const ColMask mask{tab, ldtab, blk};
+  if (!transa) return launch_t<false, false>(c, a, b, m, n, k, lda, ldb, ldc, mask, stream);
+  return launch_t<true, false>(c, a, b, m, n, k, lda, ldb, ldc, mask, stream);
 }
 
 }  // namespace cfgmm

@@ -1,5 +1,6 @@
 // dgemm_fp64.cuh -- internal launcher of the FP64 tensor-core DGEMM.
 #pragma once
+#include <cstdint>
 #include <cuda_runtime.h>
 
 namespace cfgmm {
@@ -8,5 +9,11 @@ namespace cfgmm {
 cudaError_t dgemm_fp64(double* c, const double* a, const double* b, int m, int n, int k,
                        size_t lda, size_t ldb, size_t ldc, bool transa, bool transb,
                        cudaStream_t stream);
+
+// Masked GEMM (src/impl_matmul_non0tab.rs:210-306): B is not transposed;
+// element (p, j) of B takes part only when tab[p * ldtab + j / blk] != 0.
+cudaError_t dgemm_fp64_non0tab(double* c, const double* a, const double* b, int m, int n, int k,
+                               size_t lda, size_t ldb, size_t ldc, bool transa,
+                               const uint8_t* tab, size_t ldtab, int blk, cudaStream_t stream);
 
 }  // namespace cfgmm

@@ -153,10 +153,22 @@ emax_rows(const double* __restrict__ x, size_t ld, int rows, int k, int* __restr
   }
 }
 
+// Optional mask of the masked GEMM: element (r, p) of op(B)^T takes part only
+// when tab[p * ldtab + r / blk] != 0 (impl_matmul_non0tab.rs:196-207).
+struct Mask {
+  const uint8_t* tab;  // null: no mask
+  size_t ldtab;
+  int blk;
+  __device__ __forceinline__ bool on(int r, int p) const {
+    return !tab || tab[size_t(p) * ldtab + r / blk] != 0;
+  }
+};
+
 // element (r, p) at x[p*ld + r]: thread per r (coalesced), CTA rows of p chunks
 constexpr int kColChunk = 128;
 __global__ void __launch_bounds__(256)
-emax_cols(const double* __restrict__ x, size_t ld, int rows, int k, int* __restrict__ emax) {
+emax_cols(const double* __restrict__ x, size_t ld, int rows, int k, int* __restrict__ emax,
+          Mask mask) {
   const int r = blockIdx.x * 256 + threadIdx.x;
   const int p0 = blockIdx.y * kColChunk;
   if (r >= rows) return;
@@ -164,7 +176,7 @@ emax_cols(const double* __restrict__ x, size_t ld, int rows, int k, int* __restr
   double mx = 0.0;
   bool bad = false;
   for (int p = p0; p < p1; ++p) {
-    const double v = fabs(x[size_t(p) * ld + r]);
+    const double v = mask.on(r, p) ? fabs(x[size_t(p) * ld + r]) : 0.0;
     bad |= !(v <= 1.7976931348623157e308);
     mx = fmax(mx, v);
   }
@@ -254,13 +266,13 @@ residues_rows(const double* __restrict__ x, size_t ld, int rows, int k, size_t k
 // element (r, p) at x[p*ld + r]: 32 (r) x 64 (p) tiles transposed through shared memory
 __global__ void __launch_bounds__(256)
 residues_cols(const double* __restrict__ x, size_t ld, int rows, int k, size_t kpad,
-              const int* __restrict__ e, int8_t* __restrict__ Y, ResidueArgs a) {
+              const int* __restrict__ e, int8_t* __restrict__ Y, ResidueArgs a, Mask mask) {
   __shared__ double tile[64][33];
   const int r0 = blockIdx.x * 32, p0 = blockIdx.y * 64;
   const int tr = threadIdx.x & 31, tp = threadIdx.x >> 5;  // 8 rows of p per pass
   for (int pp = tp; pp < 64; pp += 8) {
     const int p = p0 + pp, r = r0 + tr;
-    tile[pp][tr] = (p < k && r < rows) ? x[size_t(p) * ld + r] : 0.0;
+    tile[pp][tr] = (p < k && r < rows && mask.on(r, p)) ? x[size_t(p) * ld + r] : 0.0;
   }
   __syncthreads();
   const size_t plane = size_t(rows) * kpad;
@@ -398,20 +410,21 @@ ResidueArgs residue_args(const OzakiPlan& p) {
 // `emax` is scratch for rows ints.
 cudaError_t prepare(const double* x, size_t ld, bool rows_contig, int rows, int k, size_t kpad,
                     int bits, int* emax, int* e, int8_t* Y, const ResidueArgs& ra,
-                    cudaStream_t s) {
+                    cudaStream_t s, Mask mask = Mask{nullptr, 0, 1}) {
   const int rb = (rows + 255) / 256;
   if (rows_contig) {
     emax_rows<<<rows, 256, 0, s>>>(x, ld, rows, k, emax);
   } else {
     fill_int<<<rb, 256, 0, s>>>(emax, rows, INT_MIN);
-    emax_cols<<<dim3(rb, (k + kColChunk - 1) / kColChunk), 256, 0, s>>>(x, ld, rows, k, emax);
+    emax_cols<<<dim3(rb, (k + kColChunk - 1) / kColChunk), 256, 0, s>>>(x, ld, rows, k, emax,
+                                                                         mask);
   }
   finalize_exps<<<rb, 256, 0, s>>>(emax, rows, bits, e);
   if (rows_contig) {
     residues_rows<<<rows, 256, 0, s>>>(x, ld, rows, k, kpad, e, Y, ra);
   } else {
     dim3 grid((rows + 31) / 32, (k + 63) / 64);
-    residues_cols<<<grid, 256, 0, s>>>(x, ld, rows, k, kpad, e, Y, ra);
+    residues_cols<<<grid, 256, 0, s>>>(x, ld, rows, k, kpad, e, Y, ra, mask);
   }
   return cudaGetLastError();
 }
@@ -433,7 +446,9 @@ size_t ozaki_dgemm_workspace(int m, int n, int k, int nmod) {
 
 cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int n, int k,
                         size_t lda, size_t ldb, size_t ldc, bool transa, bool transb, int nmod,
-                        void* workspace, cudaStream_t stream, const cudaEvent_t* events) {
+                        void* workspace, cudaStream_t stream, const cudaEvent_t* events,
+                        const uint8_t* tab, size_t ldtab, int blk) {
+  if (tab && transb) return cudaErrorInvalidValue;  // the masked GEMM has no transb
   if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
   auto mark = [&](int i) { if (events) cudaEventRecord(events[i], stream); };
   if (k > kOzakiMaxK) return cudaErrorInvalidValue;
@@ -453,7 +468,8 @@ cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int 
   cudaError_t err =
       prepare(a, lda, !transa, m, k, L.kpad, plan.alpha, emax, ea, a_res, ra, stream);
   if (err != cudaSuccess) return err;
-  err = prepare(b, ldb, transb, n, k, L.kpad, plan.beta, emax, eb, b_res, ra, stream);
+  err = prepare(b, ldb, transb, n, k, L.kpad, plan.beta, emax, eb, b_res, ra, stream,
+                Mask{tab, ldtab, blk > 0 ? blk : 1});
   if (err != cudaSuccess) return err;
 
   mark(1);

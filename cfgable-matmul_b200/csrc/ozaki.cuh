@@ -1,6 +1,7 @@
 // ozaki.cuh -- internal interface of the Ozaki-scheme split-precision paths.
 #pragma once
 #include <cstddef>
+#include <cstdint>
 #include <cuda_runtime.h>
 
 #include "gemm_i8.cuh"
@@ -41,10 +42,13 @@ size_t ozaki_dgemm_workspace(int m, int n, int k, int nmod);
 // C[i*ldc+j] += sum_p opA(i,p) opB(p,j) by INT8 tensor-core emulation; device
 // pointers; workspace of ozaki_dgemm_workspace bytes (256-byte aligned).
 // `events` (optional, 4 entries) are recorded before the residue preparation
-// and after the preparation, the INT8 GEMM and the reconstruction.
+// and after the preparation, the INT8 GEMM and the reconstruction.  With `tab`
+// this is the masked GEMM (B not transposed): element (p, j) of B takes part
+// only when tab[p * ldtab + j / blk] != 0.
 cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int n, int k,
                         size_t lda, size_t ldb, size_t ldc, bool transa, bool transb, int nmod,
                         void* workspace, cudaStream_t stream,
-                        const cudaEvent_t* events = nullptr);
+                        const cudaEvent_t* events = nullptr, const uint8_t* tab = nullptr,
+                        size_t ldtab = 0, int blk = 1);
 
 }  // namespace cfgmm

@@ -102,6 +102,41 @@ int cfgmm_matmul_dev(double* c, const double* a, const double* b, size_t m, size
                      size_t lda, size_t ldb, size_t ldc, uint8_t transa, uint8_t transb,
                      int precision, void* stream);
 
+/* ---- masked GEMM: C[i*ldc + j] += sum_{p: tab[p*ldtab + j/BLK]} opA(i,p) * b[p*ldb + j] ----
+ * Element (p, j) of B takes part only when its (row, column block) flag is
+ * set, whatever B holds there (impl_matmul_non0tab.rs:196-207).  B cannot be
+ * transposed: transb != 0 returns CFGMM_ERR_UNIMPLEMENTED, as the reference's
+ * `unimplemented!` (impl_matmul_non0tab.rs:181-183, 228-230). */
+
+/* Replaces matmul_anyway_full_non0tab (src/impl_matmul_non0tab.rs:308-326): BLKSIZE 48. */
+int cfgmm_matmul_anyway_full_non0tab(double* c, size_t c_len, const double* a, size_t a_len,
+                                     const double* b, size_t b_len, size_t m, size_t n, size_t k,
+                                     size_t lda, size_t ldb, size_t ldc, uint8_t transa,
+                                     uint8_t transb, const uint8_t* tab, size_t tab_len,
+                                     size_t ldtab);
+
+/* Replaces MatmulLoops::matmul_loop_parallel_mnk_pack_a_non0tab::<BLKSIZE>
+ * (src/impl_matmul_non0tab.rs:210-306); any blksize >= 1. */
+int cfgmm_matmul_loop_parallel_mnk_pack_a_non0tab(double* c, size_t c_len, const double* a,
+                                                  size_t a_len, const double* b, size_t b_len,
+                                                  size_t m, size_t n, size_t k, size_t lda,
+                                                  size_t ldb, size_t ldc, uint8_t transa,
+                                                  uint8_t transb, const uint8_t* tab,
+                                                  size_t tab_len, size_t ldtab, size_t blksize);
+
+/* Host-pointer masked GEMM with an explicit arithmetic (CFGMM_PREC_*). */
+int cfgmm_matmul_non0tab_ex(double* c, size_t c_len, const double* a, size_t a_len,
+                            const double* b, size_t b_len, size_t m, size_t n, size_t k,
+                            size_t lda, size_t ldb, size_t ldc, uint8_t transa, uint8_t transb,
+                            const uint8_t* tab, size_t tab_len, size_t ldtab, size_t blksize,
+                            int precision);
+
+/* Device-pointer masked GEMM enqueued on `stream`; `tab` is a device pointer. */
+int cfgmm_matmul_non0tab_dev(double* c, const double* a, const double* b, size_t m, size_t n,
+                             size_t k, size_t lda, size_t ldb, size_t ldc, uint8_t transa,
+                             uint8_t transb, const uint8_t* tab, size_t ldtab, size_t blksize,
+                             int precision, void* stream);
+
 /* No counterpart in the reference: benchmark instrumentation.  The device-
  * pointer DGEMM with CUDA events (cudaEvent_t, passed as void*) recorded on
  * `stream` at its phase boundaries: FP64 -- events[0] before and events[1]

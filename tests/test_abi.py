@@ -71,6 +71,22 @@ def test_gemm_zero_sizes_are_noops(cm):
     assert np.all(c == 0)
 
 
+def test_masked_gemm_transb_panics_first(cm):
+    # impl_matmul_non0tab.rs:228-230: transb panics before anything else, even
+    # for a zero-sized problem; no device is touched.
+    c = np.zeros((2, 2))
+    with pytest.raises(NotImplementedError):
+        cm.matmul_anyway_full_non0tab(c, np.ones((2, 2)), np.ones((2, 2)), 0, 0, 0, 2, 2, 2,
+                                      False, True, np.ones((2, 1), np.uint8), 1)
+
+
+def test_masked_gemm_short_tab(cm):
+    c, a, b = _gemm_args()
+    with pytest.raises(ValueError, match="slice too short"):
+        cm.matmul_anyway_full_non0tab(c, a, b, 4, 5, 6, 6, 5, 5, False, False,
+                                      np.ones(3, np.uint8), 1)
+
+
 def test_unknown_precision(cm):
     c, a, b = _gemm_args()
     with pytest.raises(ValueError, match="precision"):
