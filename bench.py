@@ -380,32 +380,47 @@ def run_ours(args, ranks: Ranks):
     tab = torch.from_numpy(p.tab).to(dev)
     rho = torch.zeros(p.nset, p.ngrid, dtype=torch.float64, device=dev)
 
-    def aodm_step():
-        rc = lib.cfgmm_aodmao2rho_dev(rho.data_ptr(), dms.data_ptr(), ao.data_ptr(), ao.data_ptr(),
+    def aodm_step(out, precision):
+        rc = lib.cfgmm_aodmao2rho_dev(out.data_ptr(), dms.data_ptr(), ao.data_ptr(), ao.data_ptr(),
                                       p.nao, p.ngrid, p.nao, p.ngrid, p.nset, tab.data_ptr(),
-                                      p.nblk, p.blksize, FP64, stream.cuda_stream)
+                                      p.nblk, p.blksize, precision, stream.cuda_stream)
         if rc != 0:
             cm._raise(rc)
 
-    for _ in range(args.warmup):
-        aodm_step()
-    torch.cuda.synchronize()
-    ranks.barrier()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
-    ev[0].record(stream)
-    for i in range(args.steps):
-        aodm_step()
-        ev[i + 1].record(stream)
-    torch.cuda.synchronize()
-    atot = ranks.max(ev[0].elapsed_time(ev[-1]))
+    def aodm_timed(precision):
+        for _ in range(args.warmup):
+            aodm_step(rho, precision)
+        torch.cuda.synchronize()
+        ranks.barrier()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+        ev[0].record(stream)
+        for i in range(args.steps):
+            aodm_step(rho, precision)
+            ev[i + 1].record(stream)
+        torch.cuda.synchronize()
+        return ranks.max(ev[0].elapsed_time(ev[-1]))
+
     aflops = p.flops()
+    atot = aodm_timed(FP64)
+    stot = aodm_timed(SPLIT)
+    r64 = torch.zeros(p.nset, p.ngrid, dtype=torch.float64, device=dev)
+    rsp = torch.zeros(p.nset, p.ngrid, dtype=torch.float64, device=dev)
+    aodm_step(r64, FP64)
+    aodm_step(rsp, SPLIT)
+    torch.cuda.synchronize()
+    aodm_err = float((rsp - r64).abs().max() / r64.abs().max())
     clk = clocks.stop()
     aodm = {"workload": p.name + f", blocks of {p.blksize}, tile density {p.density():.3f}",
-            "precision": "fp64", "value": ranks.world * aflops * args.steps / (atot * 1e-3) / 1e9,
-            "unit": "GFLOP/s", "ms_per_step": atot / args.steps, "flops_per_step": aflops,
-            "flops": "sum_s sum_b (2|I_b|^2 + 2|I_b|)|b| (masked)",
-            "frac_of_dmma_peak": (aflops / (atot / args.steps * 1e-3) / 1e12) / dmma_peak,
-            "launches_per_step": 4}
+            "flops_per_step": aflops, "flops": "sum_s sum_b (2|I_b|^2 + 2|I_b|)|b| (masked)",
+            "fp64": {"value": ranks.world * aflops * args.steps / (atot * 1e-3) / 1e9,
+                     "unit": "GFLOP/s", "ms_per_step": atot / args.steps,
+                     "frac_of_dmma_peak": (aflops / (atot / args.steps * 1e-3) / 1e12) / dmma_peak,
+                     "launches_per_step": 4},
+            "split": {"value": ranks.world * aflops * args.steps / (stot * 1e-3) / 1e9,
+                      "unit": "GFLOP/s", "ms_per_step": stot / args.steps,
+                      "error_vs_fp64": aodm_err, "scheme": "7-digit slices, 28 INT8 products",
+                      "launches_per_step": 7},
+            "speedup_split_vs_fp64": atot / stot}
 
     cpu = cpu_dgemm_sample() if (ranks.rank == 0 and ranks.world == 1 and not args.no_cpu) else None
     value = ranks.world * flops * args.steps / (split_ms * 1e-3) / 1e12

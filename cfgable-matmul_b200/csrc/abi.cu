@@ -18,6 +18,7 @@
 
 #include "../../include/cfgmm.h"
 #include "aodmao2rho_fp64.cuh"
+#include "aodmao2rho_split.cuh"
 #include "dgemm_fp64.cuh"
 #include "gemm_i8.cuh"
 #include "ozaki.cuh"
@@ -174,10 +175,12 @@ int check_split_gemm(size_t k) {
   return CFGMM_OK;
 }
 
-// Reads the sticky error word of the tcgen05 kernels after a synchronised call.
+// Reads the sticky error words of the tcgen05 kernels after a synchronised call.
 int check_device_waits() {
-  int code = 0;
+  int code = 0, code2 = 0;
   CFGMM_CUDA(cfgmm::gemm_i8_read_error(&code));
+  CFGMM_CUDA(cfgmm::aodmao2rho_split_read_error(&code2));
+  if (code == 0) code = code2;
   if (code != 0) {
     char msg[128];
     std::snprintf(msg, sizeof(msg), "a tensor-core pipeline wait timed out (code %d)", code);
@@ -322,8 +325,9 @@ int aodm_host(double* rhos, size_t rhos_len, const double* dms, size_t dms_len,
                       stride_ao, stride_grid, nao, ngrid, nset, tab, tab_len, ldtab, blksize, &ex);
   if (rc != CFGMM_OK) return rc;
   if ((rc = check_precision(precision)) != CFGMM_OK) return rc;
-  if (precision != CFGMM_PREC_FP64)
-    return fail(CFGMM_ERR_UNIMPLEMENTED, "split precision for the AO-DM-AO contraction");
+  const bool split = precision == CFGMM_PREC_OZAKI_INT8;
+  if (split && nao > 65536)
+    return fail(CFGMM_ERR_UNIMPLEMENTED, "split-precision AO-DM-AO supports nao <= 65536");
   if (ex.rhos == 0) return CFGMM_OK;
   int dev;
   if ((rc = current_device(&dev)) != CFGMM_OK) return rc;
@@ -337,7 +341,8 @@ int aodm_host(double* rhos, size_t rhos_len, const double* dms, size_t dms_len,
   const size_t o_tab = o_rhs + (same_ao ? 0 : align256(ex.ao * 8));
   const size_t o_rho = o_tab + align256(ex.tab);
   const size_t o_ws = o_rho + align256(ex.rhos * 8);
-  const size_t ws = cfgmm::aodmao2rho_fp64_workspace(nao, ngrid, nset, blksize);
+  const size_t ws = split ? cfgmm::aodmao2rho_split_workspace(nao, ngrid, nset, blksize)
+                          : cfgmm::aodmao2rho_fp64_workspace(nao, ngrid, nset, blksize);
   if ((rc = reserve(st, o_ws + ws)) != CFGMM_OK) return rc;
   char* base = static_cast<char*>(st->buf);
   double* d_dms = reinterpret_cast<double*>(base + o_dms);
@@ -351,11 +356,19 @@ int aodm_host(double* rhos, size_t rhos_len, const double* dms, size_t dms_len,
     CFGMM_CUDA(cudaMemcpyAsync(d_rhs, ao_rhs, ex.ao * 8, cudaMemcpyHostToDevice, st->stream));
   CFGMM_CUDA(cudaMemcpyAsync(d_tab, tab, ex.tab, cudaMemcpyHostToDevice, st->stream));
   CFGMM_CUDA(cudaMemcpyAsync(d_rho, rhos, ex.rhos * 8, cudaMemcpyHostToDevice, st->stream));
-  CFGMM_CUDA(cfgmm::aodmao2rho_fp64(d_rho, d_dms, d_lhs, same_ao ? d_lhs : d_rhs, stride_ao,
-                                    stride_grid, int(nao), int(ngrid), int(nset), d_tab, ldtab,
-                                    int(blksize), base + o_ws, st->stream));
+  if (split) {
+    CFGMM_CUDA(cfgmm::aodmao2rho_split_reset_error(st->stream));
+    CFGMM_CUDA(cfgmm::aodmao2rho_split(d_rho, d_dms, d_lhs, same_ao ? d_lhs : d_rhs, stride_ao,
+                                       stride_grid, int(nao), int(ngrid), int(nset), d_tab, ldtab,
+                                       int(blksize), base + o_ws, st->stream));
+  } else {
+    CFGMM_CUDA(cfgmm::aodmao2rho_fp64(d_rho, d_dms, d_lhs, same_ao ? d_lhs : d_rhs, stride_ao,
+                                      stride_grid, int(nao), int(ngrid), int(nset), d_tab, ldtab,
+                                      int(blksize), base + o_ws, st->stream));
+  }
   CFGMM_CUDA(cudaMemcpyAsync(rhos, d_rho, ex.rhos * 8, cudaMemcpyDeviceToHost, st->stream));
   CFGMM_CUDA(cudaStreamSynchronize(st->stream));
+  if (split) return check_device_waits();
   return CFGMM_OK;
 }
 
@@ -599,19 +612,23 @@ int cfgmm_aodmao2rho_dev(double* rhos, const double* dms, const double* ao_lhs,
                       stride_ao, stride_grid, nao, ngrid, nset, tab, SIZE_MAX, ldtab, blksize, &ex);
   if (rc != CFGMM_OK) return rc;
   if ((rc = check_precision(precision)) != CFGMM_OK) return rc;
-  if (precision != CFGMM_PREC_FP64)
-    return fail(CFGMM_ERR_UNIMPLEMENTED, "split precision for the AO-DM-AO contraction");
+  const bool split = precision == CFGMM_PREC_OZAKI_INT8;
+  if (split && nao > 65536)
+    return fail(CFGMM_ERR_UNIMPLEMENTED, "split-precision AO-DM-AO supports nao <= 65536");
   if (ex.rhos == 0) return CFGMM_OK;
   int dev;
   if ((rc = current_device(&dev)) != CFGMM_OK) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   // Stream-ordered scratch: safe against concurrent calls on other streams.
   void* ws = nullptr;
-  const size_t bytes = cfgmm::aodmao2rho_fp64_workspace(nao, ngrid, nset, blksize);
+  const size_t bytes = split ? cfgmm::aodmao2rho_split_workspace(nao, ngrid, nset, blksize)
+                             : cfgmm::aodmao2rho_fp64_workspace(nao, ngrid, nset, blksize);
   CFGMM_CUDA(cudaMallocAsync(&ws, bytes, s));
-  cudaError_t err = cfgmm::aodmao2rho_fp64(rhos, dms, ao_lhs, ao_rhs, stride_ao, stride_grid,
-                                           int(nao), int(ngrid), int(nset), tab, ldtab,
-                                           int(blksize), ws, s);
+  cudaError_t err =
+      split ? cfgmm::aodmao2rho_split(rhos, dms, ao_lhs, ao_rhs, stride_ao, stride_grid, int(nao),
+                                      int(ngrid), int(nset), tab, ldtab, int(blksize), ws, s)
+            : cfgmm::aodmao2rho_fp64(rhos, dms, ao_lhs, ao_rhs, stride_ao, stride_grid, int(nao),
+                                     int(ngrid), int(nset), tab, ldtab, int(blksize), ws, s);
   cudaError_t err2 = cudaFreeAsync(ws, s);
   if (err != cudaSuccess) return cuda_fail(err, "aodmao2rho_fp64");
   if (err2 != cudaSuccess) return cuda_fail(err2, "cudaFreeAsync");

@@ -387,6 +387,12 @@ Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk) {
 }
 }  // namespace
 
+cudaError_t aodm_block_lists_launch(const uint8_t* tab, size_t ldtab, int nao, int nblk,
+                                    int* lists, int* counts, cudaStream_t stream) {
+  aodm_block_lists<<<nblk, 256, 0, stream>>>(tab, ldtab, nao, nblk, lists, counts);
+  return cudaGetLastError();
+}
+
 size_t aodmao2rho_fp64_workspace(size_t nao, size_t ngrid, size_t nset, size_t blk) {
   return layout(nao, ngrid, nset, blk).total;
 }

@@ -16,4 +16,9 @@ cudaError_t aodmao2rho_fp64(double* rhos, const double* dms, const double* ao_lh
                             int ngrid, int nset, const uint8_t* tab, size_t ldtab, int blk,
                             void* workspace, cudaStream_t stream);
 
+// Builds the per-block active AO lists: lists[b*nao + i] = i-th u (ascending)
+// with tab[u*ldtab + b] != 0, counts[b] = their number.
+cudaError_t aodm_block_lists_launch(const uint8_t* tab, size_t ldtab, int nao, int nblk,
+                                    int* lists, int* counts, cudaStream_t stream);
+
 }  // namespace cfgmm

@@ -93,6 +93,23 @@ __device__ __forceinline__ void prefetch_tensormap(const CUtensorMap* map) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
 
+// Plain (non-tensor) bulk copy global -> shared, completing on `bar`; both
+// addresses 16-byte aligned, `bytes` a multiple of 16.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes,
+                                          uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Orders this thread's generic-proxy shared-memory writes before later
+// async-proxy reads (tcgen05.mma operands written by threads).
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 // ---- TMEM -----------------------------------------------------------------------
 // Allocation and release are warp-wide (.sync.aligned): call from one full warp.
 __device__ __forceinline__ void tmem_alloc(uint32_t* dst_smem, uint32_t ncols) {
@@ -167,6 +184,35 @@ __device__ __forceinline__ uint64_t smem_desc_k128(uint32_t addr) {
   d |= uint64_t(1) << 46;                    // descriptor version (tcgen05)
   d |= uint64_t(2) << 61;                    // layout: 128-byte swizzle
   return d;
+}
+
+// Descriptor of a K-major operand tile with 32-byte swizzling: rows of 32
+// bytes (one INT8 K=32 step), 8-row (256-byte) atoms at a 256-byte stride;
+// within an atom the 16-byte half c of row r sits at half c ^ ((r >> 2) & 1).
+__device__ __forceinline__ uint64_t smem_desc_k32(uint32_t addr) {
+  uint64_t d = 0;
+  d |= uint64_t((addr >> 4) & 0x3fff);  // start address
+  d |= uint64_t(1) << 16;               // leading byte offset (unused here)
+  d |= uint64_t(256 >> 4) << 32;        // stride byte offset: 8 rows x 32 B
+  d |= uint64_t(1) << 46;               // descriptor version (tcgen05)
+  d |= uint64_t(6) << 61;               // layout: 32-byte swizzle
+  return d;
+}
+
+// Byte offset of (row, 16-byte half) inside a 32-byte-swizzled K-major tile.
+__host__ __device__ __forceinline__ uint32_t sw32_offset(uint32_t row, uint32_t half) {
+  return row * 32u + ((half ^ ((row >> 2) & 1u)) << 4);
+}
+
+// 32 lanes x 16 consecutive 32-bit columns.
+__device__ __forceinline__ void tmem_ld_32x32b_x16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+        "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
 }
 
 // Instruction descriptor of tcgen05.mma kind::i8: signed INT8 A and B, both
