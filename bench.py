@@ -418,7 +418,7 @@ def run_ours(args, ranks: Ranks):
                      "launches_per_step": 4},
             "split": {"value": ranks.world * aflops * args.steps / (stot * 1e-3) / 1e9,
                       "unit": "GFLOP/s", "ms_per_step": stot / args.steps,
-                      "error_vs_fp64": aodm_err, "scheme": "7-digit slices, 28 INT8 products",
+                      "error_vs_fp64": aodm_err, "scheme": "8-digit slices, 36 INT8 products",
                       "launches_per_step": 7},
             "speedup_split_vs_fp64": atot / stot}
 
@@ -499,8 +499,9 @@ def run_profile_case(args):
         for _ in range(args.reps):
             rc = lib.cfgmm_aodmao2rho_dev(rho.data_ptr(), dms.data_ptr(), ao.data_ptr(),
                                           ao.data_ptr(), p.nao, p.ngrid, p.nao, p.ngrid, p.nset,
-                                          tab.data_ptr(), p.nblk, p.blksize, cm.PREC_FP64,
-                                          stream.cuda_stream)
+                                          tab.data_ptr(), p.nblk, p.blksize,
+                                          cm.PREC_OZAKI_INT8 if args.profile == "aodm_split"
+                                          else cm.PREC_FP64, stream.cuda_stream)
             assert rc == 0, rc
     torch.cuda.synchronize()
     print(f"profile case {args.profile} done", flush=True)
@@ -513,7 +514,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
-    ap.add_argument("--profile", choices=["dgemm", "split", "aodm"], default=None,
+    ap.add_argument("--profile", choices=["dgemm", "split", "aodm", "aodm_split"], default=None,
                     help="run one kernel on one case (ncu target) and exit")
     ap.add_argument("--m", type=int, default=4096)
     ap.add_argument("--n", type=int, default=4096)

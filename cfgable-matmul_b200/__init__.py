@@ -34,6 +34,7 @@ import numpy as np
 __all__ = [
     "MatmulLoops", "matmul_anyway_full", "aodmao2rho_anyway", "matmul_ex", "aodmao2rho_ex",
     "matmul_anyway_full_non0tab", "matmul_non0tab_ex",
+    "aodmao2rho_noalloc", "AodmPlan", "eval_ao", "mask_ao",
     "PREC_FP64", "PREC_OZAKI_INT8", "CfgmmError", "lib", "library_path",
 ]
 
@@ -48,6 +49,14 @@ ERR_NO_DEVICE = -4
 ERR_OUT_OF_MEMORY = -5
 ERR_TIMEOUT = -6
 ERR_BUSY = -7
+
+class _Batch(ctypes.Structure):
+    """struct cfgmm_aodm_batch"""
+    _fields_ = [("rhos", ctypes.c_void_p), ("ao_lhs", ctypes.c_void_p),
+                ("ao_rhs", ctypes.c_void_p), ("tab", ctypes.c_void_p),
+                ("stride_grid", ctypes.c_size_t), ("ngrid", ctypes.c_size_t),
+                ("ldtab", ctypes.c_size_t), ("nset", ctypes.c_size_t)]
+
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 library_path = os.path.join(_HERE, "libcfgmm.so")
@@ -108,6 +117,21 @@ def lib() -> ctypes.CDLL:
         L.cfgmm_last_error.restype = ctypes.c_char_p
         L.cfgmm_version.restype = I
         L.cfgmm_release_workspace.restype = I
+        L.cfgmm_aodmao2rho_dev_noalloc.argtypes = [P, P, P, P, S, S, S, S, S, P, S, S, P]
+        L.cfgmm_aodmao2rho_dev_noalloc.restype = I
+        L.cfgmm_aodm_plan_create.argtypes = [ctypes.POINTER(P), ctypes.POINTER(_Batch), S, P, S,
+                                             S, S, S, I, I, P]
+        L.cfgmm_aodm_plan_create.restype = I
+        L.cfgmm_aodm_plan_run.argtypes = [P, P]
+        L.cfgmm_aodm_plan_run.restype = I
+        L.cfgmm_aodm_plan_info.argtypes = [P]
+        L.cfgmm_aodm_plan_info.restype = ctypes.c_char_p
+        L.cfgmm_aodm_plan_destroy.argtypes = [P]
+        L.cfgmm_aodm_plan_destroy.restype = I
+        L.cfgmm_eval_ao_dev.argtypes = [P, S, P, S, P, P, P, P, P, S, P, S, P]
+        L.cfgmm_eval_ao_dev.restype = I
+        L.cfgmm_mask_ao_dev.argtypes = [P, S, S, P, P, S, P, ctypes.c_double, P, S, S, P]
+        L.cfgmm_mask_ao_dev.restype = I
         _lib = L
     return _lib
 
@@ -255,6 +279,87 @@ def aodmao2rho_anyway(rhos, dms, ao_lhs, ao_rhs, strides, shape, nset, tab, ldta
     pt, lt = _host(_as_tab(tab), np.uint8)
     _raise(lib().cfgmm_aodmao2rho_anyway(pr, lr, pd, ld, pl, ll, pq, lq, stride_ao, stride_grid,
                                          nao, ngrid, nset, pt, lt, ldtab))
+
+
+def aodmao2rho_noalloc(rhos, dms, ao_lhs, ao_rhs, strides, shape, nset, tab, ldtab,
+                       blksize=48) -> None:
+    """The FP64 contraction on device tensors with no allocation: scratch lives
+    in a fixed static device array, so overlapping calls race (see cfgmm.h)."""
+    stride_ao, stride_grid = strides
+    nao, ngrid = shape
+    tab = _as_tab(tab)
+    _raise(lib().cfgmm_aodmao2rho_dev_noalloc(
+        _dev(rhos, "torch.float64"), _dev(dms, "torch.float64"), _dev(ao_lhs, "torch.float64"),
+        _dev(ao_rhs, "torch.float64"), stride_ao, stride_grid, nao, ngrid, nset,
+        _dev(tab, "torch.uint8"), ldtab, blksize, _stream_ptr()))
+
+
+class AodmPlan:
+    """Many grid batches of one molecule contracted by one persistent launch.
+
+    ``batches`` is a list of ``(rhos, ao_lhs, ao_rhs, tab, nset)`` CUDA tensors
+    (rhos (>=nset, ngrid), phi (nao, ngrid), tab (nao, nblk) uint8); ``dms`` is
+    (nset_max, nao, nao).  The tensors are referenced, not copied: phi and the
+    masks must stay unchanged while the plan lives, the contents of ``dms`` may
+    change between runs.  ``run()`` accumulates into every batch's rho on the
+    current stream.  No counterpart in the reference, whose callers loop over
+    grid batches (src/impl_matmul.rs:354-355 is the grid loop of its driver)."""
+
+    def __init__(self, batches, dms, blksize=64, precision=PREC_FP64, graph=True, tune=True):
+        self._keep = (list(batches), dms)
+        nao = dms.shape[-1]
+        arr = (_Batch * max(1, len(batches)))()
+        for i, (rhos, ao_lhs, ao_rhs, tab, nset) in enumerate(batches):
+            tab = _as_tab(tab)
+            arr[i] = _Batch(_dev(rhos, "torch.float64"), _dev(ao_lhs, "torch.float64"),
+                            _dev(ao_rhs, "torch.float64"), _dev(tab, "torch.uint8"),
+                            ao_lhs.shape[1], ao_lhs.shape[1], tab.shape[1], nset)
+        flags = (0 if graph else 1) | (0 if tune else 2)
+        h = ctypes.c_void_p()
+        _raise(lib().cfgmm_aodm_plan_create(ctypes.byref(h), arr, len(batches),
+                                            _dev(dms, "torch.float64"), nao, nao, dms.shape[0],
+                                            blksize, precision, flags, _stream_ptr()))
+        self._h = h
+
+    def run(self) -> None:
+        _raise(lib().cfgmm_aodm_plan_run(self._h, _stream_ptr()))
+
+    def info(self) -> dict:
+        import json
+        return json.loads(lib().cfgmm_aodm_plan_info(self._h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().cfgmm_aodm_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def eval_ao(ao, points, shell_xyz, shell_l, shell_alpha, shell_norm, shell_row,
+            shell_block_max=None, blksize=64) -> None:
+    """phi (nao, ngrid) of Gaussian shells (l <= 3, real solid harmonics) on the
+    points (ngrid, 3), all CUDA tensors; optionally max|phi| per (shell, block)."""
+    ngrid = points.shape[0]
+    _raise(lib().cfgmm_eval_ao_dev(
+        _dev(ao, "torch.float64"), ao.shape[1], _dev(points, "torch.float64"), ngrid,
+        _dev(shell_xyz, "torch.float64"), _dev(shell_l, "torch.int32"),
+        _dev(shell_alpha, "torch.float64"), _dev(shell_norm, "torch.float64"),
+        _dev(shell_row, "torch.int32"), shell_l.shape[0],
+        None if shell_block_max is None else _dev(shell_block_max, "torch.float64"), blksize,
+        _stream_ptr()))
+
+
+def mask_ao(ao, ngrid, shell_l, shell_row, shell_block_max, threshold, tab, blksize=64) -> None:
+    """tab[row, b] = shell_block_max[shell(row), b] > threshold; phi zeroed where 0."""
+    _raise(lib().cfgmm_mask_ao_dev(
+        _dev(ao, "torch.float64"), ao.shape[1], ngrid, _dev(shell_l, "torch.int32"),
+        _dev(shell_row, "torch.int32"), shell_l.shape[0], _dev(shell_block_max, "torch.float64"),
+        float(threshold), _dev(tab, "torch.uint8"), tab.shape[1], blksize, _stream_ptr()))
 
 
 class MatmulLoops:

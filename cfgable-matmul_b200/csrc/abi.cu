@@ -19,6 +19,7 @@
 #include "../../include/cfgmm.h"
 #include "aodmao2rho_fp64.cuh"
 #include "aodmao2rho_split.cuh"
+#include "ao_eval.cuh"
 #include "dgemm_fp64.cuh"
 #include "gemm_i8.cuh"
 #include "ozaki.cuh"
@@ -326,8 +327,8 @@ int aodm_host(double* rhos, size_t rhos_len, const double* dms, size_t dms_len,
   if (rc != CFGMM_OK) return rc;
   if ((rc = check_precision(precision)) != CFGMM_OK) return rc;
   const bool split = precision == CFGMM_PREC_OZAKI_INT8;
-  if (split && nao > 65536)
-    return fail(CFGMM_ERR_UNIMPLEMENTED, "split-precision AO-DM-AO supports nao <= 65536");
+  if (split && nao > 65535)
+    return fail(CFGMM_ERR_UNIMPLEMENTED, "split-precision AO-DM-AO supports nao <= 65535");
   if (ex.rhos == 0) return CFGMM_OK;
   int dev;
   if ((rc = current_device(&dev)) != CFGMM_OK) return rc;
@@ -613,8 +614,8 @@ int cfgmm_aodmao2rho_dev(double* rhos, const double* dms, const double* ao_lhs,
   if (rc != CFGMM_OK) return rc;
   if ((rc = check_precision(precision)) != CFGMM_OK) return rc;
   const bool split = precision == CFGMM_PREC_OZAKI_INT8;
-  if (split && nao > 65536)
-    return fail(CFGMM_ERR_UNIMPLEMENTED, "split-precision AO-DM-AO supports nao <= 65536");
+  if (split && nao > 65535)
+    return fail(CFGMM_ERR_UNIMPLEMENTED, "split-precision AO-DM-AO supports nao <= 65535");
   if (ex.rhos == 0) return CFGMM_OK;
   int dev;
   if ((rc = current_device(&dev)) != CFGMM_OK) return rc;
@@ -632,6 +633,45 @@ int cfgmm_aodmao2rho_dev(double* rhos, const double* dms, const double* ao_lhs,
   cudaError_t err2 = cudaFreeAsync(ws, s);
   if (err != cudaSuccess) return cuda_fail(err, "aodmao2rho_fp64");
   if (err2 != cudaSuccess) return cuda_fail(err2, "cudaFreeAsync");
+  return CFGMM_OK;
+}
+
+int cfgmm_eval_ao_dev(double* ao, size_t stride_grid, const double* points, size_t ngrid,
+                      const double* shell_xyz, const int* shell_l, const double* shell_alpha,
+                      const double* shell_norm, const int* shell_row, size_t nshell,
+                      double* shell_block_max, size_t blksize, void* stream) {
+  g_last_error.clear();
+  if (ngrid == 0 || nshell == 0) return CFGMM_OK;
+  if (!ao || !points || !shell_xyz || !shell_l || !shell_alpha || !shell_norm || !shell_row)
+    return fail(CFGMM_ERR_INVALID_ARGUMENT, "null pointer");
+  if (stride_grid < ngrid || !fits_int(ngrid) || nshell > 65535 || blksize == 0 ||
+      !fits_int(blksize))
+    return fail(CFGMM_ERR_INVALID_ARGUMENT, "invalid sizes");
+  int dev;
+  int rc = current_device(&dev);
+  if (rc != CFGMM_OK) return rc;
+  CFGMM_CUDA(cfgmm::eval_ao(ao, stride_grid, points, int(ngrid), shell_xyz, shell_l, shell_alpha,
+                            shell_norm, shell_row, int(nshell), shell_block_max, int(blksize),
+                            static_cast<cudaStream_t>(stream)));
+  return CFGMM_OK;
+}
+
+int cfgmm_mask_ao_dev(double* ao, size_t stride_grid, size_t ngrid, const int* shell_l,
+                      const int* shell_row, size_t nshell, const double* shell_block_max,
+                      double threshold, uint8_t* tab, size_t ldtab, size_t blksize, void* stream) {
+  g_last_error.clear();
+  if (ngrid == 0 || nshell == 0) return CFGMM_OK;
+  if (!ao || !shell_l || !shell_row || !shell_block_max || !tab)
+    return fail(CFGMM_ERR_INVALID_ARGUMENT, "null pointer");
+  if (stride_grid < ngrid || !fits_int(ngrid) || nshell > 65535 || blksize == 0 ||
+      !fits_int(blksize) || ldtab < (ngrid + blksize - 1) / blksize)
+    return fail(CFGMM_ERR_INVALID_ARGUMENT, "invalid sizes");
+  int dev;
+  int rc = current_device(&dev);
+  if (rc != CFGMM_OK) return rc;
+  CFGMM_CUDA(cfgmm::mask_ao(ao, stride_grid, int(ngrid), shell_l, shell_row, int(nshell),
+                            shell_block_max, threshold, tab, ldtab, int(blksize),
+                            static_cast<cudaStream_t>(stream)));
   return CFGMM_OK;
 }
 

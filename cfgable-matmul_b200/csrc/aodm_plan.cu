@@ -1,0 +1,364 @@
+// aodm_plan.cu -- many grid batches of one molecule in one persistent,
+// graph-captured launch, with tile shapes chosen by an autotuner.
+//
+// A plan is built once for a set of grid batches whose phi tables and masks
+// stay resident and unchanged (the density matrices may change between runs,
+// as in an SCF loop).  Building it:
+//   1. active AO lists of every block of every batch (one kernel per batch);
+//   2. one global work list (batch, 64-point tile, 64-row tile of I(b)),
+//      heaviest items first, so the persistent kernel's atomic counter hands
+//      out work largest-first and the tail stays short;
+//   3. autotuning: every tile configuration of the main kernel (density
+//      matrices per ao_rhs tile x compacted AOs per stage) is timed on this
+//      very problem and the fastest kept; results are cached on disk
+//      (CFGMM_AUTOTUNE_CACHE, default $HOME/.cache/cfgmm/autotune.txt) under a
+//      key made of the problem's size classes;
+//   4. the run -- counter reset, persistent kernel, reduction -- is captured
+//      in a CUDA graph, so a run is one graph launch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <sys/stat.h>
+#include <vector>
+
+#include "../../include/cfgmm.h"
+#include "aodmao2rho_fp64.cuh"
+
+namespace cfgmm {
+void set_last_error(const std::string& msg);
+}
+
+struct cfgmm_aodm_plan {
+  int dev = 0;
+  cfgmm::AodmArgs args{};
+  cfgmm::AodmConfig cfg{1, 32};
+  int npairs = 0, nitems = 0;
+  void* mem = nullptr;  // one device allocation for lists, descriptors, work list, partials
+  int2* rpairs = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::string info;
+};
+
+namespace {
+
+int fail(int status, const std::string& msg) {
+  cfgmm::set_last_error(msg);
+  return status;
+}
+
+int cuda_fail(cudaError_t err, const char* where) {
+  return fail(err == cudaErrorMemoryAllocation ? CFGMM_ERR_OUT_OF_MEMORY : CFGMM_ERR_CUDA,
+              std::string(where) + ": " + cudaGetErrorName(err) + " (" + cudaGetErrorString(err) +
+                  ")");
+}
+
+#define PLAN_CUDA(call)                                  \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
+  } while (0)
+
+size_t a256(size_t v) { return (v + 255) / 256 * 256; }
+
+// ---- autotune cache: one "key ns tk ms" line per entry -------------------
+std::mutex g_cache_mu;
+
+std::string cache_path() {
+  if (const char* p = std::getenv("CFGMM_AUTOTUNE_CACHE")) return p;
+  const char* home = std::getenv("HOME");
+  return std::string(home ? home : "/tmp") + "/.cache/cfgmm/autotune.txt";
+}
+
+bool cache_lookup(const std::string& key, cfgmm::AodmConfig* cfg) {
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  FILE* f = std::fopen(cache_path().c_str(), "r");
+  if (!f) return false;
+  char k[256];
+  int ns, tk;
+  double ms;
+  bool found = false;
+  while (std::fscanf(f, "%255s %d %d %lf", k, &ns, &tk, &ms) == 4)
+    if (key == k) {
+      *cfg = cfgmm::AodmConfig{ns, tk};
+      found = true;
+    }
+  std::fclose(f);
+  return found;
+}
+
+void cache_store(const std::string& key, const cfgmm::AodmConfig& cfg, double ms) {
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  const std::string path = cache_path();
+  const size_t slash = path.rfind('/');
+  if (slash != std::string::npos) {  // mkdir -p of the parent
+    std::string dir;
+    for (size_t i = 0; i <= slash; ++i) {
+      dir += path[i];
+      if (path[i] == '/' && i > 0) mkdir(dir.c_str(), 0755);
+    }
+  }
+  if (FILE* f = std::fopen(path.c_str(), "a")) {
+    std::fprintf(f, "%s %d %d %.6f\n", key.c_str(), cfg.ns, cfg.tk, ms);
+    std::fclose(f);
+  }
+}
+
+int bucket(double v) { return v <= 0 ? 0 : int(std::floor(std::log2(v) * 2)); }  // half-octaves
+
+}  // namespace
+
+extern "C" {
+
+int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batches, size_t nbatch,
+                           const double* dms, size_t stride_ao, size_t nao, size_t nset_max,
+                           size_t blksize, int precision, int flags, void* stream) {
+  cfgmm::set_last_error("");
+  if (!out) return fail(CFGMM_ERR_INVALID_ARGUMENT, "null plan pointer");
+  *out = nullptr;
+  if (precision != CFGMM_PREC_FP64)
+    return fail(CFGMM_ERR_UNIMPLEMENTED, "batched plans run in FP64");
+  if (!batches || nbatch == 0 || !dms || nao == 0 || nset_max == 0 || blksize == 0)
+    return fail(CFGMM_ERR_INVALID_ARGUMENT, "empty plan or null pointer");
+  if (nao > 1000000 || nset_max > 1024 || blksize > 1000000 || nbatch > 1000000)
+    return fail(CFGMM_ERR_INVALID_ARGUMENT, "plan dimensions out of range");
+  for (size_t i = 0; i < nbatch; ++i) {
+    const cfgmm_aodm_batch& b = batches[i];
+    if (!b.rhos || !b.ao_lhs || !b.ao_rhs || !b.tab || b.nset == 0 || b.nset > nset_max ||
+        b.stride_grid < b.ngrid || b.ngrid == 0 || b.ngrid > 0x7fff0000u ||
+        b.ldtab < (b.ngrid + blksize - 1) / blksize)
+      return fail(CFGMM_ERR_INVALID_ARGUMENT, "invalid batch " + std::to_string(i));
+  }
+  int dev = 0, ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0 || cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CFGMM_ERR_NO_DEVICE, "no CUDA device");
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cfgmm_aodm_plan* plan = new cfgmm_aodm_plan;
+  plan->dev = dev;
+  auto cleanup = [&](int rc) {
+    if (plan->mem) cudaFree(plan->mem);
+    delete plan;
+    return rc;
+  };
+  const int TU = cfgmm::aodm_row_tile(), TG = cfgmm::aodm_point_tile();
+  const int gsub = int((blksize + TG - 1) / TG);
+  const int max_ut = int((nao + TU - 1) / TU);
+
+  // ---- layout of the plan's device memory ----
+  std::vector<size_t> nblk(nbatch), list_off(nbatch), cnt_off(nbatch);
+  size_t lists_n = 0, cnt_n = 0;
+  for (size_t i = 0; i < nbatch; ++i) {
+    nblk[i] = (batches[i].ngrid + blksize - 1) / blksize;
+    list_off[i] = lists_n;
+    cnt_off[i] = cnt_n;
+    lists_n += nblk[i] * nao;
+    cnt_n += nblk[i];
+  }
+  const size_t slots = cnt_n * gsub * max_ut;
+  const size_t o_lists = 0;
+  const size_t o_counts = o_lists + a256(lists_n * sizeof(int));
+  const size_t o_batch = o_counts + a256(cnt_n * sizeof(int));
+  const size_t o_items = o_batch + a256(nbatch * sizeof(cfgmm::AodmBatch));
+  const size_t o_pairs = o_items + a256(slots * sizeof(int4));
+  const size_t o_ctr = o_pairs + a256(cnt_n * gsub * sizeof(int2));
+  const size_t o_part = o_ctr + a256((nset_max + 1) * sizeof(int));
+  const size_t bytes = o_part + slots * nset_max * TG * sizeof(double);
+  cudaError_t err = cudaMalloc(&plan->mem, bytes);
+  if (err != cudaSuccess) return cleanup(cuda_fail(err, "cudaMalloc(plan)"));
+  char* base = static_cast<char*>(plan->mem);
+  int* d_lists = reinterpret_cast<int*>(base + o_lists);
+  int* d_counts = reinterpret_cast<int*>(base + o_counts);
+
+  // ---- 1. active lists of every batch ----
+  for (size_t i = 0; i < nbatch; ++i) {
+    err = cfgmm::aodm_block_lists_launch(batches[i].tab, batches[i].ldtab, int(nao), int(nblk[i]),
+                                         d_lists + list_off[i], d_counts + cnt_off[i], s);
+    if (err != cudaSuccess) return cleanup(cuda_fail(err, "active lists"));
+  }
+  std::vector<int> counts(cnt_n);
+  err = cudaMemcpyAsync(counts.data(), d_counts, cnt_n * sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+  if (err != cudaSuccess) return cleanup(cuda_fail(err, "active list counts"));
+
+  // ---- 2. descriptors and the global work list, heaviest first ----
+  std::vector<cfgmm::AodmBatch> hb(nbatch);
+  std::vector<int4> items;
+  std::vector<int2> pairs;
+  long long slot = 0;
+  double work = 0.0;
+  for (size_t i = 0; i < nbatch; ++i) {
+    const cfgmm_aodm_batch& b = batches[i];
+    hb[i] = cfgmm::AodmBatch{b.ao_lhs, b.ao_rhs, b.rhos, d_lists + list_off[i],
+                             d_counts + cnt_off[i], b.stride_grid, int(b.ngrid), int(b.nset), slot};
+    for (size_t blk = 0; blk < nblk[i]; ++blk) {
+      const int nb = counts[cnt_off[i] + blk];
+      const int nt = (nb + TU - 1) / TU;
+      for (int gt = 0; gt < gsub; ++gt) {
+        const int bg = int(blk) * gsub + gt;
+        if (nt > 0) pairs.push_back(make_int2(int(i), bg));
+        for (int u = 0; u < nt; ++u) items.push_back(make_int4(int(i), bg, u, nb));
+      }
+      work += double(b.nset) * nb * nb;
+    }
+    slot += (long long)(nblk[i] * gsub * max_ut);
+  }
+  std::stable_sort(items.begin(), items.end(),
+                   [](const int4& x, const int4& y) { return x.w > y.w; });
+  plan->nitems = int(items.size());
+  plan->npairs = int(pairs.size());
+  plan->rpairs = reinterpret_cast<int2*>(base + o_pairs);
+  err = cudaMemcpyAsync(base + o_batch, hb.data(), nbatch * sizeof(cfgmm::AodmBatch),
+                        cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess && !items.empty())
+    err = cudaMemcpyAsync(base + o_items, items.data(), items.size() * sizeof(int4),
+                          cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess && !pairs.empty())
+    err = cudaMemcpyAsync(plan->rpairs, pairs.data(), pairs.size() * sizeof(int2),
+                          cudaMemcpyHostToDevice, s);
+  if (err != cudaSuccess) return cleanup(cuda_fail(err, "plan upload"));
+
+  cfgmm::AodmArgs& a = plan->args;
+  a.dms = dms;
+  a.stride_ao = stride_ao;
+  a.dm_stride = stride_ao * stride_ao;
+  a.nao = int(nao);
+  a.blk = int(blksize);
+  a.gsub = gsub;
+  a.max_utiles = max_ut;
+  a.nset_max = int(nset_max);
+  a.batches = reinterpret_cast<const cfgmm::AodmBatch*>(base + o_batch);
+  a.items = reinterpret_cast<const int4*>(base + o_items);
+  a.counters = reinterpret_cast<int*>(base + o_ctr);
+  a.partial = reinterpret_cast<double*>(base + o_part);
+
+  // ---- 3. autotuning ----
+  auto set_cfg = [&](const cfgmm::AodmConfig& c) -> cudaError_t {
+    a.ngroups = cfgmm::aodm_groups(c, int(nset_max));
+    std::vector<int> ctr(a.ngroups + 1, 0);
+    ctr[a.ngroups] = plan->nitems;
+    cudaError_t e = cudaMemcpyAsync(a.counters, ctr.data(), ctr.size() * sizeof(int),
+                                    cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e;
+  };
+  auto time_cfg = [&](const cfgmm::AodmConfig& c, double* ms) -> cudaError_t {
+    cudaError_t e = set_cfg(c);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {
+      e = cfgmm::aodm_launch_reset(a.counters, a.ngroups, s);
+      if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+      if (e == cudaSuccess) e = cfgmm::aodm_launch_main(a, c, s);
+      if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float t = 0.f;
+      if (e == cudaSuccess) cudaEventElapsedTime(&t, e0, e1);
+      if (rep > 0) best = std::min(best, t);  // the first run warms up
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = best;
+    return e;
+  };
+  char key[256];
+  std::snprintf(key, sizeof(key), "aodm_fp64:nao%d:work%d:items%d:nset%zu:blk%zu", bucket(double(nao)),
+                bucket(work), bucket(double(plan->nitems)), nset_max, blksize);
+  std::string tune = "default";
+  plan->cfg = cfgmm::aodm_default_config(int(nset_max));
+  if (!(flags & CFGMM_PLAN_NO_TUNE) && plan->nitems > 0) {
+    if (cache_lookup(key, &plan->cfg)) {
+      tune = "cache";
+    } else {
+      double best_ms = 1e30;
+      std::string trials;
+      for (int tk : {32, 16})
+        for (int ns = 1; ns <= 3 && ns <= int(nset_max); ++ns) {
+          const cfgmm::AodmConfig c{ns, tk};
+          double ms = 0;
+          err = time_cfg(c, &ms);
+          if (err != cudaSuccess) return cleanup(cuda_fail(err, "autotune"));
+          char buf[96];
+          std::snprintf(buf, sizeof(buf), "%s{\"ns\":%d,\"tk\":%d,\"ms\":%.4f}",
+                        trials.empty() ? "" : ",", ns, tk, ms);
+          trials += buf;
+          if (ms < best_ms) {
+            best_ms = ms;
+            plan->cfg = c;
+          }
+        }
+      cache_store(key, plan->cfg, best_ms);
+      tune = "[" + trials + "]";
+    }
+  }
+  if ((err = set_cfg(plan->cfg)) != cudaSuccess) return cleanup(cuda_fail(err, "plan config"));
+
+  // ---- 4. capture the run ----
+  if (!(flags & CFGMM_PLAN_NO_GRAPH)) {
+    cudaStream_t cs;
+    if ((err = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)) != cudaSuccess)
+      return cleanup(cuda_fail(err, "capture stream"));
+    // launch once outside the capture so kernel attributes are set
+    err = cfgmm::aodm_launch_main(a, plan->cfg, cs);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(cs);
+    cudaGraph_t graph = nullptr;
+    if (err == cudaSuccess) err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (err == cudaSuccess) {
+      cudaError_t e1 = cfgmm::aodm_launch_reset(a.counters, a.ngroups, cs);
+      if (e1 == cudaSuccess) e1 = cfgmm::aodm_launch_main(a, plan->cfg, cs);
+      if (e1 == cudaSuccess) e1 = cfgmm::aodm_launch_reduce(a, plan->rpairs, plan->npairs, cs);
+      err = cudaStreamEndCapture(cs, &graph);
+      if (err == cudaSuccess) err = e1;
+    }
+    if (err == cudaSuccess) err = cudaGraphInstantiate(&plan->exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamDestroy(cs);
+    if (err != cudaSuccess) return cleanup(cuda_fail(err, "graph capture"));
+  }
+  char buf[512];
+  std::snprintf(buf, sizeof(buf),
+                "{\"batches\":%zu,\"items\":%d,\"block_tiles\":%d,\"config\":{\"ns\":%d,\"tk\":%d},"
+                "\"graph\":%s,\"tuning\":",
+                nbatch, plan->nitems, plan->npairs, plan->cfg.ns, plan->cfg.tk,
+                plan->exec ? "true" : "false");
+  plan->info = std::string(buf) + (tune[0] == '[' ? tune : "\"" + tune + "\"") + ",\"key\":\"" +
+               key + "\"}";
+  *out = plan;
+  return CFGMM_OK;
+}
+
+int cfgmm_aodm_plan_run(cfgmm_aodm_plan* plan, void* stream) {
+  cfgmm::set_last_error("");
+  if (!plan) return fail(CFGMM_ERR_INVALID_ARGUMENT, "null plan");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (plan->exec) {
+    PLAN_CUDA(cudaGraphLaunch(plan->exec, s));
+    return CFGMM_OK;
+  }
+  PLAN_CUDA(cfgmm::aodm_launch_reset(plan->args.counters, plan->args.ngroups, s));
+  PLAN_CUDA(cfgmm::aodm_launch_main(plan->args, plan->cfg, s));
+  PLAN_CUDA(cfgmm::aodm_launch_reduce(plan->args, plan->rpairs, plan->npairs, s));
+  return CFGMM_OK;
+}
+
+const char* cfgmm_aodm_plan_info(const cfgmm_aodm_plan* plan) {
+  return plan ? plan->info.c_str() : "";
+}
+
+int cfgmm_aodm_plan_destroy(cfgmm_aodm_plan* plan) {
+  if (!plan) return CFGMM_OK;
+  if (plan->exec) cudaGraphExecDestroy(plan->exec);
+  if (plan->mem) cudaFree(plan->mem);
+  delete plan;
+  return CFGMM_OK;
+}
+
+}  // extern "C"

@@ -37,7 +37,6 @@ namespace {
 
 constexpr int TU = 64;   // compacted rows (u) per work item
 constexpr int TG = 64;   // grid points per work item
-constexpr int TK = 32;   // compacted v per pipeline stage
 constexpr int STAGES = 3;
 constexpr int THREADS = 256;
 constexpr int LIST_CAP = 8192;  // active-list entries staged in shared memory
@@ -77,11 +76,11 @@ aodm_block_lists(const uint8_t* __restrict__ tab, size_t ldtab, int nao, int nbl
 }
 
 // ---------------------------------------------------------------------------
-// 2. work list: items[i] = (b * gsub + gt, utile) for every row tile of every
+// 2. work list: items[i] = (0, b * gsub + gt, utile) for every row tile of every
 //    non-empty (block, grid tile), in block order; counters[g] = 0.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024)
-aodm_build_items(const int* __restrict__ counts, int nblk, int gsub, int2* __restrict__ items,
+aodm_build_items(const int* __restrict__ counts, int nblk, int gsub, int4* __restrict__ items,
                  int* __restrict__ counters, int ncounters) {
   __shared__ int warp_tot[32];
   __shared__ int base_s;
@@ -105,7 +104,7 @@ aodm_build_items(const int* __restrict__ counts, int nblk, int gsub, int2* __res
     int before = base_s;
     for (int w = 0; w < warp; ++w) before += warp_tot[w];
     before += incl - mine;
-    for (int j = 0; j < mine; ++j) items[before + j] = make_int2(b * gsub + j / nt, j % nt);
+    for (int j = 0; j < mine; ++j) items[before + j] = make_int4(0, b * gsub + j / nt, j % nt, 0);
     __syncthreads();
     if (tid == 0) {
       int t = 0;
@@ -120,77 +119,69 @@ aodm_build_items(const int* __restrict__ counts, int nblk, int gsub, int2* __res
 // ---------------------------------------------------------------------------
 // 3. main kernel
 // ---------------------------------------------------------------------------
-struct AodmArgs {
-  const double* dms;
-  const double* ao_lhs;
-  const double* ao_rhs;
-  const int* lists;
-  const int* counts;
-  const int2* items;  // work list (bg, utile)
-  int* counters;      // [ngroups] work counters, then the item total
-  int ngroups;
-  double* partial;  // [bg * max_utiles + utile][nset][TG]
-  size_t stride_ao, stride_grid, dm_stride;  // dm_stride = stride_ao^2
-  int nao, ngrid, nset, blk, gsub;           // gsub = grid tiles per block
-  int max_utiles;                            // row tiles per (block, grid tile) slot
-};
-
-template <int NS>
+template <int NS, int TKT>
 __global__ void __launch_bounds__(THREADS, 1) aodm_fp64_kernel(AodmArgs p) {
   extern __shared__ __align__(128) double smem[];
-  constexpr int D_TILE = TU * TK;  // one D tile per set
-  constexpr int P_TILE = TG * TK;  // ao_rhs tile, stored [g][k]
+  constexpr int D_TILE = TU * TKT;  // one D tile per set
+  constexpr int P_TILE = TG * TKT;  // ao_rhs tile, stored [g][k]
   constexpr int STAGE = NS * D_TILE + P_TILE;
+  constexpr int DC = TKT;           // D gather: threads per row (= columns of a chunk)
+  constexpr int DR = THREADS / DC;  // D gather: rows per pass
+  constexpr int PR = THREADS / TG;  // ao_rhs gather: k rows per pass
   int* list_s = reinterpret_cast<int*>(smem + STAGES * STAGE);  // LIST_CAP entries
-  __shared__ int item_s, blk_s;
+  __shared__ int item_s;
+  __shared__ long long key_s;
 
   const int set0 = blockIdx.y * NS;
-  const int ns = min(NS, p.nset - set0);
   const int total = p.counters[p.ngroups];
   int* counter = p.counters + blockIdx.y;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 2, wn = warp & 3;  // 2 x 4 warps; warp tile 32 (u) x 16 (g)
   const int g = lane >> 2, q = lane & 3;
-  const int c_d = tid & 31, r_d0 = tid >> 5;  // D gather: column c_d, rows r_d0 + 8i
-  const int j_p = tid & 63, c_p0 = tid >> 6;  // ao_rhs gather: point j_p, k rows c_p0 + 4i
+  const int c_d = tid % DC, r_d0 = tid / DC;  // D gather: column c_d, rows r_d0 + DR*i
+  const int j_p = tid % TG, c_p0 = tid / TG;  // ao_rhs gather: point j_p, k rows c_p0 + PR*i
 
-  if (tid == 0) blk_s = -1;
+  if (tid == 0) key_s = -1;
   for (;;) {
     if (tid == 0) item_s = atomicAdd(counter, 1);
     __syncthreads();  // also orders this item's smem use after the previous one's
     const int it = item_s;
     if (it >= total) break;
-    const int2 w = p.items[it];
-    const int bg = w.x, utile = w.y;
+    const int4 w = p.items[it];
+    const AodmBatch& B = p.batches ? p.batches[w.x] : p.one;
+    const int ns = min(NS, B.nset - set0);
+    if (ns <= 0) continue;  // this batch has fewer density matrices
+    const int bg = w.y, utile = w.z;
     const int b = bg / p.gsub, gt = bg % p.gsub;
-    const int nb = p.counts[b];
-    const int* Ig = p.lists + size_t(b) * p.nao;
+    const int nb = B.counts[b];
+    const int* Ig = B.lists + size_t(b) * p.nao;
     const bool staged = nb <= LIST_CAP;
-    if (staged && blk_s != b) {  // stage the active list of block b once
+    const long long key = (long long)w.x << 32 | b;  // (batch, block) whose list is staged
+    if (staged && key_s != key) {
       for (int i = tid; i < nb; i += THREADS) list_s[i] = Ig[i];
       __syncthreads();
-      if (tid == 0) blk_s = b;
+      if (tid == 0) key_s = key;
     }
     const int* I = staged ? list_s : Ig;
     const int u0 = utile * TU;
     const int g0 = b * p.blk + gt * TG;
-    const int gw = min(min((b + 1) * p.blk, p.ngrid), g0 + TG) - g0;
+    const int gw = min(min((b + 1) * p.blk, B.ngrid), g0 + TG) - g0;
     const int mu = min(TU, nb - u0);
     const bool jok = j_p < gw;
 
-    int urow[8];
+    int urow[TU / DR];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int r = r_d0 + 8 * i;
+    for (int i = 0; i < TU / DR; ++i) {
+      const int r = r_d0 + DR * i;
       urow[i] = (r < mu) ? I[u0 + r] : -1;
     }
 
-    const int kchunks = (nb + TK - 1) / TK;
+    const int kchunks = (nb + TKT - 1) / TKT;
     auto issue = [&](int kc) {
       double* st = smem + (kc % STAGES) * STAGE;
-      const int k0 = kc * TK;
-      const int kw = min(TK, nb - k0);
+      const int k0 = kc * TKT;
+      const int kw = min(TKT, nb - k0);
       const bool cok = c_d < kw;
       const int vcol = cok ? I[k0 + c_d] : 0;
 #pragma unroll
@@ -199,21 +190,21 @@ __global__ void __launch_bounds__(THREADS, 1) aodm_fp64_kernel(AodmArgs p) {
         const bool sok = s < ns;
         const double* dm = p.dms + size_t(set0 + (sok ? s : 0)) * p.dm_stride;
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const int r = r_d0 + 8 * i;
+        for (int i = 0; i < TU / DR; ++i) {
+          const int r = r_d0 + DR * i;
           const bool ok = sok && cok && urow[i] >= 0;
           const double* src = ok ? dm + size_t(urow[i]) * p.stride_ao + vcol : p.dms;
-          cp_async_8(Ds + swz<TK>(r, c_d), src, ok);
+          cp_async_8(Ds + swz<TKT>(r, c_d), src, ok);
         }
       }
       double* Ps = st + NS * D_TILE;
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int c = c_p0 + 4 * i;
+      for (int i = 0; i < TKT / PR; ++i) {
+        const int c = c_p0 + PR * i;
         const bool ok = jok && c < kw;
         const double* src =
-            ok ? p.ao_rhs + size_t(I[k0 + c]) * p.stride_grid + (g0 + j_p) : p.ao_rhs;
-        cp_async_8(Ps + swz<TK>(j_p, c), src, ok);
+            ok ? B.ao_rhs + size_t(I[k0 + c]) * B.stride_grid + (g0 + j_p) : B.ao_rhs;
+        cp_async_8(Ps + swz<TKT>(j_p, c), src, ok);
       }
     };
 
@@ -241,11 +232,11 @@ __global__ void __launch_bounds__(THREADS, 1) aodm_fp64_kernel(AodmArgs p) {
       const double* st = smem + (kc % STAGES) * STAGE;
       const double* Ps = st + NS * D_TILE;
 #pragma unroll
-      for (int kk = 0; kk < TK; kk += 8) {
+      for (int kk = 0; kk < TKT; kk += 8) {
         double2 bv[2];
 #pragma unroll
         for (int nt = 0; nt < 2; ++nt)
-          bv[nt] = *reinterpret_cast<const double2*>(Ps + swz<TK>(wn * 16 + nt * 8 + g, kk + 2 * q));
+          bv[nt] = *reinterpret_cast<const double2*>(Ps + swz<TKT>(wn * 16 + nt * 8 + g, kk + 2 * q));
         double2 av[NS][2][2];
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
@@ -253,8 +244,8 @@ __global__ void __launch_bounds__(THREADS, 1) aodm_fp64_kernel(AodmArgs p) {
 #pragma unroll
           for (int mt = 0; mt < 2; ++mt) {
             const int r = wm * 32 + mt * 16 + g;
-            av[s][mt][0] = *reinterpret_cast<const double2*>(Ds + swz<TK>(r, kk + 2 * q));
-            av[s][mt][1] = *reinterpret_cast<const double2*>(Ds + swz<TK>(r + 8, kk + 2 * q));
+            av[s][mt][0] = *reinterpret_cast<const double2*>(Ds + swz<TKT>(r, kk + 2 * q));
+            av[s][mt][1] = *reinterpret_cast<const double2*>(Ds + swz<TKT>(r + 8, kk + 2 * q));
           }
         }
         // k-slot .x of every tile of every set, then .y: dependent DMMAs on one
@@ -287,7 +278,7 @@ __global__ void __launch_bounds__(THREADS, 1) aodm_fp64_kernel(AodmArgs p) {
       for (int h = 0; h < 2; ++h) {
         const int r = wm * 32 + mt * 16 + g + 8 * h;
         const bool rok = r < mu;
-        const double* row = rok ? p.ao_lhs + size_t(I[u0 + r]) * p.stride_grid : nullptr;
+        const double* row = rok ? B.ao_lhs + size_t(I[u0 + r]) * B.stride_grid : nullptr;
 #pragma unroll
         for (int nt = 0; nt < 2; ++nt)
 #pragma unroll
@@ -314,56 +305,97 @@ __global__ void __launch_bounds__(THREADS, 1) aodm_fp64_kernel(AodmArgs p) {
           if (g == 0) red[(s * 2 + wm) * TG + wn * 16 + nt * 8 + 2 * q + e] = v;
         }
     __syncthreads();
-    const size_t slot = size_t(bg) * p.max_utiles + utile;
+    const size_t slot = B.partial_off + size_t(bg) * p.max_utiles + utile;
     for (int t = tid; t < ns * TG; t += THREADS) {
       const int s = t / TG, j = t % TG;
-      p.partial[(slot * p.nset + set0 + s) * TG + j] = red[(s * 2 + 0) * TG + j] + red[(s * 2 + 1) * TG + j];
+      p.partial[(slot * p.nset_max + set0 + s) * TG + j] =
+          red[(s * 2 + 0) * TG + j] + red[(s * 2 + 1) * TG + j];
     }
     // the __syncthreads at the top of the loop protects `red` and the stages
   }
 }
 
 // ---------------------------------------------------------------------------
-// 3. deterministic reduction of the row-tile partials into rho
+// 4. deterministic reduction of the row-tile partials into rho
+//    one CTA per (batch, block tile): rpairs[i] = (batch, bg), or bg = i
 // ---------------------------------------------------------------------------
-__global__ void aodm_reduce(double* __restrict__ rhos, const double* __restrict__ partial,
-                            const int* __restrict__ counts, size_t stride_grid, int ngrid,
-                            int nset, int blk, int gsub, int max_utiles, int nbg) {
-  const int bg = blockIdx.x;
-  if (bg >= nbg) return;
-  const int b = bg / gsub, gt = bg % gsub;
-  const int nt = (counts[b] + TU - 1) / TU;
+__global__ void aodm_reduce(AodmArgs p, const int2* __restrict__ rpairs, int npairs) {
+  const int i = blockIdx.x;
+  if (i >= npairs) return;
+  const int2 pr = rpairs ? rpairs[i] : make_int2(0, i);
+  const AodmBatch& B = p.batches ? p.batches[pr.x] : p.one;
+  const int bg = pr.y;
+  const int b = bg / p.gsub, gt = bg % p.gsub;
+  const int nt = (B.counts[b] + TU - 1) / TU;
   if (nt == 0) return;  // fully masked block: rho untouched, as in the reference
-  const int g0 = b * blk + gt * TG;
-  const int gend = min(min((b + 1) * blk, ngrid), g0 + TG);
-  for (int t = threadIdx.x; t < nset * TG; t += blockDim.x) {
+  const int g0 = b * p.blk + gt * TG;
+  const int gend = min(min((b + 1) * p.blk, B.ngrid), g0 + TG);
+  for (int t = threadIdx.x; t < B.nset * TG; t += blockDim.x) {
     const int s = t / TG, j = t % TG;
     if (g0 + j >= gend) continue;
     double v = 0.0;
-    for (int u = 0; u < nt; ++u) v += partial[((size_t(bg) * max_utiles + u) * nset + s) * TG + j];
-    double* r = rhos + size_t(s) * stride_grid + g0 + j;
+    for (int u = 0; u < nt; ++u)
+      v += p.partial[((B.partial_off + size_t(bg) * p.max_utiles + u) * p.nset_max + s) * TG + j];
+    double* r = B.rhos + size_t(s) * B.stride_grid + g0 + j;
     *r = v + *r;
   }
 }
 
-template <int NS>
-cudaError_t launch_main(const AodmArgs& a, int ngroups, cudaStream_t stream) {
-  constexpr size_t smem = size_t(STAGES) * (NS * TU * TK + TG * TK) * sizeof(double) +
+__global__ void aodm_reset_counters(int* counters, int ngroups) {
+  if (threadIdx.x < ngroups) counters[threadIdx.x] = 0;
+}
+
+template <int NS, int TKT>
+cudaError_t launch_main_t(const AodmArgs& a, cudaStream_t stream) {
+  constexpr size_t smem = size_t(STAGES) * (NS * TU * TKT + TG * TKT) * sizeof(double) +
                           size_t(LIST_CAP) * sizeof(int);
-  static_assert(NS * 2 * TG <= STAGES * (NS * TU * TK + TG * TK), "reduction buffer fits");
+  static_assert(NS * 2 * TG <= STAGES * (NS * TU * TKT + TG * TKT), "reduction buffer fits");
   static_assert(smem <= 227 * 1024, "shared memory budget");
-  cudaError_t err = cudaFuncSetAttribute(aodm_fp64_kernel<NS>,
+  cudaError_t err = cudaFuncSetAttribute(aodm_fp64_kernel<NS, TKT>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (err != cudaSuccess) return err;
   int dev = 0, nsm = 0;
   if ((err = cudaGetDevice(&dev)) != cudaSuccess) return err;
   if ((err = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
     return err;
-  aodm_fp64_kernel<NS><<<dim3(nsm, ngroups), THREADS, smem, stream>>>(a);
+  aodm_fp64_kernel<NS, TKT><<<dim3(nsm, a.ngroups), THREADS, smem, stream>>>(a);
   return cudaGetLastError();
 }
 
 }  // namespace
+
+int aodm_groups(const AodmConfig& cfg, int nset_max) {
+  return (nset_max + cfg.ns - 1) / cfg.ns;
+}
+
+AodmConfig aodm_default_config(int nset) {
+  return AodmConfig{nset >= 3 ? 3 : nset, 32};
+}
+
+cudaError_t aodm_launch_main(const AodmArgs& a, const AodmConfig& cfg, cudaStream_t stream) {
+  if (cfg.tk == 32) {
+    if (cfg.ns == 1) return launch_main_t<1, 32>(a, stream);
+    if (cfg.ns == 2) return launch_main_t<2, 32>(a, stream);
+    if (cfg.ns == 3) return launch_main_t<3, 32>(a, stream);
+  } else if (cfg.tk == 16) {
+    if (cfg.ns == 1) return launch_main_t<1, 16>(a, stream);
+    if (cfg.ns == 2) return launch_main_t<2, 16>(a, stream);
+    if (cfg.ns == 3) return launch_main_t<3, 16>(a, stream);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t aodm_launch_reduce(const AodmArgs& a, const int2* rpairs, int npairs,
+                               cudaStream_t stream) {
+  if (npairs <= 0) return cudaSuccess;
+  aodm_reduce<<<npairs, 128, 0, stream>>>(a, rpairs, npairs);
+  return cudaGetLastError();
+}
+
+cudaError_t aodm_launch_reset(int* counters, int ngroups, cudaStream_t stream) {
+  aodm_reset_counters<<<1, 32, 0, stream>>>(counters, ngroups);
+  return cudaGetLastError();
+}
 
 namespace {
 struct Layout {
@@ -374,13 +406,13 @@ Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk) {
   const size_t nblk = (ngrid + blk - 1) / blk;
   const size_t gsub = (blk + TG - 1) / TG;
   const size_t max_utiles = (nao + TU - 1) / TU;
-  const size_t ngroups = (nset + 2) / 3;
+  const size_t ngroups = nset;  // upper bound for any set grouping
   auto a256 = [](size_t v) { return (v + 255) / 256 * 256; };
   Layout L;
   L.lists = 0;
   L.counts = L.lists + a256(nblk * nao * sizeof(int));
   L.items = L.counts + a256(nblk * sizeof(int));
-  L.counters = L.items + a256(nblk * gsub * max_utiles * sizeof(int2));
+  L.counters = L.items + a256(nblk * gsub * max_utiles * sizeof(int4));
   L.partial = L.counters + a256((ngroups + 1) * sizeof(int));
   L.total = L.partial + nblk * gsub * max_utiles * nset * TG * sizeof(double);
   return L;
@@ -392,6 +424,9 @@ cudaError_t aodm_block_lists_launch(const uint8_t* tab, size_t ldtab, int nao, i
   aodm_block_lists<<<nblk, 256, 0, stream>>>(tab, ldtab, nao, nblk, lists, counts);
   return cudaGetLastError();
 }
+
+int aodm_row_tile() { return TU; }
+int aodm_point_tile() { return TG; }
 
 size_t aodmao2rho_fp64_workspace(size_t nao, size_t ngrid, size_t nset, size_t blk) {
   return layout(nao, ngrid, nset, blk).total;
@@ -405,12 +440,13 @@ cudaError_t aodmao2rho_fp64(double* rhos, const double* dms, const double* ao_lh
   const int nblk = (ngrid + blk - 1) / blk;
   const int gsub = (blk + TG - 1) / TG;
   const int max_utiles = (nao + TU - 1) / TU;
-  const int ngroups = (nset + 2) / 3;
+  const AodmConfig cfg = aodm_default_config(nset);
+  const int ngroups = aodm_groups(cfg, nset);
   const Layout L = layout(nao, ngrid, nset, blk);
   char* ws = static_cast<char*>(workspace);
   int* lists = reinterpret_cast<int*>(ws + L.lists);
   int* counts = reinterpret_cast<int*>(ws + L.counts);
-  int2* items = reinterpret_cast<int2*>(ws + L.items);
+  int4* items = reinterpret_cast<int4*>(ws + L.items);
   int* counters = reinterpret_cast<int*>(ws + L.counters);
   double* partial = reinterpret_cast<double*>(ws + L.partial);
 
@@ -420,35 +456,23 @@ cudaError_t aodmao2rho_fp64(double* rhos, const double* dms, const double* ao_lh
   aodm_build_items<<<1, 1024, 0, stream>>>(counts, nblk, gsub, items, counters, ngroups);
   if ((err = cudaGetLastError()) != cudaSuccess) return err;
 
-  AodmArgs a;
+  AodmArgs a{};
   a.dms = dms;
-  a.ao_lhs = ao_lhs;
-  a.ao_rhs = ao_rhs;
-  a.lists = lists;
-  a.counts = counts;
+  a.stride_ao = stride_ao;
+  a.dm_stride = stride_ao * stride_ao;
+  a.nao = nao;
+  a.blk = blk;
+  a.gsub = gsub;
+  a.max_utiles = max_utiles;
+  a.nset_max = nset;
+  a.batches = nullptr;
+  a.one = AodmBatch{ao_lhs, ao_rhs, rhos, lists, counts, stride_grid, ngrid, nset, 0};
   a.items = items;
   a.counters = counters;
   a.ngroups = ngroups;
   a.partial = partial;
-  a.stride_ao = stride_ao;
-  a.stride_grid = stride_grid;
-  a.dm_stride = stride_ao * stride_ao;
-  a.nao = nao;
-  a.ngrid = ngrid;
-  a.nset = nset;
-  a.blk = blk;
-  a.gsub = gsub;
-  a.max_utiles = max_utiles;
-  // Sets are processed in groups sharing one ao_rhs tile: 3 at a time (the
-  // register budget of the FP64 accumulators), the remainder in one group.
-  if (nset == 1) err = launch_main<1>(a, 1, stream);
-  else if (nset == 2) err = launch_main<2>(a, 1, stream);
-  else err = launch_main<3>(a, ngroups, stream);
-  if (err != cudaSuccess) return err;
-  const int nbg = nblk * gsub;
-  aodm_reduce<<<nbg, 128, 0, stream>>>(rhos, partial, counts, stride_grid, ngrid, nset, blk, gsub,
-                                       max_utiles, nbg);
-  return cudaGetLastError();
+  if ((err = aodm_launch_main(a, cfg, stream)) != cudaSuccess) return err;
+  return aodm_launch_reduce(a, nullptr, nblk * gsub, stream);
 }
 
 }  // namespace cfgmm

@@ -1,12 +1,55 @@
-// aodmao2rho_fp64.cuh -- internal launcher of the FP64 masked AO-DM-AO contraction.
+// aodmao2rho_fp64.cuh -- internal interface of the FP64 masked AO-DM-AO contraction.
 #pragma once
+#include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
 
 namespace cfgmm {
 
-// Device scratch (bytes) the contraction needs for the given problem: the
-// per-block active AO lists, their counts and the per-row-tile partial sums.
+// One grid batch: its phi tables, rho, active lists and point count.
+struct AodmBatch {
+  const double* ao_lhs;
+  const double* ao_rhs;
+  double* rhos;            // (nset, stride_grid)
+  const int* lists;        // [nblk][nao] active AOs per block
+  const int* counts;       // [nblk]
+  size_t stride_grid;
+  int ngrid;
+  int nset;                // density matrices used by this batch (<= nset_max)
+  long long partial_off;   // first partial-sum slot of this batch
+};
+
+// Kernel arguments: density matrices shared by all batches, and either a
+// device array of batch descriptors or one descriptor by value.
+struct AodmArgs {
+  const double* dms;
+  size_t stride_ao, dm_stride;  // dm_stride = stride_ao^2
+  int nao, blk, gsub;           // gsub = 64-point tiles per grid block
+  int max_utiles;               // partial slots per (batch, block tile)
+  int nset_max;
+  const AodmBatch* batches;     // null: use `one`
+  AodmBatch one;
+  const int4* items;            // work list: (batch, block tile, row tile, 0)
+  int* counters;                // [ngroups] work counters, then the item total
+  int ngroups;
+  double* partial;              // [slot][nset_max][64]
+};
+
+// Tile configuration of the main kernel (the autotuner's search space):
+// `ns` density matrices share one ao_rhs tile (1..3), `tk` compacted AOs per
+// pipeline stage (16 or 32).
+struct AodmConfig {
+  int ns;
+  int tk;
+};
+
+AodmConfig aodm_default_config(int nset);
+int aodm_groups(const AodmConfig& cfg, int nset_max);
+int aodm_row_tile();    // compacted rows per work item (64)
+int aodm_point_tile();  // grid points per work item (64)
+
+// Device scratch (bytes) the single-call contraction needs: the per-block
+// active AO lists, their counts, the work list and the partial sums.
 size_t aodmao2rho_fp64_workspace(size_t nao, size_t ngrid, size_t nset, size_t blk);
 
 // rhos[s*stride_grid+g] += ... (see cfgmm.h) on `stream`; device pointers,
@@ -20,5 +63,12 @@ cudaError_t aodmao2rho_fp64(double* rhos, const double* dms, const double* ao_lh
 // with tab[u*ldtab + b] != 0, counts[b] = their number.
 cudaError_t aodm_block_lists_launch(const uint8_t* tab, size_t ldtab, int nao, int nblk,
                                     int* lists, int* counts, cudaStream_t stream);
+
+// Pieces of a batched run: counter reset, the persistent kernel, and the
+// reduction over (batch, block tile) pairs (rpairs null: batch 0, bg = index).
+cudaError_t aodm_launch_reset(int* counters, int ngroups, cudaStream_t stream);
+cudaError_t aodm_launch_main(const AodmArgs& a, const AodmConfig& cfg, cudaStream_t stream);
+cudaError_t aodm_launch_reduce(const AodmArgs& a, const int2* rpairs, int npairs,
+                               cudaStream_t stream);
 
 }  // namespace cfgmm

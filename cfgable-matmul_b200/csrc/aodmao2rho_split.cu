@@ -4,14 +4,16 @@
 //
 //   Every row u of D_s is scaled by 2^tau_u and every grid point g of phi by
 //   2^sigma_g so that the scaled values are below 2^6 in magnitude; each is
-//   then written as seven signed digits  x' = sum_{j<7} x_j 2^(-7j)  with
-//   x_0 in [-64, 64] and x_j in [-64, 64] (round to nearest at every step), 48
-//   bits in all.  The products of the digits of D and phi whose levels add up
-//   to L = i + j <= 6 are summed EXACTLY in one INT32 accumulator per level:
-//     S_L[u][g] = sum_{i+j=L} sum_v d_i(u,v) p_j(v,g)        (28 INT8 MMAs)
+//   then written as eight signed digits  x' = sum_{j<8} x_j 2^(-7j)  with
+//   every x_j in [-64, 64] (round to nearest at every step).  The products of
+//   the digits of D and phi whose levels add up to L = i + j <= 7 are summed
+//   EXACTLY in one INT32 accumulator per level:
+//     S_L[u][g] = sum_{i+j=L} sum_v d_i(u,v) p_j(v,g)        (36 INT8 MMAs)
 //   and X[u][g] = 2^-(tau_u + sigma_g) sum_L 2^(-7L) S_L[u][g] in FP64.  The
-//   dropped levels L >= 7 weigh at most 2^-49 of the scaled products, so X
-//   carries about 46 bits relative to sum_v |D_uv| |phi_vg|.
+//   dropped levels L >= 8 weigh at most 7 * 2^-56 of the largest scaled
+//   product and the digit remainders 2^-56 each, so X carries about 52 bits
+//   relative to sum_v |D_uv| |phi_vg|.  |S_L| <= 8 * 4096 * nao keeps the INT32
+//   sums exact for nao <= 65535.
 //
 // The contraction itself follows aodmao2rho_loop_parallel
 // (src/impl_aodmao2rho.rs:171-244): per grid block b the active list I(b) of
@@ -20,25 +22,28 @@
 // and rho[s][g] += sum_{u in I} phi[u][g] X[u][g].
 //
 // Kernels:
-//   split_d_slices    one CTA per row of D_s: row scale, 7 digits per element
+//   split_d_slices    one CTA per row of D_s: row scale, 8 digits per element
 //                     stored as 8 bytes, so the gather of one element is one
 //                     8-byte load -- the same traffic as the FP64 kernel.
-//   split_phi_sigma / split_phi_slices   per (block, 64-point tile): point
-//                     scales and the digit tiles of phi[I(b), tile], written
-//                     chunk by chunk (32 compacted AOs) directly in the UMMA
-//                     32-byte-swizzled K-major layout, so one bulk copy moves
-//                     the 7 digit tiles of a chunk into shared memory.
+//   split_phi         per (block, 64-point tile): point scales, then the digit
+//                     tiles of phi[I(b), tile] chunk by chunk (32 compacted
+//                     AOs), staged in shared memory and written out in the
+//                     UMMA 32-byte-swizzled K-major layout, so one bulk copy
+//                     moves the 8 digit tiles of a chunk into shared memory.
 //   split_build       work list (block tile, 128-row tile of I(b), DM) and
 //                     chunk offsets.
-//   split_main        persistent, 6 warps: warps 0-3 gather the D digits of
-//                     128 rows x 32 compacted columns (thread = row), transpose
-//                     the bytes into 7 swizzled A tiles and later run the
-//                     epilogue; warp 5 bulk-loads the phi digit tiles; warp 4
-//                     issues the 28 MMAs of a chunk (M=128, N=64, K=32) into 7
-//                     TMEM level accumulators (448 of 512 columns).  The
-//                     epilogue rebuilds X in FP64, weights it with phi and
-//                     reduces over the 128 rows; X never leaves the SM.
-//   split_reduce      adds the row-tile partial sums in a fixed order.
+//   split_main        persistent, 10 warps: warps 0-7 gather the D digits of
+//                     128 rows x 32 compacted columns in two groups of four
+//                     that take alternate chunks (a lane loads 8 bytes; lanes
+//                     along a row read consecutive columns; two shuffle rounds
+//                     turn the 8-byte elements into digit planes, stored
+//                     without bank conflicts) and later run the epilogue;
+//                     warp 8 issues the 36 MMAs of a chunk (M=128, N=64, K=32)
+//                     into 8 TMEM level accumulators (all 512 columns); warp 9
+//                     bulk-loads the phi digit tiles.  The epilogue rebuilds X
+//                     in FP64, weights it with phi and reduces over the rows
+//                     of each warp; X never leaves the SM.
+//   split_reduce      adds the (row tile, warp) partial sums in a fixed order.
 // Every mbarrier wait is bounded (tcgen05.cuh).
 #include <cuda_runtime.h>
 
@@ -55,14 +60,16 @@ namespace {
 constexpr int TU = 128;   // compacted rows per item (TMEM lanes)
 constexpr int TG = 64;    // grid points per item
 constexpr int TK = 32;    // compacted columns per chunk (one INT8 MMA K step)
-constexpr int NSL = 7;    // digits per value
+constexpr int NSL = 8;    // digits per value
 constexpr int STAGES = 4;
 constexpr uint32_t A_SLICE = TU * TK;        // 4096 B
 constexpr uint32_t B_SLICE = TG * TK;        // 2048 B
-constexpr uint32_t A_STAGE = NSL * A_SLICE;  // 28672 B
-constexpr uint32_t B_STAGE = NSL * B_SLICE;  // 14336 B
+constexpr uint32_t A_STAGE = NSL * A_SLICE;  // 32768 B
+constexpr uint32_t B_STAGE = NSL * B_SLICE;  // 16384 B
 constexpr uint32_t STAGE = A_STAGE + B_STAGE;
-constexpr int THREADS = 192;
+constexpr int GATHER_WARPS = 8;               // two groups of four
+constexpr int THREADS = 32 * (GATHER_WARPS + 2);
+constexpr int EPI_PARTS = 4;                  // partial sums per item (one per row quarter)
 constexpr int kBadExp = INT_MAX;  // scale of a row / point holding Inf or NaN
 
 __device__ int g_split_error;
@@ -75,7 +82,7 @@ __device__ __forceinline__ int exp_for(double amax) {  // 2^6 > amax * 2^exp
   return 6 - E;
 }
 
-// x (|x| < 2^6 after scaling) -> 7 signed digits, x = sum_j d_j 2^(-7j) + O(2^-49).
+// x (|x| < 2^6 after scaling) -> 8 signed digits, x = sum_j d_j 2^(-7j) + O(2^-50).
 __device__ __forceinline__ void digits(double x, int (&d)[NSL]) {
   double r = x;
 #pragma unroll
@@ -92,7 +99,7 @@ __device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
 }
 
 // ---------------------------------------------------------------------------
-// D digits: dsl[s][u][v] = 8 bytes (digits 0..6, 0), tau[s][u]
+// D digits: dsl[s][u][v] = 8 bytes (digits 0..7), tau[s][u]
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
 split_d_slices(const double* __restrict__ dms, size_t stride_ao, size_t dm_stride, int nao,
@@ -133,75 +140,86 @@ split_d_slices(const double* __restrict__ dms, size_t stride_ao, size_t dm_strid
   const int e = e_s;
   uint2* out = dsl + size_t(row) * nao;
   for (int v = threadIdx.x; v < nao; v += 256) {
-    int dg[NSL] = {0, 0, 0, 0, 0, 0, 0};
+    int dg[NSL] = {0, 0, 0, 0, 0, 0, 0, 0};
     if (e != kBadExp) digits(ldexp(d[v], e), dg);
-    out[v] = make_uint2(pack4(dg[0], dg[1], dg[2], dg[3]), pack4(dg[4], dg[5], dg[6], 0));
+    out[v] = make_uint2(pack4(dg[0], dg[1], dg[2], dg[3]), pack4(dg[4], dg[5], dg[6], dg[7]));
   }
 }
 
 // ---------------------------------------------------------------------------
-// phi scales: sigma[g] for the 64 points of each (block, tile)
+// phi: point scales sigma[g], then for chunk c of (block tile bg) and digit j
+// a 64 x 32-byte K-major tile (row = point, byte = compacted AO within the
+// chunk) in the 32-byte-swizzled layout, at phisl + ((cbase[bg] + c) * 8 + j) * 2048.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(64)
-split_phi_sigma(const double* __restrict__ ao, size_t stride_grid, const int* __restrict__ lists,
-                const int* __restrict__ counts, int nao, int ngrid, int blk, int gsub,
-                int* __restrict__ sigma) {
-  const int bg = blockIdx.x;
-  const int b = bg / gsub, gt = bg % gsub;
-  const int g0 = b * blk + gt * TG;
-  const int gend = min(min((b + 1) * blk, ngrid), g0 + TG);
-  const int g = g0 + threadIdx.x;
-  if (g >= gend) return;
-  const int nb = counts[b];
-  const int* I = lists + size_t(b) * nao;
-  double mx = 0.0;
-  bool bad = false;
-  for (int i = 0; i < nb; ++i) {
-    const double a = fabs(ao[size_t(I[i]) * stride_grid + g]);
-    bad |= !(a <= 1.7976931348623157e308);
-    mx = fmax(mx, a);
-  }
-  sigma[g] = bad ? kBadExp : exp_for(mx);
-}
-
-// phi digit tiles: for chunk c of (block tile bg), digit j: a 64 x 32-byte
-// K-major tile (row = point, byte = compacted AO within the chunk) in the
-// 32-byte-swizzled layout, at phisl + ((cbase[bg] + c) * 7 + j) * 2048.
 __global__ void __launch_bounds__(256)
-split_phi_slices(const double* __restrict__ ao, size_t stride_grid,
-                 const int* __restrict__ lists, const int* __restrict__ counts,
-                 const int* __restrict__ cbase, const int* __restrict__ sigma, int nao, int ngrid,
-                 int blk, int gsub, uint8_t* __restrict__ phisl) {
+split_phi(const double* __restrict__ ao, size_t stride_grid, const int* __restrict__ lists,
+          const int* __restrict__ counts, const int* __restrict__ cbase, int nao, int ngrid,
+          int blk, int gsub, int* __restrict__ sigma, uint8_t* __restrict__ phisl) {
+  __shared__ double red[4][TG];
+  __shared__ int e_s[TG];
+  // staged digit words [digit][quad of 4 AOs][point], rows padded to 68 words
+  // so that the read-out below is free of bank conflicts
+  __shared__ uint32_t stage[NSL][8][TG + 4];
   const int bg = blockIdx.x;
   const int b = bg / gsub, gt = bg % gsub;
   const int g0 = b * blk + gt * TG;
   const int gend = min(min((b + 1) * blk, ngrid), g0 + TG);
   const int nb = counts[b];
-  const int kc = (nb + TK - 1) / TK;
   const int* I = lists + size_t(b) * nao;
-  uint8_t* base = phisl + size_t(cbase[bg]) * NSL * B_SLICE;
-  // units: (chunk c, point row g, quad q of 4 compacted AOs): kc * 64 * 8
-  for (int unit = threadIdx.x; unit < kc * TG * 8; unit += 256) {
-    const int c = unit / (TG * 8);
-    const int rem = unit % (TG * 8);
-    const int gr = rem >> 3, q = rem & 7;
-    const int g = g0 + gr;
-    const int e = (g < gend) ? sigma[g] : 0;
-    int dg[4][NSL];
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const int i = c * TK + q * 4 + t;
-#pragma unroll
-      for (int j = 0; j < NSL; ++j) dg[t][j] = 0;
-      if (g < gend && i < nb && e != kBadExp)
-        digits(ldexp(ao[size_t(I[i]) * stride_grid + g], e), dg[t]);
+  const int gr = threadIdx.x & (TG - 1), rg = threadIdx.x >> 6;
+  const int g = g0 + gr;
+  const bool gok = g < gend;
+  // 1. max |phi| over the active AOs of each point (a warp reads 32 points of a row)
+  double mx = 0.0;
+  if (gok) {
+    bool bad = false;
+#pragma unroll 4
+    for (int i = rg; i < nb; i += 4) {
+      const double a = fabs(ao[size_t(__ldg(I + i)) * stride_grid + g]);
+      bad |= !(a <= 1.7976931348623157e308);
+      mx = fmax(mx, a);
     }
-    uint8_t* tile0 = base + size_t(c) * NSL * B_SLICE;
-    const uint32_t off = tc::sw32_offset(uint32_t(gr), uint32_t(q >> 2)) + uint32_t(q & 3) * 4;
+    if (bad) mx = __longlong_as_double(0x7ff0000000000000LL);  // +Inf marks the point
+  }
+  red[rg][gr] = mx;
+  __syncthreads();
+  if (threadIdx.x < TG) {
+    const int e = exp_for(fmax(fmax(red[0][gr], red[1][gr]), fmax(red[2][gr], red[3][gr])));
+    e_s[gr] = e;
+    if (gok) sigma[g] = e;
+  }
+  __syncthreads();
+  const int e = e_s[gr];
+  // 2. digit tiles, one chunk of 32 compacted AOs at a time
+  const int kc = (nb + TK - 1) / TK;
+  uint8_t* base = phisl + size_t(cbase[bg]) * B_STAGE;
+  for (int c = 0; c < kc; ++c) {
 #pragma unroll
-    for (int j = 0; j < NSL; ++j)
-      *reinterpret_cast<uint32_t*>(tile0 + j * B_SLICE + off) =
-          pack4(dg[0][j], dg[1][j], dg[2][j], dg[3][j]);
+    for (int hq = 0; hq < 2; ++hq) {
+      const int q = rg + 4 * hq;  // quad of 4 compacted AOs
+      int dg[4][NSL];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int i = c * TK + q * 4 + t;
+#pragma unroll
+        for (int j = 0; j < NSL; ++j) dg[t][j] = 0;
+        if (gok && i < nb && e != kBadExp)
+          digits(ldexp(ao[size_t(__ldg(I + i)) * stride_grid + g], e), dg[t]);
+      }
+#pragma unroll
+      for (int j = 0; j < NSL; ++j) stage[j][q][gr] = pack4(dg[0][j], dg[1][j], dg[2][j], dg[3][j]);
+    }
+    __syncthreads();
+    // write-out: (digit, point row, 16-byte half) vectors, consecutive threads
+    // covering consecutive rows -> coalesced 16-byte stores
+    uint8_t* tile0 = base + size_t(c) * B_STAGE;
+    for (int v = threadIdx.x; v < NSL * TG * 2; v += 256) {
+      const int h = v & 1, r = (v >> 1) & (TG - 1), j = v >> 7;
+      const uint4 w = make_uint4(stage[j][4 * h][r], stage[j][4 * h + 1][r], stage[j][4 * h + 2][r],
+                                 stage[j][4 * h + 3][r]);
+      *reinterpret_cast<uint4*>(tile0 + j * B_SLICE + tc::sw32_offset(uint32_t(r), uint32_t(h))) = w;
+    }
+    __syncthreads();
   }
 }
 
@@ -277,23 +295,23 @@ struct MainArgs {
   const int* cbase;
   const int4* items;
   const int* total;  // [0] items x sets, [1] items per set
-  double* partial;   // [(bg * max_ut + ut) * nset + s][TG]
+  double* partial;   // [((bg * max_ut + ut) * nset + s) * EPI_PARTS + quarter][TG]
   size_t stride_grid;
   int nao, ngrid, nset, blk, gsub, max_ut;
 };
 
-// 4x4 byte transpose: out_i holds byte i of w0..w3 (w_t in byte t).
-__device__ __forceinline__ void transpose4(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3,
-                                           uint32_t& o0, uint32_t& o1, uint32_t& o2,
-                                           uint32_t& o3) {
-  const uint32_t a = __byte_perm(w0, w1, 0x5140);  // w0.b0 w1.b0 w0.b1 w1.b1
-  const uint32_t b = __byte_perm(w0, w1, 0x7362);  // w0.b2 w1.b2 w0.b3 w1.b3
-  const uint32_t c = __byte_perm(w2, w3, 0x5140);
-  const uint32_t d = __byte_perm(w2, w3, 0x7362);
-  o0 = __byte_perm(a, c, 0x5410);
-  o1 = __byte_perm(a, c, 0x7632);
-  o2 = __byte_perm(b, d, 0x5410);
-  o3 = __byte_perm(b, d, 0x7632);
+// Byte selector that assembles, from `keep` (bytes 0..3) and `recv` (4..7) of
+// the gather's second shuffle round, the digit word of 4 consecutive columns:
+// column qd comes from keep.b0, qd^2 from keep.b2, qd^1 from recv.b0 and qd^3
+// from recv.b2 (the second digit plane of the lane: +1 on every nibble).
+__device__ __forceinline__ uint32_t gather_selector(int qd) {
+  uint32_t sel = 0;
+#pragma unroll
+  for (int col = 0; col < 4; ++col) {
+    const uint32_t src = col == qd ? 0u : col == (qd ^ 2) ? 2u : col == (qd ^ 1) ? 4u : 6u;
+    sel |= src << (4 * col);
+  }
+  return sel;
 }
 
 __global__ void __launch_bounds__(THREADS, 1) split_main(MainArgs p) {
@@ -308,22 +326,21 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(MainArgs p) {
   uint64_t* acc_empty = acc_full + 1;
   uint64_t* drain = acc_full + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_full + 3);
-  __shared__ double red[4][TG];
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int* err = &g_split_error;
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
-      tc::mbar_init(&full_a[s], 128);
+      tc::mbar_init(&full_a[s], 128);  // the four warps of one gather group
       tc::mbar_init(&full_b[s], 1);
       tc::mbar_init(&empty[s], 1);
     }
     tc::mbar_init(acc_full, 1);
-    tc::mbar_init(acc_empty, 128);
+    tc::mbar_init(acc_empty, 32 * GATHER_WARPS);
     tc::mbar_init(drain, 1);
     tc::mbar_fence_init();
   }
-  if (warp == 4) {
+  if (warp == GATHER_WARPS) {
     tc::tmem_alloc(tmem_slot, 512);
     tc::tmem_relinquish();
   }
@@ -333,11 +350,18 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(MainArgs p) {
   const uint32_t tmem = *tmem_slot;
   const int total = p.total[0], per_set = p.total[1];
 
-  if (warp < 4) {
+  if (warp < GATHER_WARPS) {
     // ---------------- gather D digits, then the epilogue ----------------
-    const int tid = threadIdx.x;  // tile row
-    uint32_t uses[STAGES] = {0, 0, 0, 0};
-    int stage = 0;
+    // Group grp takes the chunks c = grp, grp+2, ... of every item; warp wq
+    // of the group fills tile rows 32wq .. 32wq+31, four rows per step.
+    // Lane (qd, ri, hh) = lane bits (4:3, 2:1, 0) loads, for row 4*step+ri,
+    // the columns 16hh + 4k + qd (k = 0..3) and ends up holding digit planes
+    // 2qd and 2qd+1 of the 16-byte half hh of that row.
+    const int grp = warp >> 2, wq = warp & 3;
+    const int qd = lane >> 3, ri = (lane >> 1) & 3, hh = lane & 1;
+    const bool b1 = (qd & 2) != 0, b0 = (qd & 1) != 0;
+    const uint32_t sel_a = gather_selector(qd), sel_b = sel_a + 0x1111u;
+    uint32_t seq0 = 0;  // CTA-wide sequence number of the item's first chunk
     uint32_t nitem = 0;
     bool ok = true;
     for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++nitem) {
@@ -348,100 +372,133 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(MainArgs p) {
       const int nb = p.counts[b];
       const int kc = (nb + TK - 1) / TK;
       const int* I = p.lists + size_t(b) * p.nao;
-      const int row = ut * TU + tid;
-      const bool rvalid = row < nb;
-      const int iu = rvalid ? I[row] : 0;
-      const uint2* drow = p.dsl + (size_t(s) * p.nao + iu) * p.nao;
-      for (int c = 0; c < kc; ++c) {
-        if (uses[stage] > 0 && !tc::mbar_wait(&empty[stage], (uses[stage] - 1) & 1, err, 11)) {
+      const uint2* dset = p.dsl + size_t(s) * p.nao * p.nao;
+      int iu[8];
+#pragma unroll
+      for (int st = 0; st < 8; ++st) {
+        const int row = ut * TU + 32 * wq + 4 * st + ri;
+        iu[st] = row < nb ? __ldg(I + row) : -1;
+      }
+      for (int c = grp; c < kc; c += 2) {
+        const uint32_t seq = seq0 + uint32_t(c);
+        const int stg = int(seq % STAGES);
+        const uint32_t use = seq / STAGES;
+        if (use > 0 && !tc::mbar_wait(&empty[stg], (use - 1) & 1, err, 11)) {
           ok = false;
           break;
         }
-        uint2 w[TK];
+        int iv[4];
 #pragma unroll
-        for (int j = 0; j < TK; ++j) {
-          const int k = c * TK + j;
-          const int iv = (k < nb) ? __ldg(I + k) : -1;
-          w[j] = (rvalid && iv >= 0) ? __ldg(drow + iv) : make_uint2(0u, 0u);
+        for (int k = 0; k < 4; ++k) {
+          const int kk = c * TK + 16 * hh + 4 * k + qd;
+          iv[k] = kk < nb ? __ldg(I + kk) : -1;
         }
-        uint8_t* As = smem + stage * STAGE;
+        uint2 w[8][4];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {  // 16-byte halves of the row (16 columns each)
-          uint32_t o[NSL][4];
+        for (int st = 0; st < 8; ++st)
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {  // 4 columns per 32-bit word
-            const int j0 = h * 16 + q * 4;
-            uint32_t x0, x1, x2, x3, y0, y1, y2, y3;
-            transpose4(w[j0].x, w[j0 + 1].x, w[j0 + 2].x, w[j0 + 3].x, x0, x1, x2, x3);
-            transpose4(w[j0].y, w[j0 + 1].y, w[j0 + 2].y, w[j0 + 3].y, y0, y1, y2, y3);
-            o[0][q] = x0;
-            o[1][q] = x1;
-            o[2][q] = x2;
-            o[3][q] = x3;
-            o[4][q] = y0;
-            o[5][q] = y1;
-            o[6][q] = y2;
+          for (int k = 0; k < 4; ++k)
+            w[st][k] = (iu[st] >= 0 && iv[k] >= 0)
+                           ? __ldg(dset + size_t(iu[st]) * p.nao + iv[k])
+                           : make_uint2(0u, 0u);
+        uint8_t* As = smem + stg * STAGE;
+#pragma unroll
+        for (int st = 0; st < 8; ++st) {
+          uint32_t wa[4], wb[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            // round 1 (lanes qd, qd^2): keep digits 0-3 (b1 = 0) or 4-7 (b1 = 1)
+            const uint32_t x = b1 ? w[st][k].y : w[st][k].x;
+            const uint32_t y = __shfl_xor_sync(0xffffffffu, b1 ? w[st][k].x : w[st][k].y, 16);
+            // round 2 (lanes qd, qd^1): keep two of those four digits
+            const uint32_t lo = __byte_perm(x, y, 0x5410), hi = __byte_perm(x, y, 0x7632);
+            const uint32_t keep = b0 ? hi : lo;
+            const uint32_t recv = __shfl_xor_sync(0xffffffffu, b0 ? lo : hi, 8);
+            wa[k] = __byte_perm(keep, recv, sel_a);
+            wb[k] = __byte_perm(keep, recv, sel_b);
           }
-          const uint32_t off = tc::sw32_offset(uint32_t(tid), uint32_t(h));
-#pragma unroll
-          for (int sl = 0; sl < NSL; ++sl)
-            *reinterpret_cast<uint4*>(As + sl * A_SLICE + off) =
-                make_uint4(o[sl][0], o[sl][1], o[sl][2], o[sl][3]);
+          const uint32_t off = tc::sw32_offset(uint32_t(32 * wq + 4 * st + ri), uint32_t(hh));
+          *reinterpret_cast<uint4*>(As + (2 * qd) * A_SLICE + off) =
+              make_uint4(wa[0], wa[1], wa[2], wa[3]);
+          *reinterpret_cast<uint4*>(As + (2 * qd + 1) * A_SLICE + off) =
+              make_uint4(wb[0], wb[1], wb[2], wb[3]);
         }
         tc::fence_proxy_async_smem();
-        tc::mbar_arrive(&full_a[stage]);
-        ++uses[stage];
-        stage = (stage + 1) % STAGES;
+        tc::mbar_arrive(&full_a[stg]);
       }
+      seq0 += uint32_t(kc);
       if (!ok) break;
-      // ---- epilogue: rho partial over the 128 rows of this item ----
+      // ---- epilogue: group grp reduces points 32grp .. 32grp+31 over the
+      // 32 rows of warp wq (TMEM lanes 32wq ..) ----
       if (!tc::mbar_wait(acc_full, nitem & 1, err, 12)) break;
       tc::fence_after_sync();
       const int g0 = b * p.blk + gt * TG;
       const int gw = min(min((b + 1) * p.blk, p.ngrid), g0 + TG) - g0;
-      const int tu = p.tau[size_t(s) * p.nao + iu];
-      const double* lrow = p.ao_lhs + size_t(iu) * p.stride_grid + g0;
-      const uint32_t trow = tmem + (uint32_t(32 * warp) << 16);
+      const int erow = ut * TU + 32 * wq + lane;
+      const bool ev = erow < nb;
+      const int eu = ev ? __ldg(I + erow) : 0;
+      const int tu = p.tau[size_t(s) * p.nao + eu];
+      const double* lrow = p.ao_lhs + size_t(eu) * p.stride_grid + g0;
+      const uint32_t trow = tmem + (uint32_t(32 * wq) << 16);
+      const size_t slot = ((size_t(bg) * p.max_ut + ut) * p.nset + s) * EPI_PARTS + wq;
 #pragma unroll 1
-      for (int cc = 0; cc < TG; cc += 16) {
+      for (int cc = 32 * grp; cc < 32 * grp + 32; cc += 16) {
         uint32_t v[NSL][16];
 #pragma unroll
         for (int L = 0; L < NSL; ++L) tc::tmem_ld_32x32b_x16(trow + uint32_t(L * TG + cc), v[L]);
         tc::tmem_ld_wait();
+        double a[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const int gl = cc + j;
-          double contrib = 0.0;
-          if (rvalid && gl < gw) {
+          a[j] = 0.0;
+          if (ev && gl < gw) {
             double x = double(int(v[NSL - 1][j]));
 #pragma unroll
             for (int L = NSL - 2; L >= 0; --L) x = fma(x, 0.0078125, double(int(v[L][j])));
             const int sg = p.sigma[g0 + gl];
-            contrib = (tu == kBadExp || sg == kBadExp)
-                          ? __longlong_as_double(0x7ff8000000000000LL)
-                          : ldexp(x, -(tu + sg)) * lrow[gl];
+            a[j] = (tu == kBadExp || sg == kBadExp) ? __longlong_as_double(0x7ff8000000000000LL)
+                                                    : ldexp(x, -(tu + sg)) * lrow[gl];
           }
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) contrib += __shfl_xor_sync(0xffffffffu, contrib, o);
-          if (lane == 0) red[warp][gl] = contrib;
         }
+        // reduce-scatter over the 32 rows: 16 shuffles leave lane pair
+        // (2m, 2m+1) with the sum of point m (fixed order: deterministic)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const bool up = (lane & 16) != 0;
+          const double keep = up ? a[j + 8] : a[j];
+          a[j] = keep + __shfl_xor_sync(0xffffffffu, up ? a[j] : a[j + 8], 16);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const bool up = (lane & 8) != 0;
+          const double keep = up ? a[j + 4] : a[j];
+          a[j] = keep + __shfl_xor_sync(0xffffffffu, up ? a[j] : a[j + 4], 8);
+        }
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const bool up = (lane & 4) != 0;
+          const double keep = up ? a[j + 2] : a[j];
+          a[j] = keep + __shfl_xor_sync(0xffffffffu, up ? a[j] : a[j + 2], 4);
+        }
+        {
+          const bool up = (lane & 2) != 0;
+          const double keep = up ? a[1] : a[0];
+          a[0] = keep + __shfl_xor_sync(0xffffffffu, up ? a[0] : a[1], 2);
+        }
+        a[0] += __shfl_xor_sync(0xffffffffu, a[0], 1);
+        const int m = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 +
+                      ((lane >> 1) & 1);
+        if ((lane & 1) == 0) p.partial[slot * TG + cc + m] = a[0];
       }
       tc::fence_before_sync();
       tc::mbar_arrive(acc_empty);  // the MMA warp may overwrite the accumulators
-      asm volatile("bar.sync 1, 128;" ::: "memory");
-      if (tid < TG) {
-        const size_t slot = (size_t(bg) * p.max_ut + ut) * p.nset + s;
-        p.partial[slot * TG + tid] = red[0][tid] + red[1][tid] + red[2][tid] + red[3][tid];
-      }
-      asm volatile("bar.sync 1, 128;" ::: "memory");
     }
-  } else if (warp == 4) {
+  } else if (warp == GATHER_WARPS) {
     // ---------------- MMA issuer ----------------
     if (lane == 0) {
       const uint32_t idesc = tc::idesc_i8(TU, TG);
-      uint32_t fuse[STAGES] = {0, 0, 0, 0};
-      int stage = 0;
-      uint32_t nitem = 0;
+      uint32_t seq = 0, nitem = 0;
       bool ok = true;
       for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++nitem) {
         const int4 it = p.items[t % per_set];
@@ -449,15 +506,16 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(MainArgs p) {
         const int kc = (nb + TK - 1) / TK;
         if (nitem > 0 && !tc::mbar_wait(acc_empty, (nitem - 1) & 1, err, 13)) break;
         tc::fence_after_sync();
-        for (int c = 0; c < kc; ++c) {
-          if (!tc::mbar_wait(&full_a[stage], fuse[stage] & 1, err, 14) ||
-              !tc::mbar_wait(&full_b[stage], fuse[stage] & 1, err, 15)) {
+        for (int c = 0; c < kc; ++c, ++seq) {
+          const int stg = int(seq % STAGES);
+          const uint32_t par = (seq / STAGES) & 1;
+          if (!tc::mbar_wait(&full_a[stg], par, err, 14) ||
+              !tc::mbar_wait(&full_b[stg], par, err, 15)) {
             ok = false;
             break;
           }
-          ++fuse[stage];
           tc::fence_after_sync();
-          const uint32_t a0 = tc::smem_u32(smem + stage * STAGE);
+          const uint32_t a0 = tc::smem_u32(smem + stg * STAGE);
           const uint32_t b0 = a0 + A_STAGE;
 #pragma unroll
           for (int L = 0; L < NSL; ++L)
@@ -465,8 +523,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(MainArgs p) {
             for (int i = 0; i <= L; ++i)
               tc::mma_i8(tmem + uint32_t(L * TG), tc::smem_desc_k32(a0 + i * A_SLICE),
                          tc::smem_desc_k32(b0 + (L - i) * B_SLICE), idesc, c > 0 || i > 0);
-          tc::mma_commit(&empty[stage]);
-          stage = (stage + 1) % STAGES;
+          tc::mma_commit(&empty[stg]);
         }
         if (!ok) break;
         tc::mma_commit(acc_full);
@@ -477,39 +534,41 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(MainArgs p) {
   } else {
     // ---------------- phi digit tiles: bulk loads ----------------
     if (lane == 0) {
-      uint32_t uses[STAGES] = {0, 0, 0, 0};
-      int stage = 0;
+      uint32_t seq = 0;
       bool ok = true;
       for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
         const int4 it = p.items[t % per_set];
         const int nb = p.counts[it.x / p.gsub];
         const int kc = (nb + TK - 1) / TK;
         const uint8_t* src = p.phisl + size_t(p.cbase[it.x]) * B_STAGE;
-        for (int c = 0; c < kc; ++c) {
-          if (uses[stage] > 0 && !tc::mbar_wait(&empty[stage], (uses[stage] - 1) & 1, err, 17)) {
+        for (int c = 0; c < kc; ++c, ++seq) {
+          const int stg = int(seq % STAGES);
+          const uint32_t use = seq / STAGES;
+          if (use > 0 && !tc::mbar_wait(&empty[stg], (use - 1) & 1, err, 17)) {
             ok = false;
             break;
           }
-          tc::mbar_arrive_expect_tx(&full_b[stage], B_STAGE);
-          tc::bulk_load(smem + stage * STAGE + A_STAGE, src + size_t(c) * B_STAGE, B_STAGE,
-                        &full_b[stage]);
-          ++uses[stage];
-          stage = (stage + 1) % STAGES;
+          tc::mbar_arrive_expect_tx(&full_b[stg], B_STAGE);
+          tc::bulk_load(smem + stg * STAGE + A_STAGE, src + size_t(c) * B_STAGE, B_STAGE,
+                        &full_b[stg]);
         }
       }
-      for (int s = 0; s < STAGES; ++s)
-        if (uses[s] > 0) tc::mbar_wait(&full_b[s], (uses[s] - 1) & 1, err, 18, true);
+      // copies still in flight complete before the CTA exits
+      for (int s = 0; s < STAGES; ++s) {
+        const uint32_t uses = (seq + STAGES - 1 - s) / STAGES;  // chunks n < seq with n % STAGES == s
+        if (uses > 0) tc::mbar_wait(&full_b[s], (uses - 1) & 1, err, 18, true);
+      }
     }
   }
 
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
-  if (warp == 4) tc::tmem_dealloc(tmem, 512);
+  if (warp == GATHER_WARPS) tc::tmem_dealloc(tmem, 512);
 }
 
 // ---------------------------------------------------------------------------
-// deterministic reduction of the row-tile partials into rho
+// deterministic reduction of the (row tile, row quarter) partials into rho
 // ---------------------------------------------------------------------------
 __global__ void split_reduce(double* __restrict__ rhos, const double* __restrict__ partial,
                              const int* __restrict__ counts, size_t stride_grid, int ngrid,
@@ -525,7 +584,10 @@ __global__ void split_reduce(double* __restrict__ rhos, const double* __restrict
     const int s = t / TG, j = t % TG;
     if (g0 + j >= gend) continue;
     double v = 0.0;
-    for (int u = 0; u < nt; ++u) v += partial[((size_t(bg) * max_ut + u) * nset + s) * TG + j];
+    for (int u = 0; u < nt; ++u) {
+      const double* q = partial + ((size_t(bg) * max_ut + u) * nset + s) * EPI_PARTS * TG + j;
+      for (int w = 0; w < EPI_PARTS; ++w) v += q[w * TG];
+    }
     double* r = rhos + size_t(s) * stride_grid + g0 + j;
     *r = v + *r;
   }
@@ -554,7 +616,7 @@ Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk) {
   L.sigma = L.tau + a256(nset * nao * sizeof(int));
   L.phisl = L.sigma + a256(ngrid * sizeof(int));
   L.partial = L.phisl + a256(nbg * max_kc * B_STAGE);
-  L.bytes = L.partial + nbg * max_ut * nset * TG * sizeof(double);
+  L.bytes = L.partial + nbg * max_ut * nset * EPI_PARTS * TG * sizeof(double);
   return L;
 }
 
@@ -591,10 +653,8 @@ cudaError_t aodmao2rho_split(double* rhos, const double* dms, const double* ao_l
   split_build<<<1, 1024, 0, stream>>>(counts, nbg, gsub, nset, max_ut, cbase, items, total);
   split_d_slices<<<nset * nao, 256, 0, stream>>>(dms, stride_ao, stride_ao * stride_ao, nao, dsl,
                                                  tau);
-  split_phi_sigma<<<nbg, TG, 0, stream>>>(ao_rhs, stride_grid, lists, counts, nao, ngrid, blk,
-                                          gsub, sigma);
-  split_phi_slices<<<nbg, 256, 0, stream>>>(ao_rhs, stride_grid, lists, counts, cbase, sigma, nao,
-                                            ngrid, blk, gsub, phisl);
+  split_phi<<<nbg, 256, 0, stream>>>(ao_rhs, stride_grid, lists, counts, cbase, nao, ngrid, blk,
+                                     gsub, sigma, phisl);
   if ((err = cudaGetLastError()) != cudaSuccess) return err;
 
   MainArgs a;

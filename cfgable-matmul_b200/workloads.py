@@ -182,55 +182,173 @@ def shell_sizes_for(rng, nshell: int, nao: int) -> np.ndarray:
     return sizes
 
 
-def geometric(seed: int = 0, nao: int = 2228, nshell: int = 400, natom: int = 110,
-              ngrid: int = 16384, blksize: int = 64, nset: int = 3, density: float = 0.3,
-              box_angstrom: float = 16.0) -> AodmProblem:
-    """Taxol-sized geometric contraction: natom centres uniform in a cube of
-    `box_angstrom`; each shell sits on a centre (AOs ordered by centre), has
-    exponent alpha log-uniform in [0.05, 20] bohr^-2 and the real solid
-    harmonics of its angular momentum (sizes 1,3,5,7 = s,p,d,f); each block of
-    `blksize` grid points is sampled around one centre (Gaussian offsets,
-    sigma 1.5 bohr), as atom-centred DFT grids grouped into blocks are.  The
-    (shell, block) mask keeps the `density` fraction of tiles with the
-    largest max|phi|; phi is zeroed in the other tiles."""
+@dataclass
+class Molecule:
+    """Shells of Gaussian AOs on atom centres (AOs ordered by centre)."""
+    centres: np.ndarray      # (natom, 3) bohr
+    shell_atom: np.ndarray   # (nshell,)
+    shell_l: np.ndarray      # (nshell,) angular momentum 0..3
+    alpha: np.ndarray        # (nshell,) bohr^-2
+    sizes: np.ndarray        # (nshell,) 2l+1
+
+    @property
+    def nao(self): return int(self.sizes.sum())
+
+    @property
+    def nshell(self): return len(self.sizes)
+
+    @property
+    def rows(self): return np.concatenate([[0], np.cumsum(self.sizes)[:-1]]).astype(np.int32)
+
+    @property
+    def norm(self):
+        a, l = self.alpha, self.shell_l
+        return (2 * a / np.pi) ** 0.75 * (4 * a) ** (l / 2)
+
+    @property
+    def shell_xyz(self): return np.ascontiguousarray(self.centres[self.shell_atom])
+
+
+def molecule(seed: int = 0, nao: int = 2228, nshell: int = 400, natom: int = 110,
+             box_angstrom: float = 16.0) -> Molecule:
+    """natom centres uniform in a cube of `box_angstrom`; shells of sizes
+    1,3,5,7 (s,p,d,f) summing to nao, sorted onto centres; exponents
+    log-uniform in [0.05, 20] bohr^-2."""
     rng = np.random.default_rng(seed)
-    bohr = 1.0 / 0.529177210903
-    box = box_angstrom * bohr
+    box = box_angstrom / 0.529177210903
     centres = rng.uniform(0.0, box, (natom, 3))
     sizes = shell_sizes_for(rng, nshell, nao)
     shell_atom = np.sort(rng.integers(0, natom, nshell))
     alpha = np.exp(rng.uniform(np.log(0.05), np.log(20.0), nshell))
+    return Molecule(centres, shell_atom, (sizes - 1) // 2, alpha, sizes)
+
+
+def grid_points(rng, mol: Molecule, ngrid: int, blksize: int) -> np.ndarray:
+    """Each block of `blksize` points is sampled around one centre (Gaussian
+    offsets, sigma 1.5 bohr), as atom-centred DFT grids grouped into blocks are."""
     nblk = -(-ngrid // blksize)
-    blk_atom = rng.integers(0, natom, nblk)
-    pts = centres[np.repeat(blk_atom, blksize)[:ngrid]] + rng.normal(0.0, 1.5, (ngrid, 3))
-    ao = np.empty((nao, ngrid))
-    row = 0
-    for s in range(nshell):
-        d = pts - centres[shell_atom[s]]
+    blk_atom = rng.integers(0, len(mol.centres), nblk)
+    return mol.centres[np.repeat(blk_atom, blksize)[:ngrid]] + rng.normal(0.0, 1.5, (ngrid, 3))
+
+
+def eval_ao_numpy(mol: Molecule, pts: np.ndarray) -> np.ndarray:
+    """phi[row + f][g] = N exp(-alpha r^2) Y_f, Y_f the real solid harmonics."""
+    ao = np.empty((mol.nao, len(pts)))
+    rows, norm = mol.rows, mol.norm
+    for s in range(mol.nshell):
+        d = pts - mol.centres[mol.shell_atom[s]]
         x, y, z = d[:, 0], d[:, 1], d[:, 2]
-        r2 = x * x + y * y + z * z
-        a = alpha[s]
-        l = (sizes[s] - 1) // 2
-        norm = (2 * a / np.pi) ** 0.75 * (4 * a) ** (l / 2)
-        radial = norm * np.exp(-a * r2)
-        for f in _solid_harmonics(l, x, y, z):
-            ao[row] = radial * f
-            row += 1
-    # (shell, block) maxima and the density quantile
-    starts = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+        radial = norm[s] * np.exp(-mol.alpha[s] * (x * x + y * y + z * z))
+        for f, h in enumerate(_solid_harmonics(int(mol.shell_l[s]), x, y, z)):
+            ao[rows[s] + f] = radial * h
+    return ao
+
+
+def shell_block_max(mol: Molecule, ao: np.ndarray, blksize: int) -> np.ndarray:
+    nao, ngrid = ao.shape
+    nblk = -(-ngrid // blksize)
     absao = np.abs(ao)
     pad = nblk * blksize - ngrid
     if pad:
         absao = np.concatenate([absao, np.zeros((nao, pad))], axis=1)
     blkmax = absao.reshape(nao, nblk, blksize).max(axis=2)
-    shmax = np.maximum.reduceat(blkmax, starts, axis=0)
-    thr = np.quantile(shmax, 1.0 - density)
-    sh_tab = (shmax > thr).astype(np.uint8)
-    tab = np.repeat(sh_tab, sizes, axis=0)
+    return np.maximum.reduceat(blkmax, mol.rows, axis=0)
+
+
+def density_threshold(shmax: np.ndarray, density: float) -> float:
+    """Threshold keeping the `density` fraction of (shell, block) tiles."""
+    return float(np.quantile(shmax, 1.0 - density))
+
+
+def geometric(seed: int = 0, nao: int = 2228, nshell: int = 400, natom: int = 110,
+              ngrid: int = 16384, blksize: int = 64, nset: int = 3, density: float = 0.3,
+              box_angstrom: float = 16.0) -> AodmProblem:
+    """Taxol-sized geometric contraction (numpy): molecule(seed) and a grid
+    drawn from the same seed; the (shell, block) mask keeps the `density`
+    fraction of tiles with the largest max|phi|; phi is zeroed elsewhere."""
+    mol = molecule(seed, nao, nshell, natom, box_angstrom)
+    rng = np.random.default_rng(seed + 1_000_003)
+    pts = grid_points(rng, mol, ngrid, blksize)
+    ao = eval_ao_numpy(mol, pts)
+    shmax = shell_block_max(mol, ao, blksize)
+    sh_tab = (shmax > density_threshold(shmax, density)).astype(np.uint8)
+    tab = np.repeat(sh_tab, mol.sizes, axis=0)
     ao[~expand_mask(tab, ngrid, blksize)] = 0.0
     return AodmProblem(np.ascontiguousarray(ao), sym_dms(rng, nset, nao),
-                       np.ascontiguousarray(tab), blksize, sizes,
+                       np.ascontiguousarray(tab), blksize, mol.sizes,
                        f"geometric nao={nao} ngrid={ngrid} nset={nset}")
+
+
+# ---------------------------------------------------------------------------
+# device-side generation through the library's AO evaluator
+# ---------------------------------------------------------------------------
+class DeviceMolecule:
+    """A Molecule's shell arrays on the device, for cfgmm_eval_ao_dev."""
+
+    def __init__(self, mol: Molecule, device="cuda"):
+        import torch
+        self.mol = mol
+        self.xyz = torch.from_numpy(mol.shell_xyz).to(device)
+        self.l = torch.from_numpy(mol.shell_l.astype(np.int32)).to(device)
+        self.alpha = torch.from_numpy(mol.alpha.astype(np.float64)).to(device)
+        self.norm = torch.from_numpy(mol.norm.astype(np.float64)).to(device)
+        self.row = torch.from_numpy(mol.rows).to(device)
+
+
+def device_grid(cm, dmol: DeviceMolecule, pts: np.ndarray, blksize: int, density: float):
+    """phi (nao, ngrid) and tab (nao, nblk) on the device: AOs evaluated by the
+    library, mask at the `density` quantile of the (shell, block) maxima."""
+    import torch
+    mol = dmol.mol
+    ngrid = len(pts)
+    nblk = -(-ngrid // blksize)
+    dev = dmol.xyz.device
+    p = torch.from_numpy(np.ascontiguousarray(pts)).to(dev)
+    ao = torch.empty(mol.nao, ngrid, dtype=torch.float64, device=dev)
+    bmax = torch.empty(mol.nshell, nblk, dtype=torch.float64, device=dev)
+    tab = torch.empty(mol.nao, nblk, dtype=torch.uint8, device=dev)
+    cm.eval_ao(ao, p, dmol.xyz, dmol.l, dmol.alpha, dmol.norm, dmol.row, bmax, blksize)
+    thr = float(torch.quantile(bmax.flatten(), 1.0 - density))
+    cm.mask_ao(ao, ngrid, dmol.l, dmol.row, bmax, thr, tab, blksize)
+    return ao, tab
+
+
+@dataclass
+class BatchedProblem:
+    mol: Molecule
+    dms: object             # torch (nset_max, nao, nao)
+    batches: list           # [(ao, tab, ngrid, nset, density)] device tensors
+    blksize: int
+
+    def flops(self) -> float:
+        tot = 0.0
+        for ao, tab, ngrid, nset, _ in self.batches:
+            tot += masked_flops(tab.cpu().numpy(), ngrid, self.blksize, nset)
+        return tot
+
+    def points(self) -> int:
+        return sum(b[2] for b in self.batches)
+
+
+def batched_uneven(cm, seed: int = 0, nbatch: int = 256, nao: int = 2228, nshell: int = 400,
+                   natom: int = 110, gmin: int = 128, gmax: int = 4096, dmin: float = 0.05,
+                   dmax: float = 0.6, nset_max: int = 3, blksize: int = 64) -> BatchedProblem:
+    """Uneven grid batches of one taxol-sized molecule: ngrid log-uniform in
+    [gmin, gmax], tile density uniform in [dmin, dmax], 1..nset_max DMs each;
+    phi and masks evaluated on the device."""
+    import torch
+    mol = molecule(seed, nao, nshell, natom)
+    rng = np.random.default_rng(seed + 7)
+    dmol = DeviceMolecule(mol)
+    batches = []
+    for _ in range(nbatch):
+        ngrid = int(np.exp(rng.uniform(np.log(gmin), np.log(gmax))))
+        dens = float(rng.uniform(dmin, dmax))
+        nset = int(rng.integers(1, nset_max + 1))
+        ao, tab = device_grid(cm, dmol, grid_points(rng, mol, ngrid, blksize), blksize, dens)
+        batches.append((ao, tab, ngrid, nset, dens))
+    dms = torch.from_numpy(sym_dms(rng, nset_max, nao)).cuda()
+    return BatchedProblem(mol, dms, batches, blksize)
 
 
 def dgemm_uniform(m: int = 3527, n: int = 9583, k: int = 6581, transa: bool = False,

@@ -219,6 +219,58 @@ int cfgmm_aodmao2rho_dev_noalloc(double* rhos, const double* dms, const double* 
                                  size_t nao, size_t ngrid, size_t nset, const uint8_t* tab,
                                  size_t ldtab, size_t blksize, void* stream);
 
+/* ---- batched plans: many grid batches of one molecule in one launch ------
+ * No counterpart in the reference (whose callers batch grids themselves,
+ * impl_matmul.rs:354-355): a plan holds device pointers to every batch's phi
+ * tables, mask and rho plus the density matrices shared by all batches.  It
+ * builds the active lists and one global work list once, picks the kernel's
+ * tile configuration with an autotuner (timed on the problem, cached in
+ * CFGMM_AUTOTUNE_CACHE), and captures the run in a CUDA graph.  phi and the
+ * masks must not change while the plan lives; the contents of `dms` may (an
+ * SCF step); each run accumulates into every batch's rho. */
+typedef struct cfgmm_aodm_batch {
+  double* rhos;            /* (nset, stride_grid), device */
+  const double* ao_lhs;    /* (nao, stride_grid), device */
+  const double* ao_rhs;    /* (nao, stride_grid), device */
+  const uint8_t* tab;      /* (nao, ldtab), device */
+  size_t stride_grid, ngrid, ldtab;
+  size_t nset;             /* uses density matrices 0 .. nset-1 (<= the plan's nset_max) */
+} cfgmm_aodm_batch;
+
+typedef struct cfgmm_aodm_plan cfgmm_aodm_plan;
+
+#define CFGMM_PLAN_NO_GRAPH 1 /* run with plain launches instead of a CUDA graph */
+#define CFGMM_PLAN_NO_TUNE  2 /* skip the autotuner: default tiles */
+
+int cfgmm_aodm_plan_create(cfgmm_aodm_plan** plan, const cfgmm_aodm_batch* batches, size_t nbatch,
+                           const double* dms, size_t stride_ao, size_t nao, size_t nset_max,
+                           size_t blksize, int precision, int flags, void* stream);
+int cfgmm_aodm_plan_run(cfgmm_aodm_plan* plan, void* stream);
+/* JSON description: batch and item counts, chosen tiles, autotuner timings. */
+const char* cfgmm_aodm_plan_info(const cfgmm_aodm_plan* plan);
+int cfgmm_aodm_plan_destroy(cfgmm_aodm_plan* plan);
+
+/* ---- the step before the contraction: AOs on the grid, on the device ------
+ * No counterpart in the reference (its callers tabulate phi themselves).
+ * phi[shell_row[sh] + f][g] = shell_norm[sh] exp(-shell_alpha[sh] r^2) Y_f(x,y,z)
+ * for the 2*shell_l[sh]+1 real solid harmonics Y_f (l <= 3, unnormalised
+ * polynomials), (x,y,z) = points[g] - shell_xyz[sh], r^2 = x^2+y^2+z^2.
+ * All arrays are device arrays; points and shell_xyz are (n, 3); nshell <=
+ * 65535 and shell_l[sh] in 0..3 (checked by neither call: device data).  With
+ * shell_block_max != NULL also writes max |phi| per (shell, block of blksize
+ * points), a (nshell, ceil(ngrid/blksize)) array. */
+int cfgmm_eval_ao_dev(double* ao, size_t stride_grid, const double* points, size_t ngrid,
+                      const double* shell_xyz, const int* shell_l, const double* shell_alpha,
+                      const double* shell_norm, const int* shell_row, size_t nshell,
+                      double* shell_block_max, size_t blksize, void* stream);
+
+/* The mask of the contraction from those maxima: tab[row][b] = 1 for every row
+ * of shell sh when shell_block_max[sh][b] > threshold, else 0 with phi zeroed
+ * on that (row, block). */
+int cfgmm_mask_ao_dev(double* ao, size_t stride_grid, size_t ngrid, const int* shell_l,
+                      const int* shell_row, size_t nshell, const double* shell_block_max,
+                      double threshold, uint8_t* tab, size_t ldtab, size_t blksize, void* stream);
+
 /* Releases the calling device's cached workspaces (they are otherwise kept
  * and reused across calls until process exit). */
 int cfgmm_release_workspace(void);

@@ -1,0 +1,140 @@
+"""GPU tests of batched AO-DM-AO plans (cfgmm_aodm_plan_*).
+
+A plan contracts many grid batches of one molecule in one persistent launch.
+Its result must equal, batch by batch, the single-call contraction (which is
+itself pinned to the oracle), with and without the CUDA graph and the
+autotuner; runs accumulate; new density-matrix contents are picked up by the
+captured graph; the autotuner's choice is cached on disk and reused.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import normwise
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-13
+
+
+def _batches(wl, torch, seed, nbatch, nao=200, nset_max=3, blk=64):
+    """Uneven ragged batches (ngrid 1..700, densities 0..1) of random phi."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(nbatch):
+        ngrid = int(rng.integers(1, 700))
+        nblk = -(-ngrid // blk)
+        dens = [0.0, 1.0, rng.uniform(0.05, 0.6)][i % 3] if i < 6 else rng.uniform(0.05, 0.6)
+        tab = (rng.random((nao, nblk)) < dens).astype(np.uint8)
+        lhs = rng.standard_normal((nao, ngrid))
+        rhs = rng.standard_normal((nao, ngrid))
+        m = wl.expand_mask(tab, ngrid, blk)
+        lhs[~m] = 0.0
+        rhs[~m] = 0.0
+        nset = int(rng.integers(1, nset_max + 1))
+        rho0 = rng.standard_normal((nset, ngrid))
+        out.append(dict(lhs=lhs, rhs=rhs, tab=tab, nset=nset, rho0=rho0, ngrid=ngrid))
+    dms = rng.standard_normal((nset_max, nao, nao))
+    return out, dms
+
+
+def _device(torch, bs, dms):
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    dev = [(t(b["rho0"]), t(b["lhs"]), t(b["rhs"]), t(b["tab"]), b["nset"]) for b in bs]
+    return dev, t(dms)
+
+
+def _single(cm, torch, b, dms, blk):
+    nao, ngrid = b["lhs"].shape
+    rho = b["rho0"].copy()
+    cm.aodmao2rho_ex(rho, np.ascontiguousarray(dms[: b["nset"]]), b["lhs"], b["rhs"],
+                     (nao, ngrid), (nao, ngrid), b["nset"], b["tab"], b["tab"].shape[1], blk)
+    return rho
+
+
+@pytest.mark.parametrize("graph,tune", [(True, True), (False, False), (True, False)])
+def test_plan_equals_single_calls(cm, wl, tmp_path, monkeypatch, graph, tune):
+    import torch
+    monkeypatch.setenv("CFGMM_AUTOTUNE_CACHE", str(tmp_path / "tune.txt"))
+    bs, dms = _batches(wl, torch, 1, 23)
+    dev, ddms = _device(torch, bs, dms)
+    plan = cm.AodmPlan(dev, ddms, blksize=64, graph=graph, tune=tune)
+    plan.run()
+    torch.cuda.synchronize()
+    info = plan.info()
+    assert info["batches"] == 23 and info["graph"] is graph
+    for b, d in zip(bs, dev):
+        ref = _single(cm, torch, b, dms, 64)
+        assert normwise(d[0].cpu().numpy(), ref) < TOL
+    plan.close()
+
+
+def test_plan_runs_accumulate_and_follow_dms(cm, wl):
+    import torch
+    bs, dms = _batches(wl, torch, 2, 9, nao=130)
+    for b in bs:
+        b["rho0"][:] = 0.0
+    dev, ddms = _device(torch, bs, dms)
+    plan = cm.AodmPlan(dev, ddms, blksize=64, tune=False)
+    plan.run()
+    plan.run()
+    torch.cuda.synchronize()
+    for b, d in zip(bs, dev):
+        ref = _single(cm, torch, b, dms, 64)
+        assert normwise(d[0].cpu().numpy(), 2.0 * ref) < TOL
+    # new DM contents (an SCF step): the captured graph reads them
+    dms2 = -0.5 * dms + 1.0
+    ddms.copy_(torch.from_numpy(dms2))
+    for d in dev:
+        d[0].zero_()
+    plan.run()
+    torch.cuda.synchronize()
+    for b, d in zip(bs, dev):
+        ref = _single(cm, torch, b, dms2, 64)
+        assert normwise(d[0].cpu().numpy(), ref) < TOL
+    plan.close()
+
+
+def test_plan_other_block_sizes(cm, wl):
+    import torch
+    for blk in (48, 128, 200):
+        bs, dms = _batches(wl, torch, blk, 7, nao=97, blk=blk)
+        dev, ddms = _device(torch, bs, dms)
+        plan = cm.AodmPlan(dev, ddms, blksize=blk, tune=False)
+        plan.run()
+        torch.cuda.synchronize()
+        for b, d in zip(bs, dev):
+            ref = _single(cm, torch, b, dms, blk)
+            assert normwise(d[0].cpu().numpy(), ref) < TOL
+        plan.close()
+
+
+def test_autotune_cache(cm, wl, tmp_path, monkeypatch):
+    import torch
+    path = tmp_path / "sub" / "tune.txt"
+    monkeypatch.setenv("CFGMM_AUTOTUNE_CACHE", str(path))
+    bs, dms = _batches(wl, torch, 3, 12)
+    dev, ddms = _device(torch, bs, dms)
+    p1 = cm.AodmPlan(dev, ddms, blksize=64)
+    i1 = p1.info()
+    assert isinstance(i1["tuning"], list) and len(i1["tuning"]) == 6
+    assert min(t["ms"] for t in i1["tuning"]) > 0
+    lines = path.read_text().split()
+    assert lines[0] == i1["key"]
+    p2 = cm.AodmPlan(dev, ddms, blksize=64)
+    i2 = p2.info()
+    assert i2["tuning"] == "cache" and i2["config"] == i1["config"]
+    p1.close()
+    p2.close()
+
+
+def test_plan_rejections(cm, wl):
+    import torch
+    bs, dms = _batches(wl, torch, 4, 2, nset_max=2)
+    dev, ddms = _device(torch, bs, dms)
+    with pytest.raises(NotImplementedError):
+        cm.AodmPlan(dev, ddms, precision=cm.PREC_OZAKI_INT8)
+    bad = [(d[0], d[1], d[2], d[3], 3) for d in dev]  # nset above nset_max
+    with pytest.raises(ValueError):
+        cm.AodmPlan(bad, ddms)
