@@ -327,8 +327,8 @@ int aodm_host(double* rhos, size_t rhos_len, const double* dms, size_t dms_len,
   if (rc != CFGMM_OK) return rc;
   if ((rc = check_precision(precision)) != CFGMM_OK) return rc;
   const bool split = precision == CFGMM_PREC_OZAKI_INT8;
-  if (split && nao > 65535)
-    return fail(CFGMM_ERR_UNIMPLEMENTED, "split-precision AO-DM-AO supports nao <= 65535");
+  if (split && nao > 16384)
+    return fail(CFGMM_ERR_UNIMPLEMENTED, "split-precision AO-DM-AO supports nao <= 16384");
   if (ex.rhos == 0) return CFGMM_OK;
   int dev;
   if ((rc = current_device(&dev)) != CFGMM_OK) return rc;
@@ -614,8 +614,8 @@ int cfgmm_aodmao2rho_dev(double* rhos, const double* dms, const double* ao_lhs,
   if (rc != CFGMM_OK) return rc;
   if ((rc = check_precision(precision)) != CFGMM_OK) return rc;
   const bool split = precision == CFGMM_PREC_OZAKI_INT8;
-  if (split && nao > 65535)
-    return fail(CFGMM_ERR_UNIMPLEMENTED, "split-precision AO-DM-AO supports nao <= 65535");
+  if (split && nao > 16384)
+    return fail(CFGMM_ERR_UNIMPLEMENTED, "split-precision AO-DM-AO supports nao <= 16384");
   if (ex.rhos == 0) return CFGMM_OK;
   int dev;
   if ((rc = current_device(&dev)) != CFGMM_OK) return rc;

@@ -4,16 +4,17 @@
 //
 //   Every row u of D_s is scaled by 2^tau_u and every grid point g of phi by
 //   2^sigma_g so that the scaled values are below 2^6 in magnitude; each is
-//   then written as eight signed digits  x' = sum_{j<8} x_j 2^(-7j)  with
-//   every x_j in [-64, 64] (round to nearest at every step).  The products of
-//   the digits of D and phi whose levels add up to L = i + j <= 7 are summed
+//   then written as seven signed base-256 digits  x' = sum_{j<7} x_j 2^(-8j)
+//   with x_0 in [-64, 64] and x_j in [-128, 127], read off the bytes of the
+//   integer round(x' 2^48) (digits_packed below).  The products of the
+//   digits of D and phi whose levels add up to L = i + j <= 6 are summed
 //   EXACTLY in one INT32 accumulator per level:
-//     S_L[u][g] = sum_{i+j=L} sum_v d_i(u,v) p_j(v,g)        (36 INT8 MMAs)
-//   and X[u][g] = 2^-(tau_u + sigma_g) sum_L 2^(-7L) S_L[u][g] in FP64.  The
-//   dropped levels L >= 8 weigh at most 7 * 2^-56 of the largest scaled
-//   product and the digit remainders 2^-56 each, so X carries about 52 bits
-//   relative to sum_v |D_uv| |phi_vg|.  |S_L| <= 8 * 4096 * nao keeps the INT32
-//   sums exact for nao <= 65535.
+//     S_L[u][g] = sum_{i+j=L} sum_v d_i(u,v) p_j(v,g)        (28 INT8 MMAs)
+//   and X[u][g] = 2^-(tau_u + sigma_g) sum_L 2^(-8L) S_L[u][g] in FP64.  The
+//   dropped levels L >= 7 weigh at most 6 * 2^-54 of the largest scaled
+//   product and the digit remainders 2^-55 each, so X carries about 51 bits
+//   relative to sum_v |D_uv| |phi_vg|.  |S_L| <= 7 * 2^14 * nao keeps the
+//   INT32 sums exact for nao <= 16384.
 //
 // The contraction itself follows aodmao2rho_loop_parallel
 // (src/impl_aodmao2rho.rs:171-244): per grid block b the active list I(b) of
@@ -22,14 +23,16 @@
 // and rho[s][g] += sum_{u in I} phi[u][g] X[u][g].
 //
 // Kernels:
-//   split_d_slices    one CTA per row of D_s: row scale, 8 digits per element
+//   split_d_slices    a warp per row of D_s: row scale, 7 digits per element
 //                     stored as 8 bytes, so the gather of one element is one
 //                     8-byte load -- the same traffic as the FP64 kernel.
-//   split_phi         per (block, 64-point tile): point scales, then the digit
-//                     tiles of phi[I(b), tile] chunk by chunk (32 compacted
-//                     AOs), staged in shared memory and written out in the
-//                     UMMA 32-byte-swizzled K-major layout, so one bulk copy
-//                     moves the 8 digit tiles of a chunk into shared memory.
+//   split_phi_max     per (64-point tile, slab of 64 active AOs): max |phi|
+//                     per point, combined by atomic max.
+//   split_phi_digits  per (64-point tile, chunk of 32 active AOs): point
+//                     scales and the digit tiles of phi[I(b), tile], staged in
+//                     shared memory and written out in the UMMA
+//                     32-byte-swizzled K-major layout, so one bulk copy moves
+//                     the 7 digit tiles of a chunk into shared memory.
 //   split_build       work list (block tile, 128-row tile of I(b), DM) and
 //                     chunk offsets.
 //   split_main        persistent, 10 warps: warps 0-7 gather the D digits of
@@ -38,8 +41,8 @@
 //                     along a row read consecutive columns; two shuffle rounds
 //                     turn the 8-byte elements into digit planes, stored
 //                     without bank conflicts) and later run the epilogue;
-//                     warp 8 issues the 36 MMAs of a chunk (M=128, N=64, K=32)
-//                     into 8 TMEM level accumulators (all 512 columns); warp 9
+//                     warp 8 issues the 28 MMAs of a chunk (M=128, N=64, K=32)
+//                     into 7 TMEM level accumulators (448 columns); warp 9
 //                     bulk-loads the phi digit tiles.  The epilogue rebuilds X
 //                     in FP64, weights it with phi and reduces over the rows
 //                     of each warp; X never leaves the SM.
@@ -48,6 +51,7 @@
 #include <cuda_runtime.h>
 
 #include <climits>
+#include <cstdlib>
 #include <cstdint>
 
 #include "aodmao2rho_fp64.cuh"
@@ -60,12 +64,12 @@ namespace {
 constexpr int TU = 128;   // compacted rows per item (TMEM lanes)
 constexpr int TG = 64;    // grid points per item
 constexpr int TK = 32;    // compacted columns per chunk (one INT8 MMA K step)
-constexpr int NSL = 8;    // digits per value
-constexpr int STAGES = 4;
+constexpr int NSL = 7;    // digits per value
+constexpr int kDefaultStages = 3;  // pipeline depth (CFGMM_SPLIT_STAGES overrides: 2..5)
 constexpr uint32_t A_SLICE = TU * TK;        // 4096 B
 constexpr uint32_t B_SLICE = TG * TK;        // 2048 B
-constexpr uint32_t A_STAGE = NSL * A_SLICE;  // 32768 B
-constexpr uint32_t B_STAGE = NSL * B_SLICE;  // 16384 B
+constexpr uint32_t A_STAGE = NSL * A_SLICE;  // 28672 B
+constexpr uint32_t B_STAGE = NSL * B_SLICE;  // 14336 B
 constexpr uint32_t STAGE = A_STAGE + B_STAGE;
 constexpr int GATHER_WARPS = 8;               // two groups of four
 constexpr int THREADS = 32 * (GATHER_WARPS + 2);
@@ -82,144 +86,169 @@ __device__ __forceinline__ int exp_for(double amax) {  // 2^6 > amax * 2^exp
   return 6 - E;
 }
 
-// x (|x| < 2^6 after scaling) -> 8 signed digits, x = sum_j d_j 2^(-7j) + O(2^-50).
-__device__ __forceinline__ void digits(double x, int (&d)[NSL]) {
-  double r = x;
-#pragma unroll
-  for (int j = 0; j < NSL; ++j) {
-    const double t = rint(r);
-    d[j] = int(t);
-    r = (r - t) * 128.0;  // exact
-  }
+// 2^k for k in [-1022, 1023].
+__device__ __forceinline__ double pow2(int k) {
+  return __longlong_as_double(static_cast<long long>(k + 1023) << 52);
 }
 
-__device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
-  return (uint32_t(a) & 0xffu) | ((uint32_t(b) & 0xffu) << 8) | ((uint32_t(c) & 0xffu) << 16) |
-         ((uint32_t(d) & 0xffu) << 24);
+// The 7 digits of x * 2^e (|x * 2^e| < 2^6) packed as bytes 0..6 (byte 7 = 0).
+// X = round(x * 2^(e+48)) is an integer below 2^54 in magnitude; adding
+// 0x808080808080 = 128 * sum_{j<6} 256^j makes every low byte u_j of the sum
+// the unsigned form of a balanced digit u_j - 128 in [-128, 127] (flipping
+// bit 7 of the byte turns it into that signed byte), and leaves
+// floor((X + 0x808080808080) / 2^48) in [-64, 64] as the leading digit:
+//   X = d_0 256^6 + sum_{j=1..6} d_j 256^(6-j),  x 2^e = sum_j d_j 2^(-8j) + r 2^-48,
+// |r| <= 1/2.  The scaling by 2^(e+48) is done in two exact halves.
+__device__ __forceinline__ uint2 digits_packed(double x, int e) {
+  const int k = e + 48;
+  const int k1 = k / 2;
+  const long long X = __double2ll_rn(x * pow2(k1) * pow2(k - k1));
+  const unsigned long long Z =
+      static_cast<unsigned long long>(X + 0x808080808080LL) ^ 0x808080808080ULL;
+  const uint32_t lo = static_cast<uint32_t>(Z);        // d6 d5 d4 d3
+  const uint32_t hi = static_cast<uint32_t>(Z >> 32);  // d2 d1 d0 (sign byte)
+  return make_uint2(__byte_perm(hi, lo, 0x7012), __byte_perm(lo, 0u, 0x4012));
+}
+
+// 4x4 byte transpose: out_i holds byte i of w0..w3 (w_t in byte t).
+__device__ __forceinline__ void transpose4(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3,
+                                           uint32_t& o0, uint32_t& o1, uint32_t& o2,
+                                           uint32_t& o3) {
+  const uint32_t a = __byte_perm(w0, w1, 0x5140);  // w0.b0 w1.b0 w0.b1 w1.b1
+  const uint32_t b = __byte_perm(w0, w1, 0x7362);  // w0.b2 w1.b2 w0.b3 w1.b3
+  const uint32_t c = __byte_perm(w2, w3, 0x5140);
+  const uint32_t d = __byte_perm(w2, w3, 0x7362);
+  o0 = __byte_perm(a, c, 0x5410);
+  o1 = __byte_perm(a, c, 0x7632);
+  o2 = __byte_perm(b, d, 0x5410);
+  o3 = __byte_perm(b, d, 0x7632);
 }
 
 // ---------------------------------------------------------------------------
-// D digits: dsl[s][u][v] = 8 bytes (digits 0..7), tau[s][u]
+// D digits: dsl[s][u][v] = 8 bytes (digits 0..6, 0), tau[s][u]
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
 split_d_slices(const double* __restrict__ dms, size_t stride_ao, size_t dm_stride, int nao,
-               uint2* __restrict__ dsl, int* __restrict__ tau) {
-  const int row = blockIdx.x;  // s * nao + u
+               int nrows, uint2* __restrict__ dsl, int* __restrict__ tau) {
+  const int row = blockIdx.x * 8 + (threadIdx.x >> 5);  // s * nao + u, a warp per row
+  const int lane = threadIdx.x & 31;
+  if (row >= nrows) return;
   const int s = row / nao, u = row % nao;
   const double* d = dms + size_t(s) * dm_stride + size_t(u) * stride_ao;
   double mx = 0.0;
   bool bad = false;
-  for (int v = threadIdx.x; v < nao; v += 256) {
+#pragma unroll 4
+  for (int v = lane; v < nao; v += 32) {
     const double a = fabs(d[v]);
     bad |= !(a <= 1.7976931348623157e308);
     mx = fmax(mx, a);
   }
-  __shared__ double red[8];
-  __shared__ int badw[8];
-  __shared__ int e_s;
+#pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     bad |= __shfl_xor_sync(0xffffffffu, int(bad), o) != 0;
   }
-  if ((threadIdx.x & 31) == 0) {
-    red[threadIdx.x >> 5] = mx;
-    badw[threadIdx.x >> 5] = bad;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double m = 0.0;
-    int b = 0;
-    for (int w = 0; w < 8; ++w) {
-      m = fmax(m, red[w]);
-      b |= badw[w];
-    }
-    e_s = b ? kBadExp : exp_for(m);
-    tau[row] = e_s;
-  }
-  __syncthreads();
-  const int e = e_s;
+  const int e = bad ? kBadExp : exp_for(mx);
+  if (lane == 0) tau[row] = e;
   uint2* out = dsl + size_t(row) * nao;
-  for (int v = threadIdx.x; v < nao; v += 256) {
-    int dg[NSL] = {0, 0, 0, 0, 0, 0, 0, 0};
-    if (e != kBadExp) digits(ldexp(d[v], e), dg);
-    out[v] = make_uint2(pack4(dg[0], dg[1], dg[2], dg[3]), pack4(dg[4], dg[5], dg[6], dg[7]));
-  }
+#pragma unroll 4
+  for (int v = lane; v < nao; v += 32)
+    out[v] = e != kBadExp ? digits_packed(d[v], e) : make_uint2(0u, 0u);
 }
 
 // ---------------------------------------------------------------------------
-// phi: point scales sigma[g], then for chunk c of (block tile bg) and digit j
-// a 64 x 32-byte K-major tile (row = point, byte = compacted AO within the
-// chunk) in the 32-byte-swizzled layout, at phisl + ((cbase[bg] + c) * 8 + j) * 2048.
+// phi, step 1: pmax[g] = max |phi[u][g]| over the active AOs u of g's block
+// (+Inf when one of them is Inf or NaN).  CTA (block tile, slab of 64
+// compacted AOs): 64 points x 4 row groups, then one atomic max per point on
+// the bit pattern (non-negative doubles order like their bits); pmax starts at 0.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
-split_phi(const double* __restrict__ ao, size_t stride_grid, const int* __restrict__ lists,
-          const int* __restrict__ counts, const int* __restrict__ cbase, int nao, int ngrid,
-          int blk, int gsub, int* __restrict__ sigma, uint8_t* __restrict__ phisl) {
-  __shared__ double red[4][TG];
-  __shared__ int e_s[TG];
-  // staged digit words [digit][quad of 4 AOs][point], rows padded to 68 words
-  // so that the read-out below is free of bank conflicts
-  __shared__ uint32_t stage[NSL][8][TG + 4];
-  const int bg = blockIdx.x;
+split_phi_max(const double* __restrict__ ao, size_t stride_grid, const int* __restrict__ lists,
+              const int* __restrict__ counts, int nao, int ngrid, int blk, int gsub,
+              unsigned long long* __restrict__ pmax) {
+  const int bg = blockIdx.x, slab = blockIdx.y;
   const int b = bg / gsub, gt = bg % gsub;
+  const int nb = counts[b];
+  const int i0 = slab * 64;
+  if (i0 >= nb) return;
   const int g0 = b * blk + gt * TG;
   const int gend = min(min((b + 1) * blk, ngrid), g0 + TG);
-  const int nb = counts[b];
   const int* I = lists + size_t(b) * nao;
   const int gr = threadIdx.x & (TG - 1), rg = threadIdx.x >> 6;
   const int g = g0 + gr;
-  const bool gok = g < gend;
-  // 1. max |phi| over the active AOs of each point (a warp reads 32 points of a row)
+  __shared__ double red[4][TG];
   double mx = 0.0;
-  if (gok) {
+  if (g < gend) {
     bool bad = false;
+    const int iend = min(nb, i0 + 64);
 #pragma unroll 4
-    for (int i = rg; i < nb; i += 4) {
+    for (int i = i0 + rg; i < iend; i += 4) {
       const double a = fabs(ao[size_t(__ldg(I + i)) * stride_grid + g]);
       bad |= !(a <= 1.7976931348623157e308);
       mx = fmax(mx, a);
     }
-    if (bad) mx = __longlong_as_double(0x7ff0000000000000LL);  // +Inf marks the point
+    if (bad) mx = __longlong_as_double(0x7ff0000000000000LL);
   }
   red[rg][gr] = mx;
   __syncthreads();
-  if (threadIdx.x < TG) {
-    const int e = exp_for(fmax(fmax(red[0][gr], red[1][gr]), fmax(red[2][gr], red[3][gr])));
-    e_s[gr] = e;
-    if (gok) sigma[g] = e;
+  if (threadIdx.x < TG && g < gend) {
+    const double m = fmax(fmax(red[0][gr], red[1][gr]), fmax(red[2][gr], red[3][gr]));
+    atomicMax(pmax + g, static_cast<unsigned long long>(__double_as_longlong(m)));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// phi, step 2: sigma[g] and, for chunk c of (block tile bg) and digit j, a
+// 64 x 32-byte K-major tile (row = point, byte = compacted AO within the
+// chunk) in the 32-byte-swizzled layout, at phisl + ((cbase[bg] + c) * 7 + j) * 2048.
+// CTA (block tile, chunk).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+split_phi_digits(const double* __restrict__ ao, size_t stride_grid, const int* __restrict__ lists,
+                 const int* __restrict__ counts, const int* __restrict__ cbase,
+                 const unsigned long long* __restrict__ pmax, int nao, int ngrid, int blk,
+                 int gsub, int* __restrict__ sigma, uint8_t* __restrict__ phisl) {
+  const int bg = blockIdx.x, c = blockIdx.y;
+  const int b = bg / gsub, gt = bg % gsub;
+  const int nb = counts[b];
+  if (c * TK >= nb) return;
+  // staged digit words [digit][quad of 4 AOs][point], rows padded to 68 words
+  // so that the read-out below is free of bank conflicts
+  __shared__ uint32_t stage[NSL][8][TG + 4];
+  const int g0 = b * blk + gt * TG;
+  const int gend = min(min((b + 1) * blk, ngrid), g0 + TG);
+  const int* I = lists + size_t(b) * nao;
+  const int gr = threadIdx.x & (TG - 1), rg = threadIdx.x >> 6;
+  const int g = g0 + gr;
+  const bool gok = g < gend;
+  const int e = gok ? exp_for(__longlong_as_double(static_cast<long long>(pmax[g]))) : 0;
+  if (c == 0 && rg == 0 && gok) sigma[g] = e;
+#pragma unroll
+  for (int hq = 0; hq < 2; ++hq) {
+    const int q = rg + 4 * hq;  // quad of 4 compacted AOs
+    uint2 w[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int i = c * TK + q * 4 + t;
+      w[t] = (gok && i < nb && e != kBadExp)
+                 ? digits_packed(ao[size_t(__ldg(I + i)) * stride_grid + g], e)
+                 : make_uint2(0u, 0u);
+    }
+    uint32_t o[8];
+    transpose4(w[0].x, w[1].x, w[2].x, w[3].x, o[0], o[1], o[2], o[3]);
+    transpose4(w[0].y, w[1].y, w[2].y, w[3].y, o[4], o[5], o[6], o[7]);
+#pragma unroll
+    for (int j = 0; j < NSL; ++j) stage[j][q][gr] = o[j];
   }
   __syncthreads();
-  const int e = e_s[gr];
-  // 2. digit tiles, one chunk of 32 compacted AOs at a time
-  const int kc = (nb + TK - 1) / TK;
-  uint8_t* base = phisl + size_t(cbase[bg]) * B_STAGE;
-  for (int c = 0; c < kc; ++c) {
-#pragma unroll
-    for (int hq = 0; hq < 2; ++hq) {
-      const int q = rg + 4 * hq;  // quad of 4 compacted AOs
-      int dg[4][NSL];
-#pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        const int i = c * TK + q * 4 + t;
-#pragma unroll
-        for (int j = 0; j < NSL; ++j) dg[t][j] = 0;
-        if (gok && i < nb && e != kBadExp)
-          digits(ldexp(ao[size_t(__ldg(I + i)) * stride_grid + g], e), dg[t]);
-      }
-#pragma unroll
-      for (int j = 0; j < NSL; ++j) stage[j][q][gr] = pack4(dg[0][j], dg[1][j], dg[2][j], dg[3][j]);
-    }
-    __syncthreads();
-    // write-out: (digit, point row, 16-byte half) vectors, consecutive threads
-    // covering consecutive rows -> coalesced 16-byte stores
-    uint8_t* tile0 = base + size_t(c) * B_STAGE;
-    for (int v = threadIdx.x; v < NSL * TG * 2; v += 256) {
-      const int h = v & 1, r = (v >> 1) & (TG - 1), j = v >> 7;
-      const uint4 w = make_uint4(stage[j][4 * h][r], stage[j][4 * h + 1][r], stage[j][4 * h + 2][r],
-                                 stage[j][4 * h + 3][r]);
-      *reinterpret_cast<uint4*>(tile0 + j * B_SLICE + tc::sw32_offset(uint32_t(r), uint32_t(h))) = w;
-    }
-    __syncthreads();
+  // write-out: (digit, point row, 16-byte half) vectors, consecutive threads
+  // covering consecutive rows -> coalesced 16-byte stores
+  uint8_t* tile0 = phisl + (size_t(cbase[bg]) + c) * B_STAGE;
+  for (int v = threadIdx.x; v < NSL * TG * 2; v += 256) {
+    const int h = v & 1, r = (v >> 1) & (TG - 1), j = v >> 7;
+    const uint4 w = make_uint4(stage[j][4 * h][r], stage[j][4 * h + 1][r], stage[j][4 * h + 2][r],
+                               stage[j][4 * h + 3][r]);
+    *reinterpret_cast<uint4*>(tile0 + j * B_SLICE + tc::sw32_offset(uint32_t(r), uint32_t(h))) = w;
   }
 }
 
@@ -314,6 +343,7 @@ __device__ __forceinline__ uint32_t gather_selector(int qd) {
   return sel;
 }
 
+template <int STAGES>
 __global__ void __launch_bounds__(THREADS, 1) split_main(MainArgs p) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
@@ -331,12 +361,12 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(MainArgs p) {
   int* err = &g_split_error;
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
-      tc::mbar_init(&full_a[s], 128);  // the four warps of one gather group
+      tc::mbar_init(&full_a[s], 4);  // one arrival per warp of a gather group
       tc::mbar_init(&full_b[s], 1);
       tc::mbar_init(&empty[s], 1);
     }
     tc::mbar_init(acc_full, 1);
-    tc::mbar_init(acc_empty, 32 * GATHER_WARPS);
+    tc::mbar_init(acc_empty, GATHER_WARPS);
     tc::mbar_init(drain, 1);
     tc::mbar_fence_init();
   }
@@ -356,11 +386,15 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(MainArgs p) {
     // of the group fills tile rows 32wq .. 32wq+31, four rows per step.
     // Lane (qd, ri, hh) = lane bits (4:3, 2:1, 0) loads, for row 4*step+ri,
     // the columns 16hh + 4k + qd (k = 0..3) and ends up holding digit planes
-    // 2qd and 2qd+1 of the 16-byte half hh of that row.
+    // 2qd and 2qd+1 of the 16-byte half hh of that row (plane 7 is the zero
+    // padding byte and is not stored).
     const int grp = warp >> 2, wq = warp & 3;
     const int qd = lane >> 3, ri = (lane >> 1) & 3, hh = lane & 1;
     const bool b1 = (qd & 2) != 0, b0 = (qd & 1) != 0;
     const uint32_t sel_a = gather_selector(qd), sel_b = sel_a + 0x1111u;
+    // 16-byte loads of phi_lhs when every row segment starts 16-byte aligned
+    const bool vec2 = (p.stride_grid % 2 == 0) && (p.blk % 2 == 0) &&
+                      (reinterpret_cast<uintptr_t>(p.ao_lhs) % 16 == 0);
     uint32_t seq0 = 0;  // CTA-wide sequence number of the item's first chunk
     uint32_t nitem = 0;
     bool ok = true;
@@ -420,11 +454,13 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(MainArgs p) {
           const uint32_t off = tc::sw32_offset(uint32_t(32 * wq + 4 * st + ri), uint32_t(hh));
           *reinterpret_cast<uint4*>(As + (2 * qd) * A_SLICE + off) =
               make_uint4(wa[0], wa[1], wa[2], wa[3]);
-          *reinterpret_cast<uint4*>(As + (2 * qd + 1) * A_SLICE + off) =
-              make_uint4(wb[0], wb[1], wb[2], wb[3]);
+          if (qd < 3)
+            *reinterpret_cast<uint4*>(As + (2 * qd + 1) * A_SLICE + off) =
+                make_uint4(wb[0], wb[1], wb[2], wb[3]);
         }
         tc::fence_proxy_async_smem();
-        tc::mbar_arrive(&full_a[stg]);
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&full_a[stg]);
       }
       seq0 += uint32_t(kc);
       if (!ok) break;
@@ -442,57 +478,63 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(MainArgs p) {
       const uint32_t trow = tmem + (uint32_t(32 * wq) << 16);
       const size_t slot = ((size_t(bg) * p.max_ut + ut) * p.nset + s) * EPI_PARTS + wq;
 #pragma unroll 1
-      for (int cc = 32 * grp; cc < 32 * grp + 32; cc += 16) {
-        uint32_t v[NSL][16];
+      for (int cc = 32 * grp; cc < 32 * grp + 32; cc += 8) {
+        double a[8];  // phi_lhs of this row at 8 points, then its products
 #pragma unroll
-        for (int L = 0; L < NSL; ++L) tc::tmem_ld_32x32b_x16(trow + uint32_t(L * TG + cc), v[L]);
-        tc::tmem_ld_wait();
-        double a[16];
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
+        for (int j = 0; j < 8; j += 2) {
           const int gl = cc + j;
-          a[j] = 0.0;
+          if (ev && gl + 1 < gw && vec2) {
+            const double2 q = *reinterpret_cast<const double2*>(lrow + gl);
+            a[j] = q.x;
+            a[j + 1] = q.y;
+          } else {
+            a[j] = (ev && gl < gw) ? lrow[gl] : 0.0;
+            a[j + 1] = (ev && gl + 1 < gw) ? lrow[gl + 1] : 0.0;
+          }
+        }
+        uint32_t v[NSL][8];
+#pragma unroll
+        for (int L = 0; L < NSL; ++L) tc::tmem_ld_32x32b_x8(trow + uint32_t(L * TG + cc), v[L]);
+        tc::tmem_ld_wait();
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int gl = cc + j;
           if (ev && gl < gw) {
             double x = double(int(v[NSL - 1][j]));
 #pragma unroll
-            for (int L = NSL - 2; L >= 0; --L) x = fma(x, 0.0078125, double(int(v[L][j])));
+            for (int L = NSL - 2; L >= 0; --L) x = fma(x, 0.00390625, double(int(v[L][j])));
             const int sg = p.sigma[g0 + gl];
             a[j] = (tu == kBadExp || sg == kBadExp) ? __longlong_as_double(0x7ff8000000000000LL)
-                                                    : ldexp(x, -(tu + sg)) * lrow[gl];
+                                                    : ldexp(x, -(tu + sg)) * a[j];
           }
         }
-        // reduce-scatter over the 32 rows: 16 shuffles leave lane pair
-        // (2m, 2m+1) with the sum of point m (fixed order: deterministic)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const bool up = (lane & 16) != 0;
-          const double keep = up ? a[j + 8] : a[j];
-          a[j] = keep + __shfl_xor_sync(0xffffffffu, up ? a[j] : a[j + 8], 16);
-        }
+        // reduce-scatter over the 32 rows: 9 shuffles leave the lanes 4m .. 4m+3
+        // with the sum of point m (fixed order: deterministic)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          const bool up = (lane & 8) != 0;
+          const bool up = (lane & 16) != 0;
           const double keep = up ? a[j + 4] : a[j];
-          a[j] = keep + __shfl_xor_sync(0xffffffffu, up ? a[j] : a[j + 4], 8);
+          a[j] = keep + __shfl_xor_sync(0xffffffffu, up ? a[j] : a[j + 4], 16);
         }
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-          const bool up = (lane & 4) != 0;
+          const bool up = (lane & 8) != 0;
           const double keep = up ? a[j + 2] : a[j];
-          a[j] = keep + __shfl_xor_sync(0xffffffffu, up ? a[j] : a[j + 2], 4);
+          a[j] = keep + __shfl_xor_sync(0xffffffffu, up ? a[j] : a[j + 2], 8);
         }
         {
-          const bool up = (lane & 2) != 0;
+          const bool up = (lane & 4) != 0;
           const double keep = up ? a[1] : a[0];
-          a[0] = keep + __shfl_xor_sync(0xffffffffu, up ? a[0] : a[1], 2);
+          a[0] = keep + __shfl_xor_sync(0xffffffffu, up ? a[0] : a[1], 4);
         }
+        a[0] += __shfl_xor_sync(0xffffffffu, a[0], 2);
         a[0] += __shfl_xor_sync(0xffffffffu, a[0], 1);
-        const int m = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 +
-                      ((lane >> 1) & 1);
-        if ((lane & 1) == 0) p.partial[slot * TG + cc + m] = a[0];
+        const int m = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+        if ((lane & 3) == 0) p.partial[slot * TG + cc + m] = a[0];
       }
       tc::fence_before_sync();
-      tc::mbar_arrive(acc_empty);  // the MMA warp may overwrite the accumulators
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(acc_empty);  // the MMA warp may overwrite the accumulators
     }
   } else if (warp == GATHER_WARPS) {
     // ---------------- MMA issuer ----------------
@@ -593,10 +635,38 @@ __global__ void split_reduce(double* __restrict__ rhos, const double* __restrict
   }
 }
 
+template <int STAGES>
+cudaError_t launch_main_t(int nsm, const MainArgs& a, cudaStream_t stream) {
+  constexpr size_t smem = size_t(STAGES) * STAGE + 1024 + 256;
+  cudaError_t err = cudaFuncSetAttribute(split_main<STAGES>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (err != cudaSuccess) return err;
+  split_main<STAGES><<<nsm, THREADS, smem, stream>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_main(int stages, int nsm, const MainArgs& a, cudaStream_t stream) {
+  switch (stages) {
+    case 2: return launch_main_t<2>(nsm, a, stream);
+    case 3: return launch_main_t<3>(nsm, a, stream);
+    case 5: return launch_main_t<5>(nsm, a, stream);
+    default: return launch_main_t<4>(nsm, a, stream);
+  }
+}
+
+int split_stages() {
+  static const int v = [] {
+    const char* e = std::getenv("CFGMM_SPLIT_STAGES");
+    const int s = e ? std::atoi(e) : kDefaultStages;
+    return (s >= 2 && s <= 5) ? s : kDefaultStages;
+  }();
+  return v;
+}
+
 size_t a256(size_t v) { return (v + 255) / 256 * 256; }
 
 struct Layout {
-  size_t lists, counts, cbase, items, total, dsl, tau, sigma, phisl, partial, bytes;
+  size_t lists, counts, cbase, items, total, dsl, tau, sigma, pmax, phisl, partial, bytes;
 };
 
 Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk) {
@@ -614,7 +684,8 @@ Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk) {
   L.dsl = L.total + 256;
   L.tau = L.dsl + a256(nset * nao * nao * 8);
   L.sigma = L.tau + a256(nset * nao * sizeof(int));
-  L.phisl = L.sigma + a256(ngrid * sizeof(int));
+  L.pmax = L.sigma + a256(ngrid * sizeof(int));
+  L.phisl = L.pmax + a256(ngrid * sizeof(unsigned long long));
   L.partial = L.phisl + a256(nbg * max_kc * B_STAGE);
   L.bytes = L.partial + nbg * max_ut * nset * EPI_PARTS * TG * sizeof(double);
   return L;
@@ -645,16 +716,23 @@ cudaError_t aodmao2rho_split(double* rhos, const double* dms, const double* ao_l
   uint2* dsl = reinterpret_cast<uint2*>(ws + L.dsl);
   int* tau = reinterpret_cast<int*>(ws + L.tau);
   int* sigma = reinterpret_cast<int*>(ws + L.sigma);
+  unsigned long long* pmax = reinterpret_cast<unsigned long long*>(ws + L.pmax);
   uint8_t* phisl = reinterpret_cast<uint8_t*>(ws + L.phisl);
   double* partial = reinterpret_cast<double*>(ws + L.partial);
 
   cudaError_t err = aodm_block_lists_launch(tab, ldtab, nao, nblk, lists, counts, stream);
   if (err != cudaSuccess) return err;
   split_build<<<1, 1024, 0, stream>>>(counts, nbg, gsub, nset, max_ut, cbase, items, total);
-  split_d_slices<<<nset * nao, 256, 0, stream>>>(dms, stride_ao, stride_ao * stride_ao, nao, dsl,
-                                                 tau);
-  split_phi<<<nbg, 256, 0, stream>>>(ao_rhs, stride_grid, lists, counts, cbase, nao, ngrid, blk,
-                                     gsub, sigma, phisl);
+  split_d_slices<<<(nset * nao + 7) / 8, 256, 0, stream>>>(dms, stride_ao, stride_ao * stride_ao, nao,
+                                                          nset * nao, dsl, tau);
+  if ((err = cudaMemsetAsync(pmax, 0, size_t(ngrid) * sizeof(unsigned long long), stream)) !=
+      cudaSuccess)
+    return err;
+  const int max_kc = (nao + TK - 1) / TK;
+  split_phi_max<<<dim3(nbg, (nao + 63) / 64), 256, 0, stream>>>(ao_rhs, stride_grid, lists, counts,
+                                                                nao, ngrid, blk, gsub, pmax);
+  split_phi_digits<<<dim3(nbg, max_kc), 256, 0, stream>>>(ao_rhs, stride_grid, lists, counts, cbase,
+                                                          pmax, nao, ngrid, blk, gsub, sigma, phisl);
   if ((err = cudaGetLastError()) != cudaSuccess) return err;
 
   MainArgs a;
@@ -676,15 +754,11 @@ cudaError_t aodmao2rho_split(double* rhos, const double* dms, const double* ao_l
   a.blk = blk;
   a.gsub = gsub;
   a.max_ut = max_ut;
-  constexpr size_t smem = size_t(STAGES) * STAGE + 1024 + 256;
-  if ((err = cudaFuncSetAttribute(split_main, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  int(smem))) != cudaSuccess)
-    return err;
   int dev = 0, nsm = 0;
   if ((err = cudaGetDevice(&dev)) != cudaSuccess) return err;
   if ((err = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
     return err;
-  split_main<<<nsm, THREADS, smem, stream>>>(a);
+  if ((err = launch_main(split_stages(), nsm, a, stream)) != cudaSuccess) return err;
   if ((err = cudaGetLastError()) != cudaSuccess) return err;
   split_reduce<<<nbg, 128, 0, stream>>>(rhos, partial, counts, stride_grid, ngrid, nset, blk, gsub,
                                         max_ut, nbg);

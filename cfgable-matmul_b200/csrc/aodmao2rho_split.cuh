@@ -10,7 +10,7 @@ namespace cfgmm {
 // D digits (8 bytes per element of D), phi digit tiles, partial sums.
 size_t aodmao2rho_split_workspace(size_t nao, size_t ngrid, size_t nset, size_t blk);
 
-// Same contract as aodmao2rho_fp64; nao <= 65535 keeps the INT32 level sums exact.
+// Same contract as aodmao2rho_fp64; nao <= 16384 keeps the INT32 level sums exact.
 cudaError_t aodmao2rho_split(double* rhos, const double* dms, const double* ao_lhs,
                              const double* ao_rhs, size_t stride_ao, size_t stride_grid, int nao,
                              int ngrid, int nset, const uint8_t* tab, size_t ldtab, int blk,
