@@ -29,6 +29,7 @@
 
 #include "../../include/cfgmm.h"
 #include "aodmao2rho_fp64.cuh"
+#include "aodmao2rho_split.cuh"
 
 namespace cfgmm {
 void set_last_error(const std::string& msg);
@@ -36,10 +37,17 @@ void set_last_error(const std::string& msg);
 
 struct cfgmm_aodm_plan {
   int dev = 0;
+  bool split = false;
   cfgmm::AodmArgs args{};
   cfgmm::AodmConfig cfg{1, 32};
+  // split precision: D digits are rebuilt every run, phi digits once here
+  cfgmm::SplitArgs sargs{};
+  const double* dms = nullptr;
+  size_t stride_ao = 0;
+  int nao = 0, nset_max = 0, stages = 0;
   int npairs = 0, nitems = 0;
   void* mem = nullptr;  // one device allocation for lists, descriptors, work list, partials
+  void* mem2 = nullptr;  // split precision: digits, scales, its work list and partials
   int2* rpairs = nullptr;
   cudaGraphExec_t exec = nullptr;
   std::string info;
@@ -111,6 +119,246 @@ void cache_store(const std::string& key, const cfgmm::AodmConfig& cfg, double ms
 
 int bucket(double v) { return v <= 0 ? 0 : int(std::floor(std::log2(v) * 2)); }  // half-octaves
 
+
+// One split-precision run: D digits, the persistent kernel, the reduction.
+int split_run(cfgmm_aodm_plan* plan, cudaStream_t s) {
+  cudaError_t err = cfgmm::split_prepare_d(plan->dms, plan->stride_ao, plan->nao, plan->nset_max,
+                                           const_cast<uint2*>(plan->sargs.dsl),
+                                           const_cast<int*>(plan->sargs.tau), s);
+  if (err == cudaSuccess) err = cfgmm::split_launch_main(plan->sargs, s, plan->stages);
+  if (err == cudaSuccess)
+    err = cfgmm::split_launch_reduce(plan->sargs, plan->rpairs, plan->npairs, s);
+  return err == cudaSuccess ? CFGMM_OK : cuda_fail(err, "split plan run");
+}
+
+// Captures `body` (launches on the given stream) into plan->exec.
+template <class F>
+cudaError_t capture(cfgmm_aodm_plan* plan, F body) {
+  cudaStream_t cs;
+  cudaError_t err = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+  if (err != cudaSuccess) return err;
+  cudaGraph_t graph = nullptr;
+  err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (err == cudaSuccess) {
+    const cudaError_t e1 = body(cs);
+    err = cudaStreamEndCapture(cs, &graph);
+    if (err == cudaSuccess) err = e1;
+  }
+  if (err == cudaSuccess) err = cudaGraphInstantiate(&plan->exec, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  cudaStreamDestroy(cs);
+  return err;
+}
+
+// The split-precision half of cfgmm_aodm_plan_create: phi digit tiles of
+// every batch are built here once; items are (tile, row tile, matrix, batch),
+// matrix-major (one D in L2 at a time), heaviest first within a matrix.
+int build_split(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, size_t nbatch,
+                const double* dms, size_t stride_ao, size_t nao, size_t nset_max, size_t blksize,
+                int flags, int* d_lists, int* d_counts, const std::vector<size_t>& list_off,
+                const std::vector<size_t>& cnt_off, const std::vector<size_t>& nblk,
+                const std::vector<int>& counts, cudaStream_t s) {
+  const int TU = cfgmm::split_row_tile(), TG = cfgmm::split_point_tile(), TK = cfgmm::split_chunk();
+  const int gsub = int((blksize + TG - 1) / TG);
+  const int max_ut = int((nao + TU - 1) / TU);
+  const int parts = cfgmm::split_epi_parts();
+  std::vector<int> cbase;
+  std::vector<size_t> cb_off(nbatch), sg_off(nbatch);
+  std::vector<cfgmm::SplitBatch> hb(nbatch);
+  std::vector<int4> items;
+  std::vector<int2> pairs;
+  size_t ngrid_max = 0, sg_n = 0;
+  long long groups = 0;
+  int chunks = 0;
+  for (size_t i = 0; i < nbatch; ++i) {
+    const cfgmm_aodm_batch& b = batches[i];
+    ngrid_max = std::max(ngrid_max, size_t(b.ngrid));
+    cb_off[i] = cbase.size();
+    sg_off[i] = sg_n;
+    sg_n += (b.ngrid + 63) / 64 * 64;
+    for (size_t blk = 0; blk < nblk[i]; ++blk) {
+      const int nb = counts[cnt_off[i] + blk];
+      for (int gt = 0; gt < gsub; ++gt) {
+        cbase.push_back(chunks);
+        chunks += (nb + TK - 1) / TK;
+        if (nb > 0) pairs.push_back(make_int2(int(i), int(blk) * gsub + gt));
+      }
+    }
+    hb[i].partial_off = groups;
+    groups += (long long)(nblk[i] * gsub) * max_ut * (long long)b.nset * parts;
+  }
+  for (size_t sidx = 0; sidx < nset_max; ++sidx) {
+    const size_t first = items.size();
+    for (size_t i = 0; i < nbatch; ++i) {
+      if (batches[i].nset <= sidx) continue;
+      for (size_t blk = 0; blk < nblk[i]; ++blk) {
+        const int nb = counts[cnt_off[i] + blk];
+        for (int gt = 0; gt < gsub; ++gt)
+          for (int u = 0; u * TU < nb; ++u)
+            items.push_back(make_int4(int(blk) * gsub + gt, u, int(sidx), int(i)));
+      }
+    }
+    // heaviest first: chunks of the tile's block
+    std::stable_sort(items.begin() + first, items.end(), [&](const int4& x, const int4& y) {
+      return counts[cnt_off[x.w] + x.x / gsub] > counts[cnt_off[y.w] + y.x / gsub];
+    });
+  }
+  plan->nitems = int(items.size());
+  plan->npairs = int(pairs.size());
+
+  // ---- device memory ----
+  const size_t o_cbase = 0;
+  const size_t o_sigma = o_cbase + a256(std::max<size_t>(cbase.size(), 1) * sizeof(int));
+  const size_t o_pmax = o_sigma + a256(std::max<size_t>(sg_n, 1) * sizeof(int));
+  const size_t o_dsl = o_pmax + a256(ngrid_max * sizeof(unsigned long long));
+  const size_t o_tau = o_dsl + a256(nset_max * nao * nao * 8);
+  const size_t o_batch = o_tau + a256(nset_max * nao * sizeof(int));
+  const size_t o_items = o_batch + a256(nbatch * sizeof(cfgmm::SplitBatch));
+  const size_t o_total = o_items + a256(std::max<size_t>(items.size(), 1) * sizeof(int4));
+  const size_t o_pairs = o_total + 256;
+  const size_t o_phisl = o_pairs + a256(std::max<size_t>(pairs.size(), 1) * sizeof(int2));
+  const size_t o_part = o_phisl + a256(size_t(chunks) * cfgmm::split_chunk_bytes());
+  const size_t bytes = o_part + size_t(groups) * TG * sizeof(double);
+  cudaError_t err = cudaMalloc(&plan->mem2, bytes);
+  if (err != cudaSuccess) return cuda_fail(err, "cudaMalloc(split plan)");
+  char* base = static_cast<char*>(plan->mem2);
+  int* d_cbase = reinterpret_cast<int*>(base + o_cbase);
+  int* d_sigma = reinterpret_cast<int*>(base + o_sigma);
+  auto* d_pmax = reinterpret_cast<unsigned long long*>(base + o_pmax);
+  uint8_t* d_phisl = reinterpret_cast<uint8_t*>(base + o_phisl);
+  for (size_t i = 0; i < nbatch; ++i) {
+    const cfgmm_aodm_batch& b = batches[i];
+    hb[i].ao_lhs = b.ao_lhs;
+    hb[i].rhos = b.rhos;
+    hb[i].lists = d_lists + list_off[i];
+    hb[i].counts = d_counts + cnt_off[i];
+    hb[i].cbase = d_cbase + cb_off[i];
+    hb[i].sigma = d_sigma + sg_off[i];
+    hb[i].stride_grid = b.stride_grid;
+    hb[i].ngrid = int(b.ngrid);
+    hb[i].nset = int(b.nset);
+  }
+  const int total[2] = {int(items.size()), int(items.size())};
+  err = cudaMemcpyAsync(d_cbase, cbase.data(), cbase.size() * sizeof(int), cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(base + o_batch, hb.data(), nbatch * sizeof(cfgmm::SplitBatch),
+                          cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess && !items.empty())
+    err = cudaMemcpyAsync(base + o_items, items.data(), items.size() * sizeof(int4),
+                          cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(base + o_total, total, sizeof(total), cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess && !pairs.empty())
+    err = cudaMemcpyAsync(base + o_pairs, pairs.data(), pairs.size() * sizeof(int2),
+                          cudaMemcpyHostToDevice, s);
+  // phi digit tiles of every batch, once
+  for (size_t i = 0; i < nbatch && err == cudaSuccess; ++i)
+    err = cfgmm::split_prepare_phi(batches[i].ao_rhs, batches[i].stride_grid, hb[i].lists,
+                                   hb[i].counts, hb[i].cbase, int(nao), int(batches[i].ngrid),
+                                   int(blksize), d_pmax, const_cast<int*>(hb[i].sigma), d_phisl, s);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(s);  // host vectors die on return
+  if (err != cudaSuccess) return cuda_fail(err, "split plan setup");
+
+  plan->split = true;
+  plan->dms = dms;
+  plan->stride_ao = stride_ao;
+  plan->nao = int(nao);
+  plan->nset_max = int(nset_max);
+  plan->rpairs = reinterpret_cast<int2*>(base + o_pairs);
+  cfgmm::SplitArgs& a = plan->sargs;
+  a.dsl = reinterpret_cast<const uint2*>(base + o_dsl);
+  a.tau = reinterpret_cast<const int*>(base + o_tau);
+  a.phisl = d_phisl;
+  a.batches = reinterpret_cast<const cfgmm::SplitBatch*>(base + o_batch);
+  a.items = reinterpret_cast<const int4*>(base + o_items);
+  a.total = reinterpret_cast<const int*>(base + o_total);
+  a.partial = reinterpret_cast<double*>(base + o_part);
+  a.nao = int(nao);
+  a.blk = int(blksize);
+  a.gsub = gsub;
+  a.max_ut = max_ut;
+
+  // ---- autotuning: pipeline depth of the persistent kernel ----
+  std::string tune = "default";
+  char key[256];
+  double work = 0.0;
+  for (size_t i = 0; i < nbatch; ++i)
+    for (size_t blk = 0; blk < nblk[i]; ++blk) {
+      const double nb = counts[cnt_off[i] + blk];
+      work += double(batches[i].nset) * nb * nb;
+    }
+  std::snprintf(key, sizeof(key), "aodm_split:nao%d:work%d:items%d:nset%zu:blk%zu",
+                bucket(double(nao)), bucket(work), bucket(double(plan->nitems)), nset_max, blksize);
+  if (!(flags & CFGMM_PLAN_NO_TUNE) && plan->nitems > 0) {
+    cfgmm::AodmConfig c{};
+    if (cache_lookup(key, &c)) {
+      plan->stages = c.ns;
+      tune = "cache";
+    } else {
+      if ((err = cfgmm::split_prepare_d(dms, stride_ao, int(nao), int(nset_max),
+                                        const_cast<uint2*>(a.dsl), const_cast<int*>(a.tau), s)) !=
+          cudaSuccess)
+        return cuda_fail(err, "autotune");
+      cudaEvent_t e0, e1;
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      double best_ms = 1e30;
+      std::string trials;
+      for (int st : {2, 3, 4}) {
+        float best = 1e30f;
+        for (int rep = 0; rep < 3 && err == cudaSuccess; ++rep) {
+          err = cudaEventRecord(e0, s);
+          if (err == cudaSuccess) err = cfgmm::split_launch_main(a, s, st);
+          if (err == cudaSuccess) err = cudaEventRecord(e1, s);
+          if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+          float t = 0.f;
+          if (err == cudaSuccess) cudaEventElapsedTime(&t, e0, e1);
+          if (rep > 0) best = std::min(best, t);
+        }
+        if (err != cudaSuccess) break;
+        char buf[96];
+        std::snprintf(buf, sizeof(buf), "%s{\"stages\":%d,\"ms\":%.4f}", trials.empty() ? "" : ",",
+                      st, best);
+        trials += buf;
+        if (best < best_ms) {
+          best_ms = best;
+          plan->stages = st;
+        }
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      if (err != cudaSuccess) return cuda_fail(err, "autotune");
+      cache_store(key, cfgmm::AodmConfig{plan->stages, 0}, best_ms);
+      tune = "[" + trials + "]";
+    }
+  }
+
+  // ---- capture the run ----
+  if (!(flags & CFGMM_PLAN_NO_GRAPH)) {
+    // launch once outside the capture so kernel attributes are set
+    if ((err = cfgmm::split_launch_main(a, s, plan->stages)) == cudaSuccess)
+      err = cudaStreamSynchronize(s);
+    if (err == cudaSuccess)
+      err = capture(plan, [&](cudaStream_t cs) {
+        cudaError_t e = cfgmm::split_prepare_d(dms, stride_ao, int(nao), int(nset_max),
+                                               const_cast<uint2*>(a.dsl), const_cast<int*>(a.tau), cs);
+        if (e == cudaSuccess) e = cfgmm::split_launch_main(a, cs, plan->stages);
+        if (e == cudaSuccess) e = cfgmm::split_launch_reduce(a, plan->rpairs, plan->npairs, cs);
+        return e;
+      });
+    if (err != cudaSuccess) return cuda_fail(err, "graph capture");
+  }
+  char buf[512];
+  std::snprintf(buf, sizeof(buf),
+                "{\"precision\":\"split\",\"batches\":%zu,\"items\":%d,\"block_tiles\":%d,"
+                "\"phi_chunks\":%d,\"config\":{\"stages\":%d},\"graph\":%s,\"tuning\":",
+                nbatch, plan->nitems, plan->npairs, chunks, plan->stages,
+                plan->exec ? "true" : "false");
+  plan->info = std::string(buf) + (tune[0] == '[' ? tune : "\"" + tune + "\"") + ",\"key\":\"" +
+               key + "\"}";
+  return CFGMM_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -121,8 +369,10 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
   cfgmm::set_last_error("");
   if (!out) return fail(CFGMM_ERR_INVALID_ARGUMENT, "null plan pointer");
   *out = nullptr;
-  if (precision != CFGMM_PREC_FP64)
-    return fail(CFGMM_ERR_UNIMPLEMENTED, "batched plans run in FP64");
+  if (precision != CFGMM_PREC_FP64 && precision != CFGMM_PREC_OZAKI_INT8)
+    return fail(CFGMM_ERR_INVALID_ARGUMENT, "unknown precision " + std::to_string(precision));
+  if (precision == CFGMM_PREC_OZAKI_INT8 && nao > 16384)
+    return fail(CFGMM_ERR_UNIMPLEMENTED, "split-precision AO-DM-AO supports nao <= 16384");
   if (!batches || nbatch == 0 || !dms || nao == 0 || nset_max == 0 || blksize == 0)
     return fail(CFGMM_ERR_INVALID_ARGUMENT, "empty plan or null pointer");
   if (nao > 1000000 || nset_max > 1024 || blksize > 1000000 || nbatch > 1000000)
@@ -144,6 +394,7 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
   plan->dev = dev;
   auto cleanup = [&](int rc) {
     if (plan->mem) cudaFree(plan->mem);
+    if (plan->mem2) cudaFree(plan->mem2);
     delete plan;
     return rc;
   };
@@ -169,7 +420,10 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
   const size_t o_pairs = o_items + a256(slots * sizeof(int4));
   const size_t o_ctr = o_pairs + a256(cnt_n * gsub * sizeof(int2));
   const size_t o_part = o_ctr + a256((nset_max + 1) * sizeof(int));
-  const size_t bytes = o_part + slots * nset_max * TG * sizeof(double);
+  // split precision keeps only the active lists here (its own layout follows)
+  const size_t bytes = precision == CFGMM_PREC_OZAKI_INT8
+                           ? o_batch
+                           : o_part + slots * nset_max * TG * sizeof(double);
   cudaError_t err = cudaMalloc(&plan->mem, bytes);
   if (err != cudaSuccess) return cleanup(cuda_fail(err, "cudaMalloc(plan)"));
   char* base = static_cast<char*>(plan->mem);
@@ -186,6 +440,14 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
   err = cudaMemcpyAsync(counts.data(), d_counts, cnt_n * sizeof(int), cudaMemcpyDeviceToHost, s);
   if (err == cudaSuccess) err = cudaStreamSynchronize(s);
   if (err != cudaSuccess) return cleanup(cuda_fail(err, "active list counts"));
+
+  if (precision == CFGMM_PREC_OZAKI_INT8) {
+    const int rc = build_split(plan, batches, nbatch, dms, stride_ao, nao, nset_max, blksize, flags,
+                               d_lists, d_counts, list_off, cnt_off, nblk, counts, s);
+    if (rc != CFGMM_OK) return cleanup(rc);
+    *out = plan;
+    return CFGMM_OK;
+  }
 
   // ---- 2. descriptors and the global work list, heaviest first ----
   std::vector<cfgmm::AodmBatch> hb(nbatch);
@@ -325,7 +587,7 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
   }
   char buf[512];
   std::snprintf(buf, sizeof(buf),
-                "{\"batches\":%zu,\"items\":%d,\"block_tiles\":%d,\"config\":{\"ns\":%d,\"tk\":%d},"
+                "{\"precision\":\"fp64\",\"batches\":%zu,\"items\":%d,\"block_tiles\":%d,\"config\":{\"ns\":%d,\"tk\":%d},"
                 "\"graph\":%s,\"tuning\":",
                 nbatch, plan->nitems, plan->npairs, plan->cfg.ns, plan->cfg.tk,
                 plan->exec ? "true" : "false");
@@ -343,6 +605,10 @@ int cfgmm_aodm_plan_run(cfgmm_aodm_plan* plan, void* stream) {
     PLAN_CUDA(cudaGraphLaunch(plan->exec, s));
     return CFGMM_OK;
   }
+  if (plan->split) {
+    const int rc = split_run(plan, s);
+    return rc;
+  }
   PLAN_CUDA(cfgmm::aodm_launch_reset(plan->args.counters, plan->args.ngroups, s));
   PLAN_CUDA(cfgmm::aodm_launch_main(plan->args, plan->cfg, s));
   PLAN_CUDA(cfgmm::aodm_launch_reduce(plan->args, plan->rpairs, plan->npairs, s));
@@ -357,6 +623,7 @@ int cfgmm_aodm_plan_destroy(cfgmm_aodm_plan* plan) {
   if (!plan) return CFGMM_OK;
   if (plan->exec) cudaGraphExecDestroy(plan->exec);
   if (plan->mem) cudaFree(plan->mem);
+  if (plan->mem2) cudaFree(plan->mem2);
   delete plan;
   return CFGMM_OK;
 }

@@ -253,7 +253,7 @@ split_phi_digits(const double* __restrict__ ao, size_t stride_grid, const int* _
 }
 
 // ---------------------------------------------------------------------------
-// work list: cbase[bg] (prefix of chunk counts), items (bg, utile, s), total
+// work list: cbase[bg] (prefix of chunk counts), items (bg, utile, -1, 0), total
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024)
 split_build(const int* __restrict__ counts, int nbg, int gsub, int nset, int max_ut,
@@ -292,7 +292,7 @@ split_build(const int* __restrict__ counts, int nbg, int gsub, int nset, int max
     bi += ii - nut;
     if (bg < nbg) {
       cbase[bg] = bc;
-      for (int u = 0; u < nut; ++u) items[bi + u] = make_int4(bg, u, 0, 0);
+      for (int u = 0; u < nut; ++u) items[bi + u] = make_int4(bg, u, -1, 0);
     }
     __syncthreads();
     if (tid == 0) {
@@ -313,21 +313,19 @@ split_build(const int* __restrict__ counts, int nbg, int gsub, int nset, int max
 // ---------------------------------------------------------------------------
 // main kernel
 // ---------------------------------------------------------------------------
-struct MainArgs {
-  const uint2* dsl;
-  const int* tau;
-  const uint8_t* phisl;
-  const int* sigma;
-  const double* ao_lhs;
-  const int* lists;
-  const int* counts;
-  const int* cbase;
-  const int4* items;
-  const int* total;  // [0] items x sets, [1] items per set
-  double* partial;   // [((bg * max_ut + ut) * nset + s) * EPI_PARTS + quarter][TG]
-  size_t stride_grid;
-  int nao, ngrid, nset, blk, gsub, max_ut;
-};
+
+// Work item t: (64-point tile bg, 128-row tile ut, density matrix s, batch).
+// Items with s < 0 come from a list of per_set tiles run once per matrix.
+__device__ __forceinline__ int4 item_at(const SplitArgs& p, int t, int per_set) {
+  if (p.items[0].z >= 0) return p.items[t];
+  int4 it = p.items[t % per_set];
+  it.z = t / per_set;
+  return it;
+}
+
+__device__ __forceinline__ const SplitBatch& batch_of(const SplitArgs& p, int w) {
+  return p.batches ? p.batches[w] : p.one;
+}
 
 // Byte selector that assembles, from `keep` (bytes 0..3) and `recv` (4..7) of
 // the gather's second shuffle round, the digit word of 4 consecutive columns:
@@ -344,7 +342,7 @@ __device__ __forceinline__ uint32_t gather_selector(int qd) {
 }
 
 template <int STAGES>
-__global__ void __launch_bounds__(THREADS, 1) split_main(MainArgs p) {
+__global__ void __launch_bounds__(THREADS, 1) split_main(SplitArgs p) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                              ~uintptr_t(1023));
@@ -393,19 +391,17 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(MainArgs p) {
     const bool b1 = (qd & 2) != 0, b0 = (qd & 1) != 0;
     const uint32_t sel_a = gather_selector(qd), sel_b = sel_a + 0x1111u;
     // 16-byte loads of phi_lhs when every row segment starts 16-byte aligned
-    const bool vec2 = (p.stride_grid % 2 == 0) && (p.blk % 2 == 0) &&
-                      (reinterpret_cast<uintptr_t>(p.ao_lhs) % 16 == 0);
     uint32_t seq0 = 0;  // CTA-wide sequence number of the item's first chunk
     uint32_t nitem = 0;
     bool ok = true;
     for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++nitem) {
-      const int s = t / per_set;
-      const int4 it = p.items[t % per_set];
-      const int bg = it.x, ut = it.y;
+      const int4 it = item_at(p, t, per_set);
+      const int bg = it.x, ut = it.y, s = it.z;
+      const SplitBatch& B = batch_of(p, it.w);
       const int b = bg / p.gsub, gt = bg % p.gsub;
-      const int nb = p.counts[b];
+      const int nb = B.counts[b];
       const int kc = (nb + TK - 1) / TK;
-      const int* I = p.lists + size_t(b) * p.nao;
+      const int* I = B.lists + size_t(b) * p.nao;
       const uint2* dset = p.dsl + size_t(s) * p.nao * p.nao;
       int iu[8];
 #pragma unroll
@@ -469,14 +465,18 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(MainArgs p) {
       if (!tc::mbar_wait(acc_full, nitem & 1, err, 12)) break;
       tc::fence_after_sync();
       const int g0 = b * p.blk + gt * TG;
-      const int gw = min(min((b + 1) * p.blk, p.ngrid), g0 + TG) - g0;
+      const int gw = min(min((b + 1) * p.blk, B.ngrid), g0 + TG) - g0;
+      // 16-byte loads of phi_lhs when every row segment starts 16-byte aligned
+      const bool vec2 = (B.stride_grid % 2 == 0) && (p.blk % 2 == 0) &&
+                        (reinterpret_cast<uintptr_t>(B.ao_lhs) % 16 == 0);
       const int erow = ut * TU + 32 * wq + lane;
       const bool ev = erow < nb;
       const int eu = ev ? __ldg(I + erow) : 0;
       const int tu = p.tau[size_t(s) * p.nao + eu];
-      const double* lrow = p.ao_lhs + size_t(eu) * p.stride_grid + g0;
+      const double* lrow = B.ao_lhs + size_t(eu) * B.stride_grid + g0;
       const uint32_t trow = tmem + (uint32_t(32 * wq) << 16);
-      const size_t slot = ((size_t(bg) * p.max_ut + ut) * p.nset + s) * EPI_PARTS + wq;
+      const size_t slot =
+          size_t(B.partial_off) + ((size_t(bg) * p.max_ut + ut) * B.nset + s) * EPI_PARTS + wq;
 #pragma unroll 1
       for (int cc = 32 * grp; cc < 32 * grp + 32; cc += 8) {
         double a[8];  // phi_lhs of this row at 8 points, then its products
@@ -503,7 +503,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(MainArgs p) {
             double x = double(int(v[NSL - 1][j]));
 #pragma unroll
             for (int L = NSL - 2; L >= 0; --L) x = fma(x, 0.00390625, double(int(v[L][j])));
-            const int sg = p.sigma[g0 + gl];
+            const int sg = B.sigma[g0 + gl];
             a[j] = (tu == kBadExp || sg == kBadExp) ? __longlong_as_double(0x7ff8000000000000LL)
                                                     : ldexp(x, -(tu + sg)) * a[j];
           }
@@ -543,8 +543,8 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(MainArgs p) {
       uint32_t seq = 0, nitem = 0;
       bool ok = true;
       for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++nitem) {
-        const int4 it = p.items[t % per_set];
-        const int nb = p.counts[it.x / p.gsub];
+        const int4 it = item_at(p, t, per_set);
+        const int nb = batch_of(p, it.w).counts[it.x / p.gsub];
         const int kc = (nb + TK - 1) / TK;
         if (nitem > 0 && !tc::mbar_wait(acc_empty, (nitem - 1) & 1, err, 13)) break;
         tc::fence_after_sync();
@@ -579,10 +579,11 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(MainArgs p) {
       uint32_t seq = 0;
       bool ok = true;
       for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
-        const int4 it = p.items[t % per_set];
-        const int nb = p.counts[it.x / p.gsub];
+        const int4 it = item_at(p, t, per_set);
+        const SplitBatch& B = batch_of(p, it.w);
+        const int nb = B.counts[it.x / p.gsub];
         const int kc = (nb + TK - 1) / TK;
-        const uint8_t* src = p.phisl + size_t(p.cbase[it.x]) * B_STAGE;
+        const uint8_t* src = p.phisl + size_t(B.cbase[it.x]) * B_STAGE;
         for (int c = 0; c < kc; ++c, ++seq) {
           const int stg = int(seq % STAGES);
           const uint32_t use = seq / STAGES;
@@ -612,31 +613,33 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(MainArgs p) {
 // ---------------------------------------------------------------------------
 // deterministic reduction of the (row tile, row quarter) partials into rho
 // ---------------------------------------------------------------------------
-__global__ void split_reduce(double* __restrict__ rhos, const double* __restrict__ partial,
-                             const int* __restrict__ counts, size_t stride_grid, int ngrid,
-                             int nset, int blk, int gsub, int max_ut, int nbg) {
-  const int bg = blockIdx.x;
-  if (bg >= nbg) return;
-  const int b = bg / gsub, gt = bg % gsub;
-  const int nt = (counts[b] + TU - 1) / TU;
+__global__ void split_reduce(SplitArgs p, const int2* __restrict__ pairs, int npairs) {
+  const int pi = blockIdx.x;
+  if (pi >= npairs) return;
+  const int2 pr = pairs ? pairs[pi] : make_int2(0, pi);  // (batch, 64-point tile)
+  const SplitBatch& B = batch_of(p, pr.x);
+  const int bg = pr.y;
+  const int b = bg / p.gsub, gt = bg % p.gsub;
+  const int nt = (B.counts[b] + TU - 1) / TU;
   if (nt == 0) return;  // fully masked block: rho untouched
-  const int g0 = b * blk + gt * TG;
-  const int gend = min(min((b + 1) * blk, ngrid), g0 + TG);
-  for (int t = threadIdx.x; t < nset * TG; t += blockDim.x) {
+  const int g0 = b * p.blk + gt * TG;
+  const int gend = min(min((b + 1) * p.blk, B.ngrid), g0 + TG);
+  for (int t = threadIdx.x; t < B.nset * TG; t += blockDim.x) {
     const int s = t / TG, j = t % TG;
     if (g0 + j >= gend) continue;
     double v = 0.0;
     for (int u = 0; u < nt; ++u) {
-      const double* q = partial + ((size_t(bg) * max_ut + u) * nset + s) * EPI_PARTS * TG + j;
+      const double* q = p.partial + (size_t(B.partial_off) +
+                                     ((size_t(bg) * p.max_ut + u) * B.nset + s) * EPI_PARTS) * TG + j;
       for (int w = 0; w < EPI_PARTS; ++w) v += q[w * TG];
     }
-    double* r = rhos + size_t(s) * stride_grid + g0 + j;
+    double* r = B.rhos + size_t(s) * B.stride_grid + g0 + j;
     *r = v + *r;
   }
 }
 
 template <int STAGES>
-cudaError_t launch_main_t(int nsm, const MainArgs& a, cudaStream_t stream) {
+cudaError_t launch_main_t(int nsm, const SplitArgs& a, cudaStream_t stream) {
   constexpr size_t smem = size_t(STAGES) * STAGE + 1024 + 256;
   cudaError_t err = cudaFuncSetAttribute(split_main<STAGES>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
@@ -645,7 +648,7 @@ cudaError_t launch_main_t(int nsm, const MainArgs& a, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_main(int stages, int nsm, const MainArgs& a, cudaStream_t stream) {
+cudaError_t launch_main(int stages, int nsm, const SplitArgs& a, cudaStream_t stream) {
   switch (stages) {
     case 2: return launch_main_t<2>(nsm, a, stream);
     case 3: return launch_main_t<3>(nsm, a, stream);
@@ -723,47 +726,70 @@ cudaError_t aodmao2rho_split(double* rhos, const double* dms, const double* ao_l
   cudaError_t err = aodm_block_lists_launch(tab, ldtab, nao, nblk, lists, counts, stream);
   if (err != cudaSuccess) return err;
   split_build<<<1, 1024, 0, stream>>>(counts, nbg, gsub, nset, max_ut, cbase, items, total);
-  split_d_slices<<<(nset * nao + 7) / 8, 256, 0, stream>>>(dms, stride_ao, stride_ao * stride_ao, nao,
-                                                          nset * nao, dsl, tau);
-  if ((err = cudaMemsetAsync(pmax, 0, size_t(ngrid) * sizeof(unsigned long long), stream)) !=
-      cudaSuccess)
+  if ((err = split_prepare_d(dms, stride_ao, nao, nset, dsl, tau, stream)) != cudaSuccess) return err;
+  if ((err = split_prepare_phi(ao_rhs, stride_grid, lists, counts, cbase, nao, ngrid, blk, pmax,
+                               sigma, phisl, stream)) != cudaSuccess)
     return err;
-  const int max_kc = (nao + TK - 1) / TK;
-  split_phi_max<<<dim3(nbg, (nao + 63) / 64), 256, 0, stream>>>(ao_rhs, stride_grid, lists, counts,
-                                                                nao, ngrid, blk, gsub, pmax);
-  split_phi_digits<<<dim3(nbg, max_kc), 256, 0, stream>>>(ao_rhs, stride_grid, lists, counts, cbase,
-                                                          pmax, nao, ngrid, blk, gsub, sigma, phisl);
-  if ((err = cudaGetLastError()) != cudaSuccess) return err;
 
-  MainArgs a;
+  SplitArgs a{};
   a.dsl = dsl;
   a.tau = tau;
   a.phisl = phisl;
-  a.sigma = sigma;
-  a.ao_lhs = ao_lhs;
-  a.lists = lists;
-  a.counts = counts;
-  a.cbase = cbase;
+  a.batches = nullptr;
+  a.one = SplitBatch{ao_lhs, rhos, lists, counts, cbase, sigma, stride_grid, ngrid, nset, 0};
   a.items = items;
   a.total = total;
   a.partial = partial;
-  a.stride_grid = stride_grid;
   a.nao = nao;
-  a.ngrid = ngrid;
-  a.nset = nset;
   a.blk = blk;
   a.gsub = gsub;
   a.max_ut = max_ut;
-  int dev = 0, nsm = 0;
-  if ((err = cudaGetDevice(&dev)) != cudaSuccess) return err;
-  if ((err = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
-    return err;
-  if ((err = launch_main(split_stages(), nsm, a, stream)) != cudaSuccess) return err;
-  if ((err = cudaGetLastError()) != cudaSuccess) return err;
-  split_reduce<<<nbg, 128, 0, stream>>>(rhos, partial, counts, stride_grid, ngrid, nset, blk, gsub,
-                                        max_ut, nbg);
+  if ((err = split_launch_main(a, stream)) != cudaSuccess) return err;
+  return split_launch_reduce(a, nullptr, nbg, stream);
+}
+
+cudaError_t split_prepare_d(const double* dms, size_t stride_ao, int nao, int nset, uint2* dsl,
+                            int* tau, cudaStream_t stream) {
+  split_d_slices<<<(nset * nao + 7) / 8, 256, 0, stream>>>(dms, stride_ao, stride_ao * stride_ao,
+                                                           nao, nset * nao, dsl, tau);
   return cudaGetLastError();
 }
+
+cudaError_t split_prepare_phi(const double* ao_rhs, size_t stride_grid, const int* lists,
+                              const int* counts, const int* cbase, int nao, int ngrid, int blk,
+                              unsigned long long* pmax, int* sigma, uint8_t* phisl,
+                              cudaStream_t stream) {
+  const int nbg = ((ngrid + blk - 1) / blk) * ((blk + TG - 1) / TG);
+  const int gsub = (blk + TG - 1) / TG;
+  cudaError_t err = cudaMemsetAsync(pmax, 0, size_t(ngrid) * sizeof(unsigned long long), stream);
+  if (err != cudaSuccess) return err;
+  split_phi_max<<<dim3(nbg, (nao + 63) / 64), 256, 0, stream>>>(ao_rhs, stride_grid, lists, counts,
+                                                                nao, ngrid, blk, gsub, pmax);
+  split_phi_digits<<<dim3(nbg, (nao + TK - 1) / TK), 256, 0, stream>>>(
+      ao_rhs, stride_grid, lists, counts, cbase, pmax, nao, ngrid, blk, gsub, sigma, phisl);
+  return cudaGetLastError();
+}
+
+cudaError_t split_launch_main(const SplitArgs& a, cudaStream_t stream, int stages) {
+  int dev = 0, nsm = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err == cudaSuccess) err = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (err != cudaSuccess) return err;
+  return launch_main(stages > 0 ? stages : split_stages(), nsm, a, stream);
+}
+
+cudaError_t split_launch_reduce(const SplitArgs& a, const int2* pairs, int npairs,
+                                cudaStream_t stream) {
+  if (npairs <= 0) return cudaSuccess;
+  split_reduce<<<npairs, 128, 0, stream>>>(a, pairs, npairs);
+  return cudaGetLastError();
+}
+
+int split_row_tile() { return TU; }
+int split_point_tile() { return TG; }
+int split_chunk() { return TK; }
+size_t split_chunk_bytes() { return B_STAGE; }
+int split_epi_parts() { return EPI_PARTS; }
 
 cudaError_t aodmao2rho_split_reset_error(cudaStream_t stream) {
   static const int zero = 0;

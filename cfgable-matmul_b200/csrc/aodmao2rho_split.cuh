@@ -6,6 +6,33 @@
 
 namespace cfgmm {
 
+// One grid batch of the split contraction (device pointers).
+struct SplitBatch {
+  const double* ao_lhs;
+  double* rhos;             // (nset, stride_grid)
+  const int* lists;         // [nblk][nao] active AOs per block
+  const int* counts;        // [nblk]
+  const int* cbase;         // [nbg] first phi digit chunk of each 64-point tile
+  const int* sigma;         // [ngrid] point scales
+  size_t stride_grid;
+  int ngrid;
+  int nset;                 // density matrices used by this batch
+  long long partial_off;    // first partial-sum group of this batch
+};
+
+// Arguments of the persistent kernel and the reduction.
+struct SplitArgs {
+  const uint2* dsl;         // D digits [s][u][v], 8 bytes each
+  const int* tau;           // row scales [s][u]
+  const uint8_t* phisl;     // phi digit tiles of every batch
+  const SplitBatch* batches;  // device array, or null: `one`
+  SplitBatch one;
+  const int4* items;        // (tile, row tile, s, batch); s < 0: per-matrix list
+  const int* total;         // [0] items to run, [1] tiles per matrix (s < 0 lists)
+  double* partial;          // [group][64]
+  int nao, blk, gsub, max_ut;
+};
+
 // Device scratch (bytes) of the split contraction: active lists, work list,
 // D digits (8 bytes per element of D), phi digit tiles, partial sums.
 size_t aodmao2rho_split_workspace(size_t nao, size_t ngrid, size_t nset, size_t blk);
@@ -15,6 +42,28 @@ cudaError_t aodmao2rho_split(double* rhos, const double* dms, const double* ao_l
                              const double* ao_rhs, size_t stride_ao, size_t stride_grid, int nao,
                              int ngrid, int nset, const uint8_t* tab, size_t ldtab, int blk,
                              void* workspace, cudaStream_t stream);
+
+// Pieces of a batched run (the plan keeps phi digits across runs):
+//   split_prepare_d   D digits and row scales of nset matrices;
+//   split_prepare_phi point scales and phi digit tiles of one batch (pmax:
+//                     ngrid 8-byte scratch; cbase: device chunk offsets);
+//   split_launch_main / split_launch_reduce  the contraction and its reduction
+//                     over (batch, 64-point tile) pairs.
+cudaError_t split_prepare_d(const double* dms, size_t stride_ao, int nao, int nset, uint2* dsl,
+                            int* tau, cudaStream_t stream);
+cudaError_t split_prepare_phi(const double* ao_rhs, size_t stride_grid, const int* lists,
+                              const int* counts, const int* cbase, int nao, int ngrid, int blk,
+                              unsigned long long* pmax, int* sigma, uint8_t* phisl,
+                              cudaStream_t stream);
+// stages: pipeline depth 2..5, 0 = default (CFGMM_SPLIT_STAGES or 3)
+cudaError_t split_launch_main(const SplitArgs& a, cudaStream_t stream, int stages = 0);
+cudaError_t split_launch_reduce(const SplitArgs& a, const int2* pairs, int npairs,
+                                cudaStream_t stream);
+int split_row_tile();      // rows per work item (128)
+int split_point_tile();    // points per work item (64)
+int split_chunk();         // compacted AOs per chunk (32)
+size_t split_chunk_bytes();  // bytes of one chunk's phi digit tiles
+int split_epi_parts();     // partial-sum groups per (tile, row tile, matrix)
 
 // Sticky per-device error word of the split kernel's bounded waits.
 cudaError_t aodmao2rho_split_reset_error(cudaStream_t stream);

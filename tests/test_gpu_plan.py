@@ -45,11 +45,12 @@ def _device(torch, bs, dms):
     return dev, t(dms)
 
 
-def _single(cm, torch, b, dms, blk):
+def _single(cm, torch, b, dms, blk, precision=0):
     nao, ngrid = b["lhs"].shape
     rho = b["rho0"].copy()
     cm.aodmao2rho_ex(rho, np.ascontiguousarray(dms[: b["nset"]]), b["lhs"], b["rhs"],
-                     (nao, ngrid), (nao, ngrid), b["nset"], b["tab"], b["tab"].shape[1], blk)
+                     (nao, ngrid), (nao, ngrid), b["nset"], b["tab"], b["tab"].shape[1], blk,
+                     precision)
     return rho
 
 
@@ -129,12 +130,45 @@ def test_autotune_cache(cm, wl, tmp_path, monkeypatch):
     p2.close()
 
 
+@pytest.mark.parametrize("graph,tune", [(True, True), (False, False)])
+def test_split_plan_equals_single_split_calls(cm, wl, tmp_path, monkeypatch, graph, tune):
+    """The split plan keeps phi digits from creation and rebuilds D digits per
+    run; its arithmetic is the single call's, so results match bit for bit,
+    and stay within 1e-12 of FP64."""
+    import torch
+    monkeypatch.setenv("CFGMM_AUTOTUNE_CACHE", str(tmp_path / "tune.txt"))
+    bs, dms = _batches(wl, torch, 11, 17)
+    dev, ddms = _device(torch, bs, dms)
+    plan = cm.AodmPlan(dev, ddms, blksize=64, precision=cm.PREC_OZAKI_INT8, graph=graph, tune=tune)
+    info = plan.info()
+    assert info["precision"] == "split" and info["graph"] is graph
+    if tune:
+        assert [t["stages"] for t in info["tuning"]] == [2, 3, 4]
+    plan.run()
+    torch.cuda.synchronize()
+    for b, d in zip(bs, dev):
+        got = d[0].cpu().numpy()
+        assert np.array_equal(got, _single(cm, torch, b, dms, 64, cm.PREC_OZAKI_INT8))
+        assert normwise(got, _single(cm, torch, b, dms, 64)) < 1e-12
+    # an SCF step: new D contents, rho zeroed, run again through the same graph
+    dms2 = dms + 1e-3 * (dms + dms.transpose(0, 2, 1))
+    ddms.copy_(torch.from_numpy(dms2))
+    for d in dev:
+        d[0].zero_()
+    plan.run()
+    torch.cuda.synchronize()
+    for b, d in zip(bs, dev):
+        b2 = dict(b, rho0=np.zeros_like(b["rho0"]))
+        assert normwise(d[0].cpu().numpy(), _single(cm, torch, b2, dms2, 64)) < 1e-12
+    plan.close()
+
+
 def test_plan_rejections(cm, wl):
     import torch
     bs, dms = _batches(wl, torch, 4, 2, nset_max=2)
     dev, ddms = _device(torch, bs, dms)
-    with pytest.raises(NotImplementedError):
-        cm.AodmPlan(dev, ddms, precision=cm.PREC_OZAKI_INT8)
+    with pytest.raises(ValueError):
+        cm.AodmPlan(dev, ddms, precision=7)
     bad = [(d[0], d[1], d[2], d[3], 3) for d in dev]  # nset above nset_max
     with pytest.raises(ValueError):
         cm.AodmPlan(bad, ddms)
