@@ -34,7 +34,7 @@ import numpy as np
 __all__ = [
     "MatmulLoops", "matmul_anyway_full", "aodmao2rho_anyway", "matmul_ex", "aodmao2rho_ex",
     "matmul_anyway_full_non0tab", "matmul_non0tab_ex",
-    "aodmao2rho_noalloc", "AodmPlan", "eval_ao", "mask_ao",
+    "aodmao2rho_noalloc", "AodmPlan", "eval_ao", "mask_ao", "Server",
     "PREC_FP64", "PREC_OZAKI_INT8", "CfgmmError", "lib", "library_path",
 ]
 
@@ -56,6 +56,12 @@ class _Batch(ctypes.Structure):
                 ("ao_rhs", ctypes.c_void_p), ("tab", ctypes.c_void_p),
                 ("stride_grid", ctypes.c_size_t), ("ngrid", ctypes.c_size_t),
                 ("ldtab", ctypes.c_size_t), ("nset", ctypes.c_size_t)]
+
+
+class RequestStats(ctypes.Structure):
+    """struct cfgmm_request_stats"""
+    _fields_ = [("queue_ms", ctypes.c_double), ("device_ms", ctypes.c_double),
+                ("total_ms", ctypes.c_double)]
 
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -132,6 +138,24 @@ def lib() -> ctypes.CDLL:
         L.cfgmm_eval_ao_dev.restype = I
         L.cfgmm_mask_ao_dev.argtypes = [P, S, S, P, P, S, P, ctypes.c_double, P, S, S, P]
         L.cfgmm_mask_ao_dev.restype = I
+        U64 = ctypes.c_uint64
+        L.cfgmm_server_create.argtypes = [ctypes.POINTER(P), S, I, I, S]
+        L.cfgmm_server_create.restype = I
+        L.cfgmm_server_destroy.argtypes = [P]
+        L.cfgmm_server_destroy.restype = I
+        L.cfgmm_server_open.argtypes = [P, P, P, P, S, S, S, S, I, ctypes.POINTER(U64)]
+        L.cfgmm_server_open.restype = I
+        L.cfgmm_server_open_shells.argtypes = [P, P, S, P, P, P, P, S, ctypes.c_double, S,
+                                               ctypes.POINTER(U64)]
+        L.cfgmm_server_open_shells.restype = I
+        L.cfgmm_server_close.argtypes = [P, U64]
+        L.cfgmm_server_close.restype = I
+        L.cfgmm_server_submit.argtypes = [P, U64, P, S, P, ctypes.POINTER(U64)]
+        L.cfgmm_server_submit.restype = I
+        L.cfgmm_server_wait.argtypes = [P, U64, ctypes.c_double, ctypes.POINTER(RequestStats)]
+        L.cfgmm_server_wait.restype = I
+        L.cfgmm_server_stats.argtypes = [P]
+        L.cfgmm_server_stats.restype = ctypes.c_char_p
         _lib = L
     return _lib
 
@@ -360,6 +384,94 @@ def mask_ao(ao, ngrid, shell_l, shell_row, shell_block_max, threshold, tab, blks
         _dev(ao, "torch.float64"), ao.shape[1], ngrid, _dev(shell_l, "torch.int32"),
         _dev(shell_row, "torch.int32"), shell_l.shape[0], _dev(shell_block_max, "torch.float64"),
         float(threshold), _dev(tab, "torch.uint8"), tab.shape[1], blksize, _stream_ptr()))
+
+
+class Server:
+    """Density requests from many molecules with continuous batching under an
+    HBM budget (cfgmm_server_*).  No counterpart in the reference.
+
+    ``open(ao, tab, nset_max)`` takes numpy arrays (uploaded on admission;
+    keep them alive until ``close``) or CUDA tensors (used in place);
+    ``open_shells(points, shell_xyz, shell_l, shell_alpha, shell_norm,
+    density, nset_max)`` evaluates phi and the mask on the device.
+    ``submit(mol, dms, rho)`` returns a ticket at once (dms copied, rho
+    written on completion); ``wait(ticket)`` returns the request's
+    (queue_ms, device_ms, total_ms)."""
+
+    def __init__(self, hbm_budget, nslots=4, precision=PREC_FP64, blksize=64):
+        h = ctypes.c_void_p()
+        _raise(lib().cfgmm_server_create(ctypes.byref(h), int(hbm_budget), nslots, precision,
+                                         blksize))
+        self._h = h
+        self._keep = {}
+        self.blksize = blksize
+
+    def open(self, ao_lhs, tab, nset_max, ao_rhs=None):
+        tab = _as_tab(tab)
+        nao, ngrid = ao_lhs.shape
+        mol = ctypes.c_uint64()
+        if _is_torch(ao_lhs):
+            ptrs = (_dev(ao_lhs, "torch.float64"),
+                    None if ao_rhs is None else _dev(ao_rhs, "torch.float64"),
+                    _dev(tab, "torch.uint8"))
+            dev = 1
+        else:
+            ptrs = (_host(ao_lhs, np.float64)[0],
+                    None if ao_rhs is None else _host(ao_rhs, np.float64)[0],
+                    _host(tab, np.uint8)[0])
+            dev = 0
+        _raise(lib().cfgmm_server_open(self._h, ptrs[0], ptrs[1], ptrs[2], nao, ngrid,
+                                       tab.shape[1], nset_max, dev, ctypes.byref(mol)))
+        self._keep[mol.value] = (ao_lhs, ao_rhs, tab)
+        return mol.value
+
+    def open_shells(self, points, shell_xyz, shell_l, shell_alpha, shell_norm, density,
+                    nset_max):
+        arrs = [np.ascontiguousarray(points, np.float64), np.ascontiguousarray(shell_xyz, np.float64),
+                np.ascontiguousarray(shell_l, np.int32), np.ascontiguousarray(shell_alpha, np.float64),
+                np.ascontiguousarray(shell_norm, np.float64)]
+        mol = ctypes.c_uint64()
+        _raise(lib().cfgmm_server_open_shells(self._h, arrs[0].ctypes.data, len(arrs[0]),
+                                              arrs[1].ctypes.data, arrs[2].ctypes.data,
+                                              arrs[3].ctypes.data, arrs[4].ctypes.data,
+                                              len(arrs[2]), float(density), nset_max,
+                                              ctypes.byref(mol)))
+        return mol.value
+
+    def close(self, mol) -> None:
+        _raise(lib().cfgmm_server_close(self._h, mol))
+        self._keep.pop(mol, None)
+
+    def submit(self, mol, dms, rho) -> int:
+        pd, _ = _host(dms, np.float64)
+        pr, _ = _host(rho, np.float64, True)
+        t = ctypes.c_uint64()
+        _raise(lib().cfgmm_server_submit(self._h, mol, pd, dms.shape[0], pr, ctypes.byref(t)))
+        self._keep[("rho", t.value)] = rho
+        return t.value
+
+    def wait(self, ticket, timeout=-1.0):
+        st = RequestStats()
+        rc = lib().cfgmm_server_wait(self._h, ticket, float(timeout), ctypes.byref(st))
+        if rc != ERR_TIMEOUT:  # a timed-out request still owns its rho buffer
+            self._keep.pop(("rho", ticket), None)
+        _raise(rc)
+        return st.queue_ms, st.device_ms, st.total_ms
+
+    def stats(self) -> dict:
+        import json
+        return json.loads(lib().cfgmm_server_stats(self._h).decode())
+
+    def shutdown(self) -> None:
+        if getattr(self, "_h", None):
+            lib().cfgmm_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.shutdown()
+        except Exception:
+            pass
 
 
 class MatmulLoops:

@@ -219,7 +219,7 @@ int build_split(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, size_t n
   const size_t o_phisl = o_pairs + a256(std::max<size_t>(pairs.size(), 1) * sizeof(int2));
   const size_t o_part = o_phisl + a256(size_t(chunks) * cfgmm::split_chunk_bytes());
   const size_t bytes = o_part + size_t(groups) * TG * sizeof(double);
-  cudaError_t err = cudaMalloc(&plan->mem2, bytes);
+  cudaError_t err = cudaMallocAsync(&plan->mem2, bytes, s);
   if (err != cudaSuccess) return cuda_fail(err, "cudaMalloc(split plan)");
   char* base = static_cast<char*>(plan->mem2);
   int* d_cbase = reinterpret_cast<int*>(base + o_cbase);
@@ -424,7 +424,7 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
   const size_t bytes = precision == CFGMM_PREC_OZAKI_INT8
                            ? o_batch
                            : o_part + slots * nset_max * TG * sizeof(double);
-  cudaError_t err = cudaMalloc(&plan->mem, bytes);
+  cudaError_t err = cudaMallocAsync(&plan->mem, bytes, s);
   if (err != cudaSuccess) return cleanup(cuda_fail(err, "cudaMalloc(plan)"));
   char* base = static_cast<char*>(plan->mem);
   int* d_lists = reinterpret_cast<int*>(base + o_lists);
@@ -622,6 +622,7 @@ const char* cfgmm_aodm_plan_info(const cfgmm_aodm_plan* plan) {
 int cfgmm_aodm_plan_destroy(cfgmm_aodm_plan* plan) {
   if (!plan) return CFGMM_OK;
   if (plan->exec) cudaGraphExecDestroy(plan->exec);
+  // cudaFree waits for work still using the memory
   if (plan->mem) cudaFree(plan->mem);
   if (plan->mem2) cudaFree(plan->mem2);
   delete plan;
@@ -629,3 +630,18 @@ int cfgmm_aodm_plan_destroy(cfgmm_aodm_plan* plan) {
 }
 
 }  // extern "C"
+
+namespace cfgmm {
+
+// For owners that know the plan is idle (no run in flight): the memory goes
+// back to the stream-ordered pool on `stream` without a device-wide wait.
+int aodm_plan_release_idle(cfgmm_aodm_plan* plan, cudaStream_t stream) {
+  if (!plan) return CFGMM_OK;
+  if (plan->exec) cudaGraphExecDestroy(plan->exec);
+  if (plan->mem) cudaFreeAsync(plan->mem, stream);
+  if (plan->mem2) cudaFreeAsync(plan->mem2, stream);
+  delete plan;
+  return CFGMM_OK;
+}
+
+}  // namespace cfgmm

@@ -275,6 +275,65 @@ int cfgmm_mask_ao_dev(double* ao, size_t stride_grid, size_t ngrid, const int* s
  * and reused across calls until process exit). */
 int cfgmm_release_workspace(void);
 
+/* ---- serving: density requests from many molecules, continuous batching ----
+ * No counterpart in the reference (a library of blocking calls).  A server
+ * owns a worker thread and `nslots` CUDA streams on the current device.
+ * Molecules are opened once; their phi, mask, D and rho buffers and batched
+ * plan stay on the device while they have work, within `hbm_budget` bytes
+ * (the server's own buffers plus an upper bound of each plan; a device
+ * molecule's caller-owned phi and mask are counted too).  Requests are taken
+ * in arrival order as slots and memory free up; idle molecules are evicted,
+ * least recently used first, to admit others (their host or shell data is
+ * uploaded or evaluated again on their next request).  Requests of one
+ * molecule run in submission order; requests of different molecules overlap.
+ * A result does not depend on the other requests in flight.
+ * All calls are thread-safe. */
+typedef struct cfgmm_server cfgmm_server;
+
+typedef struct cfgmm_request_stats {
+  double queue_ms;   /* submit -> start on the GPU */
+  double device_ms;  /* the contraction on the GPU (CUDA events) */
+  double total_ms;   /* submit -> rho in the caller's buffer */
+} cfgmm_request_stats;
+
+int cfgmm_server_create(cfgmm_server** server, size_t hbm_budget, int nslots, int precision,
+                        size_t blksize);
+/* Finishes every submitted request, then frees everything. */
+int cfgmm_server_destroy(cfgmm_server* server);
+
+/* A molecule from phi (nao, ngrid) and mask (nao, ldtab), row-major, stride
+ * ngrid.  on_device = 0: host arrays, read on each admission (keep them until
+ * close); 1: the caller's device arrays, used in place.  ao_rhs NULL = ao_lhs.
+ * Fails with CFGMM_ERR_OUT_OF_MEMORY when one molecule exceeds the budget. */
+int cfgmm_server_open(cfgmm_server* server, const double* ao_lhs, const double* ao_rhs,
+                      const uint8_t* tab, size_t nao, size_t ngrid, size_t ldtab,
+                      size_t nset_max, int on_device, uint64_t* molecule);
+/* A molecule from Gaussian shells on a grid (host arrays, copied): phi as
+ * cfgmm_eval_ao_dev computes it (AO rows in shell order), and the mask keeping
+ * the `density` fraction (0 < density <= 1) of (shell, block) tiles with the
+ * largest max |phi|, phi zeroed outside it.  Evaluated on the device on
+ * admission; phi never crosses PCIe. */
+int cfgmm_server_open_shells(cfgmm_server* server, const double* points, size_t ngrid,
+                             const double* shell_xyz, const int* shell_l,
+                             const double* shell_alpha, const double* shell_norm, size_t nshell,
+                             double density, size_t nset_max, uint64_t* molecule);
+/* No more requests for the molecule; its memory is freed once they finish. */
+int cfgmm_server_close(cfgmm_server* server, uint64_t molecule);
+
+/* rhos (nset, ngrid), host = the contraction of the molecule's phi with dms
+ * (nset, nao, nao), host, nset <= nset_max (rhos is overwritten, not
+ * accumulated into).  dms is copied before the call returns; rhos must stay
+ * valid until the ticket is waited for.  Every ticket must be waited for. */
+int cfgmm_server_submit(cfgmm_server* server, uint64_t molecule, const double* dms, size_t nset,
+                        double* rhos, uint64_t* ticket);
+/* Waits for a request (timeout_s < 0: no limit; CFGMM_ERR_TIMEOUT leaves the
+ * ticket valid) and returns its status; stats may be NULL. */
+int cfgmm_server_wait(cfgmm_server* server, uint64_t ticket, double timeout_s,
+                      cfgmm_request_stats* stats);
+/* JSON: completed/failed counts, molecules resident, evictions, budget, used
+ * and peak bytes, and p50/p99 latency (total, queue, device) in ms. */
+const char* cfgmm_server_stats(cfgmm_server* server);
+
 #ifdef __cplusplus
 }
 #endif

@@ -142,3 +142,6 @@ def test_no_cpu_fallback_without_device(cm):
     with pytest.raises(cm.CfgmmError):
         cm.aodmao2rho_anyway(rho, dms, ao, ao, (10, 100), (10, 100), 2, tab, nblk)
     assert np.all(c == 0) and np.all(rho == 0)
+    with pytest.raises(cm.CfgmmError) as e:
+        cm.Server(1 << 30)
+    assert e.value.status == -4
