@@ -276,6 +276,131 @@ class Timed:
         return [self.ev[s][i0].elapsed_time(self.ev[s][i1]) for s in range(steps)]
 
 
+def batched_section(args, cm, wl, stream):
+    """Uneven grid batches of one molecule in one graph-captured persistent
+    launch (a plan), FP64 and split precision: 2228 AOs, 256 batches with
+    ngrid log-uniform in [128, 4096], tile density U[0.05, 0.6], 1-3 DMs."""
+    import torch
+    bp = wl.batched_uneven(cm, seed=0)
+    nset_max = bp.dms.shape[0]
+    res = {"workload": f"nao={bp.mol.nao}, {len(bp.batches)} batches, "
+                       f"{bp.points()} points, ngrid log-uniform [128, 4096], "
+                       "density U[0.05, 0.6], 1-3 DMs per batch, blocks of 64"}
+    rhos = {}
+    for name, prec in (("fp64", cm.PREC_FP64), ("split", cm.PREC_OZAKI_INT8)):
+        outs = [torch.zeros(nset_max, ao.shape[1], dtype=torch.float64, device=ao.device)
+                for ao, *_ in bp.batches]
+        batches = [(o, ao, ao, tab, nset) for o, (ao, tab, ngrid, nset, dens) in
+                   zip(outs, bp.batches)]
+        t0 = time.perf_counter()
+        plan = cm.AodmPlan(batches, bp.dms, blksize=bp.blksize, precision=prec)
+        torch.cuda.synchronize()
+        create_s = time.perf_counter() - t0
+        info = plan.info()
+        for _ in range(args.warmup):
+            plan.run()
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(stream)
+        for _ in range(args.steps):
+            plan.run()
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        ms = ev[0].elapsed_time(ev[1]) / args.steps
+        for o in outs:
+            o.zero_()
+        plan.run()
+        torch.cuda.synchronize()
+        rhos[name] = [o.clone() for o in outs]
+        res[name] = {"value": info["flops"] / (ms * 1e-3) / 1e9, "unit": "GFLOP/s",
+                     "ms_per_run": ms, "flops_per_run": info["flops"],
+                     "plan_create_s": create_s, "config": info["config"],
+                     "tuning": info["tuning"], "graph": info["graph"], "items": info["items"]}
+        plan.close()
+    num = max(float((a - b).abs().max()) for a, b in zip(rhos["split"], rhos["fp64"]))
+    den = max(float(b.abs().max()) for b in rhos["fp64"])
+    res["split"]["error_vs_fp64"] = num / den
+    res["speedup_split_vs_fp64"] = res["fp64"]["ms_per_run"] / res["split"]["ms_per_run"]
+    del bp, rhos
+    torch.cuda.empty_cache()
+    return res
+
+
+def serving_section(args, cm, wl):
+    """Density requests through the server (cfgmm_server_*): molecules with
+    nao log-uniform in [300, 4000] and ngrid log-uniform in [8192, 65536] (the
+    geometric generator: Gaussian shells on atom centres, grid points around
+    centres, (shell, block) tiles at density 0.3, phi evaluated on the device),
+    each issuing 10 SCF-like requests D_{t+1} = D_t + 1e-3 sym noise after the
+    previous result, under a fixed HBM budget.  An untimed pass fills the
+    autotune cache; then a Poisson stream of molecule arrivals gives p50/p99
+    of submit -> result latency, and a saturated run (every molecule at t = 0)
+    the aggregate GFLOP/s."""
+    import threading
+    rng = np.random.default_rng(2024)
+    mols = []
+    for i in range(args.serve_molecules):
+        nao = int(np.exp(rng.uniform(np.log(300), np.log(4000))))
+        nshell = max(2, int(round(nao / 5.57)))
+        if (nao - nshell) % 2:
+            nshell += 1
+        natom = max(1, int(round(nao / 20.25)))
+        ngrid = int(np.exp(rng.uniform(np.log(8192), np.log(65536))))
+        mol = wl.molecule(100 + i, nao=nao, nshell=nshell, natom=natom)
+        pts = wl.grid_points(np.random.default_rng(200 + i), mol, ngrid, 64)
+        nset = int(rng.integers(1, 4))
+        d0 = wl.sym_dms(np.random.default_rng(300 + i), nset, nao)
+        noise = 1e-3 * wl.sym_dms(np.random.default_rng(400 + i), nset, nao)
+        mols.append((mol, pts, nset, d0, noise))
+    gaps = rng.exponential(args.serve_gap_ms * 1e-3, len(mols))
+    poisson = np.cumsum(gaps) - gaps[0]
+    budget = int(args.serve_budget_gb * (1 << 30))
+
+    def one_pass(precision, arrivals):
+        srv = cm.Server(budget, nslots=4, precision=precision)
+        t_start = time.perf_counter()
+
+        def client(k):
+            mol, pts, nset, d0, noise = mols[k]
+            time.sleep(max(0.0, t_start + arrivals[k] - time.perf_counter()))
+            mid = srv.open_shells(pts, mol.shell_xyz, mol.shell_l, mol.alpha, mol.norm, 0.3, nset)
+            rho = np.zeros((nset, len(pts)))
+            d = d0.copy()
+            for step in range(10):
+                srv.wait(srv.submit(mid, d, rho), 600.0)
+                d += noise
+            srv.close(mid)
+
+        th = [threading.Thread(target=client, args=(k,)) for k in range(len(mols))]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        wall = time.perf_counter() - t_start
+        st = srv.stats()
+        srv.shutdown()
+        return {"value": st["flops_completed"] / wall / 1e9, "unit": "GFLOP/s",
+                "requests": st["completed"], "failed": st["failed"], "wall_s": wall,
+                "latency_ms": st["latency_ms"], "warm_latency_ms": st["warm_latency_ms"],
+                "molecule_load_ms": st["load_ms"], "plan_build_ms": st["plan_ms"],
+                "queue_ms": st["queue_ms"], "device_ms": st["device_ms"],
+                "peak_bytes": st["peak_bytes"], "evictions": st["evictions"],
+                "admitted_molecules": st["admitted_molecules"]}
+
+    res = {"workload": f"{len(mols)} molecules x 10 SCF-like requests, nao log-uniform "
+                       "[300, 4000], ngrid log-uniform [8192, 65536], density 0.3, 1-3 DMs, "
+                       "phi evaluated on the device",
+           "budget_gb": args.serve_budget_gb, "slots": 4,
+           "molecules": [[m[0].nao, len(m[1]), m[2]] for m in mols],
+           "latency": f"Poisson arrivals, mean gap {args.serve_gap_ms} ms",
+           "throughput": "every molecule arrives at t = 0 (saturated)"}
+    zero = np.zeros(len(mols))
+    for name, prec in (("fp64", cm.PREC_FP64), ("split", cm.PREC_OZAKI_INT8)):
+        one_pass(prec, zero)  # fills the autotune cache
+        res[name] = {"latency": one_pass(prec, poisson), "throughput": one_pass(prec, zero)}
+    return res
+
+
 def run_ours(args, ranks: Ranks):
     import torch
     cm = importlib.import_module("cfgable-matmul_b200")
@@ -418,9 +543,14 @@ def run_ours(args, ranks: Ranks):
                      "launches_per_step": 4},
             "split": {"value": ranks.world * aflops * args.steps / (stot * 1e-3) / 1e9,
                       "unit": "GFLOP/s", "ms_per_step": stot / args.steps,
-                      "error_vs_fp64": aodm_err, "scheme": "8-digit slices, 36 INT8 products",
-                      "launches_per_step": 7},
+                      "error_vs_fp64": aodm_err, "scheme": "7 base-256 digit slices, "
+                                                           "28 INT8 products",
+                      "launches_per_step": 8},
             "speedup_split_vs_fp64": atot / stot}
+    del ao, dms, tab, rho, r64, rsp
+    torch.cuda.empty_cache()
+    batched = batched_section(args, cm, wl, stream) if not args.no_batched else None
+    serving = serving_section(args, cm, wl) if not args.no_serving else None
 
     cpu = cpu_dgemm_sample() if (ranks.rank == 0 and ranks.world == 1 and not args.no_cpu) else None
     value = ranks.world * flops * args.steps / (split_ms * 1e-3) / 1e12
@@ -465,6 +595,10 @@ def run_ours(args, ranks: Ranks):
         "clocks": clk,
         "aodmao2rho": aodm,
     }
+    if batched:
+        out["aodmao2rho_batched"] = batched
+    if serving:
+        out["serving"] = serving
     if cpu:
         out["cpu_baseline"] = cpu
     if ranks.rank == 0:
@@ -520,6 +654,11 @@ def main():
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--k", type=int, default=4096)
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-plan section")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving section")
+    ap.add_argument("--serve-molecules", type=int, default=24)
+    ap.add_argument("--serve-gap-ms", type=float, default=40.0)
+    ap.add_argument("--serve-budget-gb", type=float, default=40.0)
     args = ap.parse_args()
     if args.profile:
         run_profile_case(args)

@@ -61,7 +61,7 @@ class _Batch(ctypes.Structure):
 class RequestStats(ctypes.Structure):
     """struct cfgmm_request_stats"""
     _fields_ = [("queue_ms", ctypes.c_double), ("device_ms", ctypes.c_double),
-                ("total_ms", ctypes.c_double)]
+                ("total_ms", ctypes.c_double), ("flops", ctypes.c_double)]
 
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -396,7 +396,7 @@ class Server:
     density, nset_max)`` evaluates phi and the mask on the device.
     ``submit(mol, dms, rho)`` returns a ticket at once (dms copied, rho
     written on completion); ``wait(ticket)`` returns the request's
-    (queue_ms, device_ms, total_ms)."""
+    (queue_ms, device_ms, total_ms, flops)."""
 
     def __init__(self, hbm_budget, nslots=4, precision=PREC_FP64, blksize=64):
         h = ctypes.c_void_p()
@@ -456,7 +456,7 @@ class Server:
         if rc != ERR_TIMEOUT:  # a timed-out request still owns its rho buffer
             self._keep.pop(("rho", ticket), None)
         _raise(rc)
-        return st.queue_ms, st.device_ms, st.total_ms
+        return st.queue_ms, st.device_ms, st.total_ms, st.flops
 
     def stats(self) -> dict:
         import json

@@ -46,6 +46,7 @@ struct cfgmm_aodm_plan {
   size_t stride_ao = 0;
   int nao = 0, nset_max = 0, stages = 0;
   int npairs = 0, nitems = 0;
+  double flops = 0.0;   // sum_batches sum_s sum_b (2|I_b|^2 + 2|I_b|)|b| per run
   void* mem = nullptr;  // one device allocation for lists, descriptors, work list, partials
   void* mem2 = nullptr;  // split precision: digits, scales, its work list and partials
   int2* rpairs = nullptr;
@@ -335,9 +336,8 @@ int build_split(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, size_t n
 
   // ---- capture the run ----
   if (!(flags & CFGMM_PLAN_NO_GRAPH)) {
-    // launch once outside the capture so kernel attributes are set
-    if ((err = cfgmm::split_launch_main(a, s, plan->stages)) == cudaSuccess)
-      err = cudaStreamSynchronize(s);
+    // kernel attributes are set outside the capture
+    err = cfgmm::split_launch_main(a, s, plan->stages, true);
     if (err == cudaSuccess)
       err = capture(plan, [&](cudaStream_t cs) {
         cudaError_t e = cfgmm::split_prepare_d(dms, stride_ao, int(nao), int(nset_max),
@@ -351,8 +351,9 @@ int build_split(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, size_t n
   char buf[512];
   std::snprintf(buf, sizeof(buf),
                 "{\"precision\":\"split\",\"batches\":%zu,\"items\":%d,\"block_tiles\":%d,"
-                "\"phi_chunks\":%d,\"config\":{\"stages\":%d},\"graph\":%s,\"tuning\":",
-                nbatch, plan->nitems, plan->npairs, chunks, plan->stages,
+                "\"phi_chunks\":%d,\"flops\":%.6e,\"config\":{\"stages\":%d},\"graph\":%s,"
+                "\"tuning\":",
+                nbatch, plan->nitems, plan->npairs, chunks, plan->flops, plan->stages,
                 plan->exec ? "true" : "false");
   plan->info = std::string(buf) + (tune[0] == '[' ? tune : "\"" + tune + "\"") + ",\"key\":\"" +
                key + "\"}";
@@ -441,6 +442,12 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
   if (err == cudaSuccess) err = cudaStreamSynchronize(s);
   if (err != cudaSuccess) return cleanup(cuda_fail(err, "active list counts"));
 
+  for (size_t i = 0; i < nbatch; ++i)
+    for (size_t blk = 0; blk < nblk[i]; ++blk) {
+      const double nb = counts[cnt_off[i] + blk];
+      const double w = double(std::min(blksize, batches[i].ngrid - blk * blksize));
+      plan->flops += double(batches[i].nset) * (2.0 * nb * nb + 2.0 * nb) * w;
+    }
   if (precision == CFGMM_PREC_OZAKI_INT8) {
     const int rc = build_split(plan, batches, nbatch, dms, stride_ao, nao, nset_max, blksize, flags,
                                d_lists, d_counts, list_off, cnt_off, nblk, counts, s);
@@ -568,9 +575,8 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
     cudaStream_t cs;
     if ((err = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)) != cudaSuccess)
       return cleanup(cuda_fail(err, "capture stream"));
-    // launch once outside the capture so kernel attributes are set
-    err = cfgmm::aodm_launch_main(a, plan->cfg, cs);
-    if (err == cudaSuccess) err = cudaStreamSynchronize(cs);
+    // kernel attributes are set outside the capture
+    err = cfgmm::aodm_launch_main(a, plan->cfg, cs, true);
     cudaGraph_t graph = nullptr;
     if (err == cudaSuccess) err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
     if (err == cudaSuccess) {
@@ -587,9 +593,9 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
   }
   char buf[512];
   std::snprintf(buf, sizeof(buf),
-                "{\"precision\":\"fp64\",\"batches\":%zu,\"items\":%d,\"block_tiles\":%d,\"config\":{\"ns\":%d,\"tk\":%d},"
-                "\"graph\":%s,\"tuning\":",
-                nbatch, plan->nitems, plan->npairs, plan->cfg.ns, plan->cfg.tk,
+                "{\"precision\":\"fp64\",\"batches\":%zu,\"items\":%d,\"block_tiles\":%d,"
+                "\"flops\":%.6e,\"config\":{\"ns\":%d,\"tk\":%d},\"graph\":%s,\"tuning\":",
+                nbatch, plan->nitems, plan->npairs, plan->flops, plan->cfg.ns, plan->cfg.tk,
                 plan->exec ? "true" : "false");
   plan->info = std::string(buf) + (tune[0] == '[' ? tune : "\"" + tune + "\"") + ",\"key\":\"" +
                key + "\"}";
@@ -643,5 +649,7 @@ int aodm_plan_release_idle(cfgmm_aodm_plan* plan, cudaStream_t stream) {
   delete plan;
   return CFGMM_OK;
 }
+
+double aodm_plan_flops(const cfgmm_aodm_plan* plan) { return plan ? plan->flops : 0.0; }
 
 }  // namespace cfgmm

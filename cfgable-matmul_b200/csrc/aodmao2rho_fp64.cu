@@ -346,14 +346,14 @@ __global__ void aodm_reset_counters(int* counters, int ngroups) {
 }
 
 template <int NS, int TKT>
-cudaError_t launch_main_t(const AodmArgs& a, cudaStream_t stream) {
+cudaError_t launch_main_t(const AodmArgs& a, cudaStream_t stream, bool attrs_only) {
   constexpr size_t smem = size_t(STAGES) * (NS * TU * TKT + TG * TKT) * sizeof(double) +
                           size_t(LIST_CAP) * sizeof(int);
   static_assert(NS * 2 * TG <= STAGES * (NS * TU * TKT + TG * TKT), "reduction buffer fits");
   static_assert(smem <= 227 * 1024, "shared memory budget");
   cudaError_t err = cudaFuncSetAttribute(aodm_fp64_kernel<NS, TKT>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  if (err != cudaSuccess) return err;
+  if (err != cudaSuccess || attrs_only) return err;
   int dev = 0, nsm = 0;
   if ((err = cudaGetDevice(&dev)) != cudaSuccess) return err;
   if ((err = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
@@ -372,15 +372,16 @@ AodmConfig aodm_default_config(int nset) {
   return AodmConfig{nset >= 3 ? 3 : nset, 32};
 }
 
-cudaError_t aodm_launch_main(const AodmArgs& a, const AodmConfig& cfg, cudaStream_t stream) {
+cudaError_t aodm_launch_main(const AodmArgs& a, const AodmConfig& cfg, cudaStream_t stream,
+                             bool attrs_only) {
   if (cfg.tk == 32) {
-    if (cfg.ns == 1) return launch_main_t<1, 32>(a, stream);
-    if (cfg.ns == 2) return launch_main_t<2, 32>(a, stream);
-    if (cfg.ns == 3) return launch_main_t<3, 32>(a, stream);
+    if (cfg.ns == 1) return launch_main_t<1, 32>(a, stream, attrs_only);
+    if (cfg.ns == 2) return launch_main_t<2, 32>(a, stream, attrs_only);
+    if (cfg.ns == 3) return launch_main_t<3, 32>(a, stream, attrs_only);
   } else if (cfg.tk == 16) {
-    if (cfg.ns == 1) return launch_main_t<1, 16>(a, stream);
-    if (cfg.ns == 2) return launch_main_t<2, 16>(a, stream);
-    if (cfg.ns == 3) return launch_main_t<3, 16>(a, stream);
+    if (cfg.ns == 1) return launch_main_t<1, 16>(a, stream, attrs_only);
+    if (cfg.ns == 2) return launch_main_t<2, 16>(a, stream, attrs_only);
+    if (cfg.ns == 3) return launch_main_t<3, 16>(a, stream, attrs_only);
   }
   return cudaErrorInvalidValue;
 }

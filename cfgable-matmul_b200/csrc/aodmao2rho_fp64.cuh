@@ -67,7 +67,9 @@ cudaError_t aodm_block_lists_launch(const uint8_t* tab, size_t ldtab, int nao, i
 // Pieces of a batched run: counter reset, the persistent kernel, and the
 // reduction over (batch, block tile) pairs (rpairs null: batch 0, bg = index).
 cudaError_t aodm_launch_reset(int* counters, int ngroups, cudaStream_t stream);
-cudaError_t aodm_launch_main(const AodmArgs& a, const AodmConfig& cfg, cudaStream_t stream);
+// attrs_only: set the kernel's attributes (before a stream capture), no launch
+cudaError_t aodm_launch_main(const AodmArgs& a, const AodmConfig& cfg, cudaStream_t stream,
+                             bool attrs_only = false);
 cudaError_t aodm_launch_reduce(const AodmArgs& a, const int2* rpairs, int npairs,
                                cudaStream_t stream);
 

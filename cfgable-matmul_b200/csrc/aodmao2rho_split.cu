@@ -639,21 +639,22 @@ __global__ void split_reduce(SplitArgs p, const int2* __restrict__ pairs, int np
 }
 
 template <int STAGES>
-cudaError_t launch_main_t(int nsm, const SplitArgs& a, cudaStream_t stream) {
+cudaError_t launch_main_t(int nsm, const SplitArgs& a, cudaStream_t stream, bool attrs_only) {
   constexpr size_t smem = size_t(STAGES) * STAGE + 1024 + 256;
   cudaError_t err = cudaFuncSetAttribute(split_main<STAGES>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  if (err != cudaSuccess) return err;
+  if (err != cudaSuccess || attrs_only) return err;
   split_main<STAGES><<<nsm, THREADS, smem, stream>>>(a);
   return cudaGetLastError();
 }
 
-cudaError_t launch_main(int stages, int nsm, const SplitArgs& a, cudaStream_t stream) {
+cudaError_t launch_main(int stages, int nsm, const SplitArgs& a, cudaStream_t stream,
+                        bool attrs_only) {
   switch (stages) {
-    case 2: return launch_main_t<2>(nsm, a, stream);
-    case 3: return launch_main_t<3>(nsm, a, stream);
-    case 5: return launch_main_t<5>(nsm, a, stream);
-    default: return launch_main_t<4>(nsm, a, stream);
+    case 2: return launch_main_t<2>(nsm, a, stream, attrs_only);
+    case 3: return launch_main_t<3>(nsm, a, stream, attrs_only);
+    case 5: return launch_main_t<5>(nsm, a, stream, attrs_only);
+    default: return launch_main_t<4>(nsm, a, stream, attrs_only);
   }
 }
 
@@ -770,12 +771,13 @@ cudaError_t split_prepare_phi(const double* ao_rhs, size_t stride_grid, const in
   return cudaGetLastError();
 }
 
-cudaError_t split_launch_main(const SplitArgs& a, cudaStream_t stream, int stages) {
+cudaError_t split_launch_main(const SplitArgs& a, cudaStream_t stream, int stages,
+                              bool attrs_only) {
   int dev = 0, nsm = 0;
   cudaError_t err = cudaGetDevice(&dev);
   if (err == cudaSuccess) err = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (err != cudaSuccess) return err;
-  return launch_main(stages > 0 ? stages : split_stages(), nsm, a, stream);
+  return launch_main(stages > 0 ? stages : split_stages(), nsm, a, stream, attrs_only);
 }
 
 cudaError_t split_launch_reduce(const SplitArgs& a, const int2* pairs, int npairs,

@@ -44,6 +44,7 @@
 namespace cfgmm {
 void set_last_error(const std::string& msg);
 int aodm_plan_release_idle(cfgmm_aodm_plan* plan, cudaStream_t stream);
+double aodm_plan_flops(const cfgmm_aodm_plan* plan);
 }  // namespace cfgmm
 
 namespace {
@@ -123,6 +124,7 @@ struct Molecule {
   std::map<size_t, cfgmm_aodm_plan*> plans;  // by nset
   size_t cost = 0;                            // bytes counted against the budget
   bool busy = false, closed = false;
+  bool loading = false;  // being put on the device by the loader thread
   int pending = 0;  // requests queued or on the GPU
   uint64_t last_use = 0;
 };
@@ -137,7 +139,9 @@ struct Request {
   size_t d_bytes = 0, rho_bytes = 0;
   Clock::time_point t_submit, t_launch, t_done;
   float device_ms = 0.f;
+  double flops = 0.0;
   int slot = -1;
+  bool cold = false;         // its molecule was put on the device for it
   bool device_done = false;  // set by the host callback
   bool finished = false;     // set by the worker
   int status = CFGMM_OK;
@@ -165,8 +169,11 @@ struct cfgmm_server {
   std::mutex mu;
   std::condition_variable cv_work;  // worker: new requests, completions, stop
   std::condition_variable cv_done;  // waiters
-  bool stop = false;
-  std::thread worker;
+  std::condition_variable cv_load;  // loader: molecules to put on the device
+  bool stop = false, stop_loader = false;  // the loader stops after the worker
+  std::thread worker, loader;
+  std::deque<uint64_t> to_load;  // tickets whose molecule is being loaded
+  int loading = 0;
 
   uint64_t next_mol = 1, next_ticket = 1, tick = 0;
   std::unordered_map<uint64_t, std::unique_ptr<Molecule>> mols;
@@ -175,7 +182,8 @@ struct cfgmm_server {
 
   size_t used = 0, peak = 0;
   uint64_t admitted_molecules = 0, evictions = 0, completed = 0, failed = 0;
-  std::vector<double> lat_total, lat_queue, lat_device;
+  double flops_done = 0.0;
+  std::vector<double> lat_total, lat_queue, lat_device, lat_warm, lat_load, lat_plan;
   std::string stats_json;
 };
 
@@ -392,6 +400,8 @@ void finish(cfgmm_server* s, Request& r, int status, const std::string& err) {
     s->lat_total.push_back(ms_between(r.t_submit, r.t_done));
     s->lat_queue.push_back(ms_between(r.t_submit, r.t_launch));
     s->lat_device.push_back(r.device_ms);
+    if (!r.cold) s->lat_warm.push_back(ms_between(r.t_submit, r.t_done));
+    s->flops_done += r.flops;
   } else {
     ++s->failed;
   }
@@ -442,6 +452,7 @@ int launch(cfgmm_server* s, Request& r, Molecule& m, Slot& sl, std::string* err)
     *err = std::string("plan: ") + cfgmm_last_error();
     return rc;
   }
+  r.flops = cfgmm::aodm_plan_flops(plan);
   r.t_launch = Clock::now();
   cudaError_t e = cudaMemcpyAsync(m.d_dms, r.pin_d, r.d_bytes, cudaMemcpyHostToDevice, sl.stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(m.d_rho, 0, r.rho_bytes, sl.stream);
@@ -462,7 +473,9 @@ int launch(cfgmm_server* s, Request& r, Molecule& m, Slot& sl, std::string* err)
 }
 
 // The next request that can start now, with its slot reserved, or null.
-// Lock held.
+// A request whose molecule is not on the device goes to the loader instead
+// (its memory reserved) and comes back to the front of the queue when the
+// molecule is resident, so warm requests keep flowing meanwhile.  Lock held.
 Request* pick(cfgmm_server* s, int* slot_out) {
   int free_slot = -1;
   for (size_t i = 0; i < s->slots.size(); ++i)
@@ -470,19 +483,31 @@ Request* pick(cfgmm_server* s, int* slot_out) {
       free_slot = int(i);
       break;
     }
-  if (free_slot < 0) return nullptr;
-  for (auto it = s->pending.begin(); it != s->pending.end(); ++it) {
-    auto rq = s->reqs.find(*it);
-    Request& r = *rq->second;
+  for (auto it = s->pending.begin(); it != s->pending.end();) {
+    Request& r = *s->reqs.find(*it)->second;
     Molecule& m = *s->mols.find(r.mol)->second;
-    if (m.busy) continue;  // one request of a molecule at a time, in order
+    if (m.busy) {  // one request of a molecule at a time, in order
+      ++it;
+      continue;
+    }
     if (!m.resident) {
-      if (!make_room(s, m.cost, m.id)) continue;  // waits for memory
-      s->used += m.cost;  // reserved; materialised below
+      if (!make_room(s, m.cost, m.id)) {  // waits for memory
+        ++it;
+        continue;
+      }
+      s->used += m.cost;  // reserved; the loader puts it on the device
       s->peak = std::max(s->peak, s->used);
       m.resident = true;
+      m.loading = true;
+      m.busy = true;
       m.mem = nullptr;
+      r.cold = true;
+      s->to_load.push_back(*it);
+      it = s->pending.erase(it);
+      s->cv_load.notify_one();
+      continue;
     }
+    if (free_slot < 0) return nullptr;
     s->pending.erase(it);
     m.busy = true;
     m.last_use = ++s->tick;
@@ -492,6 +517,51 @@ Request* pick(cfgmm_server* s, int* slot_out) {
     return &r;
   }
   return nullptr;
+}
+
+// Puts molecules on the device (phi, mask, buffers, plan) one at a time on
+// the admin stream, beside the requests running on the slots.
+void loader_loop(cfgmm_server* s) {
+  cudaSetDevice(s->dev);
+  std::unique_lock<std::mutex> lk(s->mu);
+  for (;;) {
+    s->cv_load.wait(lk, [&] { return s->stop_loader || !s->to_load.empty(); });
+    if (s->to_load.empty()) {
+      if (s->stop_loader) break;
+      continue;
+    }
+    const uint64_t ticket = s->to_load.front();
+    s->to_load.pop_front();
+    ++s->loading;
+    Request& r = *s->reqs.find(ticket)->second;
+    Molecule& m = *s->mols.find(r.mol)->second;
+    lk.unlock();
+    std::string err;
+    const Clock::time_point t0 = Clock::now();
+    int rc = materialize(s, m, &err);
+    const Clock::time_point t1 = Clock::now();
+    if (rc == CFGMM_OK && !plan_for(s, m, r.nset, &rc)) err = std::string("plan: ") + cfgmm_last_error();
+    const Clock::time_point t2 = Clock::now();
+    lk.lock();
+    s->lat_load.push_back(ms_between(t0, t1));
+    s->lat_plan.push_back(ms_between(t1, t2));
+    --s->loading;
+    m.loading = false;
+    if (rc == CFGMM_OK) {
+      ++s->admitted_molecules;
+      m.busy = false;
+      s->pending.push_front(ticket);
+    } else {
+      for (auto& kv : m.plans) cfgmm::aodm_plan_release_idle(kv.second, s->admin);
+      m.plans.clear();
+      if (m.mem) cudaFreeAsync(m.mem, s->admin);
+      m.mem = nullptr;
+      m.resident = false;
+      s->used -= m.cost;
+      finish(s, r, rc, err);
+    }
+    s->cv_work.notify_one();
+  }
 }
 
 void worker_loop(cfgmm_server* s) {
@@ -512,24 +582,11 @@ void worker_loop(cfgmm_server* s) {
     int slot = -1;
     if (Request* r = pick(s, &slot)) {
       Molecule& m = *s->mols.find(r->mol)->second;
-      const bool load = m.mem == nullptr;  // reserved by pick(), not on the device yet
       lk.unlock();
       std::string err;
-      int rc = CFGMM_OK;
-      if (load) {
-        rc = materialize(s, m, &err);
-        if (rc == CFGMM_OK) {
-          std::lock_guard<std::mutex> g(s->mu);
-          ++s->admitted_molecules;
-        }
-      }
-      if (rc == CFGMM_OK) rc = launch(s, *r, m, s->slots[slot], &err);
+      const int rc = launch(s, *r, m, s->slots[slot], &err);
       lk.lock();
       if (rc != CFGMM_OK) {
-        if (load && !m.mem) {  // nothing resident after all
-          m.resident = false;
-          s->used -= m.cost;
-        }
         s->slots[slot].req = nullptr;
         finish(s, *r, rc, err);
       }
@@ -537,7 +594,8 @@ void worker_loop(cfgmm_server* s) {
     }
     bool inflight = false;
     for (Slot& sl : s->slots) inflight |= sl.req != nullptr;
-    if (s->stop && !inflight && s->pending.empty()) break;
+    if (s->stop && !inflight && s->pending.empty() && s->to_load.empty() && s->loading == 0)
+      break;
     s->cv_work.wait_for(lk, std::chrono::milliseconds(5));
   }
 }
@@ -613,7 +671,11 @@ int cfgmm_server_create(cfgmm_server** out, size_t hbm_budget, int nslots, int p
   s->precision = precision;
   s->blksize = blksize;
   s->slots.resize(nslots);
-  cudaError_t e = cudaStreamCreateWithFlags(&s->admin, cudaStreamNonBlocking);
+  // molecule loading runs at the highest stream priority: its kernels are
+  // scheduled ahead of queued request kernels as SMs free up
+  int prio_lo = 0, prio_hi = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+  cudaError_t e = cudaStreamCreateWithPriority(&s->admin, cudaStreamNonBlocking, prio_hi);
   for (Slot& sl : s->slots) {
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&sl.e0);
@@ -622,6 +684,7 @@ int cfgmm_server_create(cfgmm_server** out, size_t hbm_budget, int nslots, int p
   if (e != cudaSuccess) return fail(CFGMM_ERR_CUDA, cuda_msg(e, "server streams"));
   cfgmm_server* raw = s.release();
   raw->worker = std::thread(worker_loop, raw);
+  raw->loader = std::thread(loader_loop, raw);
   *out = raw;
   return CFGMM_OK;
 }
@@ -634,6 +697,12 @@ int cfgmm_server_destroy(cfgmm_server* s) {
   }
   s->cv_work.notify_one();
   if (s->worker.joinable()) s->worker.join();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop_loader = true;
+  }
+  s->cv_load.notify_all();
+  if (s->loader.joinable()) s->loader.join();
   for (auto& kv : s->mols)
     if (kv.second->resident) release(s, *kv.second);
   cudaStreamSynchronize(s->admin);
@@ -786,6 +855,7 @@ int cfgmm_server_wait(cfgmm_server* s, uint64_t ticket, double timeout_s,
     stats->queue_ms = ms_between(r->t_submit, r->t_launch);
     stats->device_ms = r->device_ms;
     stats->total_ms = ms_between(r->t_submit, r->t_done);
+    stats->flops = r->flops;
   }
   const int status = r->status;
   const std::string err = r->error;
@@ -799,18 +869,22 @@ const char* cfgmm_server_stats(cfgmm_server* s) {
   std::lock_guard<std::mutex> lk(s->mu);
   size_t resident = 0;
   for (auto& kv : s->mols) resident += kv.second->resident;
-  char buf[1024];
+  char buf[1536];
   std::snprintf(
       buf, sizeof(buf),
       "{\"completed\":%llu,\"failed\":%llu,\"pending\":%zu,\"molecules\":%zu,\"resident\":%zu,"
       "\"admitted_molecules\":%llu,\"evictions\":%llu,\"budget_bytes\":%zu,\"used_bytes\":%zu,"
-      "\"peak_bytes\":%zu,\"latency_ms\":{\"p50\":%.4f,\"p99\":%.4f,\"max\":%.4f},"
+      "\"peak_bytes\":%zu,\"flops_completed\":%.6e,\"latency_ms\":{\"p50\":%.4f,\"p99\":%.4f,\"max\":%.4f},"
+      "\"warm_latency_ms\":{\"p50\":%.4f,\"p99\":%.4f,\"count\":%zu},"
+      "\"load_ms\":{\"p50\":%.4f,\"max\":%.4f},\"plan_ms\":{\"p50\":%.4f,\"max\":%.4f},"
       "\"queue_ms\":{\"p50\":%.4f,\"p99\":%.4f},\"device_ms\":{\"p50\":%.4f,\"p99\":%.4f}}",
       (unsigned long long)s->completed, (unsigned long long)s->failed, s->pending.size(),
       s->mols.size(), resident, (unsigned long long)s->admitted_molecules,
-      (unsigned long long)s->evictions, s->budget, s->used, s->peak,
+      (unsigned long long)s->evictions, s->budget, s->used, s->peak, s->flops_done,
       percentile(s->lat_total, 0.5), percentile(s->lat_total, 0.99),
-      percentile(s->lat_total, 1.0), percentile(s->lat_queue, 0.5),
+      percentile(s->lat_total, 1.0), percentile(s->lat_warm, 0.5), percentile(s->lat_warm, 0.99),
+      s->lat_warm.size(), percentile(s->lat_load, 0.5), percentile(s->lat_load, 1.0),
+      percentile(s->lat_plan, 0.5), percentile(s->lat_plan, 1.0), percentile(s->lat_queue, 0.5),
       percentile(s->lat_queue, 0.99), percentile(s->lat_device, 0.5),
       percentile(s->lat_device, 0.99));
   s->stats_json = buf;

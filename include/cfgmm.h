@@ -246,7 +246,9 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** plan, const cfgmm_aodm_batch* batch
                            const double* dms, size_t stride_ao, size_t nao, size_t nset_max,
                            size_t blksize, int precision, int flags, void* stream);
 int cfgmm_aodm_plan_run(cfgmm_aodm_plan* plan, void* stream);
-/* JSON description: batch and item counts, chosen tiles, autotuner timings. */
+/* JSON description: precision, batch and item counts, algorithmic flops of
+ * one run (sum over batches, matrices and blocks of (2|I_b|^2 + 2|I_b|)|b|),
+ * chosen tiles, autotuner timings. */
 const char* cfgmm_aodm_plan_info(const cfgmm_aodm_plan* plan);
 int cfgmm_aodm_plan_destroy(cfgmm_aodm_plan* plan);
 
@@ -294,6 +296,7 @@ typedef struct cfgmm_request_stats {
   double queue_ms;   /* submit -> start on the GPU */
   double device_ms;  /* the contraction on the GPU (CUDA events) */
   double total_ms;   /* submit -> rho in the caller's buffer */
+  double flops;      /* sum_s sum_b (2|I_b|^2 + 2|I_b|)|b| of the request */
 } cfgmm_request_stats;
 
 int cfgmm_server_create(cfgmm_server** server, size_t hbm_budget, int nslots, int precision,
@@ -331,7 +334,8 @@ int cfgmm_server_submit(cfgmm_server* server, uint64_t molecule, const double* d
 int cfgmm_server_wait(cfgmm_server* server, uint64_t ticket, double timeout_s,
                       cfgmm_request_stats* stats);
 /* JSON: completed/failed counts, molecules resident, evictions, budget, used
- * and peak bytes, and p50/p99 latency (total, queue, device) in ms. */
+ * and peak bytes, flops of the completed requests, and p50/p99 latency
+ * (total, queue, device) in ms. */
 const char* cfgmm_server_stats(cfgmm_server* server);
 
 #ifdef __cplusplus
