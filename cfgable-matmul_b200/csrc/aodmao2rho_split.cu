@@ -409,6 +409,24 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(SplitArgs p) {
         const int row = ut * TU + 32 * wq + 4 * st + ri;
         iu[st] = row < nb ? __ldg(I + row) : -1;
       }
+      // what the epilogue of this item reads is requested now, while the
+      // chunks run: the row's AO index and scale, the point scale of this
+      // lane, and the phi_lhs row segment (into L2)
+      const int g0 = b * p.blk + gt * TG;
+      const int gw = min(min((b + 1) * p.blk, B.ngrid), g0 + TG) - g0;
+      const int erow = ut * TU + 32 * wq + lane;
+      const bool ev = erow < nb;
+      const int eu = ev ? __ldg(I + erow) : 0;
+      const int tu = p.tau[size_t(s) * p.nao + eu];
+      const int sg_lane = 32 * grp + lane < gw ? B.sigma[g0 + 32 * grp + lane] : 0;
+      const double* lrow = B.ao_lhs + size_t(eu) * B.stride_grid + g0;
+      if (ev && 32 * grp < gw) {
+        const char* pf = reinterpret_cast<const char*>(lrow + 32 * grp);
+        const char* pe = reinterpret_cast<const char*>(lrow + min(gw, 32 * grp + 32));
+        for (const char* q = pf; q < pe; q += 128)
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(q));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(pe - 8));
+      }
       for (int c = grp; c < kc; c += 2) {
         const uint32_t seq = seq0 + uint32_t(c);
         const int stg = int(seq % STAGES);
@@ -464,16 +482,9 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(SplitArgs p) {
       // 32 rows of warp wq (TMEM lanes 32wq ..) ----
       if (!tc::mbar_wait(acc_full, nitem & 1, err, 12)) break;
       tc::fence_after_sync();
-      const int g0 = b * p.blk + gt * TG;
-      const int gw = min(min((b + 1) * p.blk, B.ngrid), g0 + TG) - g0;
       // 16-byte loads of phi_lhs when every row segment starts 16-byte aligned
       const bool vec2 = (B.stride_grid % 2 == 0) && (p.blk % 2 == 0) &&
                         (reinterpret_cast<uintptr_t>(B.ao_lhs) % 16 == 0);
-      const int erow = ut * TU + 32 * wq + lane;
-      const bool ev = erow < nb;
-      const int eu = ev ? __ldg(I + erow) : 0;
-      const int tu = p.tau[size_t(s) * p.nao + eu];
-      const double* lrow = B.ao_lhs + size_t(eu) * B.stride_grid + g0;
       const uint32_t trow = tmem + (uint32_t(32 * wq) << 16);
       const size_t slot =
           size_t(B.partial_off) + ((size_t(bg) * p.max_ut + ut) * B.nset + s) * EPI_PARTS + wq;
@@ -499,13 +510,20 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(SplitArgs p) {
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
           const int gl = cc + j;
+          const int sg = __shfl_sync(0xffffffffu, sg_lane, gl & 31);
           if (ev && gl < gw) {
-            double x = double(int(v[NSL - 1][j]));
-#pragma unroll
-            for (int L = NSL - 2; L >= 0; --L) x = fma(x, 0.00390625, double(int(v[L][j])));
-            const int sg = B.sigma[g0 + gl];
+            // X = sum_L S_L 2^-8L: levels 0-2 and 3-6 combined exactly in 64-bit
+            // integers (below 2^48 and 2^56), then one FMA
+            const long long hi = (static_cast<long long>(int(v[0][j])) << 16) +
+                                 (static_cast<long long>(int(v[1][j])) << 8) + int(v[2][j]);
+            const long long lo = (static_cast<long long>(int(v[3][j])) << 24) +
+                                 (static_cast<long long>(int(v[4][j])) << 16) +
+                                 (static_cast<long long>(int(v[5][j])) << 8) + int(v[6][j]);
+            const double x = fma(double(lo), 0x1p-48, double(hi) * 0x1p-16);
+            const int e = -(tu + sg);
             a[j] = (tu == kBadExp || sg == kBadExp) ? __longlong_as_double(0x7ff8000000000000LL)
-                                                    : ldexp(x, -(tu + sg)) * a[j];
+                   : (e >= -1022 && e <= 1023)      ? x * pow2(e) * a[j]
+                                                    : ldexp(x, e) * a[j];
           }
         }
         // reduce-scatter over the 32 rows: 9 shuffles leave the lanes 4m .. 4m+3
