@@ -148,6 +148,8 @@ def peaks_lib():
         getattr(L, name).restype = ctypes.c_double
     L.cfgmm_peak_i8_tops.argtypes = [ctypes.c_int]
     L.cfgmm_peak_i8_tops.restype = ctypes.c_double
+    L.cfgmm_peak_dmma_sustained.argtypes = [ctypes.c_double]
+    L.cfgmm_peak_dmma_sustained.restype = ctypes.c_double
     return L
 
 
@@ -417,6 +419,7 @@ def run_ours(args, ranks: Ranks):
     pk = peaks_lib()
     dmma_peak = max(pk.cfgmm_peak_dmma_tflops(20000, 2), pk.cfgmm_peak_dmma_tflops(20000, 4))
     dfma_peak = pk.cfgmm_peak_dfma_tflops(20000, 4)
+    dmma_sust = pk.cfgmm_peak_dmma_sustained(1.5)
     i8_peak = pk.cfgmm_peak_i8_tops(20000)
 
     g = torch.Generator(device=dev).manual_seed(1234 + ranks.rank)
@@ -539,7 +542,8 @@ def run_ours(args, ranks: Ranks):
             "flops_per_step": aflops, "flops": "sum_s sum_b (2|I_b|^2 + 2|I_b|)|b| (masked)",
             "fp64": {"value": ranks.world * aflops * args.steps / (atot * 1e-3) / 1e9,
                      "unit": "GFLOP/s", "ms_per_step": atot / args.steps,
-                     "frac_of_dmma_peak": (aflops / (atot / args.steps * 1e-3) / 1e12) / dmma_peak,
+                     "frac_of_dmma_peak": (aflops / (atot / args.steps * 1e-3) / 1e12) / dmma_sust,
+                     "frac_of_dmma_burst": (aflops / (atot / args.steps * 1e-3) / 1e12) / dmma_peak,
                      "launches_per_step": 4},
             "split": {"value": ranks.world * aflops * args.steps / (stot * 1e-3) / 1e9,
                       "unit": "GFLOP/s", "ms_per_step": stot / args.steps,
@@ -578,12 +582,17 @@ def run_ours(args, ranks: Ranks):
                  "unit": "TFLOP/s", "ms_per_step": fp64_ms / args.steps,
                  "error_vs_exact_sampled": fp64_err,
                  "roofline": {"bound": "tensor", "achieved": flops / (fp64_kernel_ms * 1e-3) / 1e12,
-                              "peak": dmma_peak, "unit": "TFLOP/s",
-                              "frac": flops / (fp64_kernel_ms * 1e-3) / 1e12 / dmma_peak,
+                              "peak": dmma_sust, "unit": "TFLOP/s",
+                              "frac": flops / (fp64_kernel_ms * 1e-3) / 1e12 / dmma_sust,
+                              "peak_burst": dmma_peak,
+                              "frac_of_burst": flops / (fp64_kernel_ms * 1e-3) / 1e12 / dmma_peak,
                               "traffic": profile_traffic("dgemm_fp64_3527x9583x6581"),
                               "kernel": "dgemm_fp64_kernel<false,false>",
-                              "peak_source": "measured in this run: DMMA m16n8k4 register loop "
-                                             f"(burst); FP64 FMA pipe {dfma_peak:.2f} TFLOP/s"},
+                              "peak_source": "measured in this run: DMMA m16n8k4 register loop on "
+                                             "every SM, sustained (1.5 s of back-to-back "
+                                             "launches, second half) for a kernel timed over "
+                                             "many back-to-back steps; burst figure beside it; "
+                                             f"FP64 FMA pipe {dfma_peak:.2f} TFLOP/s (burst)"},
                  "e2e": e2e_fp64},
         "speedup_split_vs_fp64": fp64_ms / split_ms,
         "e2e": {"value": e2e_split, "unit": "TFLOP/s",

@@ -25,6 +25,8 @@
 //     holds k = 2q and 2q+1 as MMA k-slots q and q+4), so each fragment load
 //     is one 16-byte shared-memory load; the same permutation is applied to A
 //     and B, which leaves the sum unchanged up to FP64 rounding order.
+#include <algorithm>
+
 #include "common.cuh"
 #include "dgemm_fp64.cuh"
 
@@ -114,11 +116,20 @@ struct TileCopier {
   }
 };
 
+// The tiles of a last, partial wave of CTAs may be split along K: block
+// full + j (j < tail * splits) computes K steps [s*ktiles/splits, (s+1)*ktiles/splits)
+// of tile full + j / splits (s = j % splits) and stores its partial tile in
+// ws[j]; splits == 0 means no split.
+struct TailSplit {
+  int full, splits;
+  double* ws;  // [tail * splits][BM * BN]
+};
+
 template <bool TA, bool TB>
 __global__ void __launch_bounds__(THREADS, 1)
 dgemm_fp64_kernel(double* __restrict__ c, const double* __restrict__ a,
                   const double* __restrict__ b, int m, int n, int k, size_t lda, size_t ldb,
-                  size_t ldc, ColMask mask) {
+                  size_t ldc, ColMask mask, TailSplit tail) {
   extern __shared__ __align__(128) double smem[];
   double* As = smem;
   double* Bs = smem + STAGES * TILE_DOUBLES;
@@ -131,14 +142,20 @@ dgemm_fp64_kernel(double* __restrict__ c, const double* __restrict__ a,
   // 1-D grid in groups of GROUP_M tile rows: CTAs running together share the
   // B panels of a group and the A panels of its rows in L2.
   const int tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
+  const bool split = tail.splits > 0 && int(blockIdx.x) >= tail.full;
+  const int job = split ? int(blockIdx.x) - tail.full : 0;
+  const int tile = split ? tail.full + job / tail.splits : int(blockIdx.x);
   const int per_group = GROUP_M * tiles_n;
-  const int group = blockIdx.x / per_group;
+  const int group = tile / per_group;
   const int first_m = group * GROUP_M;
   const int gsz = min(tiles_m - first_m, GROUP_M);
-  const int in_group = blockIdx.x % per_group;
+  const int in_group = tile % per_group;
   const int m0 = (first_m + in_group % gsz) * BM;
   const int n0 = (in_group / gsz) * BN;
-  const int ktiles = (k + BK - 1) / BK;
+  const int kall = (k + BK - 1) / BK;
+  const int sidx = split ? job % tail.splits : 0;
+  const int kt0 = split ? int((long long)sidx * kall / tail.splits) : 0;
+  const int kt1 = split ? int((long long)(sidx + 1) * kall / tail.splits) : kall;
 
   // A: rows m, k contiguous unless transposed.  B: rows n, k contiguous only
   // when transposed (b[j*ldb + p]).
@@ -157,23 +174,23 @@ dgemm_fp64_kernel(double* __restrict__ c, const double* __restrict__ a,
 
 #pragma unroll
   for (int s = 0; s < STAGES - 1; ++s) {
-    if (s < ktiles) {
-      ca.template issue<0, CPT>(As + s * TILE_DOUBLES, s, k);
-      cb.template issue<0, CPT>(Bs + s * TILE_DOUBLES, s, k);
+    if (kt0 + s < kt1) {
+      ca.template issue<0, CPT>(As + s * TILE_DOUBLES, kt0 + s, k);
+      cb.template issue<0, CPT>(Bs + s * TILE_DOUBLES, kt0 + s, k);
     }
     cp_async_commit();
   }
 
-  for (int kt = 0; kt < ktiles; ++kt) {
+  for (int kt = kt0; kt < kt1; ++kt) {
     cp_async_wait<STAGES - 2>();
     __syncthreads();
     const int nk = kt + STAGES - 1;  // K step whose copies go out during this one
-    const bool pre = nk < ktiles;
-    double* An = As + (nk % STAGES) * TILE_DOUBLES;
-    double* Bn = Bs + (nk % STAGES) * TILE_DOUBLES;
+    const bool pre = nk < kt1;
+    double* An = As + ((nk - kt0) % STAGES) * TILE_DOUBLES;
+    double* Bn = Bs + ((nk - kt0) % STAGES) * TILE_DOUBLES;
 
-    const double* A_s = As + (kt % STAGES) * TILE_DOUBLES;
-    const double* B_s = Bs + (kt % STAGES) * TILE_DOUBLES;
+    const double* A_s = As + ((kt - kt0) % STAGES) * TILE_DOUBLES;
+    const double* B_s = Bs + ((kt - kt0) % STAGES) * TILE_DOUBLES;
 #pragma unroll
     for (int kk = 0; kk < BK; kk += 8) {
       double2 av[4][2], bv[4];
@@ -206,6 +223,21 @@ dgemm_fp64_kernel(double* __restrict__ c, const double* __restrict__ a,
   }
   cp_async_wait<0>();
 
+  if (split) {  // the partial tile, dense 128 x 128, to the workspace
+    double* w = tail.ws + size_t(job) * (BM * BN);
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = wm * 64 + mt * 16 + g + 8 * h;
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+          *reinterpret_cast<double2*>(w + r * BN + wn * 32 + nt * 8 + 2 * q) =
+              make_double2(acc[mt][nt][2 * h], acc[mt][nt][2 * h + 1]);
+      }
+    return;
+  }
+
   // Epilogue: C += acc, element-wise bounds checks.
 #pragma unroll
   for (int mt = 0; mt < 4; ++mt)
@@ -223,6 +255,40 @@ dgemm_fp64_kernel(double* __restrict__ c, const double* __restrict__ a,
     }
 }
 
+// C[tile] += the splits' partial tiles, added in split order (deterministic).
+__global__ void __launch_bounds__(256)
+dgemm_tail_reduce(double* __restrict__ c, const double* __restrict__ ws, int m, int n,
+                  size_t ldc, int full, int splits) {
+  const int tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
+  const int tile = full + blockIdx.x;
+  const int per_group = GROUP_M * tiles_n;
+  const int group = tile / per_group;
+  const int first_m = group * GROUP_M;
+  const int gsz = min(tiles_m - first_m, GROUP_M);
+  const int in_group = tile % per_group;
+  const int m0 = (first_m + in_group % gsz) * BM;
+  const int n0 = (in_group / gsz) * BN;
+  const double* w = ws + size_t(blockIdx.x) * splits * (BM * BN);
+  for (int e = threadIdx.x; e < BM * BN; e += 256) {
+    const int r = e / BN, cc = e % BN;
+    if (m0 + r >= m || n0 + cc >= n) continue;
+    double v = 0.0;
+    for (int s2 = 0; s2 < splits; ++s2) v += w[size_t(s2) * (BM * BN) + e];
+    double* dst = c + size_t(m0 + r) * ldc + n0 + cc;
+    *dst += v;
+  }
+}
+
+int sm_count() {
+  int dev = 0, nsm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return nsm;
+}
+
 template <bool TA, bool TB>
 cudaError_t launch_t(double* c, const double* a, const double* b, int m, int n, int k,
                      size_t lda, size_t ldb, size_t ldc, ColMask mask, cudaStream_t stream) {
@@ -232,8 +298,36 @@ cudaError_t launch_t(double* c, const double* a, const double* b, int m, int n, 
   if (err != cudaSuccess) return err;
   const long long tiles = (long long)((m + BM - 1) / BM) * ((n + BN - 1) / BN);
   if (tiles > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-  kern<<<unsigned(tiles), THREADS, SMEM_BYTES, stream>>>(c, a, b, m, n, k, lda, ldb, ldc, mask);
-  return cudaGetLastError();
+  // One CTA per SM: a last wave of `tail` < nsm tiles leaves SMs idle, so its
+  // tiles are split along K (at least 4 K steps per split) over them.
+  const int nsm = sm_count();
+  const int kall = (k + BK - 1) / BK;
+  TailSplit ts{0, 0, nullptr};
+  if (nsm > 0 && tiles > nsm && tiles % nsm != 0) {
+    const int tail = int(tiles % nsm);
+    const int splits = std::min(nsm / tail, kall / 4);
+    if (splits >= 2) {
+      ts.full = int(tiles - tail);
+      ts.splits = splits;
+      err = cudaMallocAsync(reinterpret_cast<void**>(&ts.ws),
+                            size_t(tail) * splits * BM * BN * sizeof(double), stream);
+      if (err != cudaSuccess) return err;
+    }
+  }
+  const long long grid = ts.splits ? ts.full + (tiles - ts.full) * ts.splits : tiles;
+  kern<<<unsigned(grid), THREADS, SMEM_BYTES, stream>>>(c, a, b, m, n, k, lda, ldb, ldc, mask,
+                                                         ts);
+  err = cudaGetLastError();
+  if (ts.splits) {
+    if (err == cudaSuccess) {
+      dgemm_tail_reduce<<<unsigned(tiles - ts.full), 256, 0, stream>>>(c, ts.ws, m, n, ldc,
+                                                                       ts.full, ts.splits);
+      err = cudaGetLastError();
+    }
+    const cudaError_t e2 = cudaFreeAsync(ts.ws, stream);
+    if (err == cudaSuccess) err = e2;
+  }
+  return err;
 }
 
 }  // namespace

@@ -150,6 +150,42 @@ double cfgmm_peak_dmma_tflops(int iters, int ctas_per_sm) {
   return r;
 }
 
+// Sustained DMMA throughput: back-to-back launches of the same loop for about
+// `seconds`, TFLOP/s over the second half (the clock settles under the power
+// cap while it runs).  For kernels timed inside a long step.
+double cfgmm_peak_dmma_sustained(double seconds) {
+  double* out = nullptr;
+  if (cudaMalloc(&out, 8) != cudaSuccess) return -1.0;
+  const int grid = sm_count() * 2;
+  const int iters = 20000;
+  const double flops = double(grid) * 8 * iters * kChains * 2.0 * 16 * 8 * 4;
+  const double burst = time_kernel([&] { dmma_loop<kChains><<<grid, 256>>>(out, iters, 0.5); },
+                                   flops);
+  if (burst <= 0) {
+    cudaFree(out);
+    return -1.0;
+  }
+  const double launch_s = flops / (burst * 1e12);
+  const int n = int(seconds / launch_s) + 2;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  for (int i = 0; i < n / 2; ++i) dmma_loop<kChains><<<grid, 256>>>(out, iters, 0.5);
+  cudaEventRecord(e0);
+  for (int i = n / 2; i < n; ++i) dmma_loop<kChains><<<grid, 256>>>(out, iters, 0.5);
+  cudaEventRecord(e1);
+  double r = -1.0;
+  if (cudaEventSynchronize(e1) == cudaSuccess) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    r = flops * (n - n / 2) / (ms * 1e-3) / 1e12;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  return r;
+}
+
 // DMMA throughput with `chains` (4, 8 or 16) independent accumulators per warp,
 // `warps` (1..8) warps per CTA and `ctas_per_sm` CTAs per SM: how much
 // parallelism the FP64 tensor pipe needs.
