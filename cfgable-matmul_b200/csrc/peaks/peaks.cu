@@ -14,6 +14,31 @@ namespace {
 
 constexpr int kChains = 8;  // independent accumulators per warp
 
+// The same loop with the m16n8k8 shape (twice the work per instruction).
+template <int kChains>
+__global__ void __launch_bounds__(256) dmma8_loop(double* out, int iters, double seed) {
+  const int lane = threadIdx.x & 31;
+  double a0 = seed + lane * 1e-3, a1 = seed - lane * 1e-3, b0 = 1.0 + lane * 1e-6;
+  double acc[kChains][4];
+#pragma unroll
+  for (int c = 0; c < kChains; ++c)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) acc[c][e] = 0.0;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int c = 0; c < kChains; ++c)
+      asm volatile(
+          "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+          "{%8,%9}, {%0,%1,%2,%3};\n"
+          : "+d"(acc[c][0]), "+d"(acc[c][1]), "+d"(acc[c][2]), "+d"(acc[c][3])
+          : "d"(a0), "d"(a1), "d"(a1), "d"(a0), "d"(b0), "d"(b0));
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int c = 0; c < kChains; ++c) s += acc[c][0] + acc[c][1] + acc[c][2] + acc[c][3];
+  if (s == 12345.678) out[0] = s;  // keeps the loop live; never true in practice
+}
+
 template <int kChains>
 __global__ void __launch_bounds__(256) dmma_loop(double* out, int iters, double seed) {
   const int lane = threadIdx.x & 31;
@@ -182,6 +207,23 @@ double cfgmm_peak_dmma_sustained(double seconds) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  cudaFree(out);
+  return r;
+}
+
+// m16n8k8 DMMA throughput, same parameters as cfgmm_peak_dmma_sweep.
+double cfgmm_peak_dmma8_sweep(int iters, int ctas_per_sm, int warps, int chains) {
+  double* out = nullptr;
+  if (warps < 1 || warps > 8 || cudaMalloc(&out, 8) != cudaSuccess) return -1.0;
+  const int grid = sm_count() * ctas_per_sm;
+  const double flops = double(grid) * warps * iters * chains * 2.0 * 16 * 8 * 8;
+  double r = -1.0;
+  if (chains == 4)
+    r = time_kernel([&] { dmma8_loop<4><<<grid, 32 * warps>>>(out, iters, 0.5); }, flops);
+  else if (chains == 8)
+    r = time_kernel([&] { dmma8_loop<8><<<grid, 32 * warps>>>(out, iters, 0.5); }, flops);
+  else if (chains == 16)
+    r = time_kernel([&] { dmma8_loop<16><<<grid, 32 * warps>>>(out, iters, 0.5); }, flops);
   cudaFree(out);
   return r;
 }
