@@ -178,10 +178,12 @@ int check_split_gemm(size_t k) {
 
 // Reads the sticky error words of the tcgen05 kernels after a synchronised call.
 int check_device_waits() {
-  int code = 0, code2 = 0;
+  int code = 0, code2 = 0, code3 = 0;
   CFGMM_CUDA(cfgmm::gemm_i8_read_error(&code));
   CFGMM_CUDA(cfgmm::aodmao2rho_split_read_error(&code2));
+  CFGMM_CUDA(cfgmm::dgemm_read_error(&code3));
   if (code == 0) code = code2;
+  if (code == 0) code = code3;
   if (code != 0) {
     char msg[128];
     std::snprintf(msg, sizeof(msg), "a tensor-core pipeline wait timed out (code %d)", code);
@@ -268,8 +270,7 @@ int gemm_host(double* c, size_t c_len, const double* a, size_t a_len, const doub
   }
   CFGMM_CUDA(cudaMemcpyAsync(c, dc, ex.c * 8, cudaMemcpyDeviceToHost, st->stream));
   CFGMM_CUDA(cudaStreamSynchronize(st->stream));
-  if (split) return check_device_waits();
-  return CFGMM_OK;
+  return check_device_waits();
 }
 
 // ---------------------------------------------------------------------------

@@ -25,10 +25,16 @@
 //     holds k = 2q and 2q+1 as MMA k-slots q and q+4), so each fragment load
 //     is one 16-byte shared-memory load; the same permutation is applied to A
 //     and B, which leaves the sum unchanged up to FP64 rounding order.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
+#include <cstdlib>
+#include <mutex>
 
 #include "common.cuh"
 #include "dgemm_fp64.cuh"
+#include "tcgen05.cuh"
 
 namespace cfgmm {
 namespace {
@@ -255,6 +261,238 @@ dgemm_fp64_kernel(double* __restrict__ c, const double* __restrict__ a,
     }
 }
 
+// ---------------------------------------------------------------------------
+// Second form, for large products: A and B packed once into K-contiguous,
+// 16-byte-aligned buffers (the mask of the masked GEMM applied while packing),
+// tiles staged by TMA (two 128 x 16-double boxes per operand per K step, 128-
+// byte swizzle) issued by one thread, so the warps only load fragments and
+// issue DMMAs.  Same tile order, warp layout, k permutation, epilogue and K
+// split of the last wave as the first form.
+// ---------------------------------------------------------------------------
+__device__ int g_dgemm_error;
+
+constexpr uint32_t BOX_BYTES = 128 * 16 * 8;      // 16 KB: 128 rows x 16 doubles
+constexpr uint32_t OP_BYTES = 2 * BOX_BYTES;      // one operand tile, 128 x 32
+constexpr uint32_t TSTAGE = 2 * OP_BYTES;         // A and B
+constexpr size_t TMA_SMEM = size_t(STAGES) * TSTAGE + 1024 + 64;
+
+// Double offset of element (r, kp) (kp < 32) in a 128 x 32 operand tile laid
+// down by two TMA boxes with 128-byte swizzle: 16-byte chunk (kp % 16) / 2 of
+// row r sits at chunk position ((kp % 16) / 2) ^ (r % 8).
+__device__ __forceinline__ int tma_off(int r, int kp) {
+  return (kp >> 4) * (128 * 16) + r * 16 + ((((kp & 15) >> 1) ^ (r & 7)) << 1) + (kp & 1);
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar,
+                                            int c0, int c1) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%3, %4}], [%2];" ::"r"(tc::smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(tc::smem_u32(bar)), "r"(c0), "r"(c1)
+      : "memory");
+}
+
+__global__ void __launch_bounds__(THREADS, 1)
+dgemm_tma_kernel(double* __restrict__ c, int m, int n, int k, size_t ldc,
+                 const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                 TailSplit tail) {
+  extern __shared__ uint8_t tsmem_raw[];
+  uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(tsmem_raw) + 1023) &
+                                           ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm + STAGES * TSTAGE);
+  int* err = &g_dgemm_error;
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 2, wn = warp & 3;  // 2 x 4 warp grid
+  const int g = lane >> 2, q = lane & 3;
+
+  const int tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
+  const bool split = tail.splits > 0 && int(blockIdx.x) >= tail.full;
+  const int job = split ? int(blockIdx.x) - tail.full : 0;
+  const int tile = split ? tail.full + job / tail.splits : int(blockIdx.x);
+  const int per_group = GROUP_M * tiles_n;
+  const int group = tile / per_group;
+  const int first_m = group * GROUP_M;
+  const int gsz = min(tiles_m - first_m, GROUP_M);
+  const int in_group = tile % per_group;
+  const int m0 = (first_m + in_group % gsz) * BM;
+  const int n0 = (in_group / gsz) * BN;
+  const int kall = (k + BK - 1) / BK;
+  const int sidx = split ? job % tail.splits : 0;
+  const int kt0 = split ? int((long long)sidx * kall / tail.splits) : 0;
+  const int kt1 = split ? int((long long)(sidx + 1) * kall / tail.splits) : kall;
+
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; ++s) tc::mbar_init(&full[s], 1);
+    tc::mbar_fence_init();
+    tc::prefetch_tensormap(&tmA);
+    tc::prefetch_tensormap(&tmB);
+  }
+  __syncthreads();
+  auto issue = [&](int kt) {  // thread 0: both operand tiles of K step kt
+    const int s = (kt - kt0) % STAGES;
+    uint8_t* st = sm + s * TSTAGE;
+    tc::mbar_arrive_expect_tx(&full[s], TSTAGE);
+    tma_load_2d(st, &tmA, &full[s], kt * BK, m0);
+    tma_load_2d(st + BOX_BYTES, &tmA, &full[s], kt * BK + 16, m0);
+    tma_load_2d(st + OP_BYTES, &tmB, &full[s], kt * BK, n0);
+    tma_load_2d(st + OP_BYTES + BOX_BYTES, &tmB, &full[s], kt * BK + 16, n0);
+  };
+  if (tid == 0)
+    for (int kt = kt0; kt < min(kt1, kt0 + STAGES - 1); ++kt) issue(kt);
+
+  double acc[4][4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
+
+  bool ok = true;
+  int kfail = kt1;
+  for (int kt = kt0; kt < kt1 && ok; ++kt) {
+    __syncthreads();  // every warp is done with step kt-1: its stage can be refilled
+    if (tid == 0 && kt + STAGES - 1 < kt1) issue(kt + STAGES - 1);
+    const int s = (kt - kt0) % STAGES;
+    if (!tc::mbar_wait(&full[s], ((kt - kt0) / STAGES) & 1, err, 51)) {
+      ok = false;
+      kfail = kt;
+      break;
+    }
+    const double* A_s = reinterpret_cast<const double*>(sm + s * TSTAGE);
+    const double* B_s = reinterpret_cast<const double*>(sm + s * TSTAGE + OP_BYTES);
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 8) {
+      double2 av[4][2], bv[4];
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt) {
+        const int r = wm * 64 + mt * 16 + g;
+        av[mt][0] = *reinterpret_cast<const double2*>(A_s + tma_off(r, kk + 2 * q));
+        av[mt][1] = *reinterpret_cast<const double2*>(A_s + tma_off(r + 8, kk + 2 * q));
+      }
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const int r = wn * 32 + nt * 8 + g;
+        bv[nt] = *reinterpret_cast<const double2*>(B_s + tma_off(r, kk + 2 * q));
+      }
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+          dmma_16x8x8(acc[mt][nt], av[mt][0].x, av[mt][1].x, av[mt][0].y, av[mt][1].y, bv[nt].x,
+                      bv[nt].y);
+    }
+  }
+  if (!ok) {  // the copies issued for steps kfail .. kfail+STAGES-1 land before the CTA exits
+    if (tid == 0)
+      for (int kt = kfail; kt < min(kt1, kfail + STAGES); ++kt) {
+        const int s2 = (kt - kt0) % STAGES;
+        tc::mbar_wait(&full[s2], ((kt - kt0) / STAGES) & 1, err, 52, true);
+      }
+    return;
+  }
+
+  if (split) {  // the partial tile, dense 128 x 128, to the workspace
+    double* w = tail.ws + size_t(job) * (BM * BN);
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = wm * 64 + mt * 16 + g + 8 * h;
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+          *reinterpret_cast<double2*>(w + r * BN + wn * 32 + nt * 8 + 2 * q) =
+              make_double2(acc[mt][nt][2 * h], acc[mt][nt][2 * h + 1]);
+      }
+    return;
+  }
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int row = m0 + wm * 64 + mt * 16 + g + 8 * h;
+      if (row >= m) continue;
+      double* crow = c + size_t(row) * ldc;
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const int col = n0 + wn * 32 + nt * 8 + 2 * q;
+        if (col < n) crow[col] += acc[mt][nt][2 * h];
+        if (col + 1 < n) crow[col + 1] += acc[mt][nt][2 * h + 1];
+      }
+    }
+}
+
+// dst[r][kk] = src[r * ld + kk] (kk < k), 0 for k <= kk < kpad: rows of a
+// K-contiguous operand.  A warp per row, 256 columns per block.
+__global__ void __launch_bounds__(256)
+pack_rows(double* __restrict__ dst, const double* __restrict__ src, size_t ld, int rows, int k,
+          int kpad) {
+  const int r = blockIdx.y * 8 + (threadIdx.x >> 5);
+  if (r >= rows) return;
+  const double* srow = src + size_t(r) * ld;
+  double* drow = dst + size_t(r) * kpad;
+  for (int j = threadIdx.x & 31; j < 256; j += 32) {
+    const int kk = blockIdx.x * 256 + j;
+    if (kk < kpad) drow[kk] = kk < k ? srow[kk] : 0.0;
+  }
+}
+
+// dst[j][p] = src[p * ld + j] for p < k (0 for k <= p < kpad), j < cols: the
+// transpose into a K-contiguous operand, through a 32 x 32 shared tile.  With
+// a mask, element (p, j) is zero unless tab[p * ldtab + j / blk].
+__global__ void __launch_bounds__(256)
+pack_transpose(double* __restrict__ dst, const double* __restrict__ src, size_t ld, int cols,
+               int k, int kpad, const uint8_t* __restrict__ tab, size_t ldtab, int blk) {
+  __shared__ double t[32][33];
+  const int j0 = blockIdx.x * 32, p0 = blockIdx.y * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+#pragma unroll
+  for (int i = 0; i < 32; i += 8) {
+    const int p = p0 + ty + i, j = j0 + tx;
+    double v = 0.0;
+    if (p < k && j < cols) {
+      v = src[size_t(p) * ld + j];
+      if (tab && !tab[size_t(p) * ldtab + j / blk]) v = 0.0;
+    }
+    t[ty + i][tx] = v;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 32; i += 8) {
+    const int j = j0 + ty + i, p = p0 + tx;
+    if (j < cols && p < kpad) dst[size_t(j) * kpad + p] = t[tx][ty + i];
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult qr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &qr) ==
+            cudaSuccess &&
+        qr == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  });
+  return fn;
+}
+
+// 2-D map of a packed operand: rows x kpad doubles, 128 x 16 boxes, 128-byte swizzle.
+bool make_operand_map(CUtensorMap* map, const double* base, int rows, int kpad) {
+  auto enc = encode_fn();
+  if (!enc) return false;
+  cuuint64_t dims[2] = {cuuint64_t(kpad), cuuint64_t(rows)};
+  cuuint64_t strides[1] = {cuuint64_t(kpad) * sizeof(double)};
+  cuuint32_t box[2] = {16, 128};
+  cuuint32_t estr[2] = {1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dims, strides,
+             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // C[tile] += the splits' partial tiles, added in split order (deterministic).
 __global__ void __launch_bounds__(256)
 dgemm_tail_reduce(double* __restrict__ c, const double* __restrict__ ws, int m, int n,
@@ -330,6 +568,75 @@ cudaError_t launch_t(double* c, const double* a, const double* b, int m, int n, 
   return err;
 }
 
+// The TMA form: pack A and B, build their tensor maps, run, release.
+cudaError_t launch_packed(double* c, const double* a, const double* b, int m, int n, int k,
+                          size_t lda, size_t ldb, size_t ldc, bool transa, bool transb,
+                          ColMask mask, cudaStream_t stream) {
+  const int kpad = (k + 7) / 8 * 8;
+  double* ws = nullptr;
+  cudaError_t err = cudaMallocAsync(reinterpret_cast<void**>(&ws),
+                                    (size_t(m) + n) * kpad * sizeof(double), stream);
+  if (err != cudaSuccess) return err;
+  double* ap = ws;
+  double* bp = ws + size_t(m) * kpad;
+  if (!transa)
+    pack_rows<<<dim3((kpad + 255) / 256, (m + 7) / 8), 256, 0, stream>>>(ap, a, lda, m, k, kpad);
+  else
+    pack_transpose<<<dim3((m + 31) / 32, (kpad + 31) / 32), 256, 0, stream>>>(
+        ap, a, lda, m, k, kpad, nullptr, 0, 1);
+  if (transb)
+    pack_rows<<<dim3((kpad + 255) / 256, (n + 7) / 8), 256, 0, stream>>>(bp, b, ldb, n, k, kpad);
+  else
+    pack_transpose<<<dim3((n + 31) / 32, (kpad + 31) / 32), 256, 0, stream>>>(
+        bp, b, ldb, n, k, kpad, mask.tab, mask.ldtab, mask.blk);
+  err = cudaGetLastError();
+  CUtensorMap tmA, tmB;
+  if (err == cudaSuccess &&
+      (!make_operand_map(&tmA, ap, m, kpad) || !make_operand_map(&tmB, bp, n, kpad)))
+    err = cudaErrorInvalidValue;
+  if (err == cudaSuccess)
+    err = cudaFuncSetAttribute(dgemm_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(TMA_SMEM));
+  const long long tiles = (long long)((m + BM - 1) / BM) * ((n + BN - 1) / BN);
+  const int nsm = sm_count();
+  const int kall = (k + BK - 1) / BK;
+  TailSplit ts{0, 0, nullptr};
+  if (err == cudaSuccess && nsm > 0 && tiles > nsm && tiles % nsm != 0) {
+    const int tail = int(tiles % nsm);
+    const int splits = std::min(nsm / tail, kall / 4);
+    if (splits >= 2) {
+      ts.full = int(tiles - tail);
+      ts.splits = splits;
+      err = cudaMallocAsync(reinterpret_cast<void**>(&ts.ws),
+                            size_t(tail) * splits * BM * BN * sizeof(double), stream);
+      if (err != cudaSuccess) ts.splits = 0;
+    }
+  }
+  if (err == cudaSuccess) {
+    const long long grid = ts.splits ? ts.full + (tiles - ts.full) * ts.splits : tiles;
+    dgemm_tma_kernel<<<unsigned(grid), THREADS, TMA_SMEM, stream>>>(c, m, n, k, ldc, tmA, tmB, ts);
+    err = cudaGetLastError();
+    if (err == cudaSuccess && ts.splits) {
+      dgemm_tail_reduce<<<unsigned(tiles - ts.full), 256, 0, stream>>>(c, ts.ws, m, n, ldc,
+                                                                       ts.full, ts.splits);
+      err = cudaGetLastError();
+    }
+  }
+  if (ts.ws) cudaFreeAsync(ts.ws, stream);
+  const cudaError_t e2 = cudaFreeAsync(ws, stream);
+  return err != cudaSuccess ? err : e2;
+}
+
+// Products from this many flops on use the packed TMA form (the packing costs
+// one pass over A and B); CFGMM_DGEMM_PACK_MIN_FLOPS overrides, < 0 disables.
+bool use_packed(int m, int n, int k) {
+  static const double min_flops = [] {
+    const char* e = std::getenv("CFGMM_DGEMM_PACK_MIN_FLOPS");
+    return e ? std::atof(e) : 2e9;
+  }();
+  return min_flops >= 0 && 2.0 * m * n * k >= min_flops && k >= 2 * BK;
+}
+
 }  // namespace
 
 cudaError_t dgemm_fp64(double* c, const double* a, const double* b, int m, int n, int k,
@@ -337,6 +644,8 @@ cudaError_t dgemm_fp64(double* c, const double* a, const double* b, int m, int n
                        cudaStream_t stream) {
   if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
   const ColMask none{nullptr, 0, 1};
+  if (use_packed(m, n, k))
+    return launch_packed(c, a, b, m, n, k, lda, ldb, ldc, transa, transb, none, stream);
   if (!transa && !transb)
     return launch_t<false, false>(c, a, b, m, n, k, lda, ldb, ldc, none, stream);
   if (!transa && transb)
@@ -351,8 +660,20 @@ cudaError_t dgemm_fp64_non0tab(double* c, const double* a, const double* b, int 
                                const uint8_t* tab, size_t ldtab, int blk, cudaStream_t stream) {
   if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
   const ColMask mask{tab, ldtab, blk};
+  if (use_packed(m, n, k))
+    return launch_packed(c, a, b, m, n, k, lda, ldb, ldc, transa, false, mask, stream);
   if (!transa) return launch_t<false, false>(c, a, b, m, n, k, lda, ldb, ldc, mask, stream);
   return launch_t<true, false>(c, a, b, m, n, k, lda, ldb, ldc, mask, stream);
+}
+
+cudaError_t dgemm_reset_error(cudaStream_t stream) {
+  static const int zero = 0;
+  return cudaMemcpyToSymbolAsync(g_dgemm_error, &zero, sizeof(int), 0, cudaMemcpyHostToDevice,
+                                 stream);
+}
+
+cudaError_t dgemm_read_error(int* code) {
+  return cudaMemcpyFromSymbol(code, g_dgemm_error, sizeof(int));
 }
 
 }  // namespace cfgmm

@@ -16,4 +16,8 @@ cudaError_t dgemm_fp64_non0tab(double* c, const double* a, const double* b, int 
                                size_t lda, size_t ldb, size_t ldc, bool transa,
                                const uint8_t* tab, size_t ldtab, int blk, cudaStream_t stream);
 
+// Sticky error word of the TMA form's bounded waits (0 = none).
+cudaError_t dgemm_reset_error(cudaStream_t stream);
+cudaError_t dgemm_read_error(int* code);
+
 }  // namespace cfgmm
