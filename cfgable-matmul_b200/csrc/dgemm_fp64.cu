@@ -367,15 +367,21 @@ dgemm_tma_kernel(double* __restrict__ c, int m, int n, int k, size_t ldc,
     for (int kk = 0; kk < BK; kk += 8) {
       double2 av[4][2], bv[4];
 #pragma unroll
+      // k pair of this lane: the step at kk % 16 == 0 reads the even 16-byte
+      // chunks of the box row, the next one the odd chunks, so that after the
+      // swizzle (chunk ^ row % 8) the 8 lanes of a quarter warp (rows g, g^1)
+      // hit 8 different chunks.  A and B use the same order of k.
+      const int kp = (kk & 16) + 4 * q + ((kk >> 2) & 2);
+#pragma unroll
       for (int mt = 0; mt < 4; ++mt) {
         const int r = wm * 64 + mt * 16 + g;
-        av[mt][0] = *reinterpret_cast<const double2*>(A_s + tma_off(r, kk + 2 * q));
-        av[mt][1] = *reinterpret_cast<const double2*>(A_s + tma_off(r + 8, kk + 2 * q));
+        av[mt][0] = *reinterpret_cast<const double2*>(A_s + tma_off(r, kp));
+        av[mt][1] = *reinterpret_cast<const double2*>(A_s + tma_off(r + 8, kp));
       }
 #pragma unroll
       for (int nt = 0; nt < 4; ++nt) {
         const int r = wn * 32 + nt * 8 + g;
-        bv[nt] = *reinterpret_cast<const double2*>(B_s + tma_off(r, kk + 2 * q));
+        bv[nt] = *reinterpret_cast<const double2*>(B_s + tma_off(r, kp));
       }
 #pragma unroll
       for (int mt = 0; mt < 4; ++mt)
