@@ -3,24 +3,31 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Headline workload (a "step"): one FP64 DGEMM C(3527x9583) += A(3527x6581) *
+Headline workload (a "step"): one DGEMM C(3527x9583) += A(3527x6581) *
 B(6581x9583), row-major, ld = row length (the reference README's DGEMM,
-README.md:11-17), inputs resident in HBM.  value = 2*m*n*k / step time, summed
-over ranks.  With N > 1 (torchrun, one process per GPU) every rank runs an
-independent replica: the paths run on one GPU and have no exchange step.
+README.md:11-17), inputs resident in HBM, in split precision (Ozaki scheme on
+the INT8 tensor cores, error against FP64 stated in `config`).  value =
+2*m*n*k / step time, summed over ranks.  With N > 1 (torchrun, one process per
+GPU) every rank runs an independent replica: the paths run on one GPU and have
+no exchange step.
 
 Also reported in the same line:
-  * e2e       -- the same metric through the C ABI's host-pointer call
-                 (cfgmm_matmul_anyway_full) on pinned host buffers, the H2D copy
-                 of A, B, C and the D2H copy of C inside the timed region;
-  * roofline  -- achieved FP64 TFLOP/s of the DGEMM kernel (CUDA events on its
-                 stream) over the FP64 tensor-core peak measured in the same run;
+  * fp64      -- the same DGEMM on the FP64 tensor cores (DMMA), with its
+                 roofline against the DMMA peak measured in this run;
+  * e2e       -- the headline metric through the C ABI's host-pointer call
+                 (cfgmm_matmul_ex) on pinned host buffers, the H2D copy of A, B,
+                 C and the D2H copy of C inside the timed region;
+  * roofline  -- the INT8 GEMM phase of the split DGEMM (CUDA events on its
+                 stream) over the INT8 tensor-core peak measured in this run;
   * cpu_baseline -- the oracle (a C++ restatement of the reference's Rust
                  loops; the reference itself cannot be built here) on the host
                  cores, on a bounded row sample of the same DGEMM (rank 0, N=1);
   * aodmao2rho -- the masked AO-DM-AO contraction on the taxol-sized geometric
                  workload (2228 AOs, 16384 points in blocks of 64, 3 DMs, tile
-                 density 0.3) in FP64: effective masked GFLOP/s.
+                 density 0.3), FP64 and split precision;
+  * aodmao2rho_batched -- 256 uneven grid batches in one graph-captured plan;
+  * serving   -- the density server on a Poisson stream of molecules (p50/p99
+                 latency) and saturated (aggregate GFLOP/s).
 
 --impl reference times the oracle port on the host cores on the same config and
 metric (rank 0 only; other ranks exit without work).
@@ -587,7 +594,7 @@ def run_ours(args, ranks: Ranks):
                               "peak_burst": dmma_peak,
                               "frac_of_burst": flops / (fp64_kernel_ms * 1e-3) / 1e12 / dmma_peak,
                               "traffic": profile_traffic("dgemm_fp64_3527x9583x6581"),
-                              "kernel": "dgemm_fp64_kernel<false,false>",
+                              "kernel": "dgemm_tma_kernel (+ packing, tail reduce)",
                               "peak_source": "measured in this run: DMMA m16n8k4 register loop on "
                                              "every SM, sustained (1.5 s of back-to-back "
                                              "launches, second half) for a kernel timed over "
