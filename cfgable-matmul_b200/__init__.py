@@ -125,6 +125,10 @@ def lib() -> ctypes.CDLL:
         L.cfgmm_release_workspace.restype = I
         L.cfgmm_aodmao2rho_dev_noalloc.argtypes = [P, P, P, P, S, S, S, S, S, P, S, S, P]
         L.cfgmm_aodmao2rho_dev_noalloc.restype = I
+        L.cfgmm_aodm_fock.argtypes = aodm_host + [S]
+        L.cfgmm_aodm_fock.restype = I
+        L.cfgmm_aodm_fock_dev.argtypes = [P, P, P, P, S, S, S, S, S, P, S, S, P]
+        L.cfgmm_aodm_fock_dev.restype = I
         L.cfgmm_aodm_plan_create.argtypes = [ctypes.POINTER(P), ctypes.POINTER(_Batch), S, P, S,
                                              S, S, S, I, I, P]
         L.cfgmm_aodm_plan_create.restype = I
@@ -316,6 +320,30 @@ def aodmao2rho_noalloc(rhos, dms, ao_lhs, ao_rhs, strides, shape, nset, tab, ldt
         _dev(rhos, "torch.float64"), _dev(dms, "torch.float64"), _dev(ao_lhs, "torch.float64"),
         _dev(ao_rhs, "torch.float64"), stride_ao, stride_grid, nao, ngrid, nset,
         _dev(tab, "torch.uint8"), ldtab, blksize, _stream_ptr()))
+
+
+def aodm_fock(vs, ws, ao_lhs, ao_rhs, strides, shape, nset, tab, ldtab, blksize=48) -> None:
+    """The Fock-build contraction, the transpose of the AO-DM-AO one on the same
+    layouts and mask: V_s[u,v] += sum_g ao_lhs[u,g] w_s[g] ao_rhs[v,g] over the
+    points g whose block has both u and v active.  ``vs`` (nset, stride_ao,
+    stride_ao) takes D's place, ``ws`` (nset, stride_grid) rho's.  FP64 on the
+    tensor cores; numpy arrays go through host buffers, CUDA tensors run on the
+    current stream.  No counterpart in the reference."""
+    stride_ao, stride_grid = strides
+    nao, ngrid = shape
+    tab = _as_tab(tab)
+    if _is_torch(vs):
+        return _raise(lib().cfgmm_aodm_fock_dev(
+            _dev(vs, "torch.float64"), _dev(ws, "torch.float64"), _dev(ao_lhs, "torch.float64"),
+            _dev(ao_rhs, "torch.float64"), stride_ao, stride_grid, nao, ngrid, nset,
+            _dev(tab, "torch.uint8"), ldtab, blksize, _stream_ptr()))
+    pv, lv = _host(vs, np.float64, True)
+    pw, lw = _host(ws, np.float64)
+    pl, ll = _host(ao_lhs, np.float64)
+    pq, lq = _host(ao_rhs, np.float64)
+    pt, lt = _host(tab, np.uint8)
+    _raise(lib().cfgmm_aodm_fock(pv, lv, pw, lw, pl, ll, pq, lq, stride_ao, stride_grid, nao,
+                                 ngrid, nset, pt, lt, ldtab, blksize))
 
 
 class AodmPlan:

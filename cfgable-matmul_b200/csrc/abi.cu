@@ -374,6 +374,81 @@ int aodm_host(double* rhos, size_t rhos_len, const double* dms, size_t dms_len,
   return CFGMM_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Fock-build contraction (the transpose of AO-DM-AO): V_s += phi_lhs diag(w_s) phi_rhs^T
+// over the AO pairs active in each block.  Same layouts as AO-DM-AO, with the
+// weights w in rho's place and V in D's place.
+// ---------------------------------------------------------------------------
+int check_fock(double* vs, size_t vs_len, const double* ws, size_t ws_len, const double* ao_lhs,
+               size_t ao_lhs_len, const double* ao_rhs, size_t ao_rhs_len, size_t stride_ao,
+               size_t stride_grid, size_t nao, size_t ngrid, size_t nset, const uint8_t* tab,
+               size_t tab_len, size_t ldtab, size_t blksize, AodmExtents* ex) {
+  if (nao > 0 && stride_ao < nao)
+    return fail(CFGMM_ERR_INVALID_ARGUMENT, "stride_ao < nao: rows of V would overlap");
+  // w has rho's shape and V has D's: the AO-DM-AO checks cover both
+  const int rc = check_aodm(const_cast<double*>(ws), ws_len, vs, vs_len, ao_lhs, ao_lhs_len,
+                            ao_rhs, ao_rhs_len, stride_ao, stride_grid, nao, ngrid, nset, tab,
+                            tab_len, ldtab, blksize, ex);
+  if (rc != CFGMM_OK && g_last_error.find("slice too short") == 0)
+    g_last_error = "slice too short (in the names of this message, rhos = w and dms = V)" +
+                   g_last_error.substr(std::string("slice too short").size());
+  return rc;
+}
+
+int fock_run(double* d_v, const double* d_w, const double* d_lhs, const double* d_rhs,
+             size_t stride_ao, size_t stride_grid, size_t nao, size_t ngrid, size_t nset,
+             const uint8_t* d_tab, size_t ldtab, size_t blksize, void* ws, cudaStream_t s) {
+  CFGMM_CUDA(cfgmm::dgemm_reset_error(s));
+  for (size_t set = 0; set < nset; ++set)
+    CFGMM_CUDA(cfgmm::fock_fp64(d_v + set * stride_ao * stride_ao, stride_ao,
+                                d_w + set * stride_grid, d_lhs, d_rhs, stride_grid, int(nao),
+                                int(ngrid), d_tab, ldtab, int(blksize), set == 0, ws, s));
+  return CFGMM_OK;
+}
+
+int fock_host(double* vs, size_t vs_len, const double* ws, size_t ws_len, const double* ao_lhs,
+              size_t ao_lhs_len, const double* ao_rhs, size_t ao_rhs_len, size_t stride_ao,
+              size_t stride_grid, size_t nao, size_t ngrid, size_t nset, const uint8_t* tab,
+              size_t tab_len, size_t ldtab, size_t blksize) {
+  g_last_error.clear();
+  AodmExtents ex;
+  int rc = check_fock(vs, vs_len, ws, ws_len, ao_lhs, ao_lhs_len, ao_rhs, ao_rhs_len, stride_ao,
+                      stride_grid, nao, ngrid, nset, tab, tab_len, ldtab, blksize, &ex);
+  if (rc != CFGMM_OK) return rc;
+  if (ex.rhos == 0) return CFGMM_OK;
+  int dev;
+  if ((rc = current_device(&dev)) != CFGMM_OK) return rc;
+  DeviceState* st = device_state(dev);
+  std::lock_guard<std::mutex> lk(st->mu);
+  const bool same_ao = ao_lhs == ao_rhs;
+  const size_t o_w = 0;
+  const size_t o_lhs = o_w + align256(ex.rhos * 8);
+  const size_t o_rhs = o_lhs + align256(ex.ao * 8);
+  const size_t o_tab = o_rhs + (same_ao ? 0 : align256(ex.ao * 8));
+  const size_t o_v = o_tab + align256(ex.tab);
+  const size_t o_ws = o_v + align256(ex.dms * 8);
+  if ((rc = reserve(st, o_ws + cfgmm::fock_fp64_workspace(int(nao), int(ngrid)))) != CFGMM_OK)
+    return rc;
+  char* base = static_cast<char*>(st->buf);
+  double* d_w = reinterpret_cast<double*>(base + o_w);
+  double* d_lhs = reinterpret_cast<double*>(base + o_lhs);
+  double* d_rhs = reinterpret_cast<double*>(base + o_rhs);
+  uint8_t* d_tab = reinterpret_cast<uint8_t*>(base + o_tab);
+  double* d_v = reinterpret_cast<double*>(base + o_v);
+  CFGMM_CUDA(cudaMemcpyAsync(d_w, ws, ex.rhos * 8, cudaMemcpyHostToDevice, st->stream));
+  CFGMM_CUDA(cudaMemcpyAsync(d_lhs, ao_lhs, ex.ao * 8, cudaMemcpyHostToDevice, st->stream));
+  if (!same_ao)
+    CFGMM_CUDA(cudaMemcpyAsync(d_rhs, ao_rhs, ex.ao * 8, cudaMemcpyHostToDevice, st->stream));
+  CFGMM_CUDA(cudaMemcpyAsync(d_tab, tab, ex.tab, cudaMemcpyHostToDevice, st->stream));
+  CFGMM_CUDA(cudaMemcpyAsync(d_v, vs, ex.dms * 8, cudaMemcpyHostToDevice, st->stream));
+  if ((rc = fock_run(d_v, d_w, d_lhs, same_ao ? d_lhs : d_rhs, stride_ao, stride_grid, nao, ngrid,
+                     nset, d_tab, ldtab, blksize, base + o_ws, st->stream)) != CFGMM_OK)
+    return rc;
+  CFGMM_CUDA(cudaMemcpyAsync(vs, d_v, ex.dms * 8, cudaMemcpyDeviceToHost, st->stream));
+  CFGMM_CUDA(cudaStreamSynchronize(st->stream));
+  return check_device_waits();
+}
+
 }  // namespace
 
 namespace cfgmm {
@@ -673,6 +748,38 @@ int cfgmm_mask_ao_dev(double* ao, size_t stride_grid, size_t ngrid, const int* s
   CFGMM_CUDA(cfgmm::mask_ao(ao, stride_grid, int(ngrid), shell_l, shell_row, int(nshell),
                             shell_block_max, threshold, tab, ldtab, int(blksize),
                             static_cast<cudaStream_t>(stream)));
+  return CFGMM_OK;
+}
+
+int cfgmm_aodm_fock(double* vs, size_t vs_len, const double* ws, size_t ws_len,
+                    const double* ao_lhs, size_t ao_lhs_len, const double* ao_rhs,
+                    size_t ao_rhs_len, size_t stride_ao, size_t stride_grid, size_t nao,
+                    size_t ngrid, size_t nset, const uint8_t* tab, size_t tab_len, size_t ldtab,
+                    size_t blksize) {
+  return fock_host(vs, vs_len, ws, ws_len, ao_lhs, ao_lhs_len, ao_rhs, ao_rhs_len, stride_ao,
+                   stride_grid, nao, ngrid, nset, tab, tab_len, ldtab, blksize);
+}
+
+int cfgmm_aodm_fock_dev(double* vs, const double* ws, const double* ao_lhs, const double* ao_rhs,
+                        size_t stride_ao, size_t stride_grid, size_t nao, size_t ngrid,
+                        size_t nset, const uint8_t* tab, size_t ldtab, size_t blksize,
+                        void* stream) {
+  g_last_error.clear();
+  AodmExtents ex;
+  int rc = check_fock(vs, SIZE_MAX, ws, SIZE_MAX, ao_lhs, SIZE_MAX, ao_rhs, SIZE_MAX, stride_ao,
+                      stride_grid, nao, ngrid, nset, tab, SIZE_MAX, ldtab, blksize, &ex);
+  if (rc != CFGMM_OK) return rc;
+  if (ex.rhos == 0) return CFGMM_OK;
+  int dev;
+  if ((rc = current_device(&dev)) != CFGMM_OK) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  void* work = nullptr;
+  CFGMM_CUDA(cudaMallocAsync(&work, cfgmm::fock_fp64_workspace(int(nao), int(ngrid)), s));
+  rc = fock_run(vs, ws, ao_lhs, ao_rhs, stride_ao, stride_grid, nao, ngrid, nset, tab, ldtab,
+                blksize, work, s);
+  const cudaError_t e2 = cudaFreeAsync(work, s);
+  if (rc != CFGMM_OK) return rc;
+  if (e2 != cudaSuccess) return cuda_fail(e2, "cudaFreeAsync");
   return CFGMM_OK;
 }
 

@@ -430,6 +430,157 @@ dgemm_tma_kernel(double* __restrict__ c, int m, int n, int k, size_t ldc,
     }
 }
 
+// The TMA kernel with K-step activity maps (act_m: [tiles_m][ksteps], act_n:
+// [tiles_n][ksteps], nonzero = the tile has a nonzero operand row in that K
+// step): a CTA runs only the K steps active for both of its tiles.  No K split.
+__global__ void __launch_bounds__(THREADS, 1)
+dgemm_tma_act_kernel(double* __restrict__ c, int m, int n, int k, size_t ldc,
+                     const __grid_constant__ CUtensorMap tmA,
+                     const __grid_constant__ CUtensorMap tmB, const uint8_t* __restrict__ act_m,
+                     const uint8_t* __restrict__ act_n) {
+  const TailSplit tail{0, 0, nullptr};
+  extern __shared__ uint8_t tsmem_raw[];
+  uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(tsmem_raw) + 1023) &
+                                           ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm + STAGES * TSTAGE);
+  int* err = &g_dgemm_error;
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 2, wn = warp & 3;  // 2 x 4 warp grid
+  const int g = lane >> 2, q = lane & 3;
+
+  const int tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
+  const bool split = tail.splits > 0 && int(blockIdx.x) >= tail.full;
+  const int job = split ? int(blockIdx.x) - tail.full : 0;
+  const int tile = split ? tail.full + job / tail.splits : int(blockIdx.x);
+  const int per_group = GROUP_M * tiles_n;
+  const int group = tile / per_group;
+  const int first_m = group * GROUP_M;
+  const int gsz = min(tiles_m - first_m, GROUP_M);
+  const int in_group = tile % per_group;
+  const int m0 = (first_m + in_group % gsz) * BM;
+  const int n0 = (in_group / gsz) * BN;
+  const int kall = (k + BK - 1) / BK;
+  const int sidx = split ? job % tail.splits : 0;
+  const int kt0 = split ? int((long long)sidx * kall / tail.splits) : 0;
+  const int kt1 = split ? int((long long)(sidx + 1) * kall / tail.splits) : kall;
+
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; ++s) tc::mbar_init(&full[s], 1);
+    tc::mbar_fence_init();
+    tc::prefetch_tensormap(&tmA);
+    tc::prefetch_tensormap(&tmB);
+  }
+  __syncthreads();
+  const uint8_t* am = act_m + size_t(m0 / BM) * kall;
+  const uint8_t* an = act_n + size_t(n0 / BN) * kall;
+  auto next = [&](int kt) {  // first K step >= kt that this CTA runs
+    while (kt < kt1 && !(am[kt] && an[kt])) ++kt;
+    return kt;
+  };
+  auto issue = [&](int kt, int s) {  // thread 0: both operand tiles of K step kt into stage s
+    uint8_t* st = sm + s * TSTAGE;
+    tc::mbar_arrive_expect_tx(&full[s], TSTAGE);
+    tma_load_2d(st, &tmA, &full[s], kt * BK, m0);
+    tma_load_2d(st + BOX_BYTES, &tmA, &full[s], kt * BK + 16, m0);
+    tma_load_2d(st + OP_BYTES, &tmB, &full[s], kt * BK, n0);
+    tma_load_2d(st + OP_BYTES + BOX_BYTES, &tmB, &full[s], kt * BK + 16, n0);
+  };
+  // steps are consumed in order: the i-th one issued goes to stage i % STAGES
+  int kiss = next(kt0), nissued = 0;
+  for (; nissued < STAGES - 1 && kiss < kt1; ++nissued, kiss = next(kiss + 1))
+    if (tid == 0) issue(kiss, nissued % STAGES);
+
+  double acc[4][4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
+
+  bool ok = true;
+  int ncons = 0;
+  for (int kt = next(kt0); kt < kt1; kt = next(kt + 1), ++ncons) {
+    __syncthreads();  // every warp is done with the previous step: its stage can be refilled
+    if (kiss < kt1) {
+      if (tid == 0) issue(kiss, nissued % STAGES);
+      ++nissued;
+      kiss = next(kiss + 1);
+    }
+    const int s = ncons % STAGES;
+    if (!tc::mbar_wait(&full[s], (ncons / STAGES) & 1, err, 51)) {
+      ok = false;
+      break;
+    }
+    const double* A_s = reinterpret_cast<const double*>(sm + s * TSTAGE);
+    const double* B_s = reinterpret_cast<const double*>(sm + s * TSTAGE + OP_BYTES);
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 8) {
+      double2 av[4][2], bv[4];
+#pragma unroll
+      // k pair of this lane: the step at kk % 16 == 0 reads the even 16-byte
+      // chunks of the box row, the next one the odd chunks, so that after the
+      // swizzle (chunk ^ row % 8) the 8 lanes of a quarter warp (rows g, g^1)
+      // hit 8 different chunks.  A and B use the same order of k.
+      const int kp = (kk & 16) + 4 * q + ((kk >> 2) & 2);
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt) {
+        const int r = wm * 64 + mt * 16 + g;
+        av[mt][0] = *reinterpret_cast<const double2*>(A_s + tma_off(r, kp));
+        av[mt][1] = *reinterpret_cast<const double2*>(A_s + tma_off(r + 8, kp));
+      }
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const int r = wn * 32 + nt * 8 + g;
+        bv[nt] = *reinterpret_cast<const double2*>(B_s + tma_off(r, kp));
+      }
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+          dmma_16x8x8(acc[mt][nt], av[mt][0].x, av[mt][1].x, av[mt][0].y, av[mt][1].y, bv[nt].x,
+                      bv[nt].y);
+    }
+  }
+  if (!ok) {  // the copies issued and not consumed land before the CTA exits
+    if (tid == 0)
+      for (int i = ncons; i < nissued; ++i)
+        tc::mbar_wait(&full[i % STAGES], (i / STAGES) & 1, err, 52, true);
+    return;
+  }
+
+  if (split) {  // the partial tile, dense 128 x 128, to the workspace
+    double* w = tail.ws + size_t(job) * (BM * BN);
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = wm * 64 + mt * 16 + g + 8 * h;
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+          *reinterpret_cast<double2*>(w + r * BN + wn * 32 + nt * 8 + 2 * q) =
+              make_double2(acc[mt][nt][2 * h], acc[mt][nt][2 * h + 1]);
+      }
+    return;
+  }
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int row = m0 + wm * 64 + mt * 16 + g + 8 * h;
+      if (row >= m) continue;
+      double* crow = c + size_t(row) * ldc;
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const int col = n0 + wn * 32 + nt * 8 + 2 * q;
+        if (col < n) crow[col] += acc[mt][nt][2 * h];
+        if (col + 1 < n) crow[col + 1] += acc[mt][nt][2 * h + 1];
+      }
+    }
+}
+
 // dst[r][kk] = src[r * ld + kk] (kk < k), 0 for k <= kk < kpad: rows of a
 // K-contiguous operand.  A warp per row, 256 columns per block.
 __global__ void __launch_bounds__(256)
@@ -632,6 +783,93 @@ cudaError_t launch_packed(double* c, const double* a, const double* b, int m, in
   const cudaError_t e2 = cudaFreeAsync(ws, stream);
   return err != cudaSuccess ? err : e2;
 }
+
+// ---------------------------------------------------------------------------
+// Fock-build contraction V[u][v] += sum_g phi_lhs[u][g] w[g] phi_rhs[v][g] over
+// the u, v active in g's block: a product of the masked (and, on the left,
+// weighted) operands packed K-contiguous, K = grid points, run by the TMA
+// kernel with its K-step activity maps.
+// ---------------------------------------------------------------------------
+// dst[u][g] = tab[u][g / blk] ? src[u][g] * (w ? w[g] : 1) : 0 for g < ngrid, 0
+// up to kpad.  A warp per row, 256 points per block.
+__global__ void __launch_bounds__(256)
+pack_masked(double* __restrict__ dst, const double* __restrict__ src, size_t ld, int rows,
+            int ngrid, int kpad, const uint8_t* __restrict__ tab, size_t ldtab, int blk,
+            const double* __restrict__ w) {
+  const int r = blockIdx.y * 8 + (threadIdx.x >> 5);
+  if (r >= rows) return;
+  const double* srow = src + size_t(r) * ld;
+  const uint8_t* trow = tab + size_t(r) * ldtab;
+  double* drow = dst + size_t(r) * kpad;
+  for (int j = threadIdx.x & 31; j < 256; j += 32) {
+    const int g = blockIdx.x * 256 + j;
+    if (g >= kpad) continue;
+    double v = 0.0;
+    if (g < ngrid && trow[g / blk]) v = w ? srow[g] * w[g] : srow[g];
+    drow[g] = v;
+  }
+}
+
+// act[t][kt] = some AO of 128-row tile t is active in a block that K step kt
+// (points 32kt .. 32kt+31) touches.
+__global__ void __launch_bounds__(256)
+tile_activity(uint8_t* __restrict__ act, const uint8_t* __restrict__ tab, size_t ldtab, int nao,
+              int ngrid, int blk, int ksteps) {
+  const int t = blockIdx.y;
+  for (int kt = blockIdx.x * 256 + threadIdx.x; kt < ksteps; kt += gridDim.x * 256) {
+    const int g0 = kt * BK, g1 = min(ngrid, g0 + BK) - 1;
+    const int b0 = g0 / blk, b1 = g1 / blk;
+    uint8_t any = 0;
+    for (int u = t * BM; u < min(nao, t * BM + BM) && !any; ++u)
+      for (int b = b0; b <= b1; ++b) any |= tab[size_t(u) * ldtab + b];
+    act[size_t(t) * ksteps + kt] = any ? 1 : 0;
+  }
+}
+
+}  // namespace
+
+size_t fock_fp64_workspace(int nao, int ngrid) {
+  const size_t kpad = (size_t(ngrid) + 7) / 8 * 8;
+  const size_t tiles = (size_t(nao) + BM - 1) / BM, ksteps = (size_t(ngrid) + BK - 1) / BK;
+  return 2 * size_t(nao) * kpad * sizeof(double) + (tiles * ksteps + 255) / 256 * 256 + 256;
+}
+
+cudaError_t fock_fp64(double* v, size_t ldv, const double* w, const double* ao_lhs,
+                      const double* ao_rhs, size_t stride_grid, int nao, int ngrid,
+                      const uint8_t* tab, size_t ldtab, int blk, bool pack_rhs, void* workspace,
+                      cudaStream_t stream) {
+  if (nao <= 0 || ngrid <= 0) return cudaSuccess;
+  const int kpad = (ngrid + 7) / 8 * 8;
+  const int ksteps = (ngrid + BK - 1) / BK;
+  const int tiles = (nao + BM - 1) / BM;
+  double* ap = static_cast<double*>(workspace);
+  double* bp = ap + size_t(nao) * kpad;
+  uint8_t* act = reinterpret_cast<uint8_t*>(bp + size_t(nao) * kpad);
+  const dim3 pgrid((kpad + 255) / 256, (nao + 7) / 8);
+  pack_masked<<<pgrid, 256, 0, stream>>>(ap, ao_lhs, stride_grid, nao, ngrid, kpad, tab, ldtab,
+                                         blk, w);
+  if (pack_rhs) {  // the right operand and the activity map change only with phi and the mask
+    pack_masked<<<pgrid, 256, 0, stream>>>(bp, ao_rhs, stride_grid, nao, ngrid, kpad, tab, ldtab,
+                                           blk, nullptr);
+    tile_activity<<<dim3((ksteps + 255) / 256, tiles), 256, 0, stream>>>(act, tab, ldtab, nao,
+                                                                         ngrid, blk, ksteps);
+  }
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return err;
+  CUtensorMap tmA, tmB;
+  if (!make_operand_map(&tmA, ap, nao, kpad) || !make_operand_map(&tmB, bp, nao, kpad))
+    return cudaErrorInvalidValue;
+  if ((err = cudaFuncSetAttribute(dgemm_tma_act_kernel,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, int(TMA_SMEM))) !=
+      cudaSuccess)
+    return err;
+  const long long ntiles = (long long)tiles * tiles;
+  dgemm_tma_act_kernel<<<unsigned(ntiles), THREADS, TMA_SMEM, stream>>>(v, nao, nao, ngrid, ldv,
+                                                                        tmA, tmB, act, act);
+  return cudaGetLastError();
+}
+
+namespace {
 
 // Products from this many flops on use the packed TMA form (the packing costs
 // one pass over A and B); CFGMM_DGEMM_PACK_MIN_FLOPS overrides, < 0 disables.

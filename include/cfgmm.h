@@ -219,6 +219,26 @@ int cfgmm_aodmao2rho_dev_noalloc(double* rhos, const double* dms, const double* 
                                  size_t nao, size_t ngrid, size_t nset, const uint8_t* tab,
                                  size_t ldtab, size_t blksize, void* stream);
 
+/* ---- the step after the contraction: the Fock-build (V) contraction ------
+ * No counterpart in the reference (its DFT callers build V themselves); the
+ * transpose of AO-DM-AO with the same layouts and mask:
+ *   vs[s*stride_ao^2 + u*stride_ao + v] += sum over g with tab[u][g/BLK] and
+ *       tab[v][g/BLK] of ao_lhs[u][g] * ws[s*stride_grid + g] * ao_rhs[v][g]
+ * for s < nset, u, v < nao (stride_ao >= nao).  Outputs are accumulated into.
+ * FP64 on the tensor cores: the masked, weighted operands are packed with K =
+ * grid points and K steps in which a 128-AO tile has no active AO are skipped.
+ * Slices too short, BLKSIZE 0 or overlapping V rows are rejected as in the
+ * AO-DM-AO calls. */
+int cfgmm_aodm_fock(double* vs, size_t vs_len, const double* ws, size_t ws_len,
+                    const double* ao_lhs, size_t ao_lhs_len, const double* ao_rhs,
+                    size_t ao_rhs_len, size_t stride_ao, size_t stride_grid, size_t nao,
+                    size_t ngrid, size_t nset, const uint8_t* tab, size_t tab_len, size_t ldtab,
+                    size_t blksize);
+int cfgmm_aodm_fock_dev(double* vs, const double* ws, const double* ao_lhs, const double* ao_rhs,
+                        size_t stride_ao, size_t stride_grid, size_t nao, size_t ngrid,
+                        size_t nset, const uint8_t* tab, size_t ldtab, size_t blksize,
+                        void* stream);
+
 /* ---- batched plans: many grid batches of one molecule in one launch ------
  * No counterpart in the reference (whose callers batch grids themselves,
  * impl_matmul.rs:354-355): a plan holds device pointers to every batch's phi

@@ -36,6 +36,9 @@
 //   * aodmao2rho_loop_2nd (per-block compaction and skip)       src/impl_aodmao2rho.rs:97-169
 //   * aodmao2rho_loop_parallel (u->g->v task order)             src/impl_aodmao2rho.rs:171-244
 //   * aodmao2rho_anyway tuning, BLKSIZE 48                      src/impl_aodmao2rho.rs:247-261
+//   * the Fock-build contraction (V += phi_lhs diag(w) phi_rhs^T over the pairs
+//     active in each block), the transpose of aodmao2rho on its layouts and mask;
+//     the reference has no such function, so it is written from the formula.
 //
 // rayon's `into_par_iter` + AtomicUsize task counter become an OpenMP parallel
 // loop that draws task ids from a std::atomic counter; the per-tile
@@ -47,6 +50,7 @@
 // Panics of the reference (slice out of bounds, `unimplemented!` for a masked
 // transb, `assert!(NC % BLKSIZE == 0)`) become a negative return code.
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdint>
@@ -371,6 +375,39 @@ int oracle_aodmao2rho(double* rhos, const double* dms, const double* ao_lhs, con
   if (blksize == 0 || blksize % 16 != 0) return kInvalid;
   Anyway::aodmao2rho(rhos, dms, ao_lhs, ao_rhs, stride_ao, stride_grid, nao, ngrid, nset, tab,
                      ldtab, blksize, nc_for_blk(blksize), resolve_threads(nthreads));
+  return kOk;
+}
+
+// Fock-build contraction, the transpose of aodmao2rho with the same layouts
+// and mask (no counterpart in the reference, whose DFT callers form V
+// themselves):  vs[s][u][v] += sum over blocks b with tab[u][b] && tab[v][b] of
+// sum_{g in b} (ao_lhs[u][g] * ws[s][g]) * ao_rhs[v][g], one FMA per point in
+// ascending g.  Rows u are independent, so any thread count gives the same bits.
+int oracle_aodm_fock(double* vs, const double* ws, const double* ao_lhs, const double* ao_rhs,
+                     size_t stride_ao, size_t stride_grid, size_t nao, size_t ngrid, size_t nset,
+                     const uint8_t* tab, size_t ldtab, size_t blksize, int nthreads) {
+  if (blksize == 0 || (nao > 0 && stride_ao < nao)) return kInvalid;
+  const size_t nblk = (ngrid + blksize - 1) / blksize;
+  for (size_t s = 0; s < nset; ++s) {
+    double* v = vs + s * stride_ao * stride_ao;
+    const double* w = ws + s * stride_grid;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(resolve_threads(nthreads))
+    for (long long uu = 0; uu < (long long)nao; ++uu) {
+      const size_t u = size_t(uu);
+      std::vector<double> lw(ngrid);
+      for (size_t g = 0; g < ngrid; ++g) lw[g] = ao_lhs[u * stride_grid + g] * w[g];
+      for (size_t vv = 0; vv < nao; ++vv) {
+        double acc = 0.0;
+        for (size_t b = 0; b < nblk; ++b) {
+          if (!tab[u * ldtab + b] || !tab[vv * ldtab + b]) continue;
+          const size_t g1 = std::min(ngrid, (b + 1) * blksize);
+          for (size_t g = b * blksize; g < g1; ++g)
+            acc = std::fma(lw[g], ao_rhs[vv * stride_grid + g], acc);
+        }
+        v[u * stride_ao + vv] += acc;
+      }
+    }
+  }
   return kOk;
 }
 

@@ -58,6 +58,8 @@ def lib() -> ctypes.CDLL:
         L.oracle_matmul_anyway_full_non0tab.restype = I
         L.oracle_aodmao2rho.argtypes = [P, P, P, P] + [S] * 5 + [P, S, S, I]
         L.oracle_aodmao2rho.restype = I
+        L.oracle_aodm_fock.argtypes = [P, P, P, P] + [S] * 5 + [P, S, S, I]
+        L.oracle_aodm_fock.restype = I
         L.oracle_max_threads.restype = I
         _lib = L
     return _lib
@@ -118,3 +120,20 @@ def aodmao2rho(rhos, dms, ao_lhs, ao_rhs, strides, shape, nset, tab, ldtab, blks
                                  nthreads)
     if rc != 0:
         raise ValueError(f"oracle_aodmao2rho returned {rc}")
+
+
+def aodm_fock(vs, ws, ao_lhs, ao_rhs, strides, shape, nset, tab, ldtab, blksize=48,
+              nthreads=0) -> None:
+    """V_s[u,v] += sum over g in blocks where u and v are both active of
+    ao_lhs[u,g] w_s[g] ao_rhs[v,g]: the transpose of aodmao2rho on the same
+    layouts and mask, written from that formula."""
+    for x in (vs, ws, ao_lhs, ao_rhs):
+        _check(x, np.float64)
+    _check(tab, np.uint8)
+    stride_ao, stride_grid = strides
+    nao, ngrid = shape
+    rc = lib().oracle_aodm_fock(_ptr(vs), _ptr(ws), _ptr(ao_lhs), _ptr(ao_rhs), stride_ao,
+                                stride_grid, nao, ngrid, nset, _ptr(tab), ldtab, blksize,
+                                nthreads)
+    if rc != 0:
+        raise ValueError(f"oracle_aodm_fock returned {rc}")

@@ -125,6 +125,25 @@ def test_aodm_zero_sizes_are_noops(cm):
     assert np.all(rho == 0)
 
 
+def test_fock_validation(cm):
+    """The Fock-build call takes V in D's place and w in rho's: the same checks."""
+    w, v, ao, tab, nblk = _aodm_args()
+    with pytest.raises(ValueError, match="slice too short"):
+        cm.aodm_fock(v[:1], w, ao, ao, (10, 100), (10, 100), 2, tab, nblk)
+    with pytest.raises(ValueError, match="slice too short"):
+        cm.aodm_fock(v, w[:1], ao, ao, (10, 100), (10, 100), 2, tab, nblk)
+    with pytest.raises(ValueError, match="slice too short"):
+        cm.aodm_fock(v, w, ao, ao, (10, 100), (10, 100), 2, tab[:5], nblk)
+    with pytest.raises(ValueError, match="stride_ao"):
+        cm.aodm_fock(v, w, ao, ao, (5, 100), (10, 100), 2, tab, nblk)
+    with pytest.raises(ValueError, match="BLKSIZE"):
+        cm.aodm_fock(v, w, ao, ao, (10, 100), (10, 100), 2, tab, nblk, blksize=0)
+    cm.aodm_fock(v, w, ao, ao, (10, 100), (0, 100), 2, tab, nblk)  # empty: no device needed
+    cm.aodm_fock(v, w, ao, ao, (10, 100), (10, 0), 2, tab, nblk)
+    cm.aodm_fock(v, w, ao, ao, (10, 100), (10, 100), 0, tab, nblk)
+    assert np.all(v == 1)
+
+
 def test_bool_mask_is_accepted(cm):
     rho, dms, ao, tab, nblk = _aodm_args()
     with pytest.raises(ValueError, match="slice too short"):
@@ -142,6 +161,9 @@ def test_no_cpu_fallback_without_device(cm):
     with pytest.raises(cm.CfgmmError):
         cm.aodmao2rho_anyway(rho, dms, ao, ao, (10, 100), (10, 100), 2, tab, nblk)
     assert np.all(c == 0) and np.all(rho == 0)
+    with pytest.raises(cm.CfgmmError):
+        cm.aodm_fock(dms, rho, ao, ao, (10, 100), (10, 100), 2, tab, nblk)
+    assert np.all(dms == 1)
     with pytest.raises(cm.CfgmmError) as e:
         cm.Server(1 << 30)
     assert e.value.status == -4

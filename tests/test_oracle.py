@@ -122,3 +122,58 @@ def test_generators_shapes(wl):
     mask = wl.expand_mask(p.tab, p.ngrid, p.blksize)
     assert np.all(p.ao[~mask] == 0.0)
     assert abs(p.tab.astype(float).mean() - 0.3) < 0.1
+
+
+def _python_fock(lhs, rhs, ws, tab, blk):
+    """V_s[u,v] = sum over g with u and v active in g's block of lhs[u,g] w_s[g] rhs[v,g]."""
+    nao, ngrid = lhs.shape
+    vs = np.zeros((ws.shape[0], nao, nao))
+    for s in range(ws.shape[0]):
+        for g in range(ngrid):
+            idx = [u for u in range(nao) if tab[u, g // blk]]
+            for u in idx:
+                for v in idx:
+                    vs[s, u, v] += lhs[u, g] * ws[s, g] * rhs[v, g]
+    return vs
+
+
+@pytest.mark.parametrize("blk", [16, 48, 100])
+def test_oracle_fock_matches_python_loops(oracle, blk):
+    rng = np.random.default_rng(100 + blk)
+    nao, ngrid, nset = 19, 203, 2
+    nblk = -(-ngrid // blk)
+    lhs = rng.standard_normal((nao, ngrid))
+    rhs = rng.standard_normal((nao, ngrid))  # nonzero where masked: the mask must exclude them
+    ws = rng.uniform(0, 1, (nset, ngrid))
+    tab = (rng.random((nao, nblk)) < 0.5).astype(np.uint8)
+    tab[:, -1] = 0
+    vs = np.zeros((nset, nao, nao))
+    oracle.aodm_fock(vs, ws, lhs, rhs, (nao, ngrid), (nao, ngrid), nset, tab, nblk, blk)
+    assert normwise(vs, _python_fock(lhs, rhs, ws, tab, blk)) < 1e-14
+
+
+def test_oracle_fock_is_the_adjoint_of_aodmao2rho(oracle, wl):
+    """sum_uv V(w)[u,v] D[u,v] == sum_g w[g] rho(D)[g] on the same phi and mask."""
+    p = wl.small_masked(seed=5, nao=96, ngrid=960, nset=1)
+    rng = np.random.default_rng(5)
+    w = rng.uniform(0, 1, (1, p.ngrid))
+    rho = np.zeros((1, p.ngrid))
+    oracle.aodmao2rho(rho, p.dms, p.ao, p.ao, (p.nao, p.ngrid), (p.nao, p.ngrid), 1, p.tab,
+                      p.nblk, p.blksize)
+    v = np.zeros((1, p.nao, p.nao))
+    oracle.aodm_fock(v, w, p.ao, p.ao, (p.nao, p.ngrid), (p.nao, p.ngrid), 1, p.tab, p.nblk,
+                     p.blksize)
+    lhs, rhs = float(np.sum(v * p.dms)), float(np.sum(w * rho))
+    assert abs(lhs - rhs) <= 1e-12 * max(1.0, abs(rhs))
+
+
+def test_oracle_fock_threads_bitwise(oracle, wl):
+    p = wl.small_masked(seed=6, nao=136, ngrid=700, nset=2)
+    ws = np.random.default_rng(6).uniform(0, 1, (p.nset, p.ngrid))
+    v1 = np.ones((p.nset, p.nao + 3, p.nao + 3))  # padded rows, accumulated into
+    v8 = v1.copy()
+    for v, nt in ((v1, 1), (v8, 0)):
+        oracle.aodm_fock(v, ws, p.ao, p.ao, (p.nao + 3, p.ngrid), (p.nao, p.ngrid), p.nset,
+                         p.tab, p.nblk, p.blksize, nthreads=nt)
+    assert np.array_equal(v1, v8)
+    assert np.all(v1[:, p.nao:, :] == 1.0) and np.all(v1[:, :, p.nao:] == 1.0)
