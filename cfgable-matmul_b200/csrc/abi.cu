@@ -178,12 +178,14 @@ int check_split_gemm(size_t k) {
 
 // Reads the sticky error words of the tcgen05 kernels after a synchronised call.
 int check_device_waits() {
-  int code = 0, code2 = 0, code3 = 0;
+  int code = 0, code2 = 0, code3 = 0, code4 = 0;
   CFGMM_CUDA(cfgmm::gemm_i8_read_error(&code));
   CFGMM_CUDA(cfgmm::aodmao2rho_split_read_error(&code2));
   CFGMM_CUDA(cfgmm::dgemm_read_error(&code3));
+  CFGMM_CUDA(cfgmm::aodm_read_error(&code4));
   if (code == 0) code = code2;
   if (code == 0) code = code3;
+  if (code == 0) code = code4;
   if (code != 0) {
     char msg[128];
     std::snprintf(msg, sizeof(msg), "a tensor-core pipeline wait timed out (code %d)", code);
@@ -371,6 +373,13 @@ int aodm_host(double* rhos, size_t rhos_len, const double* dms, size_t dms_len,
   CFGMM_CUDA(cudaMemcpyAsync(rhos, d_rho, ex.rhos * 8, cudaMemcpyDeviceToHost, st->stream));
   CFGMM_CUDA(cudaStreamSynchronize(st->stream));
   if (split) return check_device_waits();
+  int code = 0;
+  CFGMM_CUDA(cfgmm::aodm_read_error(&code));
+  if (code != 0) {
+    char msg[128];
+    std::snprintf(msg, sizeof(msg), "a pipeline wait of the FP64 kernel timed out (code %d)", code);
+    return fail(CFGMM_ERR_TIMEOUT, msg);
+  }
   return CFGMM_OK;
 }
 

@@ -421,10 +421,11 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
   const size_t o_pairs = o_items + a256(slots * sizeof(int4));
   const size_t o_ctr = o_pairs + a256(cnt_n * gsub * sizeof(int2));
   const size_t o_part = o_ctr + a256((nset_max + 1) * sizeof(int));
+  const size_t o_maps = o_part + a256(slots * nset_max * TG * sizeof(double));
   // split precision keeps only the active lists here (its own layout follows)
   const size_t bytes = precision == CFGMM_PREC_OZAKI_INT8
                            ? o_batch
-                           : o_part + slots * nset_max * TG * sizeof(double);
+                           : o_maps + nbatch * sizeof(CUtensorMap);
   cudaError_t err = cudaMallocAsync(&plan->mem, bytes, s);
   if (err != cudaSuccess) return cleanup(cuda_fail(err, "cudaMalloc(plan)"));
   char* base = static_cast<char*>(plan->mem);
@@ -480,6 +481,12 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
   }
   std::stable_sort(items.begin(), items.end(),
                    [](const int4& x, const int4& y) { return x.w > y.w; });
+  // ao_rhs gather maps of the pipelined form, if every batch allows TMA
+  std::vector<CUtensorMap> maps(nbatch);
+  bool pipe_ok = true;
+  for (size_t i = 0; i < nbatch && pipe_ok; ++i)
+    pipe_ok = cfgmm::aodm_rhs_map(&maps[i], batches[i].ao_rhs, batches[i].stride_grid, int(nao),
+                                  int(batches[i].ngrid), int(blksize));
   plan->nitems = int(items.size());
   plan->npairs = int(pairs.size());
   plan->rpairs = reinterpret_cast<int2*>(base + o_pairs);
@@ -490,6 +497,9 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
                           cudaMemcpyHostToDevice, s);
   if (err == cudaSuccess && !pairs.empty())
     err = cudaMemcpyAsync(plan->rpairs, pairs.data(), pairs.size() * sizeof(int2),
+                          cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess && pipe_ok)
+    err = cudaMemcpyAsync(base + o_maps, maps.data(), nbatch * sizeof(CUtensorMap),
                           cudaMemcpyHostToDevice, s);
   if (err != cudaSuccess) return cleanup(cuda_fail(err, "plan upload"));
 
@@ -503,6 +513,7 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
   a.max_utiles = max_ut;
   a.nset_max = int(nset_max);
   a.batches = reinterpret_cast<const cfgmm::AodmBatch*>(base + o_batch);
+  a.rhs_maps = pipe_ok ? reinterpret_cast<const CUtensorMap*>(base + o_maps) : nullptr;
   a.items = reinterpret_cast<const int4*>(base + o_items);
   a.counters = reinterpret_cast<int*>(base + o_ctr);
   a.partial = reinterpret_cast<double*>(base + o_part);
@@ -539,17 +550,20 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
     return e;
   };
   char key[256];
-  std::snprintf(key, sizeof(key), "aodm_fp64:nao%d:work%d:items%d:nset%zu:blk%zu", bucket(double(nao)),
-                bucket(work), bucket(double(plan->nitems)), nset_max, blksize);
+  std::snprintf(key, sizeof(key), "aodm_fp64%s:nao%d:work%d:items%d:nset%zu:blk%zu",
+                pipe_ok ? "_pipe" : "", bucket(double(nao)), bucket(work),
+                bucket(double(plan->nitems)), nset_max, blksize);
   std::string tune = "default";
   plan->cfg = cfgmm::aodm_default_config(int(nset_max));
+  if (pipe_ok) plan->cfg.tk = 0;  // the pipelined form
+  const std::vector<int> tks = pipe_ok ? std::vector<int>{0, 32, 16} : std::vector<int>{32, 16};
   if (!(flags & CFGMM_PLAN_NO_TUNE) && plan->nitems > 0) {
     if (cache_lookup(key, &plan->cfg)) {
       tune = "cache";
     } else {
       double best_ms = 1e30;
       std::string trials;
-      for (int tk : {32, 16})
+      for (int tk : tks)
         for (int ns = 1; ns <= 3 && ns <= int(nset_max); ++ns) {
           const cfgmm::AodmConfig c{ns, tk};
           double ms = 0;

@@ -26,13 +26,27 @@
 //      tile is shared by all density matrices of the group.
 //      The active list of the current block is staged in shared memory, so
 //      the gather addresses never wait on global loads.
+//   3b. aodm_fp64_pipe_kernel: the same items with producer warps (D by
+//      cp.async, ao_rhs rows by TMA gather4) and consumer warps (DMMA
+//      m16n8k8) meeting on mbarriers; used whenever ao_rhs allows TMA
+//      (16-byte aligned rows, even BLKSIZE), form 3 otherwise.
 //   4. aodm_reduce: adds the per-row-tile partial sums of each grid tile in a
 //      fixed order, so results are deterministic run to run (unlike the
 //      reference, whose lock order varies).
+#include <cstdlib>
+#include <mutex>
+
+#include <cudaTypedefs.h>
+
 #include "common.cuh"
 #include "aodmao2rho_fp64.cuh"
+#include "tcgen05.cuh"
 
 namespace cfgmm {
+
+// Error word of the pipelined kernel's bounded waits (0 = none).
+__device__ int g_aodm_error;
+
 namespace {
 
 constexpr int TU = 64;   // compacted rows (u) per work item
@@ -85,7 +99,10 @@ aodm_build_items(const int* __restrict__ counts, int nblk, int gsub, int4* __res
   __shared__ int warp_tot[32];
   __shared__ int base_s;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if (tid == 0) base_s = 0;
+  if (tid == 0) {
+    base_s = 0;
+    g_aodm_error = 0;
+  }
   for (int i = tid; i <= ncounters; i += 1024) counters[i] = 0;  // [ncounters] = total
   __syncthreads();
   for (int b0 = 0; b0 < nblk; b0 += 1024) {
@@ -316,6 +333,359 @@ __global__ void __launch_bounds__(THREADS, 1) aodm_fp64_kernel(AodmArgs p) {
 }
 
 // ---------------------------------------------------------------------------
+// 3b. pipelined main kernel: the same work items and partial sums as (3), with
+//     the roles split.  Four producer warps gather D_s[I_rows, I(k0..k0+15)]
+//     with 8-byte cp.async (lanes along consecutive compacted columns, so a
+//     warp's reads coalesce over the runs of active AOs) and one producer lane
+//     fetches the ao_rhs rows I(k0..k0+15) x 64 points with TMA gather4 (four
+//     arbitrary rows per instruction).  Both complete on the stage's mbarrier;
+//     eight consumer warps run DMMA m16n8k8 from the stages and release them
+//     through a second mbarrier, so the gather of later stages -- and of the
+//     next work item -- overlaps the tensor-core work.  The roles meet only on
+//     mbarriers, and every wait is bounded (tc::mbar_wait): on a timeout the
+//     kernel records a code in g_aodm_error and every warp leaves (exit
+//     decisions are made warp-uniform, so no warp-level sync meets an exited
+//     lane).
+// ---------------------------------------------------------------------------
+namespace pipe {
+constexpr int TK = 16;         // compacted AOs per stage
+constexpr int PSTAGES = 5;     // 6 leaves too little L1 beside shared memory (measured)
+constexpr int NPROD = 128;     // producer threads (4 warps)
+constexpr int NCONS = 256;     // consumer threads (8 warps, 2 x 4 over rows x points)
+constexpr int PTHREADS = NPROD + NCONS;
+constexpr int RING = 4;        // work items in flight between the roles
+constexpr int D_BYTES = TU * TK * 8;      // one density matrix's tile per stage
+constexpr int PHI_BYTES = TK * TG * 8;    // ao_rhs rows, 64 points each, no swizzle
+constexpr int RSTEP = NPROD / TK;              // rows apart of one thread's gathers
+constexpr int ROWS_PER_THREAD = TU / RSTEP;     // 16
+
+template <int NS>
+constexpr int stage_bytes() { return NS * D_BYTES + PHI_BYTES; }
+
+template <int NS>
+constexpr int red_doubles() { return 2 * NS * 2 * TG; }  // double-buffered [2][NS][2][TG]
+
+template <int NS>
+constexpr size_t smem_bytes() {
+  return 1024 + size_t(PSTAGES) * stage_bytes<NS>() + size_t(red_doubles<NS>()) * 8 +
+         (2 * PSTAGES + 2 * RING + 2) * 8 + RING * 4;
+}
+
+// Offset (doubles) of D element (row r, stage column k) in a TU x TK tile.  The
+// 16-byte slot c = 4*(k/8) + k%4 holds columns k and k+4 of an 8-column group,
+// i.e. the (a0, a2) or (a1, a3) pair of one m16n8k8 A fragment, and the slots
+// of each 128-byte row are XOR-swizzled by swz_key(r): a fragment load's
+// phases of 8 lanes (rows 2p, 2p+1, slots c0..c0+3) meet 8 distinct slots.
+__device__ __forceinline__ int d_off(int r, int k) {
+  const int slot = ((k >> 3) << 2) | (k & 3);
+  return r * TK + ((slot ^ swz_key(r)) << 1) + ((k >> 2) & 1);
+}
+
+__device__ __forceinline__ void tma_gather4(void* dst, const CUtensorMap* map, uint64_t* bar, int x,
+                                            int r0, int r1, int r2, int r3) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%3, %4, %5, %6, %7}], [%2];" ::"r"(tc::smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(tc::smem_u32(bar)), "r"(x), "r"(r0), "r"(r1),
+      "r"(r2), "r"(r3)
+      : "memory");
+}
+
+// The mbarrier tracks the completion of all cp.async this thread issued before.
+__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(tc::smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// wait-site codes recorded in g_aodm_error
+enum : int { kErrItemEmpty = 0x4101, kErrItemFull, kErrStageEmpty, kErrStageFull, kErrEpilogue,
+             kErrTeardown };
+
+// Decoded work item (both roles decode the same one).
+struct Item {
+  const AodmBatch* B;
+  int ns, bg, utile, nb, u0, mu, g0, gw;
+  const int* I;
+};
+
+template <int NS>
+__device__ __forceinline__ Item decode(const AodmArgs& p, int4 w, int set0) {
+  Item t;
+  t.B = p.batches ? &p.batches[w.x] : &p.one;
+  t.ns = min(NS, t.B->nset - set0);
+  t.bg = w.y;
+  t.utile = w.z;
+  const int b = t.bg / p.gsub, gt = t.bg % p.gsub;
+  t.nb = t.B->counts[b];
+  t.I = t.B->lists + size_t(b) * p.nao;
+  t.u0 = t.utile * TU;
+  t.mu = min(TU, t.nb - t.u0);
+  t.g0 = b * p.blk + gt * TG;
+  t.gw = min(min((b + 1) * p.blk, t.B->ngrid), t.g0 + TG) - t.g0;
+  return t;
+}
+
+// Bounded wait whose outcome is the same for every lane of the warp.
+__device__ __forceinline__ bool warp_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
+  const bool ok = tc::mbar_wait(bar, parity, err, code);
+  return __all_sync(0xffffffffu, ok);
+}
+}  // namespace pipe
+
+template <int NS>
+__global__ void __launch_bounds__(pipe::PTHREADS, 1)
+aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
+                      const __grid_constant__ CUtensorMap rhs_map) {
+  using namespace pipe;
+  constexpr int SB = stage_bytes<NS>();
+  extern __shared__ uint8_t pipe_smem_raw[];
+  uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(pipe_smem_raw) + 1023) &
+                                           ~uintptr_t(1023));
+  double* red = reinterpret_cast<double*>(sm + PSTAGES * SB);  // [2][NS][2][TG]
+  uint64_t* full = reinterpret_cast<uint64_t*>(red + red_doubles<NS>());
+  uint64_t* empty = full + PSTAGES;
+  uint64_t* ifull = empty + PSTAGES;
+  uint64_t* iempty = ifull + RING;
+  uint64_t* epi = iempty + RING;  // [2]
+  int* ring = reinterpret_cast<int*>(epi + 2);
+  int* err = &g_aodm_error;
+
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int set0 = blockIdx.y * NS;
+  const int total = p.counters[p.ngroups];
+  int* counter = p.counters + blockIdx.y;
+
+  if (tid == 0) {
+    for (int s = 0; s < PSTAGES; ++s) {
+      tc::mbar_init(&full[s], NPROD + 1);     // 64 cp.async arrivals + the TMA's expect_tx
+      tc::mbar_init(&empty[s], NCONS / 32);   // one per consumer warp
+    }
+    for (int r = 0; r < RING; ++r) {
+      tc::mbar_init(&ifull[r], 1);
+      tc::mbar_init(&iempty[r], PTHREADS / 32);  // every warp reads every item
+    }
+    for (int e = 0; e < 2; ++e) tc::mbar_init(&epi[e], NCONS);
+    tc::mbar_fence_init();
+  }
+  __syncthreads();
+
+  if (tid < NPROD) {
+    // ------------------------------- producers -------------------------------
+    const int kcol = tid & (TK - 1);  // stage column gathered by this thread
+    const int r0 = tid / TK;          // rows r0 + RSTEP i
+    uint32_t fill = 0;                // stage fills issued so far
+    for (int n = 0;; ++n) {
+      const int slot = n % RING;
+      if (tid == 0) {  // fetch the next item for every warp of the CTA
+        int it = total;
+        if (*reinterpret_cast<volatile int*>(err) == 0 &&
+            (n < RING || tc::mbar_wait(&iempty[slot], ((n / RING) - 1) & 1, err, kErrItemEmpty)))
+          it = min(atomicAdd(counter, 1), total);
+        ring[slot] = it;
+        tc::mbar_arrive(&ifull[slot]);
+      }
+      int it = total;
+      if (warp_wait(&ifull[slot], (n / RING) & 1, err, kErrItemFull)) it = ring[slot];
+      it = __shfl_sync(0xffffffffu, it, 0);
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&iempty[slot]);
+      if (it >= total) break;
+      const int4 w = p.items[it];
+      const Item t = decode<NS>(p, w, set0);
+      const CUtensorMap* map = p.batches ? &p.rhs_maps[w.x] : &rhs_map;
+      int prow[ROWS_PER_THREAD];  // AO of each gathered row, -1 past the item's rows
+#pragma unroll
+      for (int i = 0; i < ROWS_PER_THREAD; ++i) {
+        const int r = r0 + RSTEP * i;
+        prow[i] = r < t.mu ? t.I[t.u0 + r] : -1;
+      }
+      const int kchunks = (t.nb + TK - 1) / TK;
+      // the compacted column index of the next stage is loaded one stage ahead,
+      // so the gather addresses never wait for it
+      int vnext = t.I[min(kcol, t.nb - 1)];
+      for (int kc = 0; kc < kchunks; ++kc, ++fill) {
+        const int k = kc * TK + kcol;
+        const bool kv = k < t.nb;
+        const int v = vnext;  // t.I[min(k, nb - 1)]: the last active AO stands in past the end
+        vnext = t.I[min(k + TK, t.nb - 1)];
+        const int stage = fill % PSTAGES;
+        if (fill >= PSTAGES &&
+            !warp_wait(&empty[stage], ((fill / PSTAGES) - 1) & 1, err, kErrStageEmpty)) {
+          cp_async_arrive_noinc(&full[stage]);  // keep the arrival count of the phase whole
+          break;
+        }
+        uint8_t* st = sm + stage * SB;
+        const double* dm0 = p.dms + size_t(set0) * p.dm_stride + v;
+#pragma unroll
+        for (int i = 0; i < ROWS_PER_THREAD; ++i) {
+          const bool valid = kv && prow[i] >= 0;
+          const double* src = valid ? dm0 + size_t(prow[i]) * p.stride_ao : p.dms;
+          double* dst = reinterpret_cast<double*>(st) + d_off(r0 + RSTEP * i, kcol);
+#pragma unroll 1
+          for (int s = 0; s < t.ns; ++s)
+            cp_async_8(dst + s * (D_BYTES / 8), valid ? src + s * p.dm_stride : src, valid);
+        }
+        cp_async_arrive_noinc(&full[stage]);
+        if (tid < 32) {
+          // ao_rhs rows of the stage columns, from the lanes that gather them
+          // (lane j of warp 0 holds column j; D is zero past the list's end)
+          int rows[TK];
+#pragma unroll
+          for (int j = 0; j < TK; ++j) rows[j] = __shfl_sync(0xffffffffu, v, j);
+          uint8_t* phi = st + NS * D_BYTES;
+          if (tid == 0) {
+            tc::mbar_arrive_expect_tx(&full[stage], PHI_BYTES);
+#pragma unroll
+            for (int j = 0; j < TK / 4; ++j)
+              tma_gather4(phi + j * 4 * TG * 8, map, &full[stage], t.g0, rows[4 * j],
+                          rows[4 * j + 1], rows[4 * j + 2], rows[4 * j + 3]);
+          }
+        }
+      }
+    }
+    cp_async_wait_all();
+    if (tid == 0) {
+      // let every TMA this thread issued land before the CTA exits
+      for (uint32_t f = fill > PSTAGES ? fill - PSTAGES : 0; f < fill; ++f)
+        tc::mbar_wait(&full[f % PSTAGES], (f / PSTAGES) & 1, err, kErrTeardown, true);
+    }
+  } else {
+    // ------------------------------- consumers -------------------------------
+    const int ct = tid - NPROD;
+    const int warp = ct >> 5;
+    const int wm = warp >> 2, wn = warp & 3;  // warp tile: rows wm*32.., points wn*16..
+    const int g = lane >> 2, q = lane & 3;
+    uint32_t use = 0;
+    for (int n = 0;; ++n) {
+      const int slot = n % RING;
+      int it = total;
+      if (warp_wait(&ifull[slot], (n / RING) & 1, err, kErrItemFull)) it = ring[slot];
+      it = __shfl_sync(0xffffffffu, it, 0);
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&iempty[slot]);
+      if (it >= total) break;
+      const Item t = decode<NS>(p, p.items[it], set0);
+
+      // the phi_lhs rows of this thread's epilogue (rows wm*32 + mt*16 + g + 8h,
+      // points wn*16 + nt*8 + 2q + e) are brought into L2 now, so that the
+      // epilogue's loads hit while the tensor pipe waits for them
+      int urow[2][2];
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int r = wm * 32 + mt * 16 + g + 8 * h;
+          urow[mt][h] = r < t.mu ? t.I[t.u0 + r] : -1;
+          if (urow[mt][h] >= 0)
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt)
+              asm volatile("prefetch.global.L2 [%0];" ::"l"(
+                  t.B->ao_lhs + size_t(urow[mt][h]) * t.B->stride_grid + t.g0 + wn * 16 + nt * 8));
+        }
+
+      double acc[NS][2][2][4];
+#pragma unroll
+      for (int s = 0; s < NS; ++s)
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+          for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[s][i][j][e] = 0.0;
+
+      const int kchunks = (t.nb + TK - 1) / TK;
+      bool ok = true;
+      for (int kc = 0; kc < kchunks; ++kc, ++use) {
+        const int stage = use % PSTAGES;
+        if (!warp_wait(&full[stage], (use / PSTAGES) & 1, err, kErrStageFull)) {
+          ok = false;
+          break;
+        }
+        const uint8_t* st = sm + stage * SB;
+        const double* phi = reinterpret_cast<const double*>(st + NS * D_BYTES);
+#pragma unroll
+        for (int kk = 0; kk < TK; kk += 8) {
+          double b0[2], b1[2];
+#pragma unroll
+          for (int nt = 0; nt < 2; ++nt) {
+            const int col = wn * 16 + nt * 8 + g;
+            b0[nt] = phi[(kk + q) * TG + col];
+            b1[nt] = phi[(kk + q + 4) * TG + col];
+          }
+          const int slot8 = ((kk >> 3) << 2) | q;
+#pragma unroll
+          for (int s = 0; s < NS; ++s) {
+            const double* Ds = reinterpret_cast<const double*>(st + s * D_BYTES);
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) {
+              const int r = wm * 32 + mt * 16 + g;
+              const double2 lo =
+                  *reinterpret_cast<const double2*>(Ds + r * TK + ((slot8 ^ swz_key(r)) << 1));
+              const double2 hi = *reinterpret_cast<const double2*>(
+                  Ds + (r + 8) * TK + ((slot8 ^ swz_key(r + 8)) << 1));
+#pragma unroll
+              for (int nt = 0; nt < 2; ++nt)
+                dmma_16x8x8(acc[s][mt][nt], lo.x, hi.x, lo.y, hi.y, b0[nt], b1[nt]);
+            }
+          }
+        }
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&empty[stage]);
+      }
+      if (!ok) break;
+
+      // rho_part[s][j] = sum_r phi_lhs[I[u0+r]][g0+j] * X[s][r][j]: rows reduced
+      // in registers and shuffles, the two row halves (wm) through `red`
+      double lhs[2][2][2][2];  // [mt][h][nt][e]
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const double* row =
+              urow[mt][h] >= 0 ? t.B->ao_lhs + size_t(urow[mt][h]) * t.B->stride_grid : nullptr;
+#pragma unroll
+          for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              const int j = wn * 16 + nt * 8 + 2 * q + e;
+              lhs[mt][h][nt][e] = (row && j < t.gw) ? row[t.g0 + j] : 0.0;
+            }
+        }
+      double* rb = red + (n & 1) * (NS * 2 * TG);
+#pragma unroll
+      for (int s = 0; s < NS; ++s)
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            double v = 0.0;
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+              for (int h = 0; h < 2; ++h)
+                v = fma(acc[s][mt][nt][2 * h + e], lhs[mt][h][nt][e], v);
+            v += __shfl_xor_sync(0xffffffffu, v, 4);
+            v += __shfl_xor_sync(0xffffffffu, v, 8);
+            v += __shfl_xor_sync(0xffffffffu, v, 16);
+            if (g == 0) rb[(s * 2 + wm) * TG + wn * 16 + nt * 8 + 2 * q + e] = v;
+          }
+      tc::mbar_arrive(&epi[n & 1]);
+      // The buffer is written again two items later, after every consumer has
+      // passed the next item's epilogue barrier, i.e. finished reading this one.
+      if (!warp_wait(&epi[n & 1], (n >> 1) & 1, err, kErrEpilogue)) break;
+      const size_t pslot = t.B->partial_off + size_t(t.bg) * p.max_utiles + t.utile;
+      for (int i = ct; i < t.ns * TG; i += NCONS) {
+        const int s = i / TG, j = i % TG;
+        p.partial[(pslot * p.nset_max + set0 + s) * TG + j] =
+            rb[(s * 2 + 0) * TG + j] + rb[(s * 2 + 1) * TG + j];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // 4. deterministic reduction of the row-tile partials into rho
 //    one CTA per (batch, block tile): rpairs[i] = (batch, bg), or bg = i
 // ---------------------------------------------------------------------------
@@ -343,6 +713,7 @@ __global__ void aodm_reduce(AodmArgs p, const int2* __restrict__ rpairs, int npa
 
 __global__ void aodm_reset_counters(int* counters, int ngroups) {
   if (threadIdx.x < ngroups) counters[threadIdx.x] = 0;
+  if (threadIdx.x == 0) g_aodm_error = 0;
 }
 
 template <int NS, int TKT>
@@ -362,7 +733,76 @@ cudaError_t launch_main_t(const AodmArgs& a, cudaStream_t stream, bool attrs_onl
   return cudaGetLastError();
 }
 
+template <int NS>
+cudaError_t launch_pipe_t(const AodmArgs& a, const CUtensorMap& map, cudaStream_t stream,
+                          bool attrs_only) {
+  constexpr size_t smem = pipe::smem_bytes<NS>();
+  static_assert(smem <= 227 * 1024, "shared memory budget");
+  cudaError_t err = cudaFuncSetAttribute(aodm_fp64_pipe_kernel<NS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (err != cudaSuccess || attrs_only) return err;
+  int dev = 0, nsm = 0;
+  if ((err = cudaGetDevice(&dev)) != cudaSuccess) return err;
+  if ((err = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+    return err;
+  aodm_fp64_pipe_kernel<NS><<<dim3(nsm, a.ngroups), pipe::PTHREADS, smem, stream>>>(a, map);
+  return cudaGetLastError();
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult qr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &qr) ==
+            cudaSuccess &&
+        qr == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  });
+  return fn;
+}
+
+// The pipelined form is used unless CFGMM_AODM_PIPE=0.
+bool pipe_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("CFGMM_AODM_PIPE");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 }  // namespace
+
+bool aodm_rhs_map(CUtensorMap* map, const double* ao_rhs, size_t stride_grid, int nao, int ngrid,
+                  int blk) {
+  // TMA: 16-byte aligned base and row pitch; the x coordinate of every load
+  // (a 64-point tile start b*blk + 64*gt) must be even, so blk must be even.
+  if (!pipe_enabled() || nao <= 0 || ngrid <= 0 || blk % 2 != 0 ||
+      reinterpret_cast<uintptr_t>(ao_rhs) % 16 != 0 || (stride_grid * sizeof(double)) % 16 != 0)
+    return false;
+  auto enc = encode_tiled();
+  if (!enc) return false;
+  cuuint64_t dims[2] = {cuuint64_t(ngrid), cuuint64_t(nao)};
+  cuuint64_t strides[1] = {cuuint64_t(stride_grid) * sizeof(double)};
+  cuuint32_t box[2] = {cuuint32_t(TG), 1};  // gather4: one row per box, four rows per load
+  cuuint32_t estr[2] = {1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(ao_rhs), dims, strides,
+             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+cudaError_t aodm_launch_pipe(const AodmArgs& a, int ns, const CUtensorMap& map,
+                             cudaStream_t stream, bool attrs_only) {
+  if (ns == 1) return launch_pipe_t<1>(a, map, stream, attrs_only);
+  if (ns == 2) return launch_pipe_t<2>(a, map, stream, attrs_only);
+  if (ns == 3) return launch_pipe_t<3>(a, map, stream, attrs_only);
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t aodm_read_error(int* code) {
+  return cudaMemcpyFromSymbol(code, g_aodm_error, sizeof(int));
+}
 
 int aodm_groups(const AodmConfig& cfg, int nset_max) {
   return (nset_max + cfg.ns - 1) / cfg.ns;
@@ -374,6 +814,10 @@ AodmConfig aodm_default_config(int nset) {
 
 cudaError_t aodm_launch_main(const AodmArgs& a, const AodmConfig& cfg, cudaStream_t stream,
                              bool attrs_only) {
+  if (cfg.tk == 0) {  // pipelined form over the batches' maps
+    if (!a.batches || !a.rhs_maps) return cudaErrorInvalidValue;
+    return aodm_launch_pipe(a, cfg.ns, CUtensorMap{}, stream, attrs_only);
+  }
   if (cfg.tk == 32) {
     if (cfg.ns == 1) return launch_main_t<1, 32>(a, stream, attrs_only);
     if (cfg.ns == 2) return launch_main_t<2, 32>(a, stream, attrs_only);
@@ -472,7 +916,12 @@ cudaError_t aodmao2rho_fp64(double* rhos, const double* dms, const double* ao_lh
   a.counters = counters;
   a.ngroups = ngroups;
   a.partial = partial;
-  if ((err = aodm_launch_main(a, cfg, stream)) != cudaSuccess) return err;
+  CUtensorMap map;
+  if (aodm_rhs_map(&map, ao_rhs, stride_grid, nao, ngrid, blk))
+    err = aodm_launch_pipe(a, cfg.ns, map, stream);
+  else
+    err = aodm_launch_main(a, cfg, stream);
+  if (err != cudaSuccess) return err;
   return aodm_launch_reduce(a, nullptr, nblk * gsub, stream);
 }
 

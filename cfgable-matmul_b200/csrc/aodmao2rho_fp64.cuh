@@ -2,6 +2,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace cfgmm {
@@ -28,6 +29,7 @@ struct AodmArgs {
   int max_utiles;               // partial slots per (batch, block tile)
   int nset_max;
   const AodmBatch* batches;     // null: use `one`
+  const CUtensorMap* rhs_maps;  // with batches: ao_rhs gather map of each batch (pipelined form)
   AodmBatch one;
   const int4* items;            // work list: (batch, block tile, row tile, 0)
   int* counters;                // [ngroups] work counters, then the item total
@@ -37,7 +39,8 @@ struct AodmArgs {
 
 // Tile configuration of the main kernel (the autotuner's search space):
 // `ns` density matrices share one ao_rhs tile (1..3), `tk` compacted AOs per
-// pipeline stage (16 or 32).
+// pipeline stage of form 3 (16 or 32), or tk = 0 for the pipelined form
+// (which then takes the ao_rhs maps from AodmArgs::rhs_maps).
 struct AodmConfig {
   int ns;
   int tk;
@@ -72,5 +75,18 @@ cudaError_t aodm_launch_main(const AodmArgs& a, const AodmConfig& cfg, cudaStrea
                              bool attrs_only = false);
 cudaError_t aodm_launch_reduce(const AodmArgs& a, const int2* rpairs, int npairs,
                                cudaStream_t stream);
+
+// Pipelined form of the main kernel (warp-specialised, ao_rhs rows by TMA
+// gather4).  aodm_rhs_map builds the gather map of one ao_rhs table and returns
+// false where the form does not apply (base or row pitch not 16-byte aligned,
+// odd BLKSIZE, CFGMM_AODM_PIPE=0).  `map` is used when a.batches is null,
+// a.rhs_maps (a 64-byte aligned device array, one map per batch) otherwise.
+bool aodm_rhs_map(CUtensorMap* map, const double* ao_rhs, size_t stride_grid, int nao, int ngrid,
+                  int blk);
+cudaError_t aodm_launch_pipe(const AodmArgs& a, int ns, const CUtensorMap& map,
+                             cudaStream_t stream, bool attrs_only = false);
+// Code of the first timed-out wait of the pipelined kernel since the last
+// call's setup kernel (0: none).
+cudaError_t aodm_read_error(int* code);
 
 }  // namespace cfgmm

@@ -145,3 +145,37 @@ def test_device_pointers_and_determinism(cm, wl):
     assert np.array_equal(outs[0], outs[1])  # fixed reduction order
     ref = wl.dense_rho(p.ao, p.ao, p.dms, p.tab, p.blksize)
     assert normwise(outs[0], ref) < TOL
+
+
+@pytest.mark.parametrize("stride_pad", [0, 1])
+def test_pipelined_and_plain_forms_agree(cm, oracle, stride_pad):
+    """The pipelined kernel (TMA gather of phi rows; used when the rows are
+    16-byte aligned and BLKSIZE is even) and the form it replaces, forced with
+    CFGMM_AODM_PIPE=0, on the same inputs; an odd row pitch (stride_pad 1)
+    takes the plain form in both runs.  Both within 1e-13 of the oracle."""
+    import json, os, subprocess, sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    tmp = os.environ.get("TMPDIR", "/tmp")
+    code = ("import importlib,sys,numpy as np; sys.path.insert(0,'.');"
+            "cm=importlib.import_module('cfgable-matmul_b200');"
+            "wl=importlib.import_module('cfgable-matmul_b200.workloads');"
+            "pad=int(sys.argv[2]); p=wl.small_masked(seed=9,nao=768,ngrid=5000,blksize=64,nset=3);"
+            "sg=p.ngrid+pad; ao=np.zeros((p.nao,sg)); ao[:,:p.ngrid]=p.ao;"
+            "rho=np.zeros((p.nset,sg)); "
+            "cm.aodmao2rho_ex(rho,p.dms,ao,ao,(p.nao,sg),(p.nao,p.ngrid),p.nset,p.tab,p.nblk,64);"
+            "np.save(sys.argv[1], rho)")
+    outs = []
+    for pipe in ("1", "0"):
+        path = os.path.join(tmp, f"cfgmm_aodm_pipe{pipe}_{stride_pad}.npy")
+        env = dict(os.environ, CFGMM_AODM_PIPE=pipe)
+        subprocess.run([sys.executable, "-c", code, path, str(stride_pad)], cwd=root, env=env,
+                       check=True)
+        outs.append(np.load(path))
+    wl = __import__("importlib").import_module("cfgable-matmul_b200.workloads")
+    p = wl.small_masked(seed=9, nao=768, ngrid=5000, blksize=64, nset=3)
+    ref = np.zeros((p.nset, p.ngrid))
+    oracle.aodmao2rho(ref, p.dms, p.ao, p.ao, (p.nao, p.ngrid), (p.nao, p.ngrid), p.nset, p.tab,
+                      p.nblk, 64)
+    for o in outs:
+        assert normwise(o[:, :p.ngrid], ref) < TOL
+    assert normwise(outs[0], outs[1]) < 1e-14
