@@ -420,7 +420,7 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
   const size_t o_items = o_batch + a256(nbatch * sizeof(cfgmm::AodmBatch));
   const size_t o_pairs = o_items + a256(slots * sizeof(int4));
   const size_t o_ctr = o_pairs + a256(cnt_n * gsub * sizeof(int2));
-  const size_t o_part = o_ctr + a256((nset_max + 1) * sizeof(int));
+  const size_t o_part = o_ctr + a256((nset_max + 2) * sizeof(int));  // + total, asymmetry flag
   const size_t o_maps = o_part + a256(slots * nset_max * TG * sizeof(double));
   // split precision keeps only the active lists here (its own layout follows)
   const size_t bytes = precision == CFGMM_PREC_OZAKI_INT8
@@ -516,6 +516,17 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
   a.rhs_maps = pipe_ok ? reinterpret_cast<const CUtensorMap*>(base + o_maps) : nullptr;
   a.items = reinterpret_cast<const int4*>(base + o_items);
   a.counters = reinterpret_cast<int*>(base + o_ctr);
+  const bool sym = pipe_ok && cfgmm::aodm_sym_enabled();
+  // reset, symmetry check of D, main kernel (the reduction follows in a run)
+  auto launch = [&](const cfgmm::AodmConfig& c, cudaStream_t st) -> cudaError_t {
+    a.asym = sym && c.tk == 0 ? a.counters + a.ngroups + 1 : nullptr;
+    cudaError_t e = cfgmm::aodm_launch_reset(a.counters, a.ngroups, st);
+    if (e == cudaSuccess && a.asym)
+      e = cfgmm::aodm_launch_sym_check(dms, stride_ao, int(nao), int(nset_max),
+                                       a.counters + a.ngroups + 1, st);
+    if (e == cudaSuccess) e = cfgmm::aodm_launch_main(a, c, st);
+    return e;
+  };
   a.partial = reinterpret_cast<double*>(base + o_part);
 
   // ---- 3. autotuning ----
@@ -535,9 +546,8 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
     cudaEventCreate(&e1);
     float best = 1e30f;
     for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {
-      e = cfgmm::aodm_launch_reset(a.counters, a.ngroups, s);
-      if (e == cudaSuccess) e = cudaEventRecord(e0, s);
-      if (e == cudaSuccess) e = cfgmm::aodm_launch_main(a, c, s);
+      e = cudaEventRecord(e0, s);
+      if (e == cudaSuccess) e = launch(c, s);
       if (e == cudaSuccess) e = cudaEventRecord(e1, s);
       if (e == cudaSuccess) e = cudaEventSynchronize(e1);
       float t = 0.f;
@@ -583,6 +593,7 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
     }
   }
   if ((err = set_cfg(plan->cfg)) != cudaSuccess) return cleanup(cuda_fail(err, "plan config"));
+  a.asym = sym && plan->cfg.tk == 0 ? a.counters + a.ngroups + 1 : nullptr;
 
   // ---- 4. capture the run ----
   if (!(flags & CFGMM_PLAN_NO_GRAPH)) {
@@ -594,8 +605,7 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
     cudaGraph_t graph = nullptr;
     if (err == cudaSuccess) err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
     if (err == cudaSuccess) {
-      cudaError_t e1 = cfgmm::aodm_launch_reset(a.counters, a.ngroups, cs);
-      if (e1 == cudaSuccess) e1 = cfgmm::aodm_launch_main(a, plan->cfg, cs);
+      cudaError_t e1 = launch(plan->cfg, cs);
       if (e1 == cudaSuccess) e1 = cfgmm::aodm_launch_reduce(a, plan->rpairs, plan->npairs, cs);
       err = cudaStreamEndCapture(cs, &graph);
       if (err == cudaSuccess) err = e1;
@@ -629,7 +639,11 @@ int cfgmm_aodm_plan_run(cfgmm_aodm_plan* plan, void* stream) {
     const int rc = split_run(plan, s);
     return rc;
   }
-  PLAN_CUDA(cfgmm::aodm_launch_reset(plan->args.counters, plan->args.ngroups, s));
+  const cfgmm::AodmArgs& a = plan->args;
+  PLAN_CUDA(cfgmm::aodm_launch_reset(a.counters, a.ngroups, s));
+  if (a.asym)
+    PLAN_CUDA(cfgmm::aodm_launch_sym_check(a.dms, a.stride_ao, a.nao, a.nset_max,
+                                           a.counters + a.ngroups + 1, s));
   PLAN_CUDA(cfgmm::aodm_launch_main(plan->args, plan->cfg, s));
   PLAN_CUDA(cfgmm::aodm_launch_reduce(plan->args, plan->rpairs, plan->npairs, s));
   return CFGMM_OK;

@@ -103,7 +103,8 @@ aodm_build_items(const int* __restrict__ counts, int nblk, int gsub, int4* __res
     base_s = 0;
     g_aodm_error = 0;
   }
-  for (int i = tid; i <= ncounters; i += 1024) counters[i] = 0;  // [ncounters] = total
+  // [ncounters] = total, [ncounters + 1] = asymmetry flag
+  for (int i = tid; i <= ncounters + 1; i += 1024) counters[i] = 0;
   __syncthreads();
   for (int b0 = 0; b0 < nblk; b0 += 1024) {
     const int b = b0 + tid;
@@ -427,6 +428,11 @@ __device__ __forceinline__ Item decode(const AodmArgs& p, int4 w, int set0) {
   return t;
 }
 
+// Weight of D[u0 + r][u0 + c] in the diagonal tile of the symmetric mode.
+__device__ __forceinline__ double sym_factor(int r, int c) {
+  return c < r ? 0.0 : (c == r ? 0.5 : 1.0);
+}
+
 // Bounded wait whose outcome is the same for every lane of the warp.
 __device__ __forceinline__ bool warp_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
   const bool ok = tc::mbar_wait(bar, parity, err, code);
@@ -456,10 +462,11 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
   const int set0 = blockIdx.y * NS;
   const int total = p.counters[p.ngroups];
   int* counter = p.counters + blockIdx.y;
+  const bool sym = p.asym != nullptr && *p.asym == 0;
 
   if (tid == 0) {
     for (int s = 0; s < PSTAGES; ++s) {
-      tc::mbar_init(&full[s], NPROD + 1);     // 64 cp.async arrivals + the TMA's expect_tx
+      tc::mbar_init(&full[s], NPROD + 1);     // NPROD cp.async arrivals + the TMA's expect_tx
       tc::mbar_init(&empty[s], NCONS / 32);   // one per consumer warp
     }
     for (int r = 0; r < RING; ++r) {
@@ -502,10 +509,11 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
         prow[i] = r < t.mu ? t.I[t.u0 + r] : -1;
       }
       const int kchunks = (t.nb + TK - 1) / TK;
+      const int kc0 = sym ? t.u0 / TK : 0;  // symmetric D: from the tile's own columns on
       // the compacted column index of the next stage is loaded one stage ahead,
       // so the gather addresses never wait for it
-      int vnext = t.I[min(kcol, t.nb - 1)];
-      for (int kc = 0; kc < kchunks; ++kc, ++fill) {
+      int vnext = t.I[min(kc0 * TK + kcol, t.nb - 1)];
+      for (int kc = kc0; kc < kchunks; ++kc, ++fill) {
         const int k = kc * TK + kcol;
         const bool kv = k < t.nb;
         const int v = vnext;  // t.I[min(k, nb - 1)]: the last active AO stands in past the end
@@ -596,8 +604,9 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
             for (int e = 0; e < 4; ++e) acc[s][i][j][e] = 0.0;
 
       const int kchunks = (t.nb + TK - 1) / TK;
+      const int kc0 = sym ? t.u0 / TK : 0;
       bool ok = true;
-      for (int kc = 0; kc < kchunks; ++kc, ++use) {
+      for (int kc = kc0; kc < kchunks; ++kc, ++use) {
         const int stage = use % PSTAGES;
         if (!warp_wait(&full[stage], (use / PSTAGES) & 1, err, kErrStageFull)) {
           ok = false;
@@ -605,6 +614,8 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
         }
         const uint8_t* st = sm + stage * SB;
         const double* phi = reinterpret_cast<const double*>(st + NS * D_BYTES);
+        // symmetric D, diagonal tile: D' = strict upper triangle + half diagonal
+        const bool diag = sym && kc < kc0 + TU / TK;
 #pragma unroll
         for (int kk = 0; kk < TK; kk += 8) {
           double b0[2], b1[2];
@@ -621,10 +632,17 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
 #pragma unroll
             for (int mt = 0; mt < 2; ++mt) {
               const int r = wm * 32 + mt * 16 + g;
-              const double2 lo =
+              double2 lo =
                   *reinterpret_cast<const double2*>(Ds + r * TK + ((slot8 ^ swz_key(r)) << 1));
-              const double2 hi = *reinterpret_cast<const double2*>(
+              double2 hi = *reinterpret_cast<const double2*>(
                   Ds + (r + 8) * TK + ((slot8 ^ swz_key(r + 8)) << 1));
+              if (diag) {
+                const int c = (kc - kc0) * TK + kk + q;  // column within the diagonal tile
+                lo.x *= sym_factor(r, c);
+                lo.y *= sym_factor(r, c + 4);
+                hi.x *= sym_factor(r + 8, c);
+                hi.y *= sym_factor(r + 8, c + 4);
+              }
 #pragma unroll
               for (int nt = 0; nt < 2; ++nt)
                 dmma_16x8x8(acc[s][mt][nt], lo.x, hi.x, lo.y, hi.y, b0[nt], b1[nt]);
@@ -678,8 +696,8 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
       const size_t pslot = t.B->partial_off + size_t(t.bg) * p.max_utiles + t.utile;
       for (int i = ct; i < t.ns * TG; i += NCONS) {
         const int s = i / TG, j = i % TG;
-        p.partial[(pslot * p.nset_max + set0 + s) * TG + j] =
-            rb[(s * 2 + 0) * TG + j] + rb[(s * 2 + 1) * TG + j];
+        const double v = rb[(s * 2 + 0) * TG + j] + rb[(s * 2 + 1) * TG + j];
+        p.partial[(pslot * p.nset_max + set0 + s) * TG + j] = sym ? 2.0 * v : v;
       }
     }
   }
@@ -713,7 +731,33 @@ __global__ void aodm_reduce(AodmArgs p, const int2* __restrict__ rpairs, int npa
 
 __global__ void aodm_reset_counters(int* counters, int ngroups) {
   if (threadIdx.x < ngroups) counters[threadIdx.x] = 0;
-  if (threadIdx.x == 0) g_aodm_error = 0;
+  if (threadIdx.x == 0) {
+    counters[ngroups + 1] = 0;  // asymmetry flag (counters[ngroups] holds the item total)
+    g_aodm_error = 0;
+  }
+}
+
+// *asym = 1 if some D_s differs from its transpose.  Block (bx, by, s) with
+// by <= bx compares the 32 x 32 tile (by, bx) with the transpose of (bx, by).
+__global__ void __launch_bounds__(256)
+aodm_sym_check(const double* __restrict__ dms, size_t stride_ao, size_t dm_stride, int nao,
+               int* asym) {
+  const int bx = blockIdx.x, by = blockIdx.y;
+  if (by > bx) return;
+  __shared__ double tile[32][33];
+  const double* d = dms + size_t(blockIdx.z) * dm_stride;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int i = ty; i < 32; i += 8) {
+    const int r = by * 32 + i, c = bx * 32 + tx;
+    tile[i][tx] = (r < nao && c < nao) ? d[size_t(r) * stride_ao + c] : 0.0;
+  }
+  __syncthreads();
+  bool bad = false;
+  for (int i = ty; i < 32; i += 8) {
+    const int r = bx * 32 + i, c = by * 32 + tx;
+    if (r < nao && c < nao) bad |= !(d[size_t(r) * stride_ao + c] == tile[tx][i]);
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(asym, 1);
 }
 
 template <int NS, int TKT>
@@ -800,6 +844,23 @@ cudaError_t aodm_launch_pipe(const AodmArgs& a, int ns, const CUtensorMap& map,
   return cudaErrorInvalidValue;
 }
 
+bool aodm_sym_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("CFGMM_AODM_SYM");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+cudaError_t aodm_launch_sym_check(const double* dms, size_t stride_ao, int nao, int nset,
+                                  int* asym, cudaStream_t stream) {
+  if (nao <= 0 || nset <= 0) return cudaSuccess;
+  const unsigned nt = unsigned((nao + 31) / 32);
+  aodm_sym_check<<<dim3(nt, nt, unsigned(nset)), 256, 0, stream>>>(dms, stride_ao,
+                                                                  stride_ao * stride_ao, nao, asym);
+  return cudaGetLastError();
+}
+
 cudaError_t aodm_read_error(int* code) {
   return cudaMemcpyFromSymbol(code, g_aodm_error, sizeof(int));
 }
@@ -858,7 +919,7 @@ Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk) {
   L.counts = L.lists + a256(nblk * nao * sizeof(int));
   L.items = L.counts + a256(nblk * sizeof(int));
   L.counters = L.items + a256(nblk * gsub * max_utiles * sizeof(int4));
-  L.partial = L.counters + a256((ngroups + 1) * sizeof(int));
+  L.partial = L.counters + a256((ngroups + 2) * sizeof(int));  // + item total, asymmetry flag
   L.total = L.partial + nblk * gsub * max_utiles * nset * TG * sizeof(double);
   return L;
 }
@@ -917,8 +978,15 @@ cudaError_t aodmao2rho_fp64(double* rhos, const double* dms, const double* ao_lh
   a.ngroups = ngroups;
   a.partial = partial;
   CUtensorMap map;
-  if (aodm_rhs_map(&map, ao_rhs, stride_grid, nao, ngrid, blk))
+  if (aodm_rhs_map(&map, ao_rhs, stride_grid, nao, ngrid, blk)) {
+    if (aodm_sym_enabled()) {
+      a.asym = counters + ngroups + 1;
+      if ((err = aodm_launch_sym_check(dms, stride_ao, nao, nset, counters + ngroups + 1,
+                                       stream)) != cudaSuccess)
+        return err;
+    }
     err = aodm_launch_pipe(a, cfg.ns, map, stream);
+  }
   else
     err = aodm_launch_main(a, cfg, stream);
   if (err != cudaSuccess) return err;

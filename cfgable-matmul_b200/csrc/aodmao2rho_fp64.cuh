@@ -32,8 +32,9 @@ struct AodmArgs {
   const CUtensorMap* rhs_maps;  // with batches: ao_rhs gather map of each batch (pipelined form)
   AodmBatch one;
   const int4* items;            // work list: (batch, block tile, row tile, 0)
-  int* counters;                // [ngroups] work counters, then the item total
+  int* counters;                // [ngroups] work counters, the item total, the asymmetry flag
   int ngroups;
+  const int* asym;              // null, or counters + ngroups + 1: 0 when every D_s is symmetric
   double* partial;              // [slot][nset_max][64]
 };
 
@@ -88,5 +89,17 @@ cudaError_t aodm_launch_pipe(const AodmArgs& a, int ns, const CUtensorMap& map,
 // Code of the first timed-out wait of the pipelined kernel since the last
 // call's setup kernel (0: none).
 cudaError_t aodm_read_error(int* code);
+
+// Symmetric-D mode of the pipelined form: aodm_launch_sym_check sets
+// *asym = 1 unless every D_s (s < nset) equals its transpose bit for bit
+// (*asym is zeroed by the setup kernels).  With a.asym pointing at the flag and
+// the flag 0, row tile a of a block contracts only the compacted columns from
+// its own first one on, rho += 2 phi_a^T (D'_aa phi_a + D_{a,>a} phi_>a) with
+// D'_aa the upper triangle of the diagonal tile and half its diagonal: about
+// half the D gather and the FLOPs.  aodm_sym_enabled() is false when
+// CFGMM_AODM_SYM=0.
+bool aodm_sym_enabled();
+cudaError_t aodm_launch_sym_check(const double* dms, size_t stride_ao, int nao, int nset,
+                                  int* asym, cudaStream_t stream);
 
 }  // namespace cfgmm

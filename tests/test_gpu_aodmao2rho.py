@@ -179,3 +179,28 @@ def test_pipelined_and_plain_forms_agree(cm, oracle, stride_pad):
     for o in outs:
         assert normwise(o[:, :p.ngrid], ref) < TOL
     assert normwise(outs[0], outs[1]) < 1e-14
+
+
+@pytest.mark.parametrize("kind", ["symmetric", "one_entry_off", "general"])
+@pytest.mark.parametrize("nset", [1, 3])
+def test_symmetric_d_mode_and_its_check(cm, oracle, kind, nset):
+    """The pipelined form contracts only the upper half of D when every D_s
+    equals its transpose bit for bit (checked on the device each call); one
+    differing entry, or a general D, must take the full contraction.  The
+    oracle never assumes symmetry, so a wrongly taken symmetric mode fails."""
+    rng = np.random.default_rng(40 + nset)
+    from importlib import import_module
+    wl = import_module("cfgable-matmul_b200.workloads")
+    p = wl.small_masked(seed=40 + nset, nao=600, ngrid=3000, blksize=64, nset=nset, density=0.5)
+    dms = p.dms.copy()
+    if kind == "one_entry_off":
+        dms[nset - 1, 17, 411] += 10.0  # D[17][411] != D[411][17]; both active in ~1/4 of blocks
+    elif kind == "general":
+        dms = rng.uniform(-1, 1, dms.shape)
+    tab = p.tab
+    rho = np.zeros((nset, p.ngrid))
+    ref = np.zeros((nset, p.ngrid))
+    args = ((p.nao, p.ngrid), (p.nao, p.ngrid), nset, tab, p.nblk)
+    cm.aodmao2rho_ex(rho, dms, p.ao, p.ao, *args, blksize=64)
+    oracle.aodmao2rho(ref, dms, p.ao, p.ao, *args, 64)
+    assert normwise(rho, ref) < TOL
