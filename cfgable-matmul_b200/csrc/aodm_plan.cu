@@ -121,11 +121,27 @@ void cache_store(const std::string& key, const cfgmm::AodmConfig& cfg, double ms
 int bucket(double v) { return v <= 0 ? 0 : int(std::floor(std::log2(v) * 2)); }  // half-octaves
 
 
+// D digits of a split-precision run, after the device-side symmetry check
+// that selects the symmetric mode (sargs.asym, null when it is switched off).
+cudaError_t split_prepare_run(cfgmm_aodm_plan* plan, cudaStream_t s) {
+  const cfgmm::SplitArgs& a = plan->sargs;
+  int* asym = const_cast<int*>(a.asym);
+  cudaError_t err = cudaSuccess;
+  if (asym) {
+    err = cudaMemsetAsync(asym, 0, sizeof(int), s);
+    if (err == cudaSuccess)
+      err = cfgmm::aodm_launch_sym_check(plan->dms, plan->stride_ao, plan->nao, plan->nset_max,
+                                         asym, s);
+  }
+  if (err == cudaSuccess)
+    err = cfgmm::split_prepare_d(plan->dms, plan->stride_ao, plan->nao, plan->nset_max,
+                                 const_cast<uint2*>(a.dsl), const_cast<int*>(a.tau), s, asym);
+  return err;
+}
+
 // One split-precision run: D digits, the persistent kernel, the reduction.
 int split_run(cfgmm_aodm_plan* plan, cudaStream_t s) {
-  cudaError_t err = cfgmm::split_prepare_d(plan->dms, plan->stride_ao, plan->nao, plan->nset_max,
-                                           const_cast<uint2*>(plan->sargs.dsl),
-                                           const_cast<int*>(plan->sargs.tau), s);
+  cudaError_t err = split_prepare_run(plan, s);
   if (err == cudaSuccess) err = cfgmm::split_launch_main(plan->sargs, s, plan->stages);
   if (err == cudaSuccess)
     err = cfgmm::split_launch_reduce(plan->sargs, plan->rpairs, plan->npairs, s);
@@ -278,6 +294,8 @@ int build_split(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, size_t n
   a.blk = int(blksize);
   a.gsub = gsub;
   a.max_ut = max_ut;
+  // total[2]: the asymmetry flag of the symmetric mode
+  a.asym = cfgmm::aodm_sym_enabled() ? reinterpret_cast<const int*>(base + o_total) + 2 : nullptr;
 
   // ---- autotuning: pipeline depth of the persistent kernel ----
   std::string tune = "default";
@@ -296,10 +314,7 @@ int build_split(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, size_t n
       plan->stages = c.ns;
       tune = "cache";
     } else {
-      if ((err = cfgmm::split_prepare_d(dms, stride_ao, int(nao), int(nset_max),
-                                        const_cast<uint2*>(a.dsl), const_cast<int*>(a.tau), s)) !=
-          cudaSuccess)
-        return cuda_fail(err, "autotune");
+      if ((err = split_prepare_run(plan, s)) != cudaSuccess) return cuda_fail(err, "autotune");
       cudaEvent_t e0, e1;
       cudaEventCreate(&e0);
       cudaEventCreate(&e1);
@@ -340,8 +355,7 @@ int build_split(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, size_t n
     err = cfgmm::split_launch_main(a, s, plan->stages, true);
     if (err == cudaSuccess)
       err = capture(plan, [&](cudaStream_t cs) {
-        cudaError_t e = cfgmm::split_prepare_d(dms, stride_ao, int(nao), int(nset_max),
-                                               const_cast<uint2*>(a.dsl), const_cast<int*>(a.tau), cs);
+        cudaError_t e = split_prepare_run(plan, cs);
         if (e == cudaSuccess) e = cfgmm::split_launch_main(a, cs, plan->stages);
         if (e == cudaSuccess) e = cfgmm::split_launch_reduce(a, plan->rpairs, plan->npairs, cs);
         return e;

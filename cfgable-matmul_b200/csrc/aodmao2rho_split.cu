@@ -129,10 +129,12 @@ __device__ __forceinline__ void transpose4(uint32_t w0, uint32_t w1, uint32_t w2
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
 split_d_slices(const double* __restrict__ dms, size_t stride_ao, size_t dm_stride, int nao,
-               int nrows, uint2* __restrict__ dsl, int* __restrict__ tau) {
+               int nrows, uint2* __restrict__ dsl, int* __restrict__ tau,
+               const int* __restrict__ asym) {
   const int row = blockIdx.x * 8 + (threadIdx.x >> 5);  // s * nao + u, a warp per row
   const int lane = threadIdx.x & 31;
   if (row >= nrows) return;
+  const bool half_diag = asym != nullptr && *asym == 0;
   const int s = row / nao, u = row % nao;
   const double* d = dms + size_t(s) * dm_stride + size_t(u) * stride_ao;
   double mx = 0.0;
@@ -153,7 +155,8 @@ split_d_slices(const double* __restrict__ dms, size_t stride_ao, size_t dm_strid
   uint2* out = dsl + size_t(row) * nao;
 #pragma unroll 4
   for (int v = lane; v < nao; v += 32)
-    out[v] = e != kBadExp ? digits_packed(d[v], e) : make_uint2(0u, 0u);
+    out[v] = e != kBadExp ? digits_packed(half_diag && v == u ? 0.5 * d[v] : d[v], e)
+                          : make_uint2(0u, 0u);
 }
 
 // ---------------------------------------------------------------------------
@@ -377,6 +380,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(SplitArgs p) {
   tc::fence_after_sync();
   const uint32_t tmem = *tmem_slot;
   const int total = p.total[0], per_set = p.total[1];
+  const bool sym = p.asym != nullptr && *p.asym == 0;
 
   if (warp < GATHER_WARPS) {
     // ---------------- gather D digits, then the epilogue ----------------
@@ -401,6 +405,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(SplitArgs p) {
       const int b = bg / p.gsub, gt = bg % p.gsub;
       const int nb = B.counts[b];
       const int kc = (nb + TK - 1) / TK;
+      const int kc0 = sym ? ut * (TU / TK) : 0;  // symmetric D: from the tile's own columns on
       const int* I = B.lists + size_t(b) * p.nao;
       const uint2* dset = p.dsl + size_t(s) * p.nao * p.nao;
       int iu[8];
@@ -427,8 +432,8 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(SplitArgs p) {
           asm volatile("prefetch.global.L2 [%0];" ::"l"(q));
         asm volatile("prefetch.global.L2 [%0];" ::"l"(pe - 8));
       }
-      for (int c = grp; c < kc; c += 2) {
-        const uint32_t seq = seq0 + uint32_t(c);
+      for (int c = kc0 + grp; c < kc; c += 2) {
+        const uint32_t seq = seq0 + uint32_t(c - kc0);
         const int stg = int(seq % STAGES);
         const uint32_t use = seq / STAGES;
         if (use > 0 && !tc::mbar_wait(&empty[stg], (use - 1) & 1, err, 11)) {
@@ -441,12 +446,16 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(SplitArgs p) {
           const int kk = c * TK + 16 * hh + 4 * k + qd;
           iv[k] = kk < nb ? __ldg(I + kk) : -1;
         }
+        // symmetric D, diagonal tile: the strict lower triangle (column before
+        // row in the compacted order) is left out; elsewhere nothing is
+        const int lower_lim = sym && c < kc0 + TU / TK ? c * TK - ut * TU : TU;
         uint2 w[8][4];
 #pragma unroll
         for (int st = 0; st < 8; ++st)
 #pragma unroll
           for (int k = 0; k < 4; ++k)
-            w[st][k] = (iu[st] >= 0 && iv[k] >= 0)
+            w[st][k] = (iu[st] >= 0 && iv[k] >= 0 &&
+                        lower_lim + 16 * hh + 4 * k + qd >= 32 * wq + 4 * st + ri)
                            ? __ldg(dset + size_t(iu[st]) * p.nao + iv[k])
                            : make_uint2(0u, 0u);
         uint8_t* As = smem + stg * STAGE;
@@ -476,7 +485,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(SplitArgs p) {
         __syncwarp();
         if (lane == 0) tc::mbar_arrive(&full_a[stg]);
       }
-      seq0 += uint32_t(kc);
+      seq0 += uint32_t(kc - kc0);
       if (!ok) break;
       // ---- epilogue: group grp reduces points 32grp .. 32grp+31 over the
       // 32 rows of warp wq (TMEM lanes 32wq ..) ----
@@ -548,7 +557,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(SplitArgs p) {
         a[0] += __shfl_xor_sync(0xffffffffu, a[0], 2);
         a[0] += __shfl_xor_sync(0xffffffffu, a[0], 1);
         const int m = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
-        if ((lane & 3) == 0) p.partial[slot * TG + cc + m] = a[0];
+        if ((lane & 3) == 0) p.partial[slot * TG + cc + m] = sym ? 2.0 * a[0] : a[0];
       }
       tc::fence_before_sync();
       __syncwarp();
@@ -564,9 +573,10 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(SplitArgs p) {
         const int4 it = item_at(p, t, per_set);
         const int nb = batch_of(p, it.w).counts[it.x / p.gsub];
         const int kc = (nb + TK - 1) / TK;
+        const int kc0 = sym ? it.y * (TU / TK) : 0;
         if (nitem > 0 && !tc::mbar_wait(acc_empty, (nitem - 1) & 1, err, 13)) break;
         tc::fence_after_sync();
-        for (int c = 0; c < kc; ++c, ++seq) {
+        for (int c = kc0; c < kc; ++c, ++seq) {
           const int stg = int(seq % STAGES);
           const uint32_t par = (seq / STAGES) & 1;
           if (!tc::mbar_wait(&full_a[stg], par, err, 14) ||
@@ -582,7 +592,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(SplitArgs p) {
 #pragma unroll
             for (int i = 0; i <= L; ++i)
               tc::mma_i8(tmem + uint32_t(L * TG), tc::smem_desc_k32(a0 + i * A_SLICE),
-                         tc::smem_desc_k32(b0 + (L - i) * B_SLICE), idesc, c > 0 || i > 0);
+                         tc::smem_desc_k32(b0 + (L - i) * B_SLICE), idesc, c > kc0 || i > 0);
           tc::mma_commit(&empty[stg]);
         }
         if (!ok) break;
@@ -601,8 +611,9 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(SplitArgs p) {
         const SplitBatch& B = batch_of(p, it.w);
         const int nb = B.counts[it.x / p.gsub];
         const int kc = (nb + TK - 1) / TK;
+        const int kc0 = sym ? it.y * (TU / TK) : 0;
         const uint8_t* src = p.phisl + size_t(B.cbase[it.x]) * B_STAGE;
-        for (int c = 0; c < kc; ++c, ++seq) {
+        for (int c = kc0; c < kc; ++c, ++seq) {
           const int stg = int(seq % STAGES);
           const uint32_t use = seq / STAGES;
           if (use > 0 && !tc::mbar_wait(&empty[stg], (use - 1) & 1, err, 17)) {
@@ -745,7 +756,14 @@ cudaError_t aodmao2rho_split(double* rhos, const double* dms, const double* ao_l
   cudaError_t err = aodm_block_lists_launch(tab, ldtab, nao, nblk, lists, counts, stream);
   if (err != cudaSuccess) return err;
   split_build<<<1, 1024, 0, stream>>>(counts, nbg, gsub, nset, max_ut, cbase, items, total);
-  if ((err = split_prepare_d(dms, stride_ao, nao, nset, dsl, tau, stream)) != cudaSuccess) return err;
+  int* asym = aodm_sym_enabled() ? total + 2 : nullptr;  // total[2]: asymmetry flag
+  if (asym) {
+    if ((err = cudaMemsetAsync(asym, 0, sizeof(int), stream)) != cudaSuccess) return err;
+    if ((err = aodm_launch_sym_check(dms, stride_ao, nao, nset, asym, stream)) != cudaSuccess)
+      return err;
+  }
+  if ((err = split_prepare_d(dms, stride_ao, nao, nset, dsl, tau, stream, asym)) != cudaSuccess)
+    return err;
   if ((err = split_prepare_phi(ao_rhs, stride_grid, lists, counts, cbase, nao, ngrid, blk, pmax,
                                sigma, phisl, stream)) != cudaSuccess)
     return err;
@@ -763,14 +781,15 @@ cudaError_t aodmao2rho_split(double* rhos, const double* dms, const double* ao_l
   a.blk = blk;
   a.gsub = gsub;
   a.max_ut = max_ut;
+  a.asym = asym;
   if ((err = split_launch_main(a, stream)) != cudaSuccess) return err;
   return split_launch_reduce(a, nullptr, nbg, stream);
 }
 
 cudaError_t split_prepare_d(const double* dms, size_t stride_ao, int nao, int nset, uint2* dsl,
-                            int* tau, cudaStream_t stream) {
+                            int* tau, cudaStream_t stream, const int* asym) {
   split_d_slices<<<(nset * nao + 7) / 8, 256, 0, stream>>>(dms, stride_ao, stride_ao * stride_ao,
-                                                           nao, nset * nao, dsl, tau);
+                                                           nao, nset * nao, dsl, tau, asym);
   return cudaGetLastError();
 }
 

@@ -31,6 +31,10 @@ struct SplitArgs {
   const int* total;         // [0] items to run, [1] tiles per matrix (s < 0 lists)
   double* partial;          // [group][64]
   int nao, blk, gsub, max_ut;
+  const int* asym;          // null, or a flag that is 0 when every D_s is symmetric: then row
+                            // tile a contracts only the compacted columns from its own on
+                            // (the diagonal tile's strict upper triangle and half diagonal,
+                            // times 2), as in the FP64 kernel's symmetric mode
 };
 
 // Device scratch (bytes) of the split contraction: active lists, work list,
@@ -49,8 +53,10 @@ cudaError_t aodmao2rho_split(double* rhos, const double* dms, const double* ao_l
 //                     ngrid 8-byte scratch; cbase: device chunk offsets);
 //   split_launch_main / split_launch_reduce  the contraction and its reduction
 //                     over (batch, 64-point tile) pairs.
+// With asym non-null and *asym == 0 (symmetric mode) the diagonal entries'
+// digits are those of D_uu / 2.
 cudaError_t split_prepare_d(const double* dms, size_t stride_ao, int nao, int nset, uint2* dsl,
-                            int* tau, cudaStream_t stream);
+                            int* tau, cudaStream_t stream, const int* asym = nullptr);
 cudaError_t split_prepare_phi(const double* ao_rhs, size_t stride_grid, const int* lists,
                               const int* counts, const int* cbase, int nao, int ngrid, int blk,
                               unsigned long long* pmax, int* sigma, uint8_t* phisl,

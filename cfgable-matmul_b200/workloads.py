@@ -99,6 +99,25 @@ def masked_flops(tab: np.ndarray, ngrid: int, blksize: int, nset: int) -> float:
     return float(nset * np.sum((2.0 * nb * nb + 2.0 * nb) * sizes))
 
 
+def symmetric_flops(tab: np.ndarray, ngrid: int, blksize: int, nset: int,
+                    tile: int = 64) -> float:
+    """FLOPs the FP64 kernel's symmetric-D mode executes: row tile a of a block
+    (|I_b| compacted AOs in tiles of `tile`) contracts the compacted columns from
+    a*tile on, sum_s sum_b |b| (sum_a 2 m_a (|I_b| - a*tile) + 2 |I_b|) with
+    m_a = min(tile, |I_b| - a*tile)."""
+    nb = tab.astype(bool).sum(axis=0).astype(np.int64)
+    nblk = tab.shape[1]
+    sizes = np.full(nblk, float(blksize))
+    sizes[-1] = ngrid - blksize * (nblk - 1)
+    tot = 0.0
+    for n, w in zip(nb, sizes):
+        k = 0.0
+        for a0 in range(0, int(n), tile):
+            k += 2.0 * min(tile, n - a0) * (n - a0)
+        tot += (k + 2.0 * n) * w
+    return float(nset * tot)
+
+
 # ---------------------------------------------------------------------------
 # benchmark workloads
 # ---------------------------------------------------------------------------

@@ -91,3 +91,24 @@ def test_split_aodm_device_pointers_repeatable(cm, wl):
         outs.append(rho.cpu().numpy())
     assert np.array_equal(outs[0], outs[1])
     assert normwise(outs[0], wl.dense_rho(p.ao, p.ao, p.dms, p.tab, p.blksize)) < TOL
+
+
+@pytest.mark.parametrize("kind", ["symmetric", "one_entry_off", "general"])
+@pytest.mark.parametrize("nao", [296, 600])
+def test_split_symmetric_d_mode_and_its_check(cm, oracle, wl, kind, nao):
+    """Symmetric D takes the half contraction (row tiles of 128 from their own
+    compacted columns on, the diagonal tile's strict upper triangle and half
+    diagonal); one differing entry, or a general D, the full one.  The oracle
+    never assumes symmetry."""
+    p = wl.small_masked(seed=50 + nao, nao=nao, ngrid=2500, blksize=64, nset=2, density=0.5)
+    dms = p.dms.copy()
+    if kind == "one_entry_off":
+        dms[1, 17, nao - 5] += 10.0
+    elif kind == "general":
+        dms = np.random.default_rng(nao).uniform(-1, 1, dms.shape)
+    rho = np.zeros((2, p.ngrid))
+    ref = np.zeros((2, p.ngrid))
+    args = ((p.nao, p.ngrid), (p.nao, p.ngrid), 2, p.tab, p.nblk, 64)
+    split(cm, rho, dms, p.ao, p.ao, *args)
+    oracle.aodmao2rho(ref, dms, p.ao, p.ao, *args)
+    assert normwise(rho, ref) < TOL
