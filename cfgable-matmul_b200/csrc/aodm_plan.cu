@@ -495,12 +495,16 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
   }
   std::stable_sort(items.begin(), items.end(),
                    [](const int4& x, const int4& y) { return x.w > y.w; });
-  // ao_rhs gather maps of the pipelined form, if every batch allows TMA
+  // ao_rhs gather maps of the pipelined form (batches whose rows TMA cannot
+  // address are gathered by cp.async)
+  const bool pipe_ok = cfgmm::aodm_pipe_enabled();
   std::vector<CUtensorMap> maps(nbatch);
-  bool pipe_ok = true;
+  std::memset(maps.data(), 0, nbatch * sizeof(CUtensorMap));
   for (size_t i = 0; i < nbatch && pipe_ok; ++i)
-    pipe_ok = cfgmm::aodm_rhs_map(&maps[i], batches[i].ao_rhs, batches[i].stride_grid, int(nao),
-                                  int(batches[i].ngrid), int(blksize));
+    hb[i].rhs_tma = cfgmm::aodm_rhs_map(&maps[i], batches[i].ao_rhs, batches[i].stride_grid,
+                                        int(nao), int(batches[i].ngrid), int(blksize))
+                        ? 1
+                        : 0;
   plan->nitems = int(items.size());
   plan->npairs = int(pairs.size());
   plan->rpairs = reinterpret_cast<int2*>(base + o_pairs);

@@ -27,9 +27,10 @@
 //      The active list of the current block is staged in shared memory, so
 //      the gather addresses never wait on global loads.
 //   3b. aodm_fp64_pipe_kernel: the same items with producer warps (D by
-//      cp.async, ao_rhs rows by TMA gather4) and consumer warps (DMMA
-//      m16n8k8) meeting on mbarriers; used whenever ao_rhs allows TMA
-//      (16-byte aligned rows, even BLKSIZE), form 3 otherwise.
+//      cp.async; ao_rhs rows by TMA gather4 where the rows are 16-byte
+//      aligned and BLKSIZE is even, by cp.async otherwise) and consumer warps
+//      (DMMA m16n8k8) meeting on mbarriers; with a symmetric-D mode.  The
+//      form used; form 3 remains for CFGMM_AODM_PIPE=0.
 //   4. aodm_reduce: adds the per-row-tile partial sums of each grid tile in a
 //      fixed order, so results are deterministic run to run (unlike the
 //      reference, whose lock order varies).
@@ -535,21 +536,40 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
           for (int s = 0; s < t.ns; ++s)
             cp_async_8(dst + s * (D_BYTES / 8), valid ? src + s * p.dm_stride : src, valid);
         }
-        cp_async_arrive_noinc(&full[stage]);
-        if (tid < 32) {
-          // ao_rhs rows of the stage columns, from the lanes that gather them
-          // (lane j of warp 0 holds column j; D is zero past the list's end)
-          int rows[TK];
+        uint8_t* phi = st + NS * D_BYTES;
+        if (!t.B->rhs_tma) {
+          // ao_rhs rows [TK][TG] by cp.async: lanes along points; the row of
+          // stage column j comes from lane j of this warp (kcol = lane & 15)
+          const int pt = tid & (TG - 1);
+          const bool pv = t.g0 + pt < t.B->ngrid;
 #pragma unroll
-          for (int j = 0; j < TK; ++j) rows[j] = __shfl_sync(0xffffffffu, v, j);
-          uint8_t* phi = st + NS * D_BYTES;
-          if (tid == 0) {
-            tc::mbar_arrive_expect_tx(&full[stage], PHI_BYTES);
-#pragma unroll
-            for (int j = 0; j < TK / 4; ++j)
-              tma_gather4(phi + j * 4 * TG * 8, map, &full[stage], t.g0, rows[4 * j],
-                          rows[4 * j + 1], rows[4 * j + 2], rows[4 * j + 3]);
+          for (int i = 0; i < TK / (NPROD / TG); ++i) {
+            const int j = (tid / TG) + (NPROD / TG) * i;
+            const int row = __shfl_sync(0xffffffffu, v, j);
+            cp_async_8(reinterpret_cast<double*>(phi) + j * TG + pt,
+                       pv ? t.B->ao_rhs + size_t(row) * t.B->stride_grid + t.g0 + pt
+                          : t.B->ao_rhs,
+                       pv);
           }
+        }
+        cp_async_arrive_noinc(&full[stage]);
+        if (t.B->rhs_tma) {
+          if (tid < 32) {
+            // ao_rhs rows of the stage columns, from the lanes that gather them
+            // (lane j of warp 0 holds column j; D is zero past the list's end)
+            int rows[TK];
+#pragma unroll
+            for (int j = 0; j < TK; ++j) rows[j] = __shfl_sync(0xffffffffu, v, j);
+            if (tid == 0) {
+              tc::mbar_arrive_expect_tx(&full[stage], PHI_BYTES);
+#pragma unroll
+              for (int j = 0; j < TK / 4; ++j)
+                tma_gather4(phi + j * 4 * TG * 8, map, &full[stage], t.g0, rows[4 * j],
+                            rows[4 * j + 1], rows[4 * j + 2], rows[4 * j + 3]);
+            }
+          }
+        } else if (tid == 0) {
+          tc::mbar_arrive(&full[stage]);  // the arrival the TMA's expect_tx makes otherwise
         }
       }
     }
@@ -818,11 +838,13 @@ bool pipe_enabled() {
 
 }  // namespace
 
+bool aodm_pipe_enabled() { return pipe_enabled(); }
+
 bool aodm_rhs_map(CUtensorMap* map, const double* ao_rhs, size_t stride_grid, int nao, int ngrid,
                   int blk) {
   // TMA: 16-byte aligned base and row pitch; the x coordinate of every load
   // (a 64-point tile start b*blk + 64*gt) must be even, so blk must be even.
-  if (!pipe_enabled() || nao <= 0 || ngrid <= 0 || blk % 2 != 0 ||
+  if (nao <= 0 || ngrid <= 0 || blk % 2 != 0 ||
       reinterpret_cast<uintptr_t>(ao_rhs) % 16 != 0 || (stride_grid * sizeof(double)) % 16 != 0)
     return false;
   auto enc = encode_tiled();
@@ -977,8 +999,9 @@ cudaError_t aodmao2rho_fp64(double* rhos, const double* dms, const double* ao_lh
   a.counters = counters;
   a.ngroups = ngroups;
   a.partial = partial;
-  CUtensorMap map;
-  if (aodm_rhs_map(&map, ao_rhs, stride_grid, nao, ngrid, blk)) {
+  CUtensorMap map{};
+  if (pipe_enabled()) {
+    a.one.rhs_tma = aodm_rhs_map(&map, ao_rhs, stride_grid, nao, ngrid, blk) ? 1 : 0;
     if (aodm_sym_enabled()) {
       a.asym = counters + ngroups + 1;
       if ((err = aodm_launch_sym_check(dms, stride_ao, nao, nset, counters + ngroups + 1,

@@ -18,6 +18,7 @@ struct AodmBatch {
   int ngrid;
   int nset;                // density matrices used by this batch (<= nset_max)
   long long partial_off;   // first partial-sum slot of this batch
+  int rhs_tma;             // pipelined form: ao_rhs rows by TMA (its map is valid), else cp.async
 };
 
 // Kernel arguments: density matrices shared by all batches, and either a
@@ -77,11 +78,14 @@ cudaError_t aodm_launch_main(const AodmArgs& a, const AodmConfig& cfg, cudaStrea
 cudaError_t aodm_launch_reduce(const AodmArgs& a, const int2* rpairs, int npairs,
                                cudaStream_t stream);
 
-// Pipelined form of the main kernel (warp-specialised, ao_rhs rows by TMA
-// gather4).  aodm_rhs_map builds the gather map of one ao_rhs table and returns
-// false where the form does not apply (base or row pitch not 16-byte aligned,
-// odd BLKSIZE, CFGMM_AODM_PIPE=0).  `map` is used when a.batches is null,
-// a.rhs_maps (a 64-byte aligned device array, one map per batch) otherwise.
+// Pipelined form of the main kernel (warp-specialised; ao_rhs rows by TMA
+// gather4 where AodmBatch::rhs_tma is set, by the producers' cp.async
+// otherwise).  aodm_rhs_map builds the gather map of one ao_rhs table and
+// returns false where TMA does not apply (base or row pitch not 16-byte
+// aligned, odd BLKSIZE).  `map` is used when a.batches is null, a.rhs_maps
+// (a 64-byte aligned device array, one map per batch) otherwise.
+// aodm_pipe_enabled() is false when CFGMM_AODM_PIPE=0 (form 3 then runs).
+bool aodm_pipe_enabled();
 bool aodm_rhs_map(CUtensorMap* map, const double* ao_rhs, size_t stride_grid, int nao, int ngrid,
                   int blk);
 cudaError_t aodm_launch_pipe(const AodmArgs& a, int ns, const CUtensorMap& map,

@@ -149,10 +149,10 @@ def test_device_pointers_and_determinism(cm, wl):
 
 @pytest.mark.parametrize("stride_pad", [0, 1])
 def test_pipelined_and_plain_forms_agree(cm, oracle, stride_pad):
-    """The pipelined kernel (TMA gather of phi rows; used when the rows are
-    16-byte aligned and BLKSIZE is even) and the form it replaces, forced with
-    CFGMM_AODM_PIPE=0, on the same inputs; an odd row pitch (stride_pad 1)
-    takes the plain form in both runs.  Both within 1e-13 of the oracle."""
+    """The pipelined kernel and the form it replaces, forced with
+    CFGMM_AODM_PIPE=0, on the same inputs; the pipelined kernel fetches the
+    phi rows by TMA gather4 when they are 16-byte aligned (stride_pad 0) and
+    by cp.async otherwise (stride_pad 1).  Both within 1e-13 of the oracle."""
     import json, os, subprocess, sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     tmp = os.environ.get("TMPDIR", "/tmp")

@@ -119,7 +119,9 @@ def test_autotune_cache(cm, wl, tmp_path, monkeypatch):
     dev, ddms = _device(torch, bs, dms)
     p1 = cm.AodmPlan(dev, ddms, blksize=64)
     i1 = p1.info()
-    assert isinstance(i1["tuning"], list) and len(i1["tuning"]) == 6
+    # ns 1..3 for each form: the pipelined kernel (tk 0) and form 3 at tk 32, 16
+    assert isinstance(i1["tuning"], list) and len(i1["tuning"]) == 9
+    assert sorted({t["tk"] for t in i1["tuning"]}) == [0, 16, 32]
     assert min(t["ms"] for t in i1["tuning"]) > 0
     lines = path.read_text().split()
     assert lines[0] == i1["key"]
