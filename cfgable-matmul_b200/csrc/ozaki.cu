@@ -192,11 +192,17 @@ __global__ void finalize_exps(const int* __restrict__ emax, int rows, int bits, 
 
 // ---------------------------------------------------------------------------
 // residues: Y[l][r][p] = rint(x(r,p) 2^e[r]) mods m_l  (int8), p < k
-// The integer v (|v| <= 2^52) is split into 14-bit chunks
-// v = d3 2^42 + d2 2^28 + d1 2^14 + d0 (d3 signed, |d3| <= 2^10; d0..d2 in
-// [0, 2^14)); with symmetric c_t = 2^(14t) mods m (|c_t| <= 127) the sum
-// s = d3 c3 + d2 c2 + d1 c1 + d0 is exact in FP32 (|s| < 2^23) and congruent to
-// v, so v mods m follows from one FP32 quotient and one correction.
+// The integer v (|v| <= 2^52) is written in balanced 14-bit digits:
+// w = v + 2^13 (1 + 2^14 + 2^28) gives u_t = (w >> 14t) & 0x3fff (t < 3) and
+// d_3 = w >> 42 with v = sum_{t<3} (u_t - 2^13) 2^14t + d_3 2^42.  With the
+// symmetric c_t = 2^(14t) mods m (|c_t| <= 127) and K = -2^13 (1 + c_14 + c_28)
+//   s = u_0 + K + u_1 c_14 + u_2 c_28 + d_3 c_42,   |s| < 2.3e6 < 2^22,
+// is exact in FP32 and congruent to v.  Then q = rint(s / m) comes out exact
+// from one FMA against MAGIC = 1.5 2^23 (|s| < 2^22 keeps the error of s*inv
+// below 1/(2m), the least distance of s/m from a half-integer for odd m), the
+// residue r = s - m q is exact, and r + MAGIC holds r in the low byte of its
+// bits.  Two elements go through each packed FP32x2 instruction (sm_100).
+// Modulus 256 is the low byte of v's two's complement.
 // ---------------------------------------------------------------------------
 struct ResidueArgs {
   int nmod;
@@ -205,48 +211,93 @@ struct ResidueArgs {
   float c14[kMaxModuli], c28[kMaxModuli], c42[kMaxModuli];
 };
 
-__device__ __forceinline__ int8_t mods_f(float s, float m, float inv, float hi, float lo) {
-  const float q = rintf(s * inv);
-  float r = fmaf(-m, q, s);  // exact: |r| <= 1.5 m
-  if (r > hi) r -= m;
-  else if (r < lo) r += m;
-  return int8_t(__float2int_rn(r));
+using f32x2 = unsigned long long;  // two FP32 lanes in a 64-bit register
+
+__device__ __forceinline__ f32x2 pack2(float lo, float hi) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void unpack2(f32x2 v, uint32_t& lo, uint32_t& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=r"(lo), "=r"(hi) : "l"(v));
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
 }
 
+// rint(x 2^e) for a row exponent e (0 for a row holding Inf/NaN).  The power
+// of two is applied as one or two exact multiplications (ldexp outside the
+// normal range of the factor).
 __device__ __forceinline__ double scaled_int(double x, int e) {
-  return (e == kNonFinite) ? 0.0 : rint(ldexp(x, e));
+  if (e == kNonFinite) return 0.0;
+  if (e >= -1022 && e <= 1023)
+    return rint(x * __longlong_as_double(static_cast<long long>(e + 1023) << 52));
+  return rint(ldexp(x, e));
 }
 
-__device__ __forceinline__ void write_residues(const ResidueArgs& a, int8_t* Y, size_t plane,
-                                               size_t off, const double (&v)[4]) {
-  float d0[4], d1[4], d2[4], d3[4];
-  char4 b256;
-  int8_t* b = reinterpret_cast<int8_t*>(&b256);
+// The residues of 8 consecutive elements v[0..7] (integers, |v| <= 2^52) for
+// every modulus, 8 bytes per modulus plane at Y + l * plane + off (8-byte
+// aligned).
+__device__ __forceinline__ void write_residues8(const ResidueArgs& a, int8_t* Y, size_t plane,
+                                                size_t off, const double (&v)[8]) {
+  constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23
+  constexpr long long kBias = 8192LL * (1 + (1LL << 14) + (1LL << 28));
+  f32x2 P0[4], P1[4], P2[4], P3[4];
+  uint32_t lowb[2] = {0u, 0u};
 #pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const long long iv = static_cast<long long>(v[j]);
-    b[j] = int8_t(iv);  // modulus 256: the low byte of the two's complement
-    d3[j] = float(iv >> 42);
-    d2[j] = float(int((iv >> 28) & 0x3fff));
-    d1[j] = float(int((iv >> 14) & 0x3fff));
-    d0[j] = float(int(iv & 0x3fff));
-  }
-  *reinterpret_cast<char4*>(Y + off) = b256;
-  for (int l = 1; l < a.nmod; ++l) {
-    const float m = float(a.mod[l]), inv = a.inv[l];
-    const float hi = float((a.mod[l] - 1) >> 1), lo = -float(a.mod[l] >> 1);
-    char4 out;
-    int8_t* o = reinterpret_cast<int8_t*>(&out);
+  for (int j = 0; j < 8; j += 2) {
+    float u[2][4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const float s = fmaf(d3[j], a.c42[l], fmaf(d2[j], a.c28[l], fmaf(d1[j], a.c14[l], d0[j])));
-      o[j] = mods_f(s, m, inv, hi, lo);
+    for (int h = 0; h < 2; ++h) {
+      const long long iv = static_cast<long long>(v[j + h]);
+      lowb[(j + h) >> 2] |= uint32_t(iv & 0xff) << (8 * ((j + h) & 3));  // modulus 256
+      const long long w = iv + kBias;
+      u[h][0] = float(int(w & 0x3fff));
+      u[h][1] = float(int((w >> 14) & 0x3fff));
+      u[h][2] = float(int((w >> 28) & 0x3fff));
+      u[h][3] = float(int(w >> 42));
     }
-    *reinterpret_cast<char4*>(Y + size_t(l) * plane + off) = out;
+    P0[j >> 1] = pack2(u[0][0], u[1][0]);
+    P1[j >> 1] = pack2(u[0][1], u[1][1]);
+    P2[j >> 1] = pack2(u[0][2], u[1][2]);
+    P3[j >> 1] = pack2(u[0][3], u[1][3]);
+  }
+  *reinterpret_cast<uint2*>(Y + off) = make_uint2(lowb[0], lowb[1]);
+  const f32x2 MAG = pack2(kMagic, kMagic), NMAG = pack2(-kMagic, -kMagic);
+  for (int l = 1; l < a.nmod; ++l) {
+    const float k0 = -8192.0f * (1.0f + a.c14[l] + a.c28[l]);
+    const f32x2 K = pack2(k0, k0), C14 = pack2(a.c14[l], a.c14[l]),
+                C28 = pack2(a.c28[l], a.c28[l]), C42 = pack2(a.c42[l], a.c42[l]),
+                INV = pack2(a.inv[l], a.inv[l]);
+    const float nm = -float(a.mod[l]);
+    const f32x2 NM = pack2(nm, nm);
+    uint32_t bits[8];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      f32x2 S = add2(P0[q], K);
+      S = fma2(P1[q], C14, S);
+      S = fma2(P2[q], C28, S);
+      S = fma2(P3[q], C42, S);                      // s, exact
+      const f32x2 Q = add2(fma2(S, INV, MAG), NMAG);  // rint(s / m), exact
+      const f32x2 R = add2(fma2(NM, Q, S), MAG);      // (s - m q) + MAGIC
+      unpack2(R, bits[2 * q], bits[2 * q + 1]);
+    }
+    const uint32_t w0 = __byte_perm(__byte_perm(bits[0], bits[1], 0x0040),
+                                    __byte_perm(bits[2], bits[3], 0x0040), 0x5410);
+    const uint32_t w1 = __byte_perm(__byte_perm(bits[4], bits[5], 0x0040),
+                                    __byte_perm(bits[6], bits[7], 0x0040), 0x5410);
+    *reinterpret_cast<uint2*>(Y + size_t(l) * plane + off) = make_uint2(w0, w1);
   }
 }
 
-// element (r, p) at x[r*ld + p]: CTA per row, thread per 4 consecutive p
+// element (r, p) at x[r*ld + p]: CTA per row, thread per 8 consecutive p
 __global__ void __launch_bounds__(256)
 residues_rows(const double* __restrict__ x, size_t ld, int rows, int k, size_t kpad,
               const int* __restrict__ e, int8_t* __restrict__ Y, ResidueArgs a) {
@@ -255,11 +306,11 @@ residues_rows(const double* __restrict__ x, size_t ld, int rows, int k, size_t k
   const int er = e[r];
   const double* row = x + size_t(r) * ld;
   const size_t plane = size_t(rows) * kpad;
-  for (int p = 4 * threadIdx.x; p < k; p += 4 * 256) {
-    double v[4];
+  for (int p = 8 * threadIdx.x; p < k; p += 8 * 256) {
+    double v[8];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) v[j] = (p + j < k) ? scaled_int(row[p + j], er) : 0.0;
-    write_residues(a, Y, plane, size_t(r) * kpad + p, v);
+    for (int j = 0; j < 8; ++j) v[j] = (p + j < k) ? scaled_int(row[p + j], er) : 0.0;
+    write_residues8(a, Y, plane, size_t(r) * kpad + p, v);
   }
 }
 
@@ -270,23 +321,22 @@ residues_cols(const double* __restrict__ x, size_t ld, int rows, int k, size_t k
   __shared__ double tile[64][33];
   const int r0 = blockIdx.x * 32, p0 = blockIdx.y * 64;
   const int tr = threadIdx.x & 31, tp = threadIdx.x >> 5;  // 8 rows of p per pass
+#pragma unroll
   for (int pp = tp; pp < 64; pp += 8) {
     const int p = p0 + pp, r = r0 + tr;
     tile[pp][tr] = (p < k && r < rows && mask.on(r, p)) ? x[size_t(p) * ld + r] : 0.0;
   }
   __syncthreads();
   const size_t plane = size_t(rows) * kpad;
-  // 32 rows x 16 groups of 4 p = 512 units, 2 per thread
-  for (int u = threadIdx.x; u < 512; u += 256) {
-    const int rr = u >> 4, pg = (u & 15) * 4;
-    const int r = r0 + rr, p = p0 + pg;
-    if (r >= rows || p >= k) continue;
-    const int er = e[r];
-    double v[4];
+  // 32 rows x 8 groups of 8 p: one unit per thread
+  const int rr = threadIdx.x >> 3, pg = (threadIdx.x & 7) * 8;
+  const int r = r0 + rr, p = p0 + pg;
+  if (r >= rows || p >= k) return;
+  const int er = e[r];
+  double v[8];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) v[j] = (p + j < k) ? scaled_int(tile[pg + j][rr], er) : 0.0;
-    write_residues(a, Y, plane, size_t(r) * kpad + p, v);
-  }
+  for (int j = 0; j < 8; ++j) v[j] = (p + j < k) ? scaled_int(tile[pg + j][rr], er) : 0.0;
+  write_residues8(a, Y, plane, size_t(r) * kpad + p, v);
 }
 
 // ---------------------------------------------------------------------------
@@ -294,43 +344,70 @@ residues_cols(const double* __restrict__ x, size_t ld, int rows, int k, size_t k
 // ---------------------------------------------------------------------------
 struct ReconArgs {
   int nmod;
-  double w_frac[kMaxModuli], w_hi[kMaxModuli], w_lo[kMaxModuli];
+  double w_hi[kMaxModuli], w_lo[kMaxModuli];
+  float w_frac_f[kMaxModuli];  // w_l / M in FP32 (for the quotient only)
   double M_hi, M_lo, two_T;
 };
 
+// A thread rebuilds 8 consecutive C[i][j]: all its residue loads are issued
+// before the arithmetic (8 bytes per modulus plane), so the loads of a warp are
+// in flight together.  q = rint(t) takes t in FP32: |C'| <= M/8 keeps t within
+// 1/8 of the integer q, far above the FP32 error of sum_l r_l w_l / M (below
+// 2^-9 for |r_l| <= 128, N <= 16), so q is the one of exact arithmetic; the
+// hi / lo sums stay in FP64.
 __global__ void __launch_bounds__(256)
 reconstruct(double* __restrict__ c, size_t ldc, int m, int n, const int8_t* __restrict__ R,
             size_t ldr, const int* __restrict__ ea, const int* __restrict__ eb, ReconArgs a) {
-  const int bpr = (n + 1023) / 1024;  // CTAs per row of C
+  const int bpr = (n + 2047) / 2048;  // CTAs per row of C
   const int i = blockIdx.x / bpr;
-  const int j0 = ((blockIdx.x % bpr) * 256 + threadIdx.x) * 4;
+  const int j0 = ((blockIdx.x % bpr) * 256 + threadIdx.x) * 8;
   if (j0 >= n || i >= m) return;
   const size_t plane = size_t(m) * ldr;
+  // ldr is a multiple of 16 and j0 of 8: the 8 bytes at j0 lie inside row i
   const int8_t* Ri = R + size_t(i) * ldr + j0;
-  double t[4] = {0, 0, 0, 0}, X[4] = {0, 0, 0, 0}, Y[4] = {0, 0, 0, 0};
-  for (int l = 0; l < a.nmod; ++l) {
-    const char4 r4 = *reinterpret_cast<const char4*>(Ri + size_t(l) * plane);
-    const double rv[4] = {double(r4.x), double(r4.y), double(r4.z), double(r4.w)};
+  uint2 rv[kMaxModuli];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      t[u] = fma(rv[u], a.w_frac[l], t[u]);
-      X[u] = fma(rv[u], a.w_hi[l], X[u]);  // exact: every partial sum < 2^53
-      Y[u] = fma(rv[u], a.w_lo[l], Y[u]);
+  for (int l = 0; l < kMaxModuli; ++l)
+    if (l < a.nmod) rv[l] = __ldg(reinterpret_cast<const uint2*>(Ri + size_t(l) * plane));
+  float t[8];
+  double X[8], Y[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    t[u] = 0.f;
+    X[u] = Y[u] = 0.0;
+  }
+#pragma unroll
+  for (int l = 0; l < kMaxModuli; ++l) {
+    if (l >= a.nmod) break;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const uint32_t w = u < 4 ? rv[l].x : rv[l].y;
+      const int ri = static_cast<int8_t>(w >> (8 * (u & 3)));
+      const double r = double(ri);
+      t[u] = fmaf(float(ri), a.w_frac_f[l], t[u]);
+      X[u] = fma(r, a.w_hi[l], X[u]);  // exact: every partial sum < 2^53
+      Y[u] = fma(r, a.w_lo[l], Y[u]);
     }
   }
   const int ei = ea[i];
   double* ci = c + size_t(i) * ldc;
 #pragma unroll
-  for (int u = 0; u < 4; ++u) {
+  for (int u = 0; u < 8; ++u) {
     const int j = j0 + u;
     if (j >= n) break;
     const int fj = eb[j];
-    const double q = rint(t[u]);
+    const double q = double(rintf(t[u]));
     const double hi = fma(-q, a.M_hi, X[u]);  // exact
     const double lo = fma(-q, a.M_lo, Y[u]);
     const double cp = fma(hi, a.two_T, lo);   // C' with one rounding
-    const double val = (ei == kNonFinite || fj == kNonFinite) ? __longlong_as_double(0x7ff8000000000000LL)
-                                                              : ldexp(cp, -(ei + fj));
+    const int sc = -(ei + fj);
+    double val;
+    if (ei == kNonFinite || fj == kNonFinite)
+      val = __longlong_as_double(0x7ff8000000000000LL);
+    else if (sc >= -1022 && sc <= 1023)  // exact scaling by a normal power of two
+      val = cp * __longlong_as_double(static_cast<long long>(sc + 1023) << 52);
+    else
+      val = ldexp(cp, sc);
     ci[j] += val;
   }
 }
@@ -494,14 +571,14 @@ cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int 
   ReconArgs rc{};
   rc.nmod = plan.nmod;
   for (int l = 0; l < plan.nmod; ++l) {
-    rc.w_frac[l] = plan.w_frac[l];
+    rc.w_frac_f[l] = float(plan.w_frac[l]);
     rc.w_hi[l] = plan.w_hi[l];
     rc.w_lo[l] = plan.w_lo[l];
   }
   rc.M_hi = plan.M_hi;
   rc.M_lo = plan.M_lo;
   rc.two_T = plan.two_T;
-  const long long rgrid = (long long)((n + 1023) / 1024) * m;
+  const long long rgrid = (long long)((n + 2047) / 2048) * m;
   if (rgrid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
   reconstruct<<<unsigned(rgrid), 256, 0, stream>>>(c, ldc, m, n, r, L.ldr, ea, eb, rc);
   mark(3);
