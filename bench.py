@@ -591,7 +591,9 @@ def run_ours(args, ranks: Ranks):
         "roofline": {"bound": "tensor", "achieved": i8_achieved, "peak": i8_peak,
                      "unit": "TOP/s (INT8)", "frac": i8_achieved / i8_peak,
                      "traffic": profile_traffic("gemm_i8_mod_3527x9583x6581"),
-                     "kernel": "gemm_i8_mod_kernel", "kernel_ms": gemm_ms,
+                     "kernel": "gemm_i8_mod_pair_kernel (CTA pairs, tcgen05.mma.cta_group::2)"
+                               if os.environ.get("CFGMM_GEMM_PAIR", "1") != "0"
+                               else "gemm_i8_mod_kernel", "kernel_ms": gemm_ms,
                      "work": f"{nmod} x 2mnk INT8 ops per launch",
                      "peak_source": "measured in this run: tcgen05.mma kind::i8 128x256x32 loop "
                                     "on every SM (burst)"},
@@ -618,7 +620,9 @@ def run_ours(args, ranks: Ranks):
                 "d2h_bytes_per_step": 8 * M * N,
                 "path": "cfgmm_matmul_ex(CFGMM_PREC_OZAKI_INT8) on pinned host buffers "
                         "(synchronous)"},
-        "gpu_launches": 6 * args.steps,
+        # per split step: emax, exponents and residues of A (3) and of B (4, with
+        # the fill of the column maxima), the INT8 GEMM, the reconstruction
+        "gpu_launches": 9 * args.steps,
         "clocks": clk,
         "aodmao2rho": aodm,
     }
