@@ -129,6 +129,14 @@ def lib() -> ctypes.CDLL:
         L.cfgmm_aodm_fock.restype = I
         L.cfgmm_aodm_fock_dev.argtypes = [P, P, P, P, S, S, S, S, S, P, S, S, P]
         L.cfgmm_aodm_fock_dev.restype = I
+        L.cfgmm_matmul_f32.argtypes = [P, S, P, S, P, S] + [S] * 6 + [U8, U8, I]
+        L.cfgmm_matmul_f32.restype = I
+        L.cfgmm_matmul_f32_dev.argtypes = [P, P, P] + [S] * 6 + [U8, U8, I, P]
+        L.cfgmm_matmul_f32_dev.restype = I
+        L.cfgmm_aodmao2rho_f32.argtypes = aodm_host + [S, I]
+        L.cfgmm_aodmao2rho_f32.restype = I
+        L.cfgmm_aodmao2rho_f32_dev.argtypes = [P, P, P, P, S, S, S, S, S, P, S, S, I, P]
+        L.cfgmm_aodmao2rho_f32_dev.restype = I
         L.cfgmm_aodm_plan_create.argtypes = [ctypes.POINTER(P), ctypes.POINTER(_Batch), S, P, S,
                                              S, S, S, I, I, P]
         L.cfgmm_aodm_plan_create.restype = I
@@ -320,6 +328,42 @@ def aodmao2rho_noalloc(rhos, dms, ao_lhs, ao_rhs, strides, shape, nset, tab, ldt
         _dev(rhos, "torch.float64"), _dev(dms, "torch.float64"), _dev(ao_lhs, "torch.float64"),
         _dev(ao_rhs, "torch.float64"), stride_ao, stride_grid, nao, ngrid, nset,
         _dev(tab, "torch.uint8"), ldtab, blksize, _stream_ptr()))
+
+
+def matmul_f32(c, a, b, m, n, k, lda, ldb, ldc, transa, transb, precision=PREC_FP64) -> None:
+    """C += op(A) op(B) on f32 data (MatmulLoops<f32>; the reference implements
+    only f64, src/structs.rs:19-20): f64 arithmetic inside, one rounding to f32.
+    numpy float32 arrays (synchronous) or float32 CUDA tensors (current stream)."""
+    if _is_torch(c):
+        return _raise(lib().cfgmm_matmul_f32_dev(
+            _dev(c, "torch.float32"), _dev(a, "torch.float32"), _dev(b, "torch.float32"),
+            m, n, k, lda, ldb, ldc, int(transa), int(transb), precision, _stream_ptr()))
+    pc, lc = _host(c, np.float32, True)
+    pa, la = _host(a, np.float32)
+    pb, lb = _host(b, np.float32)
+    _raise(lib().cfgmm_matmul_f32(pc, lc, pa, la, pb, lb, m, n, k, lda, ldb, ldc, int(transa),
+                                  int(transb), precision))
+
+
+def aodmao2rho_f32(rhos, dms, ao_lhs, ao_rhs, strides, shape, nset, tab, ldtab, blksize=48,
+                   precision=PREC_FP64) -> None:
+    """The masked AO-DM-AO contraction on f32 data, f64 arithmetic inside and
+    one rounding of rho to f32; arguments as aodmao2rho_ex."""
+    stride_ao, stride_grid = strides
+    nao, ngrid = shape
+    tab = _as_tab(tab)
+    if _is_torch(rhos):
+        return _raise(lib().cfgmm_aodmao2rho_f32_dev(
+            _dev(rhos, "torch.float32"), _dev(dms, "torch.float32"), _dev(ao_lhs, "torch.float32"),
+            _dev(ao_rhs, "torch.float32"), stride_ao, stride_grid, nao, ngrid, nset,
+            _dev(tab, "torch.uint8"), ldtab, blksize, precision, _stream_ptr()))
+    pr, lr = _host(rhos, np.float32, True)
+    pd, ld = _host(dms, np.float32)
+    pl, ll = _host(ao_lhs, np.float32)
+    pq, lq = _host(ao_rhs, np.float32)
+    pt, lt = _host(tab, np.uint8)
+    _raise(lib().cfgmm_aodmao2rho_f32(pr, lr, pd, ld, pl, ll, pq, lq, stride_ao, stride_grid, nao,
+                                      ngrid, nset, pt, lt, ldtab, blksize, precision))
 
 
 def aodm_fock(vs, ws, ao_lhs, ao_rhs, strides, shape, nset, tab, ldtab, blksize=48) -> None:

@@ -21,6 +21,7 @@
 #include "aodmao2rho_split.cuh"
 #include "ao_eval.cuh"
 #include "dgemm_fp64.cuh"
+#include "f32.cuh"
 #include "gemm_i8.cuh"
 #include "ozaki.cuh"
 
@@ -137,7 +138,8 @@ struct GemmExtents {
   size_t a, b, c;
 };
 
-int check_gemm(const double* c, size_t c_len, const double* a, size_t a_len, const double* b,
+// Element counts only (any element type): pointers are checked for null.
+int check_gemm(const void* c, size_t c_len, const void* a, size_t a_len, const void* b,
                size_t b_len, size_t m, size_t n, size_t k, size_t lda, size_t ldb, size_t ldc,
                bool ta, bool tb, GemmExtents* ex) {
   if (m == 0 || n == 0 || k == 0) {
@@ -282,8 +284,8 @@ struct AodmExtents {
   size_t rhos, dms, ao, tab;
 };
 
-int check_aodm(const double* rhos, size_t rhos_len, const double* dms, size_t dms_len,
-               const double* ao_lhs, size_t ao_lhs_len, const double* ao_rhs, size_t ao_rhs_len,
+int check_aodm(const void* rhos, size_t rhos_len, const void* dms, size_t dms_len,
+               const void* ao_lhs, size_t ao_lhs_len, const void* ao_rhs, size_t ao_rhs_len,
                size_t stride_ao, size_t stride_grid, size_t nao, size_t ngrid, size_t nset,
                const uint8_t* tab, size_t tab_len, size_t ldtab, size_t blksize,
                AodmExtents* ex) {
@@ -456,6 +458,80 @@ int fock_host(double* vs, size_t vs_len, const double* ws, size_t ws_len, const 
   CFGMM_CUDA(cudaMemcpyAsync(vs, d_v, ex.dms * 8, cudaMemcpyDeviceToHost, st->stream));
   CFGMM_CUDA(cudaStreamSynchronize(st->stream));
   return check_device_waits();
+}
+
+// ---------------------------------------------------------------------------
+// f32 forms: operands widened exactly to f64 in stream-ordered scratch, the f64
+// kernels, the result rounded back to f32 once.
+// ---------------------------------------------------------------------------
+struct StreamScratch {
+  cudaStream_t s;
+  std::vector<void*> blocks;
+  explicit StreamScratch(cudaStream_t st) : s(st) {}
+  ~StreamScratch() {
+    for (void* q : blocks) cudaFreeAsync(q, s);
+  }
+  cudaError_t get(void** out, size_t bytes) {
+    const cudaError_t e = cudaMallocAsync(out, bytes > 0 ? bytes : 1, s);
+    if (e == cudaSuccess) blocks.push_back(*out);
+    return e;
+  }
+};
+
+constexpr int kF32OperandBits = 26;  // f32 mantissa (24 bits) and two guard bits
+
+int matmul_f32_run(float* c, const float* a, const float* b, size_t m, size_t n, size_t k,
+                   size_t lda, size_t ldb, size_t ldc, bool ta, bool tb, const GemmExtents& ex,
+                   int precision, cudaStream_t s) {
+  StreamScratch sc(s);
+  double *da = nullptr, *db = nullptr, *dc = nullptr;
+  CFGMM_CUDA(sc.get(reinterpret_cast<void**>(&da), ex.a * 8));
+  CFGMM_CUDA(sc.get(reinterpret_cast<void**>(&db), ex.b * 8));
+  CFGMM_CUDA(sc.get(reinterpret_cast<void**>(&dc), ex.c * 8));
+  CFGMM_CUDA(cfgmm::widen_f32(a, da, ex.a, s));
+  CFGMM_CUDA(cfgmm::widen_f32(b, db, ex.b, s));
+  CFGMM_CUDA(cfgmm::widen_f32(c, dc, ex.c, s));
+  if (precision == CFGMM_PREC_OZAKI_INT8) {
+    const int nmod = cfgmm::ozaki_moduli_for_bits(int(k), kF32OperandBits);
+    void* ws = nullptr;
+    CFGMM_CUDA(sc.get(&ws, cfgmm::ozaki_dgemm_workspace(int(m), int(n), int(k), nmod)));
+    CFGMM_CUDA(cfgmm::ozaki_dgemm(dc, da, db, int(m), int(n), int(k), lda, ldb, ldc, ta, tb, nmod,
+                                  ws, s));
+  } else {
+    CFGMM_CUDA(cfgmm::dgemm_fp64(dc, da, db, int(m), int(n), int(k), lda, ldb, ldc, ta, tb, s));
+  }
+  CFGMM_CUDA(cfgmm::narrow_f64(dc, c, ex.c, s));
+  return CFGMM_OK;
+}
+
+int aodm_f32_run(float* rhos, const float* dms, const float* ao_lhs, const float* ao_rhs,
+                 size_t stride_ao, size_t stride_grid, size_t nao, size_t ngrid, size_t nset,
+                 const uint8_t* tab, size_t ldtab, size_t blksize, const AodmExtents& ex,
+                 int precision, cudaStream_t s) {
+  StreamScratch sc(s);
+  const bool same_ao = ao_lhs == ao_rhs;
+  double *d_rho = nullptr, *d_dms = nullptr, *d_lhs = nullptr, *d_rhs = nullptr;
+  CFGMM_CUDA(sc.get(reinterpret_cast<void**>(&d_rho), ex.rhos * 8));
+  CFGMM_CUDA(sc.get(reinterpret_cast<void**>(&d_dms), ex.dms * 8));
+  CFGMM_CUDA(sc.get(reinterpret_cast<void**>(&d_lhs), ex.ao * 8));
+  if (!same_ao) CFGMM_CUDA(sc.get(reinterpret_cast<void**>(&d_rhs), ex.ao * 8));
+  CFGMM_CUDA(cfgmm::widen_f32(rhos, d_rho, ex.rhos, s));
+  CFGMM_CUDA(cfgmm::widen_f32(dms, d_dms, ex.dms, s));
+  CFGMM_CUDA(cfgmm::widen_f32(ao_lhs, d_lhs, ex.ao, s));
+  if (!same_ao) CFGMM_CUDA(cfgmm::widen_f32(ao_rhs, d_rhs, ex.ao, s));
+  const bool split = precision == CFGMM_PREC_OZAKI_INT8;
+  void* ws = nullptr;
+  CFGMM_CUDA(sc.get(&ws, split ? cfgmm::aodmao2rho_split_workspace(nao, ngrid, nset, blksize)
+                               : cfgmm::aodmao2rho_fp64_workspace(nao, ngrid, nset, blksize)));
+  const double* rhs = same_ao ? d_lhs : d_rhs;
+  CFGMM_CUDA(split ? cfgmm::aodmao2rho_split(d_rho, d_dms, d_lhs, rhs, stride_ao, stride_grid,
+                                             int(nao), int(ngrid), int(nset), tab, ldtab,
+                                             int(blksize), ws, s)
+                   : cfgmm::aodmao2rho_fp64(d_rho, d_dms, d_lhs, rhs, stride_ao, stride_grid,
+                                            int(nao), int(ngrid), int(nset), tab, ldtab,
+                                            int(blksize), ws, s));
+  CFGMM_CUDA(cfgmm::narrow_f64(d_rho, rhos, ex.rhos, s));
+  return CFGMM_OK;
 }
 
 }  // namespace
@@ -790,6 +866,128 @@ int cfgmm_aodm_fock_dev(double* vs, const double* ws, const double* ao_lhs, cons
   if (rc != CFGMM_OK) return rc;
   if (e2 != cudaSuccess) return cuda_fail(e2, "cudaFreeAsync");
   return CFGMM_OK;
+}
+
+int cfgmm_matmul_f32(float* c, size_t c_len, const float* a, size_t a_len, const float* b,
+                     size_t b_len, size_t m, size_t n, size_t k, size_t lda, size_t ldb,
+                     size_t ldc, uint8_t transa, uint8_t transb, int precision) {
+  g_last_error.clear();
+  GemmExtents ex;
+  int rc = check_gemm(c, c_len, a, a_len, b, b_len, m, n, k, lda, ldb, ldc, transa != 0,
+                      transb != 0, &ex);
+  if (rc != CFGMM_OK) return rc;
+  if ((rc = check_precision(precision)) != CFGMM_OK) return rc;
+  if (ex.c == 0) return CFGMM_OK;
+  if (precision == CFGMM_PREC_OZAKI_INT8 && (rc = check_split_gemm(k)) != CFGMM_OK) return rc;
+  int dev;
+  if ((rc = current_device(&dev)) != CFGMM_OK) return rc;
+  DeviceState* st = device_state(dev);
+  std::lock_guard<std::mutex> lk(st->mu);
+  cudaStream_t s = st->stream;
+  {
+    StreamScratch sc(s);
+    float *da = nullptr, *db = nullptr, *dc = nullptr;
+    CFGMM_CUDA(sc.get(reinterpret_cast<void**>(&da), ex.a * 4));
+    CFGMM_CUDA(sc.get(reinterpret_cast<void**>(&db), ex.b * 4));
+    CFGMM_CUDA(sc.get(reinterpret_cast<void**>(&dc), ex.c * 4));
+    CFGMM_CUDA(cudaMemcpyAsync(da, a, ex.a * 4, cudaMemcpyHostToDevice, s));
+    CFGMM_CUDA(cudaMemcpyAsync(db, b, ex.b * 4, cudaMemcpyHostToDevice, s));
+    CFGMM_CUDA(cudaMemcpyAsync(dc, c, ex.c * 4, cudaMemcpyHostToDevice, s));
+    if (precision == CFGMM_PREC_OZAKI_INT8) CFGMM_CUDA(cfgmm::gemm_i8_reset_error(s));
+    if ((rc = matmul_f32_run(dc, da, db, m, n, k, lda, ldb, ldc, transa != 0, transb != 0, ex,
+                             precision, s)) != CFGMM_OK)
+      return rc;
+    CFGMM_CUDA(cudaMemcpyAsync(c, dc, ex.c * 4, cudaMemcpyDeviceToHost, s));
+  }
+  CFGMM_CUDA(cudaStreamSynchronize(s));
+  return check_device_waits();
+}
+
+int cfgmm_matmul_f32_dev(float* c, const float* a, const float* b, size_t m, size_t n, size_t k,
+                         size_t lda, size_t ldb, size_t ldc, uint8_t transa, uint8_t transb,
+                         int precision, void* stream) {
+  g_last_error.clear();
+  GemmExtents ex;
+  int rc = check_gemm(c, SIZE_MAX, a, SIZE_MAX, b, SIZE_MAX, m, n, k, lda, ldb, ldc, transa != 0,
+                      transb != 0, &ex);
+  if (rc != CFGMM_OK) return rc;
+  if ((rc = check_precision(precision)) != CFGMM_OK) return rc;
+  if (ex.c == 0) return CFGMM_OK;
+  if (precision == CFGMM_PREC_OZAKI_INT8 && (rc = check_split_gemm(k)) != CFGMM_OK) return rc;
+  int dev;
+  if ((rc = current_device(&dev)) != CFGMM_OK) return rc;
+  return matmul_f32_run(c, a, b, m, n, k, lda, ldb, ldc, transa != 0, transb != 0, ex, precision,
+                        static_cast<cudaStream_t>(stream));
+}
+
+int cfgmm_aodmao2rho_f32(float* rhos, size_t rhos_len, const float* dms, size_t dms_len,
+                         const float* ao_lhs, size_t ao_lhs_len, const float* ao_rhs,
+                         size_t ao_rhs_len, size_t stride_ao, size_t stride_grid, size_t nao,
+                         size_t ngrid, size_t nset, const uint8_t* tab, size_t tab_len,
+                         size_t ldtab, size_t blksize, int precision) {
+  g_last_error.clear();
+  AodmExtents ex;
+  int rc = check_aodm(rhos, rhos_len, dms, dms_len, ao_lhs, ao_lhs_len, ao_rhs, ao_rhs_len,
+                      stride_ao, stride_grid, nao, ngrid, nset, tab, tab_len, ldtab, blksize, &ex);
+  if (rc != CFGMM_OK) return rc;
+  if ((rc = check_precision(precision)) != CFGMM_OK) return rc;
+  const bool split = precision == CFGMM_PREC_OZAKI_INT8;
+  if (split && nao > 16384)
+    return fail(CFGMM_ERR_UNIMPLEMENTED, "split-precision AO-DM-AO supports nao <= 16384");
+  if (ex.rhos == 0) return CFGMM_OK;
+  int dev;
+  if ((rc = current_device(&dev)) != CFGMM_OK) return rc;
+  DeviceState* st = device_state(dev);
+  std::lock_guard<std::mutex> lk(st->mu);
+  cudaStream_t s = st->stream;
+  const bool same_ao = ao_lhs == ao_rhs;
+  {
+    StreamScratch sc(s);
+    float *d_rho = nullptr, *d_dms = nullptr, *d_lhs = nullptr, *d_rhs = nullptr;
+    uint8_t* d_tab = nullptr;
+    CFGMM_CUDA(sc.get(reinterpret_cast<void**>(&d_rho), ex.rhos * 4));
+    CFGMM_CUDA(sc.get(reinterpret_cast<void**>(&d_dms), ex.dms * 4));
+    CFGMM_CUDA(sc.get(reinterpret_cast<void**>(&d_lhs), ex.ao * 4));
+    if (!same_ao) CFGMM_CUDA(sc.get(reinterpret_cast<void**>(&d_rhs), ex.ao * 4));
+    CFGMM_CUDA(sc.get(reinterpret_cast<void**>(&d_tab), ex.tab));
+    CFGMM_CUDA(cudaMemcpyAsync(d_rho, rhos, ex.rhos * 4, cudaMemcpyHostToDevice, s));
+    CFGMM_CUDA(cudaMemcpyAsync(d_dms, dms, ex.dms * 4, cudaMemcpyHostToDevice, s));
+    CFGMM_CUDA(cudaMemcpyAsync(d_lhs, ao_lhs, ex.ao * 4, cudaMemcpyHostToDevice, s));
+    if (!same_ao)
+      CFGMM_CUDA(cudaMemcpyAsync(d_rhs, ao_rhs, ex.ao * 4, cudaMemcpyHostToDevice, s));
+    CFGMM_CUDA(cudaMemcpyAsync(d_tab, tab, ex.tab, cudaMemcpyHostToDevice, s));
+    if (split) CFGMM_CUDA(cfgmm::aodmao2rho_split_reset_error(s));
+    if ((rc = aodm_f32_run(d_rho, d_dms, d_lhs, same_ao ? d_lhs : d_rhs, stride_ao, stride_grid,
+                           nao, ngrid, nset, d_tab, ldtab, blksize, ex, precision, s)) !=
+        CFGMM_OK)
+      return rc;
+    CFGMM_CUDA(cudaMemcpyAsync(rhos, d_rho, ex.rhos * 4, cudaMemcpyDeviceToHost, s));
+  }
+  CFGMM_CUDA(cudaStreamSynchronize(s));
+  if (split) return check_device_waits();
+  int code = 0;
+  CFGMM_CUDA(cfgmm::aodm_read_error(&code));
+  if (code != 0) return fail(CFGMM_ERR_TIMEOUT, "a pipeline wait of the FP64 kernel timed out");
+  return CFGMM_OK;
+}
+
+int cfgmm_aodmao2rho_f32_dev(float* rhos, const float* dms, const float* ao_lhs,
+                             const float* ao_rhs, size_t stride_ao, size_t stride_grid,
+                             size_t nao, size_t ngrid, size_t nset, const uint8_t* tab,
+                             size_t ldtab, size_t blksize, int precision, void* stream) {
+  g_last_error.clear();
+  AodmExtents ex;
+  int rc = check_aodm(rhos, SIZE_MAX, dms, SIZE_MAX, ao_lhs, SIZE_MAX, ao_rhs, SIZE_MAX,
+                      stride_ao, stride_grid, nao, ngrid, nset, tab, SIZE_MAX, ldtab, blksize, &ex);
+  if (rc != CFGMM_OK) return rc;
+  if ((rc = check_precision(precision)) != CFGMM_OK) return rc;
+  if (precision == CFGMM_PREC_OZAKI_INT8 && nao > 16384)
+    return fail(CFGMM_ERR_UNIMPLEMENTED, "split-precision AO-DM-AO supports nao <= 16384");
+  if (ex.rhos == 0) return CFGMM_OK;
+  int dev;
+  if ((rc = current_device(&dev)) != CFGMM_OK) return rc;
+  return aodm_f32_run(rhos, dms, ao_lhs, ao_rhs, stride_ao, stride_grid, nao, ngrid, nset, tab,
+                      ldtab, blksize, ex, precision, static_cast<cudaStream_t>(stream));
 }
 
 int cfgmm_release_workspace(void) {

@@ -517,6 +517,8 @@ int ozaki_default_moduli(int k) {
   return ozaki_plan(k, 0, kOzakiMinBits).nmod;
 }
 
+int ozaki_moduli_for_bits(int k, int bits) { return ozaki_plan(k, 0, bits).nmod; }
+
 size_t ozaki_dgemm_workspace(int m, int n, int k, int nmod) {
   return dgemm_layout(m, n, k, nmod).total;
 }

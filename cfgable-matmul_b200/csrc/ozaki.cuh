@@ -36,6 +36,8 @@ OzakiPlan ozaki_plan(int k, int nmod, int min_bits);
 // Moduli used for contraction length k (environment CFGMM_OZAKI_MODULI
 // overrides, 2..16).
 int ozaki_default_moduli(int k);
+// Moduli that give operands of at least `bits` bits at this k (26 for f32 data).
+int ozaki_moduli_for_bits(int k, int bits);
 
 size_t ozaki_dgemm_workspace(int m, int n, int k, int nmod);
 

@@ -239,6 +239,31 @@ int cfgmm_aodm_fock_dev(double* vs, const double* ws, const double* ao_lhs, cons
                         size_t nset, const uint8_t* tab, size_t ldtab, size_t blksize,
                         void* stream);
 
+/* ---- f32 forms of the two paths (MatmulLoops<f32, ...>) -------------------
+ * The reference's MatmulLoops is generic over T (src/structs.rs:3-13) but
+ * implements f64 only (src/structs.rs:19-20); these are its f32 instantiations
+ * with the arguments, layouts, mask and accumulate-into semantics of the f64
+ * calls above (cfgmm_matmul_ex, cfgmm_aodmao2rho_ex and their _dev forms).
+ * Operands are widened exactly to f64 on the device, the f64 kernels run
+ * (CFGMM_PREC_FP64 on DMMA; CFGMM_PREC_OZAKI_INT8 with the moduli that 26-bit
+ * operands need, fewer than for f64 data) and each output element is rounded
+ * back to f32 once. */
+int cfgmm_matmul_f32(float* c, size_t c_len, const float* a, size_t a_len, const float* b,
+                     size_t b_len, size_t m, size_t n, size_t k, size_t lda, size_t ldb,
+                     size_t ldc, uint8_t transa, uint8_t transb, int precision);
+int cfgmm_matmul_f32_dev(float* c, const float* a, const float* b, size_t m, size_t n, size_t k,
+                         size_t lda, size_t ldb, size_t ldc, uint8_t transa, uint8_t transb,
+                         int precision, void* stream);
+int cfgmm_aodmao2rho_f32(float* rhos, size_t rhos_len, const float* dms, size_t dms_len,
+                         const float* ao_lhs, size_t ao_lhs_len, const float* ao_rhs,
+                         size_t ao_rhs_len, size_t stride_ao, size_t stride_grid, size_t nao,
+                         size_t ngrid, size_t nset, const uint8_t* tab, size_t tab_len,
+                         size_t ldtab, size_t blksize, int precision);
+int cfgmm_aodmao2rho_f32_dev(float* rhos, const float* dms, const float* ao_lhs,
+                             const float* ao_rhs, size_t stride_ao, size_t stride_grid,
+                             size_t nao, size_t ngrid, size_t nset, const uint8_t* tab,
+                             size_t ldtab, size_t blksize, int precision, void* stream);
+
 /* ---- batched plans: many grid batches of one molecule in one launch ------
  * No counterpart in the reference (whose callers batch grids themselves,
  * impl_matmul.rs:354-355): a plan holds device pointers to every batch's phi

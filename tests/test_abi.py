@@ -144,6 +144,30 @@ def test_fock_validation(cm):
     assert np.all(v == 1)
 
 
+def test_f32_validation(cm):
+    """The f32 forms take the f64 calls' checks (lengths in elements)."""
+    a = np.ones((4, 6), np.float32)
+    b = np.ones((6, 5), np.float32)
+    c = np.zeros((4, 5), np.float32)
+    with pytest.raises(ValueError, match="slice too short"):
+        cm.matmul_f32(c, a[:2], b, 4, 5, 6, 6, 5, 5, False, False)
+    with pytest.raises(ValueError, match="precision"):
+        cm.matmul_f32(c, a, b, 4, 5, 6, 6, 5, 5, False, False, precision=9)
+    with pytest.raises(TypeError, match="float32"):
+        cm.matmul_f32(c.astype(np.float64), a, b, 4, 5, 6, 6, 5, 5, False, False)
+    cm.matmul_f32(c, a, b, 0, 5, 6, 6, 5, 5, False, False)  # empty: no device needed
+    rho = np.zeros((2, 100), np.float32)
+    dms = np.ones((2, 10, 10), np.float32)
+    ao = np.ones((10, 100), np.float32)
+    tab = np.ones((10, 3), np.uint8)
+    with pytest.raises(ValueError, match="slice too short"):
+        cm.aodmao2rho_f32(rho, dms[:1], ao, ao, (10, 100), (10, 100), 2, tab, 3)
+    with pytest.raises(ValueError, match="BLKSIZE"):
+        cm.aodmao2rho_f32(rho, dms, ao, ao, (10, 100), (10, 100), 2, tab, 3, blksize=0)
+    cm.aodmao2rho_f32(rho, dms, ao, ao, (10, 100), (10, 100), 0, tab, 3)
+    assert np.all(c == 0) and np.all(rho == 0)
+
+
 def test_bool_mask_is_accepted(cm):
     rho, dms, ao, tab, nblk = _aodm_args()
     with pytest.raises(ValueError, match="slice too short"):
