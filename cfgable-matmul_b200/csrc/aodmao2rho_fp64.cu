@@ -364,8 +364,15 @@ constexpr int ROWS_PER_THREAD = TU / RSTEP;     // 16
 template <int NS>
 constexpr int stage_bytes() { return NS * D_BYTES + PHI_BYTES; }
 
+// consumer warp grid: CWM warps along the item's rows x CWN along its points;
+// each warp holds MT x NT m16n8 tiles per density matrix.  Four row warps of
+// 16 rows share their phi (B) fragments over 32 points: per k step of 8 a warp
+// loads 2 A fragment pairs per matrix and 4 B fragment pairs.
+constexpr int CWM = 4, CWN = 2;
+constexpr int MT = TU / CWM / 16, NT = TG / CWN / 8;
+
 template <int NS>
-constexpr int red_doubles() { return 2 * NS * 2 * TG; }  // double-buffered [2][NS][2][TG]
+constexpr int red_doubles() { return 2 * NS * CWM * TG; }  // double-buffered [2][NS][CWM][TG]
 
 template <int NS>
 constexpr size_t smem_bytes() {
@@ -583,7 +590,7 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
     // ------------------------------- consumers -------------------------------
     const int ct = tid - NPROD;
     const int warp = ct >> 5;
-    const int wm = warp >> 2, wn = warp & 3;  // warp tile: rows wm*32.., points wn*16..
+    const int wm = warp / CWN, wn = warp % CWN;  // warp tile: rows wm*16*MT.., points wn*8*NT..
     const int g = lane >> 2, q = lane & 3;
     uint32_t use = 0;
     for (int n = 0;; ++n) {
@@ -596,30 +603,31 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
       if (it >= total) break;
       const Item t = decode<NS>(p, p.items[it], set0);
 
-      // the phi_lhs rows of this thread's epilogue (rows wm*32 + mt*16 + g + 8h,
-      // points wn*16 + nt*8 + 2q + e) are brought into L2 now, so that the
+      // the phi_lhs rows of this thread's epilogue (rows wm*16*MT + mt*16 + g + 8h,
+      // points wn*8*NT + nt*8 + 2q + e) are brought into L2 now, so that the
       // epilogue's loads hit while the tensor pipe waits for them
-      int urow[2][2];
+      int urow[MT][2];
 #pragma unroll
-      for (int mt = 0; mt < 2; ++mt)
+      for (int mt = 0; mt < MT; ++mt)
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          const int r = wm * 32 + mt * 16 + g + 8 * h;
+          const int r = wm * 16 * MT + mt * 16 + g + 8 * h;
           urow[mt][h] = r < t.mu ? t.I[t.u0 + r] : -1;
           if (urow[mt][h] >= 0)
 #pragma unroll
-            for (int nt = 0; nt < 2; ++nt)
+            for (int nt = 0; nt < NT; nt += 2)
               asm volatile("prefetch.global.L2 [%0];" ::"l"(
-                  t.B->ao_lhs + size_t(urow[mt][h]) * t.B->stride_grid + t.g0 + wn * 16 + nt * 8));
+                  t.B->ao_lhs + size_t(urow[mt][h]) * t.B->stride_grid + t.g0 + wn * 8 * NT +
+                  nt * 8));
         }
 
-      double acc[NS][2][2][4];
+      double acc[NS][MT][NT][4];
 #pragma unroll
       for (int s = 0; s < NS; ++s)
 #pragma unroll
-        for (int i = 0; i < 2; ++i)
+        for (int i = 0; i < MT; ++i)
 #pragma unroll
-          for (int j = 0; j < 2; ++j)
+          for (int j = 0; j < NT; ++j)
 #pragma unroll
             for (int e = 0; e < 4; ++e) acc[s][i][j][e] = 0.0;
 
@@ -638,10 +646,10 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
         const bool diag = sym && kc < kc0 + TU / TK;
 #pragma unroll
         for (int kk = 0; kk < TK; kk += 8) {
-          double b0[2], b1[2];
+          double b0[NT], b1[NT];
 #pragma unroll
-          for (int nt = 0; nt < 2; ++nt) {
-            const int col = wn * 16 + nt * 8 + g;
+          for (int nt = 0; nt < NT; ++nt) {
+            const int col = wn * 8 * NT + nt * 8 + g;
             b0[nt] = phi[(kk + q) * TG + col];
             b1[nt] = phi[(kk + q + 4) * TG + col];
           }
@@ -650,8 +658,8 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
           for (int s = 0; s < NS; ++s) {
             const double* Ds = reinterpret_cast<const double*>(st + s * D_BYTES);
 #pragma unroll
-            for (int mt = 0; mt < 2; ++mt) {
-              const int r = wm * 32 + mt * 16 + g;
+            for (int mt = 0; mt < MT; ++mt) {
+              const int r = wm * 16 * MT + mt * 16 + g;
               double2 lo =
                   *reinterpret_cast<const double2*>(Ds + r * TK + ((slot8 ^ swz_key(r)) << 1));
               double2 hi = *reinterpret_cast<const double2*>(
@@ -664,7 +672,7 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
                 hi.y *= sym_factor(r + 8, c + 4);
               }
 #pragma unroll
-              for (int nt = 0; nt < 2; ++nt)
+              for (int nt = 0; nt < NT; ++nt)
                 dmma_16x8x8(acc[s][mt][nt], lo.x, hi.x, lo.y, hi.y, b0[nt], b1[nt]);
             }
           }
@@ -675,39 +683,39 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
       if (!ok) break;
 
       // rho_part[s][j] = sum_r phi_lhs[I[u0+r]][g0+j] * X[s][r][j]: rows reduced
-      // in registers and shuffles, the two row halves (wm) through `red`
-      double lhs[2][2][2][2];  // [mt][h][nt][e]
+      // in registers and shuffles, the CWM row groups (wm) through `red`
+      double lhs[MT][2][NT][2];  // [mt][h][nt][e]
 #pragma unroll
-      for (int mt = 0; mt < 2; ++mt)
+      for (int mt = 0; mt < MT; ++mt)
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const double* row =
               urow[mt][h] >= 0 ? t.B->ao_lhs + size_t(urow[mt][h]) * t.B->stride_grid : nullptr;
 #pragma unroll
-          for (int nt = 0; nt < 2; ++nt)
+          for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
-              const int j = wn * 16 + nt * 8 + 2 * q + e;
+              const int j = wn * 8 * NT + nt * 8 + 2 * q + e;
               lhs[mt][h][nt][e] = (row && j < t.gw) ? row[t.g0 + j] : 0.0;
             }
         }
-      double* rb = red + (n & 1) * (NS * 2 * TG);
+      double* rb = red + (n & 1) * (NS * CWM * TG);
 #pragma unroll
       for (int s = 0; s < NS; ++s)
 #pragma unroll
-        for (int nt = 0; nt < 2; ++nt)
+        for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
           for (int e = 0; e < 2; ++e) {
             double v = 0.0;
 #pragma unroll
-            for (int mt = 0; mt < 2; ++mt)
+            for (int mt = 0; mt < MT; ++mt)
 #pragma unroll
               for (int h = 0; h < 2; ++h)
                 v = fma(acc[s][mt][nt][2 * h + e], lhs[mt][h][nt][e], v);
             v += __shfl_xor_sync(0xffffffffu, v, 4);
             v += __shfl_xor_sync(0xffffffffu, v, 8);
             v += __shfl_xor_sync(0xffffffffu, v, 16);
-            if (g == 0) rb[(s * 2 + wm) * TG + wn * 16 + nt * 8 + 2 * q + e] = v;
+            if (g == 0) rb[(s * CWM + wm) * TG + wn * 8 * NT + nt * 8 + 2 * q + e] = v;
           }
       tc::mbar_arrive(&epi[n & 1]);
       // The buffer is written again two items later, after every consumer has
@@ -716,7 +724,9 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
       const size_t pslot = t.B->partial_off + size_t(t.bg) * p.max_utiles + t.utile;
       for (int i = ct; i < t.ns * TG; i += NCONS) {
         const int s = i / TG, j = i % TG;
-        const double v = rb[(s * 2 + 0) * TG + j] + rb[(s * 2 + 1) * TG + j];
+        double v = 0.0;
+#pragma unroll
+        for (int w = 0; w < CWM; ++w) v += rb[(s * CWM + w) * TG + j];
         p.partial[(pslot * p.nset_max + set0 + s) * TG + j] = sym ? 2.0 * v : v;
       }
     }
