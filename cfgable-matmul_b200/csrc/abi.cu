@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <climits>
+#include <cstdlib>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -22,6 +23,7 @@
 #include "ao_eval.cuh"
 #include "dgemm_fp64.cuh"
 #include "f32.cuh"
+#include "fock.cuh"
 #include "gemm_i8.cuh"
 #include "ozaki.cuh"
 
@@ -406,9 +408,30 @@ int check_fock(double* vs, size_t vs_len, const double* ws, size_t ws_len, const
   return rc;
 }
 
+// The compacted form (fock.cu) unless CFGMM_FOCK_DENSE=1 selects the dense
+// product with K-step skipping (dgemm_fp64.cu).
+bool fock_dense() {
+  static const bool on = [] {
+    const char* e = std::getenv("CFGMM_FOCK_DENSE");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
+size_t fock_workspace(size_t nao, size_t ngrid, size_t nset, size_t blksize) {
+  return fock_dense() ? cfgmm::fock_fp64_workspace(int(nao), int(ngrid))
+                      : cfgmm::fock_compact_workspace(nao, ngrid, nset, blksize);
+}
+
 int fock_run(double* d_v, const double* d_w, const double* d_lhs, const double* d_rhs,
              size_t stride_ao, size_t stride_grid, size_t nao, size_t ngrid, size_t nset,
              const uint8_t* d_tab, size_t ldtab, size_t blksize, void* ws, cudaStream_t s) {
+  if (!fock_dense()) {
+    CFGMM_CUDA(cfgmm::fock_compact_fp64(d_v, d_w, d_lhs, d_rhs, stride_ao, stride_grid,
+                                        int(nao), int(ngrid), int(nset), d_tab, ldtab,
+                                        int(blksize), ws, s));
+    return CFGMM_OK;
+  }
   CFGMM_CUDA(cfgmm::dgemm_reset_error(s));
   for (size_t set = 0; set < nset; ++set)
     CFGMM_CUDA(cfgmm::fock_fp64(d_v + set * stride_ao * stride_ao, stride_ao,
@@ -438,8 +461,7 @@ int fock_host(double* vs, size_t vs_len, const double* ws, size_t ws_len, const 
   const size_t o_tab = o_rhs + (same_ao ? 0 : align256(ex.ao * 8));
   const size_t o_v = o_tab + align256(ex.tab);
   const size_t o_ws = o_v + align256(ex.dms * 8);
-  if ((rc = reserve(st, o_ws + cfgmm::fock_fp64_workspace(int(nao), int(ngrid)))) != CFGMM_OK)
-    return rc;
+  if ((rc = reserve(st, o_ws + fock_workspace(nao, ngrid, nset, blksize))) != CFGMM_OK) return rc;
   char* base = static_cast<char*>(st->buf);
   double* d_w = reinterpret_cast<double*>(base + o_w);
   double* d_lhs = reinterpret_cast<double*>(base + o_lhs);
@@ -859,7 +881,7 @@ int cfgmm_aodm_fock_dev(double* vs, const double* ws, const double* ao_lhs, cons
   if ((rc = current_device(&dev)) != CFGMM_OK) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   void* work = nullptr;
-  CFGMM_CUDA(cudaMallocAsync(&work, cfgmm::fock_fp64_workspace(int(nao), int(ngrid)), s));
+  CFGMM_CUDA(cudaMallocAsync(&work, fock_workspace(nao, ngrid, nset, blksize), s));
   rc = fock_run(vs, ws, ao_lhs, ao_rhs, stride_ao, stride_grid, nao, ngrid, nset, tab, ldtab,
                 blksize, work, s);
   const cudaError_t e2 = cudaFreeAsync(work, s);

@@ -957,6 +957,12 @@ Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk) {
 }
 }  // namespace
 
+cudaError_t aodm_build_items_launch(const int* counts, int nblk, int gsub, int4* items,
+                                    int* counters, int ncounters, cudaStream_t stream) {
+  aodm_build_items<<<1, 1024, 0, stream>>>(counts, nblk, gsub, items, counters, ncounters);
+  return cudaGetLastError();
+}
+
 cudaError_t aodm_block_lists_launch(const uint8_t* tab, size_t ldtab, int nao, int nblk,
                                     int* lists, int* counts, cudaStream_t stream) {
   aodm_block_lists<<<nblk, 256, 0, stream>>>(tab, ldtab, nao, nblk, lists, counts);

@@ -69,6 +69,12 @@ cudaError_t aodmao2rho_fp64(double* rhos, const double* dms, const double* ao_lh
 cudaError_t aodm_block_lists_launch(const uint8_t* tab, size_t ldtab, int nao, int nblk,
                                     int* lists, int* counts, cudaStream_t stream);
 
+// Work list of one grid batch: items[i] = (0, block tile, row tile of 64 active
+// AOs, 0) in block order; counters[0..ncounters) = 0, counters[ncounters] = the
+// item count, counters[ncounters + 1] = 0.
+cudaError_t aodm_build_items_launch(const int* counts, int nblk, int gsub, int4* items,
+                                    int* counters, int ncounters, cudaStream_t stream);
+
 // Pieces of a batched run: counter reset, the persistent kernel, and the
 // reduction over (batch, block tile) pairs (rpairs null: batch 0, bg = index).
 cudaError_t aodm_launch_reset(int* counters, int ngroups, cudaStream_t stream);

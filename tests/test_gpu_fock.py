@@ -96,3 +96,27 @@ def test_fock_is_the_adjoint_of_aodmao2rho(cm, wl):
     scale = float(np.sum(np.abs(v) * np.abs(p.dms)))
     assert abs(float(np.sum(v * p.dms)) - float(np.sum(w * rho))) <= 1e-13 * scale
     assert np.allclose(v[0], v[0].T, rtol=0, atol=1e-12 * np.abs(v).max())  # phi_lhs == phi_rhs
+
+
+def test_fock_compacted_and_dense_forms_agree(cm, oracle):
+    """The compacted form (per-block active lists, V scattered by FP64 atomics)
+    and the dense product with K-step skipping (CFGMM_FOCK_DENSE=1) on the same
+    inputs, both within 1e-13 of the oracle."""
+    import os, subprocess, sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    tmp = os.environ.get("TMPDIR", "/tmp")
+    code = ("import importlib,sys,numpy as np; sys.path.insert(0,'.'); sys.path.insert(0,'tests');"
+            "cm=importlib.import_module('cfgable-matmul_b200');"
+            "from test_gpu_fock import _case;"
+            "lhs,rhs,ws,tab,vs,st,sh=_case(77,700,3000,2,64,pad_ao=2,pad_grid=1);"
+            "cm.aodm_fock(vs,ws,lhs,rhs,st,sh,2,tab,tab.shape[1],64); np.save(sys.argv[1], vs)")
+    outs = []
+    for dense in ("0", "1"):
+        path = os.path.join(tmp, f"cfgmm_fock_dense{dense}.npy")
+        subprocess.run([sys.executable, "-c", code, path], cwd=root, check=True,
+                       env=dict(os.environ, CFGMM_FOCK_DENSE=dense))
+        outs.append(np.load(path))
+    lhs, rhs, ws, tab, vs, strides, shape = _case(77, 700, 3000, 2, 64, pad_ao=2, pad_grid=1)
+    oracle.aodm_fock(vs, ws, lhs, rhs, strides, shape, 2, tab, tab.shape[1], 64)
+    for o in outs:
+        assert normwise(o, vs) < TOL
