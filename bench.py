@@ -78,6 +78,7 @@ class Ranks:
             import torch.distributed as dist
             dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
             self.dist = dist
+            self.device = "cuda" if backend == "nccl" else "cpu"
 
     def barrier(self):
         if self.dist:
@@ -87,7 +88,7 @@ class Ranks:
         if not self.dist:
             return x
         import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 
@@ -655,6 +656,30 @@ def run_profile_case(args):
             rc = lib.cfgmm_matmul_dev(c.data_ptr(), a.data_ptr(), b.data_ptr(), m, n, k, k, n, n,
                                       0, 0, prec, stream.cuda_stream)
             assert rc == 0, rc
+    elif args.profile == "fock":
+        # Fock build V_s += phi diag(w_s) phi^T over the masked pairs (one phi
+        # array for both sides), timed per call with CUDA events
+        p = wl.geometric(seed=0)
+        ao = torch.from_numpy(p.ao).cuda()
+        tab = torch.from_numpy(p.tab).cuda()
+        g = torch.Generator(device="cuda").manual_seed(0)
+        w = torch.rand(p.nset, p.ngrid, dtype=torch.float64, device="cuda", generator=g)
+        v = torch.zeros(p.nset, p.nao, p.nao, dtype=torch.float64, device="cuda")
+        times = []
+        for _ in range(args.reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rc = lib.cfgmm_aodm_fock_dev(v.data_ptr(), w.data_ptr(), ao.data_ptr(), ao.data_ptr(),
+                                         p.nao, p.ngrid, p.nao, p.ngrid, p.nset, tab.data_ptr(),
+                                         p.nblk, p.blksize, stream.cuda_stream)
+            e1.record(stream)
+            assert rc == 0, rc
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        nb = p.tab.astype(bool).sum(axis=0).astype(np.float64)
+        pts = np.minimum(p.blksize, p.ngrid - p.blksize * np.arange(p.nblk)).astype(np.float64)
+        flops = 2.0 * p.nset * float(np.sum(nb * nb * pts))  # sum_s sum_b 2 |I_b|^2 |b|
+        print(json.dumps({"fock_ms": times, "flops": flops}), flush=True)
     else:
         p = wl.geometric(seed=0)
         ao = torch.from_numpy(p.ao).cuda()
@@ -679,7 +704,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
-    ap.add_argument("--profile", choices=["dgemm", "split", "aodm", "aodm_split"], default=None,
+    ap.add_argument("--profile", choices=["dgemm", "split", "aodm", "aodm_split", "fock"],
+                    default=None,
                     help="run one kernel on one case (ncu target) and exit")
     ap.add_argument("--m", type=int, default=4096)
     ap.add_argument("--n", type=int, default=4096)
