@@ -205,6 +205,19 @@ def cpu_dgemm_sample(target_s: float = 10.0) -> dict:
                       f"{dt:.2f} s"}
 
 
+def cpu_aodm_run(p) -> dict:
+    """Times the oracle's restatement of aodmao2rho_loop_parallel on the whole
+    taxol-size workload (one call, every host thread)."""
+    oracle = oracle_mod()
+    rho = np.zeros((p.nset, p.ngrid))
+    t0 = time.perf_counter()
+    oracle.aodmao2rho(rho, p.dms, p.ao, p.ao, (p.nao, p.ngrid), (p.nao, p.ngrid), p.nset, p.tab,
+                      p.nblk, p.blksize)
+    dt = time.perf_counter() - t0
+    return {"value": p.flops() / dt / 1e9, "unit": "GFLOP/s", "cores": oracle.max_threads(),
+            "kind": "port", "sample": f"the whole workload, one call, {dt:.2f} s"}
+
+
 # ---------------------------------------------------------------------------
 # the reference arm
 # ---------------------------------------------------------------------------
@@ -570,6 +583,8 @@ def run_ours(args, ranks: Ranks):
                                                            "28 INT8 products",
                       "launches_per_step": 8},
             "speedup_split_vs_fp64": atot / stot}
+    if ranks.rank == 0 and ranks.world == 1 and not args.no_cpu:
+        aodm["cpu_baseline"] = cpu_aodm_run(p)
     del ao, dms, tab, rho, r64, rsp
     torch.cuda.empty_cache()
     batched = batched_section(args, cm, wl, stream) if not args.no_batched else None

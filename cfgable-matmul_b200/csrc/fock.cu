@@ -12,8 +12,11 @@
 // m16n8k8 and adds it into V[I rows][I chunk] with FP64 atomics (red.add): the
 // same (u, v) receives one addition per block in which both are active.  Only
 // the masked products are formed (a dense product over all AO pairs runs ~10x
-// their number on the taxol-size mask).  Sums over blocks arrive in completion
-// order, so the last bits of V vary from run to run.
+// their number on the taxol-size mask).  When phi_lhs and phi_rhs are the same
+// array the block's contribution is symmetric in (u, v): row tile a then walks
+// the chunks from its own (chunk a) on and adds each product of a later chunk
+// to V[u][v] and V[v][u], half the products.  Sums over blocks arrive in
+// completion order, so the last bits of V vary from run to run.
 #include "common.cuh"
 #include "aodmao2rho_fp64.cuh"
 #include "fock.cuh"
@@ -44,6 +47,7 @@ struct FockArgs {
   const int* lists;  // [nblk][nao]
   const int* counts;
   int nao, ngrid, blk, gsub;
+  int sym;  // ao_lhs == ao_rhs: chunks from the row tile's own on, mirrored
   const int4* items;
   int* counters;  // [nset] work counters, [nset] = item total
 };
@@ -99,11 +103,12 @@ fock_compact_kernel(const __grid_constant__ FockArgs p) {
       cp_async_commit();
     };
     const int nch = (nb + FT - 1) / FT;
-    issue(0);
+    const int ch0 = p.sym ? a : 0;
+    issue(ch0);
     const int r_lo = wm * 16 + g, r_hi = r_lo + 8;
     const int u_lo = r_lo < mu ? I[u0 + r_lo] : -1;
     const int u_hi = r_hi < mu ? I[u0 + r_hi] : -1;
-    for (int ch = 0; ch < nch; ++ch) {
+    for (int ch = ch0; ch < nch; ++ch) {
       if (ch + 1 < nch) {
         issue(ch + 1);
         cp_async_wait<1>();
@@ -132,8 +137,9 @@ fock_compact_kernel(const __grid_constant__ FockArgs p) {
           dmma_16x8x8(acc[nt], lo.x, hi.x, lo.y, hi.y, bv.x, bv.y);
         }
       }
-      // V[u][v] += the chunk's products
+      // V[u][v] += the chunk's products (and V[v][u] past the diagonal tile)
       const int c0 = ch * FT;
+      const bool mirror = p.sym && ch != a;
 #pragma unroll
       for (int nt = 0; nt < 4; ++nt)
 #pragma unroll
@@ -143,6 +149,10 @@ fock_compact_kernel(const __grid_constant__ FockArgs p) {
           const size_t vcol = size_t(I[c]);
           if (u_lo >= 0) atomicAdd(V + size_t(u_lo) * p.stride_ao + vcol, acc[nt][e]);
           if (u_hi >= 0) atomicAdd(V + size_t(u_hi) * p.stride_ao + vcol, acc[nt][2 + e]);
+          if (mirror) {
+            if (u_lo >= 0) atomicAdd(V + vcol * p.stride_ao + u_lo, acc[nt][e]);
+            if (u_hi >= 0) atomicAdd(V + vcol * p.stride_ao + u_hi, acc[nt][2 + e]);
+          }
         }
       __syncthreads();  // chunk ch's buffer is refilled by chunk ch + 2
     }
@@ -207,6 +217,7 @@ cudaError_t fock_compact_fp64(double* vs, const double* ws, const double* ao_lhs
   a.ngrid = ngrid;
   a.blk = blk;
   a.gsub = gsub;
+  a.sym = ao_lhs == ao_rhs;
   a.items = items;
   a.counters = counters;
   const size_t dyn = 2 * TILE * sizeof(double);

@@ -4,6 +4,8 @@ has both u and v active.  Checked against the oracle's restatement of that
 formula on the same seeded inputs: ragged and partial blocks, BLKSIZE 16, 48,
 64 and 100, a single partial 128-AO tile, padded strides, phi_lhs != phi_rhs,
 masked entries holding nonzero phi, accumulation into a nonzero V, nset > 1,
+one array passed as both phi_lhs and phi_rhs (the compacted form then forms
+half the products and mirrors them),
 fully masked tables, device tensors; at a molecule-sized case through the
 size-independent identity sum(V(w) * D) == sum(w * rho(D)) with the GPU
 AO-DM-AO contraction.  FP64 results within 1e-13 normwise of the oracle."""
@@ -34,6 +36,7 @@ def _case(seed, nao, ngrid, nset, blk, pad_ao=0, pad_grid=0, density=0.4, same=F
     (513, 3001, 1, 100, 0, 3, False),    # BLKSIZE not a multiple of the 32-point K step
     (257, 2048, 3, 16, 1, 0, True),      # blocks smaller than a K step
     (40, 10, 1, 16, 0, 0, False),        # fewer points than a K step
+    (700, 3000, 2, 64, 2, 1, True),      # one array for both sides: mirrored products
 ])
 def test_fock_matches_oracle(cm, oracle, nao, ngrid, nset, blk, pad_ao, pad_grid, same):
     lhs, rhs, ws, tab, vs, strides, shape = _case(nao + ngrid, nao, ngrid, nset, blk, pad_ao,
