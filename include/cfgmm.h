@@ -225,10 +225,13 @@ int cfgmm_aodmao2rho_dev_noalloc(double* rhos, const double* dms, const double* 
  *   vs[s*stride_ao^2 + u*stride_ao + v] += sum over g with tab[u][g/BLK] and
  *       tab[v][g/BLK] of ao_lhs[u][g] * ws[s*stride_grid + g] * ao_rhs[v][g]
  * for s < nset, u, v < nao (stride_ao >= nao).  Outputs are accumulated into.
- * FP64 on the tensor cores: the masked, weighted operands are packed with K =
- * grid points and K steps in which a 128-AO tile has no active AO are skipped.
- * Slices too short, BLKSIZE 0 or overlapping V rows are rejected as in the
- * AO-DM-AO calls. */
+ * FP64 on the tensor cores over the per-block compacted AO lists: only the
+ * masked products are formed, and when ao_lhs and ao_rhs are the same array
+ * each symmetric pair of products is formed once and added to V[u][v] and
+ * V[v][u].  V is accumulated with FP64 atomics, so its last bits depend on the
+ * order in which blocks finish.  Setting CFGMM_FOCK_DENSE=1 in the environment
+ * selects the dense product over packed operands instead.  Slices too short,
+ * BLKSIZE 0 or overlapping V rows are rejected as in the AO-DM-AO calls. */
 int cfgmm_aodm_fock(double* vs, size_t vs_len, const double* ws, size_t ws_len,
                     const double* ao_lhs, size_t ao_lhs_len, const double* ao_rhs,
                     size_t ao_rhs_len, size_t stride_ao, size_t stride_grid, size_t nao,
