@@ -73,6 +73,10 @@ bool fits_int(size_t v) { return v <= size_t(INT_MAX) - 4096; }
 struct DeviceState {
   std::mutex mu;
   cudaStream_t stream = nullptr;
+  // second copy stream and its events: C's upload overlaps the split
+  // DGEMM's residues and INT8 GEMM (C is first read by the reconstruction)
+  cudaStream_t copy = nullptr;
+  cudaEvent_t ab_done = nullptr, c_ready = nullptr;
   void* buf = nullptr;
   size_t cap = 0;
 };
@@ -115,6 +119,14 @@ DeviceState* device_state(int dev) {
   if (g_devices.size() <= size_t(dev)) g_devices.resize(dev + 1);
   if (!g_devices[dev]) g_devices[dev].reset(new DeviceState);
   return g_devices[dev].get();
+}
+
+// Creates the copy stream and events of the overlapped C upload (caller holds st->mu).
+int ensure_copy_stream(DeviceState* st) {
+  if (!st->copy) CFGMM_CUDA(cudaStreamCreateWithFlags(&st->copy, cudaStreamNonBlocking));
+  if (!st->ab_done) CFGMM_CUDA(cudaEventCreateWithFlags(&st->ab_done, cudaEventDisableTiming));
+  if (!st->c_ready) CFGMM_CUDA(cudaEventCreateWithFlags(&st->c_ready, cudaEventDisableTiming));
+  return CFGMM_OK;
 }
 
 // Grows the device's staging buffer to at least `bytes` (caller holds st->mu).
@@ -260,17 +272,32 @@ int gemm_host(double* c, size_t c_len, const double* a, size_t a_len, const doub
   uint8_t* dt = masked ? reinterpret_cast<uint8_t*>(base + ot) : nullptr;
   CFGMM_CUDA(cudaMemcpyAsync(da, a, ex.a * 8, cudaMemcpyHostToDevice, st->stream));
   CFGMM_CUDA(cudaMemcpyAsync(db, b, ex.b * 8, cudaMemcpyHostToDevice, st->stream));
-  CFGMM_CUDA(cudaMemcpyAsync(dc, c, ex.c * 8, cudaMemcpyHostToDevice, st->stream));
   if (masked) CFGMM_CUDA(cudaMemcpyAsync(dt, mk.tab, tab_ext, cudaMemcpyHostToDevice, st->stream));
   if (split) {
-    CFGMM_CUDA(cfgmm::gemm_i8_reset_error(st->stream));
-    CFGMM_CUDA(cfgmm::ozaki_dgemm(dc, da, db, int(m), int(n), int(k), lda, ldb, ldc, transa != 0,
-                                  transb != 0, nmod, base + ows, st->stream, nullptr, dt,
-                                  mk.ldtab, int(mk.blk)));
+    // C goes up on the copy stream once A and B are in, while the residues
+    // and the INT8 GEMM run; the reconstruction waits for it
+    if ((rc = ensure_copy_stream(st)) != CFGMM_OK) return rc;
+    CFGMM_CUDA(cudaEventRecord(st->ab_done, st->stream));
+    CFGMM_CUDA(cudaStreamWaitEvent(st->copy, st->ab_done, 0));
+    CFGMM_CUDA(cudaMemcpyAsync(dc, c, ex.c * 8, cudaMemcpyHostToDevice, st->copy));
+    CFGMM_CUDA(cudaEventRecord(st->c_ready, st->copy));
+    cudaError_t err = cfgmm::gemm_i8_reset_error(st->stream);
+    if (err == cudaSuccess)
+      err = cfgmm::ozaki_dgemm(dc, da, db, int(m), int(n), int(k), lda, ldb, ldc, transa != 0,
+                               transb != 0, nmod, base + ows, st->stream, nullptr, dt, mk.ldtab,
+                               int(mk.blk), st->c_ready);
+    // C is complete before it goes back, whichever path ozaki_dgemm took
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(st->stream, st->c_ready, 0);
+    if (err != cudaSuccess) {
+      cudaStreamSynchronize(st->copy);  // the staging buffer is not reused under a live copy
+      return cuda_fail(err, "ozaki_dgemm");
+    }
   } else if (masked) {
+    CFGMM_CUDA(cudaMemcpyAsync(dc, c, ex.c * 8, cudaMemcpyHostToDevice, st->stream));
     CFGMM_CUDA(cfgmm::dgemm_fp64_non0tab(dc, da, db, int(m), int(n), int(k), lda, ldb, ldc,
                                          transa != 0, dt, mk.ldtab, int(mk.blk), st->stream));
   } else {
+    CFGMM_CUDA(cudaMemcpyAsync(dc, c, ex.c * 8, cudaMemcpyHostToDevice, st->stream));
     CFGMM_CUDA(cfgmm::dgemm_fp64(dc, da, db, int(m), int(n), int(k), lda, ldb, ldc, transa != 0,
                                  transb != 0, st->stream));
   }

@@ -526,7 +526,7 @@ size_t ozaki_dgemm_workspace(int m, int n, int k, int nmod) {
 cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int n, int k,
                         size_t lda, size_t ldb, size_t ldc, bool transa, bool transb, int nmod,
                         void* workspace, cudaStream_t stream, const cudaEvent_t* events,
-                        const uint8_t* tab, size_t ldtab, int blk) {
+                        const uint8_t* tab, size_t ldtab, int blk, cudaEvent_t c_ready) {
   if (tab && transb) return cudaErrorInvalidValue;  // the masked GEMM has no transb
   if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
   auto mark = [&](int i) { if (events) cudaEventRecord(events[i], stream); };
@@ -582,6 +582,7 @@ cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int 
   rc.two_T = plan.two_T;
   const long long rgrid = (long long)((n + 2047) / 2048) * m;
   if (rgrid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+  if (c_ready && (err = cudaStreamWaitEvent(stream, c_ready, 0)) != cudaSuccess) return err;
   reconstruct<<<unsigned(rgrid), 256, 0, stream>>>(c, ldc, m, n, r, L.ldr, ea, eb, rc);
   mark(3);
   return cudaGetLastError();

@@ -46,11 +46,13 @@ size_t ozaki_dgemm_workspace(int m, int n, int k, int nmod);
 // `events` (optional, 4 entries) are recorded before the residue preparation
 // and after the preparation, the INT8 GEMM and the reconstruction.  With `tab`
 // this is the masked GEMM (B not transposed): element (p, j) of B takes part
-// only when tab[p * ldtab + j / blk] != 0.
+// only when tab[p * ldtab + j / blk] != 0.  C is first read by the
+// reconstruction: when `c_ready` is given the stream waits for it just before,
+// so that C may still be arriving while the residues and the INT8 GEMM run.
 cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int n, int k,
                         size_t lda, size_t ldb, size_t ldc, bool transa, bool transb, int nmod,
                         void* workspace, cudaStream_t stream,
                         const cudaEvent_t* events = nullptr, const uint8_t* tab = nullptr,
-                        size_t ldtab = 0, int blk = 1);
+                        size_t ldtab = 0, int blk = 1, cudaEvent_t c_ready = nullptr);
 
 }  // namespace cfgmm
