@@ -320,7 +320,8 @@ int build_split(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, size_t n
       cudaEventCreate(&e1);
       double best_ms = 1e30;
       std::string trials;
-      for (int st : {2, 3, 4}) {
+      const int st0 = cfgmm::split_min_stages();
+      for (int st : {st0, st0 + 1, st0 + 2}) {
         float best = 1e30f;
         for (int rep = 0; rep < 3 && err == cudaSuccess; ++rep) {
           err = cudaEventRecord(e0, s);

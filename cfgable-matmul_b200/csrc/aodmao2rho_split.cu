@@ -35,14 +35,14 @@
 //                     the 7 digit tiles of a chunk into shared memory.
 //   split_build       work list (block tile, 128-row tile of I(b), DM) and
 //                     chunk offsets.
-//   split_main        persistent, 10 warps: warps 0-7 gather the D digits of
-//                     128 rows x 32 compacted columns in two groups of four
-//                     that take alternate chunks (a lane loads 8 bytes; lanes
+//   split_main        persistent, 14 warps: warps 0-11 gather the D digits of
+//                     128 rows x 32 compacted columns in three groups of four
+//                     that take turns by chunk (a lane loads 8 bytes; lanes
 //                     along a row read consecutive columns; two shuffle rounds
 //                     turn the 8-byte elements into digit planes, stored
 //                     without bank conflicts) and later run the epilogue;
-//                     warp 8 issues the 28 MMAs of a chunk (M=128, N=64, K=32)
-//                     into 7 TMEM level accumulators (448 columns); warp 9
+//                     warp 12 issues the 28 MMAs of a chunk (M=128, N=64, K=32)
+//                     into 7 TMEM level accumulators (448 columns); warp 13
 //                     bulk-loads the phi digit tiles.  The epilogue rebuilds X
 //                     in FP64, weights it with phi and reduces over the rows
 //                     of each warp; X never leaves the SM.
@@ -65,13 +65,25 @@ constexpr int TU = 128;   // compacted rows per item (TMEM lanes)
 constexpr int TG = 64;    // grid points per item
 constexpr int TK = 32;    // compacted columns per chunk (one INT8 MMA K step)
 constexpr int NSL = 7;    // digits per value
-constexpr int kDefaultStages = 3;  // pipeline depth (CFGMM_SPLIT_STAGES overrides: 2..5)
+constexpr int kDefaultStages = 3;  // pipeline depth (CFGMM_SPLIT_STAGES overrides: 3..5)
 constexpr uint32_t A_SLICE = TU * TK;        // 4096 B
 constexpr uint32_t B_SLICE = TG * TK;        // 2048 B
 constexpr uint32_t A_STAGE = NSL * A_SLICE;  // 28672 B
 constexpr uint32_t B_STAGE = NSL * B_SLICE;  // 14336 B
 constexpr uint32_t STAGE = A_STAGE + B_STAGE;
-constexpr int GATHER_WARPS = 8;               // two groups of four
+constexpr int NGROUPS = 3;                    // gather groups of four warps (128 rows each)
+constexpr int GATHER_WARPS = 4 * NGROUPS;
+// points of an item's epilogue per group: multiples of 8 (the TMEM load width)
+constexpr int EPI_SPAN = (TG / NGROUPS + 7) / 8 * 8;
+static_assert(EPI_SPAN <= 32 && NGROUPS * EPI_SPAN >= TG, "a lane holds one point scale");
+// A group's consecutive chunks of an item are NGROUPS apart in the stage
+// sequence, and its wait for a stage names the phase by parity only: with at
+// least NGROUPS stages the phase before the awaited one has completed by then
+// (the group's own previous wait saw a later MMA finish), so a parity wait
+// cannot pass a phase early.  Across items the epilogue's accumulator wait
+// orders every MMA of the previous item first.
+constexpr int kMinStages = NGROUPS;
+static_assert(kDefaultStages >= kMinStages, "default pipeline too shallow for the groups");
 constexpr int THREADS = 32 * (GATHER_WARPS + 2);
 constexpr int EPI_PARTS = 4;                  // partial sums per item (one per row quarter)
 constexpr int kBadExp = INT_MAX;  // scale of a row / point holding Inf or NaN
@@ -384,7 +396,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(SplitArgs p) {
 
   if (warp < GATHER_WARPS) {
     // ---------------- gather D digits, then the epilogue ----------------
-    // Group grp takes the chunks c = grp, grp+2, ... of every item; warp wq
+    // Group grp takes the chunks c = grp, grp+NGROUPS, ... of every item; warp wq
     // of the group fills tile rows 32wq .. 32wq+31, four rows per step.
     // Lane (qd, ri, hh) = lane bits (4:3, 2:1, 0) loads, for row 4*step+ri,
     // the columns 16hh + 4k + qd (k = 0..3) and ends up holding digit planes
@@ -423,23 +435,22 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(SplitArgs p) {
       const bool ev = erow < nb;
       const int eu = ev ? __ldg(I + erow) : 0;
       const int tu = p.tau[size_t(s) * p.nao + eu];
-      const int sg_lane = 32 * grp + lane < gw ? B.sigma[g0 + 32 * grp + lane] : 0;
+      // the group's epilogue points ep0 .. ep1-1; lane l holds the scale of point ep0 + l
+      const int ep0 = grp * EPI_SPAN, ep1 = min(TG, ep0 + EPI_SPAN);
+      const int sg_lane = ep0 + lane < min(ep1, gw) ? B.sigma[g0 + ep0 + lane] : 0;
       const double* lrow = B.ao_lhs + size_t(eu) * B.stride_grid + g0;
-      if (ev && 32 * grp < gw) {
-        const char* pf = reinterpret_cast<const char*>(lrow + 32 * grp);
-        const char* pe = reinterpret_cast<const char*>(lrow + min(gw, 32 * grp + 32));
+      if (ev && ep0 < gw) {
+        const char* pf = reinterpret_cast<const char*>(lrow + ep0);
+        const char* pe = reinterpret_cast<const char*>(lrow + min(gw, ep1));
         for (const char* q = pf; q < pe; q += 128)
           asm volatile("prefetch.global.L2 [%0];" ::"l"(q));
         asm volatile("prefetch.global.L2 [%0];" ::"l"(pe - 8));
       }
-      for (int c = kc0 + grp; c < kc; c += 2) {
+      for (int c = kc0 + grp; c < kc; c += NGROUPS) {
         const uint32_t seq = seq0 + uint32_t(c - kc0);
         const int stg = int(seq % STAGES);
         const uint32_t use = seq / STAGES;
-        if (use > 0 && !tc::mbar_wait(&empty[stg], (use - 1) & 1, err, 11)) {
-          ok = false;
-          break;
-        }
+        // the loads go out first; the stage has to be free only for the stores
         int iv[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -458,6 +469,10 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(SplitArgs p) {
                         lower_lim + 16 * hh + 4 * k + qd >= 32 * wq + 4 * st + ri)
                            ? __ldg(dset + size_t(iu[st]) * p.nao + iv[k])
                            : make_uint2(0u, 0u);
+        if (use > 0 && !tc::mbar_wait(&empty[stg], (use - 1) & 1, err, 11)) {
+          ok = false;
+          break;
+        }
         uint8_t* As = smem + stg * STAGE;
 #pragma unroll
         for (int st = 0; st < 8; ++st) {
@@ -487,7 +502,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(SplitArgs p) {
       }
       seq0 += uint32_t(kc - kc0);
       if (!ok) break;
-      // ---- epilogue: group grp reduces points 32grp .. 32grp+31 over the
+      // ---- epilogue: group grp reduces points ep0 .. ep1-1 over the
       // 32 rows of warp wq (TMEM lanes 32wq ..) ----
       if (!tc::mbar_wait(acc_full, nitem & 1, err, 12)) break;
       tc::fence_after_sync();
@@ -498,7 +513,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(SplitArgs p) {
       const size_t slot =
           size_t(B.partial_off) + ((size_t(bg) * p.max_ut + ut) * B.nset + s) * EPI_PARTS + wq;
 #pragma unroll 1
-      for (int cc = 32 * grp; cc < 32 * grp + 32; cc += 8) {
+      for (int cc = ep0; cc < ep1; cc += 8) {
         double a[8];  // phi_lhs of this row at 8 points, then its products
 #pragma unroll
         for (int j = 0; j < 8; j += 2) {
@@ -519,7 +534,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(SplitArgs p) {
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
           const int gl = cc + j;
-          const int sg = __shfl_sync(0xffffffffu, sg_lane, gl & 31);
+          const int sg = __shfl_sync(0xffffffffu, sg_lane, gl - ep0);
           if (ev && gl < gw) {
             // X = sum_L S_L 2^-8L: levels 0-2 and 3-6 combined exactly in 64-bit
             // integers (below 2^48 and 2^56), then one FMA
@@ -679,8 +694,8 @@ cudaError_t launch_main_t(int nsm, const SplitArgs& a, cudaStream_t stream, bool
 
 cudaError_t launch_main(int stages, int nsm, const SplitArgs& a, cudaStream_t stream,
                         bool attrs_only) {
-  switch (stages) {
-    case 2: return launch_main_t<2>(nsm, a, stream, attrs_only);
+  static_assert(kMinStages == 3, "instantiated depths: 3, 4, 5");
+  switch (stages < kMinStages ? kMinStages : stages) {
     case 3: return launch_main_t<3>(nsm, a, stream, attrs_only);
     case 5: return launch_main_t<5>(nsm, a, stream, attrs_only);
     default: return launch_main_t<4>(nsm, a, stream, attrs_only);
@@ -691,7 +706,7 @@ int split_stages() {
   static const int v = [] {
     const char* e = std::getenv("CFGMM_SPLIT_STAGES");
     const int s = e ? std::atoi(e) : kDefaultStages;
-    return (s >= 2 && s <= 5) ? s : kDefaultStages;
+    return (s >= kMinStages && s <= 5) ? s : kDefaultStages;
   }();
   return v;
 }
@@ -824,6 +839,7 @@ cudaError_t split_launch_reduce(const SplitArgs& a, const int2* pairs, int npair
   return cudaGetLastError();
 }
 
+int split_min_stages() { return kMinStages; }
 int split_row_tile() { return TU; }
 int split_point_tile() { return TG; }
 int split_chunk() { return TK; }

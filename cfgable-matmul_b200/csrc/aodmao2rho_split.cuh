@@ -61,12 +61,14 @@ cudaError_t split_prepare_phi(const double* ao_rhs, size_t stride_grid, const in
                               const int* counts, const int* cbase, int nao, int ngrid, int blk,
                               unsigned long long* pmax, int* sigma, uint8_t* phisl,
                               cudaStream_t stream);
-// stages: pipeline depth 2..5, 0 = default (CFGMM_SPLIT_STAGES or 3);
+// stages: pipeline depth split_min_stages()..5 (shallower requests run at the
+// minimum), 0 = default (CFGMM_SPLIT_STAGES or 3);
 // attrs_only: set the kernel's attributes (before a stream capture), no launch
 cudaError_t split_launch_main(const SplitArgs& a, cudaStream_t stream, int stages = 0,
                               bool attrs_only = false);
 cudaError_t split_launch_reduce(const SplitArgs& a, const int2* pairs, int npairs,
                                 cudaStream_t stream);
+int split_min_stages();    // shallowest pipeline of the main kernel (3)
 int split_row_tile();      // rows per work item (128)
 int split_point_tile();    // points per work item (64)
 int split_chunk();         // compacted AOs per chunk (32)

@@ -145,7 +145,7 @@ def test_split_plan_equals_single_split_calls(cm, wl, tmp_path, monkeypatch, gra
     info = plan.info()
     assert info["precision"] == "split" and info["graph"] is graph
     if tune:
-        assert [t["stages"] for t in info["tuning"]] == [2, 3, 4]
+        assert [t["stages"] for t in info["tuning"]] == [3, 4, 5]
     plan.run()
     torch.cuda.synchronize()
     for b, d in zip(bs, dev):
