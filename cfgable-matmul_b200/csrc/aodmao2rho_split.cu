@@ -42,7 +42,9 @@
 //                     turn the 8-byte elements into digit planes, stored
 //                     without bank conflicts) and later run the epilogue;
 //                     warp 12 issues the 28 MMAs of a chunk (M=128, N=64, K=32)
-//                     into 7 TMEM level accumulators (448 columns); warp 13
+//                     into 7 TMEM level accumulators (448 columns), grouped by
+//                     D digit so that each D plane is read once and reused
+//                     from the tensor core's collector buffer; warp 13
 //                     bulk-loads the phi digit tiles.  The epilogue rebuilds X
 //                     in FP64, weights it with phi and reduces over the rows
 //                     of each warp; X never leaves the SM.
@@ -602,12 +604,28 @@ __global__ void __launch_bounds__(THREADS, 1) split_main(SplitArgs p) {
           tc::fence_after_sync();
           const uint32_t a0 = tc::smem_u32(smem + stg * STAGE);
           const uint32_t b0 = a0 + A_STAGE;
+          // D digit i meets phi digits 0 .. NSL-1-i (levels i .. NSL-1) in
+          // consecutive MMAs, so its plane is read from shared memory once and
+          // held in the collector buffer for the rest; level L still receives
+          // its products in the order i = 0, 1, ..., L.
 #pragma unroll
-          for (int L = 0; L < NSL; ++L)
+          for (int i = 0; i < NSL; ++i) {
+            const uint64_t ad = tc::smem_desc_k32(a0 + i * A_SLICE);
+            const bool acc = c > kc0 || i > 0;
 #pragma unroll
-            for (int i = 0; i <= L; ++i)
-              tc::mma_i8(tmem + uint32_t(L * TG), tc::smem_desc_k32(a0 + i * A_SLICE),
-                         tc::smem_desc_k32(b0 + (L - i) * B_SLICE), idesc, c > kc0 || i > 0);
+            for (int L = i; L < NSL; ++L) {
+              const uint32_t d = tmem + uint32_t(L * TG);
+              const uint64_t bd = tc::smem_desc_k32(b0 + (L - i) * B_SLICE);
+              if (i == NSL - 1)
+                tc::mma_i8(d, ad, bd, idesc, acc);
+              else if (L == i)
+                tc::mma_i8_collect<tc::ACollector::kFill>(d, ad, bd, idesc, acc);
+              else if (L == NSL - 1)
+                tc::mma_i8_collect<tc::ACollector::kLastUse>(d, ad, bd, idesc, acc);
+              else
+                tc::mma_i8_collect<tc::ACollector::kUse>(d, ad, bd, idesc, acc);
+            }
+          }
           tc::mma_commit(&empty[stg]);
         }
         if (!ok) break;

@@ -145,6 +145,41 @@ __device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t
       : "memory");
 }
 
+// mma_i8 with the A operand kept in the tensor core's collector buffer across
+// consecutive MMAs that share it: kFill reads A from shared memory and keeps
+// it, kUse reads the kept copy, kLastUse reads it and releases it.  The same A
+// descriptor is passed each time.
+enum class ACollector { kFill, kUse, kLastUse };
+template <ACollector U>
+__device__ __forceinline__ void mma_i8_collect(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                               uint32_t idesc, bool accumulate) {
+  if constexpr (U == ACollector::kFill) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8.collector::a::fill [%0], %1, %2, %3, p;\n\t}" ::"r"(
+            d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(uint32_t(accumulate))
+        : "memory");
+  } else if constexpr (U == ACollector::kUse) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8.collector::a::use [%0], %1, %2, %3, p;\n\t}" ::"r"(
+            d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(uint32_t(accumulate))
+        : "memory");
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8.collector::a::lastuse [%0], %1, %2, %3, p;\n\t}" ::"r"(
+            d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(uint32_t(accumulate))
+        : "memory");
+  }
+}
+
 // Arrives once on `bar` when all previously issued tcgen05.mma of this thread
 // have completed (their shared-memory operands may then be overwritten).
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
