@@ -195,9 +195,11 @@ __global__ void finalize_exps(const int* __restrict__ emax, int rows, int bits, 
 // The integer v (|v| <= 2^52) is written in balanced 14-bit digits:
 // w = v + 2^13 (1 + 2^14 + 2^28) gives u_t = (w >> 14t) & 0x3fff (t < 3) and
 // d_3 = w >> 42 with v = sum_{t<3} (u_t - 2^13) 2^14t + d_3 2^42.  With the
-// symmetric c_t = 2^(14t) mods m (|c_t| <= 127) and K = -2^13 (1 + c_14 + c_28)
-//   s = u_0 + K + u_1 c_14 + u_2 c_28 + d_3 c_42,   |s| < 2.3e6 < 2^22,
-// is exact in FP32 and congruent to v.  Then q = rint(s / m) comes out exact
+// symmetric c_t = 2^(14t) mods m (|c_t| <= 127) and the balanced digits
+// b_t = u_t - 2^13 (formed once per element, before the modulus loop)
+//   s = b_0 + b_1 c_14 + b_2 c_28 + d_3 c_42,   |s| < 2.3e6 < 2^22,
+// (three FMAs per modulus, every partial sum below 2^22) is exact in FP32 and
+// congruent to v.  Then q = rint(s / m) comes out exact
 // from one FMA against MAGIC = 1.5 2^23 (|s| < 2^22 keeps the error of s*inv
 // below 1/(2m), the least distance of s/m from a half-integer for odd m), the
 // residue r = s - m q is exact, and r + MAGIC holds r in the low byte of its
@@ -259,9 +261,9 @@ __device__ __forceinline__ void write_residues8(const ResidueArgs& a, int8_t* Y,
       const long long iv = static_cast<long long>(v[j + h]);
       lowb[(j + h) >> 2] |= uint32_t(iv & 0xff) << (8 * ((j + h) & 3));  // modulus 256
       const long long w = iv + kBias;
-      u[h][0] = float(int(w & 0x3fff));
-      u[h][1] = float(int((w >> 14) & 0x3fff));
-      u[h][2] = float(int((w >> 28) & 0x3fff));
+      u[h][0] = float(int(w & 0x3fff) - 8192);
+      u[h][1] = float(int((w >> 14) & 0x3fff) - 8192);
+      u[h][2] = float(int((w >> 28) & 0x3fff) - 8192);
       u[h][3] = float(int(w >> 42));
     }
     P0[j >> 1] = pack2(u[0][0], u[1][0]);
@@ -272,8 +274,7 @@ __device__ __forceinline__ void write_residues8(const ResidueArgs& a, int8_t* Y,
   *reinterpret_cast<uint2*>(Y + off) = make_uint2(lowb[0], lowb[1]);
   const f32x2 MAG = pack2(kMagic, kMagic), NMAG = pack2(-kMagic, -kMagic);
   for (int l = 1; l < a.nmod; ++l) {
-    const float k0 = -8192.0f * (1.0f + a.c14[l] + a.c28[l]);
-    const f32x2 K = pack2(k0, k0), C14 = pack2(a.c14[l], a.c14[l]),
+    const f32x2 C14 = pack2(a.c14[l], a.c14[l]),
                 C28 = pack2(a.c28[l], a.c28[l]), C42 = pack2(a.c42[l], a.c42[l]),
                 INV = pack2(a.inv[l], a.inv[l]);
     const float nm = -float(a.mod[l]);
@@ -281,8 +282,7 @@ __device__ __forceinline__ void write_residues8(const ResidueArgs& a, int8_t* Y,
     uint32_t bits[8];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      f32x2 S = add2(P0[q], K);
-      S = fma2(P1[q], C14, S);
+      f32x2 S = fma2(P1[q], C14, P0[q]);
       S = fma2(P2[q], C28, S);
       S = fma2(P3[q], C42, S);                      // s, exact
       const f32x2 Q = add2(fma2(S, INV, MAG), NMAG);  // rint(s / m), exact
@@ -345,58 +345,56 @@ residues_cols(const double* __restrict__ x, size_t ld, int rows, int k, size_t k
 struct ReconArgs {
   int nmod;
   double w_hi[kMaxModuli], w_lo[kMaxModuli];
-  float w_frac_f[kMaxModuli];  // w_l / M in FP32 (for the quotient only)
+  double w_frac[kMaxModuli];  // w_l / M (for the quotient only)
   double M_hi, M_lo, two_T;
 };
 
-// A thread rebuilds 8 consecutive C[i][j]: all its residue loads are issued
-// before the arithmetic (8 bytes per modulus plane), so the loads of a warp are
-// in flight together.  q = rint(t) takes t in FP32: |C'| <= M/8 keeps t within
-// 1/8 of the integer q, far above the FP32 error of sum_l r_l w_l / M (below
-// 2^-9 for |r_l| <= 128, N <= 16), so q is the one of exact arithmetic; the
-// hi / lo sums stay in FP64.
+// A thread rebuilds 4 consecutive C[i][j]: its residue loads (4 bytes per
+// modulus plane) are all issued before the arithmetic.  A residue byte becomes
+// an exact double without a conversion instruction: with its sign bit flipped
+// it is r + 128 in [0, 255], placed in the low word of 2^52 and the 2^52 + 128
+// subtracted again.  t = sum_l r_l w_l / M in FP64 is within 2^-40 of the
+// exact value, and |C'| <= M/8 keeps the exact value within 1/8 of the
+// integer q, so q = rint(t) is the one of exact arithmetic; the hi / lo sums
+// are exact (every partial sum < 2^53).
 __global__ void __launch_bounds__(256)
 reconstruct(double* __restrict__ c, size_t ldc, int m, int n, const int8_t* __restrict__ R,
             size_t ldr, const int* __restrict__ ea, const int* __restrict__ eb, ReconArgs a) {
-  const int bpr = (n + 2047) / 2048;  // CTAs per row of C
+  const int bpr = (n + 1023) / 1024;  // CTAs per row of C
   const int i = blockIdx.x / bpr;
-  const int j0 = ((blockIdx.x % bpr) * 256 + threadIdx.x) * 8;
+  const int j0 = ((blockIdx.x % bpr) * 256 + threadIdx.x) * 4;
   if (j0 >= n || i >= m) return;
   const size_t plane = size_t(m) * ldr;
-  // ldr is a multiple of 16 and j0 of 8: the 8 bytes at j0 lie inside row i
+  // ldr is a multiple of 16 and j0 of 4: the 4 bytes at j0 lie inside row i
   const int8_t* Ri = R + size_t(i) * ldr + j0;
-  uint2 rv[kMaxModuli];
+  uint32_t rv[kMaxModuli];
 #pragma unroll
   for (int l = 0; l < kMaxModuli; ++l)
-    if (l < a.nmod) rv[l] = __ldg(reinterpret_cast<const uint2*>(Ri + size_t(l) * plane));
-  float t[8];
-  double X[8], Y[8];
+    if (l < a.nmod) rv[l] = __ldg(reinterpret_cast<const uint32_t*>(Ri + size_t(l) * plane));
+  constexpr double kBias = 4503599627370624.0;  // 2^52 + 128
+  double t[4], X[4], Y[4];
 #pragma unroll
-  for (int u = 0; u < 8; ++u) {
-    t[u] = 0.f;
-    X[u] = Y[u] = 0.0;
-  }
+  for (int u = 0; u < 4; ++u) t[u] = X[u] = Y[u] = 0.0;
 #pragma unroll
   for (int l = 0; l < kMaxModuli; ++l) {
     if (l >= a.nmod) break;
+    const uint32_t wb = rv[l] ^ 0x80808080u;  // r + 128 in every byte
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const uint32_t w = u < 4 ? rv[l].x : rv[l].y;
-      const int ri = static_cast<int8_t>(w >> (8 * (u & 3)));
-      const double r = double(ri);
-      t[u] = fmaf(float(ri), a.w_frac_f[l], t[u]);
-      X[u] = fma(r, a.w_hi[l], X[u]);  // exact: every partial sum < 2^53
+    for (int u = 0; u < 4; ++u) {
+      const double r = __hiloint2double(0x43300000, int(__byte_perm(wb, 0u, 0x4440u + u))) - kBias;
+      t[u] = fma(r, a.w_frac[l], t[u]);
+      X[u] = fma(r, a.w_hi[l], X[u]);  // exact
       Y[u] = fma(r, a.w_lo[l], Y[u]);
     }
   }
   const int ei = ea[i];
   double* ci = c + size_t(i) * ldc;
 #pragma unroll
-  for (int u = 0; u < 8; ++u) {
+  for (int u = 0; u < 4; ++u) {
     const int j = j0 + u;
     if (j >= n) break;
     const int fj = eb[j];
-    const double q = double(rintf(t[u]));
+    const double q = rint(t[u]);
     const double hi = fma(-q, a.M_hi, X[u]);  // exact
     const double lo = fma(-q, a.M_lo, Y[u]);
     const double cp = fma(hi, a.two_T, lo);   // C' with one rounding
@@ -573,14 +571,14 @@ cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int 
   ReconArgs rc{};
   rc.nmod = plan.nmod;
   for (int l = 0; l < plan.nmod; ++l) {
-    rc.w_frac_f[l] = float(plan.w_frac[l]);
+    rc.w_frac[l] = plan.w_frac[l];
     rc.w_hi[l] = plan.w_hi[l];
     rc.w_lo[l] = plan.w_lo[l];
   }
   rc.M_hi = plan.M_hi;
   rc.M_lo = plan.M_lo;
   rc.two_T = plan.two_T;
-  const long long rgrid = (long long)((n + 2047) / 2048) * m;
+  const long long rgrid = (long long)((n + 1023) / 1024) * m;
   if (rgrid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
   if (c_ready && (err = cudaStreamWaitEvent(stream, c_ready, 0)) != cudaSuccess) return err;
   reconstruct<<<unsigned(rgrid), 256, 0, stream>>>(c, ldc, m, n, r, L.ldr, ea, eb, rc);
