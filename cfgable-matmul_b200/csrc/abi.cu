@@ -7,6 +7,7 @@
 // device or an output buffer.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <climits>
 #include <cstdlib>
 #include <cstdint>
@@ -77,6 +78,10 @@ struct DeviceState {
   // DGEMM's residues and INT8 GEMM (C is first read by the reconstruction)
   cudaStream_t copy = nullptr;
   cudaEvent_t ab_done = nullptr, c_ready = nullptr;
+  // row-blocked host GEMM: uploads on `copy`, compute on `stream`, downloads
+  // on `down`, one pair of events per block
+  cudaStream_t down = nullptr;
+  cudaEvent_t up[4] = {}, done[4] = {};
   void* buf = nullptr;
   size_t cap = 0;
 };
@@ -126,6 +131,18 @@ int ensure_copy_stream(DeviceState* st) {
   if (!st->copy) CFGMM_CUDA(cudaStreamCreateWithFlags(&st->copy, cudaStreamNonBlocking));
   if (!st->ab_done) CFGMM_CUDA(cudaEventCreateWithFlags(&st->ab_done, cudaEventDisableTiming));
   if (!st->c_ready) CFGMM_CUDA(cudaEventCreateWithFlags(&st->c_ready, cudaEventDisableTiming));
+  return CFGMM_OK;
+}
+
+// The download stream and block events of the row-blocked host GEMM (caller holds st->mu).
+int ensure_block_pipeline(DeviceState* st) {
+  int rc = ensure_copy_stream(st);
+  if (rc != CFGMM_OK) return rc;
+  if (!st->down) CFGMM_CUDA(cudaStreamCreateWithFlags(&st->down, cudaStreamNonBlocking));
+  for (int i = 0; i < 4; ++i) {
+    if (!st->up[i]) CFGMM_CUDA(cudaEventCreateWithFlags(&st->up[i], cudaEventDisableTiming));
+    if (!st->done[i]) CFGMM_CUDA(cudaEventCreateWithFlags(&st->done[i], cudaEventDisableTiming));
+  }
   return CFGMM_OK;
 }
 
@@ -238,6 +255,60 @@ int check_mask(const GemmMask& mk, size_t n, size_t k, uint8_t transb, size_t* t
   return CFGMM_OK;
 }
 
+// A large host-pointer GEMM in 4 blocks of rows of C and op(A): B goes up once,
+// then each block's rows of op(A) and C go up on the copy stream, the block is
+// computed on the compute stream and its rows of C come back on the download
+// stream, so that the transfers of one block overlap the work and the
+// transfers of the others (the PCIe link carries both directions at once).
+// The device buffers keep the host layouts; every element of C is computed
+// from the same row of op(A) and column of op(B) as in one call.
+int gemm_host_blocked(DeviceState* st, double* c, const double* a, const double* b, size_t m,
+                      size_t n, size_t k, size_t lda, size_t ldb, size_t ldc, bool transa,
+                      bool transb, bool split, int nmod, double* da, double* db, double* dc,
+                      void* ws) {
+  int rc = ensure_block_pipeline(st);
+  if (rc != CFGMM_OK) return rc;
+  constexpr size_t kBlocks = 4;
+  const size_t mb = (m + kBlocks - 1) / kBlocks;
+  const size_t eb = transb ? (n - 1) * ldb + k : (k - 1) * ldb + n;
+  cudaError_t err = cudaSuccess;
+  if (split) err = cfgmm::gemm_i8_reset_error(st->stream);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(db, b, eb * 8, cudaMemcpyHostToDevice, st->copy);
+  size_t blk = 0;
+  for (size_t i0 = 0; err == cudaSuccess && i0 < m; i0 += mb, ++blk) {
+    const size_t mk = std::min(mb, m - i0);
+    // this block's rows of op(A) (columns of A when transposed) and of C
+    err = transa ? cudaMemcpy2DAsync(da + i0, lda * 8, a + i0, lda * 8, mk * 8, k,
+                                     cudaMemcpyHostToDevice, st->copy)
+                 : cudaMemcpy2DAsync(da + i0 * lda, lda * 8, a + i0 * lda, lda * 8, k * 8, mk,
+                                     cudaMemcpyHostToDevice, st->copy);
+    if (err == cudaSuccess)
+      err = cudaMemcpy2DAsync(dc + i0 * ldc, ldc * 8, c + i0 * ldc, ldc * 8, n * 8, mk,
+                              cudaMemcpyHostToDevice, st->copy);
+    if (err == cudaSuccess) err = cudaEventRecord(st->up[blk], st->copy);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(st->stream, st->up[blk], 0);
+    const double* dak = transa ? da + i0 : da + i0 * lda;
+    if (err == cudaSuccess)
+      err = split ? cfgmm::ozaki_dgemm(dc + i0 * ldc, dak, db, int(mk), int(n), int(k), lda, ldb,
+                                       ldc, transa, transb, nmod, ws, st->stream)
+                  : cfgmm::dgemm_fp64(dc + i0 * ldc, dak, db, int(mk), int(n), int(k), lda, ldb,
+                                      ldc, transa, transb, st->stream);
+    if (err == cudaSuccess) err = cudaEventRecord(st->done[blk], st->stream);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(st->down, st->done[blk], 0);
+    if (err == cudaSuccess)
+      err = cudaMemcpy2DAsync(c + i0 * ldc, ldc * 8, dc + i0 * ldc, ldc * 8, n * 8, mk,
+                              cudaMemcpyDeviceToHost, st->down);
+  }
+  // every stream drained before the staging buffer can be reused
+  const cudaError_t e1 = cudaStreamSynchronize(st->copy);
+  const cudaError_t e2 = cudaStreamSynchronize(st->stream);
+  const cudaError_t e3 = cudaStreamSynchronize(st->down);
+  if (err == cudaSuccess) err = e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3);
+  if (err != cudaSuccess) return cuda_fail(err, "row-blocked GEMM");
+  return check_device_waits();
+}
+
 int gemm_host(double* c, size_t c_len, const double* a, size_t a_len, const double* b,
               size_t b_len, size_t m, size_t n, size_t k, size_t lda, size_t ldb, size_t ldc,
               uint8_t transa, uint8_t transb, int precision,
@@ -270,6 +341,9 @@ int gemm_host(double* c, size_t c_len, const double* a, size_t a_len, const doub
   double* db = reinterpret_cast<double*>(base + ob);
   double* dc = reinterpret_cast<double*>(base + oc);
   uint8_t* dt = masked ? reinterpret_cast<uint8_t*>(base + ot) : nullptr;
+  if (!masked && ex.c * 8 >= (size_t(64) << 20) && m >= 512)
+    return gemm_host_blocked(st, c, a, b, m, n, k, lda, ldb, ldc, transa != 0, transb != 0, split,
+                             nmod, da, db, dc, base + ows);
   CFGMM_CUDA(cudaMemcpyAsync(da, a, ex.a * 8, cudaMemcpyHostToDevice, st->stream));
   CFGMM_CUDA(cudaMemcpyAsync(db, b, ex.b * 8, cudaMemcpyHostToDevice, st->stream));
   if (masked) CFGMM_CUDA(cudaMemcpyAsync(dt, mk.tab, tab_ext, cudaMemcpyHostToDevice, st->stream));
