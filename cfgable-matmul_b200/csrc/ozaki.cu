@@ -371,6 +371,16 @@ reconstruct(double* __restrict__ c, size_t ldc, int m, int n, const int8_t* __re
 #pragma unroll
   for (int l = 0; l < kMaxModuli; ++l)
     if (l < a.nmod) rv[l] = __ldg(reinterpret_cast<const uint32_t*>(Ri + size_t(l) * plane));
+  // C and the column scales are requested with the residues (one round trip)
+  double* ci = c + size_t(i) * ldc;
+  double c_old[4];
+  int fj[4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const bool in = j0 + u < n;
+    c_old[u] = in ? ci[j0 + u] : 0.0;
+    fj[u] = in ? __ldg(eb + j0 + u) : 0;
+  }
   constexpr double kBias = 4503599627370624.0;  // 2^52 + 128
   double t[4], X[4], Y[4];
 #pragma unroll
@@ -388,25 +398,23 @@ reconstruct(double* __restrict__ c, size_t ldc, int m, int n, const int8_t* __re
     }
   }
   const int ei = ea[i];
-  double* ci = c + size_t(i) * ldc;
 #pragma unroll
   for (int u = 0; u < 4; ++u) {
     const int j = j0 + u;
     if (j >= n) break;
-    const int fj = eb[j];
     const double q = rint(t[u]);
     const double hi = fma(-q, a.M_hi, X[u]);  // exact
     const double lo = fma(-q, a.M_lo, Y[u]);
     const double cp = fma(hi, a.two_T, lo);   // C' with one rounding
-    const int sc = -(ei + fj);
+    const int sc = -(ei + fj[u]);
     double val;
-    if (ei == kNonFinite || fj == kNonFinite)
+    if (ei == kNonFinite || fj[u] == kNonFinite)
       val = __longlong_as_double(0x7ff8000000000000LL);
     else if (sc >= -1022 && sc <= 1023)  // exact scaling by a normal power of two
       val = cp * __longlong_as_double(static_cast<long long>(sc + 1023) << 52);
     else
       val = ldexp(cp, sc);
-    ci[j] += val;
+    ci[j] = c_old[u] + val;
   }
 }
 
