@@ -71,6 +71,9 @@ bool fits_int(size_t v) { return v <= size_t(INT_MAX) - 4096; }
 // ---------------------------------------------------------------------------
 // per-device state for the host-pointer entry points
 // ---------------------------------------------------------------------------
+// Row blocks of a large host-pointer GEMM (see gemm_host_blocked).
+constexpr size_t kHostBlocks = 4;
+
 struct DeviceState {
   std::mutex mu;
   cudaStream_t stream = nullptr;
@@ -81,7 +84,7 @@ struct DeviceState {
   // row-blocked host GEMM: uploads on `copy`, compute on `stream`, downloads
   // on `down`, one pair of events per block
   cudaStream_t down = nullptr;
-  cudaEvent_t up[4] = {}, done[4] = {};
+  cudaEvent_t up[kHostBlocks] = {}, done[kHostBlocks] = {};
   void* buf = nullptr;
   size_t cap = 0;
 };
@@ -139,7 +142,7 @@ int ensure_block_pipeline(DeviceState* st) {
   int rc = ensure_copy_stream(st);
   if (rc != CFGMM_OK) return rc;
   if (!st->down) CFGMM_CUDA(cudaStreamCreateWithFlags(&st->down, cudaStreamNonBlocking));
-  for (int i = 0; i < 4; ++i) {
+  for (size_t i = 0; i < kHostBlocks; ++i) {
     if (!st->up[i]) CFGMM_CUDA(cudaEventCreateWithFlags(&st->up[i], cudaEventDisableTiming));
     if (!st->done[i]) CFGMM_CUDA(cudaEventCreateWithFlags(&st->done[i], cudaEventDisableTiming));
   }
@@ -255,7 +258,7 @@ int check_mask(const GemmMask& mk, size_t n, size_t k, uint8_t transb, size_t* t
   return CFGMM_OK;
 }
 
-// A large host-pointer GEMM in 4 blocks of rows of C and op(A): B goes up once,
+// A large host-pointer GEMM in kHostBlocks blocks of rows of C and op(A): B goes up once,
 // then each block's rows of op(A) and C go up on the copy stream, the block is
 // computed on the compute stream and its rows of C come back on the download
 // stream, so that the transfers of one block overlap the work and the
@@ -268,8 +271,7 @@ int gemm_host_blocked(DeviceState* st, double* c, const double* a, const double*
                       void* ws) {
   int rc = ensure_block_pipeline(st);
   if (rc != CFGMM_OK) return rc;
-  constexpr size_t kBlocks = 4;
-  const size_t mb = (m + kBlocks - 1) / kBlocks;
+  const size_t mb = (m + kHostBlocks - 1) / kHostBlocks;
   const size_t eb = transb ? (n - 1) * ldb + k : (k - 1) * ldb + n;
   cudaError_t err = cudaSuccess;
   if (split) err = cfgmm::gemm_i8_reset_error(st->stream);
