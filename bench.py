@@ -252,7 +252,8 @@ def run_reference(args, ranks: Ranks):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": value / PUBLISHED_TFLOPS, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "m": M, "n": N, "k": K, "parallelism": "host threads"},
+        "config": {"workload": WORKLOAD, "arithmetic": "FP64 (the reference has no split-precision "
+                   "form)", "m": M, "n": N, "k": K, "parallelism": "host threads"},
         "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": oracle.max_threads(),
                          "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
@@ -599,7 +600,8 @@ def run_ours(args, ranks: Ranks):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": value / PUBLISHED_TFLOPS,
         "dtype": "i8 tensor cores + f64 reconstruction (Ozaki split precision)",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD + ", split precision", "m": M, "n": N, "k": K,
+        "config": {"workload": WORKLOAD, "arithmetic": "split precision (Ozaki CRT form on the "
+                   "INT8 tensor cores)", "m": M, "n": N, "k": K,
                    "moduli": nmod, "error_vs_fp64": split_err, "error_bar": 1e-12,
                    "parallelism": f"{ranks.world} independent replica(s), one per GPU",
                    "l2": "inputs larger than L2 (961 MB of A, B, C per step)",
