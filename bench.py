@@ -300,6 +300,74 @@ class Timed:
         return [self.ev[s][i0].elapsed_time(self.ev[s][i1]) for s in range(steps)]
 
 
+def next_rows_section(args, cm, wl, stream, p):
+    """The callers either side of the path, timed like the path itself (device
+    tensors, CUDA events on the launching stream, warm-up first): the masked
+    GEMM at the reference's own test shape (A 2228x2228, B 2228x16384, BLKSIZE
+    48, the periodic 30 % pattern over (k, block), masked B entries zero;
+    impl_matmul_non0tab.rs:328-377) in FP64 and split precision, and the
+    Fock-build contraction V_s += phi diag(w_s) phi^T on the taxol-size
+    geometric workload `p` (one phi array for both sides)."""
+    import torch
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    m, n, k, blk = 2228, 16384, 2228, 48
+    a, b, lda, ldb, tab, nblk = wl.ref_matmul_non0tab_inputs(m, n, k, blk)
+    da, db = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+    dtab = torch.from_numpy(tab).cuda()
+    c64 = torch.zeros(m, n, dtype=torch.float64, device="cuda")
+    csp = torch.zeros(m, n, dtype=torch.float64, device="cuda")
+    active = float(wl.expand_mask(tab, n, blk).sum())  # (p, j) pairs that take part
+    res = {"masked_gemm": {
+        "workload": "C(2228x16384) += A(2228x2228) B(2228x16384) over tab[p][j/48], periodic 30 % "
+                    "pattern (the reference's masked GEMM test), masked B entries zero",
+        "flops_per_call_masked": 2.0 * m * active, "flops_per_call_dense": 2.0 * m * n * k}}
+    for name, prec, out in (("fp64", cm.PREC_FP64, c64), ("split", cm.PREC_OZAKI_INT8, csp)):
+        ms = timed(lambda: cm.matmul_non0tab_ex(out, da, db, m, n, k, lda, ldb, n, False, False,
+                                                dtab, nblk, blk, prec))
+        res["masked_gemm"][name] = {"ms_per_call": ms,
+                                    "masked_tflops": 2.0 * m * active / (ms * 1e-3) / 1e12,
+                                    "dense_equivalent_tflops": 2.0 * m * n * k / (ms * 1e-3) / 1e12}
+    # one more call each from zero, to compare the two arithmetics
+    c64.zero_(); csp.zero_()
+    cm.matmul_non0tab_ex(c64, da, db, m, n, k, lda, ldb, n, False, False, dtab, nblk, blk,
+                         cm.PREC_FP64)
+    cm.matmul_non0tab_ex(csp, da, db, m, n, k, lda, ldb, n, False, False, dtab, nblk, blk,
+                         cm.PREC_OZAKI_INT8)
+    torch.cuda.synchronize()
+    res["masked_gemm"]["split"]["error_vs_fp64"] = float((csp - c64).abs().max() / c64.abs().max())
+    del da, db, dtab, c64, csp
+
+    ao = torch.from_numpy(p.ao).cuda()
+    ptab = torch.from_numpy(p.tab).cuda()
+    g = torch.Generator(device="cuda").manual_seed(5)
+    w = torch.rand(p.nset, p.ngrid, dtype=torch.float64, device="cuda", generator=g)
+    v = torch.zeros(p.nset, p.nao, p.nao, dtype=torch.float64, device="cuda")
+    nb = p.tab.astype(bool).sum(axis=0).astype(np.float64)
+    pts = np.minimum(p.blksize, p.ngrid - p.blksize * np.arange(p.nblk)).astype(np.float64)
+    fflops = 2.0 * p.nset * float(np.sum(nb * nb * pts))  # sum_s sum_b 2 |I_b|^2 |b|
+    ms = timed(lambda: cm.aodm_fock(v, w, ao, ao, (p.nao, p.ngrid), (p.nao, p.ngrid), p.nset,
+                                    ptab, p.nblk, p.blksize))
+    res["fock"] = {"workload": p.name + f", blocks of {p.blksize}, one phi array for both sides",
+                   "ms_per_call": ms, "flops_per_call": fflops,
+                   "tflops": fflops / (ms * 1e-3) / 1e12,
+                   "form": "compacted AO lists, symmetric pairs formed once, FP64 atomics into V"}
+    del ao, ptab, w, v
+    torch.cuda.empty_cache()
+    return res
+
+
 def batched_section(args, cm, wl, stream):
     """Uneven grid batches of one molecule in one graph-captured persistent
     launch (a plan), FP64 and split precision: 2228 AOs, 256 batches with
@@ -588,6 +656,7 @@ def run_ours(args, ranks: Ranks):
         aodm["cpu_baseline"] = cpu_aodm_run(p)
     del ao, dms, tab, rho, r64, rsp
     torch.cuda.empty_cache()
+    nextrows = next_rows_section(args, cm, wl, stream, p) if not args.no_next else None
     batched = batched_section(args, cm, wl, stream) if not args.no_batched else None
     serving = serving_section(args, cm, wl) if not args.no_serving else None
 
@@ -644,6 +713,8 @@ def run_ours(args, ranks: Ranks):
         "clocks": clk,
         "aodmao2rho": aodm,
     }
+    if nextrows:
+        out.update(nextrows)
     if batched:
         out["aodmao2rho_batched"] = batched
     if serving:
@@ -729,6 +800,8 @@ def main():
     ap.add_argument("--k", type=int, default=4096)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-plan section")
+    ap.add_argument("--no-next", action="store_true",
+                    help="skip the masked-GEMM and Fock-build sections")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving section")
     ap.add_argument("--serve-molecules", type=int, default=24)
     ap.add_argument("--serve-gap-ms", type=float, default=40.0)
