@@ -777,15 +777,24 @@ aodm_sym_check(const double* __restrict__ dms, size_t stride_ao, size_t dm_strid
   __shared__ double tile[32][33];
   const double* d = dms + size_t(blockIdx.z) * dm_stride;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  for (int i = ty; i < 32; i += 8) {
+  // both tiles are requested before the barrier: tile (by, bx) into shared
+  // memory, this thread's elements of tile (bx, by) into registers
+  double mine[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int i = ty + 8 * k;
     const int r = by * 32 + i, c = bx * 32 + tx;
     tile[i][tx] = (r < nao && c < nao) ? d[size_t(r) * stride_ao + c] : 0.0;
+    const int r2 = bx * 32 + i, c2 = by * 32 + tx;
+    mine[k] = (r2 < nao && c2 < nao) ? d[size_t(r2) * stride_ao + c2] : 0.0;
   }
   __syncthreads();
   bool bad = false;
-  for (int i = ty; i < 32; i += 8) {
-    const int r = bx * 32 + i, c = by * 32 + tx;
-    if (r < nao && c < nao) bad |= !(d[size_t(r) * stride_ao + c] == tile[tx][i]);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int i = ty + 8 * k;
+    const int r2 = bx * 32 + i, c2 = by * 32 + tx;
+    if (r2 < nao && c2 < nao) bad |= !(mine[k] == tile[tx][i]);
   }
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(asym, 1);
 }
