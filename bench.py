@@ -43,6 +43,7 @@ import re
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -108,7 +109,9 @@ class Clocks:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv")
+        # the raw samples (a CSV per rank) go to CFGMM_CLOCKS_DIR, else the temp directory
+        out_dir = os.environ.get("CFGMM_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(out_dir, f"cfgmm_clocks_rank{gpu_index}.csv")
 
     def start(self):
         try:

@@ -1,7 +1,7 @@
 """GPU tests of the split-precision DGEMM (Ozaki scheme on INT8 tcgen05 tensor
 cores) through the C ABI.  Bar: within 1e-12 normwise of FP64 (the oracle, or
 the reference tests' dense comparator); the reference has no such path, so
-the FP64 oracle is the only judge of accuracy here."""
+the FP64 oracle is the only reference for its accuracy."""
 import numpy as np
 import pytest
 
