@@ -115,9 +115,9 @@ def test_split_full_size_sampled(cm, wl, ta, tb):
     assert normwise(c[i, j], ref) < TOL
 
 
-@pytest.mark.parametrize("ta", [False, True])
+@pytest.mark.parametrize("ta,tb", [(False, False), (True, False), (False, True), (True, True)])
 @pytest.mark.parametrize("prec", [0, 1])
-def test_large_host_call_in_row_blocks(cm, ta, prec):
+def test_large_host_call_in_row_blocks(cm, ta, tb, prec):
     """A host-pointer call with C above 64 MB runs in blocks of rows whose
     transfers overlap the work: accumulation into a nonzero C, odd lda/ldc, and
     (split precision) the same bits as one device-pointer call."""
@@ -125,19 +125,21 @@ def test_large_host_call_in_row_blocks(cm, ta, prec):
     m, n, k = 1100, 8000, 600
     lda = (m if ta else k) + 5
     ldc = n + 3
-    rng = np.random.default_rng(40 + 2 * ta + prec)
+    ldb = (k if tb else n) + 2
+    rng = np.random.default_rng(40 + 4 * ta + 2 * tb + prec)
     a = rng.uniform(-1, 1, (k, lda) if ta else (m, lda))
-    b = rng.uniform(-1, 1, (k, n))
+    b = rng.uniform(-1, 1, (n, ldb) if tb else (k, ldb))
     c0 = rng.uniform(-1, 1, (m, ldc))
     c = c0.copy()
-    cm.matmul_ex(c, a, b, m, n, k, lda, n, ldc, ta, False, prec)
+    cm.matmul_ex(c, a, b, m, n, k, lda, ldb, ldc, ta, tb, prec)
     A = a[:, :m].T if ta else a[:, :k]
-    ref = c0[:, :n] + A @ b
+    B = b[:, :k].T if tb else b[:, :n]
+    ref = c0[:, :n] + A @ B
     assert normwise(c[:, :n], ref) < (1e-12 if prec else 1e-13)
     assert np.array_equal(c[:, n:], c0[:, n:])  # padding of C untouched
     if prec:
         dc = torch.from_numpy(c0.copy()).cuda()
-        cm.matmul_ex(dc, torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda(), m, n, k, lda, n,
-                     ldc, ta, False, prec)
+        cm.matmul_ex(dc, torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda(), m, n, k, lda, ldb,
+                     ldc, ta, tb, prec)
         torch.cuda.synchronize()
         assert np.array_equal(dc.cpu().numpy(), c)
