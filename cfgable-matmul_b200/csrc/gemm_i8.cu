@@ -32,7 +32,7 @@ namespace {
 
 constexpr int BM = 128, BN = 256, BK = 128, STAGES = 4, KSTEPS = BK / 32;
 constexpr int THREADS = 192;
-constexpr int GROUP_M = 8;
+constexpr int GROUP_M = 16;
 constexpr uint32_t A_STAGE = BM * BK, B_STAGE = BN * BK;  // bytes
 constexpr uint32_t STAGE_BYTES = A_STAGE + B_STAGE;
 constexpr uint32_t TMEM_COLS = 512;
