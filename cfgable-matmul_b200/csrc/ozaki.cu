@@ -298,7 +298,7 @@ __device__ __forceinline__ void write_residues8(const ResidueArgs& a, int8_t* Y,
 }
 
 // element (r, p) at x[r*ld + p]: CTA per row, thread per 8 consecutive p
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 5)
 residues_rows(const double* __restrict__ x, size_t ld, int rows, int k, size_t kpad,
               const int* __restrict__ e, int8_t* __restrict__ Y, ResidueArgs a) {
   const int r = blockIdx.x;
@@ -315,7 +315,7 @@ residues_rows(const double* __restrict__ x, size_t ld, int rows, int k, size_t k
 }
 
 // element (r, p) at x[p*ld + r]: 32 (r) x 64 (p) tiles transposed through shared memory
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 5)
 residues_cols(const double* __restrict__ x, size_t ld, int rows, int k, size_t kpad,
               const int* __restrict__ e, int8_t* __restrict__ Y, ResidueArgs a, Mask mask) {
   __shared__ double tile[64][33];
