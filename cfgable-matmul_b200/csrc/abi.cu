@@ -271,15 +271,23 @@ int gemm_host_blocked(DeviceState* st, double* c, const double* a, const double*
                       void* ws) {
   int rc = ensure_block_pipeline(st);
   if (rc != CFGMM_OK) return rc;
-  const size_t mb = (m + kHostBlocks - 1) / kHostBlocks;
+  // shrinking blocks (34, 28, 22, 16 % of the rows): the last block's work and
+  // download, which nothing overlaps, are the smallest
+  static constexpr double kShare[kHostBlocks] = {0.34, 0.28, 0.22, 0.16};
+  size_t bound[kHostBlocks + 1] = {0};
+  double acc = 0.0;
+  for (size_t i = 0; i < kHostBlocks; ++i) {
+    acc += kShare[i];
+    bound[i + 1] = i + 1 == kHostBlocks ? m : std::min(m, size_t(acc * double(m) + 0.5));
+  }
   const size_t eb = transb ? (n - 1) * ldb + k : (k - 1) * ldb + n;
   cudaError_t err = cudaSuccess;
   if (split) err = cfgmm::gemm_i8_reset_error(st->stream);
   if (err == cudaSuccess)
     err = cudaMemcpyAsync(db, b, eb * 8, cudaMemcpyHostToDevice, st->copy);
-  size_t blk = 0;
-  for (size_t i0 = 0; err == cudaSuccess && i0 < m; i0 += mb, ++blk) {
-    const size_t mk = std::min(mb, m - i0);
+  for (size_t blk = 0; err == cudaSuccess && blk < kHostBlocks; ++blk) {
+    const size_t i0 = bound[blk], mk = bound[blk + 1] - i0;
+    if (mk == 0) continue;
     // this block's rows of op(A) (columns of A when transposed) and of C
     err = transa ? cudaMemcpy2DAsync(da + i0, lda * 8, a + i0, lda * 8, mk * 8, k,
                                      cudaMemcpyHostToDevice, st->copy)
