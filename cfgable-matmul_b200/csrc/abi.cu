@@ -264,7 +264,8 @@ int check_mask(const GemmMask& mk, size_t n, size_t k, uint8_t transb, size_t* t
 // stream, so that the transfers of one block overlap the work and the
 // transfers of the others (the PCIe link carries both directions at once).
 // The device buffers keep the host layouts; every element of C is computed
-// from the same row of op(A) and column of op(B) as in one call.
+// from the same row of op(A) and column of op(B) as in one call.  In split
+// precision the residues of B are formed by the first block and reused.
 int gemm_host_blocked(DeviceState* st, double* c, const double* a, const double* b, size_t m,
                       size_t n, size_t k, size_t lda, size_t ldb, size_t ldc, bool transa,
                       bool transb, bool split, int nmod, double* da, double* db, double* dc,
@@ -301,7 +302,8 @@ int gemm_host_blocked(DeviceState* st, double* c, const double* a, const double*
     const double* dak = transa ? da + i0 : da + i0 * lda;
     if (err == cudaSuccess)
       err = split ? cfgmm::ozaki_dgemm(dc + i0 * ldc, dak, db, int(mk), int(n), int(k), lda, ldb,
-                                       ldc, transa, transb, nmod, ws, st->stream)
+                                       ldc, transa, transb, nmod, ws, st->stream, nullptr,
+                                       nullptr, 0, 1, nullptr, int(m), blk > 0)
                   : cfgmm::dgemm_fp64(dc + i0 * ldc, dak, db, int(mk), int(n), int(k), lda, ldb,
                                       ldc, transa, transb, st->stream);
     if (err == cudaSuccess) err = cudaEventRecord(st->done[blk], st->stream);

@@ -532,13 +532,15 @@ size_t ozaki_dgemm_workspace(int m, int n, int k, int nmod) {
 cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int n, int k,
                         size_t lda, size_t ldb, size_t ldc, bool transa, bool transb, int nmod,
                         void* workspace, cudaStream_t stream, const cudaEvent_t* events,
-                        const uint8_t* tab, size_t ldtab, int blk, cudaEvent_t c_ready) {
+                        const uint8_t* tab, size_t ldtab, int blk, cudaEvent_t c_ready,
+                        int m_layout, bool reuse_b) {
   if (tab && transb) return cudaErrorInvalidValue;  // the masked GEMM has no transb
   if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
   auto mark = [&](int i) { if (events) cudaEventRecord(events[i], stream); };
   if (k > kOzakiMaxK) return cudaErrorInvalidValue;
   const OzakiPlan plan = ozaki_plan(k, nmod, 0);
-  const DgemmLayout L = dgemm_layout(m, n, k, plan.nmod);
+  if (m_layout < m) m_layout = m;
+  const DgemmLayout L = dgemm_layout(m_layout, n, k, plan.nmod);
   char* ws = static_cast<char*>(workspace);
   int8_t* a_res = reinterpret_cast<int8_t*>(ws + L.a_res);
   int8_t* b_res = reinterpret_cast<int8_t*>(ws + L.b_res);
@@ -553,9 +555,11 @@ cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int 
   cudaError_t err =
       prepare(a, lda, !transa, m, k, L.kpad, plan.alpha, emax, ea, a_res, ra, stream);
   if (err != cudaSuccess) return err;
-  err = prepare(b, ldb, transb, n, k, L.kpad, plan.beta, emax, eb, b_res, ra, stream,
-                Mask{tab, ldtab, blk > 0 ? blk : 1});
-  if (err != cudaSuccess) return err;
+  if (!reuse_b) {
+    err = prepare(b, ldb, transb, n, k, L.kpad, plan.beta, emax, eb, b_res, ra, stream,
+                  Mask{tab, ldtab, blk > 0 ? blk : 1});
+    if (err != cudaSuccess) return err;
+  }
 
   mark(1);
   CUtensorMap tmA, tmB;
