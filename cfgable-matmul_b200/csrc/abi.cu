@@ -71,7 +71,7 @@ bool fits_int(size_t v) { return v <= size_t(INT_MAX) - 4096; }
 // ---------------------------------------------------------------------------
 // per-device state for the host-pointer entry points
 // ---------------------------------------------------------------------------
-// Row blocks of a large host-pointer GEMM (see gemm_host_blocked).
+// Blocks of a large host-pointer GEMM (see gemm_host_blocked).
 constexpr size_t kHostBlocks = 4;
 
 struct DeviceState {
@@ -81,8 +81,8 @@ struct DeviceState {
   // DGEMM's residues and INT8 GEMM (C is first read by the reconstruction)
   cudaStream_t copy = nullptr;
   cudaEvent_t ab_done = nullptr, c_ready = nullptr;
-  // row-blocked host GEMM: uploads on `copy`, compute on `stream`, downloads
-  // on `down`, one pair of events per block
+  // blocked host GEMM: uploads on `copy`, compute on `stream`, downloads on
+  // `down`, one pair of events per block
   cudaStream_t down = nullptr;
   cudaEvent_t up[kHostBlocks] = {}, done[kHostBlocks] = {};
   void* buf = nullptr;
@@ -137,7 +137,7 @@ int ensure_copy_stream(DeviceState* st) {
   return CFGMM_OK;
 }
 
-// The download stream and block events of the row-blocked host GEMM (caller holds st->mu).
+// The download stream and block events of the blocked host GEMM (caller holds st->mu).
 int ensure_block_pipeline(DeviceState* st) {
   int rc = ensure_copy_stream(st);
   if (rc != CFGMM_OK) return rc;
@@ -258,66 +258,87 @@ int check_mask(const GemmMask& mk, size_t n, size_t k, uint8_t transb, size_t* t
   return CFGMM_OK;
 }
 
-// A large host-pointer GEMM in kHostBlocks blocks of rows of C and op(A): B goes up once,
-// then each block's rows of op(A) and C go up on the copy stream, the block is
-// computed on the compute stream and its rows of C come back on the download
-// stream, so that the transfers of one block overlap the work and the
-// transfers of the others (the PCIe link carries both directions at once).
-// The device buffers keep the host layouts; every element of C is computed
-// from the same row of op(A) and column of op(B) as in one call.  In split
-// precision the residues of B are formed by the first block and reused.
+// A large host-pointer GEMM in kHostBlocks blocks, so that the PCIe transfers
+// of one block overlap the work and the transfers of the others (the link
+// carries both directions at once): one operand goes up whole first, then each
+// block's part of the other operand and of C go up on the copy stream, the
+// block is computed on the compute stream and its part of C comes back on the
+// download stream.  The blocks shrink (34, 28, 22, 16 %): the last block's work
+// and download, which nothing overlaps, are the smallest.  In split precision
+// the blocks are rows of C and op(A), B goes up first and its residues are
+// formed once (the transfers bound the call, and whole rows copy fastest); in
+// FP64 they are columns of C and op(B) and A goes up first (186 MB instead of
+// 505 MB at the headline shape, so the work, which bounds that call, starts
+// sooner).  The device buffers keep the host layouts; every element of C is
+// computed from the same row of op(A) and column of op(B) as in one call.
 int gemm_host_blocked(DeviceState* st, double* c, const double* a, const double* b, size_t m,
                       size_t n, size_t k, size_t lda, size_t ldb, size_t ldc, bool transa,
                       bool transb, bool split, int nmod, double* da, double* db, double* dc,
                       void* ws) {
   int rc = ensure_block_pipeline(st);
   if (rc != CFGMM_OK) return rc;
-  // shrinking blocks (34, 28, 22, 16 % of the rows): the last block's work and
-  // download, which nothing overlaps, are the smallest
+  const bool by_rows = split;
+  const size_t extent = by_rows ? m : n;
   static constexpr double kShare[kHostBlocks] = {0.34, 0.28, 0.22, 0.16};
   size_t bound[kHostBlocks + 1] = {0};
   double acc = 0.0;
   for (size_t i = 0; i < kHostBlocks; ++i) {
     acc += kShare[i];
-    bound[i + 1] = i + 1 == kHostBlocks ? m : std::min(m, size_t(acc * double(m) + 0.5));
+    bound[i + 1] =
+        i + 1 == kHostBlocks ? extent : std::min(extent, size_t(acc * double(extent) + 0.5));
   }
+  const size_t ea = transa ? (k - 1) * lda + m : (m - 1) * lda + k;
   const size_t eb = transb ? (n - 1) * ldb + k : (k - 1) * ldb + n;
   cudaError_t err = cudaSuccess;
   if (split) err = cfgmm::gemm_i8_reset_error(st->stream);
   if (err == cudaSuccess)
-    err = cudaMemcpyAsync(db, b, eb * 8, cudaMemcpyHostToDevice, st->copy);
+    err = by_rows ? cudaMemcpyAsync(db, b, eb * 8, cudaMemcpyHostToDevice, st->copy)
+                  : cudaMemcpyAsync(da, a, ea * 8, cudaMemcpyHostToDevice, st->copy);
+  size_t done_blocks = 0;
   for (size_t blk = 0; err == cudaSuccess && blk < kHostBlocks; ++blk) {
-    const size_t i0 = bound[blk], mk = bound[blk + 1] - i0;
-    if (mk == 0) continue;
-    // this block's rows of op(A) (columns of A when transposed) and of C
-    err = transa ? cudaMemcpy2DAsync(da + i0, lda * 8, a + i0, lda * 8, mk * 8, k,
-                                     cudaMemcpyHostToDevice, st->copy)
-                 : cudaMemcpy2DAsync(da + i0 * lda, lda * 8, a + i0 * lda, lda * 8, k * 8, mk,
-                                     cudaMemcpyHostToDevice, st->copy);
+    const size_t x0 = bound[blk], xk = bound[blk + 1] - x0;
+    if (xk == 0) continue;
+    // the block of C: rows x0.. (by_rows) or columns x0..; pointers into the
+    // device copies, which keep the host layouts
+    const size_t i0 = by_rows ? x0 : 0, mk = by_rows ? xk : m;
+    const size_t j0 = by_rows ? 0 : x0, nk = by_rows ? n : xk;
+    if (by_rows)  // rows of op(A): columns of A when transposed
+      err = transa ? cudaMemcpy2DAsync(da + i0, lda * 8, a + i0, lda * 8, mk * 8, k,
+                                       cudaMemcpyHostToDevice, st->copy)
+                   : cudaMemcpy2DAsync(da + i0 * lda, lda * 8, a + i0 * lda, lda * 8, k * 8, mk,
+                                       cudaMemcpyHostToDevice, st->copy);
+    else  // columns of op(B): rows of B when transposed
+      err = transb ? cudaMemcpy2DAsync(db + j0 * ldb, ldb * 8, b + j0 * ldb, ldb * 8, k * 8, nk,
+                                       cudaMemcpyHostToDevice, st->copy)
+                   : cudaMemcpy2DAsync(db + j0, ldb * 8, b + j0, ldb * 8, nk * 8, k,
+                                       cudaMemcpyHostToDevice, st->copy);
+    double* dck = dc + i0 * ldc + j0;
     if (err == cudaSuccess)
-      err = cudaMemcpy2DAsync(dc + i0 * ldc, ldc * 8, c + i0 * ldc, ldc * 8, n * 8, mk,
+      err = cudaMemcpy2DAsync(dck, ldc * 8, c + i0 * ldc + j0, ldc * 8, nk * 8, mk,
                               cudaMemcpyHostToDevice, st->copy);
     if (err == cudaSuccess) err = cudaEventRecord(st->up[blk], st->copy);
     if (err == cudaSuccess) err = cudaStreamWaitEvent(st->stream, st->up[blk], 0);
     const double* dak = transa ? da + i0 : da + i0 * lda;
+    const double* dbk = transb ? db + j0 * ldb : db + j0;
     if (err == cudaSuccess)
-      err = split ? cfgmm::ozaki_dgemm(dc + i0 * ldc, dak, db, int(mk), int(n), int(k), lda, ldb,
-                                       ldc, transa, transb, nmod, ws, st->stream, nullptr,
-                                       nullptr, 0, 1, nullptr, int(m), blk > 0)
-                  : cfgmm::dgemm_fp64(dc + i0 * ldc, dak, db, int(mk), int(n), int(k), lda, ldb,
-                                      ldc, transa, transb, st->stream);
+      err = split ? cfgmm::ozaki_dgemm(dck, dak, dbk, int(mk), int(nk), int(k), lda, ldb, ldc,
+                                       transa, transb, nmod, ws, st->stream, nullptr, nullptr, 0,
+                                       1, nullptr, int(m), int(n), false, done_blocks > 0)
+                  : cfgmm::dgemm_fp64(dck, dak, dbk, int(mk), int(nk), int(k), lda, ldb, ldc,
+                                      transa, transb, st->stream);
     if (err == cudaSuccess) err = cudaEventRecord(st->done[blk], st->stream);
     if (err == cudaSuccess) err = cudaStreamWaitEvent(st->down, st->done[blk], 0);
     if (err == cudaSuccess)
-      err = cudaMemcpy2DAsync(c + i0 * ldc, ldc * 8, dc + i0 * ldc, ldc * 8, n * 8, mk,
+      err = cudaMemcpy2DAsync(c + i0 * ldc + j0, ldc * 8, dck, ldc * 8, nk * 8, mk,
                               cudaMemcpyDeviceToHost, st->down);
+    ++done_blocks;
   }
   // every stream drained before the staging buffer can be reused
   const cudaError_t e1 = cudaStreamSynchronize(st->copy);
   const cudaError_t e2 = cudaStreamSynchronize(st->stream);
   const cudaError_t e3 = cudaStreamSynchronize(st->down);
   if (err == cudaSuccess) err = e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3);
-  if (err != cudaSuccess) return cuda_fail(err, "row-blocked GEMM");
+  if (err != cudaSuccess) return cuda_fail(err, "blocked host GEMM");
   return check_device_waits();
 }
 
@@ -353,7 +374,7 @@ int gemm_host(double* c, size_t c_len, const double* a, size_t a_len, const doub
   double* db = reinterpret_cast<double*>(base + ob);
   double* dc = reinterpret_cast<double*>(base + oc);
   uint8_t* dt = masked ? reinterpret_cast<uint8_t*>(base + ot) : nullptr;
-  if (!masked && ex.c * 8 >= (size_t(64) << 20) && m >= 512)
+  if (!masked && ex.c * 8 >= (size_t(64) << 20) && (split ? m : n) >= 512)
     return gemm_host_blocked(st, c, a, b, m, n, k, lda, ldb, ldc, transa != 0, transb != 0, split,
                              nmod, da, db, dc, base + ows);
   CFGMM_CUDA(cudaMemcpyAsync(da, a, ex.a * 8, cudaMemcpyHostToDevice, st->stream));

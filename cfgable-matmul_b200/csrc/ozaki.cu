@@ -533,14 +533,15 @@ cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int 
                         size_t lda, size_t ldb, size_t ldc, bool transa, bool transb, int nmod,
                         void* workspace, cudaStream_t stream, const cudaEvent_t* events,
                         const uint8_t* tab, size_t ldtab, int blk, cudaEvent_t c_ready,
-                        int m_layout, bool reuse_b) {
+                        int m_layout, int n_layout, bool reuse_a, bool reuse_b) {
   if (tab && transb) return cudaErrorInvalidValue;  // the masked GEMM has no transb
   if (m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
   auto mark = [&](int i) { if (events) cudaEventRecord(events[i], stream); };
   if (k > kOzakiMaxK) return cudaErrorInvalidValue;
   const OzakiPlan plan = ozaki_plan(k, nmod, 0);
   if (m_layout < m) m_layout = m;
-  const DgemmLayout L = dgemm_layout(m_layout, n, k, plan.nmod);
+  if (n_layout < n) n_layout = n;
+  const DgemmLayout L = dgemm_layout(m_layout, n_layout, k, plan.nmod);
   char* ws = static_cast<char*>(workspace);
   int8_t* a_res = reinterpret_cast<int8_t*>(ws + L.a_res);
   int8_t* b_res = reinterpret_cast<int8_t*>(ws + L.b_res);
@@ -552,9 +553,11 @@ cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int 
   // op(A) rows are i (k contiguous unless transa); op(B) "rows" are j
   // (k contiguous only when transb).
   int* emax = reinterpret_cast<int*>(ws + L.emax);
-  cudaError_t err =
-      prepare(a, lda, !transa, m, k, L.kpad, plan.alpha, emax, ea, a_res, ra, stream);
-  if (err != cudaSuccess) return err;
+  cudaError_t err = cudaSuccess;
+  if (!reuse_a) {
+    err = prepare(a, lda, !transa, m, k, L.kpad, plan.alpha, emax, ea, a_res, ra, stream);
+    if (err != cudaSuccess) return err;
+  }
   if (!reuse_b) {
     err = prepare(b, ldb, transb, n, k, L.kpad, plan.beta, emax, eb, b_res, ra, stream,
                   Mask{tab, ldtab, blk > 0 ? blk : 1});

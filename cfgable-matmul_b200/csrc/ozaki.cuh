@@ -49,15 +49,17 @@ size_t ozaki_dgemm_workspace(int m, int n, int k, int nmod);
 // only when tab[p * ldtab + j / blk] != 0.  C is first read by the
 // reconstruction: when `c_ready` is given the stream waits for it just before,
 // so that C may still be arriving while the residues and the INT8 GEMM run.
-// Row blocks of one product: every call lays the workspace out for
-// `m_layout` rows (>= m; 0: m), so that a call with `reuse_b` takes the
-// residues and column exponents of B that an earlier call on the same stream,
-// workspace, B, n, k and nmod left there instead of forming them again.
+// Blocks of one product: every call lays the workspace out for `m_layout`
+// rows and `n_layout` columns (>= m, n; 0: m, n), so that a call with
+// `reuse_a` (`reuse_b`) takes the residues and exponents of A (B) that an
+// earlier call on the same stream, workspace, A (B), k and nmod left there
+// instead of forming them again.
 cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int n, int k,
                         size_t lda, size_t ldb, size_t ldc, bool transa, bool transb, int nmod,
                         void* workspace, cudaStream_t stream,
                         const cudaEvent_t* events = nullptr, const uint8_t* tab = nullptr,
                         size_t ldtab = 0, int blk = 1, cudaEvent_t c_ready = nullptr,
-                        int m_layout = 0, bool reuse_b = false);
+                        int m_layout = 0, int n_layout = 0, bool reuse_a = false,
+                        bool reuse_b = false);
 
 }  // namespace cfgmm

@@ -117,8 +117,8 @@ def test_split_full_size_sampled(cm, wl, ta, tb):
 
 @pytest.mark.parametrize("ta,tb", [(False, False), (True, False), (False, True), (True, True)])
 @pytest.mark.parametrize("prec", [0, 1])
-def test_large_host_call_in_row_blocks(cm, ta, tb, prec):
-    """A host-pointer call with C above 64 MB runs in blocks of rows whose
+def test_large_host_call_in_blocks(cm, ta, tb, prec):
+    """A host-pointer call with C above 64 MB runs in blocks of columns whose
     transfers overlap the work: accumulation into a nonzero C, odd lda/ldc, and
     (split precision) the same bits as one device-pointer call."""
     import torch
