@@ -71,8 +71,8 @@ bool fits_int(size_t v) { return v <= size_t(INT_MAX) - 4096; }
 // ---------------------------------------------------------------------------
 // per-device state for the host-pointer entry points
 // ---------------------------------------------------------------------------
-// Blocks of a large host-pointer GEMM (see gemm_host_blocked).
-constexpr size_t kHostBlocks = 4;
+// Most blocks of a large host-pointer GEMM (see gemm_host_blocked).
+constexpr size_t kHostBlocks = 8;
 
 struct DeviceState {
   std::mutex mu;
@@ -263,13 +263,13 @@ int check_mask(const GemmMask& mk, size_t n, size_t k, uint8_t transb, size_t* t
 // carries both directions at once): one operand goes up whole first, then each
 // block's part of the other operand and of C go up on the copy stream, the
 // block is computed on the compute stream and its part of C comes back on the
-// download stream.  The blocks shrink (34, 28, 22, 16 %): the last block's work
-// and download, which nothing overlaps, are the smallest.  In split precision
-// the blocks are rows of C and op(A), B goes up first and its residues are
-// formed once (the transfers bound the call, and whole rows copy fastest); in
-// FP64 they are columns of C and op(B) and A goes up first (186 MB instead of
-// 505 MB at the headline shape, so the work, which bounds that call, starts
-// sooner).  The device buffers keep the host layouts; every element of C is
+// download stream.  In split precision the transfers bound the call: 4 blocks
+// of rows of C and op(A) that shrink (34, 28, 22, 16 %), so that the last
+// block's work and download, which nothing overlaps, are the smallest; B goes
+// up first and its residues are formed once.  In FP64 the work bounds the
+// call: 8 equal blocks of columns of C and op(B), A going up first (186 MB
+// instead of 505 MB at the headline shape), so that the work starts early and
+// each block's upload takes about as long as the previous block's work.  The device buffers keep the host layouts; every element of C is
 // computed from the same row of op(A) and column of op(B) as in one call.
 int gemm_host_blocked(DeviceState* st, double* c, const double* a, const double* b, size_t m,
                       size_t n, size_t k, size_t lda, size_t ldb, size_t ldc, bool transa,
@@ -279,13 +279,14 @@ int gemm_host_blocked(DeviceState* st, double* c, const double* a, const double*
   if (rc != CFGMM_OK) return rc;
   const bool by_rows = split;
   const size_t extent = by_rows ? m : n;
-  static constexpr double kShare[kHostBlocks] = {0.34, 0.28, 0.22, 0.16};
+  static constexpr double kSplitShare[4] = {0.34, 0.28, 0.22, 0.16};
+  const size_t nblocks = by_rows ? 4 : kHostBlocks;
   size_t bound[kHostBlocks + 1] = {0};
   double acc = 0.0;
-  for (size_t i = 0; i < kHostBlocks; ++i) {
-    acc += kShare[i];
+  for (size_t i = 0; i < nblocks; ++i) {
+    acc += by_rows ? kSplitShare[i] : 1.0 / double(nblocks);
     bound[i + 1] =
-        i + 1 == kHostBlocks ? extent : std::min(extent, size_t(acc * double(extent) + 0.5));
+        i + 1 == nblocks ? extent : std::min(extent, size_t(acc * double(extent) + 0.5));
   }
   const size_t ea = transa ? (k - 1) * lda + m : (m - 1) * lda + k;
   const size_t eb = transb ? (n - 1) * ldb + k : (k - 1) * ldb + n;
@@ -295,7 +296,7 @@ int gemm_host_blocked(DeviceState* st, double* c, const double* a, const double*
     err = by_rows ? cudaMemcpyAsync(db, b, eb * 8, cudaMemcpyHostToDevice, st->copy)
                   : cudaMemcpyAsync(da, a, ea * 8, cudaMemcpyHostToDevice, st->copy);
   size_t done_blocks = 0;
-  for (size_t blk = 0; err == cudaSuccess && blk < kHostBlocks; ++blk) {
+  for (size_t blk = 0; err == cudaSuccess && blk < nblocks; ++blk) {
     const size_t x0 = bound[blk], xk = bound[blk + 1] - x0;
     if (xk == 0) continue;
     // the block of C: rows x0.. (by_rows) or columns x0..; pointers into the
