@@ -263,8 +263,8 @@ int check_mask(const GemmMask& mk, size_t n, size_t k, uint8_t transb, size_t* t
 // carries both directions at once): one operand goes up whole first, then each
 // block's part of the other operand and of C go up on the copy stream, the
 // block is computed on the compute stream and its part of C comes back on the
-// download stream.  In split precision the transfers bound the call: 4 blocks
-// of rows of C and op(A) that shrink (34, 28, 22, 16 %), so that the last
+// download stream.  In split precision the transfers bound the call: 5 blocks
+// of rows of C and op(A) that shrink (30, 25, 20, 15, 10 %), so that the last
 // block's work and download, which nothing overlaps, are the smallest; B goes
 // up first and its residues are formed once.  In FP64 the work bounds the
 // call: 8 equal blocks of columns of C and op(B), A going up first (186 MB
@@ -279,8 +279,8 @@ int gemm_host_blocked(DeviceState* st, double* c, const double* a, const double*
   if (rc != CFGMM_OK) return rc;
   const bool by_rows = split;
   const size_t extent = by_rows ? m : n;
-  static constexpr double kSplitShare[4] = {0.34, 0.28, 0.22, 0.16};
-  const size_t nblocks = by_rows ? 4 : kHostBlocks;
+  static constexpr double kSplitShare[5] = {0.30, 0.25, 0.20, 0.15, 0.10};
+  const size_t nblocks = by_rows ? 5 : kHostBlocks;
   size_t bound[kHostBlocks + 1] = {0};
   double acc = 0.0;
   for (size_t i = 0; i < nblocks; ++i) {
