@@ -655,6 +655,39 @@ def run_ours(args, ranks: Ranks):
                                                            "28 INT8 products",
                       "launches_per_step": 8},
             "speedup_split_vs_fp64": atot / stot}
+    # the drop-in host-pointer call (cfgmm_aodmao2rho_ex, aodmao2rho_loop_parallel's
+    # form) end to end on pinned host buffers: phi, D and the mask up, rho up and back
+    hao = torch.from_numpy(p.ao).pin_memory()
+    hdm = torch.from_numpy(p.dms).pin_memory()
+    htab = torch.from_numpy(p.tab).pin_memory()
+    hrho = torch.zeros(p.nset, p.ngrid, dtype=torch.float64).pin_memory()
+
+    def aodm_e2e(precision):
+        def step():
+            rc = lib.cfgmm_aodmao2rho_ex(hrho.data_ptr(), hrho.numel(), hdm.data_ptr(), hdm.numel(),
+                                         hao.data_ptr(), hao.numel(), hao.data_ptr(), hao.numel(),
+                                         p.nao, p.ngrid, p.nao, p.ngrid, p.nset, htab.data_ptr(),
+                                         htab.numel(), p.nblk, p.blksize, precision)
+            if rc != 0:
+                cm._raise(rc)
+        for _ in range(max(1, args.warmup)):
+            step()
+        ranks.barrier()
+        ts = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            step()
+            ts.append(time.perf_counter() - t0)
+        return ranks.max(sum(ts)) / args.steps * 1e3
+    h2d = (hao.numel() + hdm.numel() + hrho.numel()) * 8 + htab.numel()
+    for name, prec in (("fp64", FP64), ("split", SPLIT)):
+        ms = aodm_e2e(prec)
+        aodm[name]["e2e"] = {"value": ranks.world * aflops / (ms * 1e-3) / 1e9, "unit": "GFLOP/s",
+                             "ms_per_step": ms, "h2d_bytes_per_step": h2d,
+                             "d2h_bytes_per_step": hrho.numel() * 8,
+                             "path": "cfgmm_aodmao2rho_ex on pinned host buffers (synchronous)"}
+    lib.cfgmm_release_workspace()
+    del hao, hdm, htab, hrho
     if ranks.rank == 0 and ranks.world == 1 and not args.no_cpu:
         aodm["cpu_baseline"] = cpu_aodm_run(p)
     del ao, dms, tab, rho, r64, rsp

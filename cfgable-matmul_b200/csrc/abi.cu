@@ -458,6 +458,78 @@ int check_aodm(const void* rhos, size_t rhos_len, const void* dms, size_t dms_le
   return CFGMM_OK;
 }
 
+// The status of a finished AO-DM-AO run: a timed-out pipeline wait of either kernel family.
+int aodm_device_status(bool split) {
+  if (split) return check_device_waits();
+  int code = 0;
+  CFGMM_CUDA(cfgmm::aodm_read_error(&code));
+  if (code != 0) {
+    char msg[128];
+    std::snprintf(msg, sizeof(msg), "a pipeline wait of the FP64 kernel timed out (code %d)", code);
+    return fail(CFGMM_ERR_TIMEOUT, msg);
+  }
+  return CFGMM_OK;
+}
+
+// A host-pointer AO-DM-AO contraction whose phi tables exceed 64 MB, in 4
+// blocks of whole grid blocks so that the PCIe transfers of one block overlap
+// the work and the transfers of the others: D, the mask and rho go up first,
+// then each block's columns of phi go up on the copy stream, the block is
+// contracted on the compute stream and its columns of rho come back on the
+// download stream.  Every grid block is contracted exactly as in one call (its
+// rho depends only on its own phi columns, D and its mask column).
+int aodm_host_blocked(DeviceState* st, double* rhos, const double* dms, const double* ao_lhs,
+                      const double* ao_rhs, size_t stride_ao, size_t stride_grid, size_t nao,
+                      size_t ngrid, size_t nset, const uint8_t* tab, size_t ldtab,
+                      size_t blksize, bool split, const AodmExtents& ex, double* d_dms,
+                      double* d_lhs, double* d_rhs, uint8_t* d_tab, double* d_rho, void* ws) {
+  int rc = ensure_block_pipeline(st);
+  if (rc != CFGMM_OK) return rc;
+  constexpr size_t kBlocks = 4;
+  const size_t nblk = (ngrid + blksize - 1) / blksize;
+  size_t bound[kBlocks + 1] = {0};
+  for (size_t i = 1; i <= kBlocks; ++i) bound[i] = std::min(ngrid, (nblk * i / kBlocks) * blksize);
+  bound[kBlocks] = ngrid;
+  const bool same_ao = d_lhs == d_rhs;
+  cudaError_t err = split ? cfgmm::aodmao2rho_split_reset_error(st->stream) : cudaSuccess;
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(d_dms, dms, ex.dms * 8, cudaMemcpyHostToDevice, st->copy);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(d_tab, tab, ex.tab, cudaMemcpyHostToDevice, st->copy);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(d_rho, rhos, ex.rhos * 8, cudaMemcpyHostToDevice, st->copy);
+  for (size_t blk = 0; err == cudaSuccess && blk < kBlocks; ++blk) {
+    const size_t g0 = bound[blk], gk = bound[blk + 1] - g0;
+    if (gk == 0) continue;
+    err = cudaMemcpy2DAsync(d_lhs + g0, stride_grid * 8, ao_lhs + g0, stride_grid * 8, gk * 8, nao,
+                            cudaMemcpyHostToDevice, st->copy);
+    if (err == cudaSuccess && !same_ao)
+      err = cudaMemcpy2DAsync(d_rhs + g0, stride_grid * 8, ao_rhs + g0, stride_grid * 8, gk * 8,
+                              nao, cudaMemcpyHostToDevice, st->copy);
+    if (err == cudaSuccess) err = cudaEventRecord(st->up[blk], st->copy);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(st->stream, st->up[blk], 0);
+    const size_t b0 = g0 / blksize;
+    if (err == cudaSuccess)
+      err = split ? cfgmm::aodmao2rho_split(d_rho + g0, d_dms, d_lhs + g0, d_rhs + g0, stride_ao,
+                                            stride_grid, int(nao), int(gk), int(nset), d_tab + b0,
+                                            ldtab, int(blksize), ws, st->stream)
+                  : cfgmm::aodmao2rho_fp64(d_rho + g0, d_dms, d_lhs + g0, d_rhs + g0, stride_ao,
+                                           stride_grid, int(nao), int(gk), int(nset), d_tab + b0,
+                                           ldtab, int(blksize), ws, st->stream);
+    if (err == cudaSuccess) err = cudaEventRecord(st->done[blk], st->stream);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(st->down, st->done[blk], 0);
+    if (err == cudaSuccess)
+      err = cudaMemcpy2DAsync(rhos + g0, stride_grid * 8, d_rho + g0, stride_grid * 8, gk * 8, nset,
+                              cudaMemcpyDeviceToHost, st->down);
+  }
+  // every stream drained before the staging buffer can be reused
+  const cudaError_t e1 = cudaStreamSynchronize(st->copy);
+  const cudaError_t e2 = cudaStreamSynchronize(st->stream);
+  const cudaError_t e3 = cudaStreamSynchronize(st->down);
+  if (err == cudaSuccess) err = e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3);
+  if (err != cudaSuccess) return cuda_fail(err, "blocked AO-DM-AO");
+  return aodm_device_status(split);
+}
+
 int aodm_host(double* rhos, size_t rhos_len, const double* dms, size_t dms_len,
               const double* ao_lhs, size_t ao_lhs_len, const double* ao_rhs, size_t ao_rhs_len,
               size_t stride_ao, size_t stride_grid, size_t nao, size_t ngrid, size_t nset,
@@ -493,6 +565,10 @@ int aodm_host(double* rhos, size_t rhos_len, const double* dms, size_t dms_len,
   double* d_rhs = reinterpret_cast<double*>(base + o_rhs);
   uint8_t* d_tab = reinterpret_cast<uint8_t*>(base + o_tab);
   double* d_rho = reinterpret_cast<double*>(base + o_rho);
+  if (ex.ao * 8 >= (size_t(64) << 20) && ngrid >= 4 * blksize)
+    return aodm_host_blocked(st, rhos, dms, ao_lhs, ao_rhs, stride_ao, stride_grid, nao, ngrid,
+                             nset, tab, ldtab, blksize, split, ex, d_dms, d_lhs,
+                             same_ao ? d_lhs : d_rhs, d_tab, d_rho, base + o_ws);
   CFGMM_CUDA(cudaMemcpyAsync(d_dms, dms, ex.dms * 8, cudaMemcpyHostToDevice, st->stream));
   CFGMM_CUDA(cudaMemcpyAsync(d_lhs, ao_lhs, ex.ao * 8, cudaMemcpyHostToDevice, st->stream));
   if (!same_ao)

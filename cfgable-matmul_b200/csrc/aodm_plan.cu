@@ -170,6 +170,13 @@ cudaError_t capture(cfgmm_aodm_plan* plan, F body) {
 // The split-precision half of cfgmm_aodm_plan_create: phi digit tiles of
 // every batch are built here once; items are (tile, row tile, matrix, batch),
 // matrix-major (one D in L2 at a time), heaviest first within a matrix.
+// Whether every batch passes one phi array for both sides of the contraction.
+bool same_phi(const cfgmm_aodm_batch* batches, size_t nbatch) {
+  for (size_t i = 0; i < nbatch; ++i)
+    if (batches[i].ao_lhs != batches[i].ao_rhs) return false;
+  return true;
+}
+
 int build_split(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, size_t nbatch,
                 const double* dms, size_t stride_ao, size_t nao, size_t nset_max, size_t blksize,
                 int flags, int* d_lists, int* d_counts, const std::vector<size_t>& list_off,
@@ -294,8 +301,11 @@ int build_split(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, size_t n
   a.blk = int(blksize);
   a.gsub = gsub;
   a.max_ut = max_ut;
-  // total[2]: the asymmetry flag of the symmetric mode
-  a.asym = cfgmm::aodm_sym_enabled() ? reinterpret_cast<const int*>(base + o_total) + 2 : nullptr;
+  // total[2]: the asymmetry flag of the symmetric mode, which also needs every
+  // batch to use one phi array for both sides
+  a.asym = cfgmm::aodm_sym_enabled() && same_phi(batches, nbatch)
+               ? reinterpret_cast<const int*>(base + o_total) + 2
+               : nullptr;
 
   // ---- autotuning: pipeline depth of the persistent kernel ----
   std::string tune = "default";
@@ -535,7 +545,8 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
   a.rhs_maps = pipe_ok ? reinterpret_cast<const CUtensorMap*>(base + o_maps) : nullptr;
   a.items = reinterpret_cast<const int4*>(base + o_items);
   a.counters = reinterpret_cast<int*>(base + o_ctr);
-  const bool sym = pipe_ok && cfgmm::aodm_sym_enabled();
+  // the half contraction needs D = D^T and, in every batch, phi_lhs = phi_rhs
+  const bool sym = pipe_ok && cfgmm::aodm_sym_enabled() && same_phi(batches, nbatch);
   // reset, symmetry check of D, main kernel (the reduction follows in a run)
   auto launch = [&](const cfgmm::AodmConfig& c, cudaStream_t st) -> cudaError_t {
     a.asym = sym && c.tk == 0 ? a.counters + a.ngroups + 1 : nullptr;

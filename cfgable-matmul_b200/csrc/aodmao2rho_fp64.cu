@@ -1027,7 +1027,8 @@ cudaError_t aodmao2rho_fp64(double* rhos, const double* dms, const double* ao_lh
   CUtensorMap map{};
   if (pipe_enabled()) {
     a.one.rhs_tma = aodm_rhs_map(&map, ao_rhs, stride_grid, nao, ngrid, blk) ? 1 : 0;
-    if (aodm_sym_enabled()) {
+    // the half contraction needs D = D^T and phi_lhs = phi_rhs (one array)
+    if (aodm_sym_enabled() && ao_lhs == ao_rhs) {
       a.asym = counters + ngroups + 1;
       if ((err = aodm_launch_sym_check(dms, stride_ao, nao, nset, counters + ngroups + 1,
                                        stream)) != cudaSuccess)

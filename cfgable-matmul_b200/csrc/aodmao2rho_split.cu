@@ -789,7 +789,8 @@ cudaError_t aodmao2rho_split(double* rhos, const double* dms, const double* ao_l
   cudaError_t err = aodm_block_lists_launch(tab, ldtab, nao, nblk, lists, counts, stream);
   if (err != cudaSuccess) return err;
   split_build<<<1, 1024, 0, stream>>>(counts, nbg, gsub, nset, max_ut, cbase, items, total);
-  int* asym = aodm_sym_enabled() ? total + 2 : nullptr;  // total[2]: asymmetry flag
+  // total[2]: asymmetry flag; the half contraction needs D = D^T and phi_lhs = phi_rhs
+  int* asym = aodm_sym_enabled() && ao_lhs == ao_rhs ? total + 2 : nullptr;
   if (asym) {
     if ((err = cudaMemsetAsync(asym, 0, sizeof(int), stream)) != cudaSuccess) return err;
     if ((err = aodm_launch_sym_check(dms, stride_ao, nao, nset, asym, stream)) != cudaSuccess)

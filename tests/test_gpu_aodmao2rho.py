@@ -204,3 +204,55 @@ def test_symmetric_d_mode_and_its_check(cm, oracle, kind, nset):
     cm.aodmao2rho_ex(rho, dms, p.ao, p.ao, *args, blksize=64)
     oracle.aodmao2rho(ref, dms, p.ao, p.ao, *args, 64)
     assert normwise(rho, ref) < TOL
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_large_host_call_in_blocks(cm, oracle, prec):
+    """A host-pointer call whose phi table exceeds 64 MB runs in blocks of grid
+    blocks whose transfers overlap the work: the same bits as one
+    device-pointer call (each grid block is contracted alike), accumulation
+    into a nonzero rho, padded strides, phi_lhs != phi_rhs, and the oracle's
+    result within the parity tolerance."""
+    import torch
+    nao, ngrid, nset, blk = 1100, 8000, 2, 64
+    sa, sg = nao + 3, ngrid + 5
+    rng = np.random.default_rng(77 + prec)
+    nblk = -(-ngrid // blk)
+    tab = (rng.random((nao, nblk + 1)) < 0.35).astype(np.uint8)
+    lhs = rng.standard_normal((nao, sg))
+    rhs = rng.standard_normal((nao, sg))
+    a = rng.uniform(-1, 1, (nset, sa, sa))
+    dms = np.ascontiguousarray(0.5 * (a + a.transpose(0, 2, 1)))
+    rho0 = rng.uniform(-1, 1, (nset, sg))
+    rho = rho0.copy()
+    cm.aodmao2rho_ex(rho, dms, lhs, rhs, (sa, sg), (nao, ngrid), nset, tab, tab.shape[1], blk, prec)
+    d = {k: torch.from_numpy(np.ascontiguousarray(x)).cuda()
+         for k, x in dict(rho=rho0, dms=dms, lhs=lhs, rhs=rhs, tab=tab).items()}
+    cm.aodmao2rho_ex(d["rho"], d["dms"], d["lhs"], d["rhs"], (sa, sg), (nao, ngrid), nset, d["tab"],
+                     tab.shape[1], blk, prec)
+    torch.cuda.synchronize()
+    assert np.array_equal(d["rho"].cpu().numpy(), rho)
+    ref = rho0.copy()
+    oracle.aodmao2rho(ref, dms, lhs, rhs, (sa, sg), (nao, ngrid), nset, tab, tab.shape[1], blk)
+    assert normwise(rho, ref) < (1e-12 if prec else 1e-13)
+    assert np.array_equal(rho[:, ngrid:], rho0[:, ngrid:])  # padding of rho untouched
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_symmetric_d_with_two_phi_arrays(cm, oracle, prec):
+    """A symmetric D with phi_lhs != phi_rhs: the half contraction of the
+    symmetric mode does not apply (it needs one phi array for both sides), so
+    the full contraction runs; checked against the oracle."""
+    nao, ngrid, nset, blk = 300, 2000, 2, 64
+    rng = np.random.default_rng(91 + prec)
+    nblk = -(-ngrid // blk)
+    tab = (rng.random((nao, nblk)) < 0.4).astype(np.uint8)
+    lhs = rng.standard_normal((nao, ngrid))
+    rhs = rng.standard_normal((nao, ngrid))
+    a = rng.uniform(-1, 1, (nset, nao, nao))
+    dms = np.ascontiguousarray(0.5 * (a + a.transpose(0, 2, 1)))
+    rho = np.zeros((nset, ngrid))
+    ref = rho.copy()
+    cm.aodmao2rho_ex(rho, dms, lhs, rhs, (nao, ngrid), (nao, ngrid), nset, tab, nblk, blk, prec)
+    oracle.aodmao2rho(ref, dms, lhs, rhs, (nao, ngrid), (nao, ngrid), nset, tab, nblk, blk)
+    assert normwise(rho, ref) < (1e-12 if prec else 1e-13)

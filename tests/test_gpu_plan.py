@@ -174,3 +174,20 @@ def test_plan_rejections(cm, wl):
     bad = [(d[0], d[1], d[2], d[3], 3) for d in dev]  # nset above nset_max
     with pytest.raises(ValueError):
         cm.AodmPlan(bad, ddms)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_plan_symmetric_d_with_two_phi_arrays(cm, wl, precision):
+    """Plans over batches whose phi_lhs and phi_rhs differ, with a symmetric D:
+    the full contraction runs (the half one needs one phi array per batch), so
+    the plan matches the single calls."""
+    import torch
+    bs, dms = _batches(wl, torch, 5, 9)
+    dms = np.ascontiguousarray(0.5 * (dms + dms.transpose(0, 2, 1)))
+    dev, ddms = _device(torch, bs, dms)
+    plan = cm.AodmPlan(dev, ddms, blksize=64, precision=precision, graph=False, tune=False)
+    plan.run()
+    torch.cuda.synchronize()
+    for b, d in zip(bs, dev):
+        assert normwise(d[0].cpu().numpy(), _single(cm, torch, b, dms, 64, precision)) < 1e-12
+    plan.close()
