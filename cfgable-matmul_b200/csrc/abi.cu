@@ -263,7 +263,8 @@ int check_mask(const GemmMask& mk, size_t n, size_t k, uint8_t transb, size_t* t
 // carries both directions at once): one operand goes up whole first, then each
 // block's part of the other operand and of C go up on the copy stream, the
 // block is computed on the compute stream and its part of C comes back on the
-// download stream.  In split precision the transfers bound the call: 5 blocks
+// download stream.  In split precision, and for the masked GEMM (its mask runs
+// along the columns of B and goes up whole), the transfers bound the call: 5 blocks
 // of rows of C and op(A) that shrink (30, 25, 20, 15, 10 %), so that the last
 // block's work and download, which nothing overlaps, are the smallest; B goes
 // up first and its residues are formed once.  In FP64 the work bounds the
@@ -274,10 +275,10 @@ int check_mask(const GemmMask& mk, size_t n, size_t k, uint8_t transb, size_t* t
 int gemm_host_blocked(DeviceState* st, double* c, const double* a, const double* b, size_t m,
                       size_t n, size_t k, size_t lda, size_t ldb, size_t ldc, bool transa,
                       bool transb, bool split, int nmod, double* da, double* db, double* dc,
-                      void* ws) {
+                      void* ws, bool by_rows, const uint8_t* tab, uint8_t* dt, size_t tab_ext,
+                      size_t ldtab, size_t blk_mask) {
   int rc = ensure_block_pipeline(st);
   if (rc != CFGMM_OK) return rc;
-  const bool by_rows = split;
   const size_t extent = by_rows ? m : n;
   static constexpr double kSplitShare[5] = {0.30, 0.25, 0.20, 0.15, 0.10};
   const size_t nblocks = by_rows ? 5 : kHostBlocks;
@@ -295,6 +296,8 @@ int gemm_host_blocked(DeviceState* st, double* c, const double* a, const double*
   if (err == cudaSuccess)
     err = by_rows ? cudaMemcpyAsync(db, b, eb * 8, cudaMemcpyHostToDevice, st->copy)
                   : cudaMemcpyAsync(da, a, ea * 8, cudaMemcpyHostToDevice, st->copy);
+  if (err == cudaSuccess && dt)  // the mask of the masked GEMM, whole
+    err = cudaMemcpyAsync(dt, tab, tab_ext, cudaMemcpyHostToDevice, st->copy);
   size_t done_blocks = 0;
   for (size_t blk = 0; err == cudaSuccess && blk < nblocks; ++blk) {
     const size_t x0 = bound[blk], xk = bound[blk + 1] - x0;
@@ -323,10 +326,13 @@ int gemm_host_blocked(DeviceState* st, double* c, const double* a, const double*
     const double* dbk = transb ? db + j0 * ldb : db + j0;
     if (err == cudaSuccess)
       err = split ? cfgmm::ozaki_dgemm(dck, dak, dbk, int(mk), int(nk), int(k), lda, ldb, ldc,
-                                       transa, transb, nmod, ws, st->stream, nullptr, nullptr, 0,
-                                       1, nullptr, int(m), int(n), false, done_blocks > 0)
-                  : cfgmm::dgemm_fp64(dck, dak, dbk, int(mk), int(nk), int(k), lda, ldb, ldc,
-                                      transa, transb, st->stream);
+                                       transa, transb, nmod, ws, st->stream, nullptr, dt, ldtab,
+                                       int(blk_mask), nullptr, int(m), int(n), false,
+                                       done_blocks > 0)
+            : dt ? cfgmm::dgemm_fp64_non0tab(dck, dak, dbk, int(mk), int(nk), int(k), lda, ldb,
+                                             ldc, transa, dt, ldtab, int(blk_mask), st->stream)
+                 : cfgmm::dgemm_fp64(dck, dak, dbk, int(mk), int(nk), int(k), lda, ldb, ldc,
+                                     transa, transb, st->stream);
     if (err == cudaSuccess) err = cudaEventRecord(st->done[blk], st->stream);
     if (err == cudaSuccess) err = cudaStreamWaitEvent(st->down, st->done[blk], 0);
     if (err == cudaSuccess)
@@ -375,9 +381,13 @@ int gemm_host(double* c, size_t c_len, const double* a, size_t a_len, const doub
   double* db = reinterpret_cast<double*>(base + ob);
   double* dc = reinterpret_cast<double*>(base + oc);
   uint8_t* dt = masked ? reinterpret_cast<uint8_t*>(base + ot) : nullptr;
-  if (!masked && ex.c * 8 >= (size_t(64) << 20) && (split ? m : n) >= 512)
+  // masked products block by rows (the mask runs along B's columns and is
+  // needed whole); unmasked FP64 ones by columns
+  const bool by_rows = split || masked;
+  if (ex.c * 8 >= (size_t(64) << 20) && (by_rows ? m : n) >= 512)
     return gemm_host_blocked(st, c, a, b, m, n, k, lda, ldb, ldc, transa != 0, transb != 0, split,
-                             nmod, da, db, dc, base + ows);
+                             nmod, da, db, dc, base + ows, by_rows, mk.tab, dt, tab_ext,
+                             mk.ldtab, mk.blk);
   CFGMM_CUDA(cudaMemcpyAsync(da, a, ex.a * 8, cudaMemcpyHostToDevice, st->stream));
   CFGMM_CUDA(cudaMemcpyAsync(db, b, ex.b * 8, cudaMemcpyHostToDevice, st->stream));
   if (masked) CFGMM_CUDA(cudaMemcpyAsync(dt, mk.tab, tab_ext, cudaMemcpyHostToDevice, st->stream));

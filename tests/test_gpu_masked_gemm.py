@@ -86,3 +86,33 @@ def test_non0tab_device_pointers(cm):
     mask = tab.cpu().numpy().astype(bool).repeat(blk, axis=1)
     ref = a.cpu().numpy() @ np.where(mask, b.cpu().numpy(), 0.0)
     assert normwise(c.cpu().numpy(), ref) < TOL
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_large_masked_host_call_in_blocks(cm, wl, prec):
+    """A host-pointer masked GEMM with C above 64 MB runs in blocks of rows
+    whose transfers overlap the work: accumulation into a nonzero C, odd
+    lda/ldc, the mask whole on the device; (split precision) the same bits as
+    one device-pointer call, and within the parity bar of FP64 numpy."""
+    import torch
+    m, n, k, blk = 1100, 8000, 600, 48
+    lda, ldc = k + 5, n + 3
+    rng = np.random.default_rng(60 + prec)
+    a = rng.uniform(-1, 1, (m, lda))
+    b = rng.uniform(-1, 1, (k, n))
+    nblk = -(-n // blk)
+    tab = (rng.random((k, nblk)) < 0.3).astype(np.uint8)
+    c0 = rng.uniform(-1, 1, (m, ldc))
+    c = c0.copy()
+    cm.matmul_non0tab_ex(c, a, b, m, n, k, lda, n, ldc, False, False, tab, nblk, blk, prec)
+    bm = np.where(wl.expand_mask(tab, n, blk), b, 0.0)
+    ref = c0[:, :n] + a[:, :k] @ bm
+    assert normwise(c[:, :n], ref) < (1e-12 if prec else 1e-13)
+    assert np.array_equal(c[:, n:], c0[:, n:])
+    if prec:
+        dc = torch.from_numpy(c0.copy()).cuda()
+        cm.matmul_non0tab_ex(dc, torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda(), m, n, k,
+                             lda, n, ldc, False, False, torch.from_numpy(tab).cuda(), nblk, blk,
+                             prec)
+        torch.cuda.synchronize()
+        assert np.array_equal(dc.cpu().numpy(), c)
