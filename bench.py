@@ -351,6 +351,34 @@ def next_rows_section(args, cm, wl, stream, p):
     torch.cuda.synchronize()
     res["masked_gemm"]["split"]["error_vs_fp64"] = float((csp - c64).abs().max() / c64.abs().max())
     del da, db, dtab, c64, csp
+    torch.cuda.empty_cache()
+
+    # the host-pointer call (cfgmm_matmul_non0tab_ex) end to end on pinned buffers:
+    # A, B, C and the mask up, C back (row blocks overlap the copies above 64 MB of C)
+    ha, hb = torch.from_numpy(a).pin_memory(), torch.from_numpy(b).pin_memory()
+    htab = torch.from_numpy(np.ascontiguousarray(tab)).pin_memory()
+    hc = torch.zeros(m, n, dtype=torch.float64).pin_memory()
+    lib = cm.lib()
+    for name, prec in (("fp64", cm.PREC_FP64), ("split", cm.PREC_OZAKI_INT8)):
+        def step():
+            rc = lib.cfgmm_matmul_non0tab_ex(hc.data_ptr(), hc.numel(), ha.data_ptr(), ha.numel(),
+                                             hb.data_ptr(), hb.numel(), m, n, k, lda, ldb, n, 0,
+                                             0, htab.data_ptr(), htab.numel(), nblk, blk, prec)
+            if rc != 0:
+                cm._raise(rc)
+        for _ in range(max(1, args.warmup)):
+            step()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step()
+        ms = (time.perf_counter() - t0) / args.steps * 1e3
+        res["masked_gemm"][name]["e2e"] = {
+            "ms_per_call": ms, "masked_tflops": 2.0 * m * active / (ms * 1e-3) / 1e12,
+            "h2d_bytes_per_step": (ha.numel() + hb.numel() + hc.numel()) * 8 + htab.numel(),
+            "d2h_bytes_per_step": hc.numel() * 8,
+            "path": "cfgmm_matmul_non0tab_ex on pinned host buffers (synchronous)"}
+    lib.cfgmm_release_workspace()
+    del ha, hb, htab, hc
 
     ao = torch.from_numpy(p.ao).cuda()
     ptab = torch.from_numpy(p.tab).cuda()
@@ -366,7 +394,32 @@ def next_rows_section(args, cm, wl, stream, p):
                    "ms_per_call": ms, "flops_per_call": fflops,
                    "tflops": fflops / (ms * 1e-3) / 1e12,
                    "form": "compacted AO lists, symmetric pairs formed once, FP64 atomics into V"}
-    del ao, ptab, w, v
+    # end to end through the host-pointer call on pinned buffers: phi, w, V and the
+    # mask up, V back
+    hao, hw = torch.from_numpy(p.ao).pin_memory(), w.cpu().pin_memory()
+    htab = torch.from_numpy(np.ascontiguousarray(p.tab)).pin_memory()
+    hv = torch.zeros(p.nset, p.nao, p.nao, dtype=torch.float64).pin_memory()
+
+    def fock_step():
+        rc = lib.cfgmm_aodm_fock(hv.data_ptr(), hv.numel(), hw.data_ptr(), hw.numel(),
+                                 hao.data_ptr(), hao.numel(), hao.data_ptr(), hao.numel(), p.nao,
+                                 p.ngrid, p.nao, p.ngrid, p.nset, htab.data_ptr(), htab.numel(),
+                                 p.nblk, p.blksize)
+        if rc != 0:
+            cm._raise(rc)
+    for _ in range(max(1, args.warmup)):
+        fock_step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        fock_step()
+    ms = (time.perf_counter() - t0) / args.steps * 1e3
+    res["fock"]["e2e"] = {"ms_per_call": ms, "tflops": fflops / (ms * 1e-3) / 1e12,
+                          "h2d_bytes_per_step": (hao.numel() + hw.numel() + hv.numel()) * 8
+                          + htab.numel(),
+                          "d2h_bytes_per_step": hv.numel() * 8,
+                          "path": "cfgmm_aodm_fock on pinned host buffers (synchronous)"}
+    lib.cfgmm_release_workspace()
+    del ao, ptab, w, v, hao, hw, htab, hv
     torch.cuda.empty_cache()
     return res
 
