@@ -26,6 +26,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
+#include <cstring>
 #include <mutex>
 
 #include "gemm_i8.cuh"
@@ -206,14 +207,14 @@ __global__ void finalize_exps(const int* __restrict__ emax, int rows, int bits, 
 // bits.  Two elements go through each packed FP32x2 instruction (sm_100).
 // Modulus 256 is the low byte of v's two's complement.
 // ---------------------------------------------------------------------------
+using f32x2 = unsigned long long;  // two FP32 lanes in a 64-bit register
+
+// Per modulus l (index 0 is 256, taken from the low byte): c_14, c_28, c_42,
+// 1/m and -m, each in both lanes of an FP32x2 word.
 struct ResidueArgs {
   int nmod;
-  int mod[kMaxModuli];
-  float inv[kMaxModuli];
-  float c14[kMaxModuli], c28[kMaxModuli], c42[kMaxModuli];
+  f32x2 c14[kMaxModuli], c28[kMaxModuli], c42[kMaxModuli], inv[kMaxModuli], nm[kMaxModuli];
 };
-
-using f32x2 = unsigned long long;  // two FP32 lanes in a 64-bit register
 
 __device__ __forceinline__ f32x2 pack2(float lo, float hi) {
   f32x2 r;
@@ -244,13 +245,37 @@ __device__ __forceinline__ double scaled_int(double x, int e) {
   return rint(ldexp(x, e));
 }
 
-// The residues of 8 consecutive elements v[0..7] (integers, |v| <= 2^52) for
-// every modulus, 8 bytes per modulus plane at Y + l * plane + off (8-byte
-// aligned).
+constexpr long long kDigitBias = 8192LL * (1 + (1LL << 14) + (1LL << 28));
+// 1.5 2^52 + kDigitBias: for an integer v with |v| <= 2^50, v + kRoundBias lies in
+// [2^52, 2^53), where the spacing of doubles is 1, so its mantissa field holds
+// w + 2^51 (w = v + kDigitBias) and the rounding that forms it is rint(v).
+constexpr double kRoundBias = 6755399441055744.0 + double(kDigitBias);
+
+// The operand element x(r, p) 2^e as the input of write_residues8: rint(x 2^e)
+// (the plain form), or that integer plus kRoundBias, rounded once by the FMA
+// (the biased form, for |x 2^e| < 2^50).  e = kNonFinite gives 0.
+template <bool kBiased>
+__device__ __forceinline__ double scaled(double x, int e) {
+  if constexpr (kBiased) {
+    if (e == kNonFinite) return kRoundBias;
+    if (e >= -1022 && e <= 1023)
+      return fma(x, __longlong_as_double(static_cast<long long>(e + 1023) << 52), kRoundBias);
+    return rint(ldexp(x, e)) + kRoundBias;
+  } else {
+    return scaled_int(x, e);
+  }
+}
+template <bool kBiased>
+__device__ __forceinline__ double scaled_zero() { return kBiased ? kRoundBias : 0.0; }
+
+// The residues of 8 consecutive elements for every modulus, 8 bytes per modulus
+// plane at Y + l * plane + off (8-byte aligned).  v[] holds integers |v| <= 2^52
+// (plain form) or |v| <= 2^50 plus kRoundBias (biased form: the digits are bit
+// fields of the double, with no conversion to a 64-bit integer).
+template <bool kBiased>
 __device__ __forceinline__ void write_residues8(const ResidueArgs& a, int8_t* Y, size_t plane,
                                                 size_t off, const double (&v)[8]) {
   constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23
-  constexpr long long kBias = 8192LL * (1 + (1LL << 14) + (1LL << 28));
   f32x2 P0[4], P1[4], P2[4], P3[4];
   uint32_t lowb[2] = {0u, 0u};
 #pragma unroll
@@ -258,13 +283,23 @@ __device__ __forceinline__ void write_residues8(const ResidueArgs& a, int8_t* Y,
     float u[2][4];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const long long iv = static_cast<long long>(v[j + h]);
-      lowb[(j + h) >> 2] |= uint32_t(iv & 0xff) << (8 * ((j + h) & 3));  // modulus 256
-      const long long w = iv + kBias;
-      u[h][0] = float(int(w & 0x3fff) - 8192);
-      u[h][1] = float(int((w >> 14) & 0x3fff) - 8192);
-      u[h][2] = float(int((w >> 28) & 0x3fff) - 8192);
-      u[h][3] = float(int(w >> 42));
+      if constexpr (kBiased) {
+        // mantissa field = w + 2^51: bits 0..41 are w's, bits 42..51 are (w >> 42) + 2^9
+        const uint32_t lo = __double2loint(v[j + h]), hi = __double2hiint(v[j + h]);
+        lowb[(j + h) >> 2] |= (lo & 0xffu) << (8 * ((j + h) & 3));  // modulus 256
+        u[h][0] = float(int(lo & 0x3fffu) - 8192);
+        u[h][1] = float(int((lo >> 14) & 0x3fffu) - 8192);
+        u[h][2] = float(int(__funnelshift_r(lo, hi, 28) & 0x3fffu) - 8192);
+        u[h][3] = float(int((hi >> 10) & 0x3ffu) - 512);
+      } else {
+        const long long iv = static_cast<long long>(v[j + h]);
+        lowb[(j + h) >> 2] |= uint32_t(iv & 0xff) << (8 * ((j + h) & 3));  // modulus 256
+        const long long w = iv + kDigitBias;
+        u[h][0] = float(int(w & 0x3fff) - 8192);
+        u[h][1] = float(int((w >> 14) & 0x3fff) - 8192);
+        u[h][2] = float(int((w >> 28) & 0x3fff) - 8192);
+        u[h][3] = float(int(w >> 42));
+      }
     }
     P0[j >> 1] = pack2(u[0][0], u[1][0]);
     P1[j >> 1] = pack2(u[0][1], u[1][1]);
@@ -273,12 +308,11 @@ __device__ __forceinline__ void write_residues8(const ResidueArgs& a, int8_t* Y,
   }
   *reinterpret_cast<uint2*>(Y + off) = make_uint2(lowb[0], lowb[1]);
   const f32x2 MAG = pack2(kMagic, kMagic), NMAG = pack2(-kMagic, -kMagic);
-  for (int l = 1; l < a.nmod; ++l) {
-    const f32x2 C14 = pack2(a.c14[l], a.c14[l]),
-                C28 = pack2(a.c28[l], a.c28[l]), C42 = pack2(a.c42[l], a.c42[l]),
-                INV = pack2(a.inv[l], a.inv[l]);
-    const float nm = -float(a.mod[l]);
-    const f32x2 NM = pack2(nm, nm);
+  // unrolled: every constant is read at a fixed offset of the parameter bank
+#pragma unroll
+  for (int l = 1; l < kMaxModuli; ++l) {
+    if (l >= a.nmod) break;
+    const f32x2 C14 = a.c14[l], C28 = a.c28[l], C42 = a.c42[l], INV = a.inv[l], NM = a.nm[l];
     uint32_t bits[8];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -298,6 +332,7 @@ __device__ __forceinline__ void write_residues8(const ResidueArgs& a, int8_t* Y,
 }
 
 // element (r, p) at x[r*ld + p]: CTA per row, thread per 8 consecutive p
+template <bool kBiased>
 __global__ void __launch_bounds__(256, 5)
 residues_rows(const double* __restrict__ x, size_t ld, int rows, int k, size_t kpad,
               const int* __restrict__ e, int8_t* __restrict__ Y, ResidueArgs a) {
@@ -309,22 +344,30 @@ residues_rows(const double* __restrict__ x, size_t ld, int rows, int k, size_t k
   for (int p = 8 * threadIdx.x; p < k; p += 8 * 256) {
     double v[8];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) v[j] = (p + j < k) ? scaled_int(row[p + j], er) : 0.0;
-    write_residues8(a, Y, plane, size_t(r) * kpad + p, v);
+    for (int j = 0; j < 8; ++j)
+      v[j] = (p + j < k) ? scaled<kBiased>(row[p + j], er) : scaled_zero<kBiased>();
+    write_residues8<kBiased>(a, Y, plane, size_t(r) * kpad + p, v);
   }
 }
 
-// element (r, p) at x[p*ld + r]: 32 (r) x 64 (p) tiles transposed through shared memory
+// element (r, p) at x[p*ld + r]: 32 (r) x 64 (p) tiles transposed through shared
+// memory.  Element (p, r) sits in column r ^ 2 (p / 8) of row p: a row is written
+// by one warp (a permutation of its 32 columns), and each half-warp of the
+// read side (two r, eight groups of p) meets 16 distinct 8-byte bank pairs.
+__device__ __forceinline__ int tile_col(int p, int r) { return r ^ ((p >> 2) & 14); }
+
+template <bool kBiased>
 __global__ void __launch_bounds__(256, 5)
 residues_cols(const double* __restrict__ x, size_t ld, int rows, int k, size_t kpad,
               const int* __restrict__ e, int8_t* __restrict__ Y, ResidueArgs a, Mask mask) {
-  __shared__ double tile[64][33];
+  __shared__ double tile[64][32];
   const int r0 = blockIdx.x * 32, p0 = blockIdx.y * 64;
   const int tr = threadIdx.x & 31, tp = threadIdx.x >> 5;  // 8 rows of p per pass
 #pragma unroll
   for (int pp = tp; pp < 64; pp += 8) {
     const int p = p0 + pp, r = r0 + tr;
-    tile[pp][tr] = (p < k && r < rows && mask.on(r, p)) ? x[size_t(p) * ld + r] : 0.0;
+    tile[pp][tile_col(pp, tr)] =
+        (p < k && r < rows && mask.on(r, p)) ? x[size_t(p) * ld + r] : 0.0;
   }
   __syncthreads();
   const size_t plane = size_t(rows) * kpad;
@@ -335,8 +378,10 @@ residues_cols(const double* __restrict__ x, size_t ld, int rows, int k, size_t k
   const int er = e[r];
   double v[8];
 #pragma unroll
-  for (int j = 0; j < 8; ++j) v[j] = (p + j < k) ? scaled_int(tile[pg + j][rr], er) : 0.0;
-  write_residues8(a, Y, plane, size_t(r) * kpad + p, v);
+  for (int j = 0; j < 8; ++j)
+    v[j] = (p + j < k) ? scaled<kBiased>(tile[pg + j][tile_col(pg + j, rr)], er)
+                       : scaled_zero<kBiased>();
+  write_residues8<kBiased>(a, Y, plane, size_t(r) * kpad + p, v);
 }
 
 // ---------------------------------------------------------------------------
@@ -476,15 +521,22 @@ int mods_host(long long v, int m) {  // symmetric residue
   return int(r);
 }
 
+// both FP32 lanes of a packed word set to v
+f32x2 splat2(float v) {
+  uint32_t b;
+  std::memcpy(&b, &v, sizeof b);
+  return (f32x2(b) << 32) | b;
+}
+
 ResidueArgs residue_args(const OzakiPlan& p) {
   ResidueArgs a{};
   a.nmod = p.nmod;
   for (int l = 0; l < p.nmod; ++l) {
-    a.mod[l] = p.mod[l];
-    a.inv[l] = p.inv_f[l];
-    a.c14[l] = float(mods_host(1LL << 14, p.mod[l]));
-    a.c28[l] = float(mods_host(1LL << 28, p.mod[l]));
-    a.c42[l] = float(mods_host(1LL << 42, p.mod[l]));
+    a.inv[l] = splat2(p.inv_f[l]);
+    a.nm[l] = splat2(-float(p.mod[l]));
+    a.c14[l] = splat2(float(mods_host(1LL << 14, p.mod[l])));
+    a.c28[l] = splat2(float(mods_host(1LL << 28, p.mod[l])));
+    a.c42[l] = splat2(float(mods_host(1LL << 42, p.mod[l])));
   }
   return a;
 }
@@ -503,11 +555,15 @@ cudaError_t prepare(const double* x, size_t ld, bool rows_contig, int rows, int 
                                                                          mask);
   }
   finalize_exps<<<rb, 256, 0, s>>>(emax, rows, bits, e);
+  // scaled elements below 2^50 take the biased form of the digit split
+  const bool biased = bits <= 50;
   if (rows_contig) {
-    residues_rows<<<rows, 256, 0, s>>>(x, ld, rows, k, kpad, e, Y, ra);
+    (biased ? residues_rows<true> : residues_rows<false>)<<<rows, 256, 0, s>>>(
+        x, ld, rows, k, kpad, e, Y, ra);
   } else {
     dim3 grid((rows + 31) / 32, (k + 63) / 64);
-    residues_cols<<<grid, 256, 0, s>>>(x, ld, rows, k, kpad, e, Y, ra, mask);
+    (biased ? residues_cols<true> : residues_cols<false>)<<<grid, 256, 0, s>>>(
+        x, ld, rows, k, kpad, e, Y, ra, mask);
   }
   return cudaGetLastError();
 }

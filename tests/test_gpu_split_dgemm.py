@@ -143,3 +143,20 @@ def test_large_host_call_in_blocks(cm, ta, tb, prec):
                      ldc, ta, tb, prec)
         torch.cuda.synchronize()
         assert np.array_equal(dc.cpu().numpy(), c)
+
+
+@pytest.mark.parametrize("nmod,k", [(14, 33), (15, 1000), (16, 1000), (16, 6581)])
+def test_split_moduli_override(cm, oracle, monkeypatch, nmod, k):
+    """More moduli than the default (CFGMM_OZAKI_MODULI) scale the operands past
+    50 bits, where the residue split takes its 64-bit integer form instead of
+    the biased-double form (for A, B or both): same accuracy, to the oracle."""
+    monkeypatch.setenv("CFGMM_OZAKI_MODULI", str(nmod))
+    m, n = 131, 257
+    rng = np.random.default_rng(nmod * 7 + k)
+    a = rng.uniform(-1, 1, (m, k))
+    b = rng.uniform(-1, 1, (k, n))
+    c0 = rng.uniform(-1, 1, (m, n))
+    c, ref = c0.copy(), c0.copy()
+    split(cm, c, a, b, m, n, k, k, n, n, False, False)
+    oracle.matmul_anyway_full(ref, a, b, m, n, k, k, n, n, False, False)
+    assert normwise(c, ref) < 1e-13
