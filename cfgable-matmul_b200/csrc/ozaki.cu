@@ -497,7 +497,7 @@ bool make_plane_map(CUtensorMap* map, void* base, int k, int rows, int nplanes, 
 size_t a256(size_t v) { return (v + 255) / 256 * 256; }
 
 struct DgemmLayout {
-  size_t kpad, ldr, a_res, b_res, r, ea, eb, emax, total;
+  size_t kpad, ldr, a_res, b_res, r, ea, eb, emax_a, emax_b, total;
 };
 
 DgemmLayout dgemm_layout(int m, int n, int k, int nmod) {
@@ -509,8 +509,9 @@ DgemmLayout dgemm_layout(int m, int n, int k, int nmod) {
   L.r = L.b_res + a256(size_t(nmod) * n * L.kpad);
   L.ea = L.r + a256(size_t(nmod) * m * L.ldr);
   L.eb = L.ea + a256(size_t(m) * sizeof(int));
-  L.emax = L.eb + a256(size_t(n) * sizeof(int));
-  L.total = L.emax + a256(size_t(std::max(m, n)) * sizeof(int));
+  L.emax_a = L.eb + a256(size_t(n) * sizeof(int));
+  L.emax_b = L.emax_a + a256(size_t(m) * sizeof(int));
+  L.total = L.emax_b + a256(size_t(n) * sizeof(int));
   return L;
 }
 
@@ -568,6 +569,37 @@ cudaError_t prepare(const double* x, size_t ld, bool rows_contig, int rows, int 
   return cudaGetLastError();
 }
 
+// A non-blocking stream and its fork / join events per host thread and device,
+// made on first use and kept for the life of the thread (per thread, so that
+// calls from several threads never record over one another's fork event).
+struct SideStream {
+  cudaStream_t s = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+
+const SideStream* side_stream() {
+  constexpr int kMaxDevices = 64;
+  thread_local SideStream streams[kMaxDevices];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+  SideStream& st = streams[dev];
+  if (!st.s) {
+    SideStream t;
+    if (cudaStreamCreateWithFlags(&t.s, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+    if (cudaEventCreateWithFlags(&t.fork, cudaEventDisableTiming) != cudaSuccess) {
+      cudaStreamDestroy(t.s);
+      return nullptr;
+    }
+    if (cudaEventCreateWithFlags(&t.join, cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventDestroy(t.fork);
+      cudaStreamDestroy(t.s);
+      return nullptr;
+    }
+    st = t;
+  }
+  return &st;
+}
+
 }  // namespace
 
 int ozaki_default_moduli(int k) {
@@ -608,16 +640,34 @@ cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int 
   mark(0);
   // op(A) rows are i (k contiguous unless transa); op(B) "rows" are j
   // (k contiguous only when transb).
-  int* emax = reinterpret_cast<int*>(ws + L.emax);
+  int* emax_a = reinterpret_cast<int*>(ws + L.emax_a);
+  int* emax_b = reinterpret_cast<int*>(ws + L.emax_b);
   cudaError_t err = cudaSuccess;
+  // With both operands to prepare, A's kernels run on a side stream beside B's:
+  // the residue kernels are bound by instruction issue and the exponent scans
+  // by DRAM, so the two chains overlap.  The side stream joins back before the
+  // GEMM (the fork and join are events, so a stream capture follows them).
+  const SideStream* side = (!reuse_a && !reuse_b) ? side_stream() : nullptr;
+  cudaStream_t sa = stream;
+  if (side) {
+    if ((err = cudaEventRecord(side->fork, stream)) != cudaSuccess ||
+        (err = cudaStreamWaitEvent(side->s, side->fork, 0)) != cudaSuccess)
+      return err;
+    sa = side->s;
+  }
   if (!reuse_a) {
-    err = prepare(a, lda, !transa, m, k, L.kpad, plan.alpha, emax, ea, a_res, ra, stream);
+    err = prepare(a, lda, !transa, m, k, L.kpad, plan.alpha, emax_a, ea, a_res, ra, sa);
     if (err != cudaSuccess) return err;
   }
   if (!reuse_b) {
-    err = prepare(b, ldb, transb, n, k, L.kpad, plan.beta, emax, eb, b_res, ra, stream,
+    err = prepare(b, ldb, transb, n, k, L.kpad, plan.beta, emax_b, eb, b_res, ra, stream,
                   Mask{tab, ldtab, blk > 0 ? blk : 1});
     if (err != cudaSuccess) return err;
+  }
+  if (side) {
+    if ((err = cudaEventRecord(side->join, side->s)) != cudaSuccess ||
+        (err = cudaStreamWaitEvent(stream, side->join, 0)) != cudaSuccess)
+      return err;
   }
 
   mark(1);
