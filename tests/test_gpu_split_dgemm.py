@@ -160,3 +160,37 @@ def test_split_moduli_override(cm, oracle, monkeypatch, nmod, k):
     split(cm, c, a, b, m, n, k, k, n, n, False, False)
     oracle.matmul_anyway_full(ref, a, b, m, n, k, k, n, n, False, False)
     assert normwise(c, ref) < 1e-13
+
+
+def test_split_device_call_in_cuda_graph(cm):
+    """The device-pointer split call, whose operand preparation forks onto a side
+    stream and joins back, records into a CUDA graph: a replay gives the bits of
+    a direct call, and a second replay accumulates onto them."""
+    import torch
+    m, n, k = 257, 300, 700
+    g = torch.Generator(device="cuda").manual_seed(8)
+    a = torch.rand(m, k, dtype=torch.float64, device="cuda", generator=g) - 0.5
+    b = torch.rand(k, n, dtype=torch.float64, device="cuda", generator=g) - 0.5
+    ref = torch.zeros(m, n, dtype=torch.float64, device="cuda")
+    c = torch.zeros_like(ref)
+
+    def call(out):
+        cm.matmul_ex(out, a, b, m, n, k, k, n, n, False, False, precision=cm.PREC_OZAKI_INT8)
+
+    call(ref)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        call(c)  # warm-up on a side stream before the capture
+    torch.cuda.current_stream().wait_stream(s)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        call(c)
+    c.zero_()
+    graph.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(c, ref)
+    graph.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(c, 2 * ref)
+    del graph
