@@ -58,6 +58,7 @@
 
 #include "aodmao2rho_fp64.cuh"
 #include "aodmao2rho_split.cuh"
+#include "side_stream.cuh"
 #include "tcgen05.cuh"
 
 namespace cfgmm {
@@ -786,21 +787,32 @@ cudaError_t aodmao2rho_split(double* rhos, const double* dms, const double* ao_l
   uint8_t* phisl = reinterpret_cast<uint8_t*>(ws + L.phisl);
   double* partial = reinterpret_cast<double*>(ws + L.partial);
 
-  cudaError_t err = aodm_block_lists_launch(tab, ldtab, nao, nblk, lists, counts, stream);
-  if (err != cudaSuccess) return err;
-  split_build<<<1, 1024, 0, stream>>>(counts, nbg, gsub, nset, max_ut, cbase, items, total);
+  // The D chain (symmetry check, D slices) runs on a side stream beside the phi
+  // chain (block lists, items, phi slices); the side stream joins back before
+  // the main kernel.
+  const SideStream* side = side_stream();
+  cudaStream_t sd = stream;
+  cudaError_t err = cudaSuccess;
+  if (side) {
+    if ((err = side_fork(side, stream)) != cudaSuccess) return err;
+    sd = side->s;
+  }
   // total[2]: asymmetry flag; the half contraction needs D = D^T and phi_lhs = phi_rhs
   int* asym = aodm_sym_enabled() && ao_lhs == ao_rhs ? total + 2 : nullptr;
   if (asym) {
-    if ((err = cudaMemsetAsync(asym, 0, sizeof(int), stream)) != cudaSuccess) return err;
-    if ((err = aodm_launch_sym_check(dms, stride_ao, nao, nset, asym, stream)) != cudaSuccess)
+    if ((err = cudaMemsetAsync(asym, 0, sizeof(int), sd)) != cudaSuccess) return err;
+    if ((err = aodm_launch_sym_check(dms, stride_ao, nao, nset, asym, sd)) != cudaSuccess)
       return err;
   }
-  if ((err = split_prepare_d(dms, stride_ao, nao, nset, dsl, tau, stream, asym)) != cudaSuccess)
+  if ((err = split_prepare_d(dms, stride_ao, nao, nset, dsl, tau, sd, asym)) != cudaSuccess)
     return err;
+  if ((err = aodm_block_lists_launch(tab, ldtab, nao, nblk, lists, counts, stream)) != cudaSuccess)
+    return err;
+  split_build<<<1, 1024, 0, stream>>>(counts, nbg, gsub, nset, max_ut, cbase, items, total);
   if ((err = split_prepare_phi(ao_rhs, stride_grid, lists, counts, cbase, nao, ngrid, blk, pmax,
                                sigma, phisl, stream)) != cudaSuccess)
     return err;
+  if (side && (err = side_join(side, stream)) != cudaSuccess) return err;
 
   SplitArgs a{};
   a.dsl = dsl;

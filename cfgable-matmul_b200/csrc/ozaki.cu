@@ -31,6 +31,7 @@
 
 #include "gemm_i8.cuh"
 #include "ozaki.cuh"
+#include "side_stream.cuh"
 
 namespace cfgmm {
 
@@ -569,13 +570,7 @@ cudaError_t prepare(const double* x, size_t ld, bool rows_contig, int rows, int 
   return cudaGetLastError();
 }
 
-// A non-blocking stream and its fork / join events per host thread and device,
-// made on first use and kept for the life of the thread (per thread, so that
-// calls from several threads never record over one another's fork event).
-struct SideStream {
-  cudaStream_t s = nullptr;
-  cudaEvent_t fork = nullptr, join = nullptr;
-};
+}  // namespace
 
 const SideStream* side_stream() {
   constexpr int kMaxDevices = 64;
@@ -600,7 +595,6 @@ const SideStream* side_stream() {
   return &st;
 }
 
-}  // namespace
 
 int ozaki_default_moduli(int k) {
   const char* env = std::getenv("CFGMM_OZAKI_MODULI");
@@ -650,9 +644,7 @@ cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int 
   const SideStream* side = (!reuse_a && !reuse_b) ? side_stream() : nullptr;
   cudaStream_t sa = stream;
   if (side) {
-    if ((err = cudaEventRecord(side->fork, stream)) != cudaSuccess ||
-        (err = cudaStreamWaitEvent(side->s, side->fork, 0)) != cudaSuccess)
-      return err;
+    if ((err = side_fork(side, stream)) != cudaSuccess) return err;
     sa = side->s;
   }
   if (!reuse_a) {
@@ -664,11 +656,7 @@ cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int 
                   Mask{tab, ldtab, blk > 0 ? blk : 1});
     if (err != cudaSuccess) return err;
   }
-  if (side) {
-    if ((err = cudaEventRecord(side->join, side->s)) != cudaSuccess ||
-        (err = cudaStreamWaitEvent(stream, side->join, 0)) != cudaSuccess)
-      return err;
-  }
+  if (side && (err = side_join(side, stream)) != cudaSuccess) return err;
 
   mark(1);
   CUtensorMap tmA, tmB;
