@@ -783,6 +783,17 @@ namespace cfgmm {
 // Lets entry points defined in other translation units report a detail
 // message through cfgmm_last_error().
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+// The argument checks of cfgmm_aodmao2rho_dev (device pointers: no slice
+// lengths, so every length is unbounded) for entry points in other
+// translation units; sets the detail message on failure.
+int check_aodm_dev(const void* rhos, const void* dms, const void* ao_lhs, const void* ao_rhs,
+                   size_t stride_ao, size_t stride_grid, size_t nao, size_t ngrid, size_t nset,
+                   const uint8_t* tab, size_t ldtab, size_t blksize) {
+  AodmExtents ex;
+  return check_aodm(rhos, SIZE_MAX, dms, SIZE_MAX, ao_lhs, SIZE_MAX, ao_rhs, SIZE_MAX, stride_ao,
+                    stride_grid, nao, ngrid, nset, tab, SIZE_MAX, ldtab, blksize, &ex);
+}
 }  // namespace cfgmm
 
 extern "C" {

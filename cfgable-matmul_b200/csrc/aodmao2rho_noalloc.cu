@@ -16,6 +16,12 @@
 // process exits.  Problems whose scratch would not fit are refused with
 // CFGMM_ERR_INVALID_ARGUMENT and a message giving the size they need.
 //
+// The first call on a device loads the library's device image there and looks
+// up the array's device address; make that first call before any stream
+// capture.  Every later call looks the address up again (a lookup in the
+// runtime's table, no allocation), so a device reset and a new context between
+// two calls can never leave a stale address behind.
+//
 // All calls share the one array and it keeps whatever the previous call left
 // in it.  Nothing in it needs to start at zero: the list kernel writes every
 // count and list entry the later kernels read, the work-list kernel writes the
@@ -25,9 +31,7 @@
 // the array and may return wrong results; the caller must order them.
 #include <cuda_runtime.h>
 
-#include <climits>
 #include <cstdio>
-#include <mutex>
 #include <string>
 
 #include "../../include/cfgmm.h"
@@ -35,18 +39,17 @@
 
 namespace cfgmm {
 void set_last_error(const std::string& msg);
+int check_aodm_dev(const void* rhos, const void* dms, const void* ao_lhs, const void* ao_rhs,
+                   size_t stride_ao, size_t stride_grid, size_t nao, size_t ngrid, size_t nset,
+                   const uint8_t* tab, size_t ldtab, size_t blksize);
 }
 
 namespace {
 
 // Host code must never hand `g_noalloc_scratch` itself to a kernel: on the
 // host the name only stands in for the symbol.  Its device address comes from
-// cudaGetSymbolAddress, once per device, below.
+// cudaGetSymbolAddress with the calling device current, below.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[CFGMM_NOALLOC_SCRATCH_BYTES];
-
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mu;
-void* g_scratch_ptr[kMaxDevices] = {};
 
 int fail(int status, const std::string& msg) {
   cfgmm::set_last_error(msg);
@@ -59,23 +62,16 @@ int cuda_fail(cudaError_t err, const char* where) {
                   ")");
 }
 
-// Device address of this device's copy of the scratch array.  Set up on the
-// first call made with `dev` current; later calls reuse the cached address.
-int scratch_address(int dev, void** out) {
-  if (dev < 0 || dev >= kMaxDevices) return fail(CFGMM_ERR_INVALID_ARGUMENT, "device index");
-  std::lock_guard<std::mutex> lk(g_setup_mu);
-  if (!g_scratch_ptr[dev]) {
-    void* p = nullptr;
-    cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (err != cudaSuccess) return cuda_fail(err, "cudaGetSymbolAddress(scratch)");
-    if (!p) return fail(CFGMM_ERR_CUDA, "cudaGetSymbolAddress returned a null address");
-    g_scratch_ptr[dev] = p;
-  }
-  *out = g_scratch_ptr[dev];
+// Device address of the current device's copy of the scratch array, in the
+// current context.  Not cached: a cached address would outlive a device reset.
+int scratch_address(void** out) {
+  void* p = nullptr;
+  cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (err != cudaSuccess) return cuda_fail(err, "cudaGetSymbolAddress(scratch)");
+  if (!p) return fail(CFGMM_ERR_CUDA, "cudaGetSymbolAddress returned a null address");
+  *out = p;
   return CFGMM_OK;
 }
-
-bool fits_int(size_t v) { return v <= size_t(INT_MAX) - 4096; }
 
 }  // namespace
 
@@ -85,14 +81,11 @@ extern "C" int cfgmm_aodmao2rho_dev_noalloc(double* rhos, const double* dms, con
                                             size_t nset, const uint8_t* tab, size_t ldtab,
                                             size_t blksize, void* stream) {
   cfgmm::set_last_error("");
-  if (blksize == 0) return fail(CFGMM_ERR_INVALID_ARGUMENT, "BLKSIZE must be at least 1");
+  // the same checks, in the same order, as cfgmm_aodmao2rho_dev
+  int rc = cfgmm::check_aodm_dev(rhos, dms, ao_lhs, ao_rhs, stride_ao, stride_grid, nao, ngrid,
+                                 nset, tab, ldtab, blksize);
+  if (rc != CFGMM_OK) return rc;
   if (nao == 0 || ngrid == 0 || nset == 0) return CFGMM_OK;
-  if (!fits_int(nao) || !fits_int(ngrid) || !fits_int(nset) || !fits_int(blksize))
-    return fail(CFGMM_ERR_INVALID_ARGUMENT, "nao, ngrid, nset and BLKSIZE must be below 2^31");
-  if (stride_grid < ngrid)
-    return fail(CFGMM_ERR_INVALID_ARGUMENT, "stride_grid < ngrid: rows of rho would overlap");
-  if (!rhos || !dms || !ao_lhs || !ao_rhs || !tab)
-    return fail(CFGMM_ERR_INVALID_ARGUMENT, "null pointer");
   const size_t need = cfgmm::aodmao2rho_fp64_workspace(nao, ngrid, nset, blksize);
   if (need > size_t(CFGMM_NOALLOC_SCRATCH_BYTES)) {
     char msg[256];
@@ -102,12 +95,14 @@ extern "C" int cfgmm_aodmao2rho_dev_noalloc(double* rhos, const double* dms, con
                   need, size_t(CFGMM_NOALLOC_SCRATCH_BYTES));
     return fail(CFGMM_ERR_INVALID_ARGUMENT, msg);
   }
-  int dev = 0;
-  cudaError_t err = cudaGetDevice(&dev);
-  if (err != cudaSuccess) return cuda_fail(err, "cudaGetDevice");
+  int ndev = 0;
+  cudaError_t err = cudaGetDeviceCount(&ndev);
+  if (err != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(CFGMM_ERR_NO_DEVICE, "no CUDA device is visible");
+  }
   void* ws = nullptr;
-  int rc = scratch_address(dev, &ws);
-  if (rc != CFGMM_OK) return rc;
+  if ((rc = scratch_address(&ws)) != CFGMM_OK) return rc;
   err = cfgmm::aodmao2rho_fp64(rhos, dms, ao_lhs, ao_rhs, stride_ao, stride_grid, int(nao),
                                int(ngrid), int(nset), tab, ldtab, int(blksize), ws,
                                static_cast<cudaStream_t>(stream));

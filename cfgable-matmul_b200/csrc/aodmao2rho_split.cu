@@ -790,13 +790,10 @@ cudaError_t aodmao2rho_split(double* rhos, const double* dms, const double* ao_l
   // The D chain (symmetry check, D slices) runs on a side stream beside the phi
   // chain (block lists, items, phi slices); the side stream joins back before
   // the main kernel.
-  const SideStream* side = side_stream();
-  cudaStream_t sd = stream;
-  cudaError_t err = cudaSuccess;
-  if (side) {
-    if ((err = side_fork(side, stream)) != cudaSuccess) return err;
-    sd = side->s;
-  }
+  SideScope side(side_stream(), stream);
+  cudaError_t err = side.fork();
+  if (err != cudaSuccess) return err;
+  const cudaStream_t sd = side.stream();
   // total[2]: asymmetry flag; the half contraction needs D = D^T and phi_lhs = phi_rhs
   int* asym = aodm_sym_enabled() && ao_lhs == ao_rhs ? total + 2 : nullptr;
   if (asym) {
@@ -812,7 +809,7 @@ cudaError_t aodmao2rho_split(double* rhos, const double* dms, const double* ao_l
   if ((err = split_prepare_phi(ao_rhs, stride_grid, lists, counts, cbase, nao, ngrid, blk, pmax,
                                sigma, phisl, stream)) != cudaSuccess)
     return err;
-  if (side && (err = side_join(side, stream)) != cudaSuccess) return err;
+  if ((err = side.join()) != cudaSuccess) return err;
 
   SplitArgs a{};
   a.dsl = dsl;

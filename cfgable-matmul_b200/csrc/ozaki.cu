@@ -578,19 +578,21 @@ const SideStream* side_stream() {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
   SideStream& st = streams[dev];
-  if (!st.s) {
-    SideStream t;
-    if (cudaStreamCreateWithFlags(&t.s, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
-    if (cudaEventCreateWithFlags(&t.fork, cudaEventDisableTiming) != cudaSuccess) {
-      cudaStreamDestroy(t.s);
+  if (!st.join) {
+    // made in place; a partial set (one creation failed) is kept, released at
+    // thread exit, and completed by a later call
+    if (!st.s && cudaStreamCreateWithFlags(&st.s, cudaStreamNonBlocking) != cudaSuccess) {
+      st.s = nullptr;
       return nullptr;
     }
-    if (cudaEventCreateWithFlags(&t.join, cudaEventDisableTiming) != cudaSuccess) {
-      cudaEventDestroy(t.fork);
-      cudaStreamDestroy(t.s);
+    if (!st.fork && cudaEventCreateWithFlags(&st.fork, cudaEventDisableTiming) != cudaSuccess) {
+      st.fork = nullptr;
       return nullptr;
     }
-    st = t;
+    if (cudaEventCreateWithFlags(&st.join, cudaEventDisableTiming) != cudaSuccess) {
+      st.join = nullptr;
+      return nullptr;
+    }
   }
   return &st;
 }
@@ -641,12 +643,9 @@ cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int 
   // the residue kernels are bound by instruction issue and the exponent scans
   // by DRAM, so the two chains overlap.  The side stream joins back before the
   // GEMM (the fork and join are events, so a stream capture follows them).
-  const SideStream* side = (!reuse_a && !reuse_b) ? side_stream() : nullptr;
-  cudaStream_t sa = stream;
-  if (side) {
-    if ((err = side_fork(side, stream)) != cudaSuccess) return err;
-    sa = side->s;
-  }
+  SideScope side((!reuse_a && !reuse_b) ? side_stream() : nullptr, stream);
+  if ((err = side.fork()) != cudaSuccess) return err;
+  const cudaStream_t sa = side.stream();
   if (!reuse_a) {
     err = prepare(a, lda, !transa, m, k, L.kpad, plan.alpha, emax_a, ea, a_res, ra, sa);
     if (err != cudaSuccess) return err;
@@ -656,7 +655,7 @@ cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int 
                   Mask{tab, ldtab, blk > 0 ? blk : 1});
     if (err != cudaSuccess) return err;
   }
-  if (side && (err = side_join(side, stream)) != cudaSuccess) return err;
+  if ((err = side.join()) != cudaSuccess) return err;
 
   mark(1);
   CUtensorMap tmA, tmB;

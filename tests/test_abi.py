@@ -191,3 +191,36 @@ def test_no_cpu_fallback_without_device(cm):
     with pytest.raises(cm.CfgmmError) as e:
         cm.Server(1 << 30)
     assert e.value.status == -4
+
+
+def test_noalloc_rejects_what_dev_rejects(cm):
+    """The no-allocation contraction runs the argument checks of
+    cfgmm_aodmao2rho_dev: overflowing index ranges (stride_ao^2, the set
+    stride times nset, the mask extent) get the same status from both, before
+    any device is touched."""
+    L = ctypes.CDLL(cm.library_path)
+    P, S, I = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int
+    L.cfgmm_aodmao2rho_dev_noalloc.argtypes = [P, P, P, P, S, S, S, S, S, P, S, S, P]
+    L.cfgmm_aodmao2rho_dev_noalloc.restype = I
+    L.cfgmm_aodmao2rho_dev.argtypes = [P, P, P, P, S, S, S, S, S, P, S, S, I, P]
+    L.cfgmm_aodmao2rho_dev.restype = I
+    L.cfgmm_last_error.restype = ctypes.c_char_p
+    big = 1 << 33  # stride_ao^2 = 2^66 overflows usize
+    fake = 0x1000  # never dereferenced: the checks fail first
+    cases = [
+        # (stride_ao, stride_grid, nao, ngrid, nset, ldtab, blksize)
+        (big, 100, 10, 100, 2, 3, 48),             # stride_ao^2 overflows
+        (1 << 31, 100, 10, 100, 1 << 30, 3, 48),  # (nset-1) * stride_ao^2 overflows
+        (10, 100, 10, 100, 2, (1 << 63), 48),      # (nao-1) * ldtab overflows
+        (10, 50, 10, 100, 2, 3, 48),               # stride_grid < ngrid
+        (10, 100, 10, 100, 2, 3, 0),               # BLKSIZE 0
+        (10, 100, 1 << 40, 100, 2, 3, 48),         # nao beyond 2^31
+    ]
+    for sa, sg, nao, ngrid, nset, ldtab, blk in cases:
+        args = [fake, fake, fake, fake, sa, sg, nao, ngrid, nset, fake, ldtab, blk]
+        rc_dev = L.cfgmm_aodmao2rho_dev(*args, 0, None)
+        msg_dev = L.cfgmm_last_error()
+        rc_na = L.cfgmm_aodmao2rho_dev_noalloc(*args, None)
+        msg_na = L.cfgmm_last_error()
+        assert rc_dev == -1, (sa, sg, nao, ngrid, nset, ldtab, blk, msg_dev)
+        assert rc_na == rc_dev and msg_na == msg_dev, (msg_na, msg_dev)

@@ -73,6 +73,20 @@ def test_noalloc_matches_allocating_entry_point(capi, wl):
             assert free_after == free_before
 
 
+def test_noalloc_matches_oracle(capi, wl, oracle):
+    """An independent check: the no-allocation call against the oracle (the
+    CPU restatement of the reference's loops), not only against the other
+    entry point."""
+    p = wl.small_masked(seed=11, nao=256, ngrid=2048, nset=2)
+    ao, dms, tab = _device_problem(p)
+    for _ in range(2):  # the second call starts from the first one's leftover scratch
+        got = _run(capi, "noalloc", p, ao, dms, tab)
+        ref = np.zeros((p.nset, p.ngrid))
+        oracle.aodmao2rho(ref, p.dms, p.ao, p.ao, (p.nao, p.ngrid), (p.nao, p.ngrid), p.nset,
+                          p.tab, p.nblk, p.blksize)
+        assert normwise(got, ref) < TOL
+
+
 def test_noalloc_refuses_oversized_problem(capi, wl):
     import torch
     nao, ngrid, nset, blk = 4000, 65536, 4, 64  # needs far more than 32 MiB of scratch
