@@ -223,6 +223,13 @@ int check_device_waits() {
   if (code == 0) code = code3;
   if (code == 0) code = code4;
   if (code != 0) {
+    // reported once: the words start over for the next call
+    cudaError_t e = cfgmm::gemm_i8_reset_error(nullptr);
+    if (e == cudaSuccess) e = cfgmm::aodmao2rho_split_reset_error(nullptr);
+    if (e == cudaSuccess) e = cfgmm::dgemm_reset_error(nullptr);
+    if (e == cudaSuccess) e = cfgmm::aodm_reset_error(nullptr);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(nullptr);
+    if (e != cudaSuccess) return cuda_fail(e, "resetting the device wait words");
     char msg[128];
     std::snprintf(msg, sizeof(msg), "a tensor-core pipeline wait timed out (code %d)", code);
     return fail(CFGMM_ERR_TIMEOUT, msg);
@@ -977,6 +984,17 @@ int cfgmm_matmul_dev_timed(double* c, const double* a, const double* b, size_t m
 }
 
 int cfgmm_split_moduli(size_t k) { return cfgmm::ozaki_default_moduli(int(k > 65536 ? 65536 : k)); }
+
+int cfgmm_test_arm_wait_timeout(int precision, double wait_ms) {
+  g_last_error.clear();
+  int rc = check_precision(precision);
+  if (rc != CFGMM_OK) return rc;
+  if (!(wait_ms >= 1.0 && wait_ms <= 2000.0))
+    return fail(CFGMM_ERR_INVALID_ARGUMENT, "wait_ms must lie in [1, 2000]");
+  cfgmm::arm_wait_injection(precision == CFGMM_PREC_OZAKI_INT8 ? 1 : 0,
+                            static_cast<unsigned long long>(wait_ms * 1e6));
+  return CFGMM_OK;
+}
 
 int cfgmm_device_check(void) {
   g_last_error.clear();

@@ -42,6 +42,11 @@ struct cfgmm_aodm_plan {
   cfgmm::AodmConfig cfg{1, 32};
   // split precision: D digits are rebuilt every run, phi digits once here
   cfgmm::SplitArgs sargs{};
+  // the pair form of split precision (two alike block tiles per item)
+  bool pair = false;
+  int nsl = 7;
+  cfgmm::PairArgs pargs{};
+  int* d_npairs = nullptr;  // device: the plan's pair count (the reduction's grid bound)
   const double* dms = nullptr;
   size_t stride_ao = 0;
   int nao = 0, nset_max = 0, stages = 0;
@@ -49,6 +54,7 @@ struct cfgmm_aodm_plan {
   double flops = 0.0;   // sum_batches sum_s sum_b (2|I_b|^2 + 2|I_b|)|b| per run
   void* mem = nullptr;  // one device allocation for lists, descriptors, work list, partials
   void* mem2 = nullptr;  // split precision: digits, scales, its work list and partials
+  void* mem3 = nullptr;  // pair form: the partial sums
   int2* rpairs = nullptr;
   cudaGraphExec_t exec = nullptr;
   std::string info;
@@ -139,8 +145,39 @@ cudaError_t split_prepare_run(cfgmm_aodm_plan* plan, cudaStream_t s) {
   return err;
 }
 
+// D digits of a pair-form run, after the symmetry check.
+cudaError_t pair_prepare_run(cfgmm_aodm_plan* plan, cudaStream_t s) {
+  const cfgmm::PairArgs& a = plan->pargs;
+  int* asym = const_cast<int*>(a.asym);
+  cudaError_t err = cudaSuccess;
+  if (asym) {
+    err = cudaMemsetAsync(asym, 0, sizeof(int), s);
+    if (err == cudaSuccess)
+      err = cfgmm::aodm_launch_sym_check(plan->dms, plan->stride_ao, plan->nao, plan->nset_max,
+                                         asym, s);
+  }
+  if (err == cudaSuccess)
+    err = cfgmm::split_pair_prepare_d(plan->dms, plan->stride_ao, plan->nao, plan->nset_max,
+                                      plan->nsl, const_cast<uint2*>(a.dsl),
+                                      const_cast<int*>(a.tau), s, asym);
+  return err;
+}
+
+cudaError_t pair_run_on(cfgmm_aodm_plan* plan, cudaStream_t s) {
+  cudaError_t err = pair_prepare_run(plan, s);
+  if (err == cudaSuccess) err = cfgmm::split_pair_launch_main(plan->pargs, plan->nsl, s);
+  if (err == cudaSuccess)
+    err = cfgmm::split_pair_launch_reduce(plan->pargs, plan->nsl, plan->d_npairs, 0, plan->npairs,
+                                          s);
+  return err;
+}
+
 // One split-precision run: D digits, the persistent kernel, the reduction.
 int split_run(cfgmm_aodm_plan* plan, cudaStream_t s) {
+  if (plan->pair) {
+    const cudaError_t err = pair_run_on(plan, s);
+    return err == cudaSuccess ? CFGMM_OK : cuda_fail(err, "split plan run");
+  }
   cudaError_t err = split_prepare_run(plan, s);
   if (err == cudaSuccess) err = cfgmm::split_launch_main(plan->sargs, s, plan->stages);
   if (err == cudaSuccess)
@@ -385,6 +422,216 @@ int build_split(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, size_t n
   return CFGMM_OK;
 }
 
+// The pair form of the split-precision plan: every batch's pairing, unions,
+// work list and phi digit tiles are built once here on the device (batch by
+// batch, the host reading each batch's pair and chunk counts to place the
+// next), then the work list is ordered matrix by matrix, heaviest first, and
+// the run (D digits, persistent kernel, reduction) is captured in a graph.
+// Per batch the result equals the single call's bit for bit: the same pairs,
+// unions, tiles and fixed-order sums.
+int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, size_t nbatch,
+                     const double* dms, size_t stride_ao, size_t nao, size_t nset_max,
+                     size_t blksize, int flags, int* d_lists, int* d_counts,
+                     const std::vector<size_t>& list_off, const std::vector<size_t>& cnt_off,
+                     const std::vector<size_t>& nblk, const std::vector<int>& counts,
+                     cudaStream_t s) {
+  const int nsl = cfgmm::split_pair_digits();
+  const int tn = cfgmm::split_pair_row_tile(nsl);
+  constexpr int HT = 64, TK = 32, PT = 128, WIN2 = 64;
+  const int gsub = int((blksize + HT - 1) / HT);
+  const size_t nwords = (nao + 31) / 32;
+  const size_t a_stage = size_t(nsl) * PT * TK;
+  size_t nbg_tot = 0, nbg_max = 0, ngrid_max = 0, sg_n = 0, chunk_bound = 0, item_bound = 0;
+  std::vector<size_t> sg_off(nbatch);
+  for (size_t i = 0; i < nbatch; ++i) {
+    const size_t nbg = nblk[i] * gsub;
+    nbg_tot += nbg;
+    nbg_max = std::max(nbg_max, nbg);
+    ngrid_max = std::max(ngrid_max, size_t(batches[i].ngrid));
+    sg_off[i] = sg_n;
+    sg_n += (batches[i].ngrid + 63) / 64 * 64;
+    for (size_t b = 0; b < nblk[i]; ++b) {
+      const size_t nb = size_t(counts[cnt_off[i] + b]);
+      // |U| <= |I_a| + |I_b|: a pair's chunks and row tiles are bounded by its tiles'
+      chunk_bound += gsub * ((nb + TK - 1) / TK);
+      item_bound += gsub * ((nb + tn - 1) / tn) * batches[i].nset;
+    }
+  }
+  // ---- device memory (the partial sums follow once the pairs are known) ----
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    const size_t off = o;
+    o += a256(std::max<size_t>(bytes, 1));
+    return off;
+  };
+  const size_t o_bits = take(nbg_max * nwords * 4), o_cnt = take(nbg_max * 4),
+               o_key = take(nbg_max * 8), o_order = take(nbg_max * 4),
+               o_cand = take(nbg_max * WIN2 * 4), o_ncand = take(nbg_max * 4),
+               o_partner = take(nbg_max * 4), o_pos = take(nbg_max * 4),
+               o_choice = take(nbg_max * 4), o_pmax = take(ngrid_max * 8),
+               o_pairs = take(nbg_tot * sizeof(int4)), o_np = take(8),
+               o_ulist = take(nbg_tot * nao * 4), o_uflag = take(nbg_tot * nao),
+               o_ucount = take(nbg_tot * 4), o_cbase = take((nbg_tot + 1) * 4),
+               o_poff = take((nbg_tot + 1) * 4), o_items = take(item_bound * sizeof(int4)),
+               o_total = take(16), o_sigma = take(sg_n * 4),
+               o_dsl = take(nset_max * nao * nao * 8), o_tau = take(nset_max * nao * 4),
+               o_batch = take(nbatch * sizeof(cfgmm::PairBatch)),
+               o_phisl = take(chunk_bound * a_stage);
+  cudaError_t err = cudaMallocAsync(&plan->mem2, o, s);
+  if (err != cudaSuccess) return cuda_fail(err, "cudaMalloc(split plan)");
+  char* base = static_cast<char*>(plan->mem2);
+  auto at = [&](size_t off) { return static_cast<void*>(base + off); };
+  int* d_np = static_cast<int*>(at(o_np));
+  int* d_total = static_cast<int*>(at(o_total));
+  err = cudaMemsetAsync(d_total, 0, 16, s);
+
+  std::vector<cfgmm::PairBatch> hb(nbatch);
+  int pair0 = 0, chunk0 = 0;
+  for (size_t i = 0; i < nbatch && err == cudaSuccess; ++i) {
+    const cfgmm_aodm_batch& b = batches[i];
+    cfgmm::PairPrep q{};
+    q.tab = b.tab;
+    q.ldtab = b.ldtab;
+    q.ao_rhs = b.ao_rhs;
+    q.stride_grid = b.stride_grid;
+    q.nao = int(nao);
+    q.ngrid = int(b.ngrid);
+    q.blk = int(blksize);
+    q.nset = int(b.nset);
+    q.nsl = nsl;
+    q.batch = int(i);
+    q.pair0 = pair0;
+    q.chunk0 = chunk0;
+    q.lists = d_lists + list_off[i];
+    q.counts = d_counts + cnt_off[i];
+    q.bits = static_cast<uint32_t*>(at(o_bits));
+    q.cnt = static_cast<int*>(at(o_cnt));
+    q.key = static_cast<unsigned long long*>(at(o_key));
+    q.order = static_cast<int*>(at(o_order));
+    q.cand = static_cast<int*>(at(o_cand));
+    q.ncand = static_cast<int*>(at(o_ncand));
+    q.partner = static_cast<int*>(at(o_partner));
+    q.pos = static_cast<int*>(at(o_pos));
+    q.choice = static_cast<int*>(at(o_choice));
+    q.pairs = static_cast<int4*>(at(o_pairs));
+    q.npairs = d_np + 1;  // this batch's count, read back below
+    q.ulist = static_cast<int*>(at(o_ulist));
+    q.uflag = static_cast<uint8_t*>(at(o_uflag));
+    q.ucount = static_cast<int*>(at(o_ucount));
+    q.cbase = static_cast<int*>(at(o_cbase));
+    q.items = static_cast<int4*>(at(o_items));
+    q.total = d_total;
+    q.chunks_end = d_total + 2;
+    q.sigma = static_cast<int*>(at(o_sigma)) + sg_off[i];
+    q.pmax = static_cast<unsigned long long*>(at(o_pmax));
+    q.phisl = static_cast<uint8_t*>(at(o_phisl));
+    err = cfgmm::split_pair_prepare_batch(q, s);
+    int got[2] = {0, 0};
+    if (err == cudaSuccess) err = cudaMemcpyAsync(&got[0], d_np + 1, 4, cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess)
+      err = cudaMemcpyAsync(&got[1], d_total + 2, 4, cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    pair0 += got[0];
+    chunk0 = got[1];
+    hb[i] = cfgmm::PairBatch{b.ao_lhs, b.rhos, q.sigma, b.stride_grid, int(b.ngrid), int(b.nset)};
+  }
+  if (err != cudaSuccess) return cuda_fail(err, "split plan setup");
+  const int P = pair0;
+  if (size_t(chunk0) > chunk_bound) return fail(CFGMM_ERR_CUDA, "split plan: chunk bound exceeded");
+  // ---- work list: matrix-major (one D in L2 at a time), heaviest first ----
+  int nitems = 0;
+  err = cudaMemcpyAsync(&nitems, d_total, 4, cudaMemcpyDeviceToHost, s);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+  if (err != cudaSuccess) return cuda_fail(err, "split plan work list");
+  if (size_t(nitems) > item_bound) return fail(CFGMM_ERR_CUDA, "split plan: item bound exceeded");
+  std::vector<int4> items(size_t(std::max(nitems, 0)));
+  std::vector<int> ucount(size_t(std::max(P, 1)));
+  if (err == cudaSuccess && nitems > 0)
+    err = cudaMemcpyAsync(items.data(), at(o_items), size_t(nitems) * sizeof(int4),
+                          cudaMemcpyDeviceToHost, s);
+  if (err == cudaSuccess && P > 0)
+    err = cudaMemcpyAsync(ucount.data(), at(o_ucount), size_t(P) * 4, cudaMemcpyDeviceToHost, s);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+  if (err != cudaSuccess) return cuda_fail(err, "split plan work list");
+  auto weight = [&](const int4& it) {
+    const int nu = ucount[it.x];
+    return (nu + TK - 1) / TK - (it.y * tn) / TK;
+  };
+  std::stable_sort(items.begin(), items.end(), [&](const int4& x, const int4& y) {
+    if (x.z != y.z) return x.z < y.z;
+    return weight(x) > weight(y);
+  });
+  // partial row tiles: exact, from the unions
+  std::vector<int> poff(size_t(P) + 1, 0);
+  for (int q = 0; q < P; ++q) poff[q + 1] = poff[q] + (ucount[q] + tn - 1) / tn;
+  const size_t part_bytes = size_t(poff[P]) * nset_max * PT * sizeof(double);
+  err = cudaMallocAsync(&plan->mem3, std::max<size_t>(part_bytes, 256), s);
+  if (err != cudaSuccess) return cuda_fail(err, "cudaMalloc(split plan partials)");
+  const int np_all = P;
+  if (nitems > 0)
+    err = cudaMemcpyAsync(at(o_items), items.data(), size_t(nitems) * sizeof(int4),
+                          cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(at(o_poff), poff.data(), poff.size() * 4, cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(d_np, &np_all, 4, cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(at(o_batch), hb.data(), nbatch * sizeof(cfgmm::PairBatch),
+                          cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(s);  // host vectors die on return
+  if (err != cudaSuccess) return cuda_fail(err, "split plan upload");
+
+  plan->split = true;
+  plan->pair = true;
+  plan->nsl = nsl;
+  plan->dms = dms;
+  plan->stride_ao = stride_ao;
+  plan->nao = int(nao);
+  plan->nset_max = int(nset_max);
+  plan->nitems = nitems;
+  plan->npairs = P;
+  plan->d_npairs = d_np;
+  cfgmm::PairArgs& a = plan->pargs;
+  a.dsl = static_cast<const uint2*>(at(o_dsl));
+  a.tau = static_cast<const int*>(at(o_tau));
+  a.phisl = static_cast<const uint8_t*>(at(o_phisl));
+  a.items = static_cast<const int4*>(at(o_items));
+  a.total = d_total;
+  a.pairs = static_cast<const int4*>(at(o_pairs));
+  a.ucount = static_cast<const int*>(at(o_ucount));
+  a.ulist = static_cast<const int*>(at(o_ulist));
+  a.uflag = static_cast<const uint8_t*>(at(o_uflag));
+  a.cbase = static_cast<const int*>(at(o_cbase));
+  a.batches = static_cast<const cfgmm::PairBatch*>(at(o_batch));
+  a.partial = static_cast<double*>(plan->mem3);
+  a.poff = static_cast<const int*>(at(o_poff));
+  a.nao = int(nao);
+  a.blk = int(blksize);
+  a.gsub = gsub;
+  a.max_t = int((nao + tn - 1) / tn);
+  a.nset_max = int(nset_max);
+  a.wait_ns = 0;  // the default bound
+  a.inject = 0;
+  // total[1]: the asymmetry flag (the half contraction also needs one phi array per batch)
+  a.asym = cfgmm::aodm_sym_enabled() && same_phi(batches, nbatch) ? d_total + 1 : nullptr;
+
+  // ---- capture the run ----
+  if (!(flags & CFGMM_PLAN_NO_GRAPH)) {
+    err = cfgmm::split_pair_launch_main(a, nsl, s, true);  // attributes outside the capture
+    if (err == cudaSuccess)
+      err = capture(plan, [&](cudaStream_t cs) { return pair_run_on(plan, cs); });
+    if (err != cudaSuccess) return cuda_fail(err, "graph capture");
+  }
+  char buf[512];
+  std::snprintf(buf, sizeof(buf),
+                "{\"precision\":\"split\",\"form\":\"pair\",\"digits\":%d,\"batches\":%zu,"
+                "\"items\":%d,\"block_tiles\":%zu,\"pairs\":%d,\"phi_chunks\":%d,"
+                "\"flops\":%.6e,\"config\":{\"row_tile\":%d},\"graph\":%s,\"tuning\":\"none\"}",
+                nsl, nbatch, nitems, nbg_tot, P, chunk0, plan->flops, tn,
+                plan->exec ? "true" : "false");
+  plan->info = buf;
+  return CFGMM_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -421,6 +668,7 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
   auto cleanup = [&](int rc) {
     if (plan->mem) cudaFree(plan->mem);
     if (plan->mem2) cudaFree(plan->mem2);
+    if (plan->mem3) cudaFree(plan->mem3);
     delete plan;
     return rc;
   };
@@ -475,8 +723,12 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
       plan->flops += double(batches[i].nset) * (2.0 * nb * nb + 2.0 * nb) * w;
     }
   if (precision == CFGMM_PREC_OZAKI_INT8) {
-    const int rc = build_split(plan, batches, nbatch, dms, stride_ao, nao, nset_max, blksize, flags,
-                               d_lists, d_counts, list_off, cnt_off, nblk, counts, s);
+    const int rc =
+        cfgmm::split_pair_form()
+            ? build_split_pair(plan, batches, nbatch, dms, stride_ao, nao, nset_max, blksize,
+                               flags, d_lists, d_counts, list_off, cnt_off, nblk, counts, s)
+            : build_split(plan, batches, nbatch, dms, stride_ao, nao, nset_max, blksize, flags,
+                          d_lists, d_counts, list_off, cnt_off, nblk, counts, s);
     if (rc != CFGMM_OK) return cleanup(rc);
     *out = plan;
     return CFGMM_OK;
@@ -689,6 +941,7 @@ int cfgmm_aodm_plan_destroy(cfgmm_aodm_plan* plan) {
   // cudaFree waits for work still using the memory
   if (plan->mem) cudaFree(plan->mem);
   if (plan->mem2) cudaFree(plan->mem2);
+  if (plan->mem3) cudaFree(plan->mem3);
   delete plan;
   return CFGMM_OK;
 }
@@ -704,6 +957,7 @@ int aodm_plan_release_idle(cfgmm_aodm_plan* plan, cudaStream_t stream) {
   if (plan->exec) cudaGraphExecDestroy(plan->exec);
   if (plan->mem) cudaFreeAsync(plan->mem, stream);
   if (plan->mem2) cudaFreeAsync(plan->mem2, stream);
+  if (plan->mem3) cudaFreeAsync(plan->mem3, stream);
   delete plan;
   return CFGMM_OK;
 }

@@ -442,8 +442,9 @@ __device__ __forceinline__ double sym_factor(int r, int c) {
 }
 
 // Bounded wait whose outcome is the same for every lane of the warp.
-__device__ __forceinline__ bool warp_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
-  const bool ok = tc::mbar_wait(bar, parity, err, code);
+__device__ __forceinline__ bool warp_wait(uint64_t* bar, uint32_t parity, int* err, int code,
+                                          uint64_t lim) {
+  const bool ok = tc::mbar_wait(bar, parity, err, code, false, lim);
   return __all_sync(0xffffffffu, ok);
 }
 }  // namespace pipe
@@ -465,6 +466,7 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
   uint64_t* epi = iempty + RING;  // [2]
   int* ring = reinterpret_cast<int*>(epi + 2);
   int* err = &g_aodm_error;
+  const uint64_t lim = p.wait_ns ? p.wait_ns : tc::kWaitLimitNs;
 
   const int tid = threadIdx.x, lane = tid & 31;
   const int set0 = blockIdx.y * NS;
@@ -496,13 +498,14 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
       if (tid == 0) {  // fetch the next item for every warp of the CTA
         int it = total;
         if (*reinterpret_cast<volatile int*>(err) == 0 &&
-            (n < RING || tc::mbar_wait(&iempty[slot], ((n / RING) - 1) & 1, err, kErrItemEmpty)))
+            (n < RING ||
+             tc::mbar_wait(&iempty[slot], ((n / RING) - 1) & 1, err, kErrItemEmpty, false, lim)))
           it = min(atomicAdd(counter, 1), total);
         ring[slot] = it;
         tc::mbar_arrive(&ifull[slot]);
       }
       int it = total;
-      if (warp_wait(&ifull[slot], (n / RING) & 1, err, kErrItemFull)) it = ring[slot];
+      if (warp_wait(&ifull[slot], (n / RING) & 1, err, kErrItemFull, lim)) it = ring[slot];
       it = __shfl_sync(0xffffffffu, it, 0);
       __syncwarp();
       if (lane == 0) tc::mbar_arrive(&iempty[slot]);
@@ -528,7 +531,7 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
         vnext = t.I[min(k + TK, t.nb - 1)];
         const int stage = fill % PSTAGES;
         if (fill >= PSTAGES &&
-            !warp_wait(&empty[stage], ((fill / PSTAGES) - 1) & 1, err, kErrStageEmpty)) {
+            !warp_wait(&empty[stage], ((fill / PSTAGES) - 1) & 1, err, kErrStageEmpty, lim)) {
           cp_async_arrive_noinc(&full[stage]);  // keep the arrival count of the phase whole
           break;
         }
@@ -560,8 +563,11 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
           }
         }
         cp_async_arrive_noinc(&full[stage]);
+        // test hook: the first stage's last arrival (the TMA's expect_tx, or
+        // its stand-in) is never made, so the consumers' bounded wait runs out
+        const bool withhold = p.inject && fill == 0;
         if (t.B->rhs_tma) {
-          if (tid < 32) {
+          if (tid < 32 && !withhold) {
             // ao_rhs rows of the stage columns, from the lanes that gather them
             // (lane j of warp 0 holds column j; D is zero past the list's end)
             int rows[TK];
@@ -575,7 +581,7 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
                             rows[4 * j + 1], rows[4 * j + 2], rows[4 * j + 3]);
             }
           }
-        } else if (tid == 0) {
+        } else if (tid == 0 && !withhold) {
           tc::mbar_arrive(&full[stage]);  // the arrival the TMA's expect_tx makes otherwise
         }
       }
@@ -584,7 +590,7 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
     if (tid == 0) {
       // let every TMA this thread issued land before the CTA exits
       for (uint32_t f = fill > PSTAGES ? fill - PSTAGES : 0; f < fill; ++f)
-        tc::mbar_wait(&full[f % PSTAGES], (f / PSTAGES) & 1, err, kErrTeardown, true);
+        tc::mbar_wait(&full[f % PSTAGES], (f / PSTAGES) & 1, err, kErrTeardown, true, lim);
     }
   } else {
     // ------------------------------- consumers -------------------------------
@@ -596,7 +602,7 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
     for (int n = 0;; ++n) {
       const int slot = n % RING;
       int it = total;
-      if (warp_wait(&ifull[slot], (n / RING) & 1, err, kErrItemFull)) it = ring[slot];
+      if (warp_wait(&ifull[slot], (n / RING) & 1, err, kErrItemFull, lim)) it = ring[slot];
       it = __shfl_sync(0xffffffffu, it, 0);
       __syncwarp();
       if (lane == 0) tc::mbar_arrive(&iempty[slot]);
@@ -636,7 +642,7 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
       bool ok = true;
       for (int kc = kc0; kc < kchunks; ++kc, ++use) {
         const int stage = use % PSTAGES;
-        if (!warp_wait(&full[stage], (use / PSTAGES) & 1, err, kErrStageFull)) {
+        if (!warp_wait(&full[stage], (use / PSTAGES) & 1, err, kErrStageFull, lim)) {
           ok = false;
           break;
         }
@@ -720,7 +726,7 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
       tc::mbar_arrive(&epi[n & 1]);
       // The buffer is written again two items later, after every consumer has
       // passed the next item's epilogue barrier, i.e. finished reading this one.
-      if (!warp_wait(&epi[n & 1], (n >> 1) & 1, err, kErrEpilogue)) break;
+      if (!warp_wait(&epi[n & 1], (n >> 1) & 1, err, kErrEpilogue, lim)) break;
       const size_t pslot = t.B->partial_off + size_t(t.bg) * p.max_utiles + t.utile;
       for (int i = ct; i < t.ns * TG; i += NCONS) {
         const int s = i / TG, j = i % TG;
@@ -906,6 +912,33 @@ cudaError_t aodm_read_error(int* code) {
   return cudaMemcpyFromSymbol(code, g_aodm_error, sizeof(int));
 }
 
+cudaError_t aodm_reset_error(cudaStream_t stream) {
+  static const int zero = 0;
+  return cudaMemcpyToSymbolAsync(g_aodm_error, &zero, sizeof(int), 0, cudaMemcpyHostToDevice,
+                                 stream);
+}
+
+namespace {
+struct WaitInjection {
+  bool armed[2] = {false, false};
+  unsigned long long ns = 0;
+};
+thread_local WaitInjection g_wait_injection;
+}  // namespace
+
+void arm_wait_injection(int kind, unsigned long long wait_ns) {
+  if (kind < 0 || kind > 1) return;
+  g_wait_injection.armed[kind] = true;
+  g_wait_injection.ns = wait_ns;
+}
+
+bool take_wait_injection(int kind, unsigned long long* wait_ns) {
+  if (kind < 0 || kind > 1 || !g_wait_injection.armed[kind]) return false;
+  g_wait_injection.armed[kind] = false;
+  *wait_ns = g_wait_injection.ns;
+  return true;
+}
+
 int aodm_groups(const AodmConfig& cfg, int nset_max) {
   return (nset_max + cfg.ns - 1) / cfg.ns;
 }
@@ -1033,6 +1066,11 @@ cudaError_t aodmao2rho_fp64(double* rhos, const double* dms, const double* ao_lh
       if ((err = aodm_launch_sym_check(dms, stride_ao, nao, nset, counters + ngroups + 1,
                                        stream)) != cudaSuccess)
         return err;
+    }
+    unsigned long long ns = 0;
+    if (take_wait_injection(0, &ns)) {  // cfgmm_test_arm_wait_timeout
+      a.inject = 1;
+      a.wait_ns = ns;
     }
     err = aodm_launch_pipe(a, cfg.ns, map, stream);
   }

@@ -37,7 +37,17 @@ struct AodmArgs {
   int ngroups;
   const int* asym;              // null, or counters + ngroups + 1: 0 when every D_s is symmetric
   double* partial;              // [slot][nset_max][64]
+  unsigned long long wait_ns;   // bound of the pipelined kernel's waits (0: the default 2 s)
+  int inject;                   // test hook: the pipelined kernel's first stage is never published
 };
+
+// Test hook of the failure detection (cfgmm_test_arm_wait_timeout): arms the
+// calling thread's next contraction of `kind` (0: the FP64 pipelined kernel,
+// 1: the split pair kernel) to run with waits bounded by `wait_ns` and one
+// producer that never publishes its first stage.  take_wait_injection returns
+// whether the next launch of `kind` is armed (and disarms it).
+void arm_wait_injection(int kind, unsigned long long wait_ns);
+bool take_wait_injection(int kind, unsigned long long* wait_ns);
 
 // Tile configuration of the main kernel (the autotuner's search space):
 // `ns` density matrices share one ao_rhs tile (1..3), `tk` compacted AOs per
@@ -99,6 +109,7 @@ cudaError_t aodm_launch_pipe(const AodmArgs& a, int ns, const CUtensorMap& map,
 // Code of the first timed-out wait of the pipelined kernel since the last
 // call's setup kernel (0: none).
 cudaError_t aodm_read_error(int* code);
+cudaError_t aodm_reset_error(cudaStream_t stream);
 
 // Symmetric-D mode of the pipelined form: aodm_launch_sym_check sets
 // *asym = 1 unless every D_s (s < nset) equals its transpose bit for bit

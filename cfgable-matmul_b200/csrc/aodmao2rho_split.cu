@@ -760,8 +760,22 @@ Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk) {
 
 }  // namespace
 
+// Which form a call runs: the row form of this file (one block tile, 128
+// compacted rows per item) unless CFGMM_SPLIT_FORM=pair selects the pair form
+// (two alike block tiles per item, aodmao2rho_split_pair.cu).  Read on every
+// call; the workspace covers both.
+bool split_pair_form() {
+  const char* e = std::getenv("CFGMM_SPLIT_FORM");
+  return e && e[0] == 'p';
+}
+
 size_t aodmao2rho_split_workspace(size_t nao, size_t ngrid, size_t nset, size_t blk) {
-  return layout(nao, ngrid, nset, blk).bytes;
+  size_t w = layout(nao, ngrid, nset, blk).bytes;
+  for (int nsl = 6; nsl <= 7; ++nsl) {
+    const size_t wp = aodmao2rho_split_pair_workspace(nao, ngrid, nset, blk, nsl);
+    w = wp > w ? wp : w;
+  }
+  return w;
 }
 
 cudaError_t aodmao2rho_split(double* rhos, const double* dms, const double* ao_lhs,
@@ -769,6 +783,9 @@ cudaError_t aodmao2rho_split(double* rhos, const double* dms, const double* ao_l
                              int ngrid, int nset, const uint8_t* tab, size_t ldtab, int blk,
                              void* workspace, cudaStream_t stream) {
   if (nao <= 0 || ngrid <= 0 || nset <= 0) return cudaSuccess;
+  if (split_pair_form())
+    return aodmao2rho_split_pair(rhos, dms, ao_lhs, ao_rhs, stride_ao, stride_grid, nao, ngrid,
+                                 nset, tab, ldtab, blk, split_pair_digits(), workspace, stream);
   const int nblk = (ngrid + blk - 1) / blk;
   const int gsub = (blk + TG - 1) / TG;
   const int nbg = nblk * gsub;
@@ -876,12 +893,16 @@ int split_epi_parts() { return EPI_PARTS; }
 
 cudaError_t aodmao2rho_split_reset_error(cudaStream_t stream) {
   static const int zero = 0;
-  return cudaMemcpyToSymbolAsync(g_split_error, &zero, sizeof(int), 0, cudaMemcpyHostToDevice,
-                                 stream);
+  cudaError_t err = cudaMemcpyToSymbolAsync(g_split_error, &zero, sizeof(int), 0,
+                                            cudaMemcpyHostToDevice, stream);
+  return err != cudaSuccess ? err : aodmao2rho_split_pair_reset_error(stream);
 }
 
+// Either form's first timed-out wait (0: none).
 cudaError_t aodmao2rho_split_read_error(int* code) {
-  return cudaMemcpyFromSymbol(code, g_split_error, sizeof(int));
+  cudaError_t err = cudaMemcpyFromSymbol(code, g_split_error, sizeof(int));
+  if (err != cudaSuccess || *code != 0) return err;
+  return aodmao2rho_split_pair_read_error(code);
 }
 
 }  // namespace cfgmm

@@ -75,6 +75,92 @@ int split_chunk();         // compacted AOs per chunk (32)
 size_t split_chunk_bytes();  // bytes of one chunk's phi digit tiles
 int split_epi_parts();     // partial-sum groups per (tile, row tile, matrix)
 
+// ---- the pair form: two grid block tiles with alike active lists per item ----
+// (aodmao2rho_split_pair.cu)  NSL = 7 digits (about 2^-51 of
+// sum_v |D_uv||phi_vg|) or 6 (about 2^-43, fewer MMAs and larger tiles).
+
+// One grid batch of the pair form (device pointers).
+struct PairBatch {
+  const double* ao_lhs;
+  double* rhos;        // (nset, stride_grid)
+  const int* sigma;    // [ngrid] point scales
+  size_t stride_grid;
+  int ngrid;
+  int nset;
+};
+
+// Arguments of the pair form's persistent kernel and reduction.
+struct PairArgs {
+  const uint2* dsl;       // D digits [s][u][v], 8 bytes each
+  const int* tau;         // row scales [s][u]
+  const uint8_t* phisl;   // phi digit tiles [chunk][NSL][128 x 32]
+  const int4* items;      // (pair, row tile, s, batch)
+  const int* total;       // [0] items
+  const int4* pairs;      // (lo tile, hi tile or -1, batch, 0), tiles local to the batch
+  const int* ucount;      // [pair] union size
+  const int* ulist;       // [pair][nao] union AOs, ascending
+  const uint8_t* uflag;   // [pair][nao] bit 0 / 1: active in the lo / hi tile's block
+  const int* cbase;       // [pair] first phi chunk
+  const PairBatch* batches;  // device array, or null: `one`
+  PairBatch one;
+  double* partial;        // [poff[pair] + row tile][nset_max][128]
+  const int* poff;        // [pair] first partial row tile, or null: pair * max_t
+  int nao, blk, gsub, max_t, nset_max;
+  const int* asym;        // null, or 0 when every D_s is symmetric (half contraction)
+  unsigned long long wait_ns;  // bound of every wait in the kernel (0: the default 2 s)
+  int inject;             // test hook: nonzero = the first phi stage is never published
+};
+
+// Device pointers of the preparation of one batch (pairing, unions, work
+// list, phi tiles); see split_pair_prepare_batch.
+struct PairPrep {
+  const uint8_t* tab;
+  size_t ldtab;
+  const double* ao_rhs;
+  size_t stride_grid;
+  int nao, ngrid, blk, nset, nsl, batch, pair0, chunk0;
+  const int* lists;       // [nblk][nao] active AOs of each block, built
+  const int* counts;      // [nblk]
+  uint32_t* bits;         // scratch [nbg][ceil(nao/32)]
+  int* cnt;               // scratch [nbg]
+  unsigned long long* key;  // scratch [nbg]
+  int *order, *cand, *ncand, *partner, *pos, *choice;  // scratch
+  int4* pairs;            // out: pairs pair0 ..
+  int* npairs;            // out: [0] pairs of this batch
+  int* ulist;             // out: [pair][nao]
+  uint8_t* uflag;         // out: [pair][nao]
+  int* ucount;            // out: [pair]
+  int* cbase;             // out: [pair]
+  int4* items;            // out: appended at *total
+  int* total;             // in/out: items so far
+  int* chunks_end;        // out: chunk0 + this batch's chunks
+  int* sigma;             // out: [ngrid]
+  unsigned long long* pmax;  // scratch [ngrid]
+  uint8_t* phisl;         // out: phi tiles from chunk0
+};
+
+size_t aodmao2rho_split_pair_workspace(size_t nao, size_t ngrid, size_t nset, size_t blk,
+                                       int nsl);
+// The single-call contraction in the pair form (same contract as
+// aodmao2rho_split); inject / wait_ns: test hooks (0 = off / the default bound).
+cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double* ao_lhs,
+                                  const double* ao_rhs, size_t stride_ao, size_t stride_grid,
+                                  int nao, int ngrid, int nset, const uint8_t* tab, size_t ldtab,
+                                  int blk, int nsl, void* workspace, cudaStream_t stream,
+                                  int inject = 0, unsigned long long wait_ns = 0);
+cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream);
+cudaError_t split_pair_prepare_d(const double* dms, size_t stride_ao, int nao, int nset, int nsl,
+                                 uint2* dsl, int* tau, cudaStream_t stream, const int* asym);
+cudaError_t split_pair_launch_main(const PairArgs& a, int nsl, cudaStream_t stream,
+                                   bool attrs_only = false);
+cudaError_t split_pair_launch_reduce(const PairArgs& a, int nsl, const int* npairs, int pair0,
+                                     int max_pairs, cudaStream_t stream);
+bool split_pair_form();            // single calls and plans run the pair form (CFGMM_SPLIT_FORM)
+int split_pair_row_tile(int nsl);  // D rows per item (the MMA N): 80 (6 digits), 64 (7)
+int split_pair_digits();           // digit count (CFGMM_SPLIT_DIGITS, default 7), read per call
+cudaError_t aodmao2rho_split_pair_reset_error(cudaStream_t stream);
+cudaError_t aodmao2rho_split_pair_read_error(int* code);
+
 // Sticky per-device error word of the split kernel's bounded waits.
 cudaError_t aodmao2rho_split_reset_error(cudaStream_t stream);
 cudaError_t aodmao2rho_split_read_error(int* code);

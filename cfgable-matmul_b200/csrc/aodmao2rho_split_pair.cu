@@ -1,0 +1,1310 @@
+// aodmao2rho_split_pair.cu -- the masked AO-DM-AO contraction in split
+// precision with two grid block tiles per work item.
+//
+// Arithmetic: the slice form of the Ozaki scheme (Ozaki, Ogita, Oishi and Rump
+// 2012), restated.  Every row u of D_s is scaled by 2^tau_u and every grid
+// point g of phi by 2^sigma_g so that the scaled values are below 2^6; each is
+// written as NSL signed base-256 digits x' = sum_{j<NSL} x_j 2^(-8j) read off
+// the bytes of round(x' 2^(8(NSL-1))) (digits_of below).  The digit products
+// whose levels add up to L = i + j <= NSL-1 are summed EXACTLY in one INT32
+// TMEM accumulator per level (INT8 tcgen05.mma, NSL(NSL+1)/2 MMAs per chunk):
+//   S_L[g][u] = sum_{i+j=L} sum_v phi_j(v,g) d_i(u,v),
+// and X[u][g] = 2^-(tau_u + sigma_g) sum_L 2^(-8L) S_L[g][u] in FP64.  With
+// NSL = 7 the dropped levels weigh about 2^-51 of sum_v |D_uv| |phi_vg|, with
+// NSL = 6 about 2^-43.  |S_L| <= NSL 2^14 nao keeps the INT32 sums exact for
+// nao <= 16384.
+//
+// Work items.  The contraction follows aodmao2rho_loop_parallel
+// (src/impl_aodmao2rho.rs:171-244): per grid block b the active AO list I(b)
+// (the reference's compaction, impl_matmul_non0tab.rs:118-129) and
+// rho[s][g] += sum_{u,v in I(b)} phi[u][g] D_s[u][v] phi[v][g].  Here one item
+// covers TWO 64-point block tiles whose active lists are alike (atom-centred
+// grids put many blocks around one centre): the MMA's M = 128 rows are the
+// points of both tiles, K runs over the union U of the two lists, N = TN rows
+// of D (TN = 80 for NSL = 6, 64 for NSL = 7: NSL x TN <= 512 TMEM columns).
+// Where an AO of U is inactive in a point's block the point's phi digits are
+// zero there (in the tiles below) and the AO takes no part in the point's
+// epilogue, so each point's sum runs over exactly its own block's list: the
+// integer sums are unchanged by the zero digits.  Every D element gathered
+// from L2 then serves 128 points instead of 64.  The pairing is a matching on
+// the mask, on the device: tiles sorted by a min-hash signature of their
+// lists, each tile scored against its kWin neighbours on either side by the
+// MMA work that pairing saves (|I_a|^2 + |I_b|^2 - |I_a u I_b|^2), mutual best
+// candidates paired; tiles without a profitable partner run alone (the other
+// half of the lanes idle).
+//
+// Kernels (one call):
+//   pair_sig      per block tile: bit set of I(b) and a 64-bit min-hash key
+//   pair_sort     one CTA: tiles in key order (bitonic sort in shared memory)
+//   pair_scores   per tile: the profitable neighbours, best first
+//   pair_match    one CTA: mutual-best rounds -> pairs and singles
+//   pair_union    per pair: the union list U and per-AO membership flags
+//   pair_build    one CTA: chunk offsets and the work list (pair, row tile,
+//                 DM), heaviest items first
+//   pair_phi_max, pair_phi_tiles  point scales and the phi digit tiles of
+//                 every (pair, chunk of 32 union AOs): NSL planes of 128 rows
+//                 (points) x 32 bytes in the UMMA 32-byte-swizzled K-major
+//                 layout, so one bulk copy moves a chunk
+//   pair_d_digits D digits (8 bytes per element) and row scales
+//   pair_main     persistent, 14 warps: 12 warps gather the D digits of TN
+//                 rows x 32 union columns in three groups that take turns by
+//                 chunk and later run the epilogue; 1 warp issues the MMAs;
+//                 1 warp bulk-loads the phi tiles.  The epilogue reads each
+//                 point's TMEM row (lane = point), rebuilds X in FP64, weights
+//                 it with phi_lhs and sums over the row's AOs -- no
+//                 cross-lane reduction; X never leaves the SM.
+//   pair_reduce   adds the row tiles' partial sums of each point in a fixed
+//                 order (deterministic).
+// Every mbarrier wait is bounded (tcgen05.cuh).
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cstdint>
+#include <cstdlib>
+
+#include "aodmao2rho_fp64.cuh"
+#include "aodmao2rho_split.cuh"
+#include "side_stream.cuh"
+#include "tcgen05.cuh"
+
+namespace cfgmm {
+namespace {
+
+constexpr int PT = 128;   // points per item: MMA M, TMEM lanes
+constexpr int HT = 64;    // points per block tile (half an item)
+constexpr int TK = 32;    // union AOs per chunk: one INT8 MMA K step
+constexpr int NG = 3;     // gather groups of four warps
+constexpr int GW = 4 * NG;
+constexpr int THREADS = 32 * (GW + 2);
+constexpr int kStages = 4;        // pipeline depth (at least NG: see the row form)
+constexpr int kBadExp = INT_MAX;  // scale of a row / point holding Inf or NaN
+constexpr int kWin = 32;          // pairing candidates on each side in key order
+constexpr int kSortMax = 4096;    // tiles sorted in shared memory (more: caller's order)
+constexpr int kRounds = 8;        // mutual-best matching rounds
+static_assert(kStages >= NG, "a group's parity wait needs at least NG stages");
+
+template <int NSL>
+struct Cfg {
+  static constexpr int TN = NSL == 6 ? 80 : 64;  // D rows per item (MMA N)
+  static constexpr uint32_t A_SLICE = PT * TK;   // one phi digit plane: 4096 B
+  static constexpr uint32_t B_SLICE = TN * TK;   // one D digit plane
+  static constexpr uint32_t A_STAGE = NSL * A_SLICE;
+  static constexpr uint32_t B_STAGE = NSL * B_SLICE;
+  static constexpr uint32_t STAGE = A_STAGE + B_STAGE;
+  static constexpr int WROWS = TN / 4;     // D rows per gather warp
+  static constexpr int STEPS = WROWS / 4;  // four rows per step
+  static constexpr int OCTETS = TN / 8;    // TMEM column octets of one level
+  static_assert(NSL * TN <= 512, "level accumulators exceed the TMEM columns");
+  static_assert(STAGE % 256 == 0 && A_STAGE % 256 == 0, "32-byte swizzle atoms");
+  static_assert(WROWS % 4 == 0 && (OCTETS + NG - 1) / NG * 8 <= 32, "epilogue columns per group");
+};
+
+__device__ int g_pair_error;
+
+__device__ __forceinline__ int exp_for(double amax) {  // 2^6 > amax * 2^exp
+  if (!(amax <= 1.7976931348623157e308)) return kBadExp;
+  if (amax == 0.0) return 0;
+  int E;
+  frexp(amax, &E);
+  return 6 - E;
+}
+
+__device__ __forceinline__ double pow2(int k) {  // k in [-1022, 1023]
+  return __longlong_as_double(static_cast<long long>(k + 1023) << 52);
+}
+
+// The NSL digits of x * 2^e (|x * 2^e| < 2^6), digit j (j = 0 leading) in
+// byte j of the returned 8 bytes, the rest zero.  X = round(x 2^(e + 8(NSL-1)))
+// plus the bias 128 * sum_{j < NSL-1} 256^j makes every low byte the unsigned
+// form of a balanced digit in [-128, 127] (flipping bit 7 turns it into the
+// signed byte), and leaves the leading digit, in [-64, 64], above them:
+//   x 2^e = sum_j d_j 2^(-8j) + r 2^(-8(NSL-1)),  |r| <= 1/2.
+// The scaling is done in two exact halves.
+template <int NSL>
+__device__ __forceinline__ uint2 digits_of(double x, int e) {
+  static_assert(NSL == 6 || NSL == 7, "6 or 7 digits");
+  constexpr int SH = 8 * (NSL - 1);
+  constexpr long long BIAS = NSL == 7 ? 0x808080808080LL : 0x8080808080LL;
+  const int k = e + SH;
+  const int k1 = k / 2;
+  const long long X = __double2ll_rn(x * pow2(k1) * pow2(k - k1));
+  const unsigned long long Z = static_cast<unsigned long long>(X + BIAS) ^
+                               static_cast<unsigned long long>(BIAS);
+  const uint32_t lo = static_cast<uint32_t>(Z), hi = static_cast<uint32_t>(Z >> 32);
+  if constexpr (NSL == 7) {
+    // hi = d2 d1 d0 -, lo = d6 d5 d4 d3 (byte 0 first)
+    return make_uint2(__byte_perm(hi, lo, 0x7012), __byte_perm(lo, 0u, 0x4012));
+  } else {
+    // hi = d1 d0 - -, lo = d5 d4 d3 d2
+    return make_uint2(__byte_perm(hi, lo, 0x6701), __byte_perm(lo, 0u, 0x4401));
+  }
+}
+
+// 4x4 byte transpose: out_i holds byte i of w0..w3 (w_t in byte t).
+__device__ __forceinline__ void transpose4(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3,
+                                           uint32_t& o0, uint32_t& o1, uint32_t& o2,
+                                           uint32_t& o3) {
+  const uint32_t a = __byte_perm(w0, w1, 0x5140);
+  const uint32_t b = __byte_perm(w0, w1, 0x7362);
+  const uint32_t c = __byte_perm(w2, w3, 0x5140);
+  const uint32_t d = __byte_perm(w2, w3, 0x7362);
+  o0 = __byte_perm(a, c, 0x5410);
+  o1 = __byte_perm(a, c, 0x7632);
+  o2 = __byte_perm(b, d, 0x5410);
+  o3 = __byte_perm(b, d, 0x7632);
+}
+
+// X' = sum_L 2^(-8L) S_L, combined exactly in 64-bit integers, then one FMA.
+template <int NSL>
+__device__ __forceinline__ double combine_levels(const uint32_t (&v)[NSL]) {
+  const long long hi = (static_cast<long long>(int(v[0])) << 16) +
+                       (static_cast<long long>(int(v[1])) << 8) + int(v[2]);
+  if constexpr (NSL == 7) {
+    const long long lo = (static_cast<long long>(int(v[3])) << 24) +
+                         (static_cast<long long>(int(v[4])) << 16) +
+                         (static_cast<long long>(int(v[5])) << 8) + int(v[6]);
+    return fma(double(lo), 0x1p-48, double(hi) * 0x1p-16);
+  } else {
+    const long long lo = (static_cast<long long>(int(v[3])) << 16) +
+                         (static_cast<long long>(int(v[4])) << 8) + int(v[5]);
+    return fma(double(lo), 0x1p-40, double(hi) * 0x1p-16);
+  }
+}
+
+// Point range of block tile bg (local to its batch): [*g0, *gend).
+__device__ __forceinline__ void tile_points(int bg, int blk, int gsub, int ngrid, int* g0,
+                                            int* gend) {
+  const int b = bg / gsub, gt = bg % gsub;
+  *g0 = b * blk + gt * HT;
+  *gend = min(min((b + 1) * blk, ngrid), *g0 + HT);
+}
+
+__device__ __forceinline__ const PairBatch& batch_of(const PairArgs& p, int w) {
+  return p.batches ? p.batches[w] : p.one;
+}
+
+// ---------------------------------------------------------------------------
+// pairing
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t mix32(uint32_t x, uint32_t seed) {
+  x ^= seed;
+  x *= 0x9E3779B1u;
+  x ^= x >> 15;
+  x *= 0x85EBCA77u;
+  x ^= x >> 13;
+  return x;
+}
+
+// Per block tile: bits[bg][w] (bit u%32 of word u/32: AO u active in the
+// tile's block), count, and the min-hash key (two hashes; empty -> ~0).
+__global__ void __launch_bounds__(256)
+pair_sig(const uint8_t* __restrict__ tab, size_t ldtab, int nao, int nbg, int gsub, int nwords,
+         uint32_t* __restrict__ bits, int* __restrict__ cnt, unsigned long long* __restrict__ key) {
+  const int bg = blockIdx.x;
+  if (bg >= nbg) return;
+  const int b = bg / gsub;
+  const int tid = threadIdx.x, lane = tid & 31;
+  uint32_t h1 = 0xffffffffu, h2 = 0xffffffffu;
+  int n = 0;
+  for (int u0 = 0; u0 < nao; u0 += 256) {
+    const int u = u0 + tid;
+    const bool on = u < nao && tab[size_t(u) * ldtab + b] != 0;
+    const uint32_t bal = __ballot_sync(0xffffffffu, on);
+    const int wbase = u0 + (tid & ~31);
+    if (lane == 0 && wbase < nao) bits[size_t(bg) * nwords + wbase / 32] = bal;
+    n += on;
+    if (on) {
+      h1 = min(h1, mix32(uint32_t(u), 0x2545F491u));
+      h2 = min(h2, mix32(uint32_t(u), 0x6C8E9CF5u));
+    }
+  }
+  __shared__ uint32_t s1[8], s2[8];
+  __shared__ int sn[8];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    h1 = min(h1, __shfl_xor_sync(0xffffffffu, h1, o));
+    h2 = min(h2, __shfl_xor_sync(0xffffffffu, h2, o));
+    n += __shfl_xor_sync(0xffffffffu, n, o);
+  }
+  if (lane == 0) {
+    s1[tid >> 5] = h1;
+    s2[tid >> 5] = h2;
+    sn[tid >> 5] = n;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    uint32_t a = s1[0], c = s2[0];
+    int t = sn[0];
+    for (int w = 1; w < 8; ++w) {
+      a = min(a, s1[w]);
+      c = min(c, s2[w]);
+      t += sn[w];
+    }
+    cnt[bg] = t;
+    key[bg] = t == 0 ? ~0ull : (static_cast<unsigned long long>(a) << 32) | c;
+  }
+}
+
+// order[q] = tile at sorted position q (keys ascending, ties by index); above
+// kSortMax tiles the caller's order.
+__global__ void __launch_bounds__(1024)
+pair_sort(const unsigned long long* __restrict__ key, int nbg, int* __restrict__ order) {
+  extern __shared__ unsigned long long sk[];  // kSortMax keys, then kSortMax indices
+  int* id = reinterpret_cast<int*>(sk + kSortMax);
+  const int tid = threadIdx.x;
+  if (nbg > kSortMax) {
+    for (int i = tid; i < nbg; i += 1024) order[i] = i;
+    return;
+  }
+  int n2 = 1;
+  while (n2 < nbg) n2 <<= 1;
+  for (int i = tid; i < n2; i += 1024) {
+    sk[i] = i < nbg ? key[i] : ~0ull;
+    id[i] = i < nbg ? i : INT_MAX;
+  }
+  __syncthreads();
+  for (int size = 2; size <= n2; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = tid; i < n2; i += 1024) {
+        const int j = i ^ stride;
+        if (j > i) {
+          const bool up = (i & size) == 0;
+          const bool gt = sk[i] > sk[j] || (sk[i] == sk[j] && id[i] > id[j]);
+          if (gt == up) {
+            const unsigned long long tk = sk[i];
+            sk[i] = sk[j];
+            sk[j] = tk;
+            const int ti = id[i];
+            id[i] = id[j];
+            id[j] = ti;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int i = tid; i < nbg; i += 1024) order[i] = id[i];
+}
+
+// Per sorted position q: the neighbours within kWin positions whose pairing
+// with tile order[q] saves MMA work (|I_a|^2 + |I_b|^2 > |I_a u I_b|^2), best
+// first: cand[q][0 .. ncand[q]).  CTA per position, thread per candidate.
+__global__ void __launch_bounds__(2 * kWin)
+pair_scores(const uint32_t* __restrict__ bits, const int* __restrict__ cnt,
+            const int* __restrict__ order, int nbg, int nwords, int* __restrict__ cand,
+            int* __restrict__ ncand) {
+  const int q = blockIdx.x;
+  if (q >= nbg) return;
+  const int tid = threadIdx.x;
+  __shared__ long long sc[2 * kWin];
+  __shared__ int who[2 * kWin];
+  const int a = order[q];
+  const int na = cnt[a];
+  const int off = tid < kWin ? tid - kWin : tid - kWin + 1;  // -kWin..-1, 1..kWin
+  const int qb = q + off;
+  long long score = LLONG_MIN;
+  int b = -1;
+  if (na > 0 && qb >= 0 && qb < nbg) {
+    b = order[qb];
+    const int nb = cnt[b];
+    if (nb > 0) {
+      int inter = 0;
+      const uint32_t* x = bits + size_t(a) * nwords;
+      const uint32_t* y = bits + size_t(b) * nwords;
+      for (int w = 0; w < nwords; ++w) inter += __popc(x[w] & y[w]);
+      const long long un = na + nb - inter;
+      score = static_cast<long long>(na) * na + static_cast<long long>(nb) * nb - un * un;
+    }
+  }
+  sc[tid] = score;
+  who[tid] = b;
+  __syncthreads();
+  if (tid == 0) {
+    // the profitable candidates (score > 0), best first, ties by tile index
+    int m = 0;
+    for (;;) {
+      long long best = 0;
+      int bi = -1;
+      for (int i = 0; i < 2 * kWin; ++i)
+        if (sc[i] > best || (sc[i] == best && bi >= 0 && sc[i] > 0 && who[i] < who[bi])) {
+          best = sc[i];
+          bi = i;
+        }
+      if (bi < 0) break;
+      cand[size_t(q) * 2 * kWin + m++] = who[bi];
+      sc[bi] = LLONG_MIN;
+    }
+    ncand[q] = m;
+  }
+}
+
+// Mutual-best matching over the candidate lists (kRounds rounds), then the
+// pair list in key order: pairs[i] = (lo tile, hi tile or -1, batch, 0) for
+// every non-empty tile in exactly one entry; npairs[0] = their number.
+__global__ void __launch_bounds__(1024)
+pair_match(const int* __restrict__ order, const int* __restrict__ cand,
+           const int* __restrict__ ncand, const int* __restrict__ cnt, int nbg, int batch,
+           int* __restrict__ partner, int* __restrict__ pos, int* __restrict__ choice,
+           int4* __restrict__ pairs, int* __restrict__ npairs) {
+  const int tid = threadIdx.x;
+  __shared__ int changed;
+  __shared__ int warp_tot[32];
+  __shared__ int base_s;
+  // partner[t]: -2 free, -1 single, -3 empty (never emitted), >= 0 paired
+  for (int q = tid; q < nbg; q += 1024) {
+    const int t = order[q];
+    pos[t] = q;
+    partner[t] = cnt[t] > 0 ? -2 : -3;
+  }
+  __syncthreads();
+  for (int r = 0; r < kRounds; ++r) {
+    if (tid == 0) changed = 0;
+    // every free tile picks its best free candidate
+    for (int q = tid; q < nbg; q += 1024) {
+      const int t = order[q];
+      int pick = -1;
+      if (partner[t] == -2) {
+        const int n = ncand[q];
+        for (int i = 0; i < n; ++i) {
+          const int c = cand[size_t(q) * 2 * kWin + i];
+          if (partner[c] == -2) {
+            pick = c;
+            break;
+          }
+        }
+      }
+      choice[t] = pick;
+    }
+    __syncthreads();
+    // mutual choices become pairs (written by the member with the lower index)
+    for (int q = tid; q < nbg; q += 1024) {
+      const int t = order[q];
+      const int c = choice[t];
+      if (c >= 0 && t < c && choice[c] == t) {
+        partner[t] = c;
+        partner[c] = t;
+        changed = 1;
+      }
+    }
+    __syncthreads();
+    const int ch = changed;
+    __syncthreads();
+    if (!ch) break;
+  }
+  for (int q = tid; q < nbg; q += 1024) {
+    const int t = order[q];
+    if (partner[t] == -2) partner[t] = -1;
+  }
+  if (tid == 0) base_s = 0;
+  __syncthreads();
+  // one entry per leader (a single, or the member at the lower position)
+  const int lane = tid & 31, warp = tid >> 5;
+  for (int q0 = 0; q0 < nbg; q0 += 1024) {
+    const int q = q0 + tid;
+    int t = -1, c = -3;
+    bool lead = false;
+    if (q < nbg) {
+      t = order[q];
+      c = partner[t];
+      lead = c == -1 || (c >= 0 && pos[c] > q);
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, lead);
+    if (lane == 0) warp_tot[warp] = __popc(bal);
+    __syncthreads();
+    int before = base_s;
+    for (int w = 0; w < warp; ++w) before += warp_tot[w];
+    if (lead)
+      pairs[before + __popc(bal & ((1u << lane) - 1u))] = make_int4(t, c >= 0 ? c : -1, batch, 0);
+    __syncthreads();
+    if (tid == 0)
+      for (int w = 0; w < 32; ++w) base_s += warp_tot[w];
+    __syncthreads();
+  }
+  if (tid == 0) npairs[0] = base_s;
+}
+
+// Per pair: U = ascending union of the two tiles' active lists, flags bit 0 /
+// bit 1 = active in the lo / hi tile's block; ucount.
+__global__ void __launch_bounds__(256)
+pair_union(const uint8_t* __restrict__ tab, size_t ldtab, int nao, int gsub,
+           const int4* __restrict__ pairs, const int* __restrict__ npairs, int pair0,
+           int* __restrict__ ulist, uint8_t* __restrict__ uflag, int* __restrict__ ucount) {
+  const int pl = blockIdx.x;
+  if (pl >= npairs[0]) return;
+  const int pi = pair0 + pl;
+  const int4 pr = pairs[pi];
+  const int b0 = pr.x / gsub, b1 = pr.y >= 0 ? pr.y / gsub : -1;
+  __shared__ int warp_tot[8];
+  __shared__ int base_s;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) base_s = 0;
+  __syncthreads();
+  int* U = ulist + size_t(pi) * nao;
+  uint8_t* F = uflag + size_t(pi) * nao;
+  for (int u0 = 0; u0 < nao; u0 += 256) {
+    const int u = u0 + tid;
+    uint32_t f = 0;
+    if (u < nao) {
+      f = tab[size_t(u) * ldtab + b0] != 0 ? 1u : 0u;
+      if (b1 >= 0 && tab[size_t(u) * ldtab + b1] != 0) f |= 2u;
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, f != 0);
+    if (lane == 0) warp_tot[warp] = __popc(bal);
+    __syncthreads();
+    int before = base_s;
+    for (int w = 0; w < warp; ++w) before += warp_tot[w];
+    if (f) {
+      const int at = before + __popc(bal & ((1u << lane) - 1u));
+      U[at] = u;
+      F[at] = uint8_t(f);
+    }
+    __syncthreads();
+    if (tid == 0)
+      for (int w = 0; w < 8; ++w) base_s += warp_tot[w];
+    __syncthreads();
+  }
+  if (tid == 0) ucount[pi] = base_s;
+}
+
+// cbase[pi] (first phi chunk of each pair, from chunk0), and the items
+// (pair, row tile, DM, batch) of pairs pair0 .. pair0+npairs-1, heaviest
+// first (a counting sort on the chunks an item runs in the symmetric mode),
+// appended at items + *total; *total grows by their number, *chunks_end is
+// the chunk after the batch's last.
+__global__ void __launch_bounds__(1024)
+pair_build(const int* __restrict__ ucount, const int* __restrict__ npairs_d, int pair0, int nset,
+           int batch, int tn, int max_kc, int chunk0, int* __restrict__ cbase,
+           int4* __restrict__ items, int* __restrict__ total, int* __restrict__ chunks_end) {
+  extern __shared__ int hist[];  // max_kc + 2 counters
+  __shared__ int warp_c[32];
+  __shared__ int base_c;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int np = npairs_d[0];
+  for (int i = tid; i <= max_kc + 1; i += 1024) hist[i] = 0;
+  if (tid == 0) base_c = chunk0;
+  __syncthreads();
+  // chunk offsets
+  for (int p0 = 0; p0 < np; p0 += 1024) {
+    const int pl = p0 + tid;
+    const int kc = pl < np ? (ucount[pair0 + pl] + TK - 1) / TK : 0;
+    int ic = kc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, ic, o);
+      if (lane >= o) ic += t;
+    }
+    if (lane == 31) warp_c[warp] = ic;
+    __syncthreads();
+    int bc = base_c;
+    for (int w = 0; w < warp; ++w) bc += warp_c[w];
+    if (pl < np) cbase[pair0 + pl] = bc + ic - kc;
+    __syncthreads();
+    if (tid == 0)
+      for (int w = 0; w < 32; ++w) base_c += warp_c[w];
+    __syncthreads();
+  }
+  // histogram of item weights (chunks from the row tile's own on)
+  for (int pl = tid; pl < np; pl += 1024) {
+    const int nu = ucount[pair0 + pl];
+    const int kc = (nu + TK - 1) / TK, nt = (nu + tn - 1) / tn;
+    for (int t = 0; t < nt; ++t) atomicAdd(&hist[kc - (t * tn) / TK], nset);
+  }
+  __syncthreads();
+  if (tid == 0) {  // heaviest first: cursor[w] = items of weight > w
+    int run = 0;
+    for (int w = max_kc; w >= 0; --w) {
+      const int c = hist[w];
+      hist[w] = run;
+      run += c;
+    }
+    hist[max_kc + 1] = run;
+  }
+  __syncthreads();
+  const int start = total[0];
+  for (int pl = tid; pl < np; pl += 1024) {
+    const int nu = ucount[pair0 + pl];
+    const int kc = (nu + TK - 1) / TK, nt = (nu + tn - 1) / tn;
+    for (int t = 0; t < nt; ++t) {
+      const int w = kc - (t * tn) / TK;
+      const int at = start + atomicAdd(&hist[w], nset);
+      for (int s = 0; s < nset; ++s) items[at + s] = make_int4(pair0 + pl, t, s, batch);
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    total[0] = start + hist[max_kc + 1];
+    chunks_end[0] = base_c;
+  }
+}
+
+// pmax[g] = max |phi[u][g]| over the active AOs of g's block (+Inf for Inf or
+// NaN); CTA (block tile, slab of 64 active AOs); pmax starts at 0.
+__global__ void __launch_bounds__(256)
+pair_phi_max(const double* __restrict__ ao, size_t stride_grid, const int* __restrict__ lists,
+             const int* __restrict__ counts, int nao, int ngrid, int blk, int gsub,
+             unsigned long long* __restrict__ pmax) {
+  const int bg = blockIdx.x, slab = blockIdx.y;
+  const int b = bg / gsub;
+  const int nb = counts[b];
+  const int i0 = slab * 64;
+  if (i0 >= nb) return;
+  int g0, gend;
+  tile_points(bg, blk, gsub, ngrid, &g0, &gend);
+  const int* I = lists + size_t(b) * nao;
+  const int gr = threadIdx.x & (HT - 1), rg = threadIdx.x >> 6;
+  const int g = g0 + gr;
+  __shared__ double red[4][HT];
+  double mx = 0.0;
+  if (g < gend) {
+    bool bad = false;
+    const int iend = min(nb, i0 + 64);
+    for (int i = i0 + rg; i < iend; i += 4) {
+      const double a = fabs(ao[size_t(__ldg(I + i)) * stride_grid + g]);
+      bad |= !(a <= 1.7976931348623157e308);
+      mx = fmax(mx, a);
+    }
+    if (bad) mx = __longlong_as_double(0x7ff0000000000000LL);
+  }
+  red[rg][gr] = mx;
+  __syncthreads();
+  if (threadIdx.x < HT && g < gend) {
+    const double m = fmax(fmax(red[0][gr], red[1][gr]), fmax(red[2][gr], red[3][gr]));
+    atomicMax(pmax + g, static_cast<unsigned long long>(__double_as_longlong(m)));
+  }
+}
+
+// The phi digit tiles of chunk c of pair pi: NSL planes of 128 rows (points:
+// rows 0-63 the lo tile, 64-127 the hi tile) x 32 bytes (union AOs
+// 32c .. 32c+31), 32-byte swizzled, at phisl + (cbase[pi] + c) * A_STAGE;
+// sigma[g] from pmax.  CTA (pair, chunk).
+template <int NSL>
+__global__ void __launch_bounds__(256)
+pair_phi_tiles(const double* __restrict__ ao, size_t stride_grid,
+               const unsigned long long* __restrict__ pmax, const int4* __restrict__ pairs,
+               const int* __restrict__ npairs, int pair0, const int* __restrict__ ulist,
+               const uint8_t* __restrict__ uflag, const int* __restrict__ ucount,
+               const int* __restrict__ cbase, int nao, int ngrid, int blk, int gsub,
+               int* __restrict__ sigma, uint8_t* __restrict__ phisl) {
+  using C = Cfg<NSL>;
+  const int pl = blockIdx.x, c = blockIdx.y;
+  if (pl >= npairs[0]) return;
+  const int pi = pair0 + pl;
+  const int nu = ucount[pi];
+  if (c * TK >= nu) return;
+  const int4 pr = pairs[pi];
+  // staged digit words [plane][quad of 4 AOs][point], rows padded to 132 words
+  __shared__ uint32_t stage[NSL][8][PT + 4];
+  const int* U = ulist + size_t(pi) * nao;
+  const uint8_t* F = uflag + size_t(pi) * nao;
+  {
+    const int v = threadIdx.x;
+    const int r = v & (PT - 1), hq = v >> 7;  // point row, half of the quads
+    const int h = r >> 6, j = r & (HT - 1);
+    const int tile = h ? pr.y : pr.x;
+    int g = -1;
+    if (tile >= 0) {
+      int g0, gend;
+      tile_points(tile, blk, gsub, ngrid, &g0, &gend);
+      if (g0 + j < gend) g = g0 + j;
+    }
+    const int e = g >= 0 ? exp_for(__longlong_as_double(static_cast<long long>(pmax[g]))) : 0;
+    if (c == 0 && hq == 0 && g >= 0) sigma[g] = e;
+#pragma unroll
+    for (int qq = 0; qq < 4; ++qq) {
+      const int q = hq * 4 + qq;
+      uint2 w[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int k = c * TK + q * 4 + t;
+        bool on = g >= 0 && k < nu && e != kBadExp;
+        if (on) on = ((F[k] >> h) & 1u) != 0;
+        w[t] = on ? digits_of<NSL>(ao[size_t(U[k]) * stride_grid + g], e) : make_uint2(0u, 0u);
+      }
+      uint32_t o[8];
+      transpose4(w[0].x, w[1].x, w[2].x, w[3].x, o[0], o[1], o[2], o[3]);
+      transpose4(w[0].y, w[1].y, w[2].y, w[3].y, o[4], o[5], o[6], o[7]);
+#pragma unroll
+      for (int pl2 = 0; pl2 < NSL; ++pl2) stage[pl2][q][r] = o[pl2];
+    }
+  }
+  __syncthreads();
+  uint8_t* tile0 = phisl + (size_t(cbase[pi]) + c) * C::A_STAGE;
+  for (int v = threadIdx.x; v < NSL * PT * 2; v += 256) {
+    const int hh = v & 1, r = (v >> 1) & (PT - 1), j = v >> 8;
+    const uint4 w = make_uint4(stage[j][4 * hh][r], stage[j][4 * hh + 1][r],
+                               stage[j][4 * hh + 2][r], stage[j][4 * hh + 3][r]);
+    *reinterpret_cast<uint4*>(tile0 + j * C::A_SLICE + tc::sw32_offset(uint32_t(r), uint32_t(hh))) = w;
+  }
+}
+
+// D digits: dsl[s][u][v] (NSL digits in 8 bytes), tau[s][u]; a warp per row.
+// With asym non-null and 0 (symmetric mode) the diagonal carries D_uu / 2.
+template <int NSL>
+__global__ void __launch_bounds__(256)
+pair_d_digits(const double* __restrict__ dms, size_t stride_ao, size_t dm_stride, int nao,
+              int nrows, uint2* __restrict__ dsl, int* __restrict__ tau,
+              const int* __restrict__ asym) {
+  const int row = blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= nrows) return;
+  const bool half_diag = asym != nullptr && *asym == 0;
+  const int s = row / nao, u = row % nao;
+  const double* d = dms + size_t(s) * dm_stride + size_t(u) * stride_ao;
+  double mx = 0.0;
+  bool bad = false;
+#pragma unroll 4
+  for (int v = lane; v < nao; v += 32) {
+    const double a = fabs(d[v]);
+    bad |= !(a <= 1.7976931348623157e308);
+    mx = fmax(mx, a);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    bad |= __shfl_xor_sync(0xffffffffu, int(bad), o) != 0;
+  }
+  const int e = bad ? kBadExp : exp_for(mx);
+  if (lane == 0) tau[row] = e;
+  uint2* out = dsl + size_t(row) * nao;
+#pragma unroll 4
+  for (int v = lane; v < nao; v += 32)
+    out[v] = e != kBadExp ? digits_of<NSL>(half_diag && v == u ? 0.5 * d[v] : d[v], e)
+                          : make_uint2(0u, 0u);
+}
+
+// Byte selector assembling, from `keep` (bytes 0..3) and `recv` (4..7) of the
+// gather's second shuffle round, the digit word of 4 consecutive columns:
+// column qd from keep.b0, qd^2 from keep.b2, qd^1 from recv.b0, qd^3 from
+// recv.b2 (the lane's second digit plane: +1 on every nibble).
+__device__ __forceinline__ uint32_t gather_selector(int qd) {
+  uint32_t sel = 0;
+#pragma unroll
+  for (int col = 0; col < 4; ++col) {
+    const uint32_t src = col == qd ? 0u : col == (qd ^ 2) ? 2u : col == (qd ^ 1) ? 4u : 6u;
+    sel |= src << (4 * col);
+  }
+  return sel;
+}
+
+// ---------------------------------------------------------------------------
+// main kernel
+// ---------------------------------------------------------------------------
+template <int NSL, int STAGES>
+__global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
+  using C = Cfg<NSL>;
+  constexpr int TN = C::TN;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                             ~uintptr_t(1023));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * C::STAGE);
+  uint64_t* full_phi = bars;            // phi tile landed (bulk copy)
+  uint64_t* full_d = bars + STAGES;     // D digits stored (4 gather warps)
+  uint64_t* empty = bars + 2 * STAGES;  // the stage's MMAs completed
+  uint64_t* acc_full = bars + 3 * STAGES;
+  uint64_t* acc_empty = acc_full + 1;
+  uint64_t* drain = acc_full + 2;
+  uint64_t* epi_full = acc_full + 3;  // [2]: the groups' sums of an item are in `epi`
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_full + 5);
+  // the groups' per-point sums of an item, combined by group 0 (two items in
+  // flight at most: a group cannot reach item n+2's epilogue before group 0
+  // has finished item n+1's)
+  double* epi = reinterpret_cast<double*>(smem + STAGES * C::STAGE + 256);  // [2][NG][PT]
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int* err = &g_pair_error;
+  const uint64_t lim = p.wait_ns ? p.wait_ns : tc::kWaitLimitNs;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      tc::mbar_init(&full_phi[s], 1);
+      tc::mbar_init(&full_d[s], 4);
+      tc::mbar_init(&empty[s], 1);
+    }
+    tc::mbar_init(acc_full, 1);
+    tc::mbar_init(acc_empty, GW);
+    tc::mbar_init(drain, 1);
+    tc::mbar_init(&epi_full[0], GW);
+    tc::mbar_init(&epi_full[1], GW);
+    tc::mbar_fence_init();
+  }
+  if (warp == GW) {
+    tc::tmem_alloc(tmem_slot, 512);
+    tc::tmem_relinquish();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *tmem_slot;
+  const int total = p.total[0];
+  const bool sym = p.asym != nullptr && *p.asym == 0;
+
+  if (warp < GW) {
+    // ---------------- gather D digits, then the epilogue ----------------
+    // Group grp takes the chunks c = kc0 + grp, + NG, ... of every item; warp
+    // wq of the group fills D rows WROWS*wq .. of the tile, four rows per step.
+    // Lane (qd, ri, hh) = lane bits (4:3, 2:1, 0) loads, for row 4*step+ri,
+    // the union columns 16hh + 4k + qd (k = 0..3) and ends up holding digit
+    // planes 2qd and 2qd+1 of the 16-byte half hh of that row.
+    const int grp = warp >> 2, wq = warp & 3;
+    const int qd = lane >> 3, ri = (lane >> 1) & 3, hh = lane & 1;
+    const bool b1 = (qd & 2) != 0, b0 = (qd & 1) != 0;
+    const uint32_t sel_a = gather_selector(qd), sel_b = sel_a + 0x1111u;
+    uint32_t seq0 = 0, nitem = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++nitem) {
+      const int4 it = p.items[t];
+      const int pi = it.x, ut = it.y, s = it.z;
+      const PairBatch& B = batch_of(p, it.w);
+      const int nu = p.ucount[pi];
+      const int kc = (nu + TK - 1) / TK;
+      const int kc0 = sym ? (ut * TN) / TK : 0;
+      const int* U = p.ulist + size_t(pi) * p.nao;
+      const uint2* dset = p.dsl + size_t(s) * p.nao * p.nao;
+      int iu[C::STEPS], prow[C::STEPS];
+#pragma unroll
+      for (int st = 0; st < C::STEPS; ++st) {
+        prow[st] = ut * TN + C::WROWS * wq + 4 * st + ri;
+        iu[st] = prow[st] < nu ? __ldg(U + prow[st]) : -1;
+      }
+      // what the epilogue reads is requested now, while the chunks run: lane l
+      // holds column l of the group's columns (octets grp, grp+NG, ...): its
+      // AO, membership flags and row scale; phi_lhs of those rows at this
+      // warp's 32 points goes to L2
+      const int4 pr = p.pairs[pi];
+      const int h = wq >> 1;
+      const int tile = h ? pr.y : pr.x;
+      int g0 = 0, gend = 0;
+      if (tile >= 0) tile_points(tile, p.blk, p.gsub, B.ngrid, &g0, &gend);
+      const int r = 32 * wq + lane;  // TMEM lane = point row
+      const int gpt = g0 + (r & (HT - 1));
+      const bool gval = tile >= 0 && gpt < gend;
+      const int col_l = (grp + NG * (lane >> 3)) * 8 + (lane & 7);  // this lane's column
+      const int kpos_l = ut * TN + col_l;
+      const bool cval_l = col_l < TN && kpos_l < nu;
+      const int u_l = cval_l ? __ldg(U + kpos_l) : 0;
+      const int f_l = cval_l ? int(p.uflag[size_t(pi) * p.nao + kpos_l]) : 0;
+      const int tu_l = cval_l ? p.tau[size_t(s) * p.nao + u_l] : 0;
+      const int sg = gval ? B.sigma[gpt] : 0;
+      const int wg0 = g0 + 32 * (wq & 1);  // this warp's first point
+      if (cval_l && ((f_l >> h) & 1) && tile >= 0 && wg0 < gend) {
+        const char* q0 = reinterpret_cast<const char*>(B.ao_lhs + size_t(u_l) * B.stride_grid + wg0);
+        const int last = min(gend - wg0, 32) - 1;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(q0));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(q0 + 8 * last));
+      }
+      for (int c = kc0 + grp; c < kc; c += NG) {
+        const uint32_t seq = seq0 + uint32_t(c - kc0);
+        const int stg = int(seq % STAGES);
+        const uint32_t use = seq / STAGES;
+        int iv[4], pc[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          pc[k] = c * TK + 16 * hh + 4 * k + qd;
+          iv[k] = pc[k] < nu ? __ldg(U + pc[k]) : -1;
+        }
+        // symmetric D: only columns from the row's own position on (the
+        // diagonal digits carry D_uu / 2)
+        uint2 w[C::STEPS][4];
+#pragma unroll
+        for (int st = 0; st < C::STEPS; ++st)
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            w[st][k] = (iu[st] >= 0 && iv[k] >= 0 && (!sym || pc[k] >= prow[st]))
+                           ? __ldg(dset + size_t(iu[st]) * p.nao + iv[k])
+                           : make_uint2(0u, 0u);
+        if (use > 0 && !tc::mbar_wait(&empty[stg], (use - 1) & 1, err, 31, false, lim)) {
+          ok = false;
+          break;
+        }
+        uint8_t* Bs = smem + stg * C::STAGE + C::A_STAGE;
+#pragma unroll
+        for (int st = 0; st < C::STEPS; ++st) {
+          uint32_t wa[4], wb[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            // round 1 (lanes qd, qd^2): keep digits 0-3 (b1 = 0) or 4-7 (b1 = 1)
+            const uint32_t x = b1 ? w[st][k].y : w[st][k].x;
+            const uint32_t y = __shfl_xor_sync(0xffffffffu, b1 ? w[st][k].x : w[st][k].y, 16);
+            // round 2 (lanes qd, qd^1): keep two of those four digits
+            const uint32_t lo = __byte_perm(x, y, 0x5410), hi = __byte_perm(x, y, 0x7632);
+            const uint32_t keep = b0 ? hi : lo;
+            const uint32_t recv = __shfl_xor_sync(0xffffffffu, b0 ? lo : hi, 8);
+            wa[k] = __byte_perm(keep, recv, sel_a);
+            wb[k] = __byte_perm(keep, recv, sel_b);
+          }
+          const uint32_t off =
+              tc::sw32_offset(uint32_t(C::WROWS * wq + 4 * st + ri), uint32_t(hh));
+          if (2 * qd < NSL)
+            *reinterpret_cast<uint4*>(Bs + (2 * qd) * C::B_SLICE + off) =
+                make_uint4(wa[0], wa[1], wa[2], wa[3]);
+          if (2 * qd + 1 < NSL)
+            *reinterpret_cast<uint4*>(Bs + (2 * qd + 1) * C::B_SLICE + off) =
+                make_uint4(wb[0], wb[1], wb[2], wb[3]);
+        }
+        tc::fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&full_d[stg]);
+      }
+      seq0 += uint32_t(kc - kc0);
+      if (!ok) break;
+      // ---- epilogue: this warp's 32 points (TMEM lanes 32wq ..) over the
+      // group's column octets ----
+      if (!tc::mbar_wait(acc_full, nitem & 1, err, 32, false, lim)) break;
+      tc::fence_after_sync();
+      const uint32_t trow = tmem + (uint32_t(32 * wq) << 16);
+      double acc = 0.0;
+      bool badrow = false;
+#pragma unroll 1
+      for (int oi = 0; grp + NG * oi < C::OCTETS; ++oi) {
+        const int col0 = (grp + NG * oi) * 8;
+        if (ut * TN + col0 >= nu) break;  // warp-uniform: the rest of the tile is past U
+        uint32_t v[NSL][8];
+#pragma unroll
+        for (int L = 0; L < NSL; ++L)
+          tc::tmem_ld_32x32b_x8(trow + uint32_t(L * TN + col0), v[L]);
+        // phi_lhs of the 8 columns at this lane's point, for AOs active in its block
+        double a[8];
+        int tus[8];
+        bool on[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int src = oi * 8 + j;
+          const int uj = __shfl_sync(0xffffffffu, u_l, src);
+          const int fj = __shfl_sync(0xffffffffu, f_l, src);
+          tus[j] = __shfl_sync(0xffffffffu, tu_l, src);
+          on[j] = gval && ut * TN + col0 + j < nu && ((fj >> h) & 1);
+          a[j] = on[j] ? B.ao_lhs[size_t(uj) * B.stride_grid + gpt] : 0.0;
+        }
+        tc::tmem_ld_wait();
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          uint32_t lv[NSL];
+#pragma unroll
+          for (int L = 0; L < NSL; ++L) lv[L] = v[L][j];
+          if (on[j]) {  // AOs inactive in this point's block take no part
+            if (tus[j] == kBadExp) {
+              badrow = true;
+            } else {
+              const double x = combine_levels<NSL>(lv);
+              const int e = -tus[j];
+              acc = fma(a[j], (e >= -1022 && e <= 1023) ? x * pow2(e) : ldexp(x, e), acc);
+            }
+          }
+        }
+      }
+      double res = 0.0;
+      if (gval) {
+        const int e = -sg;
+        res = (sg == kBadExp || badrow) ? __longlong_as_double(0x7ff8000000000000LL)
+              : (e >= -1022 && e <= 1023) ? acc * pow2(e)
+                                          : ldexp(acc, e);
+        if (sym) res *= 2.0;
+      }
+      tc::fence_before_sync();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(acc_empty);  // the MMA warp may overwrite the accumulators
+      double* e2 = epi + (nitem & 1) * (NG * PT);
+      e2[grp * PT + r] = res;
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&epi_full[nitem & 1]);
+      if (grp == 0) {
+        if (!tc::mbar_wait(&epi_full[nitem & 1], (nitem >> 1) & 1, err, 39, false, lim)) break;
+        double sum = e2[r];
+#pragma unroll
+        for (int w = 1; w < NG; ++w) sum += e2[w * PT + r];
+        const size_t pbase = p.poff ? size_t(p.poff[pi]) : size_t(pi) * p.max_t;
+        p.partial[((pbase + ut) * p.nset_max + s) * PT + r] = sum;
+      }
+    }
+  } else if (warp == GW) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      const uint32_t idesc = tc::idesc_i8(PT, TN);
+      uint32_t seq = 0, nitem = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++nitem) {
+        const int4 it = p.items[t];
+        const int nu = p.ucount[it.x];
+        const int kc = (nu + TK - 1) / TK;
+        const int kc0 = sym ? (it.y * TN) / TK : 0;
+        if (nitem > 0 && !tc::mbar_wait(acc_empty, (nitem - 1) & 1, err, 33, false, lim)) break;
+        tc::fence_after_sync();
+        for (int c = kc0; c < kc; ++c, ++seq) {
+          const int stg = int(seq % STAGES);
+          const uint32_t par = (seq / STAGES) & 1;
+          if (!tc::mbar_wait(&full_phi[stg], par, err, 34, false, lim) ||
+              !tc::mbar_wait(&full_d[stg], par, err, 35, false, lim)) {
+            ok = false;
+            break;
+          }
+          tc::fence_after_sync();
+          const uint32_t a0 = tc::smem_u32(smem + stg * C::STAGE);
+          const uint32_t b0 = a0 + C::A_STAGE;
+          // phi digit j (the A operand) meets D digits 0 .. NSL-1-j (levels
+          // j .. NSL-1) in consecutive MMAs: its plane is read from shared
+          // memory once and held in the collector buffer for the rest
+#pragma unroll
+          for (int j = 0; j < NSL; ++j) {
+            const uint64_t ad = tc::smem_desc_k32(a0 + j * C::A_SLICE);
+            const bool acc = c > kc0 || j > 0;
+#pragma unroll
+            for (int i = 0; i + j < NSL; ++i) {
+              const uint32_t d = tmem + uint32_t((i + j) * TN);
+              const uint64_t bd = tc::smem_desc_k32(b0 + i * C::B_SLICE);
+              if (j == NSL - 1)
+                tc::mma_i8(d, ad, bd, idesc, acc);
+              else if (i == 0)
+                tc::mma_i8_collect<tc::ACollector::kFill>(d, ad, bd, idesc, acc);
+              else if (i + j == NSL - 1)
+                tc::mma_i8_collect<tc::ACollector::kLastUse>(d, ad, bd, idesc, acc);
+              else
+                tc::mma_i8_collect<tc::ACollector::kUse>(d, ad, bd, idesc, acc);
+            }
+          }
+          tc::mma_commit(&empty[stg]);
+        }
+        if (!ok) break;
+        tc::mma_commit(acc_full);
+      }
+      tc::mma_commit(drain);
+      tc::mbar_wait(drain, 0, err, 36, true, lim);
+    }
+  } else {
+    // ---------------- phi digit tiles: bulk loads ----------------
+    if (lane == 0) {
+      uint32_t seq = 0;
+      uint32_t issued[STAGES];
+#pragma unroll
+      for (int s = 0; s < STAGES; ++s) issued[s] = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+        const int4 it = p.items[t];
+        const int nu = p.ucount[it.x];
+        const int kc = (nu + TK - 1) / TK;
+        const int kc0 = sym ? (it.y * TN) / TK : 0;
+        const uint8_t* src = p.phisl + size_t(p.cbase[it.x]) * C::A_STAGE;
+        for (int c = kc0; c < kc; ++c, ++seq) {
+          const int stg = int(seq % STAGES);
+          const uint32_t use = seq / STAGES;
+          if (use > 0 && !tc::mbar_wait(&empty[stg], (use - 1) & 1, err, 37, false, lim)) {
+            ok = false;
+            break;
+          }
+          // test hook: the first stage is never published, so the MMA warp's
+          // bounded wait runs out and the call reports a timeout
+          if (p.inject && seq == 0) continue;
+          tc::mbar_arrive_expect_tx(&full_phi[stg], C::A_STAGE);
+          tc::bulk_load(smem + stg * C::STAGE, src + size_t(c) * C::A_STAGE, C::A_STAGE,
+                        &full_phi[stg]);
+#pragma unroll
+          for (int s = 0; s < STAGES; ++s) issued[s] += s == stg;
+        }
+      }
+      // copies still in flight complete before the CTA exits
+#pragma unroll
+      for (int s = 0; s < STAGES; ++s)
+        if (issued[s] > 0) tc::mbar_wait(&full_phi[s], (issued[s] - 1) & 1, err, 38, true, lim);
+    }
+  }
+
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  if (warp == GW) tc::tmem_dealloc(tmem, 512);
+}
+
+// ---------------------------------------------------------------------------
+// deterministic reduction: rho[s][g] += sum over the row tiles, in order
+// ---------------------------------------------------------------------------
+template <int TN>
+__global__ void __launch_bounds__(256)
+pair_reduce(PairArgs p, const int* __restrict__ npairs, int pair0) {
+  const int pl = blockIdx.x;
+  if (pl >= npairs[0]) return;
+  const int pi = pair0 + pl;
+  const int4 pr = p.pairs[pi];
+  const PairBatch& B = batch_of(p, pr.z);
+  const int nt = (p.ucount[pi] + TN - 1) / TN;
+  if (nt == 0) return;
+  const size_t pbase = p.poff ? size_t(p.poff[pi]) : size_t(pi) * p.max_t;
+  for (int v = threadIdx.x; v < B.nset * PT; v += 256) {
+    const int s = v / PT, r = v % PT;
+    const int h = r >> 6;
+    const int tile = h ? pr.y : pr.x;
+    if (tile < 0) continue;
+    int g0, gend;
+    tile_points(tile, p.blk, p.gsub, B.ngrid, &g0, &gend);
+    const int g = g0 + (r & (HT - 1));
+    if (g >= gend) continue;
+    double acc = 0.0;
+    for (int t = 0; t < nt; ++t) acc += p.partial[((pbase + t) * p.nset_max + s) * PT + r];
+    double* out = B.rhos + size_t(s) * B.stride_grid + g;
+    *out = acc + *out;
+  }
+}
+
+template <int NSL, int STAGES>
+cudaError_t launch_pair_main_t(int nsm, const PairArgs& a, cudaStream_t stream, bool attrs_only) {
+  constexpr size_t smem = size_t(STAGES) * Cfg<NSL>::STAGE + 1024 + 256 + 2 * NG * PT * 8;
+  cudaError_t err = cudaFuncSetAttribute(pair_main<NSL, STAGES>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (err != cudaSuccess || attrs_only) return err;
+  pair_main<NSL, STAGES><<<nsm, THREADS, smem, stream>>>(a);
+  return cudaGetLastError();
+}
+
+size_t a256(size_t v) { return (v + 255) / 256 * 256; }
+
+struct Layout {
+  size_t lists, counts, bits, cnt, key, order, cand, ncand, partner, pos, choice, pairs, npairs,
+      ulist, uflag, ucount, cbase, items, total, dsl, tau, sigma, pmax, phisl, partial, bytes;
+};
+
+Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk, int nsl) {
+  const size_t nblk = (ngrid + blk - 1) / blk;
+  const size_t gsub = (blk + HT - 1) / HT;
+  const size_t nbg = nblk * gsub;
+  const size_t tn = nsl == 6 ? Cfg<6>::TN : Cfg<7>::TN;
+  const size_t max_t = (nao + tn - 1) / tn;
+  const size_t max_kc = (nao + TK - 1) / TK;
+  const size_t nwords = (nao + 31) / 32;
+  const size_t a_stage = size_t(nsl) * PT * TK;
+  Layout L;
+  L.lists = 0;
+  L.counts = L.lists + a256(nblk * nao * sizeof(int));
+  L.bits = L.counts + a256(nblk * sizeof(int));
+  L.cnt = L.bits + a256(nbg * nwords * sizeof(uint32_t));
+  L.key = L.cnt + a256(nbg * sizeof(int));
+  L.order = L.key + a256(nbg * sizeof(unsigned long long));
+  L.cand = L.order + a256(nbg * sizeof(int));
+  L.ncand = L.cand + a256(nbg * 2 * kWin * sizeof(int));
+  L.partner = L.ncand + a256(nbg * sizeof(int));
+  L.pos = L.partner + a256(nbg * sizeof(int));
+  L.choice = L.pos + a256(nbg * sizeof(int));
+  L.pairs = L.choice + a256(nbg * sizeof(int));
+  L.npairs = L.pairs + a256(nbg * sizeof(int4));
+  L.ulist = L.npairs + 256;
+  L.uflag = L.ulist + a256(nbg * nao * sizeof(int));
+  L.ucount = L.uflag + a256(nbg * nao);
+  L.cbase = L.ucount + a256(nbg * sizeof(int));
+  L.items = L.cbase + a256((nbg + 1) * sizeof(int));
+  L.total = L.items + a256(nbg * max_t * nset * sizeof(int4));
+  L.dsl = L.total + 256;
+  L.tau = L.dsl + a256(nset * nao * nao * 8);
+  L.sigma = L.tau + a256(nset * nao * sizeof(int));
+  L.pmax = L.sigma + a256(ngrid * sizeof(int));
+  L.phisl = L.pmax + a256(ngrid * sizeof(unsigned long long));
+  L.partial = L.phisl + a256(nbg * max_kc * a_stage);
+  L.bytes = L.partial + nbg * max_t * nset * PT * sizeof(double);
+  return L;
+}
+
+}  // namespace
+
+int split_pair_row_tile(int nsl) { return nsl == 6 ? Cfg<6>::TN : Cfg<7>::TN; }
+
+int split_pair_digits() {  // read on every call: the workspace covers both counts
+  const char* e = std::getenv("CFGMM_SPLIT_DIGITS");
+  const int d = e ? std::atoi(e) : 7;
+  return (d == 6 || d == 7) ? d : 7;
+}
+
+size_t aodmao2rho_split_pair_workspace(size_t nao, size_t ngrid, size_t nset, size_t blk,
+                                       int nsl) {
+  return layout(nao, ngrid, nset, blk, nsl).bytes;
+}
+
+cudaError_t split_pair_launch_main(const PairArgs& a, int nsl, cudaStream_t stream,
+                                   bool attrs_only) {
+  int dev = 0, nsm = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err == cudaSuccess) err = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (err != cudaSuccess) return err;
+  return nsl == 6 ? launch_pair_main_t<6, kStages>(nsm, a, stream, attrs_only)
+                  : launch_pair_main_t<7, kStages>(nsm, a, stream, attrs_only);
+}
+
+cudaError_t split_pair_launch_reduce(const PairArgs& a, int nsl, const int* npairs, int pair0,
+                                     int max_pairs, cudaStream_t stream) {
+  if (max_pairs <= 0) return cudaSuccess;
+  if (nsl == 6)
+    pair_reduce<Cfg<6>::TN><<<max_pairs, 256, 0, stream>>>(a, npairs, pair0);
+  else
+    pair_reduce<Cfg<7>::TN><<<max_pairs, 256, 0, stream>>>(a, npairs, pair0);
+  return cudaGetLastError();
+}
+
+cudaError_t split_pair_prepare_d(const double* dms, size_t stride_ao, int nao, int nset, int nsl,
+                                 uint2* dsl, int* tau, cudaStream_t stream, const int* asym) {
+  const unsigned grid = unsigned((nset * nao + 7) / 8);
+  if (nsl == 6)
+    pair_d_digits<6><<<grid, 256, 0, stream>>>(dms, stride_ao, stride_ao * stride_ao, nao,
+                                                nset * nao, dsl, tau, asym);
+  else
+    pair_d_digits<7><<<grid, 256, 0, stream>>>(dms, stride_ao, stride_ao * stride_ao, nao,
+                                                nset * nao, dsl, tau, asym);
+  return cudaGetLastError();
+}
+
+// Pairing, union lists, work list and phi digit tiles of one grid batch whose
+// active lists (lists, counts) are built: pairs from q.pair0 (at most nbg of
+// them), chunks from q.chunk0, items appended at *q.total.
+cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream) {
+  const int nblk = (q.ngrid + q.blk - 1) / q.blk;
+  const int gsub = (q.blk + HT - 1) / HT;
+  const int nbg = nblk * gsub;
+  const int nwords = (q.nao + 31) / 32;
+  const int tn = q.nsl == 6 ? Cfg<6>::TN : Cfg<7>::TN;
+  const int max_kc = (q.nao + TK - 1) / TK;
+  if (nbg <= 0) return cudaSuccess;
+  constexpr size_t sort_smem = size_t(kSortMax) * (sizeof(unsigned long long) + sizeof(int));
+  static const cudaError_t sort_attr = cudaFuncSetAttribute(
+      pair_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sort_smem));
+  if (sort_attr != cudaSuccess) return sort_attr;
+  pair_sig<<<nbg, 256, 0, stream>>>(q.tab, q.ldtab, q.nao, nbg, gsub, nwords, q.bits, q.cnt,
+                                    q.key);
+  pair_sort<<<1, 1024, sort_smem, stream>>>(q.key, nbg, q.order);
+  pair_scores<<<nbg, 2 * kWin, 0, stream>>>(q.bits, q.cnt, q.order, nbg, nwords, q.cand,
+                                            q.ncand);
+  pair_match<<<1, 1024, 0, stream>>>(q.order, q.cand, q.ncand, q.cnt, nbg, q.batch, q.partner,
+                                     q.pos, q.choice, q.pairs + q.pair0, q.npairs);
+  pair_union<<<nbg, 256, 0, stream>>>(q.tab, q.ldtab, q.nao, gsub, q.pairs, q.npairs, q.pair0,
+                                      q.ulist, q.uflag, q.ucount);
+  const size_t hist = size_t(max_kc + 2) * sizeof(int);
+  pair_build<<<1, 1024, hist, stream>>>(q.ucount, q.npairs, q.pair0, q.nset, q.batch, tn, max_kc,
+                                        q.chunk0, q.cbase, q.items, q.total, q.chunks_end);
+  cudaError_t err = cudaMemsetAsync(q.pmax, 0, size_t(q.ngrid) * sizeof(unsigned long long),
+                                    stream);
+  if (err != cudaSuccess) return err;
+  pair_phi_max<<<dim3(nbg, (q.nao + 63) / 64), 256, 0, stream>>>(
+      q.ao_rhs, q.stride_grid, q.lists, q.counts, q.nao, q.ngrid, q.blk, gsub, q.pmax);
+  const dim3 tg(nbg, max_kc);
+  if (q.nsl == 6)
+    pair_phi_tiles<6><<<tg, 256, 0, stream>>>(q.ao_rhs, q.stride_grid, q.pmax, q.pairs, q.npairs,
+                                              q.pair0, q.ulist, q.uflag, q.ucount, q.cbase, q.nao,
+                                              q.ngrid, q.blk, gsub, q.sigma, q.phisl);
+  else
+    pair_phi_tiles<7><<<tg, 256, 0, stream>>>(q.ao_rhs, q.stride_grid, q.pmax, q.pairs, q.npairs,
+                                              q.pair0, q.ulist, q.uflag, q.ucount, q.cbase, q.nao,
+                                              q.ngrid, q.blk, gsub, q.sigma, q.phisl);
+  return cudaGetLastError();
+}
+
+cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double* ao_lhs,
+                                  const double* ao_rhs, size_t stride_ao, size_t stride_grid,
+                                  int nao, int ngrid, int nset, const uint8_t* tab, size_t ldtab,
+                                  int blk, int nsl, void* workspace, cudaStream_t stream,
+                                  int inject, unsigned long long wait_ns) {
+  if (nao <= 0 || ngrid <= 0 || nset <= 0) return cudaSuccess;
+  if (nsl != 6 && nsl != 7) return cudaErrorInvalidValue;
+  const int nblk = (ngrid + blk - 1) / blk;
+  const int gsub = (blk + HT - 1) / HT;
+  const int nbg = nblk * gsub;
+  const int tn = nsl == 6 ? Cfg<6>::TN : Cfg<7>::TN;
+  const Layout L = layout(nao, ngrid, nset, blk, nsl);
+  char* ws = static_cast<char*>(workspace);
+  auto at = [&](size_t off) { return static_cast<void*>(ws + off); };
+  int* lists = static_cast<int*>(at(L.lists));
+  int* counts = static_cast<int*>(at(L.counts));
+  PairPrep q{};
+  q.tab = tab;
+  q.ldtab = ldtab;
+  q.ao_rhs = ao_rhs;
+  q.stride_grid = stride_grid;
+  q.nao = nao;
+  q.ngrid = ngrid;
+  q.blk = blk;
+  q.nset = nset;
+  q.nsl = nsl;
+  q.batch = 0;
+  q.pair0 = 0;
+  q.chunk0 = 0;
+  q.lists = lists;
+  q.counts = counts;
+  q.bits = static_cast<uint32_t*>(at(L.bits));
+  q.cnt = static_cast<int*>(at(L.cnt));
+  q.key = static_cast<unsigned long long*>(at(L.key));
+  q.order = static_cast<int*>(at(L.order));
+  q.cand = static_cast<int*>(at(L.cand));
+  q.ncand = static_cast<int*>(at(L.ncand));
+  q.partner = static_cast<int*>(at(L.partner));
+  q.pos = static_cast<int*>(at(L.pos));
+  q.choice = static_cast<int*>(at(L.choice));
+  q.pairs = static_cast<int4*>(at(L.pairs));
+  q.npairs = static_cast<int*>(at(L.npairs));
+  q.ulist = static_cast<int*>(at(L.ulist));
+  q.uflag = static_cast<uint8_t*>(at(L.uflag));
+  q.ucount = static_cast<int*>(at(L.ucount));
+  q.cbase = static_cast<int*>(at(L.cbase));
+  q.items = static_cast<int4*>(at(L.items));
+  q.total = static_cast<int*>(at(L.total));
+  q.chunks_end = q.total + 2;
+  q.sigma = static_cast<int*>(at(L.sigma));
+  q.pmax = static_cast<unsigned long long*>(at(L.pmax));
+  q.phisl = static_cast<uint8_t*>(at(L.phisl));
+  uint2* dsl = static_cast<uint2*>(at(L.dsl));
+  int* tau = static_cast<int*>(at(L.tau));
+
+  // total[0]: items, total[1]: asymmetry flag, total[2]: chunks
+  int* asym = aodm_sym_enabled() && ao_lhs == ao_rhs ? q.total + 1 : nullptr;
+  cudaError_t err = cudaMemsetAsync(q.total, 0, 3 * sizeof(int), stream);
+  if (err != cudaSuccess) return err;
+  // The D chain (symmetry check, D digits) runs on a side stream beside the
+  // phi chain (block lists, pairing, unions, work list, phi tiles); the side
+  // stream joins back before the main kernel.
+  SideScope side(side_stream(), stream);
+  if ((err = side.fork()) != cudaSuccess) return err;
+  const cudaStream_t sd = side.stream();
+  if (asym && (err = aodm_launch_sym_check(dms, stride_ao, nao, nset, asym, sd)) != cudaSuccess)
+    return err;
+  if ((err = split_pair_prepare_d(dms, stride_ao, nao, nset, nsl, dsl, tau, sd, asym)) !=
+      cudaSuccess)
+    return err;
+  if ((err = aodm_block_lists_launch(tab, ldtab, nao, nblk, lists, counts, stream)) !=
+      cudaSuccess)
+    return err;
+  if ((err = split_pair_prepare_batch(q, stream)) != cudaSuccess) return err;
+  if ((err = side.join()) != cudaSuccess) return err;
+
+  PairArgs a{};
+  a.dsl = dsl;
+  a.tau = tau;
+  a.phisl = q.phisl;
+  a.items = q.items;
+  a.total = q.total;
+  a.pairs = q.pairs;
+  a.ucount = q.ucount;
+  a.ulist = q.ulist;
+  a.uflag = q.uflag;
+  a.cbase = q.cbase;
+  a.batches = nullptr;
+  a.one = PairBatch{ao_lhs, rhos, q.sigma, stride_grid, ngrid, nset};
+  a.partial = static_cast<double*>(at(L.partial));
+  a.poff = nullptr;
+  a.nao = nao;
+  a.blk = blk;
+  a.gsub = gsub;
+  a.max_t = (nao + tn - 1) / tn;
+  a.nset_max = nset;
+  a.asym = asym;
+  unsigned long long armed_ns = 0;
+  if (take_wait_injection(1, &armed_ns)) {  // cfgmm_test_arm_wait_timeout
+    inject = 1;
+    wait_ns = armed_ns;
+  }
+  a.wait_ns = wait_ns;
+  a.inject = inject;
+  if ((err = split_pair_launch_main(a, nsl, stream, false)) != cudaSuccess) return err;
+  return split_pair_launch_reduce(a, nsl, q.npairs, 0, nbg, stream);
+}
+
+cudaError_t aodmao2rho_split_pair_reset_error(cudaStream_t stream) {
+  static const int zero = 0;
+  return cudaMemcpyToSymbolAsync(g_pair_error, &zero, sizeof(int), 0, cudaMemcpyHostToDevice,
+                                 stream);
+}
+
+cudaError_t aodmao2rho_split_pair_read_error(int* code) {
+  return cudaMemcpyFromSymbol(code, g_pair_error, sizeof(int));
+}
+
+}  // namespace cfgmm

@@ -59,19 +59,20 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Waits for phase `parity` of `bar`.  Returns false (after recording `code`
-// in *err) if it has not completed within kWaitLimitNs, or -- unless
-// `teardown` -- as soon as another thread has recorded an error.  Teardown
-// waits (letting issued copies and MMAs land before the CTA exits) are bounded
-// by time only.
+// in *err) if it has not completed within `limit_ns` (kWaitLimitNs unless a
+// kernel passes its own), or -- unless `teardown` -- as soon as another thread
+// has recorded an error.  Teardown waits (letting issued copies and MMAs land
+// before the CTA exits) are bounded by time only.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code,
-                                          bool teardown = false) {
+                                          bool teardown = false,
+                                          uint64_t limit_ns = kWaitLimitNs) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer();
   for (uint32_t it = 0;; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
     if ((it & 63) == 0) {
       if (!teardown && *reinterpret_cast<volatile int*>(err) != 0) return false;
-      if (globaltimer() - t0 > kWaitLimitNs) {
+      if (globaltimer() - t0 > limit_ns) {
         atomicCAS(err, 0, code);
         return false;
       }

@@ -156,8 +156,22 @@ int cfgmm_split_moduli(size_t k);
 
 /* No counterpart in the reference: synchronises the current device and
  * reports CFGMM_ERR_TIMEOUT if a tensor-core pipeline wait of an earlier
- * asynchronous (_dev) call gave up; CFGMM_OK otherwise. */
+ * asynchronous (_dev) call gave up; CFGMM_OK otherwise.  A timeout is reported
+ * once: the device's wait words are cleared when it is. */
 int cfgmm_device_check(void);
+
+/* No counterpart in the reference: the test hook of the device-side failure
+ * detection.  Arms the calling thread's NEXT masked AO-DM-AO contraction in
+ * `precision` (CFGMM_PREC_FP64: the pipelined FP64 kernel; OZAKI_INT8 with
+ * CFGMM_SPLIT_FORM=pair: the split pair kernel) so that one producer never
+ * publishes the first pipeline stage and every wait in the kernel gives up
+ * after `wait_ms` (1..2000) milliseconds instead of 2 s.  The waiting warp
+ * records a timeout, every warp leaves, copies in flight land, tensor memory
+ * is freed and the kernel returns: the call (a host-pointer one) or the next
+ * cfgmm_device_check (after a _dev one) returns CFGMM_ERR_TIMEOUT, and the
+ * calls after it run normally.  Nothing faults or hangs; the results of the
+ * armed call are not defined. */
+int cfgmm_test_arm_wait_timeout(int precision, double wait_ms);
 
 /* ======================================================================== */
 /* 2. Masked AO-DM-AO contraction                                           */

@@ -116,6 +116,7 @@ extern "C" {
     ) -> c_int;
     pub fn cfgmm_split_moduli(k: usize) -> c_int;
     pub fn cfgmm_device_check() -> c_int;
+    pub fn cfgmm_test_arm_wait_timeout(precision: c_int, wait_ms: f64) -> c_int;
 
     // ---- 2. masked AO-DM-AO ---------------------------------------------
     pub fn cfgmm_aodmao2rho_loop_parallel(

@@ -224,3 +224,13 @@ def test_noalloc_rejects_what_dev_rejects(cm):
         msg_na = L.cfgmm_last_error()
         assert rc_dev == -1, (sa, sg, nao, ngrid, nset, ldtab, blk, msg_dev)
         assert rc_na == rc_dev and msg_na == msg_dev, (msg_na, msg_dev)
+
+
+def test_arm_wait_timeout_validation(cm):
+    """The failure-detection test hook checks its arguments on the host."""
+    L = ctypes.CDLL(cm.library_path)
+    L.cfgmm_test_arm_wait_timeout.argtypes = [ctypes.c_int, ctypes.c_double]
+    L.cfgmm_test_arm_wait_timeout.restype = ctypes.c_int
+    assert L.cfgmm_test_arm_wait_timeout(7, 10.0) == -1      # unknown precision
+    assert L.cfgmm_test_arm_wait_timeout(0, 0.0) == -1       # below 1 ms
+    assert L.cfgmm_test_arm_wait_timeout(1, 5000.0) == -1    # above 2 s
