@@ -538,7 +538,8 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
   if (err != cudaSuccess) return cuda_fail(err, "split plan setup");
   const int P = pair0;
   if (size_t(chunk0) > chunk_bound) return fail(CFGMM_ERR_CUDA, "split plan: chunk bound exceeded");
-  // ---- work list: matrix-major (one D in L2 at a time), heaviest first ----
+  // ---- work list: pair-major (a pair's phi tiles and D rows shared in L2 by
+  // the CTAs running at one time), heaviest pairs first ----
   int nitems = 0;
   err = cudaMemcpyAsync(&nitems, d_total, 4, cudaMemcpyDeviceToHost, s);
   if (err == cudaSuccess) err = cudaStreamSynchronize(s);
@@ -553,13 +554,12 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
     err = cudaMemcpyAsync(ucount.data(), at(o_ucount), size_t(P) * 4, cudaMemcpyDeviceToHost, s);
   if (err == cudaSuccess) err = cudaStreamSynchronize(s);
   if (err != cudaSuccess) return cuda_fail(err, "split plan work list");
-  auto weight = [&](const int4& it) {
-    const int nu = ucount[it.x];
-    return (nu + TK - 1) / TK - (it.y * tn) / TK;
-  };
   std::stable_sort(items.begin(), items.end(), [&](const int4& x, const int4& y) {
-    if (x.z != y.z) return x.z < y.z;
-    return weight(x) > weight(y);
+    const int kx = (ucount[x.x] + TK - 1) / TK, ky = (ucount[y.x] + TK - 1) / TK;
+    if (kx != ky) return kx > ky;
+    if (x.x != y.x) return x.x < y.x;
+    if (x.y != y.y) return x.y < y.y;
+    return x.z < y.z;
   });
   // partial row tiles: exact, from the unions
   std::vector<int> poff(size_t(P) + 1, 0);

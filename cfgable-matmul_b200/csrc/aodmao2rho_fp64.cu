@@ -532,7 +532,8 @@ aodm_fp64_pipe_kernel(const __grid_constant__ AodmArgs p,
         const int stage = fill % PSTAGES;
         if (fill >= PSTAGES &&
             !warp_wait(&empty[stage], ((fill / PSTAGES) - 1) & 1, err, kErrStageEmpty, lim)) {
-          cp_async_arrive_noinc(&full[stage]);  // keep the arrival count of the phase whole
+          // nothing is issued for this fill: no asynchronous arrival may be
+          // left pending on a barrier that no one waits for when the CTA exits
           break;
         }
         uint8_t* st = sm + stage * SB;

@@ -319,23 +319,19 @@ pair_scores(const uint32_t* __restrict__ bits, const int* __restrict__ cnt,
   sc[tid] = score;
   who[tid] = b;
   __syncthreads();
-  if (tid == 0) {
-    // the profitable candidates (score > 0), best first, ties by tile index
-    int m = 0;
-    for (;;) {
-      long long best = 0;
-      int bi = -1;
-      for (int i = 0; i < 2 * kWin; ++i)
-        if (sc[i] > best || (sc[i] == best && bi >= 0 && sc[i] > 0 && who[i] < who[bi])) {
-          best = sc[i];
-          bi = i;
-        }
-      if (bi < 0) break;
-      cand[size_t(q) * 2 * kWin + m++] = who[bi];
-      sc[bi] = LLONG_MIN;
-    }
-    ncand[q] = m;
+  // the profitable candidates (score > 0), best first, ties by tile index: each
+  // thread's rank is the number of candidates ordered before its own
+  if (score > 0) {
+    int rank = 0;
+    for (int i = 0; i < 2 * kWin; ++i)
+      rank += sc[i] > score || (sc[i] == score && who[i] < b);
+    cand[size_t(q) * 2 * kWin + rank] = b;
   }
+  const unsigned pos_w = __ballot_sync(0xffffffffu, score > 0);
+  __shared__ int npos[2];
+  if ((tid & 31) == 0) npos[tid >> 5] = __popc(pos_w);
+  __syncthreads();
+  if (tid == 0) ncand[q] = npos[0] + npos[1];
 }
 
 // Mutual-best matching over the candidate lists (kRounds rounds), then the
@@ -467,10 +463,11 @@ pair_union(const uint8_t* __restrict__ tab, size_t ldtab, int nao, int gsub,
 }
 
 // cbase[pi] (first phi chunk of each pair, from chunk0), and the items
-// (pair, row tile, DM, batch) of pairs pair0 .. pair0+npairs-1, heaviest
-// first (a counting sort on the chunks an item runs in the symmetric mode),
-// appended at items + *total; *total grows by their number, *chunks_end is
-// the chunk after the batch's last.
+// (pair, row tile, DM, batch) of pairs pair0 .. pair0+npairs-1 appended at
+// items + *total: pair-major (all of a pair's items together, so that the
+// CTAs running at one time share a few pairs' phi tiles and D rows in L2),
+// heaviest pairs first (a counting sort on the pair's chunk count);
+// *total grows by their number, *chunks_end is the chunk after the batch's last.
 __global__ void __launch_bounds__(1024)
 pair_build(const int* __restrict__ ucount, const int* __restrict__ npairs_d, int pair0, int nset,
            int batch, int tn, int max_kc, int chunk0, int* __restrict__ cbase,
@@ -503,14 +500,14 @@ pair_build(const int* __restrict__ ucount, const int* __restrict__ npairs_d, int
       for (int w = 0; w < 32; ++w) base_c += warp_c[w];
     __syncthreads();
   }
-  // histogram of item weights (chunks from the row tile's own on)
+  // items per chunk-count class of the pairs
   for (int pl = tid; pl < np; pl += 1024) {
     const int nu = ucount[pair0 + pl];
     const int kc = (nu + TK - 1) / TK, nt = (nu + tn - 1) / tn;
-    for (int t = 0; t < nt; ++t) atomicAdd(&hist[kc - (t * tn) / TK], nset);
+    atomicAdd(&hist[kc], nt * nset);
   }
   __syncthreads();
-  if (tid == 0) {  // heaviest first: cursor[w] = items of weight > w
+  if (tid == 0) {  // heaviest first: cursor[w] = items of pairs with more chunks than w
     int run = 0;
     for (int w = max_kc; w >= 0; --w) {
       const int c = hist[w];
@@ -524,11 +521,9 @@ pair_build(const int* __restrict__ ucount, const int* __restrict__ npairs_d, int
   for (int pl = tid; pl < np; pl += 1024) {
     const int nu = ucount[pair0 + pl];
     const int kc = (nu + TK - 1) / TK, nt = (nu + tn - 1) / tn;
-    for (int t = 0; t < nt; ++t) {
-      const int w = kc - (t * tn) / TK;
-      const int at = start + atomicAdd(&hist[w], nset);
-      for (int s = 0; s < nset; ++s) items[at + s] = make_int4(pair0 + pl, t, s, batch);
-    }
+    int at = start + atomicAdd(&hist[kc], nt * nset);
+    for (int t = 0; t < nt; ++t)
+      for (int s = 0; s < nset; ++s) items[at++] = make_int4(pair0 + pl, t, s, batch);
   }
   __syncthreads();
   if (tid == 0) {
