@@ -76,7 +76,7 @@ constexpr int TK = 32;    // union AOs per chunk: one INT8 MMA K step
 constexpr int NG = 3;     // gather groups of four warps
 constexpr int GW = 4 * NG;
 constexpr int THREADS = 32 * (GW + 2);
-constexpr int kStages = 4;        // pipeline depth (at least NG: see the row form)
+constexpr int kStages = 5;        // pipeline depth (at least NG: see the row form)
 constexpr int kBadExp = INT_MAX;  // scale of a row / point holding Inf or NaN
 constexpr int kWin = 32;          // pairing candidates on each side in key order
 constexpr int kSortMax = 4096;    // tiles sorted in shared memory (more: caller's order)
@@ -337,11 +337,18 @@ pair_scores(const uint32_t* __restrict__ bits, const int* __restrict__ cnt,
 // Mutual-best matching over the candidate lists (kRounds rounds), then the
 // pair list in key order: pairs[i] = (lo tile, hi tile or -1, batch, 0) for
 // every non-empty tile in exactly one entry; npairs[0] = their number.
+// The per-tile state lives in shared memory when it fits (kSortMax tiles),
+// else in the global scratch arrays.
 __global__ void __launch_bounds__(1024)
 pair_match(const int* __restrict__ order, const int* __restrict__ cand,
            const int* __restrict__ ncand, const int* __restrict__ cnt, int nbg, int batch,
-           int* __restrict__ partner, int* __restrict__ pos, int* __restrict__ choice,
+           int* __restrict__ partner_g, int* __restrict__ pos_g, int* __restrict__ choice_g,
            int4* __restrict__ pairs, int* __restrict__ npairs) {
+  extern __shared__ int match_s[];  // 3 * kSortMax ints when nbg <= kSortMax
+  const bool in_smem = nbg <= kSortMax;
+  int* partner = in_smem ? match_s : partner_g;
+  int* pos = in_smem ? match_s + kSortMax : pos_g;
+  int* choice = in_smem ? match_s + 2 * kSortMax : choice_g;
   const int tid = threadIdx.x;
   __shared__ int changed;
   __shared__ int warp_tot[32];
@@ -685,7 +692,7 @@ __device__ __forceinline__ uint32_t gather_selector(int qd) {
 // main kernel
 // ---------------------------------------------------------------------------
 template <int NSL, int STAGES>
-__global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
+__global__ void __maxnreg__(144) pair_main(PairArgs p) {  // 448 threads x 144 registers fit one SM
   using C = Cfg<NSL>;
   constexpr int TN = C::TN;
   extern __shared__ uint8_t smem_raw[];
@@ -786,6 +793,14 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
         asm volatile("prefetch.global.L2 [%0];" ::"l"(q0));
         asm volatile("prefetch.global.L2 [%0];" ::"l"(q0 + 8 * last));
       }
+      // the union columns of the group's next chunk are loaded one chunk ahead,
+      // so the D gather addresses never wait for them
+      int ivn[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int pcn = (kc0 + grp) * TK + 16 * hh + 4 * k + qd;
+        ivn[k] = pcn < nu ? __ldg(U + pcn) : -1;
+      }
       for (int c = kc0 + grp; c < kc; c += NG) {
         const uint32_t seq = seq0 + uint32_t(c - kc0);
         const int stg = int(seq % STAGES);
@@ -794,7 +809,9 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           pc[k] = c * TK + 16 * hh + 4 * k + qd;
-          iv[k] = pc[k] < nu ? __ldg(U + pc[k]) : -1;
+          iv[k] = ivn[k];
+          const int pcn = pc[k] + NG * TK;
+          ivn[k] = pcn < nu ? __ldg(U + pcn) : -1;
         }
         // symmetric D: only columns from the row's own position on (the
         // diagonal digits carry D_uu / 2)
@@ -847,44 +864,68 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
       tc::fence_after_sync();
       const uint32_t trow = tmem + (uint32_t(32 * wq) << 16);
       double acc = 0.0;
-      bool badrow = false;
-#pragma unroll 1
-      for (int oi = 0; grp + NG * oi < C::OCTETS; ++oi) {
+      bool badrow = false, released = false;
+      // the group's octets of this tile (warp-uniform): grp, grp+NG, ... below
+      // OCTETS whose first column lies inside U
+      int nocts = 0;
+      while (grp + NG * nocts < C::OCTETS && ut * TN + (grp + NG * nocts) * 8 < nu) ++nocts;
+      // phi_lhs of an octet's 8 columns at this lane's point, for AOs active in
+      // its block; the next octet's are requested before this one is combined
+      auto fetch = [&](int oi, double (&a)[8], bool (&on)[8]) {
         const int col0 = (grp + NG * oi) * 8;
-        if (ut * TN + col0 >= nu) break;  // warp-uniform: the rest of the tile is past U
-        uint32_t v[NSL][8];
-#pragma unroll
-        for (int L = 0; L < NSL; ++L)
-          tc::tmem_ld_32x32b_x8(trow + uint32_t(L * TN + col0), v[L]);
-        // phi_lhs of the 8 columns at this lane's point, for AOs active in its block
-        double a[8];
-        int tus[8];
-        bool on[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
           const int src = oi * 8 + j;
           const int uj = __shfl_sync(0xffffffffu, u_l, src);
           const int fj = __shfl_sync(0xffffffffu, f_l, src);
-          tus[j] = __shfl_sync(0xffffffffu, tu_l, src);
           on[j] = gval && ut * TN + col0 + j < nu && ((fj >> h) & 1);
           a[j] = on[j] ? B.ao_lhs[size_t(uj) * B.stride_grid + gpt] : 0.0;
         }
+      };
+      double a[8], an[8];
+      bool on[8], onn[8];
+      if (nocts > 0) fetch(0, a, on);
+#pragma unroll 1
+      for (int oi = 0; oi < nocts; ++oi) {
+        const int col0 = (grp + NG * oi) * 8;
+        uint32_t v[NSL][8];
+#pragma unroll
+        for (int L = 0; L < NSL; ++L)
+          tc::tmem_ld_32x32b_x8(trow + uint32_t(L * TN + col0), v[L]);
+        if (oi + 1 < nocts) fetch(oi + 1, an, onn);
         tc::tmem_ld_wait();
+        if (oi + 1 == nocts) {  // the accumulators are read: the MMA warp may go on
+          tc::fence_before_sync();
+          __syncwarp();
+          if (lane == 0) tc::mbar_arrive(acc_empty);
+          released = true;
+        }
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
+          const int tuj = __shfl_sync(0xffffffffu, tu_l, oi * 8 + j);
           uint32_t lv[NSL];
 #pragma unroll
           for (int L = 0; L < NSL; ++L) lv[L] = v[L][j];
           if (on[j]) {  // AOs inactive in this point's block take no part
-            if (tus[j] == kBadExp) {
+            if (tuj == kBadExp) {
               badrow = true;
             } else {
               const double x = combine_levels<NSL>(lv);
-              const int e = -tus[j];
+              const int e = -tuj;
               acc = fma(a[j], (e >= -1022 && e <= 1023) ? x * pow2(e) : ldexp(x, e), acc);
             }
           }
         }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          a[j] = an[j];
+          on[j] = onn[j];
+        }
+      }
+      if (!released) {
+        tc::fence_before_sync();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(acc_empty);
       }
       double res = 0.0;
       if (gval) {
@@ -894,9 +935,6 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
                                           : ldexp(acc, e);
         if (sym) res *= 2.0;
       }
-      tc::fence_before_sync();
-      __syncwarp();
-      if (lane == 0) tc::mbar_arrive(acc_empty);  // the MMA warp may overwrite the accumulators
       double* e2 = epi + (nitem & 1) * (NG * PT);
       e2[grp * PT + r] = res;
       __syncwarp();
@@ -1160,8 +1198,13 @@ cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream) {
   pair_sort<<<1, 1024, sort_smem, stream>>>(q.key, nbg, q.order);
   pair_scores<<<nbg, 2 * kWin, 0, stream>>>(q.bits, q.cnt, q.order, nbg, nwords, q.cand,
                                             q.ncand);
-  pair_match<<<1, 1024, 0, stream>>>(q.order, q.cand, q.ncand, q.cnt, nbg, q.batch, q.partner,
-                                     q.pos, q.choice, q.pairs + q.pair0, q.npairs);
+  constexpr size_t match_smem = size_t(3) * kSortMax * sizeof(int);
+  static const cudaError_t match_attr = cudaFuncSetAttribute(
+      pair_match, cudaFuncAttributeMaxDynamicSharedMemorySize, int(match_smem));
+  if (match_attr != cudaSuccess) return match_attr;
+  pair_match<<<1, 1024, match_smem, stream>>>(q.order, q.cand, q.ncand, q.cnt, nbg, q.batch,
+                                              q.partner, q.pos, q.choice, q.pairs + q.pair0,
+                                              q.npairs);
   pair_union<<<nbg, 256, 0, stream>>>(q.tab, q.ldtab, q.nao, gsub, q.pairs, q.npairs, q.pair0,
                                       q.ulist, q.uflag, q.ucount);
   const size_t hist = size_t(max_kc + 2) * sizeof(int);
