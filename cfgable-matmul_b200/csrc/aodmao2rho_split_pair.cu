@@ -692,7 +692,7 @@ __device__ __forceinline__ uint32_t gather_selector(int qd) {
 // main kernel
 // ---------------------------------------------------------------------------
 template <int NSL, int STAGES>
-__global__ void __maxnreg__(144) pair_main(PairArgs p) {  // 448 threads x 144 registers fit one SM
+__global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
   using C = Cfg<NSL>;
   constexpr int TN = C::TN;
   extern __shared__ uint8_t smem_raw[];

@@ -50,6 +50,7 @@ double aodm_plan_flops(const cfgmm_aodm_plan* plan);
 namespace {
 
 using Clock = std::chrono::steady_clock;
+constexpr int kLoaders = 4;  // molecules put on the device at once
 
 double ms_between(Clock::time_point a, Clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
@@ -170,8 +171,14 @@ struct cfgmm_server {
   std::condition_variable cv_work;  // worker: new requests, completions, stop
   std::condition_variable cv_done;  // waiters
   std::condition_variable cv_load;  // loader: molecules to put on the device
-  bool stop = false, stop_loader = false;  // the loader stops after the worker
-  std::thread worker, loader;
+  bool stop = false, stop_loader = false;  // the loaders stop after the worker
+  std::thread worker;
+  // molecules are put on the device by several loader threads at once, each on
+  // its own high-priority stream (the eval / mask / plan work of one molecule
+  // is serial, of different molecules independent)
+  std::vector<std::thread> loaders;
+  std::vector<cudaStream_t> load_streams;
+  size_t inflight = 0, max_inflight = 0;  // requests on the slots, and their maximum
   std::deque<uint64_t> to_load;  // tickets whose molecule is being loaded
   int loading = 0;
 
@@ -267,12 +274,12 @@ void release(cfgmm_server* s, Molecule& m) {
 // Puts the molecule's phi, mask and buffers on the device (worker thread,
 // without the lock: the molecule is reserved; the GPU work is on the admin
 // stream and finished on return).
-int materialize(cfgmm_server* s, Molecule& m, std::string* err) {
+int materialize(cfgmm_server* s, Molecule& m, cudaStream_t st, std::string* err) {
   const size_t phi = m.nao * m.ngrid * sizeof(double);
   const size_t nblk = (m.ngrid + s->blksize - 1) / s->blksize;
   const size_t nsh = m.sl.size();
   const MolLayout L = mol_layout(m, s->blksize);
-  cudaError_t e = cudaMallocAsync(&m.mem, L.bytes, s->admin);
+  cudaError_t e = cudaMallocAsync(&m.mem, L.bytes, st);
   if (e != cudaSuccess) {
     m.mem = nullptr;
     *err = cuda_msg(e, "molecule memory");
@@ -293,13 +300,13 @@ int materialize(cfgmm_server* s, Molecule& m, std::string* err) {
   }
   if (m.kind == kHost) {
     e = cudaMemcpyAsync(const_cast<double*>(m.d_lhs), m.src_lhs, phi, cudaMemcpyHostToDevice,
-                        s->admin);
+                        st);
     if (e == cudaSuccess && m.d_rhs != m.d_lhs)
       e = cudaMemcpyAsync(const_cast<double*>(m.d_rhs), m.src_rhs, phi, cudaMemcpyHostToDevice,
-                          s->admin);
+                          st);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(const_cast<uint8_t*>(m.d_tab), m.src_tab, m.nao * m.ldtab,
-                          cudaMemcpyHostToDevice, s->admin);
+                          cudaMemcpyHostToDevice, st);
   } else if (m.kind == kShells) {
     double* d_pts = reinterpret_cast<double*>(base + L.pts);
     double* d_xyz = reinterpret_cast<double*>(base + L.xyz);
@@ -308,27 +315,27 @@ int materialize(cfgmm_server* s, Molecule& m, std::string* err) {
     int* d_l = reinterpret_cast<int*>(base + L.l);
     int* d_row = reinterpret_cast<int*>(base + L.row);
     double* d_bmax = reinterpret_cast<double*>(base + L.bmax);
-    e = cudaMemcpyAsync(d_pts, m.pts.data(), m.ngrid * 3 * 8, cudaMemcpyHostToDevice, s->admin);
+    e = cudaMemcpyAsync(d_pts, m.pts.data(), m.ngrid * 3 * 8, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(d_xyz, m.sxyz.data(), nsh * 3 * 8, cudaMemcpyHostToDevice, s->admin);
+      e = cudaMemcpyAsync(d_xyz, m.sxyz.data(), nsh * 3 * 8, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(d_alpha, m.salpha.data(), nsh * 8, cudaMemcpyHostToDevice, s->admin);
+      e = cudaMemcpyAsync(d_alpha, m.salpha.data(), nsh * 8, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(d_norm, m.snorm.data(), nsh * 8, cudaMemcpyHostToDevice, s->admin);
+      e = cudaMemcpyAsync(d_norm, m.snorm.data(), nsh * 8, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(d_l, m.sl.data(), nsh * 4, cudaMemcpyHostToDevice, s->admin);
+      e = cudaMemcpyAsync(d_l, m.sl.data(), nsh * 4, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(d_row, m.srow.data(), nsh * 4, cudaMemcpyHostToDevice, s->admin);
+      e = cudaMemcpyAsync(d_row, m.srow.data(), nsh * 4, cudaMemcpyHostToDevice, st);
     double* ao = const_cast<double*>(m.d_lhs);
     if (e == cudaSuccess)
       e = cfgmm::eval_ao(ao, m.ngrid, d_pts, int(m.ngrid), d_xyz, d_l, d_alpha, d_norm, d_row,
-                         int(nsh), d_bmax, int(s->blksize), s->admin);
+                         int(nsh), d_bmax, int(s->blksize), st);
     // threshold: the (1 - density) quantile of the (shell, block) maxima
     double thr = -1.0;
     if (e == cudaSuccess && m.density < 1.0) {
       std::vector<double> h(nsh * nblk);
-      e = cudaMemcpyAsync(h.data(), d_bmax, h.size() * 8, cudaMemcpyDeviceToHost, s->admin);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(s->admin);
+      e = cudaMemcpyAsync(h.data(), d_bmax, h.size() * 8, cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
       if (e == cudaSuccess) {
         const size_t k = std::min(h.size() - 1, size_t((1.0 - m.density) * double(h.size() - 1)));
         std::nth_element(h.begin(), h.begin() + k, h.end());
@@ -337,19 +344,19 @@ int materialize(cfgmm_server* s, Molecule& m, std::string* err) {
     }
     if (e == cudaSuccess)
       e = cfgmm::mask_ao(ao, m.ngrid, int(m.ngrid), d_l, d_row, int(nsh), d_bmax, thr,
-                         const_cast<uint8_t*>(m.d_tab), m.ldtab, int(s->blksize), s->admin);
+                         const_cast<uint8_t*>(m.d_tab), m.ldtab, int(s->blksize), st);
   }
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s->admin);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     *err = cuda_msg(e, "molecule upload");
-    cudaFreeAsync(m.mem, s->admin);
+    cudaFreeAsync(m.mem, st);
     m.mem = nullptr;
     return CFGMM_ERR_CUDA;
   }
   return CFGMM_OK;
 }
 
-cfgmm_aodm_plan* plan_for(cfgmm_server* s, Molecule& m, size_t nset, int* rc) {
+cfgmm_aodm_plan* plan_for(cfgmm_server* s, Molecule& m, size_t nset, cudaStream_t st, int* rc) {
   auto it = m.plans.find(nset);
   if (it != m.plans.end()) return it->second;
   cfgmm_aodm_batch b;
@@ -363,7 +370,7 @@ cfgmm_aodm_plan* plan_for(cfgmm_server* s, Molecule& m, size_t nset, int* rc) {
   b.nset = nset;
   cfgmm_aodm_plan* plan = nullptr;
   *rc = cfgmm_aodm_plan_create(&plan, &b, 1, m.d_dms, m.nao, m.nao, nset, s->blksize, s->precision,
-                               0, s->admin);
+                               0, st);
   if (*rc != CFGMM_OK) return nullptr;
   m.plans[nset] = plan;
   return plan;
@@ -447,7 +454,7 @@ bool make_room(cfgmm_server* s, size_t need, uint64_t keep) {
 // molecule and the slot are reserved).  Returns a status and message.
 int launch(cfgmm_server* s, Request& r, Molecule& m, Slot& sl, std::string* err) {
   int rc = CFGMM_OK;
-  cfgmm_aodm_plan* plan = plan_for(s, m, r.nset, &rc);
+  cfgmm_aodm_plan* plan = plan_for(s, m, r.nset, s->admin, &rc);
   if (!plan) {
     *err = std::string("plan: ") + cfgmm_last_error();
     return rc;
@@ -521,7 +528,7 @@ Request* pick(cfgmm_server* s, int* slot_out) {
 
 // Puts molecules on the device (phi, mask, buffers, plan) one at a time on
 // the admin stream, beside the requests running on the slots.
-void loader_loop(cfgmm_server* s) {
+void loader_loop(cfgmm_server* s, cudaStream_t st) {
   cudaSetDevice(s->dev);
   std::unique_lock<std::mutex> lk(s->mu);
   for (;;) {
@@ -538,9 +545,17 @@ void loader_loop(cfgmm_server* s) {
     lk.unlock();
     std::string err;
     const Clock::time_point t0 = Clock::now();
-    int rc = materialize(s, m, &err);
+    int rc = materialize(s, m, st, &err);
     const Clock::time_point t1 = Clock::now();
-    if (rc == CFGMM_OK && !plan_for(s, m, r.nset, &rc)) err = std::string("plan: ") + cfgmm_last_error();
+    if (rc == CFGMM_OK && !plan_for(s, m, r.nset, st, &rc))
+      err = std::string("plan: ") + cfgmm_last_error();
+    if (rc == CFGMM_OK) {  // the worker's streams use the molecule after this
+      const cudaError_t e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) {
+        rc = CFGMM_ERR_CUDA;
+        err = cuda_msg(e, "molecule load");
+      }
+    }
     const Clock::time_point t2 = Clock::now();
     lk.lock();
     s->lat_load.push_back(ms_between(t0, t1));
@@ -574,6 +589,7 @@ void worker_loop(cfgmm_server* s) {
         Request& r = *sl.req;
         cudaEventElapsedTime(&r.device_ms, sl.e0, sl.e1);
         sl.req = nullptr;
+        --s->inflight;
         finish(s, r, CFGMM_OK, "");
       }
     }
@@ -582,12 +598,14 @@ void worker_loop(cfgmm_server* s) {
     int slot = -1;
     if (Request* r = pick(s, &slot)) {
       Molecule& m = *s->mols.find(r->mol)->second;
+      s->max_inflight = std::max(s->max_inflight, ++s->inflight);
       lk.unlock();
       std::string err;
       const int rc = launch(s, *r, m, s->slots[slot], &err);
       lk.lock();
       if (rc != CFGMM_OK) {
         s->slots[slot].req = nullptr;
+        --s->inflight;
         finish(s, *r, rc, err);
       }
       continue;  // look for more work before sleeping
@@ -676,6 +694,9 @@ int cfgmm_server_create(cfgmm_server** out, size_t hbm_budget, int nslots, int p
   int prio_lo = 0, prio_hi = 0;
   cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
   cudaError_t e = cudaStreamCreateWithPriority(&s->admin, cudaStreamNonBlocking, prio_hi);
+  s->load_streams.assign(kLoaders, nullptr);
+  for (cudaStream_t& ls : s->load_streams)
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&ls, cudaStreamNonBlocking, prio_hi);
   for (Slot& sl : s->slots) {
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&sl.e0);
@@ -684,7 +705,7 @@ int cfgmm_server_create(cfgmm_server** out, size_t hbm_budget, int nslots, int p
   if (e != cudaSuccess) return fail(CFGMM_ERR_CUDA, cuda_msg(e, "server streams"));
   cfgmm_server* raw = s.release();
   raw->worker = std::thread(worker_loop, raw);
-  raw->loader = std::thread(loader_loop, raw);
+  for (cudaStream_t ls : raw->load_streams) raw->loaders.emplace_back(loader_loop, raw, ls);
   *out = raw;
   return CFGMM_OK;
 }
@@ -702,7 +723,8 @@ int cfgmm_server_destroy(cfgmm_server* s) {
     s->stop_loader = true;
   }
   s->cv_load.notify_all();
-  if (s->loader.joinable()) s->loader.join();
+  for (std::thread& t : s->loaders)
+    if (t.joinable()) t.join();
   for (auto& kv : s->mols)
     if (kv.second->resident) release(s, *kv.second);
   cudaStreamSynchronize(s->admin);
@@ -710,6 +732,10 @@ int cfgmm_server_destroy(cfgmm_server* s) {
     cudaStreamDestroy(sl.stream);
     cudaEventDestroy(sl.e0);
     cudaEventDestroy(sl.e1);
+  }
+  for (cudaStream_t ls : s->load_streams) {
+    cudaStreamSynchronize(ls);
+    cudaStreamDestroy(ls);
   }
   cudaStreamDestroy(s->admin);
   delete s;
@@ -877,7 +903,8 @@ const char* cfgmm_server_stats(cfgmm_server* s) {
       "\"peak_bytes\":%zu,\"flops_completed\":%.6e,\"latency_ms\":{\"p50\":%.4f,\"p99\":%.4f,\"max\":%.4f},"
       "\"warm_latency_ms\":{\"p50\":%.4f,\"p99\":%.4f,\"count\":%zu},"
       "\"load_ms\":{\"p50\":%.4f,\"max\":%.4f},\"plan_ms\":{\"p50\":%.4f,\"max\":%.4f},"
-      "\"queue_ms\":{\"p50\":%.4f,\"p99\":%.4f},\"device_ms\":{\"p50\":%.4f,\"p99\":%.4f}}",
+      "\"queue_ms\":{\"p50\":%.4f,\"p99\":%.4f},\"device_ms\":{\"p50\":%.4f,\"p99\":%.4f},"
+      "\"max_inflight\":%zu,\"loaders\":%d}",
       (unsigned long long)s->completed, (unsigned long long)s->failed, s->pending.size(),
       s->mols.size(), resident, (unsigned long long)s->admitted_molecules,
       (unsigned long long)s->evictions, s->budget, s->used, s->peak, s->flops_done,
@@ -886,7 +913,7 @@ const char* cfgmm_server_stats(cfgmm_server* s) {
       s->lat_warm.size(), percentile(s->lat_load, 0.5), percentile(s->lat_load, 1.0),
       percentile(s->lat_plan, 0.5), percentile(s->lat_plan, 1.0), percentile(s->lat_queue, 0.5),
       percentile(s->lat_queue, 0.99), percentile(s->lat_device, 0.5),
-      percentile(s->lat_device, 0.99));
+      percentile(s->lat_device, 0.99), s->max_inflight, kLoaders);
   s->stats_json = buf;
   return s->stats_json.c_str();
 }
