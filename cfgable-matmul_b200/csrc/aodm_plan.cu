@@ -165,7 +165,8 @@ cudaError_t pair_prepare_run(cfgmm_aodm_plan* plan, cudaStream_t s) {
 
 cudaError_t pair_run_on(cfgmm_aodm_plan* plan, cudaStream_t s) {
   cudaError_t err = pair_prepare_run(plan, s);
-  if (err == cudaSuccess) err = cfgmm::split_pair_launch_main(plan->pargs, plan->nsl, s);
+  if (err == cudaSuccess)
+    err = cfgmm::split_pair_launch_main(plan->pargs, plan->nsl, s, false, plan->stages);
   if (err == cudaSuccess)
     err = cfgmm::split_pair_launch_reduce(plan->pargs, plan->nsl, plan->d_npairs, 0, plan->npairs,
                                           s);
@@ -614,9 +615,59 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
   // total[1]: the asymmetry flag (the half contraction also needs one phi array per batch)
   a.asym = cfgmm::aodm_sym_enabled() && same_phi(batches, nbatch) ? d_total + 1 : nullptr;
 
+  // ---- autotuning: pipeline depth of the persistent kernel ----
+  std::string tune = "default";
+  char key[256];
+  double work = 0.0;
+  for (int q = 0; q < P; ++q) work += double(ucount[q]) * ucount[q];
+  std::snprintf(key, sizeof(key), "aodm_split_pair%d:nao%d:work%d:items%d:nset%zu:blk%zu", nsl,
+                bucket(double(nao)), bucket(work), bucket(double(nitems)), nset_max, blksize);
+  plan->stages = 0;
+  if (!(flags & CFGMM_PLAN_NO_TUNE) && nitems > 0) {
+    cfgmm::AodmConfig c{};
+    if (cache_lookup(key, &c)) {
+      plan->stages = c.ns;
+      tune = "cache";
+    } else {
+      if ((err = pair_prepare_run(plan, s)) != cudaSuccess) return cuda_fail(err, "autotune");
+      cudaEvent_t e0, e1;
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      double best_ms = 1e30;
+      std::string trials;
+      for (int st : {3, 4, 5}) {
+        float best = 1e30f;
+        for (int rep = 0; rep < 3 && err == cudaSuccess; ++rep) {
+          err = cudaEventRecord(e0, s);
+          if (err == cudaSuccess) err = cfgmm::split_pair_launch_main(a, nsl, s, false, st);
+          if (err == cudaSuccess) err = cudaEventRecord(e1, s);
+          if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+          float t = 0.f;
+          if (err == cudaSuccess) cudaEventElapsedTime(&t, e0, e1);
+          if (rep > 0) best = std::min(best, t);
+        }
+        if (err != cudaSuccess) break;
+        char tb[96];
+        std::snprintf(tb, sizeof(tb), "%s{\"stages\":%d,\"ms\":%.4f}", trials.empty() ? "" : ",",
+                      st, best);
+        trials += tb;
+        if (best < best_ms) {
+          best_ms = best;
+          plan->stages = st;
+        }
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      if (err != cudaSuccess) return cuda_fail(err, "autotune");
+      cache_store(key, cfgmm::AodmConfig{plan->stages, 0}, best_ms);
+      tune = "[" + trials + "]";
+    }
+  }
+
   // ---- capture the run ----
   if (!(flags & CFGMM_PLAN_NO_GRAPH)) {
-    err = cfgmm::split_pair_launch_main(a, nsl, s, true);  // attributes outside the capture
+    // attributes outside the capture
+    err = cfgmm::split_pair_launch_main(a, nsl, s, true, plan->stages);
     if (err == cudaSuccess)
       err = capture(plan, [&](cudaStream_t cs) { return pair_run_on(plan, cs); });
     if (err != cudaSuccess) return cuda_fail(err, "graph capture");
@@ -625,10 +676,12 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
   std::snprintf(buf, sizeof(buf),
                 "{\"precision\":\"split\",\"form\":\"pair\",\"digits\":%d,\"batches\":%zu,"
                 "\"items\":%d,\"block_tiles\":%zu,\"pairs\":%d,\"phi_chunks\":%d,"
-                "\"flops\":%.6e,\"config\":{\"row_tile\":%d},\"graph\":%s,\"tuning\":\"none\"}",
-                nsl, nbatch, nitems, nbg_tot, P, chunk0, plan->flops, tn,
+                "\"flops\":%.6e,\"config\":{\"row_tile\":%d,\"stages\":%d},\"graph\":%s,"
+                "\"tuning\":",
+                nsl, nbatch, nitems, nbg_tot, P, chunk0, plan->flops, tn, plan->stages,
                 plan->exec ? "true" : "false");
-  plan->info = buf;
+  plan->info = std::string(buf) + (tune[0] == '[' ? tune : "\"" + tune + "\"") + ",\"key\":\"" +
+               key + "\"}";
   return CFGMM_OK;
 }
 

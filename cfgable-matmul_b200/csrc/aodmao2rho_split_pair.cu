@@ -76,7 +76,7 @@ constexpr int TK = 32;    // union AOs per chunk: one INT8 MMA K step
 constexpr int NG = 3;     // gather groups of four warps
 constexpr int GW = 4 * NG;
 constexpr int THREADS = 32 * (GW + 2);
-constexpr int kStages = 5;        // pipeline depth (at least NG: see the row form)
+constexpr int kStages = 4;        // default pipeline depth (at least NG: see the row form)
 constexpr int kBadExp = INT_MAX;  // scale of a row / point holding Inf or NaN
 constexpr int kWin = 32;          // pairing candidates on each side in key order
 constexpr int kSortMax = 4096;    // tiles sorted in shared memory (more: caller's order)
@@ -668,8 +668,11 @@ pair_d_digits(const double* __restrict__ dms, size_t stride_ao, size_t dm_stride
   const int e = bad ? kBadExp : exp_for(mx);
   if (lane == 0) tau[row] = e;
   uint2* out = dsl + size_t(row) * nao;
+  // symmetric mode: the gather reads only v >= u (union positions ascend with
+  // the AO index), so the strict lower triangle is not written
+  const int v0 = half_diag ? (u & ~31) + lane : lane;
 #pragma unroll 4
-  for (int v = lane; v < nao; v += 32)
+  for (int v = v0; v < nao; v += 32)
     out[v] = e != kBadExp ? digits_of<NSL>(half_diag && v == u ? 0.5 * d[v] : d[v], e)
                           : make_uint2(0u, 0u);
 }
@@ -864,49 +867,52 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
       tc::fence_after_sync();
       const uint32_t trow = tmem + (uint32_t(32 * wq) << 16);
       double acc = 0.0;
-      bool badrow = false, released = false;
-      // the group's octets of this tile (warp-uniform): grp, grp+NG, ... below
-      // OCTETS whose first column lies inside U
+      bool badrow = false;
+      // the group's columns of this tile, in quartets (warp-uniform): octets
+      // grp, grp+NG, ... below OCTETS whose first column lies inside U
       int nocts = 0;
       while (grp + NG * nocts < C::OCTETS && ut * TN + (grp + NG * nocts) * 8 < nu) ++nocts;
-      // phi_lhs of an octet's 8 columns at this lane's point, for AOs active in
-      // its block; the next octet's are requested before this one is combined
-      auto fetch = [&](int oi, double (&a)[8], bool (&on)[8]) {
-        const int col0 = (grp + NG * oi) * 8;
+      const int nq = 2 * nocts;
+      // phi_lhs of a quartet's 4 columns at this lane's point, for AOs active in
+      // its block (0 and inactive elsewhere); the next quartet's are requested
+      // before this one is combined
+      auto fetch = [&](int qi, double (&a)[4], uint32_t& on) {
+        const int col0 = (grp + NG * (qi >> 1)) * 8 + 4 * (qi & 1);
+        on = 0;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const int src = oi * 8 + j;
+        for (int j = 0; j < 4; ++j) {
+          const int src = qi * 4 + j;  // lane holding the column (octet qi/2, column 4(qi&1)+j)
           const int uj = __shfl_sync(0xffffffffu, u_l, src);
           const int fj = __shfl_sync(0xffffffffu, f_l, src);
-          on[j] = gval && ut * TN + col0 + j < nu && ((fj >> h) & 1);
-          a[j] = on[j] ? B.ao_lhs[size_t(uj) * B.stride_grid + gpt] : 0.0;
+          const bool o = gval && ut * TN + col0 + j < nu && ((fj >> h) & 1);
+          on |= uint32_t(o) << j;
+          a[j] = o ? B.ao_lhs[size_t(uj) * B.stride_grid + gpt] : 0.0;
         }
       };
-      double a[8], an[8];
-      bool on[8], onn[8];
-      if (nocts > 0) fetch(0, a, on);
+      double a[4], an[4];
+      uint32_t on = 0, onn = 0;
+      if (nq > 0) fetch(0, a, on);
 #pragma unroll 1
-      for (int oi = 0; oi < nocts; ++oi) {
-        const int col0 = (grp + NG * oi) * 8;
-        uint32_t v[NSL][8];
+      for (int qi = 0; qi < nq; ++qi) {
+        const int col0 = (grp + NG * (qi >> 1)) * 8 + 4 * (qi & 1);
+        uint32_t v[NSL][4];
 #pragma unroll
         for (int L = 0; L < NSL; ++L)
-          tc::tmem_ld_32x32b_x8(trow + uint32_t(L * TN + col0), v[L]);
-        if (oi + 1 < nocts) fetch(oi + 1, an, onn);
+          tc::tmem_ld_32x32b_x4(trow + uint32_t(L * TN + col0), v[L]);
+        if (qi + 1 < nq) fetch(qi + 1, an, onn);
         tc::tmem_ld_wait();
-        if (oi + 1 == nocts) {  // the accumulators are read: the MMA warp may go on
+        if (qi + 1 == nq) {  // the accumulators are read: the MMA warp may go on
           tc::fence_before_sync();
           __syncwarp();
           if (lane == 0) tc::mbar_arrive(acc_empty);
-          released = true;
         }
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const int tuj = __shfl_sync(0xffffffffu, tu_l, oi * 8 + j);
+        for (int j = 0; j < 4; ++j) {
+          const int tuj = __shfl_sync(0xffffffffu, tu_l, qi * 4 + j);
           uint32_t lv[NSL];
 #pragma unroll
           for (int L = 0; L < NSL; ++L) lv[L] = v[L][j];
-          if (on[j]) {  // AOs inactive in this point's block take no part
+          if ((on >> j) & 1) {  // AOs inactive in this point's block take no part
             if (tuj == kBadExp) {
               badrow = true;
             } else {
@@ -917,12 +923,10 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
           }
         }
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          a[j] = an[j];
-          on[j] = onn[j];
-        }
+        for (int j = 0; j < 4; ++j) a[j] = an[j];
+        on = onn;
       }
-      if (!released) {
+      if (nq == 0) {
         tc::fence_before_sync();
         __syncwarp();
         if (lane == 0) tc::mbar_arrive(acc_empty);
@@ -1146,14 +1150,27 @@ size_t aodmao2rho_split_pair_workspace(size_t nao, size_t ngrid, size_t nset, si
   return layout(nao, ngrid, nset, blk, nsl).bytes;
 }
 
+int split_pair_stages() {  // CFGMM_SPLIT_STAGES (3..5) or the default, read per call
+  const char* e = std::getenv("CFGMM_SPLIT_STAGES");
+  const int v = e ? std::atoi(e) : kStages;
+  return v >= NG && v <= 5 ? v : kStages;
+}
+
 cudaError_t split_pair_launch_main(const PairArgs& a, int nsl, cudaStream_t stream,
-                                   bool attrs_only) {
+                                   bool attrs_only, int stages) {
   int dev = 0, nsm = 0;
   cudaError_t err = cudaGetDevice(&dev);
   if (err == cudaSuccess) err = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (err != cudaSuccess) return err;
-  return nsl == 6 ? launch_pair_main_t<6, kStages>(nsm, a, stream, attrs_only)
-                  : launch_pair_main_t<7, kStages>(nsm, a, stream, attrs_only);
+  if (stages < NG || stages > 5) stages = split_pair_stages();
+  if (nsl == 6) {
+    if (stages == 3) return launch_pair_main_t<6, 3>(nsm, a, stream, attrs_only);
+    if (stages == 5) return launch_pair_main_t<6, 5>(nsm, a, stream, attrs_only);
+    return launch_pair_main_t<6, 4>(nsm, a, stream, attrs_only);
+  }
+  if (stages == 3) return launch_pair_main_t<7, 3>(nsm, a, stream, attrs_only);
+  if (stages == 5) return launch_pair_main_t<7, 5>(nsm, a, stream, attrs_only);
+  return launch_pair_main_t<7, 4>(nsm, a, stream, attrs_only);
 }
 
 cudaError_t split_pair_launch_reduce(const PairArgs& a, int nsl, const int* npairs, int pair0,
