@@ -164,7 +164,8 @@ cudaError_t pair_prepare_run(cfgmm_aodm_plan* plan, cudaStream_t s) {
 }
 
 cudaError_t pair_run_on(cfgmm_aodm_plan* plan, cudaStream_t s) {
-  cudaError_t err = pair_prepare_run(plan, s);
+  cudaError_t err = cudaMemsetAsync(plan->pargs.counter, 0, sizeof(int), s);
+  if (err == cudaSuccess) err = pair_prepare_run(plan, s);
   if (err == cudaSuccess)
     err = cfgmm::split_pair_launch_main(plan->pargs, plan->nsl, s, false, plan->stages);
   if (err == cudaSuccess)
@@ -610,6 +611,7 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
   a.gsub = gsub;
   a.max_t = int((nao + tn - 1) / tn);
   a.nset_max = int(nset_max);
+  a.counter = d_total + 3;
   a.wait_ns = 0;  // the default bound
   a.inject = 0;
   // total[1]: the asymmetry flag (the half contraction also needs one phi array per batch)
@@ -638,7 +640,8 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
       for (int st : {3, 4, 5}) {
         float best = 1e30f;
         for (int rep = 0; rep < 3 && err == cudaSuccess; ++rep) {
-          err = cudaEventRecord(e0, s);
+          err = cudaMemsetAsync(a.counter, 0, sizeof(int), s);
+          if (err == cudaSuccess) err = cudaEventRecord(e0, s);
           if (err == cudaSuccess) err = cfgmm::split_pair_launch_main(a, nsl, s, false, st);
           if (err == cudaSuccess) err = cudaEventRecord(e1, s);
           if (err == cudaSuccess) err = cudaEventSynchronize(e1);

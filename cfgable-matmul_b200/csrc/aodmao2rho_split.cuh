@@ -107,6 +107,7 @@ struct PairArgs {
   const int* poff;        // [pair] first partial row tile, or null: pair * max_t
   int nao, blk, gsub, max_t, nset_max;
   const int* asym;        // null, or 0 when every D_s is symmetric (half contraction)
+  int* counter;           // work items drawn so far (zeroed before each launch)
   unsigned long long wait_ns;  // bound of every wait in the kernel (0: the default 2 s)
   int inject;             // test hook: nonzero = the first phi stage is never published
 };

@@ -81,6 +81,7 @@ constexpr int kBadExp = INT_MAX;  // scale of a row / point holding Inf or NaN
 constexpr int kWin = 32;          // pairing candidates on each side in key order
 constexpr int kSortMax = 4096;    // tiles sorted in shared memory (more: caller's order)
 constexpr int kRounds = 8;        // mutual-best matching rounds
+constexpr int kRing = 4;          // work items in flight between the kernel's roles
 static_assert(kStages >= NG, "a group's parity wait needs at least NG stages");
 
 template <int NSL>
@@ -714,6 +715,12 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
   // flight at most: a group cannot reach item n+2's epilogue before group 0
   // has finished item n+1's)
   double* epi = reinterpret_cast<double*>(smem + STAGES * C::STAGE + 256);  // [2][NG][PT]
+  // the work-item ring: the loader thread draws items from the global counter
+  // (dynamic scheduling: the list is pair-major, heaviest pairs first) and
+  // every role reads them from here in the same order
+  uint64_t* ifull = reinterpret_cast<uint64_t*>(epi + 2 * NG * PT);  // [kRing]
+  uint64_t* iempty = ifull + kRing;                                   // [kRing]
+  int* ring = reinterpret_cast<int*>(iempty + kRing);                 // [kRing]
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int* err = &g_pair_error;
@@ -729,6 +736,10 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
     tc::mbar_init(drain, 1);
     tc::mbar_init(&epi_full[0], GW);
     tc::mbar_init(&epi_full[1], GW);
+    for (int r = 0; r < kRing; ++r) {
+      tc::mbar_init(&ifull[r], 1);
+      tc::mbar_init(&iempty[r], GW + 2);  // every warp reads every item
+    }
     tc::mbar_fence_init();
   }
   if (warp == GW) {
@@ -741,6 +752,18 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
   const uint32_t tmem = *tmem_slot;
   const int total = p.total[0];
   const bool sym = p.asym != nullptr && *p.asym == 0;
+  // item n of this CTA (total when there are no more), read from the ring by
+  // lane 0 of the calling warp and broadcast; every warp calls it for n = 0, 1, ...
+  auto item_of = [&](uint32_t n, bool whole_warp) -> int {
+    int t = total;
+    if (!whole_warp || lane == 0) {
+      if (tc::mbar_wait(&ifull[n % kRing], (n / kRing) & 1, err, 40, false, lim))
+        t = *reinterpret_cast<volatile int*>(&ring[n % kRing]);
+      tc::mbar_arrive(&iempty[n % kRing]);
+    }
+    if (whole_warp) t = __shfl_sync(0xffffffffu, t, 0);
+    return t;
+  };
 
   if (warp < GW) {
     // ---------------- gather D digits, then the epilogue ----------------
@@ -755,7 +778,9 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
     const uint32_t sel_a = gather_selector(qd), sel_b = sel_a + 0x1111u;
     uint32_t seq0 = 0, nitem = 0;
     bool ok = true;
-    for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++nitem) {
+    for (;; ++nitem) {
+      const int t = item_of(nitem, true);
+      if (t >= total || !ok) break;
       const int4 it = p.items[t];
       const int pi = it.x, ut = it.y, s = it.z;
       const PairBatch& B = batch_of(p, it.w);
@@ -958,7 +983,9 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
       const uint32_t idesc = tc::idesc_i8(PT, TN);
       uint32_t seq = 0, nitem = 0;
       bool ok = true;
-      for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++nitem) {
+      for (;; ++nitem) {
+        const int t = item_of(nitem, false);
+        if (t >= total || !ok) break;
         const int4 it = p.items[t];
         const int nu = p.ucount[it.x];
         const int kc = (nu + TK - 1) / TK;
@@ -1013,7 +1040,20 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
 #pragma unroll
       for (int s = 0; s < STAGES; ++s) issued[s] = 0;
       bool ok = true;
-      for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+      for (uint32_t n = 0;; ++n) {
+        // draw the next item into the ring slot, once every warp has read the
+        // slot's previous item
+        const int slot = int(n % kRing);
+        int t = total;
+        if (ok && (n < kRing || tc::mbar_wait(&iempty[slot], ((n / kRing) - 1) & 1, err, 41,
+                                              false, lim))) {
+          t = atomicAdd(p.counter, 1);
+          if (t > total) t = total;
+        }
+        ring[slot] = t;
+        tc::mbar_arrive(&ifull[slot]);  // release: the slot's value is visible to the waiters
+        tc::mbar_arrive(&iempty[slot]);  // this warp's own read
+        if (t >= total || !ok) break;
         const int4 it = p.items[t];
         const int nu = p.ucount[it.x];
         const int kc = (nu + TK - 1) / TK;
@@ -1081,7 +1121,8 @@ pair_reduce(PairArgs p, const int* __restrict__ npairs, int pair0) {
 
 template <int NSL, int STAGES>
 cudaError_t launch_pair_main_t(int nsm, const PairArgs& a, cudaStream_t stream, bool attrs_only) {
-  constexpr size_t smem = size_t(STAGES) * Cfg<NSL>::STAGE + 1024 + 256 + 2 * NG * PT * 8;
+  constexpr size_t smem =
+      size_t(STAGES) * Cfg<NSL>::STAGE + 1024 + 256 + 2 * NG * PT * 8 + kRing * (16 + 4);
   cudaError_t err = cudaFuncSetAttribute(pair_main<NSL, STAGES>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (err != cudaSuccess || attrs_only) return err;
@@ -1299,9 +1340,9 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   uint2* dsl = static_cast<uint2*>(at(L.dsl));
   int* tau = static_cast<int*>(at(L.tau));
 
-  // total[0]: items, total[1]: asymmetry flag, total[2]: chunks
+  // total[0]: items, total[1]: asymmetry flag, total[2]: chunks, total[3]: item counter
   int* asym = aodm_sym_enabled() && ao_lhs == ao_rhs ? q.total + 1 : nullptr;
-  cudaError_t err = cudaMemsetAsync(q.total, 0, 3 * sizeof(int), stream);
+  cudaError_t err = cudaMemsetAsync(q.total, 0, 4 * sizeof(int), stream);
   if (err != cudaSuccess) return err;
   // The D chain (symmetry check, D digits) runs on a side stream beside the
   // phi chain (block lists, pairing, unions, work list, phi tiles); the side
@@ -1341,6 +1382,7 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   a.max_t = (nao + tn - 1) / tn;
   a.nset_max = nset;
   a.asym = asym;
+  a.counter = q.total + 3;
   unsigned long long armed_ns = 0;
   if (take_wait_injection(1, &armed_ns)) {  // cfgmm_test_arm_wait_timeout
     inject = 1;
