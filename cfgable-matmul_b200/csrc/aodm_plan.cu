@@ -637,7 +637,7 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
       cudaEventCreate(&e1);
       double best_ms = 1e30;
       std::string trials;
-      for (int st : {3, 4, 5}) {
+      for (int st : {cfgmm::split_pair_stages()}) {
         float best = 1e30f;
         for (int rep = 0; rep < 3 && err == cudaSuccess; ++rep) {
           err = cudaMemsetAsync(a.counter, 0, sizeof(int), s);

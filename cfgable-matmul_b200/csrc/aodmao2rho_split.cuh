@@ -152,7 +152,8 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
 cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream);
 cudaError_t split_pair_prepare_d(const double* dms, size_t stride_ao, int nao, int nset, int nsl,
                                  uint2* dsl, int* tau, cudaStream_t stream, const int* asym);
-// stages: pipeline depth 3..5, 0 = CFGMM_SPLIT_STAGES or the default (4)
+int split_pair_stages();  // the pair kernel's pipeline depth
+// stages: ignored (the pair form's pipeline depth is fixed: split_pair_stages())
 cudaError_t split_pair_launch_main(const PairArgs& a, int nsl, cudaStream_t stream,
                                    bool attrs_only = false, int stages = 0);
 cudaError_t split_pair_launch_reduce(const PairArgs& a, int nsl, const int* npairs, int pair0,

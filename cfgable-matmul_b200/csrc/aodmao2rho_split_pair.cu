@@ -64,6 +64,7 @@
 
 #include "aodmao2rho_fp64.cuh"
 #include "aodmao2rho_split.cuh"
+#include "common.cuh"
 #include "side_stream.cuh"
 #include "tcgen05.cuh"
 
@@ -76,7 +77,7 @@ constexpr int TK = 32;    // union AOs per chunk: one INT8 MMA K step
 constexpr int NG = 3;     // gather groups of four warps
 constexpr int GW = 4 * NG;
 constexpr int THREADS = 32 * (GW + 2);
-constexpr int kStages = 4;        // default pipeline depth (at least NG: see the row form)
+constexpr int kStages = 3;        // pipeline depth (at least NG: see the row form)
 constexpr int kBadExp = INT_MAX;  // scale of a row / point holding Inf or NaN
 constexpr int kWin = 32;          // pairing candidates on each side in key order
 constexpr int kSortMax = 4096;    // tiles sorted in shared memory (more: caller's order)
@@ -95,6 +96,14 @@ struct Cfg {
   static constexpr int WROWS = TN / 4;     // D rows per gather warp
   static constexpr int STEPS = WROWS / 4;  // four rows per step
   static constexpr int OCTETS = TN / 8;    // TMEM column octets of one level
+  static constexpr int MAXQ = 2 * ((OCTETS + NG - 1) / NG);  // epilogue quartets per group
+  // shared memory of a launch: stages, barriers, the groups' sums, the
+  // item ring and the epilogue's phi_lhs values ([warp][column][lane])
+  template <int STAGES>
+  static constexpr size_t smem_bytes() {
+    return size_t(STAGES) * STAGE + 1024 + 256 + 2 * NG * PT * 8 + kRing * (16 + 4) +
+           size_t(GW) * 4 * MAXQ * 32 * 8;
+  }
   static_assert(NSL * TN <= 512, "level accumulators exceed the TMEM columns");
   static_assert(STAGE % 256 == 0 && A_STAGE % 256 == 0, "32-byte swizzle atoms");
   static_assert(WROWS % 4 == 0 && (OCTETS + NG - 1) / NG * 8 <= 32, "epilogue columns per group");
@@ -721,6 +730,7 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
   uint64_t* ifull = reinterpret_cast<uint64_t*>(epi + 2 * NG * PT);  // [kRing]
   uint64_t* iempty = ifull + kRing;                                   // [kRing]
   int* ring = reinterpret_cast<int*>(iempty + kRing);                 // [kRing]
+  double* phl_all = reinterpret_cast<double*>(ring + kRing);          // [GW][4 MAXQ][32]
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int* err = &g_pair_error;
@@ -776,30 +786,143 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
     const int qd = lane >> 3, ri = (lane >> 1) & 3, hh = lane & 1;
     const bool b1 = (qd & 2) != 0, b0 = (qd & 1) != 0;
     const uint32_t sel_a = gather_selector(qd), sel_b = sel_a + 0x1111u;
-    uint32_t seq0 = 0, nitem = 0;
-    bool ok = true;
-    for (;; ++nitem) {
-      const int t = item_of(nitem, true);
-      if (t >= total || !ok) break;
+    // this warp's phi_lhs values for the epilogue: [group column][lane]
+    double* phl = phl_all + size_t(warp) * (4 * C::MAXQ * 32);
+    struct Item {
+      int t, pi, ut, s, w, nu, kc, kc0;
+      int iu[C::STEPS];  // AO of the D row this lane loads at each step (-1: none)
+    };
+    auto setup = [&](int t, Item& g) {
+      g.t = t;
+      if (t >= total) return;
       const int4 it = p.items[t];
-      const int pi = it.x, ut = it.y, s = it.z;
-      const PairBatch& B = batch_of(p, it.w);
-      const int nu = p.ucount[pi];
-      const int kc = (nu + TK - 1) / TK;
-      const int kc0 = sym ? (ut * TN) / TK : 0;
-      const int* U = p.ulist + size_t(pi) * p.nao;
-      const uint2* dset = p.dsl + size_t(s) * p.nao * p.nao;
-      int iu[C::STEPS], prow[C::STEPS];
+      g.pi = it.x;
+      g.ut = it.y;
+      g.s = it.z;
+      g.w = it.w;
+      g.nu = p.ucount[g.pi];
+      g.kc = (g.nu + TK - 1) / TK;
+      g.kc0 = sym ? (g.ut * TN) / TK : 0;
+      const int* U = p.ulist + size_t(g.pi) * p.nao;
 #pragma unroll
       for (int st = 0; st < C::STEPS; ++st) {
-        prow[st] = ut * TN + C::WROWS * wq + 4 * st + ri;
-        iu[st] = prow[st] < nu ? __ldg(U + prow[st]) : -1;
+        const int prow = g.ut * TN + C::WROWS * wq + 4 * st + ri;
+        g.iu[st] = prow < g.nu ? __ldg(U + prow) : -1;
       }
-      // what the epilogue reads is requested now, while the chunks run: lane l
-      // holds column l of the group's columns (octets grp, grp+NG, ...): its
-      // AO, membership flags and row scale; phi_lhs of those rows at this
-      // warp's 32 points goes to L2
-      const int4 pr = p.pairs[pi];
+    };
+    // the union columns this lane loads in chunk c (-1: past the list)
+    auto columns = [&](const Item& g, int c, int (&iv)[4]) {
+      const int* U = p.ulist + size_t(g.pi) * p.nao;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int pc = c * TK + 16 * hh + 4 * k + qd;
+        iv[k] = pc < g.nu ? __ldg(U + pc) : -1;
+      }
+    };
+    // The MMAs of every chunk up to `done` (stage sequence number) are known
+    // to have completed.  A parity wait names a phase only while the phase
+    // before it has completed, so stage_free steps through the completions
+    // in order: waiting for chunk y is safe once chunk y - STAGES is done.
+    long long done = -1;
+    auto stage_free = [&](uint32_t seq) -> bool {
+      const long long need = static_cast<long long>(seq) - STAGES;
+      while (done < need) {
+        const long long y = done + STAGES < need ? done + STAGES : need;
+        if (!tc::mbar_wait(&empty[y % STAGES], uint32_t((y / STAGES) & 1), err, 31, false, lim))
+          return false;
+        done = y;
+      }
+      return true;
+    };
+    // chunk c of item g into stage seq % STAGES (false: a wait ran out)
+    auto gather = [&](const Item& g, int c, uint32_t seq, const int (&iv)[4]) -> bool {
+      const uint2* dset = p.dsl + size_t(g.s) * p.nao * p.nao;
+      // symmetric D: only columns from the row's own position on (the
+      // diagonal digits carry D_uu / 2)
+      uint2 w[C::STEPS][4];
+#pragma unroll
+      for (int st = 0; st < C::STEPS; ++st) {
+        const int prow = g.ut * TN + C::WROWS * wq + 4 * st + ri;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int pc = c * TK + 16 * hh + 4 * k + qd;
+          w[st][k] = (g.iu[st] >= 0 && iv[k] >= 0 && (!sym || pc >= prow))
+                         ? __ldg(dset + size_t(g.iu[st]) * p.nao + iv[k])
+                         : make_uint2(0u, 0u);
+        }
+      }
+      if (!stage_free(seq)) return false;
+      const int stg = int(seq % STAGES);
+      uint8_t* Bs = smem + stg * C::STAGE + C::A_STAGE;
+#pragma unroll
+      for (int st = 0; st < C::STEPS; ++st) {
+        uint32_t wa[4], wb[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          // round 1 (lanes qd, qd^2): keep digits 0-3 (b1 = 0) or 4-7 (b1 = 1)
+          const uint32_t x = b1 ? w[st][k].y : w[st][k].x;
+          const uint32_t y = __shfl_xor_sync(0xffffffffu, b1 ? w[st][k].x : w[st][k].y, 16);
+          // round 2 (lanes qd, qd^1): keep two of those four digits
+          const uint32_t lo = __byte_perm(x, y, 0x5410), hi = __byte_perm(x, y, 0x7632);
+          const uint32_t keep = b0 ? hi : lo;
+          const uint32_t recv = __shfl_xor_sync(0xffffffffu, b0 ? lo : hi, 8);
+          wa[k] = __byte_perm(keep, recv, sel_a);
+          wb[k] = __byte_perm(keep, recv, sel_b);
+        }
+        const uint32_t off =
+            tc::sw32_offset(uint32_t(C::WROWS * wq + 4 * st + ri), uint32_t(hh));
+        if (2 * qd < NSL)
+          *reinterpret_cast<uint4*>(Bs + (2 * qd) * C::B_SLICE + off) =
+              make_uint4(wa[0], wa[1], wa[2], wa[3]);
+        if (2 * qd + 1 < NSL)
+          *reinterpret_cast<uint4*>(Bs + (2 * qd + 1) * C::B_SLICE + off) =
+              make_uint4(wb[0], wb[1], wb[2], wb[3]);
+      }
+      tc::fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&full_d[stg]);
+      return true;
+    };
+
+    uint32_t seq0 = 0;  // stage sequence number of the current item's first chunk
+    bool ok = true, ahead = false;
+    Item cur, nxt;
+    setup(item_of(0, true), cur);
+    for (uint32_t nitem = 0; ok && cur.t < total; ++nitem) {
+      // the group's chunks of the item (the first one already gathered when
+      // `ahead`), the union columns of the next one loaded a chunk ahead
+      int c = cur.kc0 + grp + (ahead ? NG : 0);
+      int ivn[4];
+      columns(cur, c, ivn);
+      for (; c < cur.kc; c += NG) {
+        int iv[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) iv[k] = ivn[k];
+        columns(cur, c + NG, ivn);
+        if (!gather(cur, c, seq0 + uint32_t(c - cur.kc0), iv)) {
+          ok = false;
+          break;
+        }
+      }
+      if (!ok) break;
+      const uint32_t seq1 = seq0 + uint32_t(cur.kc - cur.kc0);
+      // The next item's first chunk of this group is gathered before this
+      // item's epilogue, so the MMAs go on as soon as the accumulators are
+      // read.  Its stage was last used by chunk seq1 + grp - STAGES < seq1
+      // (NG <= STAGES): a chunk of this item or before, whose MMAs complete
+      // without this epilogue.
+      setup(item_of(nitem + 1, true), nxt);
+      ahead = false;
+      if (nxt.t < total && nxt.kc0 + grp < nxt.kc) {
+        int iv[4];
+        columns(nxt, nxt.kc0 + grp, iv);
+        if (!gather(nxt, nxt.kc0 + grp, seq1 + uint32_t(grp), iv)) break;
+        ahead = true;
+      }
+      // ---- epilogue: this warp's 32 points (TMEM lanes 32wq ..) over the
+      // group's column octets ----
+      const PairBatch& B = batch_of(p, cur.w);
+      const int4 pr = p.pairs[cur.pi];
       const int h = wq >> 1;
       const int tile = h ? pr.y : pr.x;
       int g0 = 0, gend = 0;
@@ -807,149 +930,82 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
       const int r = 32 * wq + lane;  // TMEM lane = point row
       const int gpt = g0 + (r & (HT - 1));
       const bool gval = tile >= 0 && gpt < gend;
-      const int col_l = (grp + NG * (lane >> 3)) * 8 + (lane & 7);  // this lane's column
-      const int kpos_l = ut * TN + col_l;
-      const bool cval_l = col_l < TN && kpos_l < nu;
-      const int u_l = cval_l ? __ldg(U + kpos_l) : 0;
-      const int f_l = cval_l ? int(p.uflag[size_t(pi) * p.nao + kpos_l]) : 0;
-      const int tu_l = cval_l ? p.tau[size_t(s) * p.nao + u_l] : 0;
-      const int sg = gval ? B.sigma[gpt] : 0;
-      const int wg0 = g0 + 32 * (wq & 1);  // this warp's first point
-      if (cval_l && ((f_l >> h) & 1) && tile >= 0 && wg0 < gend) {
-        const char* q0 = reinterpret_cast<const char*>(B.ao_lhs + size_t(u_l) * B.stride_grid + wg0);
-        const int last = min(gend - wg0, 32) - 1;
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(q0));
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(q0 + 8 * last));
-      }
-      // the union columns of the group's next chunk are loaded one chunk ahead,
-      // so the D gather addresses never wait for them
-      int ivn[4];
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const int pcn = (kc0 + grp) * TK + 16 * hh + 4 * k + qd;
-        ivn[k] = pcn < nu ? __ldg(U + pcn) : -1;
-      }
-      for (int c = kc0 + grp; c < kc; c += NG) {
-        const uint32_t seq = seq0 + uint32_t(c - kc0);
-        const int stg = int(seq % STAGES);
-        const uint32_t use = seq / STAGES;
-        int iv[4], pc[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          pc[k] = c * TK + 16 * hh + 4 * k + qd;
-          iv[k] = ivn[k];
-          const int pcn = pc[k] + NG * TK;
-          ivn[k] = pcn < nu ? __ldg(U + pcn) : -1;
-        }
-        // symmetric D: only columns from the row's own position on (the
-        // diagonal digits carry D_uu / 2)
-        uint2 w[C::STEPS][4];
-#pragma unroll
-        for (int st = 0; st < C::STEPS; ++st)
-#pragma unroll
-          for (int k = 0; k < 4; ++k)
-            w[st][k] = (iu[st] >= 0 && iv[k] >= 0 && (!sym || pc[k] >= prow[st]))
-                           ? __ldg(dset + size_t(iu[st]) * p.nao + iv[k])
-                           : make_uint2(0u, 0u);
-        if (use > 0 && !tc::mbar_wait(&empty[stg], (use - 1) & 1, err, 31, false, lim)) {
-          ok = false;
-          break;
-        }
-        uint8_t* Bs = smem + stg * C::STAGE + C::A_STAGE;
-#pragma unroll
-        for (int st = 0; st < C::STEPS; ++st) {
-          uint32_t wa[4], wb[4];
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            // round 1 (lanes qd, qd^2): keep digits 0-3 (b1 = 0) or 4-7 (b1 = 1)
-            const uint32_t x = b1 ? w[st][k].y : w[st][k].x;
-            const uint32_t y = __shfl_xor_sync(0xffffffffu, b1 ? w[st][k].x : w[st][k].y, 16);
-            // round 2 (lanes qd, qd^1): keep two of those four digits
-            const uint32_t lo = __byte_perm(x, y, 0x5410), hi = __byte_perm(x, y, 0x7632);
-            const uint32_t keep = b0 ? hi : lo;
-            const uint32_t recv = __shfl_xor_sync(0xffffffffu, b0 ? lo : hi, 8);
-            wa[k] = __byte_perm(keep, recv, sel_a);
-            wb[k] = __byte_perm(keep, recv, sel_b);
-          }
-          const uint32_t off =
-              tc::sw32_offset(uint32_t(C::WROWS * wq + 4 * st + ri), uint32_t(hh));
-          if (2 * qd < NSL)
-            *reinterpret_cast<uint4*>(Bs + (2 * qd) * C::B_SLICE + off) =
-                make_uint4(wa[0], wa[1], wa[2], wa[3]);
-          if (2 * qd + 1 < NSL)
-            *reinterpret_cast<uint4*>(Bs + (2 * qd + 1) * C::B_SLICE + off) =
-                make_uint4(wb[0], wb[1], wb[2], wb[3]);
-        }
-        tc::fence_proxy_async_smem();
-        __syncwarp();
-        if (lane == 0) tc::mbar_arrive(&full_d[stg]);
-      }
-      seq0 += uint32_t(kc - kc0);
-      if (!ok) break;
-      // ---- epilogue: this warp's 32 points (TMEM lanes 32wq ..) over the
-      // group's column octets ----
-      if (!tc::mbar_wait(acc_full, nitem & 1, err, 32, false, lim)) break;
-      tc::fence_after_sync();
-      const uint32_t trow = tmem + (uint32_t(32 * wq) << 16);
-      double acc = 0.0;
-      bool badrow = false;
       // the group's columns of this tile, in quartets (warp-uniform): octets
       // grp, grp+NG, ... below OCTETS whose first column lies inside U
       int nocts = 0;
-      while (grp + NG * nocts < C::OCTETS && ut * TN + (grp + NG * nocts) * 8 < nu) ++nocts;
+      while (grp + NG * nocts < C::OCTETS && cur.ut * TN + (grp + NG * nocts) * 8 < cur.nu) ++nocts;
       const int nq = 2 * nocts;
-      // phi_lhs of a quartet's 4 columns at this lane's point, for AOs active in
-      // its block (0 and inactive elsewhere); the next quartet's are requested
-      // before this one is combined
-      auto fetch = [&](int qi, double (&a)[4], uint32_t& on) {
-        const int col0 = (grp + NG * (qi >> 1)) * 8 + 4 * (qi & 1);
-        on = 0;
+      // lane l holds column l of the group's columns: its AO, membership
+      // flags and row scale
+      const int col_l = (grp + NG * (lane >> 3)) * 8 + (lane & 7);
+      const int kpos_l = cur.ut * TN + col_l;
+      const bool cval_l = col_l < TN && kpos_l < cur.nu;
+      const int u_l = cval_l ? __ldg(p.ulist + size_t(cur.pi) * p.nao + kpos_l) : 0;
+      const int f_l = cval_l ? int(p.uflag[size_t(cur.pi) * p.nao + kpos_l]) : 0;
+      const int tu_l = cval_l ? p.tau[size_t(cur.s) * p.nao + u_l] : 0;
+      const int sg = gval ? B.sigma[gpt] : 0;
+      // phi_lhs of every group column at this lane's point, for AOs active in
+      // its block (zero-filled elsewhere), copied to shared memory while the
+      // item's last MMAs run; bit 4qi+j of `on` marks column j of quartet qi
+      uint32_t on = 0;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int src = qi * 4 + j;  // lane holding the column (octet qi/2, column 4(qi&1)+j)
-          const int uj = __shfl_sync(0xffffffffu, u_l, src);
-          const int fj = __shfl_sync(0xffffffffu, f_l, src);
-          const bool o = gval && ut * TN + col0 + j < nu && ((fj >> h) & 1);
-          on |= uint32_t(o) << j;
-          a[j] = o ? B.ao_lhs[size_t(uj) * B.stride_grid + gpt] : 0.0;
+      for (int qi = 0; qi < C::MAXQ; ++qi) {
+        if (qi < nq) {
+          const int col0 = (grp + NG * (qi >> 1)) * 8 + 4 * (qi & 1);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int src = qi * 4 + j;  // lane holding the column
+            const int uj = __shfl_sync(0xffffffffu, u_l, src);
+            const int fj = __shfl_sync(0xffffffffu, f_l, src);
+            const bool o = gval && cur.ut * TN + col0 + j < cur.nu && ((fj >> h) & 1);
+            on |= uint32_t(o) << src;
+            cp_async_8(phl + src * 32 + lane, B.ao_lhs + (o ? size_t(uj) * B.stride_grid + gpt : 0),
+                       o);
+          }
         }
-      };
-      double a[4], an[4];
-      uint32_t on = 0, onn = 0;
-      if (nq > 0) fetch(0, a, on);
-#pragma unroll 1
-      for (int qi = 0; qi < nq; ++qi) {
-        const int col0 = (grp + NG * (qi >> 1)) * 8 + 4 * (qi & 1);
-        uint32_t v[NSL][4];
+      }
+      cp_async_commit();
+      const bool acc_ok = tc::mbar_wait(acc_full, nitem & 1, err, 32, false, lim);
+      cp_async_wait<0>();
+      if (!acc_ok) break;
+      tc::fence_after_sync();
+      if (done < static_cast<long long>(seq1) - 1) done = static_cast<long long>(seq1) - 1;
+      const uint32_t trow = tmem + (uint32_t(32 * wq) << 16);
+      double acc = 0.0;
+      bool badrow = false;
 #pragma unroll
-        for (int L = 0; L < NSL; ++L)
-          tc::tmem_ld_32x32b_x4(trow + uint32_t(L * TN + col0), v[L]);
-        if (qi + 1 < nq) fetch(qi + 1, an, onn);
-        tc::tmem_ld_wait();
-        if (qi + 1 == nq) {  // the accumulators are read: the MMA warp may go on
-          tc::fence_before_sync();
-          __syncwarp();
-          if (lane == 0) tc::mbar_arrive(acc_empty);
-        }
+      for (int qi = 0; qi < C::MAXQ; ++qi) {
+        if (qi < nq) {
+          const int col0 = (grp + NG * (qi >> 1)) * 8 + 4 * (qi & 1);
+          uint32_t v[NSL][4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int tuj = __shfl_sync(0xffffffffu, tu_l, qi * 4 + j);
-          uint32_t lv[NSL];
+          for (int L = 0; L < NSL; ++L)
+            tc::tmem_ld_32x32b_x4(trow + uint32_t(L * TN + col0), v[L]);
+          tc::tmem_ld_wait();
+          if (qi + 1 == nq) {  // the accumulators are read: the MMA warp may go on
+            tc::fence_before_sync();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(acc_empty);
+          }
 #pragma unroll
-          for (int L = 0; L < NSL; ++L) lv[L] = v[L][j];
-          if ((on >> j) & 1) {  // AOs inactive in this point's block take no part
-            if (tuj == kBadExp) {
-              badrow = true;
-            } else {
-              const double x = combine_levels<NSL>(lv);
-              const int e = -tuj;
-              acc = fma(a[j], (e >= -1022 && e <= 1023) ? x * pow2(e) : ldexp(x, e), acc);
+          for (int j = 0; j < 4; ++j) {
+            const int src = qi * 4 + j;
+            const int tuj = __shfl_sync(0xffffffffu, tu_l, src);
+            if ((on >> src) & 1) {  // AOs inactive in this point's block take no part
+              if (tuj == kBadExp) {
+                badrow = true;
+              } else {
+                uint32_t lv[NSL];
+#pragma unroll
+                for (int L = 0; L < NSL; ++L) lv[L] = v[L][j];
+                const double x = combine_levels<NSL>(lv);
+                const int e = -tuj;
+                acc = fma(phl[src * 32 + lane],
+                          (e >= -1022 && e <= 1023) ? x * pow2(e) : ldexp(x, e), acc);
+              }
             }
           }
         }
-#pragma unroll
-        for (int j = 0; j < 4; ++j) a[j] = an[j];
-        on = onn;
       }
       if (nq == 0) {
         tc::fence_before_sync();
@@ -973,9 +1029,11 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
         double sum = e2[r];
 #pragma unroll
         for (int w = 1; w < NG; ++w) sum += e2[w * PT + r];
-        const size_t pbase = p.poff ? size_t(p.poff[pi]) : size_t(pi) * p.max_t;
-        p.partial[((pbase + ut) * p.nset_max + s) * PT + r] = sum;
+        const size_t pbase = p.poff ? size_t(p.poff[cur.pi]) : size_t(cur.pi) * p.max_t;
+        p.partial[((pbase + cur.ut) * p.nset_max + cur.s) * PT + r] = sum;
       }
+      seq0 = seq1;
+      cur = nxt;
     }
   } else if (warp == GW) {
     // ---------------- MMA issuer ----------------
@@ -1121,8 +1179,8 @@ pair_reduce(PairArgs p, const int* __restrict__ npairs, int pair0) {
 
 template <int NSL, int STAGES>
 cudaError_t launch_pair_main_t(int nsm, const PairArgs& a, cudaStream_t stream, bool attrs_only) {
-  constexpr size_t smem =
-      size_t(STAGES) * Cfg<NSL>::STAGE + 1024 + 256 + 2 * NG * PT * 8 + kRing * (16 + 4);
+  constexpr size_t smem = Cfg<NSL>::template smem_bytes<STAGES>();
+  static_assert(smem <= 232448, "shared memory per CTA");
   cudaError_t err = cudaFuncSetAttribute(pair_main<NSL, STAGES>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (err != cudaSuccess || attrs_only) return err;
@@ -1191,27 +1249,18 @@ size_t aodmao2rho_split_pair_workspace(size_t nao, size_t ngrid, size_t nset, si
   return layout(nao, ngrid, nset, blk, nsl).bytes;
 }
 
-int split_pair_stages() {  // CFGMM_SPLIT_STAGES (3..5) or the default, read per call
-  const char* e = std::getenv("CFGMM_SPLIT_STAGES");
-  const int v = e ? std::atoi(e) : kStages;
-  return v >= NG && v <= 5 ? v : kStages;
+int split_pair_stages() {  // fixed: with the epilogue's phi_lhs values three stages fit
+  return kStages;
 }
 
 cudaError_t split_pair_launch_main(const PairArgs& a, int nsl, cudaStream_t stream,
-                                   bool attrs_only, int stages) {
+                                   bool attrs_only, int /*stages*/) {
   int dev = 0, nsm = 0;
   cudaError_t err = cudaGetDevice(&dev);
   if (err == cudaSuccess) err = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (err != cudaSuccess) return err;
-  if (stages < NG || stages > 5) stages = split_pair_stages();
-  if (nsl == 6) {
-    if (stages == 3) return launch_pair_main_t<6, 3>(nsm, a, stream, attrs_only);
-    if (stages == 5) return launch_pair_main_t<6, 5>(nsm, a, stream, attrs_only);
-    return launch_pair_main_t<6, 4>(nsm, a, stream, attrs_only);
-  }
-  if (stages == 3) return launch_pair_main_t<7, 3>(nsm, a, stream, attrs_only);
-  if (stages == 5) return launch_pair_main_t<7, 5>(nsm, a, stream, attrs_only);
-  return launch_pair_main_t<7, 4>(nsm, a, stream, attrs_only);
+  if (nsl == 6) return launch_pair_main_t<6, kStages>(nsm, a, stream, attrs_only);
+  return launch_pair_main_t<7, kStages>(nsm, a, stream, attrs_only);
 }
 
 cudaError_t split_pair_launch_reduce(const PairArgs& a, int nsl, const int* npairs, int pair0,

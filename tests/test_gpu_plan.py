@@ -145,7 +145,9 @@ def test_split_plan_equals_single_split_calls(cm, wl, tmp_path, monkeypatch, gra
     info = plan.info()
     assert info["precision"] == "split" and info["graph"] is graph
     if tune:
-        assert [t["stages"] for t in info["tuning"]] == [3, 4, 5]
+        stages = [t["stages"] for t in info["tuning"]]
+        assert stages in ([3, 4, 5], [3])  # row form: three depths; pair form: fixed
+        assert min(t["ms"] for t in info["tuning"]) > 0
     plan.run()
     torch.cuda.synchronize()
     for b, d in zip(bs, dev):
