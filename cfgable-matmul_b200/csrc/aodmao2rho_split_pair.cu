@@ -834,12 +834,11 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
       }
       return true;
     };
-    // chunk c of item g into stage seq % STAGES (false: a wait ran out)
-    auto gather = [&](const Item& g, int c, uint32_t seq, const int (&iv)[4]) -> bool {
+    // D digits of chunk c of item g at this lane's positions (no waits)
+    auto load_chunk = [&](const Item& g, int c, const int (&iv)[4], uint2 (&w)[C::STEPS][4]) {
       const uint2* dset = p.dsl + size_t(g.s) * p.nao * p.nao;
       // symmetric D: only columns from the row's own position on (the
       // diagonal digits carry D_uu / 2)
-      uint2 w[C::STEPS][4];
 #pragma unroll
       for (int st = 0; st < C::STEPS; ++st) {
         const int prow = g.ut * TN + C::WROWS * wq + 4 * st + ri;
@@ -851,6 +850,9 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
                          : make_uint2(0u, 0u);
         }
       }
+    };
+    // the loaded digits into stage seq % STAGES as digit planes (false: a wait ran out)
+    auto store_chunk = [&](uint32_t seq, const uint2 (&w)[C::STEPS][4]) -> bool {
       if (!stage_free(seq)) return false;
       const int stg = int(seq % STAGES);
       uint8_t* Bs = smem + stg * C::STAGE + C::A_STAGE;
@@ -884,13 +886,65 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
       return true;
     };
 
+    const int h = wq >> 1;           // the warp's block tile: lo (0) or hi (1)
+    const int r = 32 * wq + lane;    // TMEM lane = point row
+    const uint32_t trow = tmem + (uint32_t(32 * wq) << 16);
     uint32_t seq0 = 0;  // stage sequence number of the current item's first chunk
     bool ok = true, ahead = false;
     Item cur, nxt;
     setup(item_of(0, true), cur);
     for (uint32_t nitem = 0; ok && cur.t < total; ++nitem) {
-      // the group's chunks of the item (the first one already gathered when
-      // `ahead`), the union columns of the next one loaded a chunk ahead
+      // ---- what the epilogue needs, requested first: lane l holds column l
+      // of the group's columns (octets grp, grp+NG, ...): its AO, membership
+      // flags and row scale; phi_lhs of every group column at this lane's
+      // point, for AOs active in its block (zero-filled elsewhere), is copied
+      // to shared memory while the item's chunks run; bit 4qi+j of `on`
+      // marks column j of quartet qi ----
+      const PairBatch& B = batch_of(p, cur.w);
+      int gpt, sg, tu_l, nq;
+      bool gval;
+      uint32_t on = 0;
+      {
+        const int4 pr = p.pairs[cur.pi];
+        const int tile = h ? pr.y : pr.x;
+        int g0 = 0, gend = 0;
+        if (tile >= 0) tile_points(tile, p.blk, p.gsub, B.ngrid, &g0, &gend);
+        gpt = g0 + (r & (HT - 1));
+        gval = tile >= 0 && gpt < gend;
+        // the group's columns of this tile, in quartets (warp-uniform):
+        // octets grp, grp+NG, ... below OCTETS whose first column lies inside U
+        int nocts = 0;
+        while (grp + NG * nocts < C::OCTETS && cur.ut * TN + (grp + NG * nocts) * 8 < cur.nu)
+          ++nocts;
+        nq = 2 * nocts;
+        const int col_l = (grp + NG * (lane >> 3)) * 8 + (lane & 7);
+        const int kpos_l = cur.ut * TN + col_l;
+        const bool cval_l = col_l < TN && kpos_l < cur.nu;
+        const int u_l = cval_l ? __ldg(p.ulist + size_t(cur.pi) * p.nao + kpos_l) : 0;
+        const int f_l = cval_l ? int(p.uflag[size_t(cur.pi) * p.nao + kpos_l]) : 0;
+        tu_l = cval_l ? p.tau[size_t(cur.s) * p.nao + u_l] : 0;
+        sg = gval ? B.sigma[gpt] : 0;
+#pragma unroll
+        for (int qi = 0; qi < C::MAXQ; ++qi) {
+          if (qi < nq) {
+            const int col0 = (grp + NG * (qi >> 1)) * 8 + 4 * (qi & 1);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              const int src = qi * 4 + j;  // lane holding the column
+              const int uj = __shfl_sync(0xffffffffu, u_l, src);
+              const int fj = __shfl_sync(0xffffffffu, f_l, src);
+              const bool o = gval && cur.ut * TN + col0 + j < cur.nu && ((fj >> h) & 1);
+              on |= uint32_t(o) << src;
+              cp_async_8(phl + src * 32 + lane,
+                         B.ao_lhs + (o ? size_t(uj) * B.stride_grid + gpt : 0), o);
+            }
+          }
+        }
+        cp_async_commit();
+      }
+      // ---- the group's chunks of the item (the first one already in its
+      // stage when `ahead`), the union columns of the next one loaded a
+      // chunk ahead ----
       int c = cur.kc0 + grp + (ahead ? NG : 0);
       int ivn[4];
       columns(cur, c, ivn);
@@ -899,78 +953,35 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
 #pragma unroll
         for (int k = 0; k < 4; ++k) iv[k] = ivn[k];
         columns(cur, c + NG, ivn);
-        if (!gather(cur, c, seq0 + uint32_t(c - cur.kc0), iv)) {
+        uint2 w[C::STEPS][4];
+        load_chunk(cur, c, iv, w);
+        if (!store_chunk(seq0 + uint32_t(c - cur.kc0), w)) {
           ok = false;
           break;
         }
       }
       if (!ok) break;
       const uint32_t seq1 = seq0 + uint32_t(cur.kc - cur.kc0);
-      // The next item's first chunk of this group is gathered before this
-      // item's epilogue, so the MMAs go on as soon as the accumulators are
-      // read.  Its stage was last used by chunk seq1 + grp - STAGES < seq1
-      // (NG <= STAGES): a chunk of this item or before, whose MMAs complete
-      // without this epilogue.
+      // ---- the next item's first chunk of this group: loaded now, stored
+      // as soon as the accumulators are read, so the MMAs go on at once.
+      // Its stage was last used by chunk seq1 + grp - STAGES < seq1
+      // (NG <= STAGES): a chunk of this item or before, done once the
+      // accumulators are full ----
       setup(item_of(nitem + 1, true), nxt);
-      ahead = false;
-      if (nxt.t < total && nxt.kc0 + grp < nxt.kc) {
+      ahead = nxt.t < total && nxt.kc0 + grp < nxt.kc;
+      uint2 wn[C::STEPS][4];
+      if (ahead) {
         int iv[4];
         columns(nxt, nxt.kc0 + grp, iv);
-        if (!gather(nxt, nxt.kc0 + grp, seq1 + uint32_t(grp), iv)) break;
-        ahead = true;
+        load_chunk(nxt, nxt.kc0 + grp, iv, wn);
       }
       // ---- epilogue: this warp's 32 points (TMEM lanes 32wq ..) over the
       // group's column octets ----
-      const PairBatch& B = batch_of(p, cur.w);
-      const int4 pr = p.pairs[cur.pi];
-      const int h = wq >> 1;
-      const int tile = h ? pr.y : pr.x;
-      int g0 = 0, gend = 0;
-      if (tile >= 0) tile_points(tile, p.blk, p.gsub, B.ngrid, &g0, &gend);
-      const int r = 32 * wq + lane;  // TMEM lane = point row
-      const int gpt = g0 + (r & (HT - 1));
-      const bool gval = tile >= 0 && gpt < gend;
-      // the group's columns of this tile, in quartets (warp-uniform): octets
-      // grp, grp+NG, ... below OCTETS whose first column lies inside U
-      int nocts = 0;
-      while (grp + NG * nocts < C::OCTETS && cur.ut * TN + (grp + NG * nocts) * 8 < cur.nu) ++nocts;
-      const int nq = 2 * nocts;
-      // lane l holds column l of the group's columns: its AO, membership
-      // flags and row scale
-      const int col_l = (grp + NG * (lane >> 3)) * 8 + (lane & 7);
-      const int kpos_l = cur.ut * TN + col_l;
-      const bool cval_l = col_l < TN && kpos_l < cur.nu;
-      const int u_l = cval_l ? __ldg(p.ulist + size_t(cur.pi) * p.nao + kpos_l) : 0;
-      const int f_l = cval_l ? int(p.uflag[size_t(cur.pi) * p.nao + kpos_l]) : 0;
-      const int tu_l = cval_l ? p.tau[size_t(cur.s) * p.nao + u_l] : 0;
-      const int sg = gval ? B.sigma[gpt] : 0;
-      // phi_lhs of every group column at this lane's point, for AOs active in
-      // its block (zero-filled elsewhere), copied to shared memory while the
-      // item's last MMAs run; bit 4qi+j of `on` marks column j of quartet qi
-      uint32_t on = 0;
-#pragma unroll
-      for (int qi = 0; qi < C::MAXQ; ++qi) {
-        if (qi < nq) {
-          const int col0 = (grp + NG * (qi >> 1)) * 8 + 4 * (qi & 1);
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const int src = qi * 4 + j;  // lane holding the column
-            const int uj = __shfl_sync(0xffffffffu, u_l, src);
-            const int fj = __shfl_sync(0xffffffffu, f_l, src);
-            const bool o = gval && cur.ut * TN + col0 + j < cur.nu && ((fj >> h) & 1);
-            on |= uint32_t(o) << src;
-            cp_async_8(phl + src * 32 + lane, B.ao_lhs + (o ? size_t(uj) * B.stride_grid + gpt : 0),
-                       o);
-          }
-        }
-      }
-      cp_async_commit();
       const bool acc_ok = tc::mbar_wait(acc_full, nitem & 1, err, 32, false, lim);
       cp_async_wait<0>();
       if (!acc_ok) break;
       tc::fence_after_sync();
       if (done < static_cast<long long>(seq1) - 1) done = static_cast<long long>(seq1) - 1;
-      const uint32_t trow = tmem + (uint32_t(32 * wq) << 16);
       double acc = 0.0;
       bool badrow = false;
 #pragma unroll
@@ -1012,6 +1023,7 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
         __syncwarp();
         if (lane == 0) tc::mbar_arrive(acc_empty);
       }
+      if (ahead && !store_chunk(seq1 + uint32_t(grp), wn)) break;
       double res = 0.0;
       if (gval) {
         const int e = -sg;

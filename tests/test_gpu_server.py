@@ -79,32 +79,36 @@ def test_server_alone_and_in_the_mix(cm, wl, tmp_path, monkeypatch, precision, t
 
 @pytest.mark.parametrize("precision,tol", [(0, 1e-13), (1, 1e-12)])
 def test_server_requests_overlap_on_the_device(cm, wl, tmp_path, monkeypatch, precision, tol):
-    """Four molecules of 1000-1600 AOs on 16384 points (device-evaluated phi,
-    density 0.3), two requests each submitted at once: requests of different
-    molecules are on the device together -- the server's max_inflight stat
-    reaches 2 or more, and the requests' device spans (events on their slot
-    streams) add up to more than the wall-clock span of the whole batch --
-    and every result matches the single call."""
+    """Four molecules of 300-450 AOs on 262144 points each (device-evaluated
+    phi, density 0.4): a request's device work (milliseconds) outlasts its
+    submission (a copy of its 2 D matrices), so with two requests per
+    molecule submitted at once, requests of different molecules are on the
+    device together -- the server's max_inflight stat reaches 2 or more, and
+    the requests' device spans (events on their slot streams) add up to more
+    than the wall-clock span of the whole batch -- and every result matches
+    the single call."""
     import time
     import torch
     monkeypatch.setenv("CFGMM_AUTOTUNE_CACHE", str(tmp_path / "tune.txt"))
+    ngrid = 262144
     mols = []
-    for i, nao in enumerate((1000, 1200, 1400, 1600)):
-        mol = wl.molecule(50 + i, nao=nao, nshell=2 * int(nao / 11.14), natom=nao // 20)
-        pts = wl.grid_points(np.random.default_rng(60 + i), mol, 16384, 64)
-        ao, tab = wl.device_grid(cm, wl.DeviceMolecule(mol), pts, 64, 0.3)
+    for i, nao in enumerate((300, 350, 400, 450)):
+        mol = wl.molecule(50 + i, nao=nao, nshell=2 * int(nao / 11.14), natom=nao // 20,
+                          box_angstrom=8.0)
+        pts = wl.grid_points(np.random.default_rng(60 + i), mol, ngrid, 64)
+        ao, tab = wl.device_grid(cm, wl.DeviceMolecule(mol), pts, 64, 0.4)
         dms = [wl.sym_dms(np.random.default_rng(70 + 3 * i + k), 2, nao) for k in range(3)]
         mols.append(dict(ao=ao, tab=tab, dms=dms))
     srv = cm.Server(24 << 30, nslots=4, precision=precision)
     try:
         ids = [srv.open(m["ao"], m["tab"], 2) for m in mols]
         for i, m in zip(ids, mols):  # resident, plans built and tuned
-            srv.wait(srv.submit(i, m["dms"][0], np.zeros((2, 16384))), WAIT)
+            srv.wait(srv.submit(i, m["dms"][0], np.zeros((2, ngrid))), WAIT)
         outs, tickets = [], []
         t0 = time.perf_counter()
         for step in (1, 2):
             for i, m in zip(ids, mols):
-                o = np.zeros((2, 16384))
+                o = np.zeros((2, ngrid))
                 outs.append((m, step, o))
                 tickets.append(srv.submit(i, m["dms"][step], o))
         device_ms = sum(srv.wait(t, WAIT)[1] for t in tickets)
@@ -117,8 +121,8 @@ def test_server_requests_overlap_on_the_device(cm, wl, tmp_path, monkeypatch, pr
     assert st["failed"] == 0 and st["max_inflight"] >= 2, st
     assert device_ms > wall_ms, (device_ms, wall_ms)
     for m, step, o in outs:
-        ref = torch.zeros(2, 16384, dtype=torch.float64, device="cuda")
-        nao, ngrid = m["ao"].shape
+        ref = torch.zeros(2, ngrid, dtype=torch.float64, device="cuda")
+        nao = m["ao"].shape[0]
         cm.aodmao2rho_ex(ref, torch.from_numpy(m["dms"][step]).cuda(), m["ao"], m["ao"],
                          (nao, ngrid), (nao, ngrid), 2, m["tab"], m["tab"].shape[1], 64, 0)
         assert normwise(o, ref.cpu().numpy()) < tol

@@ -94,18 +94,17 @@ class Model:
                 yield from gather(seq0 + c - kc0)
                 c += NG
             seq1 = seq0 + kc - kc0
+            # the next item's first chunk of the group: loaded before the
+            # accumulator wait, stored once the accumulators are read
             tn = yield from self.item_of(nitem + 1)
-            ahead = False
-            if tn is not None:
-                k0, k1 = self.items[tn]
-                if k0 + grp < k1:
-                    yield from gather(seq1 + grp)
-                    ahead = True
+            ahead = tn is not None and self.items[tn][0] + grp < self.items[tn][1]
             yield lambda n=nitem: self.acc_full.passed(n & 1)
             state["done"] = max(state["done"], seq1 - 1)
             assert self.tmem_item == nitem and self.executed >= seq1 - 1
             self.tmem_read.setdefault(nitem, set()).add(w)
             self.acc_empty.arrive()
+            if ahead:
+                yield from gather(seq1 + grp)
             buf = nitem & 1
             self.epi[buf][grp] = nitem
             self.epi_full[buf].arrive()
