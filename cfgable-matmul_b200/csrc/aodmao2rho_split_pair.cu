@@ -83,6 +83,7 @@ constexpr int kWin = 32;          // pairing candidates on each side in key orde
 constexpr int kSortMax = 4096;    // tiles sorted in shared memory (more: caller's order)
 constexpr int kRounds = 8;        // mutual-best matching rounds
 constexpr int kRing = 4;          // work items in flight between the kernel's roles
+constexpr int kAhead = 2;         // items drawn ahead of the one being loaded (< kRing)
 static_assert(kStages >= NG, "a group's parity wait needs at least NG stages");
 
 template <int NSL>
@@ -1110,9 +1111,15 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
 #pragma unroll
       for (int s = 0; s < STAGES; ++s) issued[s] = 0;
       bool ok = true;
-      for (uint32_t n = 0;; ++n) {
-        // draw the next item into the ring slot, once every warp has read the
-        // slot's previous item
+      // Items are drawn kAhead ahead of the one whose tiles are loaded, so a
+      // gather group finds the next item in the ring when it reaches it.  A
+      // draw waits until every warp has read the slot's previous item; after
+      // a failed wait the terminal item goes in, so every role stops.
+      int tq[kRing];  // the drawn items by ring slot
+      uint32_t ndrawn = 0;
+      bool ended = false;
+      auto draw = [&]() {
+        const uint32_t n = ndrawn++;
         const int slot = int(n % kRing);
         int t = total;
         if (ok && (n < kRing || tc::mbar_wait(&iempty[slot], ((n / kRing) - 1) & 1, err, 41,
@@ -1121,9 +1128,15 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
           if (t > total) t = total;
         }
         ring[slot] = t;
-        tc::mbar_arrive(&ifull[slot]);  // release: the slot's value is visible to the waiters
+        tq[slot] = t;
+        tc::mbar_arrive(&ifull[slot]);   // release: the slot's value is visible to the waiters
         tc::mbar_arrive(&iempty[slot]);  // this warp's own read
-        if (t >= total || !ok) break;
+        ended = t >= total;
+      };
+      for (uint32_t n = 0;; ++n) {
+        while (!ended && ndrawn <= n + kAhead) draw();
+        const int t = tq[n % kRing];
+        if (t >= total) break;
         const int4 it = p.items[t];
         const int nu = p.ucount[it.x];
         const int kc = (nu + TK - 1) / TK;
@@ -1144,6 +1157,10 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
                         &full_phi[stg]);
 #pragma unroll
           for (int s = 0; s < STAGES; ++s) issued[s] += s == stg;
+        }
+        if (!ok) {
+          while (!ended) draw();
+          break;
         }
       }
       // copies still in flight complete before the CTA exits

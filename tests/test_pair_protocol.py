@@ -22,6 +22,7 @@ import pytest
 NG, GW = 3, 12
 STAGES = 3
 RING = 4
+AHEAD = 2
 
 
 class Bar:
@@ -142,16 +143,22 @@ class Model:
         yield lambda: self.drain.passed(0)
 
     def loader_thread(self):
-        seq, n = 0, 0
+        seq, drawn, ended = 0, 0, False
+        tq = [None] * RING
         issued = [0] * STAGES
+        n = 0
         while True:
-            slot = n % RING
-            if n >= RING:
-                yield lambda s=slot, n=n: self.iempty[s].passed(((n // RING) - 1) & 1)
-            t = n if n < len(self.items) else None
-            self.ring[slot] = t
-            self.ifull[slot].arrive()
-            self.iempty[slot].arrive()
+            while not ended and drawn <= n + AHEAD:  # items drawn AHEAD ahead
+                slot = drawn % RING
+                if drawn >= RING:
+                    yield lambda s=slot, d=drawn: self.iempty[s].passed(((d // RING) - 1) & 1)
+                t = drawn if drawn < len(self.items) else None
+                self.ring[slot] = tq[slot] = t
+                self.ifull[slot].arrive()
+                self.iempty[slot].arrive()
+                ended = t is None
+                drawn += 1
+            t = tq[n % RING]
             if t is None:
                 break
             kc0, kc = self.items[t]
