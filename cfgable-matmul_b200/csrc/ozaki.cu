@@ -570,30 +570,14 @@ cudaError_t prepare(const double* x, size_t ld, bool rows_contig, int rows, int 
   return cudaGetLastError();
 }
 
-constexpr int kMaxPanels = 4;
-static_assert(2 * kMaxPanels + 1 <= kSideEvents, "events of the panel pipeline");
-
-// Column panels of op(B) for the pipeline of ozaki_dgemm: whole 256-column
-// GEMM tiles, at least 8 tiles per panel, at most kMaxPanels; one panel for
-// the masked GEMM (its mask is indexed by absolute column).  Depends on n
-// alone, so residues kept for reuse have the layout the next call expects.
-int ozaki_panels(int n, bool masked, int* pan) {
-  const int nt = (n + 255) / 256;
-  const int np = masked ? 1 : std::min(kMaxPanels, std::max(1, nt / 8));
-  for (int j = 0; j < np; ++j) pan[j] = std::min(n, int((long long)nt * j / np) * 256);
-  pan[np] = n;
-  return np;
-}
-
 }  // namespace
 
-const SideStream* side_stream(int which) {
+const SideStream* side_stream() {
   constexpr int kMaxDevices = 64;
-  thread_local SideStream streams[kMaxDevices][2];
+  thread_local SideStream streams[kMaxDevices];
   int dev = 0;
-  if (which < 0 || which > 1) return nullptr;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
-  SideStream& st = streams[dev][which];
+  SideStream& st = streams[dev];
   if (!st.join) {
     // made in place; a partial set (one creation failed) is kept, released at
     // thread exit, and completed by a later call
@@ -613,37 +597,6 @@ const SideStream* side_stream(int which) {
   return &st;
 }
 
-namespace {
-struct EventPool {
-  cudaEvent_t ev[kSideEvents] = {};
-  bool ready = false;
-  EventPool() = default;
-  EventPool(const EventPool&) = delete;
-  EventPool& operator=(const EventPool&) = delete;
-  ~EventPool() {  // at thread exit; stale handles after a reset only return errors
-    for (cudaEvent_t e : ev)
-      if (e) cudaEventDestroy(e);
-    cudaGetLastError();
-  }
-};
-}  // namespace
-
-cudaEvent_t* side_events() {
-  constexpr int kMaxDevices = 64;
-  thread_local EventPool pools[kMaxDevices];
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
-  EventPool& p = pools[dev];
-  if (!p.ready) {
-    for (cudaEvent_t& e : p.ev)
-      if (!e && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
-        e = nullptr;
-        return nullptr;
-      }
-    p.ready = true;
-  }
-  return p.ev;
-}
 
 int ozaki_default_moduli(int k) {
   const char* env = std::getenv("CFGMM_OZAKI_MODULI");
@@ -686,18 +639,43 @@ cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int 
   int* emax_a = reinterpret_cast<int*>(ws + L.emax_a);
   int* emax_b = reinterpret_cast<int*>(ws + L.emax_b);
   cudaError_t err = cudaSuccess;
+  // With both operands to prepare, A's kernels run on a side stream beside B's:
+  // the residue kernels are bound by instruction issue and the exponent scans
+  // by DRAM, so the two chains overlap.  The side stream joins back before the
+  // GEMM (the fork and join are events, so a stream capture follows them).
+  SideScope side((!reuse_a && !reuse_b) ? side_stream() : nullptr, stream);
+  if ((err = side.fork()) != cudaSuccess) return err;
+  const cudaStream_t sa = side.stream();
+  if (!reuse_a) {
+    err = prepare(a, lda, !transa, m, k, L.kpad, plan.alpha, emax_a, ea, a_res, ra, sa);
+    if (err != cudaSuccess) return err;
+  }
+  if (!reuse_b) {
+    err = prepare(b, ldb, transb, n, k, L.kpad, plan.beta, emax_b, eb, b_res, ra, stream,
+                  Mask{tab, ldtab, blk > 0 ? blk : 1});
+    if (err != cudaSuccess) return err;
+  }
+  if ((err = side.join()) != cudaSuccess) return err;
+
+  mark(1);
   CUtensorMap tmA, tmB;
-  if (!make_plane_map(&tmA, a_res, k, m, plan.nmod, L.kpad, gemm_i8_tile_rows_a()))
+  if (!make_plane_map(&tmA, a_res, k, m, plan.nmod, L.kpad, gemm_i8_tile_rows_a()) ||
+      !make_plane_map(&tmB, b_res, k, n, plan.nmod, L.kpad, gemm_i8_tile_rows_b()))
     return cudaErrorInvalidValue;
   GemmI8Args g{};
   g.rows_a = m;
+  g.rows_b = n;
   g.k = k;
   g.nmod = plan.nmod;
+  g.out = r;
   g.ldr = L.ldr;
   for (int l = 0; l < plan.nmod; ++l) {
     g.mod[l] = plan.mod[l];
     g.inv[l] = plan.inv_f[l];
   }
+  if ((err = gemm_i8_mod(tmA, tmB, g, stream)) != cudaSuccess) return err;
+  mark(2);
+
   ReconArgs rc{};
   rc.nmod = plan.nmod;
   for (int l = 0; l < plan.nmod; ++l) {
@@ -708,95 +686,12 @@ cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int 
   rc.M_hi = plan.M_hi;
   rc.M_lo = plan.M_lo;
   rc.two_T = plan.two_T;
-  int pan[kMaxPanels + 1];
-  // op(B)'s columns [pan[j], pan[j+1]): the panel's residues (a block
-  // [nmod][n_j][kpad] of the panel-major b_res), GEMM and reconstruction
-  auto b_panel = [&](int j) { return b_res + size_t(plan.nmod) * pan[j] * L.kpad; };
-  auto prepare_b = [&](int j, cudaStream_t s) {
-    const int n0 = pan[j], nj = pan[j + 1] - pan[j];
-    return prepare(transb ? b + size_t(n0) * ldb : b + n0, ldb, transb, nj, k, L.kpad, plan.beta,
-                   emax_b + n0, eb + n0, b_panel(j), ra, s,
-                   Mask{tab, ldtab, blk > 0 ? blk : 1});
-  };
-  auto gemm = [&](int j) -> cudaError_t {
-    const int n0 = pan[j], nj = pan[j + 1] - pan[j];
-    if (!make_plane_map(&tmB, b_panel(j), k, nj, plan.nmod, L.kpad, gemm_i8_tile_rows_b()))
-      return cudaErrorInvalidValue;
-    g.rows_b = nj;
-    g.out = r + n0;
-    return gemm_i8_mod(tmA, tmB, g, stream);
-  };
-  auto recon = [&](int j, cudaStream_t s) -> cudaError_t {
-    const int n0 = pan[j], nj = pan[j + 1] - pan[j];
-    const long long rgrid = (long long)((nj + 1023) / 1024) * m;
-    if (rgrid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-    reconstruct<<<unsigned(rgrid), 256, 0, s>>>(c + n0, ldc, m, nj, r + n0, L.ldr, ea, eb + n0,
-                                                rc);
-    return cudaGetLastError();
-  };
-
-  const int np = ozaki_panels(n, tab != nullptr, pan);
-  cudaEvent_t* ev = np > 1 ? side_events() : nullptr;
-  if (!ev) {
-    // One panel.  With both operands to prepare, A's kernels run on a side
-    // stream beside B's: the residue kernels are bound by instruction issue
-    // and the exponent scans by DRAM, so the two chains overlap.  The side
-    // stream joins back before the GEMM (the fork and join are events, so a
-    // stream capture follows them).
-    pan[0] = 0;
-    pan[1] = n;
-    SideScope side((!reuse_a && !reuse_b) ? side_stream(0) : nullptr, stream);
-    if ((err = side.fork()) != cudaSuccess) return err;
-    if (!reuse_a &&
-        (err = prepare(a, lda, !transa, m, k, L.kpad, plan.alpha, emax_a, ea, a_res, ra,
-                       side.stream())) != cudaSuccess)
-      return err;
-    if (!reuse_b && (err = prepare_b(0, stream)) != cudaSuccess) return err;
-    if ((err = side.join()) != cudaSuccess) return err;
-    mark(1);
-    if ((err = gemm(0)) != cudaSuccess) return err;
-    mark(2);
-    if (c_ready && (err = cudaStreamWaitEvent(stream, c_ready, 0)) != cudaSuccess) return err;
-    if ((err = recon(0, stream)) != cudaSuccess) return err;
-    mark(3);
-    return cudaSuccess;
-  }
-  // Several panels: the residues of later panels (side stream 1) and the
-  // reconstruction of earlier ones (side stream 0, after A's residues) run
-  // beside the GEMM of the current panel on the caller's stream.  Their
-  // kernels (46-62 registers, at most 16 KB of shared memory) fit on an SM
-  // beside a GEMM CTA (96 registers x 192 threads, 198 KB), so the
-  // memory-bound steps hide under the tensor-bound GEMM.  Events: ev[j] panel
-  // j's residues are ready, ev[kMaxPanels + j] panel j's GEMM is done,
-  // ev[2 kMaxPanels] A's residues are ready.
-  SideScope s0(side_stream(0), stream), s1(side_stream(1), stream);
-  if ((err = s0.fork()) != cudaSuccess || (err = s1.fork()) != cudaSuccess) return err;
-  cudaEvent_t ev_a = ev[2 * kMaxPanels];
-  if (!reuse_a) {
-    if ((err = prepare(a, lda, !transa, m, k, L.kpad, plan.alpha, emax_a, ea, a_res, ra,
-                       s0.stream())) != cudaSuccess ||
-        (err = cudaEventRecord(ev_a, s0.stream())) != cudaSuccess ||
-        (err = cudaStreamWaitEvent(stream, ev_a, 0)) != cudaSuccess)
-      return err;
-  }
-  for (int j = 0; j < np; ++j) {
-    if (!reuse_b && (err = prepare_b(j, s1.stream())) != cudaSuccess) return err;
-    if ((err = cudaEventRecord(ev[j], s1.stream())) != cudaSuccess) return err;
-  }
-  mark(1);
-  if (c_ready && (err = cudaStreamWaitEvent(s0.stream(), c_ready, 0)) != cudaSuccess) return err;
-  for (int j = 0; j < np; ++j) {
-    if ((err = cudaStreamWaitEvent(stream, ev[j], 0)) != cudaSuccess ||
-        (err = gemm(j)) != cudaSuccess ||
-        (err = cudaEventRecord(ev[kMaxPanels + j], stream)) != cudaSuccess ||
-        (err = cudaStreamWaitEvent(s0.stream(), ev[kMaxPanels + j], 0)) != cudaSuccess ||
-        (err = recon(j, s0.stream())) != cudaSuccess)
-      return err;
-  }
-  mark(2);
-  if ((err = s1.join()) != cudaSuccess || (err = s0.join()) != cudaSuccess) return err;
+  const long long rgrid = (long long)((n + 1023) / 1024) * m;
+  if (rgrid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+  if (c_ready && (err = cudaStreamWaitEvent(stream, c_ready, 0)) != cudaSuccess) return err;
+  reconstruct<<<unsigned(rgrid), 256, 0, stream>>>(c, ldc, m, n, r, L.ldr, ea, eb, rc);
   mark(3);
-  return cudaSuccess;
+  return cudaGetLastError();
 }
 
 }  // namespace cfgmm

@@ -26,14 +26,9 @@ struct SideStream {
   }
 };
 
-// The calling thread's side stream `which` (0 or 1) on the current device, or
-// nullptr when one cannot be made (callers then stay on their own stream).
-const SideStream* side_stream(int which = 0);
-
-// The calling thread's pool of kSideEvents timing-free events on the current
-// device (ordering between a stream and its side streams), or nullptr.
-constexpr int kSideEvents = 16;
-cudaEvent_t* side_events();
+// The calling thread's side stream on the current device, or nullptr when one
+// cannot be made (callers then stay on their own stream).
+const SideStream* side_stream();
 
 // side->s waits for the work enqueued on `stream` so far.
 inline cudaError_t side_fork(const SideStream* side, cudaStream_t stream) {
