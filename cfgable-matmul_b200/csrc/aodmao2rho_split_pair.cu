@@ -902,7 +902,12 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
       // to shared memory while the item's chunks run; bit 4qi+j of `on`
       // marks column j of quartet qi ----
       const PairBatch& B = batch_of(p, cur.w);
-      int gpt, sg, tu_l, nq;
+      int gpt, sg, nq, eg;
+      // 2^(-tau - eg) of this lane's column, eg the largest -tau of the
+      // group's columns (so every factor is at most 1 and the group's sum
+      // is scaled by 2^eg once); 0 for a row holding Inf or NaN
+      double s_l;
+      uint32_t badbits;  // lanes whose column's D row holds Inf or NaN
       bool gval;
       uint32_t on = 0;
       {
@@ -923,7 +928,12 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
         const bool cval_l = col_l < TN && kpos_l < cur.nu;
         const int u_l = cval_l ? __ldg(p.ulist + size_t(cur.pi) * p.nao + kpos_l) : 0;
         const int f_l = cval_l ? int(p.uflag[size_t(cur.pi) * p.nao + kpos_l]) : 0;
-        tu_l = cval_l ? p.tau[size_t(cur.s) * p.nao + u_l] : 0;
+        const int tu_l = cval_l ? p.tau[size_t(cur.s) * p.nao + u_l] : kBadExp;
+        const bool bad_l = cval_l && tu_l == kBadExp;
+        eg = __reduce_max_sync(0xffffffffu, tu_l != kBadExp ? -tu_l : INT_MIN);
+        if (eg == INT_MIN) eg = 0;
+        s_l = tu_l != kBadExp ? ldexp(1.0, -tu_l - eg) : 0.0;
+        badbits = __ballot_sync(0xffffffffu, bad_l);
         sg = gval ? B.sigma[gpt] : 0;
 #pragma unroll
         for (int qi = 0; qi < C::MAXQ; ++qi) {
@@ -984,7 +994,8 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
       tc::fence_after_sync();
       if (done < static_cast<long long>(seq1) - 1) done = static_cast<long long>(seq1) - 1;
       double acc = 0.0;
-      bool badrow = false;
+      // an active column whose D row holds Inf or NaN makes the point's value NaN
+      const bool badrow = (on & badbits) != 0;
 #pragma unroll
       for (int qi = 0; qi < C::MAXQ; ++qi) {
         if (qi < nq) {
@@ -999,23 +1010,17 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(acc_empty);
           }
+          // phi_lhs is zero where the AO is inactive in this point's block
+          // and s is zero for a row holding Inf or NaN (flagged above), so
+          // every column goes through the same branch-free update
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
             const int src = qi * 4 + j;
-            const int tuj = __shfl_sync(0xffffffffu, tu_l, src);
-            if ((on >> src) & 1) {  // AOs inactive in this point's block take no part
-              if (tuj == kBadExp) {
-                badrow = true;
-              } else {
-                uint32_t lv[NSL];
+            const double sj = __shfl_sync(0xffffffffu, s_l, src);
+            uint32_t lv[NSL];
 #pragma unroll
-                for (int L = 0; L < NSL; ++L) lv[L] = v[L][j];
-                const double x = combine_levels<NSL>(lv);
-                const int e = -tuj;
-                acc = fma(phl[src * 32 + lane],
-                          (e >= -1022 && e <= 1023) ? x * pow2(e) : ldexp(x, e), acc);
-              }
-            }
+            for (int L = 0; L < NSL; ++L) lv[L] = v[L][j];
+            acc = fma(phl[src * 32 + lane], combine_levels<NSL>(lv) * sj, acc);
           }
         }
       }
@@ -1027,7 +1032,7 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
       if (ahead && !store_chunk(seq1 + uint32_t(grp), wn)) break;
       double res = 0.0;
       if (gval) {
-        const int e = -sg;
+        const int e = eg - sg;
         res = (sg == kBadExp || badrow) ? __longlong_as_double(0x7ff8000000000000LL)
               : (e >= -1022 && e <= 1023) ? acc * pow2(e)
                                           : ldexp(acc, e);
