@@ -164,6 +164,8 @@ def lib() -> ctypes.CDLL:
         L.cfgmm_server_close.restype = I
         L.cfgmm_server_submit.argtypes = [P, U64, P, S, P, ctypes.POINTER(U64)]
         L.cfgmm_server_submit.restype = I
+        L.cfgmm_server_submit_dev.argtypes = [P, U64, P, S, P, P, ctypes.POINTER(U64)]
+        L.cfgmm_server_submit_dev.restype = I
         L.cfgmm_server_wait.argtypes = [P, U64, ctypes.c_double, ctypes.POINTER(RequestStats)]
         L.cfgmm_server_wait.restype = I
         L.cfgmm_server_stats.argtypes = [P]
@@ -515,9 +517,23 @@ class Server:
         self._keep.pop(mol, None)
 
     def submit(self, mol, dms, rho) -> int:
+        """Host numpy arrays: D copied now, rho written on completion.  CUDA
+        tensors (cfgmm_server_submit_dev): D read once the current stream's
+        work so far is done, rho overwritten on the device; both must stay
+        untouched until the ticket is waited for."""
+        t = ctypes.c_uint64()
+        if _is_torch(dms) or _is_torch(rho):
+            if not (_is_torch(dms) and _is_torch(rho)) or dms.dim() != 3 or rho.dim() != 2 \
+                    or rho.shape[0] != dms.shape[0]:
+                raise ValueError("device submit: dms (nset, nao, nao) and rho (nset, ngrid), "
+                                 "both CUDA tensors")
+            _raise(lib().cfgmm_server_submit_dev(self._h, mol, _dev(dms, "torch.float64"),
+                                                 dms.shape[0], _dev(rho, "torch.float64"),
+                                                 _stream_ptr(), ctypes.byref(t)))
+            self._keep[("rho", t.value)] = (dms, rho)
+            return t.value
         pd, _ = _host(dms, np.float64)
         pr, _ = _host(rho, np.float64, True)
-        t = ctypes.c_uint64()
         _raise(lib().cfgmm_server_submit(self._h, mol, pd, dms.shape[0], pr, ctypes.byref(t)))
         self._keep[("rho", t.value)] = rho
         return t.value

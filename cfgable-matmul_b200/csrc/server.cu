@@ -137,6 +137,11 @@ struct Request {
   double* user_rho = nullptr;
   void* pin_d = nullptr;
   void* pin_rho = nullptr;
+  // device-resident request: the caller's D and rho on the device, D read
+  // after `ready` (recorded on the caller's stream at submit)
+  bool on_device = false;
+  const double* dev_d = nullptr;
+  cudaEvent_t ready = nullptr;
   size_t d_bytes = 0, rho_bytes = 0;
   Clock::time_point t_submit, t_launch, t_done;
   float device_ms = 0.f;
@@ -378,7 +383,7 @@ cfgmm_aodm_plan* plan_for(cfgmm_server* s, Molecule& m, size_t nset, cudaStream_
 
 void CUDART_CB on_device_done(void* arg) {
   Request* r = static_cast<Request*>(arg);
-  std::memcpy(r->user_rho, r->pin_rho, r->rho_bytes);
+  if (!r->on_device) std::memcpy(r->user_rho, r->pin_rho, r->rho_bytes);
   cfgmm_server* s = r->srv;
   {
     std::lock_guard<std::mutex> lk(s->mu);
@@ -395,6 +400,8 @@ void finish(cfgmm_server* s, Request& r, int status, const std::string& err) {
   s->pinned.put(r.pin_d);
   s->pinned.put(r.pin_rho);
   r.pin_d = r.pin_rho = nullptr;
+  if (r.ready) cudaEventDestroy(r.ready);
+  r.ready = nullptr;
   auto it = s->mols.find(r.mol);
   if (it != s->mols.end()) {
     Molecule& m = *it->second;
@@ -461,7 +468,14 @@ int launch(cfgmm_server* s, Request& r, Molecule& m, Slot& sl, std::string* err)
   }
   r.flops = cfgmm::aodm_plan_flops(plan);
   r.t_launch = Clock::now();
-  cudaError_t e = cudaMemcpyAsync(m.d_dms, r.pin_d, r.d_bytes, cudaMemcpyHostToDevice, sl.stream);
+  cudaError_t e = cudaSuccess;
+  if (r.on_device) {
+    e = cudaStreamWaitEvent(sl.stream, r.ready, 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(m.d_dms, r.dev_d, r.d_bytes, cudaMemcpyDeviceToDevice, sl.stream);
+  } else {
+    e = cudaMemcpyAsync(m.d_dms, r.pin_d, r.d_bytes, cudaMemcpyHostToDevice, sl.stream);
+  }
   if (e == cudaSuccess) e = cudaMemsetAsync(m.d_rho, 0, r.rho_bytes, sl.stream);
   if (e == cudaSuccess) e = cudaEventRecord(sl.e0, sl.stream);
   if (e == cudaSuccess && (rc = cfgmm_aodm_plan_run(plan, sl.stream)) != CFGMM_OK) {
@@ -470,7 +484,10 @@ int launch(cfgmm_server* s, Request& r, Molecule& m, Slot& sl, std::string* err)
   }
   if (e == cudaSuccess) e = cudaEventRecord(sl.e1, sl.stream);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(r.pin_rho, m.d_rho, r.rho_bytes, cudaMemcpyDeviceToHost, sl.stream);
+    e = r.on_device ? cudaMemcpyAsync(r.user_rho, m.d_rho, r.rho_bytes, cudaMemcpyDeviceToDevice,
+                                      sl.stream)
+                    : cudaMemcpyAsync(r.pin_rho, m.d_rho, r.rho_bytes, cudaMemcpyDeviceToHost,
+                                      sl.stream);
   if (e == cudaSuccess) e = cudaLaunchHostFunc(sl.stream, on_device_done, &r);
   if (e != cudaSuccess) {
     *err = cuda_msg(e, "request launch");
@@ -813,8 +830,14 @@ int cfgmm_server_close(cfgmm_server* s, uint64_t molecule) {
   return CFGMM_OK;
 }
 
-int cfgmm_server_submit(cfgmm_server* s, uint64_t molecule, const double* dms, size_t nset,
-                        double* rhos, uint64_t* ticket) {
+}  // extern "C"
+
+namespace {
+
+// Queues a request: host D copied to pinned staging now, or (on_device) the
+// caller's device D read once the work enqueued on `stream` so far is done.
+int submit_common(cfgmm_server* s, uint64_t molecule, const double* dms, size_t nset,
+                  double* rhos, bool on_device, cudaStream_t stream, uint64_t* ticket) {
   int rc = check_server(s);
   if (rc != CFGMM_OK) return rc;
   if (!dms || !rhos || !ticket) return fail(CFGMM_ERR_INVALID_ARGUMENT, "null pointer");
@@ -835,14 +858,26 @@ int cfgmm_server_submit(cfgmm_server* s, uint64_t molecule, const double* dms, s
   r->user_rho = rhos;
   r->d_bytes = nset * nao * nao * sizeof(double);
   r->rho_bytes = nset * ngrid * sizeof(double);
-  r->pin_d = s->pinned.get(r->d_bytes);
-  r->pin_rho = s->pinned.get(r->rho_bytes);
-  if (!r->pin_d || !r->pin_rho) {
-    s->pinned.put(r->pin_d);
-    s->pinned.put(r->pin_rho);
-    return fail(CFGMM_ERR_OUT_OF_MEMORY, "pinned staging");
+  r->on_device = on_device;
+  if (on_device) {
+    r->dev_d = dms;
+    cudaError_t e = cudaSetDevice(s->dev);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(r->ready, stream);
+    if (e != cudaSuccess) {
+      if (r->ready) cudaEventDestroy(r->ready);
+      return fail(CFGMM_ERR_CUDA, cuda_msg(e, "submit"));
+    }
+  } else {
+    r->pin_d = s->pinned.get(r->d_bytes);
+    r->pin_rho = s->pinned.get(r->rho_bytes);
+    if (!r->pin_d || !r->pin_rho) {
+      s->pinned.put(r->pin_d);
+      s->pinned.put(r->pin_rho);
+      return fail(CFGMM_ERR_OUT_OF_MEMORY, "pinned staging");
+    }
+    std::memcpy(r->pin_d, dms, r->d_bytes);
   }
-  std::memcpy(r->pin_d, dms, r->d_bytes);
   r->srv = s;
   r->t_submit = Clock::now();
   {
@@ -851,6 +886,7 @@ int cfgmm_server_submit(cfgmm_server* s, uint64_t molecule, const double* dms, s
     if (it == s->mols.end() || it->second->closed) {
       s->pinned.put(r->pin_d);
       s->pinned.put(r->pin_rho);
+      if (r->ready) cudaEventDestroy(r->ready);
       return fail(CFGMM_ERR_INVALID_ARGUMENT, "molecule closed during submit");
     }
     ++it->second->pending;
@@ -861,6 +897,21 @@ int cfgmm_server_submit(cfgmm_server* s, uint64_t molecule, const double* dms, s
   }
   s->cv_work.notify_one();
   return CFGMM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cfgmm_server_submit(cfgmm_server* s, uint64_t molecule, const double* dms, size_t nset,
+                        double* rhos, uint64_t* ticket) {
+  return submit_common(s, molecule, dms, nset, rhos, false, nullptr, ticket);
+}
+
+int cfgmm_server_submit_dev(cfgmm_server* s, uint64_t molecule, const double* dms, size_t nset,
+                            double* rhos, void* stream, uint64_t* ticket) {
+  return submit_common(s, molecule, dms, nset, rhos, true, static_cast<cudaStream_t>(stream),
+                       ticket);
 }
 
 int cfgmm_server_wait(cfgmm_server* s, uint64_t ticket, double timeout_s,

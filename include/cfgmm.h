@@ -391,6 +391,13 @@ int cfgmm_server_close(cfgmm_server* server, uint64_t molecule);
  * valid until the ticket is waited for.  Every ticket must be waited for. */
 int cfgmm_server_submit(cfgmm_server* server, uint64_t molecule, const double* dms, size_t nset,
                         double* rhos, uint64_t* ticket);
+/* The same with D and rho on the device (an SCF loop kept on the GPU): dms
+ * (nset, nao, nao) is read once the work enqueued on `stream` so far is done
+ * and must stay unchanged until the ticket is waited for; rhos (nset, ngrid)
+ * is overwritten by a device copy, complete when the wait returns.  No host
+ * staging and no PCIe traffic for the request. */
+int cfgmm_server_submit_dev(cfgmm_server* server, uint64_t molecule, const double* dms,
+                            size_t nset, double* rhos, void* stream, uint64_t* ticket);
 /* Waits for a request (timeout_s < 0: no limit; CFGMM_ERR_TIMEOUT leaves the
  * ticket valid) and returns its status; stats may be NULL. */
 int cfgmm_server_wait(cfgmm_server* server, uint64_t ticket, double timeout_s,

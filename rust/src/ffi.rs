@@ -226,6 +226,10 @@ extern "C" {
         server: *mut cfgmm_server, molecule: u64, dms: *const f64, nset: usize, rhos: *mut f64,
         ticket: *mut u64,
     ) -> c_int;
+    pub fn cfgmm_server_submit_dev(
+        server: *mut cfgmm_server, molecule: u64, dms: *const f64, nset: usize, rhos: *mut f64,
+        stream: *mut c_void, ticket: *mut u64,
+    ) -> c_int;
     pub fn cfgmm_server_wait(
         server: *mut cfgmm_server, ticket: u64, timeout_s: f64,
         stats: *mut cfgmm_request_stats,

@@ -124,6 +124,59 @@ def test_server_requests_overlap_on_the_device(cm, wl, tmp_path, monkeypatch, pr
         assert normwise(o, ref.cpu().numpy()) < tol
 
 
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "split"])
+def test_server_device_resident_requests(cm, wl, precision):
+    """cfgmm_server_submit_dev: D and rho on the device (an SCF loop kept on
+    the GPU).  Each step's D is written on the submitting stream after the
+    previous result; the results equal, bit for bit, the host-memory requests
+    of the same D matrices on the same server."""
+    import torch
+    mols = _molecules(wl, 11 + precision, 3)
+    srv = cm.Server(8 << 30, nslots=4, precision=precision)
+    try:
+        ids = [srv.open(m["ao"], m["tab"], m["nset"]) for m in mols]
+        host, dev = [], []
+        for i, m in zip(ids, mols):
+            rh = []
+            for step in range(3):
+                o = np.zeros((m["nset"], m["ao"].shape[1]))
+                srv.wait(srv.submit(i, m["dms"][step], o), WAIT)
+                rh.append(o)
+            host.append(rh)
+        side = torch.cuda.Stream()
+        with torch.cuda.stream(side):
+            for i, m in zip(ids, mols):
+                d = torch.from_numpy(m["dms"][0]).cuda()
+                outs = []
+                for step in range(3):
+                    rho = torch.full((m["nset"], m["ao"].shape[1]), float("nan"),
+                                     dtype=torch.float64, device="cuda")
+                    srv.wait(srv.submit(i, d, rho), WAIT)
+                    outs.append(rho)
+                    if step < 2:  # the next step's D, written on the submitting stream
+                        d = torch.empty_like(d)
+                        d.copy_(torch.from_numpy(m["dms"][step + 1]))
+                dev.append(outs)
+        torch.cuda.synchronize()
+        for i in ids:
+            srv.close(i)
+        st = srv.stats()
+    finally:
+        srv.shutdown()
+    assert st["failed"] == 0
+    for m, rh, rd in zip(mols, host, dev):
+        for step in range(3):
+            assert np.array_equal(rd[step].cpu().numpy(), rh[step])
+    with pytest.raises(ValueError):  # device D with a host rho
+        srv2 = cm.Server(1 << 30, nslots=1)
+        try:
+            i = srv2.open(mols[0]["ao"], mols[0]["tab"], mols[0]["nset"])
+            srv2.submit(i, torch.from_numpy(mols[0]["dms"][0]).cuda(),
+                        np.zeros((mols[0]["nset"], mols[0]["ao"].shape[1])))
+        finally:
+            srv2.shutdown()
+
+
 def test_server_budget_admission(cm, wl):
     """A budget that holds about one molecule: every request still completes,
     molecules are admitted one after another, and the server never holds more
