@@ -120,8 +120,6 @@ struct PairPrep {
   const double* ao_rhs;
   size_t stride_grid;
   int nao, ngrid, blk, nset, nsl, batch, pair0, chunk0;
-  const int* lists;       // [nblk][nao] active AOs of each block, built
-  const int* counts;      // [nblk]
   uint32_t* bits;         // scratch [nbg][ceil(nao/32)]
   int* cnt;               // scratch [nbg]
   unsigned long long* key;  // scratch [nbg]
@@ -136,7 +134,6 @@ struct PairPrep {
   int* total;             // in/out: items so far
   int* chunks_end;        // out: chunk0 + this batch's chunks
   int* sigma;             // out: [ngrid]
-  unsigned long long* pmax;  // scratch [ngrid]
   uint8_t* phisl;         // out: phi tiles from chunk0
 };
 

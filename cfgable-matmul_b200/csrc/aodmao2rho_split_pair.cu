@@ -41,18 +41,24 @@
 //   pair_union    per pair: the union list U and per-AO membership flags
 //   pair_build    one CTA: chunk offsets and the work list (pair, row tile,
 //                 DM), heaviest items first
-//   pair_phi_max, pair_phi_tiles  point scales and the phi digit tiles of
-//                 every (pair, chunk of 32 union AOs): NSL planes of 128 rows
+//   pair_phi      per pair: the point scales (max |phi| over the union AOs
+//                 active in each point's block), then the phi digit tiles of
+//                 every chunk of 32 union AOs: NSL planes of 128 rows
 //                 (points) x 32 bytes in the UMMA 32-byte-swizzled K-major
 //                 layout, so one bulk copy moves a chunk
 //   pair_d_digits D digits (8 bytes per element) and row scales
 //   pair_main     persistent, 14 warps: 12 warps gather the D digits of TN
 //                 rows x 32 union columns in three groups that take turns by
-//                 chunk and later run the epilogue; 1 warp issues the MMAs;
-//                 1 warp bulk-loads the phi tiles.  The epilogue reads each
-//                 point's TMEM row (lane = point), rebuilds X in FP64, weights
-//                 it with phi_lhs and sums over the row's AOs -- no
-//                 cross-lane reduction; X never leaves the SM.
+//                 chunk and run the epilogue; 1 warp issues the MMAs; 1 warp
+//                 draws work items (dynamic, through a ring in shared memory)
+//                 and bulk-loads the phi tiles.  A group copies the item's
+//                 phi_lhs values to shared memory as the item starts, loads
+//                 its first chunk of the next item before the accumulator
+//                 wait and stores it right after reading TMEM, so the MMAs
+//                 resume at once.  The epilogue reads each point's TMEM row
+//                 (lane = point), rebuilds X in FP64, weights it with phi_lhs
+//                 and sums over the row's AOs -- no cross-lane reduction; X
+//                 never leaves the SM.
 //   pair_reduce   adds the row tiles' partial sums of each point in a fixed
 //                 order (deterministic).
 // Every mbarrier wait is bounded (tcgen05.cuh).
@@ -550,103 +556,128 @@ pair_build(const int* __restrict__ ucount, const int* __restrict__ npairs_d, int
   }
 }
 
-// pmax[g] = max |phi[u][g]| over the active AOs of g's block (+Inf for Inf or
-// NaN); CTA (block tile, slab of 64 active AOs); pmax starts at 0.
-__global__ void __launch_bounds__(256)
-pair_phi_max(const double* __restrict__ ao, size_t stride_grid, const int* __restrict__ lists,
-             const int* __restrict__ counts, int nao, int ngrid, int blk, int gsub,
-             unsigned long long* __restrict__ pmax) {
-  const int bg = blockIdx.x, slab = blockIdx.y;
-  const int b = bg / gsub;
-  const int nb = counts[b];
-  const int i0 = slab * 64;
-  if (i0 >= nb) return;
-  int g0, gend;
-  tile_points(bg, blk, gsub, ngrid, &g0, &gend);
-  const int* I = lists + size_t(b) * nao;
-  const int gr = threadIdx.x & (HT - 1), rg = threadIdx.x >> 6;
-  const int g = g0 + gr;
-  __shared__ double red[4][HT];
-  double mx = 0.0;
-  if (g < gend) {
-    bool bad = false;
-    const int iend = min(nb, i0 + 64);
-    for (int i = i0 + rg; i < iend; i += 4) {
-      const double a = fabs(ao[size_t(__ldg(I + i)) * stride_grid + g]);
-      bad |= !(a <= 1.7976931348623157e308);
-      mx = fmax(mx, a);
-    }
-    if (bad) mx = __longlong_as_double(0x7ff0000000000000LL);
-  }
-  red[rg][gr] = mx;
-  __syncthreads();
-  if (threadIdx.x < HT && g < gend) {
-    const double m = fmax(fmax(red[0][gr], red[1][gr]), fmax(red[2][gr], red[3][gr]));
-    atomicMax(pmax + g, static_cast<unsigned long long>(__double_as_longlong(m)));
-  }
-}
+// The phi digit tiles of pair pi: for every chunk c of 32 union AOs, NSL
+// planes of 128 rows (points: rows 0-63 the lo tile, 64-127 the hi tile) x
+// 32 bytes (union AOs 32c .. 32c+31), 32-byte swizzled, at phisl + (cbase[pi]
+// + c) * A_STAGE.  One CTA per pair: first the point scales sigma[g] from
+// max |phi[u][g]| over the AOs of the union active in g's block (Inf or NaN
+// among them: kBadExp), then the chunks, kPhiChunks at a time.
+constexpr int kPhiChunks = 2;
+constexpr int kPhiThreads = 256 * kPhiChunks;
 
-// The phi digit tiles of chunk c of pair pi: NSL planes of 128 rows (points:
-// rows 0-63 the lo tile, 64-127 the hi tile) x 32 bytes (union AOs
-// 32c .. 32c+31), 32-byte swizzled, at phisl + (cbase[pi] + c) * A_STAGE;
-// sigma[g] from pmax.  CTA (pair, chunk).
 template <int NSL>
-__global__ void __launch_bounds__(256)
-pair_phi_tiles(const double* __restrict__ ao, size_t stride_grid,
-               const unsigned long long* __restrict__ pmax, const int4* __restrict__ pairs,
-               const int* __restrict__ npairs, int pair0, const int* __restrict__ ulist,
-               const uint8_t* __restrict__ uflag, const int* __restrict__ ucount,
-               const int* __restrict__ cbase, int nao, int ngrid, int blk, int gsub,
-               int* __restrict__ sigma, uint8_t* __restrict__ phisl) {
+__global__ void __launch_bounds__(kPhiThreads)
+pair_phi(const double* __restrict__ ao, size_t stride_grid, const int4* __restrict__ pairs,
+         const int* __restrict__ npairs, int pair0, const int* __restrict__ ulist,
+         const uint8_t* __restrict__ uflag, const int* __restrict__ ucount,
+         const int* __restrict__ cbase, int nao, int ngrid, int blk, int gsub,
+         int* __restrict__ sigma, uint8_t* __restrict__ phisl) {
   using C = Cfg<NSL>;
-  const int pl = blockIdx.x, c = blockIdx.y;
+  const int pl = blockIdx.x;
   if (pl >= npairs[0]) return;
   const int pi = pair0 + pl;
   const int nu = ucount[pi];
-  if (c * TK >= nu) return;
   const int4 pr = pairs[pi];
-  // staged digit words [plane][quad of 4 AOs][point], rows padded to 132 words
-  __shared__ uint32_t stage[NSL][8][PT + 4];
+  // staged digit words [chunk][plane][quad of 4 AOs][point], rows padded to
+  // 132 words; the scales' partial maxima reuse the space
+  extern __shared__ uint32_t phi_stage[];
+  __shared__ int esh[PT];
   const int* U = ulist + size_t(pi) * nao;
   const uint8_t* F = uflag + size_t(pi) * nao;
+  const int r = threadIdx.x & (PT - 1);  // point row
+  const int h = r >> 6;
+  int g = -1;
   {
-    const int v = threadIdx.x;
-    const int r = v & (PT - 1), hq = v >> 7;  // point row, half of the quads
-    const int h = r >> 6, j = r & (HT - 1);
     const int tile = h ? pr.y : pr.x;
-    int g = -1;
     if (tile >= 0) {
       int g0, gend;
       tile_points(tile, blk, gsub, ngrid, &g0, &gend);
-      if (g0 + j < gend) g = g0 + j;
-    }
-    const int e = g >= 0 ? exp_for(__longlong_as_double(static_cast<long long>(pmax[g]))) : 0;
-    if (c == 0 && hq == 0 && g >= 0) sigma[g] = e;
-#pragma unroll
-    for (int qq = 0; qq < 4; ++qq) {
-      const int q = hq * 4 + qq;
-      uint2 w[4];
-#pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        const int k = c * TK + q * 4 + t;
-        bool on = g >= 0 && k < nu && e != kBadExp;
-        if (on) on = ((F[k] >> h) & 1u) != 0;
-        w[t] = on ? digits_of<NSL>(ao[size_t(U[k]) * stride_grid + g], e) : make_uint2(0u, 0u);
-      }
-      uint32_t o[8];
-      transpose4(w[0].x, w[1].x, w[2].x, w[3].x, o[0], o[1], o[2], o[3]);
-      transpose4(w[0].y, w[1].y, w[2].y, w[3].y, o[4], o[5], o[6], o[7]);
-#pragma unroll
-      for (int pl2 = 0; pl2 < NSL; ++pl2) stage[pl2][q][r] = o[pl2];
+      if (g0 + (r & (HT - 1)) < gend) g = g0 + (r & (HT - 1));
     }
   }
-  __syncthreads();
-  uint8_t* tile0 = phisl + (size_t(cbase[pi]) + c) * C::A_STAGE;
-  for (int v = threadIdx.x; v < NSL * PT * 2; v += 256) {
-    const int hh = v & 1, r = (v >> 1) & (PT - 1), j = v >> 8;
-    const uint4 w = make_uint4(stage[j][4 * hh][r], stage[j][4 * hh + 1][r],
-                               stage[j][4 * hh + 2][r], stage[j][4 * hh + 3][r]);
-    *reinterpret_cast<uint4*>(tile0 + j * C::A_SLICE + tc::sw32_offset(uint32_t(r), uint32_t(hh))) = w;
+  // ---- scales: thread (row, kq) takes union positions kq, kq + KQ, ... ----
+  {
+    constexpr int KQ = kPhiThreads / PT;
+    const int kq = threadIdx.x / PT;
+    double mx = 0.0;
+    bool bad = false;
+    if (g >= 0) {
+      int k = kq;
+      for (; k + 3 * KQ < nu; k += 4 * KQ) {  // four loads in flight
+        double a[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const int kk = k + t * KQ;
+          a[t] = ((__ldg(F + kk) >> h) & 1u) ? fabs(ao[size_t(__ldg(U + kk)) * stride_grid + g])
+                                             : 0.0;
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          bad |= !(a[t] <= 1.7976931348623157e308);
+          mx = fmax(mx, a[t]);
+        }
+      }
+      for (; k < nu; k += KQ) {
+        if ((__ldg(F + k) >> h) & 1u) {
+          const double a = fabs(ao[size_t(__ldg(U + k)) * stride_grid + g]);
+          bad |= !(a <= 1.7976931348623157e308);
+          mx = fmax(mx, a);
+        }
+      }
+    }
+    double* red = reinterpret_cast<double*>(phi_stage);  // [KQ][PT]
+    red[kq * PT + r] = bad ? __longlong_as_double(0x7ff0000000000000LL) : mx;
+    __syncthreads();
+    if (threadIdx.x < PT) {
+      double m = red[r];
+#pragma unroll
+      for (int q = 1; q < KQ; ++q) m = fmax(m, red[q * PT + r]);
+      const int e = exp_for(m);
+      esh[r] = e;
+      if (g >= 0) sigma[g] = e;
+    }
+    __syncthreads();
+  }
+  // ---- digit tiles: thread (row, half of the quads, chunk slot) ----
+  const int e = esh[r];
+  const int hq = (threadIdx.x >> 7) & 1, slot = threadIdx.x >> 8;
+  uint32_t* stage = phi_stage + slot * (NSL * 8 * (PT + 4));
+  const int kc = (nu + TK - 1) / TK;
+  for (int c0 = 0; c0 < kc; c0 += kPhiChunks) {
+    const int c = c0 + slot;
+    if (c < kc) {
+      uint2 w[4][4];
+#pragma unroll
+      for (int qq = 0; qq < 4; ++qq)
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const int k = c * TK + (hq * 4 + qq) * 4 + t;
+          const bool on = g >= 0 && k < nu && e != kBadExp && ((__ldg(F + k) >> h) & 1u);
+          w[qq][t] = on ? digits_of<NSL>(ao[size_t(__ldg(U + k)) * stride_grid + g], e)
+                        : make_uint2(0u, 0u);
+        }
+#pragma unroll
+      for (int qq = 0; qq < 4; ++qq) {
+        const int q = hq * 4 + qq;
+        uint32_t o[8];
+        transpose4(w[qq][0].x, w[qq][1].x, w[qq][2].x, w[qq][3].x, o[0], o[1], o[2], o[3]);
+        transpose4(w[qq][0].y, w[qq][1].y, w[qq][2].y, w[qq][3].y, o[4], o[5], o[6], o[7]);
+#pragma unroll
+        for (int pl2 = 0; pl2 < NSL; ++pl2) stage[(pl2 * 8 + q) * (PT + 4) + r] = o[pl2];
+      }
+    }
+    __syncthreads();
+    if (c < kc) {
+      uint8_t* tile0 = phisl + (size_t(cbase[pi]) + c) * C::A_STAGE;
+      for (int v = threadIdx.x & 255; v < NSL * PT * 2; v += 256) {
+        const int hh = v & 1, rr = (v >> 1) & (PT - 1), j = v >> 8;
+        const uint32_t* sj = stage + (j * 8 + 4 * hh) * (PT + 4) + rr;
+        const uint4 wv = make_uint4(sj[0], sj[PT + 4], sj[2 * (PT + 4)], sj[3 * (PT + 4)]);
+        *reinterpret_cast<uint4*>(tile0 + j * C::A_SLICE +
+                                  tc::sw32_offset(uint32_t(rr), uint32_t(hh))) = wv;
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -1225,8 +1256,8 @@ cudaError_t launch_pair_main_t(int nsm, const PairArgs& a, cudaStream_t stream, 
 size_t a256(size_t v) { return (v + 255) / 256 * 256; }
 
 struct Layout {
-  size_t lists, counts, bits, cnt, key, order, cand, ncand, partner, pos, choice, pairs, npairs,
-      ulist, uflag, ucount, cbase, items, total, dsl, tau, sigma, pmax, phisl, partial, bytes;
+  size_t bits, cnt, key, order, cand, ncand, partner, pos, choice, pairs, npairs,
+      ulist, uflag, ucount, cbase, items, total, dsl, tau, sigma, phisl, partial, bytes;
 };
 
 Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk, int nsl) {
@@ -1239,9 +1270,7 @@ Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk, int nsl) {
   const size_t nwords = (nao + 31) / 32;
   const size_t a_stage = size_t(nsl) * PT * TK;
   Layout L;
-  L.lists = 0;
-  L.counts = L.lists + a256(nblk * nao * sizeof(int));
-  L.bits = L.counts + a256(nblk * sizeof(int));
+  L.bits = 0;
   L.cnt = L.bits + a256(nbg * nwords * sizeof(uint32_t));
   L.key = L.cnt + a256(nbg * sizeof(int));
   L.order = L.key + a256(nbg * sizeof(unsigned long long));
@@ -1261,8 +1290,7 @@ Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk, int nsl) {
   L.dsl = L.total + 256;
   L.tau = L.dsl + a256(nset * nao * nao * 8);
   L.sigma = L.tau + a256(nset * nao * sizeof(int));
-  L.pmax = L.sigma + a256(ngrid * sizeof(int));
-  L.phisl = L.pmax + a256(ngrid * sizeof(unsigned long long));
+  L.phisl = L.sigma + a256(ngrid * sizeof(int));
   L.partial = L.phisl + a256(nbg * max_kc * a_stage);
   L.bytes = L.partial + nbg * max_t * nset * PT * sizeof(double);
   return L;
@@ -1351,20 +1379,19 @@ cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream) {
   const size_t hist = size_t(max_kc + 2) * sizeof(int);
   pair_build<<<1, 1024, hist, stream>>>(q.ucount, q.npairs, q.pair0, q.nset, q.batch, tn, max_kc,
                                         q.chunk0, q.cbase, q.items, q.total, q.chunks_end);
-  cudaError_t err = cudaMemsetAsync(q.pmax, 0, size_t(q.ngrid) * sizeof(unsigned long long),
-                                    stream);
+  // one CTA per pair (nbg bounds the pairs)
+  auto launch_phi = [&](auto kern, int nsl) -> cudaError_t {
+    const size_t smem = size_t(kPhiChunks) * nsl * 8 * (PT + 4) * sizeof(uint32_t);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(smem));
+    if (e != cudaSuccess) return e;
+    kern<<<nbg, kPhiThreads, smem, stream>>>(q.ao_rhs, q.stride_grid, q.pairs, q.npairs, q.pair0,
+                                             q.ulist, q.uflag, q.ucount, q.cbase, q.nao, q.ngrid,
+                                             q.blk, gsub, q.sigma, q.phisl);
+    return cudaSuccess;
+  };
+  const cudaError_t err = q.nsl == 6 ? launch_phi(pair_phi<6>, 6) : launch_phi(pair_phi<7>, 7);
   if (err != cudaSuccess) return err;
-  pair_phi_max<<<dim3(nbg, (q.nao + 63) / 64), 256, 0, stream>>>(
-      q.ao_rhs, q.stride_grid, q.lists, q.counts, q.nao, q.ngrid, q.blk, gsub, q.pmax);
-  const dim3 tg(nbg, max_kc);
-  if (q.nsl == 6)
-    pair_phi_tiles<6><<<tg, 256, 0, stream>>>(q.ao_rhs, q.stride_grid, q.pmax, q.pairs, q.npairs,
-                                              q.pair0, q.ulist, q.uflag, q.ucount, q.cbase, q.nao,
-                                              q.ngrid, q.blk, gsub, q.sigma, q.phisl);
-  else
-    pair_phi_tiles<7><<<tg, 256, 0, stream>>>(q.ao_rhs, q.stride_grid, q.pmax, q.pairs, q.npairs,
-                                              q.pair0, q.ulist, q.uflag, q.ucount, q.cbase, q.nao,
-                                              q.ngrid, q.blk, gsub, q.sigma, q.phisl);
   return cudaGetLastError();
 }
 
@@ -1382,8 +1409,6 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   const Layout L = layout(nao, ngrid, nset, blk, nsl);
   char* ws = static_cast<char*>(workspace);
   auto at = [&](size_t off) { return static_cast<void*>(ws + off); };
-  int* lists = static_cast<int*>(at(L.lists));
-  int* counts = static_cast<int*>(at(L.counts));
   PairPrep q{};
   q.tab = tab;
   q.ldtab = ldtab;
@@ -1397,8 +1422,6 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   q.batch = 0;
   q.pair0 = 0;
   q.chunk0 = 0;
-  q.lists = lists;
-  q.counts = counts;
   q.bits = static_cast<uint32_t*>(at(L.bits));
   q.cnt = static_cast<int*>(at(L.cnt));
   q.key = static_cast<unsigned long long*>(at(L.key));
@@ -1418,7 +1441,6 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   q.total = static_cast<int*>(at(L.total));
   q.chunks_end = q.total + 2;
   q.sigma = static_cast<int*>(at(L.sigma));
-  q.pmax = static_cast<unsigned long long*>(at(L.pmax));
   q.phisl = static_cast<uint8_t*>(at(L.phisl));
   uint2* dsl = static_cast<uint2*>(at(L.dsl));
   int* tau = static_cast<int*>(at(L.tau));
@@ -1428,7 +1450,7 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   cudaError_t err = cudaMemsetAsync(q.total, 0, 4 * sizeof(int), stream);
   if (err != cudaSuccess) return err;
   // The D chain (symmetry check, D digits) runs on a side stream beside the
-  // phi chain (block lists, pairing, unions, work list, phi tiles); the side
+  // phi chain (pairing, unions, work list, phi tiles); the side
   // stream joins back before the main kernel.
   SideScope side(side_stream(), stream);
   if ((err = side.fork()) != cudaSuccess) return err;
@@ -1436,9 +1458,6 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   if (asym && (err = aodm_launch_sym_check(dms, stride_ao, nao, nset, asym, sd)) != cudaSuccess)
     return err;
   if ((err = split_pair_prepare_d(dms, stride_ao, nao, nset, nsl, dsl, tau, sd, asym)) !=
-      cudaSuccess)
-    return err;
-  if ((err = aodm_block_lists_launch(tab, ldtab, nao, nblk, lists, counts, stream)) !=
       cudaSuccess)
     return err;
   if ((err = split_pair_prepare_batch(q, stream)) != cudaSuccess) return err;
