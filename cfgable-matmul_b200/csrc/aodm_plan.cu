@@ -470,7 +470,7 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
                o_key = take(nbg_max * 8), o_order = take(nbg_max * 4),
                o_cand = take(nbg_max * WIN2 * 4), o_ncand = take(nbg_max * 4),
                o_partner = take(nbg_max * 4), o_pos = take(nbg_max * 4),
-               o_choice = take(nbg_max * 4),
+               o_choice = take(nbg_max * 4), o_pmax = take(ngrid_max * 8),
                o_pairs = take(nbg_tot * sizeof(int4)), o_np = take(8),
                o_ulist = take(nbg_tot * nao * 4), o_uflag = take(nbg_tot * nao),
                o_ucount = take(nbg_tot * 4), o_cbase = take((nbg_tot + 1) * 4),
@@ -504,6 +504,7 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
     q.batch = int(i);
     q.pair0 = pair0;
     q.chunk0 = chunk0;
+    q.pmax = static_cast<unsigned long long*>(at(o_pmax));
     q.bits = static_cast<uint32_t*>(at(o_bits));
     q.cnt = static_cast<int*>(at(o_cnt));
     q.key = static_cast<unsigned long long*>(at(o_key));

@@ -134,6 +134,7 @@ struct PairPrep {
   int* total;             // in/out: items so far
   int* chunks_end;        // out: chunk0 + this batch's chunks
   int* sigma;             // out: [ngrid]
+  unsigned long long* pmax;  // scratch [ngrid]
   uint8_t* phisl;         // out: phi tiles from chunk0
 };
 

@@ -41,9 +41,9 @@
 //   pair_union    per pair: the union list U and per-AO membership flags
 //   pair_build    one CTA: chunk offsets and the work list (pair, row tile,
 //                 DM), heaviest items first
-//   pair_phi      per pair: the point scales (max |phi| over the union AOs
-//                 active in each point's block), then the phi digit tiles of
-//                 every chunk of 32 union AOs: NSL planes of 128 rows
+//   pair_phi_max, pair_phi_tiles  point scales (max |phi| over the union
+//                 AOs active in each point's block) and the phi digit tiles of
+//                 every (pair, chunk of 32 union AOs): NSL planes of 128 rows
 //                 (points) x 32 bytes in the UMMA 32-byte-swizzled K-major
 //                 layout, so one bulk copy moves a chunk
 //   pair_d_digits D digits (8 bytes per element) and row scales
@@ -556,148 +556,141 @@ pair_build(const int* __restrict__ ucount, const int* __restrict__ npairs_d, int
   }
 }
 
-// The phi digit tiles of pair pi: for every chunk c of 32 union AOs, NSL
-// planes of 128 rows (points: rows 0-63 the lo tile, 64-127 the hi tile) x
-// 32 bytes (union AOs 32c .. 32c+31), 32-byte swizzled, at phisl + (cbase[pi]
-// + c) * A_STAGE.  One CTA per pair: first the point scales sigma[g] from
-// max |phi[u][g]| over the AOs of the union active in g's block (Inf or NaN
-// among them: kBadExp), then the chunks, kPhiChunks at a time.
-constexpr int kPhiChunks = 2;
-constexpr int kPhiThreads = 256 * kPhiChunks;
-
-template <int NSL>
-__global__ void __launch_bounds__(kPhiThreads)
-pair_phi(const double* __restrict__ ao, size_t stride_grid, const int4* __restrict__ pairs,
-         const int* __restrict__ npairs, int pair0, const int* __restrict__ ulist,
-         const uint8_t* __restrict__ uflag, const int* __restrict__ ucount,
-         const int* __restrict__ cbase, int nao, int ngrid, int blk, int gsub,
-         int* __restrict__ sigma, uint8_t* __restrict__ phisl) {
-  using C = Cfg<NSL>;
-  const int pl = blockIdx.x;
+// pmax[g] = max |phi[u][g]| over the union AOs active in g's block (+Inf for
+// Inf or NaN); CTA (pair, slab of 32 union positions); pmax starts at 0.
+__global__ void __launch_bounds__(256)
+pair_phi_max(const double* __restrict__ ao, size_t stride_grid, const int4* __restrict__ pairs,
+             const int* __restrict__ npairs, int pair0, const int* __restrict__ ulist,
+             const uint8_t* __restrict__ uflag, const int* __restrict__ ucount, int nao,
+             int ngrid, int blk, int gsub, unsigned long long* __restrict__ pmax) {
+  const int pl = blockIdx.x, slab = blockIdx.y;
   if (pl >= npairs[0]) return;
   const int pi = pair0 + pl;
   const int nu = ucount[pi];
+  const int k0 = slab * 32;
+  if (k0 >= nu) return;
   const int4 pr = pairs[pi];
-  // staged digit words [chunk][plane][quad of 4 AOs][point], rows padded to
-  // 132 words; the scales' partial maxima reuse the space
-  extern __shared__ uint32_t phi_stage[];
-  __shared__ int esh[PT];
   const int* U = ulist + size_t(pi) * nao;
   const uint8_t* F = uflag + size_t(pi) * nao;
-  const int r = threadIdx.x & (PT - 1);  // point row
+  const int r = threadIdx.x & (PT - 1), kq = threadIdx.x >> 7;  // point row, half of the slab
   const int h = r >> 6;
+  const int tile = h ? pr.y : pr.x;
   int g = -1;
+  if (tile >= 0) {
+    int g0, gend;
+    tile_points(tile, blk, gsub, ngrid, &g0, &gend);
+    if (g0 + (r & (HT - 1)) < gend) g = g0 + (r & (HT - 1));
+  }
+  __shared__ double red[2][PT];
+  double mx = 0.0;
+  if (g >= 0) {
+    bool bad = false;
+    const int kend = min(nu, k0 + 32);
+    double a[16];
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {  // every load in flight at once
+      const int k = k0 + kq + 2 * t;
+      a[t] = k < kend && ((__ldg(F + k) >> h) & 1u)
+                 ? fabs(ao[size_t(__ldg(U + k)) * stride_grid + g])
+                 : 0.0;
+    }
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+      bad |= !(a[t] <= 1.7976931348623157e308);
+      mx = fmax(mx, a[t]);
+    }
+    if (bad) mx = __longlong_as_double(0x7ff0000000000000LL);
+  }
+  red[kq][r] = mx;
+  __syncthreads();
+  if (threadIdx.x < PT && g >= 0)
+    atomicMax(pmax + g, static_cast<unsigned long long>(
+                            __double_as_longlong(fmax(red[0][r], red[1][r]))));
+}
+
+// The phi digit tiles of chunk c of pair pi: NSL planes of 128 rows (points:
+// rows 0-63 the lo tile, 64-127 the hi tile) x 32 bytes (union AOs
+// 32c .. 32c+31), 32-byte swizzled, at phisl + (cbase[pi] + c) * A_STAGE;
+// sigma[g] from pmax.  CTA (pair, chunk).
+template <int NSL>
+__global__ void __launch_bounds__(256)
+pair_phi_tiles(const double* __restrict__ ao, size_t stride_grid,
+               const unsigned long long* __restrict__ pmax, const int4* __restrict__ pairs,
+               const int* __restrict__ npairs, int pair0, const int* __restrict__ ulist,
+               const uint8_t* __restrict__ uflag, const int* __restrict__ ucount,
+               const int* __restrict__ cbase, int nao, int ngrid, int blk, int gsub,
+               int* __restrict__ sigma, uint8_t* __restrict__ phisl) {
+  using C = Cfg<NSL>;
+  const int pl = blockIdx.x, c = blockIdx.y;
+  if (pl >= npairs[0]) return;
+  const int pi = pair0 + pl;
+  const int nu = ucount[pi];
+  if (c * TK >= nu) return;
+  const int4 pr = pairs[pi];
+  // staged digit words [plane][quad of 4 AOs][point], rows padded to 132 words
+  __shared__ uint32_t stage[NSL][8][PT + 4];
+  const int* U = ulist + size_t(pi) * nao;
+  const uint8_t* F = uflag + size_t(pi) * nao;
   {
+    const int r = threadIdx.x & (PT - 1), hq = threadIdx.x >> 7;  // point row, half of the quads
+    const int h = r >> 6;
     const int tile = h ? pr.y : pr.x;
+    int g = -1;
     if (tile >= 0) {
       int g0, gend;
       tile_points(tile, blk, gsub, ngrid, &g0, &gend);
       if (g0 + (r & (HT - 1)) < gend) g = g0 + (r & (HT - 1));
     }
+    const int e = g >= 0 ? exp_for(__longlong_as_double(static_cast<long long>(pmax[g]))) : 0;
+    if (c == 0 && hq == 0 && g >= 0) sigma[g] = e;
+    uint2 w[4][4];  // every load in flight at once
+#pragma unroll
+    for (int qq = 0; qq < 4; ++qq)
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int k = c * TK + (hq * 4 + qq) * 4 + t;
+        const bool on = g >= 0 && k < nu && e != kBadExp && ((__ldg(F + k) >> h) & 1u);
+        w[qq][t] = on ? digits_of<NSL>(ao[size_t(__ldg(U + k)) * stride_grid + g], e)
+                      : make_uint2(0u, 0u);
+      }
+#pragma unroll
+    for (int qq = 0; qq < 4; ++qq) {
+      const int q = hq * 4 + qq;
+      uint32_t o[8];
+      transpose4(w[qq][0].x, w[qq][1].x, w[qq][2].x, w[qq][3].x, o[0], o[1], o[2], o[3]);
+      transpose4(w[qq][0].y, w[qq][1].y, w[qq][2].y, w[qq][3].y, o[4], o[5], o[6], o[7]);
+#pragma unroll
+      for (int pl2 = 0; pl2 < NSL; ++pl2) stage[pl2][q][r] = o[pl2];
+    }
   }
-  // ---- scales: thread (row, kq) takes union positions kq, kq + KQ, ... ----
-  {
-    constexpr int KQ = kPhiThreads / PT;
-    const int kq = threadIdx.x / PT;
-    double mx = 0.0;
-    bool bad = false;
-    if (g >= 0) {
-      int k = kq;
-      for (; k + 3 * KQ < nu; k += 4 * KQ) {  // four loads in flight
-        double a[4];
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const int kk = k + t * KQ;
-          a[t] = ((__ldg(F + kk) >> h) & 1u) ? fabs(ao[size_t(__ldg(U + kk)) * stride_grid + g])
-                                             : 0.0;
-        }
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          bad |= !(a[t] <= 1.7976931348623157e308);
-          mx = fmax(mx, a[t]);
-        }
-      }
-      for (; k < nu; k += KQ) {
-        if ((__ldg(F + k) >> h) & 1u) {
-          const double a = fabs(ao[size_t(__ldg(U + k)) * stride_grid + g]);
-          bad |= !(a <= 1.7976931348623157e308);
-          mx = fmax(mx, a);
-        }
-      }
-    }
-    double* red = reinterpret_cast<double*>(phi_stage);  // [KQ][PT]
-    red[kq * PT + r] = bad ? __longlong_as_double(0x7ff0000000000000LL) : mx;
-    __syncthreads();
-    if (threadIdx.x < PT) {
-      double m = red[r];
-#pragma unroll
-      for (int q = 1; q < KQ; ++q) m = fmax(m, red[q * PT + r]);
-      const int e = exp_for(m);
-      esh[r] = e;
-      if (g >= 0) sigma[g] = e;
-    }
-    __syncthreads();
-  }
-  // ---- digit tiles: thread (row, half of the quads, chunk slot) ----
-  const int e = esh[r];
-  const int hq = (threadIdx.x >> 7) & 1, slot = threadIdx.x >> 8;
-  uint32_t* stage = phi_stage + slot * (NSL * 8 * (PT + 4));
-  const int kc = (nu + TK - 1) / TK;
-  for (int c0 = 0; c0 < kc; c0 += kPhiChunks) {
-    const int c = c0 + slot;
-    if (c < kc) {
-      uint2 w[4][4];
-#pragma unroll
-      for (int qq = 0; qq < 4; ++qq)
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const int k = c * TK + (hq * 4 + qq) * 4 + t;
-          const bool on = g >= 0 && k < nu && e != kBadExp && ((__ldg(F + k) >> h) & 1u);
-          w[qq][t] = on ? digits_of<NSL>(ao[size_t(__ldg(U + k)) * stride_grid + g], e)
-                        : make_uint2(0u, 0u);
-        }
-#pragma unroll
-      for (int qq = 0; qq < 4; ++qq) {
-        const int q = hq * 4 + qq;
-        uint32_t o[8];
-        transpose4(w[qq][0].x, w[qq][1].x, w[qq][2].x, w[qq][3].x, o[0], o[1], o[2], o[3]);
-        transpose4(w[qq][0].y, w[qq][1].y, w[qq][2].y, w[qq][3].y, o[4], o[5], o[6], o[7]);
-#pragma unroll
-        for (int pl2 = 0; pl2 < NSL; ++pl2) stage[(pl2 * 8 + q) * (PT + 4) + r] = o[pl2];
-      }
-    }
-    __syncthreads();
-    if (c < kc) {
-      uint8_t* tile0 = phisl + (size_t(cbase[pi]) + c) * C::A_STAGE;
-      for (int v = threadIdx.x & 255; v < NSL * PT * 2; v += 256) {
-        const int hh = v & 1, rr = (v >> 1) & (PT - 1), j = v >> 8;
-        const uint32_t* sj = stage + (j * 8 + 4 * hh) * (PT + 4) + rr;
-        const uint4 wv = make_uint4(sj[0], sj[PT + 4], sj[2 * (PT + 4)], sj[3 * (PT + 4)]);
-        *reinterpret_cast<uint4*>(tile0 + j * C::A_SLICE +
-                                  tc::sw32_offset(uint32_t(rr), uint32_t(hh))) = wv;
-      }
-    }
-    __syncthreads();
+  __syncthreads();
+  uint8_t* tile0 = phisl + (size_t(cbase[pi]) + c) * C::A_STAGE;
+  for (int v = threadIdx.x; v < NSL * PT * 2; v += 256) {
+    const int hh = v & 1, r = (v >> 1) & (PT - 1), j = v >> 8;
+    const uint4 wv = make_uint4(stage[j][4 * hh][r], stage[j][4 * hh + 1][r],
+                                stage[j][4 * hh + 2][r], stage[j][4 * hh + 3][r]);
+    *reinterpret_cast<uint4*>(tile0 + j * C::A_SLICE + tc::sw32_offset(uint32_t(r), uint32_t(hh))) =
+        wv;
   }
 }
 
-// D digits: dsl[s][u][v] (NSL digits in 8 bytes), tau[s][u]; a warp per row.
-// With asym non-null and 0 (symmetric mode) the diagonal carries D_uu / 2.
+// D digits: dsl[s][u][v] (NSL digits in 8 bytes), tau[s][u]; a CTA per row
+// (its max first, then the digits, the second read from L1).  With asym
+// non-null and 0 (symmetric mode) the diagonal carries D_uu / 2.
 template <int NSL>
 __global__ void __launch_bounds__(256)
 pair_d_digits(const double* __restrict__ dms, size_t stride_ao, size_t dm_stride, int nao,
-              int nrows, uint2* __restrict__ dsl, int* __restrict__ tau,
-              const int* __restrict__ asym) {
-  const int row = blockIdx.x * 8 + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (row >= nrows) return;
+              uint2* __restrict__ dsl, int* __restrict__ tau, const int* __restrict__ asym) {
+  const int row = blockIdx.x;
   const bool half_diag = asym != nullptr && *asym == 0;
   const int s = row / nao, u = row % nao;
   const double* d = dms + size_t(s) * dm_stride + size_t(u) * stride_ao;
+  __shared__ double wmax[8];
+  __shared__ int wbad[8];
   double mx = 0.0;
   bool bad = false;
 #pragma unroll 4
-  for (int v = lane; v < nao; v += 32) {
+  for (int v = threadIdx.x; v < nao; v += 256) {
     const double a = fabs(d[v]);
     bad |= !(a <= 1.7976931348623157e308);
     mx = fmax(mx, a);
@@ -707,14 +700,27 @@ pair_d_digits(const double* __restrict__ dms, size_t stride_ao, size_t dm_stride
     mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     bad |= __shfl_xor_sync(0xffffffffu, int(bad), o) != 0;
   }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    wmax[w] = mx;
+    wbad[w] = bad;
+  }
+  __syncthreads();
+  mx = wmax[0];
+  bad = wbad[0] != 0;
+#pragma unroll
+  for (int i = 1; i < 8; ++i) {
+    mx = fmax(mx, wmax[i]);
+    bad |= wbad[i] != 0;
+  }
   const int e = bad ? kBadExp : exp_for(mx);
-  if (lane == 0) tau[row] = e;
+  if (threadIdx.x == 0) tau[row] = e;
   uint2* out = dsl + size_t(row) * nao;
   // symmetric mode: the gather reads only v >= u (union positions ascend with
   // the AO index), so the strict lower triangle is not written
-  const int v0 = half_diag ? (u & ~31) + lane : lane;
+  const int v0 = (half_diag ? (u & ~31) : 0) + int(threadIdx.x);
 #pragma unroll 4
-  for (int v = v0; v < nao; v += 32)
+  for (int v = v0; v < nao; v += 256)
     out[v] = e != kBadExp ? digits_of<NSL>(half_diag && v == u ? 0.5 * d[v] : d[v], e)
                           : make_uint2(0u, 0u);
 }
@@ -1257,7 +1263,7 @@ size_t a256(size_t v) { return (v + 255) / 256 * 256; }
 
 struct Layout {
   size_t bits, cnt, key, order, cand, ncand, partner, pos, choice, pairs, npairs,
-      ulist, uflag, ucount, cbase, items, total, dsl, tau, sigma, phisl, partial, bytes;
+      ulist, uflag, ucount, cbase, items, total, dsl, tau, sigma, pmax, phisl, partial, bytes;
 };
 
 Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk, int nsl) {
@@ -1290,7 +1296,8 @@ Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk, int nsl) {
   L.dsl = L.total + 256;
   L.tau = L.dsl + a256(nset * nao * nao * 8);
   L.sigma = L.tau + a256(nset * nao * sizeof(int));
-  L.phisl = L.sigma + a256(ngrid * sizeof(int));
+  L.pmax = L.sigma + a256(ngrid * sizeof(int));
+  L.phisl = L.pmax + a256(ngrid * sizeof(unsigned long long));
   L.partial = L.phisl + a256(nbg * max_kc * a_stage);
   L.bytes = L.partial + nbg * max_t * nset * PT * sizeof(double);
   return L;
@@ -1337,19 +1344,19 @@ cudaError_t split_pair_launch_reduce(const PairArgs& a, int nsl, const int* npai
 
 cudaError_t split_pair_prepare_d(const double* dms, size_t stride_ao, int nao, int nset, int nsl,
                                  uint2* dsl, int* tau, cudaStream_t stream, const int* asym) {
-  const unsigned grid = unsigned((nset * nao + 7) / 8);
+  const unsigned grid = unsigned(nset * nao);
   if (nsl == 6)
-    pair_d_digits<6><<<grid, 256, 0, stream>>>(dms, stride_ao, stride_ao * stride_ao, nao,
-                                                nset * nao, dsl, tau, asym);
+    pair_d_digits<6><<<grid, 256, 0, stream>>>(dms, stride_ao, stride_ao * stride_ao, nao, dsl,
+                                                tau, asym);
   else
-    pair_d_digits<7><<<grid, 256, 0, stream>>>(dms, stride_ao, stride_ao * stride_ao, nao,
-                                                nset * nao, dsl, tau, asym);
+    pair_d_digits<7><<<grid, 256, 0, stream>>>(dms, stride_ao, stride_ao * stride_ao, nao, dsl,
+                                                tau, asym);
   return cudaGetLastError();
 }
 
-// Pairing, union lists, work list and phi digit tiles of one grid batch whose
-// active lists (lists, counts) are built: pairs from q.pair0 (at most nbg of
-// them), chunks from q.chunk0, items appended at *q.total.
+// Pairing, union lists, work list and phi digit tiles of one grid batch:
+// pairs from q.pair0 (at most nbg of them), chunks from q.chunk0, items
+// appended at *q.total.
 cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream) {
   const int nblk = (q.ngrid + q.blk - 1) / q.blk;
   const int gsub = (q.blk + HT - 1) / HT;
@@ -1379,19 +1386,21 @@ cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream) {
   const size_t hist = size_t(max_kc + 2) * sizeof(int);
   pair_build<<<1, 1024, hist, stream>>>(q.ucount, q.npairs, q.pair0, q.nset, q.batch, tn, max_kc,
                                         q.chunk0, q.cbase, q.items, q.total, q.chunks_end);
-  // one CTA per pair (nbg bounds the pairs)
-  auto launch_phi = [&](auto kern, int nsl) -> cudaError_t {
-    const size_t smem = size_t(kPhiChunks) * nsl * 8 * (PT + 4) * sizeof(uint32_t);
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(smem));
-    if (e != cudaSuccess) return e;
-    kern<<<nbg, kPhiThreads, smem, stream>>>(q.ao_rhs, q.stride_grid, q.pairs, q.npairs, q.pair0,
-                                             q.ulist, q.uflag, q.ucount, q.cbase, q.nao, q.ngrid,
-                                             q.blk, gsub, q.sigma, q.phisl);
-    return cudaSuccess;
-  };
-  const cudaError_t err = q.nsl == 6 ? launch_phi(pair_phi<6>, 6) : launch_phi(pair_phi<7>, 7);
+  cudaError_t err = cudaMemsetAsync(q.pmax, 0, size_t(q.ngrid) * sizeof(unsigned long long),
+                                    stream);
   if (err != cudaSuccess) return err;
+  pair_phi_max<<<dim3(nbg, (q.nao + 31) / 32), 256, 0, stream>>>(
+      q.ao_rhs, q.stride_grid, q.pairs, q.npairs, q.pair0, q.ulist, q.uflag, q.ucount, q.nao,
+      q.ngrid, q.blk, gsub, q.pmax);
+  const dim3 tg(nbg, max_kc);
+  if (q.nsl == 6)
+    pair_phi_tiles<6><<<tg, 256, 0, stream>>>(q.ao_rhs, q.stride_grid, q.pmax, q.pairs, q.npairs,
+                                              q.pair0, q.ulist, q.uflag, q.ucount, q.cbase, q.nao,
+                                              q.ngrid, q.blk, gsub, q.sigma, q.phisl);
+  else
+    pair_phi_tiles<7><<<tg, 256, 0, stream>>>(q.ao_rhs, q.stride_grid, q.pmax, q.pairs, q.npairs,
+                                              q.pair0, q.ulist, q.uflag, q.ucount, q.cbase, q.nao,
+                                              q.ngrid, q.blk, gsub, q.sigma, q.phisl);
   return cudaGetLastError();
 }
 
@@ -1441,6 +1450,7 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   q.total = static_cast<int*>(at(L.total));
   q.chunks_end = q.total + 2;
   q.sigma = static_cast<int*>(at(L.sigma));
+  q.pmax = static_cast<unsigned long long*>(at(L.pmax));
   q.phisl = static_cast<uint8_t*>(at(L.phisl));
   uint2* dsl = static_cast<uint2*>(at(L.dsl));
   int* tau = static_cast<int*>(at(L.tau));
