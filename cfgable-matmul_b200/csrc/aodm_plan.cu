@@ -504,7 +504,8 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
     q.batch = int(i);
     q.pair0 = pair0;
     q.chunk0 = chunk0;
-    q.pmax = static_cast<unsigned long long*>(at(o_pmax));
+    q.lists = d_lists + list_off[i];
+    q.counts = d_counts + cnt_off[i];
     q.bits = static_cast<uint32_t*>(at(o_bits));
     q.cnt = static_cast<int*>(at(o_cnt));
     q.key = static_cast<unsigned long long*>(at(o_key));
@@ -524,6 +525,7 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
     q.total = d_total;
     q.chunks_end = d_total + 2;
     q.sigma = static_cast<int*>(at(o_sigma)) + sg_off[i];
+    q.pmax = static_cast<unsigned long long*>(at(o_pmax));
     q.phisl = static_cast<uint8_t*>(at(o_phisl));
     err = cfgmm::split_pair_prepare_batch(q, s);
     int got[2] = {0, 0};

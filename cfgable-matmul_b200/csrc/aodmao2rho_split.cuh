@@ -120,6 +120,8 @@ struct PairPrep {
   const double* ao_rhs;
   size_t stride_grid;
   int nao, ngrid, blk, nset, nsl, batch, pair0, chunk0;
+  const int* lists;       // [nblk][nao] active AOs of each block, built
+  const int* counts;      // [nblk]
   uint32_t* bits;         // scratch [nbg][ceil(nao/32)]
   int* cnt;               // scratch [nbg]
   unsigned long long* key;  // scratch [nbg]

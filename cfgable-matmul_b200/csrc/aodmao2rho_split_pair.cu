@@ -41,8 +41,7 @@
 //   pair_union    per pair: the union list U and per-AO membership flags
 //   pair_build    one CTA: chunk offsets and the work list (pair, row tile,
 //                 DM), heaviest items first
-//   pair_phi_max, pair_phi_tiles  point scales (max |phi| over the union
-//                 AOs active in each point's block) and the phi digit tiles of
+//   pair_phi_max, pair_phi_tiles  point scales and the phi digit tiles of
 //                 every (pair, chunk of 32 union AOs): NSL planes of 128 rows
 //                 (points) x 32 bytes in the UMMA 32-byte-swizzled K-major
 //                 layout, so one bulk copy moves a chunk
@@ -556,56 +555,40 @@ pair_build(const int* __restrict__ ucount, const int* __restrict__ npairs_d, int
   }
 }
 
-// pmax[g] = max |phi[u][g]| over the union AOs active in g's block (+Inf for
-// Inf or NaN); CTA (pair, slab of 32 union positions); pmax starts at 0.
+// pmax[g] = max |phi[u][g]| over the active AOs of g's block (+Inf for Inf or
+// NaN); CTA (block tile, slab of 64 active AOs); pmax starts at 0.
 __global__ void __launch_bounds__(256)
-pair_phi_max(const double* __restrict__ ao, size_t stride_grid, const int4* __restrict__ pairs,
-             const int* __restrict__ npairs, int pair0, const int* __restrict__ ulist,
-             const uint8_t* __restrict__ uflag, const int* __restrict__ ucount, int nao,
-             int ngrid, int blk, int gsub, unsigned long long* __restrict__ pmax) {
-  const int pl = blockIdx.x, slab = blockIdx.y;
-  if (pl >= npairs[0]) return;
-  const int pi = pair0 + pl;
-  const int nu = ucount[pi];
-  const int k0 = slab * 32;
-  if (k0 >= nu) return;
-  const int4 pr = pairs[pi];
-  const int* U = ulist + size_t(pi) * nao;
-  const uint8_t* F = uflag + size_t(pi) * nao;
-  const int r = threadIdx.x & (PT - 1), kq = threadIdx.x >> 7;  // point row, half of the slab
-  const int h = r >> 6;
-  const int tile = h ? pr.y : pr.x;
-  int g = -1;
-  if (tile >= 0) {
-    int g0, gend;
-    tile_points(tile, blk, gsub, ngrid, &g0, &gend);
-    if (g0 + (r & (HT - 1)) < gend) g = g0 + (r & (HT - 1));
-  }
-  __shared__ double red[2][PT];
+pair_phi_max(const double* __restrict__ ao, size_t stride_grid, const int* __restrict__ lists,
+             const int* __restrict__ counts, int nao, int ngrid, int blk, int gsub,
+             unsigned long long* __restrict__ pmax) {
+  const int bg = blockIdx.x, slab = blockIdx.y;
+  const int b = bg / gsub;
+  const int nb = counts[b];
+  const int i0 = slab * 64;
+  if (i0 >= nb) return;
+  int g0, gend;
+  tile_points(bg, blk, gsub, ngrid, &g0, &gend);
+  const int* I = lists + size_t(b) * nao;
+  const int gr = threadIdx.x & (HT - 1), rg = threadIdx.x >> 6;
+  const int g = g0 + gr;
+  __shared__ double red[4][HT];
   double mx = 0.0;
-  if (g >= 0) {
+  if (g < gend) {
     bool bad = false;
-    const int kend = min(nu, k0 + 32);
-    double a[16];
-#pragma unroll
-    for (int t = 0; t < 16; ++t) {  // every load in flight at once
-      const int k = k0 + kq + 2 * t;
-      a[t] = k < kend && ((__ldg(F + k) >> h) & 1u)
-                 ? fabs(ao[size_t(__ldg(U + k)) * stride_grid + g])
-                 : 0.0;
-    }
-#pragma unroll
-    for (int t = 0; t < 16; ++t) {
-      bad |= !(a[t] <= 1.7976931348623157e308);
-      mx = fmax(mx, a[t]);
+    const int iend = min(nb, i0 + 64);
+    for (int i = i0 + rg; i < iend; i += 4) {
+      const double a = fabs(ao[size_t(__ldg(I + i)) * stride_grid + g]);
+      bad |= !(a <= 1.7976931348623157e308);
+      mx = fmax(mx, a);
     }
     if (bad) mx = __longlong_as_double(0x7ff0000000000000LL);
   }
-  red[kq][r] = mx;
+  red[rg][gr] = mx;
   __syncthreads();
-  if (threadIdx.x < PT && g >= 0)
-    atomicMax(pmax + g, static_cast<unsigned long long>(
-                            __double_as_longlong(fmax(red[0][r], red[1][r]))));
+  if (threadIdx.x < HT && g < gend) {
+    const double m = fmax(fmax(red[0][gr], red[1][gr]), fmax(red[2][gr], red[3][gr]));
+    atomicMax(pmax + g, static_cast<unsigned long long>(__double_as_longlong(m)));
+  }
 }
 
 // The phi digit tiles of chunk c of pair pi: NSL planes of 128 rows (points:
@@ -632,33 +615,32 @@ pair_phi_tiles(const double* __restrict__ ao, size_t stride_grid,
   const int* U = ulist + size_t(pi) * nao;
   const uint8_t* F = uflag + size_t(pi) * nao;
   {
-    const int r = threadIdx.x & (PT - 1), hq = threadIdx.x >> 7;  // point row, half of the quads
-    const int h = r >> 6;
+    const int v = threadIdx.x;
+    const int r = v & (PT - 1), hq = v >> 7;  // point row, half of the quads
+    const int h = r >> 6, j = r & (HT - 1);
     const int tile = h ? pr.y : pr.x;
     int g = -1;
     if (tile >= 0) {
       int g0, gend;
       tile_points(tile, blk, gsub, ngrid, &g0, &gend);
-      if (g0 + (r & (HT - 1)) < gend) g = g0 + (r & (HT - 1));
+      if (g0 + j < gend) g = g0 + j;
     }
     const int e = g >= 0 ? exp_for(__longlong_as_double(static_cast<long long>(pmax[g]))) : 0;
     if (c == 0 && hq == 0 && g >= 0) sigma[g] = e;
-    uint2 w[4][4];  // every load in flight at once
-#pragma unroll
-    for (int qq = 0; qq < 4; ++qq)
-#pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        const int k = c * TK + (hq * 4 + qq) * 4 + t;
-        const bool on = g >= 0 && k < nu && e != kBadExp && ((__ldg(F + k) >> h) & 1u);
-        w[qq][t] = on ? digits_of<NSL>(ao[size_t(__ldg(U + k)) * stride_grid + g], e)
-                      : make_uint2(0u, 0u);
-      }
 #pragma unroll
     for (int qq = 0; qq < 4; ++qq) {
       const int q = hq * 4 + qq;
+      uint2 w[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int k = c * TK + q * 4 + t;
+        bool on = g >= 0 && k < nu && e != kBadExp;
+        if (on) on = ((F[k] >> h) & 1u) != 0;
+        w[t] = on ? digits_of<NSL>(ao[size_t(U[k]) * stride_grid + g], e) : make_uint2(0u, 0u);
+      }
       uint32_t o[8];
-      transpose4(w[qq][0].x, w[qq][1].x, w[qq][2].x, w[qq][3].x, o[0], o[1], o[2], o[3]);
-      transpose4(w[qq][0].y, w[qq][1].y, w[qq][2].y, w[qq][3].y, o[4], o[5], o[6], o[7]);
+      transpose4(w[0].x, w[1].x, w[2].x, w[3].x, o[0], o[1], o[2], o[3]);
+      transpose4(w[0].y, w[1].y, w[2].y, w[3].y, o[4], o[5], o[6], o[7]);
 #pragma unroll
       for (int pl2 = 0; pl2 < NSL; ++pl2) stage[pl2][q][r] = o[pl2];
     }
@@ -667,10 +649,9 @@ pair_phi_tiles(const double* __restrict__ ao, size_t stride_grid,
   uint8_t* tile0 = phisl + (size_t(cbase[pi]) + c) * C::A_STAGE;
   for (int v = threadIdx.x; v < NSL * PT * 2; v += 256) {
     const int hh = v & 1, r = (v >> 1) & (PT - 1), j = v >> 8;
-    const uint4 wv = make_uint4(stage[j][4 * hh][r], stage[j][4 * hh + 1][r],
-                                stage[j][4 * hh + 2][r], stage[j][4 * hh + 3][r]);
-    *reinterpret_cast<uint4*>(tile0 + j * C::A_SLICE + tc::sw32_offset(uint32_t(r), uint32_t(hh))) =
-        wv;
+    const uint4 w = make_uint4(stage[j][4 * hh][r], stage[j][4 * hh + 1][r],
+                               stage[j][4 * hh + 2][r], stage[j][4 * hh + 3][r]);
+    *reinterpret_cast<uint4*>(tile0 + j * C::A_SLICE + tc::sw32_offset(uint32_t(r), uint32_t(hh))) = w;
   }
 }
 
@@ -1262,7 +1243,7 @@ cudaError_t launch_pair_main_t(int nsm, const PairArgs& a, cudaStream_t stream, 
 size_t a256(size_t v) { return (v + 255) / 256 * 256; }
 
 struct Layout {
-  size_t bits, cnt, key, order, cand, ncand, partner, pos, choice, pairs, npairs,
+  size_t lists, counts, bits, cnt, key, order, cand, ncand, partner, pos, choice, pairs, npairs,
       ulist, uflag, ucount, cbase, items, total, dsl, tau, sigma, pmax, phisl, partial, bytes;
 };
 
@@ -1276,7 +1257,9 @@ Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk, int nsl) {
   const size_t nwords = (nao + 31) / 32;
   const size_t a_stage = size_t(nsl) * PT * TK;
   Layout L;
-  L.bits = 0;
+  L.lists = 0;
+  L.counts = L.lists + a256(nblk * nao * sizeof(int));
+  L.bits = L.counts + a256(nblk * sizeof(int));
   L.cnt = L.bits + a256(nbg * nwords * sizeof(uint32_t));
   L.key = L.cnt + a256(nbg * sizeof(int));
   L.order = L.key + a256(nbg * sizeof(unsigned long long));
@@ -1354,9 +1337,9 @@ cudaError_t split_pair_prepare_d(const double* dms, size_t stride_ao, int nao, i
   return cudaGetLastError();
 }
 
-// Pairing, union lists, work list and phi digit tiles of one grid batch:
-// pairs from q.pair0 (at most nbg of them), chunks from q.chunk0, items
-// appended at *q.total.
+// Pairing, union lists, work list and phi digit tiles of one grid batch whose
+// active lists (lists, counts) are built: pairs from q.pair0 (at most nbg of
+// them), chunks from q.chunk0, items appended at *q.total.
 cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream) {
   const int nblk = (q.ngrid + q.blk - 1) / q.blk;
   const int gsub = (q.blk + HT - 1) / HT;
@@ -1389,9 +1372,8 @@ cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream) {
   cudaError_t err = cudaMemsetAsync(q.pmax, 0, size_t(q.ngrid) * sizeof(unsigned long long),
                                     stream);
   if (err != cudaSuccess) return err;
-  pair_phi_max<<<dim3(nbg, (q.nao + 31) / 32), 256, 0, stream>>>(
-      q.ao_rhs, q.stride_grid, q.pairs, q.npairs, q.pair0, q.ulist, q.uflag, q.ucount, q.nao,
-      q.ngrid, q.blk, gsub, q.pmax);
+  pair_phi_max<<<dim3(nbg, (q.nao + 63) / 64), 256, 0, stream>>>(
+      q.ao_rhs, q.stride_grid, q.lists, q.counts, q.nao, q.ngrid, q.blk, gsub, q.pmax);
   const dim3 tg(nbg, max_kc);
   if (q.nsl == 6)
     pair_phi_tiles<6><<<tg, 256, 0, stream>>>(q.ao_rhs, q.stride_grid, q.pmax, q.pairs, q.npairs,
@@ -1418,6 +1400,8 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   const Layout L = layout(nao, ngrid, nset, blk, nsl);
   char* ws = static_cast<char*>(workspace);
   auto at = [&](size_t off) { return static_cast<void*>(ws + off); };
+  int* lists = static_cast<int*>(at(L.lists));
+  int* counts = static_cast<int*>(at(L.counts));
   PairPrep q{};
   q.tab = tab;
   q.ldtab = ldtab;
@@ -1431,6 +1415,8 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   q.batch = 0;
   q.pair0 = 0;
   q.chunk0 = 0;
+  q.lists = lists;
+  q.counts = counts;
   q.bits = static_cast<uint32_t*>(at(L.bits));
   q.cnt = static_cast<int*>(at(L.cnt));
   q.key = static_cast<unsigned long long*>(at(L.key));
@@ -1460,7 +1446,7 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   cudaError_t err = cudaMemsetAsync(q.total, 0, 4 * sizeof(int), stream);
   if (err != cudaSuccess) return err;
   // The D chain (symmetry check, D digits) runs on a side stream beside the
-  // phi chain (pairing, unions, work list, phi tiles); the side
+  // phi chain (block lists, pairing, unions, work list, phi tiles); the side
   // stream joins back before the main kernel.
   SideScope side(side_stream(), stream);
   if ((err = side.fork()) != cudaSuccess) return err;
@@ -1468,6 +1454,9 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   if (asym && (err = aodm_launch_sym_check(dms, stride_ao, nao, nset, asym, sd)) != cudaSuccess)
     return err;
   if ((err = split_pair_prepare_d(dms, stride_ao, nao, nset, nsl, dsl, tau, sd, asym)) !=
+      cudaSuccess)
+    return err;
+  if ((err = aodm_block_lists_launch(tab, ldtab, nao, nblk, lists, counts, stream)) !=
       cudaSuccess)
     return err;
   if ((err = split_pair_prepare_batch(q, stream)) != cudaSuccess) return err;
