@@ -688,7 +688,9 @@ def run_ours(args, ranks: Ranks):
         return ranks.max(ev[0].elapsed_time(ev[-1]))
 
     aflops = p.flops()
-    split_form = "pair" if os.environ.get("CFGMM_SPLIT_FORM", "").startswith("p") else "row"
+    form_env = os.environ.get("CFGMM_SPLIT_FORM", "")
+    split_form = ("pair" if form_env.startswith("p") else "row" if form_env.startswith("r")
+                  else "pair" if p.nao >= 1024 and p.ngrid >= 8192 else "row")
     split_digits = int(os.environ.get("CFGMM_SPLIT_DIGITS", "7")) if split_form == "pair" else 7
     # the FP64 kernel contracts half of each symmetric D (checked on the device)
     sym = bool(np.array_equal(p.dms, p.dms.transpose(0, 2, 1))) and \

@@ -779,8 +779,10 @@ int cfgmm_aodm_plan_create(cfgmm_aodm_plan** out, const cfgmm_aodm_batch* batche
       plan->flops += double(batches[i].nset) * (2.0 * nb * nb + 2.0 * nb) * w;
     }
   if (precision == CFGMM_PREC_OZAKI_INT8) {
+    size_t points = 0;
+    for (size_t i = 0; i < nbatch; ++i) points += batches[i].ngrid;
     const int rc =
-        cfgmm::split_pair_form()
+        cfgmm::split_pair_form(nao, points)
             ? build_split_pair(plan, batches, nbatch, dms, stride_ao, nao, nset_max, blksize,
                                flags, d_lists, d_counts, list_off, cnt_off, nblk, counts, s)
             : build_split(plan, batches, nbatch, dms, stride_ao, nao, nset_max, blksize, flags,

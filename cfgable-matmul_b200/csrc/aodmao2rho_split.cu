@@ -764,9 +764,12 @@ Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk) {
 // compacted rows per item) unless CFGMM_SPLIT_FORM=pair selects the pair form
 // (two alike block tiles per item, aodmao2rho_split_pair.cu).  Read on every
 // call; the workspace covers both.
-bool split_pair_form() {
+bool split_pair_form(size_t nao, size_t points) {
   const char* e = std::getenv("CFGMM_SPLIT_FORM");
-  return e && e[0] == 'p';
+  if (e && e[0] == 'p') return true;
+  if (e && e[0] == 'r') return false;
+  // the pair form's pairing and tile building pay off on large problems
+  return nao >= kPairMinAos && points >= kPairMinPoints;
 }
 
 size_t aodmao2rho_split_workspace(size_t nao, size_t ngrid, size_t nset, size_t blk) {
@@ -783,7 +786,7 @@ cudaError_t aodmao2rho_split(double* rhos, const double* dms, const double* ao_l
                              int ngrid, int nset, const uint8_t* tab, size_t ldtab, int blk,
                              void* workspace, cudaStream_t stream) {
   if (nao <= 0 || ngrid <= 0 || nset <= 0) return cudaSuccess;
-  if (split_pair_form())
+  if (split_pair_form(size_t(nao), size_t(ngrid)))
     return aodmao2rho_split_pair(rhos, dms, ao_lhs, ao_rhs, stride_ao, stride_grid, nao, ngrid,
                                  nset, tab, ldtab, blk, split_pair_digits(), workspace, stream);
   const int nblk = (ngrid + blk - 1) / blk;

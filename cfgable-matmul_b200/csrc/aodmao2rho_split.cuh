@@ -4,6 +4,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "side_stream.cuh"
+
 namespace cfgmm {
 
 // One grid batch of the split contraction (device pointers).
@@ -149,7 +151,10 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
                                   int nao, int ngrid, int nset, const uint8_t* tab, size_t ldtab,
                                   int blk, int nsl, void* workspace, cudaStream_t stream,
                                   int inject = 0, unsigned long long wait_ns = 0);
-cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream);
+// side: when given, the point scales run on its stream (forked after the
+// caller's block lists, joined before the phi tiles)
+cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream,
+                                     SideScope* side = nullptr);
 cudaError_t split_pair_prepare_d(const double* dms, size_t stride_ao, int nao, int nset, int nsl,
                                  uint2* dsl, int* tau, cudaStream_t stream, const int* asym);
 int split_pair_stages();  // the pair kernel's pipeline depth
@@ -158,7 +163,12 @@ cudaError_t split_pair_launch_main(const PairArgs& a, int nsl, cudaStream_t stre
                                    bool attrs_only = false, int stages = 0);
 cudaError_t split_pair_launch_reduce(const PairArgs& a, int nsl, const int* npairs, int pair0,
                                      int max_pairs, cudaStream_t stream);
-bool split_pair_form();            // single calls and plans run the pair form (CFGMM_SPLIT_FORM)
+// Whether a single call (points = ngrid) or a plan (points = all batches'
+// points) runs the pair form: CFGMM_SPLIT_FORM=pair / =row, else the pair
+// form from kPairMinAos AOs and kPairMinPoints points on (below that the
+// pairing and tile building cost more than the pairs save).
+constexpr size_t kPairMinAos = 1024, kPairMinPoints = 8192;
+bool split_pair_form(size_t nao, size_t points);
 int split_pair_row_tile(int nsl);  // D rows per item (the MMA N): 80 (6 digits), 64 (7)
 int split_pair_digits();           // digit count (CFGMM_SPLIT_DIGITS, default 7), read per call
 cudaError_t aodmao2rho_split_pair_reset_error(cudaStream_t stream);

@@ -1340,7 +1340,7 @@ cudaError_t split_pair_prepare_d(const double* dms, size_t stride_ao, int nao, i
 // Pairing, union lists, work list and phi digit tiles of one grid batch whose
 // active lists (lists, counts) are built: pairs from q.pair0 (at most nbg of
 // them), chunks from q.chunk0, items appended at *q.total.
-cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream) {
+cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream, SideScope* side) {
   const int nblk = (q.ngrid + q.blk - 1) / q.blk;
   const int gsub = (q.blk + HT - 1) / HT;
   const int nbg = nblk * gsub;
@@ -1352,6 +1352,16 @@ cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream) {
   static const cudaError_t sort_attr = cudaFuncSetAttribute(
       pair_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sort_smem));
   if (sort_attr != cudaSuccess) return sort_attr;
+  // the point scales need only the block lists: on the side stream (when
+  // given) beside the pairing chain
+  cudaError_t err = side ? side->fork() : cudaSuccess;
+  if (err != cudaSuccess) return err;
+  const cudaStream_t ss = side ? side->stream() : stream;
+  if ((err = cudaMemsetAsync(q.pmax, 0, size_t(q.ngrid) * sizeof(unsigned long long), ss)) !=
+      cudaSuccess)
+    return err;
+  pair_phi_max<<<dim3(nbg, (q.nao + 63) / 64), 256, 0, ss>>>(
+      q.ao_rhs, q.stride_grid, q.lists, q.counts, q.nao, q.ngrid, q.blk, gsub, q.pmax);
   pair_sig<<<nbg, 256, 0, stream>>>(q.tab, q.ldtab, q.nao, nbg, gsub, nwords, q.bits, q.cnt,
                                     q.key);
   pair_sort<<<1, 1024, sort_smem, stream>>>(q.key, nbg, q.order);
@@ -1369,11 +1379,7 @@ cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream) {
   const size_t hist = size_t(max_kc + 2) * sizeof(int);
   pair_build<<<1, 1024, hist, stream>>>(q.ucount, q.npairs, q.pair0, q.nset, q.batch, tn, max_kc,
                                         q.chunk0, q.cbase, q.items, q.total, q.chunks_end);
-  cudaError_t err = cudaMemsetAsync(q.pmax, 0, size_t(q.ngrid) * sizeof(unsigned long long),
-                                    stream);
-  if (err != cudaSuccess) return err;
-  pair_phi_max<<<dim3(nbg, (q.nao + 63) / 64), 256, 0, stream>>>(
-      q.ao_rhs, q.stride_grid, q.lists, q.counts, q.nao, q.ngrid, q.blk, gsub, q.pmax);
+  if (side && (err = side->join()) != cudaSuccess) return err;
   const dim3 tg(nbg, max_kc);
   if (q.nsl == 6)
     pair_phi_tiles<6><<<tg, 256, 0, stream>>>(q.ao_rhs, q.stride_grid, q.pmax, q.pairs, q.npairs,
@@ -1445,9 +1451,9 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   int* asym = aodm_sym_enabled() && ao_lhs == ao_rhs ? q.total + 1 : nullptr;
   cudaError_t err = cudaMemsetAsync(q.total, 0, 4 * sizeof(int), stream);
   if (err != cudaSuccess) return err;
-  // The D chain (symmetry check, D digits) runs on a side stream beside the
-  // phi chain (block lists, pairing, unions, work list, phi tiles); the side
-  // stream joins back before the main kernel.
+  // The D chain (symmetry check, D digits) and then the point scales run on
+  // a side stream beside the phi chain (block lists, pairing, unions, work
+  // list); the side stream joins back before the phi tiles.
   SideScope side(side_stream(), stream);
   if ((err = side.fork()) != cudaSuccess) return err;
   const cudaStream_t sd = side.stream();
@@ -1459,7 +1465,7 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   if ((err = aodm_block_lists_launch(tab, ldtab, nao, nblk, lists, counts, stream)) !=
       cudaSuccess)
     return err;
-  if ((err = split_pair_prepare_batch(q, stream)) != cudaSuccess) return err;
+  if ((err = split_pair_prepare_batch(q, stream, &side)) != cudaSuccess) return err;
   if ((err = side.join()) != cudaSuccess) return err;
 
   PairArgs a{};

@@ -162,8 +162,9 @@ int cfgmm_device_check(void);
 
 /* No counterpart in the reference: the test hook of the device-side failure
  * detection.  Arms the calling thread's NEXT masked AO-DM-AO contraction in
- * `precision` (CFGMM_PREC_FP64: the pipelined FP64 kernel; OZAKI_INT8 with
- * CFGMM_SPLIT_FORM=pair: the split pair kernel) so that one producer never
+ * `precision` (CFGMM_PREC_FP64: the pipelined FP64 kernel; OZAKI_INT8: the
+ * split pair kernel -- the form of contractions from 1024 AOs and 8192 points
+ * on, or of every one under CFGMM_SPLIT_FORM=pair) so that one producer never
  * publishes the first pipeline stage and every wait in the kernel gives up
  * after `wait_ms` (1..2000) milliseconds instead of 2 s.  The waiting warp
  * records a timeout, every warp leaves, copies in flight land, tensor memory
