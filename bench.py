@@ -506,7 +506,7 @@ def serving_section(args, cm, wl):
 
     def one_pass(precision, arrivals, device_dm=False):
         import torch
-        srv = cm.Server(budget, nslots=4, precision=precision)
+        srv = cm.Server(budget, nslots=args.serve_slots, precision=precision)
         t_start = time.perf_counter()
 
         def client(k):
@@ -548,7 +548,7 @@ def serving_section(args, cm, wl):
     res = {"workload": f"{len(mols)} molecules x 10 SCF-like requests, nao log-uniform "
                        "[300, 4000], ngrid log-uniform [8192, 65536], density 0.3, 1-3 DMs, "
                        "phi evaluated on the device",
-           "budget_gb": args.serve_budget_gb, "slots": 4,
+           "budget_gb": args.serve_budget_gb, "slots": args.serve_slots,
            "molecules": [[m[0].nao, len(m[1]), m[2]] for m in mols],
            "latency": f"Poisson arrivals, mean gap {args.serve_gap_ms} ms",
            "throughput": "every molecule arrives at t = 0 (saturated), D and rho in host memory",
@@ -946,6 +946,7 @@ def main():
     ap.add_argument("--serve-molecules", type=int, default=24)
     ap.add_argument("--serve-gap-ms", type=float, default=40.0)
     ap.add_argument("--serve-budget-gb", type=float, default=40.0)
+    ap.add_argument("--serve-slots", type=int, default=8, help="server slots (requests in flight)")
     args = ap.parse_args()
     if args.profile:
         run_profile_case(args)

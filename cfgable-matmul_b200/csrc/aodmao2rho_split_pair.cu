@@ -87,6 +87,7 @@ constexpr int kBadExp = INT_MAX;  // scale of a row / point holding Inf or NaN
 constexpr int kWin = 32;          // pairing candidates on each side in key order
 constexpr int kSortMax = 4096;    // tiles sorted in shared memory (more: caller's order)
 constexpr int kRounds = 8;        // mutual-best matching rounds
+constexpr int kMatchCandMax = 600;  // tiles whose candidate lists the matching stages in shared memory
 constexpr int kRing = 4;          // work items in flight between the kernel's roles
 constexpr int kAhead = 2;         // items drawn ahead of the one being loaded (< kRing)
 static_assert(kStages >= NG, "a group's parity wait needs at least NG stages");
@@ -360,12 +361,20 @@ pair_match(const int* __restrict__ order, const int* __restrict__ cand,
            const int* __restrict__ ncand, const int* __restrict__ cnt, int nbg, int batch,
            int* __restrict__ partner_g, int* __restrict__ pos_g, int* __restrict__ choice_g,
            int4* __restrict__ pairs, int* __restrict__ npairs) {
-  extern __shared__ int match_s[];  // 3 * kSortMax ints when nbg <= kSortMax
+  // 3 * kSortMax ints when nbg <= kSortMax, then the candidate lists when
+  // nbg <= kMatchCandMax
+  extern __shared__ int match_s[];
   const bool in_smem = nbg <= kSortMax;
   int* partner = in_smem ? match_s : partner_g;
   int* pos = in_smem ? match_s + kSortMax : pos_g;
   int* choice = in_smem ? match_s + 2 * kSortMax : choice_g;
   const int tid = threadIdx.x;
+  const int* cl = cand;  // candidate lists, staged in shared memory when they fit
+  if (nbg <= kMatchCandMax) {
+    int* cs = match_s + 3 * kSortMax;
+    for (int i = tid; i < nbg * 2 * kWin; i += 1024) cs[i] = cand[i];
+    cl = cs;
+  }
   __shared__ int changed;
   __shared__ int warp_tot[32];
   __shared__ int base_s;
@@ -385,7 +394,7 @@ pair_match(const int* __restrict__ order, const int* __restrict__ cand,
       if (partner[t] == -2) {
         const int n = ncand[q];
         for (int i = 0; i < n; ++i) {
-          const int c = cand[size_t(q) * 2 * kWin + i];
+          const int c = cl[size_t(q) * 2 * kWin + i];
           if (partner[c] == -2) {
             pick = c;
             break;
@@ -1367,10 +1376,13 @@ cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream, Sid
   pair_sort<<<1, 1024, sort_smem, stream>>>(q.key, nbg, q.order);
   pair_scores<<<nbg, 2 * kWin, 0, stream>>>(q.bits, q.cnt, q.order, nbg, nwords, q.cand,
                                             q.ncand);
-  constexpr size_t match_smem = size_t(3) * kSortMax * sizeof(int);
+  constexpr size_t match_base = size_t(3) * kSortMax * sizeof(int);
+  constexpr size_t match_cands = size_t(kMatchCandMax) * 2 * kWin * sizeof(int);
   static const cudaError_t match_attr = cudaFuncSetAttribute(
-      pair_match, cudaFuncAttributeMaxDynamicSharedMemorySize, int(match_smem));
+      pair_match, cudaFuncAttributeMaxDynamicSharedMemorySize, int(match_base + match_cands));
   if (match_attr != cudaSuccess) return match_attr;
+  const size_t match_smem =
+      match_base + (nbg <= kMatchCandMax ? size_t(nbg) * 2 * kWin * sizeof(int) : 0);
   pair_match<<<1, 1024, match_smem, stream>>>(q.order, q.cand, q.ncand, q.cnt, nbg, q.batch,
                                               q.partner, q.pos, q.choice, q.pairs + q.pair0,
                                               q.npairs);
