@@ -404,8 +404,10 @@ int cfgmm_server_submit_dev(cfgmm_server* server, uint64_t molecule, const doubl
 int cfgmm_server_wait(cfgmm_server* server, uint64_t ticket, double timeout_s,
                       cfgmm_request_stats* stats);
 /* JSON: completed/failed counts, molecules resident, evictions, budget, used
- * and peak bytes, flops of the completed requests, and p50/p99 latency
- * (total, queue, device) in ms. */
+ * and peak bytes, flops of the completed requests, p50/p99 latency (total,
+ * queue, device) in ms, molecule load and plan build times, the sum of the
+ * requests' device spans (device_ms_total) and the most requests in flight at
+ * once (max_inflight). */
 const char* cfgmm_server_stats(cfgmm_server* server);
 
 #ifdef __cplusplus
