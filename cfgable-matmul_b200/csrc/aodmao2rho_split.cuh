@@ -151,10 +151,13 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
                                   int nao, int ngrid, int nset, const uint8_t* tab, size_t ldtab,
                                   int blk, int nsl, void* workspace, cudaStream_t stream,
                                   int inject = 0, unsigned long long wait_ns = 0);
-// side: when given, the point scales run on its stream (forked after the
-// caller's block lists, joined before the phi tiles)
-cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream,
-                                     SideScope* side = nullptr);
+// The preparation of one grid batch whose block lists are built: point scales
+// (from the block lists), pairing and work list (from the mask), phi tiles
+// (from both); prepare_batch runs the three in that order on one stream.
+cudaError_t split_pair_prepare_scales(const PairPrep& q, cudaStream_t stream);
+cudaError_t split_pair_prepare_pairs(const PairPrep& q, cudaStream_t stream);
+cudaError_t split_pair_prepare_tiles(const PairPrep& q, cudaStream_t stream);
+cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream);
 cudaError_t split_pair_prepare_d(const double* dms, size_t stride_ao, int nao, int nset, int nsl,
                                  uint2* dsl, int* tau, cudaStream_t stream, const int* asym);
 int split_pair_stages();  // the pair kernel's pipeline depth

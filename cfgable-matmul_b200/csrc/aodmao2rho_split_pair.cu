@@ -1349,59 +1349,86 @@ cudaError_t split_pair_prepare_d(const double* dms, size_t stride_ao, int nao, i
 // Pairing, union lists, work list and phi digit tiles of one grid batch whose
 // active lists (lists, counts) are built: pairs from q.pair0 (at most nbg of
 // them), chunks from q.chunk0, items appended at *q.total.
-cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream, SideScope* side) {
-  const int nblk = (q.ngrid + q.blk - 1) / q.blk;
-  const int gsub = (q.blk + HT - 1) / HT;
-  const int nbg = nblk * gsub;
-  const int nwords = (q.nao + 31) / 32;
-  const int tn = q.nsl == 6 ? Cfg<6>::TN : Cfg<7>::TN;
-  const int max_kc = (q.nao + TK - 1) / TK;
-  if (nbg <= 0) return cudaSuccess;
+namespace {
+
+struct BatchDims {
+  int nbg, gsub, nwords, tn, max_kc;
+};
+
+BatchDims batch_dims(const PairPrep& q) {
+  BatchDims d;
+  d.gsub = (q.blk + HT - 1) / HT;
+  d.nbg = ((q.ngrid + q.blk - 1) / q.blk) * d.gsub;
+  d.nwords = (q.nao + 31) / 32;
+  d.tn = q.nsl == 6 ? Cfg<6>::TN : Cfg<7>::TN;
+  d.max_kc = (q.nao + TK - 1) / TK;
+  return d;
+}
+
+}  // namespace
+
+cudaError_t split_pair_prepare_pairs(const PairPrep& q, cudaStream_t stream) {
+  const BatchDims d = batch_dims(q);
+  if (d.nbg <= 0) return cudaSuccess;
   constexpr size_t sort_smem = size_t(kSortMax) * (sizeof(unsigned long long) + sizeof(int));
   static const cudaError_t sort_attr = cudaFuncSetAttribute(
       pair_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sort_smem));
   if (sort_attr != cudaSuccess) return sort_attr;
-  // the point scales need only the block lists: on the side stream (when
-  // given) beside the pairing chain
-  cudaError_t err = side ? side->fork() : cudaSuccess;
-  if (err != cudaSuccess) return err;
-  const cudaStream_t ss = side ? side->stream() : stream;
-  if ((err = cudaMemsetAsync(q.pmax, 0, size_t(q.ngrid) * sizeof(unsigned long long), ss)) !=
-      cudaSuccess)
-    return err;
-  pair_phi_max<<<dim3(nbg, (q.nao + 63) / 64), 256, 0, ss>>>(
-      q.ao_rhs, q.stride_grid, q.lists, q.counts, q.nao, q.ngrid, q.blk, gsub, q.pmax);
-  pair_sig<<<nbg, 256, 0, stream>>>(q.tab, q.ldtab, q.nao, nbg, gsub, nwords, q.bits, q.cnt,
-                                    q.key);
-  pair_sort<<<1, 1024, sort_smem, stream>>>(q.key, nbg, q.order);
-  pair_scores<<<nbg, 2 * kWin, 0, stream>>>(q.bits, q.cnt, q.order, nbg, nwords, q.cand,
-                                            q.ncand);
+  pair_sig<<<d.nbg, 256, 0, stream>>>(q.tab, q.ldtab, q.nao, d.nbg, d.gsub, d.nwords, q.bits,
+                                      q.cnt, q.key);
+  pair_sort<<<1, 1024, sort_smem, stream>>>(q.key, d.nbg, q.order);
+  pair_scores<<<d.nbg, 2 * kWin, 0, stream>>>(q.bits, q.cnt, q.order, d.nbg, d.nwords, q.cand,
+                                              q.ncand);
   constexpr size_t match_base = size_t(3) * kSortMax * sizeof(int);
   constexpr size_t match_cands = size_t(kMatchCandMax) * 2 * kWin * sizeof(int);
   static const cudaError_t match_attr = cudaFuncSetAttribute(
       pair_match, cudaFuncAttributeMaxDynamicSharedMemorySize, int(match_base + match_cands));
   if (match_attr != cudaSuccess) return match_attr;
   const size_t match_smem =
-      match_base + (nbg <= kMatchCandMax ? size_t(nbg) * 2 * kWin * sizeof(int) : 0);
-  pair_match<<<1, 1024, match_smem, stream>>>(q.order, q.cand, q.ncand, q.cnt, nbg, q.batch,
+      match_base + (d.nbg <= kMatchCandMax ? size_t(d.nbg) * 2 * kWin * sizeof(int) : 0);
+  pair_match<<<1, 1024, match_smem, stream>>>(q.order, q.cand, q.ncand, q.cnt, d.nbg, q.batch,
                                               q.partner, q.pos, q.choice, q.pairs + q.pair0,
                                               q.npairs);
-  pair_union<<<nbg, 256, 0, stream>>>(q.tab, q.ldtab, q.nao, gsub, q.pairs, q.npairs, q.pair0,
-                                      q.ulist, q.uflag, q.ucount);
-  const size_t hist = size_t(max_kc + 2) * sizeof(int);
-  pair_build<<<1, 1024, hist, stream>>>(q.ucount, q.npairs, q.pair0, q.nset, q.batch, tn, max_kc,
-                                        q.chunk0, q.cbase, q.items, q.total, q.chunks_end);
-  if (side && (err = side->join()) != cudaSuccess) return err;
-  const dim3 tg(nbg, max_kc);
+  pair_union<<<d.nbg, 256, 0, stream>>>(q.tab, q.ldtab, q.nao, d.gsub, q.pairs, q.npairs, q.pair0,
+                                        q.ulist, q.uflag, q.ucount);
+  const size_t hist = size_t(d.max_kc + 2) * sizeof(int);
+  pair_build<<<1, 1024, hist, stream>>>(q.ucount, q.npairs, q.pair0, q.nset, q.batch, d.tn,
+                                        d.max_kc, q.chunk0, q.cbase, q.items, q.total,
+                                        q.chunks_end);
+  return cudaGetLastError();
+}
+
+cudaError_t split_pair_prepare_scales(const PairPrep& q, cudaStream_t stream) {
+  const BatchDims d = batch_dims(q);
+  if (d.nbg <= 0) return cudaSuccess;
+  cudaError_t err = cudaMemsetAsync(q.pmax, 0, size_t(q.ngrid) * sizeof(unsigned long long),
+                                    stream);
+  if (err != cudaSuccess) return err;
+  pair_phi_max<<<dim3(d.nbg, (q.nao + 63) / 64), 256, 0, stream>>>(
+      q.ao_rhs, q.stride_grid, q.lists, q.counts, q.nao, q.ngrid, q.blk, d.gsub, q.pmax);
+  return cudaGetLastError();
+}
+
+cudaError_t split_pair_prepare_tiles(const PairPrep& q, cudaStream_t stream) {
+  const BatchDims d = batch_dims(q);
+  if (d.nbg <= 0) return cudaSuccess;
+  const dim3 tg(d.nbg, d.max_kc);
   if (q.nsl == 6)
     pair_phi_tiles<6><<<tg, 256, 0, stream>>>(q.ao_rhs, q.stride_grid, q.pmax, q.pairs, q.npairs,
                                               q.pair0, q.ulist, q.uflag, q.ucount, q.cbase, q.nao,
-                                              q.ngrid, q.blk, gsub, q.sigma, q.phisl);
+                                              q.ngrid, q.blk, d.gsub, q.sigma, q.phisl);
   else
     pair_phi_tiles<7><<<tg, 256, 0, stream>>>(q.ao_rhs, q.stride_grid, q.pmax, q.pairs, q.npairs,
                                               q.pair0, q.ulist, q.uflag, q.ucount, q.cbase, q.nao,
-                                              q.ngrid, q.blk, gsub, q.sigma, q.phisl);
+                                              q.ngrid, q.blk, d.gsub, q.sigma, q.phisl);
   return cudaGetLastError();
+}
+
+cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream) {
+  cudaError_t err = split_pair_prepare_scales(q, stream);
+  if (err == cudaSuccess) err = split_pair_prepare_pairs(q, stream);
+  if (err == cudaSuccess) err = split_pair_prepare_tiles(q, stream);
+  return err;
 }
 
 cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double* ao_lhs,
@@ -1463,21 +1490,31 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   int* asym = aodm_sym_enabled() && ao_lhs == ao_rhs ? q.total + 1 : nullptr;
   cudaError_t err = cudaMemsetAsync(q.total, 0, 4 * sizeof(int), stream);
   if (err != cudaSuccess) return err;
-  // The D chain (symmetry check, D digits) and then the point scales run on
-  // a side stream beside the phi chain (block lists, pairing, unions, work
-  // list); the side stream joins back before the phi tiles.
-  SideScope side(side_stream(), stream);
+  // Two chains: the pairing chain (block lists, signatures, sort, scores,
+  // matching, unions, work list, then the phi tiles) on a high-priority side
+  // stream, so that its small kernels are not held back behind the CTAs of
+  // the D chain (symmetry check, D digits, then the point scales) on the
+  // caller's stream.  The point scales wait for the block lists, the phi
+  // tiles for the point scales; the side stream joins back before the main
+  // kernel.
+  SideScope side(side_stream(true), stream);
   if ((err = side.fork()) != cudaSuccess) return err;
-  const cudaStream_t sd = side.stream();
-  if (asym && (err = aodm_launch_sym_check(dms, stride_ao, nao, nset, asym, sd)) != cudaSuccess)
+  const cudaStream_t sp = side.stream();
+  if (asym && (err = aodm_launch_sym_check(dms, stride_ao, nao, nset, asym, stream)) !=
+                  cudaSuccess)
     return err;
-  if ((err = split_pair_prepare_d(dms, stride_ao, nao, nset, nsl, dsl, tau, sd, asym)) !=
+  if ((err = split_pair_prepare_d(dms, stride_ao, nao, nset, nsl, dsl, tau, stream, asym)) !=
       cudaSuccess)
     return err;
-  if ((err = aodm_block_lists_launch(tab, ldtab, nao, nblk, lists, counts, stream)) !=
-      cudaSuccess)
+  if ((err = aodm_block_lists_launch(tab, ldtab, nao, nblk, lists, counts, sp)) != cudaSuccess)
     return err;
-  if ((err = split_pair_prepare_batch(q, stream, &side)) != cudaSuccess) return err;
+  const SideStream* ss = side_stream(true);
+  const bool split_streams = sp != stream && ss;
+  if (split_streams && (err = side_join(ss, stream)) != cudaSuccess) return err;  // lists -> scales
+  if ((err = split_pair_prepare_scales(q, stream)) != cudaSuccess) return err;
+  if ((err = split_pair_prepare_pairs(q, sp)) != cudaSuccess) return err;
+  if (split_streams && (err = side_fork(ss, stream)) != cudaSuccess) return err;  // scales -> tiles
+  if ((err = split_pair_prepare_tiles(q, sp)) != cudaSuccess) return err;
   if ((err = side.join()) != cudaSuccess) return err;
 
   PairArgs a{};

@@ -572,16 +572,19 @@ cudaError_t prepare(const double* x, size_t ld, bool rows_contig, int rows, int 
 
 }  // namespace
 
-const SideStream* side_stream() {
+const SideStream* side_stream(bool high_priority) {
   constexpr int kMaxDevices = 64;
-  thread_local SideStream streams[kMaxDevices];
+  thread_local SideStream streams[kMaxDevices][2];
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
-  SideStream& st = streams[dev];
+  SideStream& st = streams[dev][high_priority ? 1 : 0];
   if (!st.join) {
     // made in place; a partial set (one creation failed) is kept, released at
     // thread exit, and completed by a later call
-    if (!st.s && cudaStreamCreateWithFlags(&st.s, cudaStreamNonBlocking) != cudaSuccess) {
+    int lo = 0, hi = 0;
+    if (high_priority && cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess) return nullptr;
+    if (!st.s && cudaStreamCreateWithPriority(&st.s, cudaStreamNonBlocking, high_priority ? hi : 0) !=
+                     cudaSuccess) {
       st.s = nullptr;
       return nullptr;
     }

@@ -27,8 +27,10 @@ struct SideStream {
 };
 
 // The calling thread's side stream on the current device, or nullptr when one
-// cannot be made (callers then stay on their own stream).
-const SideStream* side_stream();
+// cannot be made (callers then stay on their own stream).  high_priority: a
+// separate stream at the device's greatest priority, whose pending CTAs the
+// block scheduler serves before those of default-priority streams.
+const SideStream* side_stream(bool high_priority = false);
 
 // side->s waits for the work enqueued on `stream` so far.
 inline cudaError_t side_fork(const SideStream* side, cudaStream_t stream) {
