@@ -566,7 +566,8 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
   // partial row tiles: exact, from the unions
   std::vector<int> poff(size_t(P) + 1, 0);
   for (int q = 0; q < P; ++q) poff[q + 1] = poff[q] + (ucount[q] + tn - 1) / tn;
-  const size_t part_bytes = size_t(poff[P]) * nset_max * PT * sizeof(double);
+  const size_t part_bytes =
+      size_t(poff[P]) * nset_max * cfgmm::split_pair_partial_points() * sizeof(double);
   err = cudaMallocAsync(&plan->mem3, std::max<size_t>(part_bytes, 256), s);
   if (err != cudaSuccess) return cuda_fail(err, "cudaMalloc(split plan partials)");
   const int np_all = P;

@@ -161,6 +161,8 @@ cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream);
 cudaError_t split_pair_prepare_d(const double* dms, size_t stride_ao, int nao, int nset, int nsl,
                                  uint2* dsl, int* tau, cudaStream_t stream, const int* asym);
 int split_pair_stages();  // the pair kernel's pipeline depth
+// partial sums per (row tile, DM) of a pair: one per gather group and point
+int split_pair_partial_points();
 // stages: ignored (the pair form's pipeline depth is fixed: split_pair_stages())
 cudaError_t split_pair_launch_main(const PairArgs& a, int nsl, cudaStream_t stream,
                                    bool attrs_only = false, int stages = 0);

@@ -58,8 +58,8 @@
 //                 (lane = point), rebuilds X in FP64, weights it with phi_lhs
 //                 and sums over the row's AOs -- no cross-lane reduction; X
 //                 never leaves the SM.
-//   pair_reduce   adds the row tiles' partial sums of each point in a fixed
-//                 order (deterministic).
+//   pair_reduce   adds the partial sums of each point (per row tile and
+//                 gather group) in a fixed order (deterministic).
 // Every mbarrier wait is bounded (tcgen05.cuh).
 #include <cuda_runtime.h>
 
@@ -104,11 +104,11 @@ struct Cfg {
   static constexpr int STEPS = WROWS / 4;  // four rows per step
   static constexpr int OCTETS = TN / 8;    // TMEM column octets of one level
   static constexpr int MAXQ = 2 * ((OCTETS + NG - 1) / NG);  // epilogue quartets per group
-  // shared memory of a launch: stages, barriers, the groups' sums, the
-  // item ring and the epilogue's phi_lhs values ([warp][column][lane])
+  // shared memory of a launch: stages, barriers, the item ring and the
+  // epilogue's phi_lhs values ([warp][column][lane])
   template <int STAGES>
   static constexpr size_t smem_bytes() {
-    return size_t(STAGES) * STAGE + 1024 + 256 + 2 * NG * PT * 8 + kRing * (16 + 4) +
+    return size_t(STAGES) * STAGE + 1024 + 256 + kRing * (16 + 4) +
            size_t(GW) * 4 * MAXQ * 32 * 8;
   }
   static_assert(NSL * TN <= 512, "level accumulators exceed the TMEM columns");
@@ -746,16 +746,11 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
   uint64_t* acc_full = bars + 3 * STAGES;
   uint64_t* acc_empty = acc_full + 1;
   uint64_t* drain = acc_full + 2;
-  uint64_t* epi_full = acc_full + 3;  // [2]: the groups' sums of an item are in `epi`
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_full + 5);
-  // the groups' per-point sums of an item, combined by group 0 (two items in
-  // flight at most: a group cannot reach item n+2's epilogue before group 0
-  // has finished item n+1's)
-  double* epi = reinterpret_cast<double*>(smem + STAGES * C::STAGE + 256);  // [2][NG][PT]
   // the work-item ring: the loader thread draws items from the global counter
   // (dynamic scheduling: the list is pair-major, heaviest pairs first) and
   // every role reads them from here in the same order
-  uint64_t* ifull = reinterpret_cast<uint64_t*>(epi + 2 * NG * PT);  // [kRing]
+  uint64_t* ifull = reinterpret_cast<uint64_t*>(smem + STAGES * C::STAGE + 256);  // [kRing]
   uint64_t* iempty = ifull + kRing;                                   // [kRing]
   int* ring = reinterpret_cast<int*>(iempty + kRing);                 // [kRing]
   double* phl_all = reinterpret_cast<double*>(ring + kRing);          // [GW][4 MAXQ][32]
@@ -772,8 +767,6 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
     tc::mbar_init(acc_full, 1);
     tc::mbar_init(acc_empty, GW);
     tc::mbar_init(drain, 1);
-    tc::mbar_init(&epi_full[0], GW);
-    tc::mbar_init(&epi_full[1], GW);
     for (int r = 0; r < kRing; ++r) {
       tc::mbar_init(&ifull[r], 1);
       tc::mbar_init(&iempty[r], GW + 2);  // every warp reads every item
@@ -1065,18 +1058,10 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
                                           : ldexp(acc, e);
         if (sym) res *= 2.0;
       }
-      double* e2 = epi + (nitem & 1) * (NG * PT);
-      e2[grp * PT + r] = res;
-      __syncwarp();
-      if (lane == 0) tc::mbar_arrive(&epi_full[nitem & 1]);
-      if (grp == 0) {
-        if (!tc::mbar_wait(&epi_full[nitem & 1], (nitem >> 1) & 1, err, 39, false, lim)) break;
-        double sum = e2[r];
-#pragma unroll
-        for (int w = 1; w < NG; ++w) sum += e2[w * PT + r];
-        const size_t pbase = p.poff ? size_t(p.poff[cur.pi]) : size_t(cur.pi) * p.max_t;
-        p.partial[((pbase + cur.ut) * p.nset_max + cur.s) * PT + r] = sum;
-      }
+      // each group's own partial sum (the reduction adds the groups and the
+      // row tiles in a fixed order), so no group waits for another here
+      const size_t pbase = p.poff ? size_t(p.poff[cur.pi]) : size_t(cur.pi) * p.max_t;
+      p.partial[(((pbase + cur.ut) * p.nset_max + cur.s) * NG + grp) * PT + r] = res;
       seq0 = seq1;
       cur = nxt;
     }
@@ -1232,7 +1217,10 @@ pair_reduce(PairArgs p, const int* __restrict__ npairs, int pair0) {
     const int g = g0 + (r & (HT - 1));
     if (g >= gend) continue;
     double acc = 0.0;
-    for (int t = 0; t < nt; ++t) acc += p.partial[((pbase + t) * p.nset_max + s) * PT + r];
+    for (int t = 0; t < nt; ++t)
+#pragma unroll
+      for (int gq = 0; gq < NG; ++gq)
+        acc += p.partial[(((pbase + t) * p.nset_max + s) * NG + gq) * PT + r];
     double* out = B.rhos + size_t(s) * B.stride_grid + g;
     *out = acc + *out;
   }
@@ -1291,7 +1279,7 @@ Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk, int nsl) {
   L.pmax = L.sigma + a256(ngrid * sizeof(int));
   L.phisl = L.pmax + a256(ngrid * sizeof(unsigned long long));
   L.partial = L.phisl + a256(nbg * max_kc * a_stage);
-  L.bytes = L.partial + nbg * max_t * nset * PT * sizeof(double);
+  L.bytes = L.partial + nbg * max_t * nset * NG * PT * sizeof(double);
   return L;
 }
 
@@ -1313,6 +1301,8 @@ size_t aodmao2rho_split_pair_workspace(size_t nao, size_t ngrid, size_t nset, si
 int split_pair_stages() {  // fixed: with the epilogue's phi_lhs values three stages fit
   return kStages;
 }
+
+int split_pair_partial_points() { return NG * PT; }
 
 cudaError_t split_pair_launch_main(const PairArgs& a, int nsl, cudaStream_t stream,
                                    bool attrs_only, int /*stages*/) {

@@ -13,7 +13,7 @@ Checked on every interleaving: no deadlock; a stage is refilled only after the
 MMAs of its previous chunk executed; the MMAs of a chunk read the D digits of
 all four warps of the chunk's group and the phi tile of the same chunk; an
 item's first MMA runs only after every warp has read the previous item's
-accumulators; group 0 sums each item's values from all three groups.
+accumulators; every group writes its partial sums of every item once.
 """
 import random
 
@@ -47,7 +47,6 @@ class Model:
         self.full_d = [Bar(4) for _ in range(STAGES)]
         self.empty = [Bar(1) for _ in range(STAGES)]
         self.acc_full, self.acc_empty, self.drain = Bar(1), Bar(GW), Bar(1)
-        self.epi_full = [Bar(GW), Bar(GW)]
         self.ifull = [Bar(1) for _ in range(RING)]
         self.iempty = [Bar(GW + 2) for _ in range(RING)]
         self.ring = [None] * RING
@@ -58,7 +57,6 @@ class Model:
         self.copies = []            # bulk copies in flight: (stage, seq)
         self.tmem_read = {}         # item -> warps that read its accumulators
         self.tmem_item = None       # item whose MMAs the accumulators hold
-        self.epi = [[None] * NG for _ in range(2)]
         self.sums = []
 
     # ---- roles (generators yield a predicate to wait on) ----
@@ -106,14 +104,8 @@ class Model:
             self.acc_empty.arrive()
             if ahead:
                 yield from gather(seq1 + grp)
-            buf = nitem & 1
-            self.epi[buf][grp] = nitem
-            self.epi_full[buf].arrive()
-            if grp == 0:
-                yield lambda n=nitem: self.epi_full[n & 1].passed((n >> 1) & 1)
-                assert self.epi[buf] == [nitem] * NG, "group sums of another item"
-                if w == 0:
-                    self.sums.append(nitem)
+            if w % 4 == 0:  # the group's partial sums of the item go out
+                self.sums.append((nitem, grp))
             seq0, t, nitem = seq1, tn, nitem + 1
 
     def mma_thread(self):
@@ -220,7 +212,7 @@ class Model:
                 waits[k] = live[k].send(None)
             except StopIteration:
                 del live[k]
-        assert self.sums == list(range(len(self.items)))
+        assert sorted(self.sums) == [(n, g) for n in range(len(self.items)) for g in range(NG)]
 
 
 def _items(rng, n):
