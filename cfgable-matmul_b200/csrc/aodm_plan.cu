@@ -150,16 +150,12 @@ cudaError_t pair_prepare_run(cfgmm_aodm_plan* plan, cudaStream_t s) {
   const cfgmm::PairArgs& a = plan->pargs;
   int* asym = const_cast<int*>(a.asym);
   cudaError_t err = cudaSuccess;
-  if (asym) {
-    err = cudaMemsetAsync(asym, 0, sizeof(int), s);
-    if (err == cudaSuccess)
-      err = cfgmm::aodm_launch_sym_check(plan->dms, plan->stride_ao, plan->nao, plan->nset_max,
-                                         asym, s);
-  }
+  if (asym) err = cudaMemsetAsync(asym, 0, sizeof(int), s);
   if (err == cudaSuccess)
     err = cfgmm::split_pair_prepare_d(plan->dms, plan->stride_ao, plan->nao, plan->nset_max,
                                       plan->nsl, const_cast<uint2*>(a.dsl),
-                                      const_cast<int*>(a.tau), s, asym);
+                                      const_cast<int*>(a.tau), const_cast<uint2*>(a.dhalf),
+                                      asym, s);
   return err;
 }
 
@@ -477,6 +473,7 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
                o_poff = take((nbg_tot + 1) * 4), o_items = take(item_bound * sizeof(int4)),
                o_total = take(16), o_sigma = take(sg_n * 4),
                o_dsl = take(nset_max * nao * nao * 8), o_tau = take(nset_max * nao * 4),
+               o_dhalf = take(nset_max * nao * 8),
                o_batch = take(nbatch * sizeof(cfgmm::PairBatch)),
                o_phisl = take(chunk_bound * a_stage);
   cudaError_t err = cudaMallocAsync(&plan->mem2, o, s);
@@ -596,6 +593,7 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
   cfgmm::PairArgs& a = plan->pargs;
   a.dsl = static_cast<const uint2*>(at(o_dsl));
   a.tau = static_cast<const int*>(at(o_tau));
+  a.dhalf = static_cast<const uint2*>(at(o_dhalf));
   a.phisl = static_cast<const uint8_t*>(at(o_phisl));
   a.items = static_cast<const int4*>(at(o_items));
   a.total = d_total;

@@ -95,6 +95,7 @@ struct PairBatch {
 struct PairArgs {
   const uint2* dsl;       // D digits [s][u][v], 8 bytes each
   const int* tau;         // row scales [s][u]
+  const uint2* dhalf;     // digits of D_uu / 2 [s][u] (the symmetric mode's diagonal)
   const uint8_t* phisl;   // phi digit tiles [chunk][NSL][128 x 32]
   const int4* items;      // (pair, row tile, s, batch)
   const int* total;       // [0] items
@@ -158,8 +159,12 @@ cudaError_t split_pair_prepare_scales(const PairPrep& q, cudaStream_t stream);
 cudaError_t split_pair_prepare_pairs(const PairPrep& q, cudaStream_t stream);
 cudaError_t split_pair_prepare_tiles(const PairPrep& q, cudaStream_t stream);
 cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream);
+// D digits of every row (dsl, tau, and dhalf: the digits of D_uu / 2 for the
+// symmetric mode's diagonal) and, when asym is non-null (zeroed by the
+// caller), the bitwise symmetry check of every D, in one launch.
 cudaError_t split_pair_prepare_d(const double* dms, size_t stride_ao, int nao, int nset, int nsl,
-                                 uint2* dsl, int* tau, cudaStream_t stream, const int* asym);
+                                 uint2* dsl, int* tau, uint2* dhalf, int* asym,
+                                 cudaStream_t stream);
 int split_pair_stages();  // the pair kernel's pipeline depth
 // partial sums per (row tile, DM) of a pair: one per gather group and point
 int split_pair_partial_points();

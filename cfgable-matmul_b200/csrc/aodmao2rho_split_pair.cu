@@ -664,15 +664,54 @@ pair_phi_tiles(const double* __restrict__ ao, size_t stride_grid,
   }
 }
 
-// D digits: dsl[s][u][v] (NSL digits in 8 bytes), tau[s][u]; a CTA per row
-// (its max first, then the digits, the second read from L1).  With asym
-// non-null and 0 (symmetric mode) the diagonal carries D_uu / 2.
+// D digits and the symmetry check in one launch.  CTAs 0 .. nset*nao-1: row
+// (s, u) -- tau[s][u], the digits dsl[s][u][v] of the whole row (its max
+// first, then the digits, the second read from L1) and dhalf[s][u], the
+// digits of D_uu / 2 that the symmetric mode uses for the diagonal.  The
+// CTAs after them (when asym is non-null): one 32 x 32 tile pair (i, j),
+// j <= i, of a D each, compared with its transpose bitwise; a difference sets
+// *asym (zeroed by the caller).
 template <int NSL>
 __global__ void __launch_bounds__(256)
-pair_d_digits(const double* __restrict__ dms, size_t stride_ao, size_t dm_stride, int nao,
-              uint2* __restrict__ dsl, int* __restrict__ tau, const int* __restrict__ asym) {
+pair_d_prep(const double* __restrict__ dms, size_t stride_ao, size_t dm_stride, int nao,
+            int nset, uint2* __restrict__ dsl, int* __restrict__ tau,
+            uint2* __restrict__ dhalf, int* __restrict__ asym) {
+  const int nrows = nset * nao;
+  if (int(blockIdx.x) >= nrows) {
+    // ---- symmetry check: tile pair k of D s (triangular index) ----
+    const int nt = (nao + 31) / 32;
+    const int ntri = nt * (nt + 1) / 2;
+    const int t = int(blockIdx.x) - nrows;
+    const int s = t / ntri, k = t % ntri;
+    int bx = int((sqrtf(8.f * float(k) + 1.f) - 1.f) * 0.5f);
+    while (bx * (bx + 1) / 2 > k) --bx;
+    while ((bx + 1) * (bx + 2) / 2 <= k) ++bx;
+    const int by = k - bx * (bx + 1) / 2;  // by <= bx
+    __shared__ double tile[32][33];
+    const double* d = dms + size_t(s) * dm_stride;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    double mine[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int i = ty + 8 * q;
+      const int r = by * 32 + i, c = bx * 32 + tx;
+      tile[i][tx] = (r < nao && c < nao) ? d[size_t(r) * stride_ao + c] : 0.0;
+      const int r2 = bx * 32 + i, c2 = by * 32 + tx;
+      mine[q] = (r2 < nao && c2 < nao) ? d[size_t(r2) * stride_ao + c2] : 0.0;
+    }
+    __syncthreads();
+    bool bad = false;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int i = ty + 8 * q;
+      const int r2 = bx * 32 + i, c2 = by * 32 + tx;
+      if (r2 < nao && c2 < nao) bad |= !(mine[q] == tile[tx][i]);
+    }
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(asym, 1);
+    return;
+  }
+  // ---- digits of row (s, u) ----
   const int row = blockIdx.x;
-  const bool half_diag = asym != nullptr && *asym == 0;
   const int s = row / nao, u = row % nao;
   const double* d = dms + size_t(s) * dm_stride + size_t(u) * stride_ao;
   __shared__ double wmax[8];
@@ -704,15 +743,14 @@ pair_d_digits(const double* __restrict__ dms, size_t stride_ao, size_t dm_stride
     bad |= wbad[i] != 0;
   }
   const int e = bad ? kBadExp : exp_for(mx);
-  if (threadIdx.x == 0) tau[row] = e;
+  if (threadIdx.x == 0) {
+    tau[row] = e;
+    dhalf[row] = e != kBadExp ? digits_of<NSL>(0.5 * d[u], e) : make_uint2(0u, 0u);
+  }
   uint2* out = dsl + size_t(row) * nao;
-  // symmetric mode: the gather reads only v >= u (union positions ascend with
-  // the AO index), so the strict lower triangle is not written
-  const int v0 = (half_diag ? (u & ~31) : 0) + int(threadIdx.x);
 #pragma unroll 4
-  for (int v = v0; v < nao; v += 256)
-    out[v] = e != kBadExp ? digits_of<NSL>(half_diag && v == u ? 0.5 * d[v] : d[v], e)
-                          : make_uint2(0u, 0u);
+  for (int v = threadIdx.x; v < nao; v += 256)
+    out[v] = e != kBadExp ? digits_of<NSL>(d[v], e) : make_uint2(0u, 0u);
 }
 
 // Byte selector assembling, from `keep` (bytes 0..3) and `recv` (4..7) of the
@@ -858,8 +896,9 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
     // D digits of chunk c of item g at this lane's positions (no waits)
     auto load_chunk = [&](const Item& g, int c, const int (&iv)[4], uint2 (&w)[C::STEPS][4]) {
       const uint2* dset = p.dsl + size_t(g.s) * p.nao * p.nao;
-      // symmetric D: only columns from the row's own position on (the
-      // diagonal digits carry D_uu / 2)
+      const uint2* dh = p.dhalf + size_t(g.s) * p.nao;
+      // symmetric D: only columns from the row's own position on, the
+      // diagonal with the digits of D_uu / 2
 #pragma unroll
       for (int st = 0; st < C::STEPS; ++st) {
         const int prow = g.ut * TN + C::WROWS * wq + 4 * st + ri;
@@ -867,7 +906,8 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
         for (int k = 0; k < 4; ++k) {
           const int pc = c * TK + 16 * hh + 4 * k + qd;
           w[st][k] = (g.iu[st] >= 0 && iv[k] >= 0 && (!sym || pc >= prow))
-                         ? __ldg(dset + size_t(g.iu[st]) * p.nao + iv[k])
+                         ? __ldg(sym && pc == prow ? dh + g.iu[st]
+                                                   : dset + size_t(g.iu[st]) * p.nao + iv[k])
                          : make_uint2(0u, 0u);
         }
       }
@@ -1241,7 +1281,8 @@ size_t a256(size_t v) { return (v + 255) / 256 * 256; }
 
 struct Layout {
   size_t lists, counts, bits, cnt, key, order, cand, ncand, partner, pos, choice, pairs, npairs,
-      ulist, uflag, ucount, cbase, items, total, dsl, tau, sigma, pmax, phisl, partial, bytes;
+      ulist, uflag, ucount, cbase, items, total, dsl, tau, dhalf, sigma, pmax, phisl, partial,
+      bytes;
 };
 
 Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk, int nsl) {
@@ -1275,7 +1316,8 @@ Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk, int nsl) {
   L.total = L.items + a256(nbg * max_t * nset * sizeof(int4));
   L.dsl = L.total + 256;
   L.tau = L.dsl + a256(nset * nao * nao * 8);
-  L.sigma = L.tau + a256(nset * nao * sizeof(int));
+  L.dhalf = L.tau + a256(nset * nao * sizeof(int));
+  L.sigma = L.dhalf + a256(nset * nao * 8);
   L.pmax = L.sigma + a256(ngrid * sizeof(int));
   L.phisl = L.pmax + a256(ngrid * sizeof(unsigned long long));
   L.partial = L.phisl + a256(nbg * max_kc * a_stage);
@@ -1325,20 +1367,21 @@ cudaError_t split_pair_launch_reduce(const PairArgs& a, int nsl, const int* npai
 }
 
 cudaError_t split_pair_prepare_d(const double* dms, size_t stride_ao, int nao, int nset, int nsl,
-                                 uint2* dsl, int* tau, cudaStream_t stream, const int* asym) {
-  const unsigned grid = unsigned(nset * nao);
+                                 uint2* dsl, int* tau, uint2* dhalf, int* asym,
+                                 cudaStream_t stream) {
+  const int nt = (nao + 31) / 32;
+  const long long tiles = asym ? (long long)nset * (nt * (nt + 1) / 2) : 0;
+  const long long grid = (long long)nset * nao + tiles;
+  if (grid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
   if (nsl == 6)
-    pair_d_digits<6><<<grid, 256, 0, stream>>>(dms, stride_ao, stride_ao * stride_ao, nao, dsl,
-                                                tau, asym);
+    pair_d_prep<6><<<unsigned(grid), 256, 0, stream>>>(dms, stride_ao, stride_ao * stride_ao, nao,
+                                                         nset, dsl, tau, dhalf, asym);
   else
-    pair_d_digits<7><<<grid, 256, 0, stream>>>(dms, stride_ao, stride_ao * stride_ao, nao, dsl,
-                                                tau, asym);
+    pair_d_prep<7><<<unsigned(grid), 256, 0, stream>>>(dms, stride_ao, stride_ao * stride_ao, nao,
+                                                         nset, dsl, tau, dhalf, asym);
   return cudaGetLastError();
 }
 
-// Pairing, union lists, work list and phi digit tiles of one grid batch whose
-// active lists (lists, counts) are built: pairs from q.pair0 (at most nbg of
-// them), chunks from q.chunk0, items appended at *q.total.
 namespace {
 
 struct BatchDims {
@@ -1475,6 +1518,7 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   q.phisl = static_cast<uint8_t*>(at(L.phisl));
   uint2* dsl = static_cast<uint2*>(at(L.dsl));
   int* tau = static_cast<int*>(at(L.tau));
+  uint2* dhalf = static_cast<uint2*>(at(L.dhalf));
 
   // total[0]: items, total[1]: asymmetry flag, total[2]: chunks, total[3]: item counter
   int* asym = aodm_sym_enabled() && ao_lhs == ao_rhs ? q.total + 1 : nullptr;
@@ -1490,11 +1534,8 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   SideScope side(side_stream(true), stream);
   if ((err = side.fork()) != cudaSuccess) return err;
   const cudaStream_t sp = side.stream();
-  if (asym && (err = aodm_launch_sym_check(dms, stride_ao, nao, nset, asym, stream)) !=
-                  cudaSuccess)
-    return err;
-  if ((err = split_pair_prepare_d(dms, stride_ao, nao, nset, nsl, dsl, tau, stream, asym)) !=
-      cudaSuccess)
+  if ((err = split_pair_prepare_d(dms, stride_ao, nao, nset, nsl, dsl, tau, dhalf, asym,
+                                  stream)) != cudaSuccess)
     return err;
   if ((err = aodm_block_lists_launch(tab, ldtab, nao, nblk, lists, counts, sp)) != cudaSuccess)
     return err;
@@ -1510,6 +1551,7 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   PairArgs a{};
   a.dsl = dsl;
   a.tau = tau;
+  a.dhalf = dhalf;
   a.phisl = q.phisl;
   a.items = q.items;
   a.total = q.total;
