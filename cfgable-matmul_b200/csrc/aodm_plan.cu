@@ -467,6 +467,7 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
                o_cand = take(nbg_max * WIN2 * 4), o_ncand = take(nbg_max * 4),
                o_partner = take(nbg_max * 4), o_pos = take(nbg_max * 4),
                o_choice = take(nbg_max * 4), o_pmax = take(ngrid_max * 8),
+               o_cpair = take(nbg_max * ((nao + 31) / 32) * 4),
                o_pairs = take(nbg_tot * sizeof(int4)), o_np = take(8),
                o_ulist = take(nbg_tot * nao * 4), o_uflag = take(nbg_tot * nao),
                o_ucount = take(nbg_tot * 4), o_cbase = take((nbg_tot + 1) * 4),
@@ -518,6 +519,7 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
     q.uflag = static_cast<uint8_t*>(at(o_uflag));
     q.ucount = static_cast<int*>(at(o_ucount));
     q.cbase = static_cast<int*>(at(o_cbase));
+    q.cpair = static_cast<int*>(at(o_cpair));
     q.items = static_cast<int4*>(at(o_items));
     q.total = d_total;
     q.chunks_end = d_total + 2;

@@ -135,6 +135,7 @@ struct PairPrep {
   uint8_t* uflag;         // out: [pair][nao]
   int* ucount;            // out: [pair]
   int* cbase;             // out: [pair]
+  int* cpair;             // out: the pair of each of the batch's chunks [nbg * ceil(nao/32)]
   int4* items;            // out: appended at *total
   int* total;             // in/out: items so far
   int* chunks_end;        // out: chunk0 + this batch's chunks

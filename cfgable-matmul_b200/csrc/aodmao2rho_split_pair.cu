@@ -63,6 +63,7 @@
 // Every mbarrier wait is bounded (tcgen05.cuh).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <climits>
 #include <cstdint>
 #include <cstdlib>
@@ -503,7 +504,8 @@ pair_union(const uint8_t* __restrict__ tab, size_t ldtab, int nao, int gsub,
 __global__ void __launch_bounds__(1024)
 pair_build(const int* __restrict__ ucount, const int* __restrict__ npairs_d, int pair0, int nset,
            int batch, int tn, int max_kc, int chunk0, int* __restrict__ cbase,
-           int4* __restrict__ items, int* __restrict__ total, int* __restrict__ chunks_end) {
+           int* __restrict__ cpair, int4* __restrict__ items, int* __restrict__ total,
+           int* __restrict__ chunks_end) {
   extern __shared__ int hist[];  // max_kc + 2 counters
   __shared__ int warp_c[32];
   __shared__ int base_c;
@@ -526,7 +528,10 @@ pair_build(const int* __restrict__ ucount, const int* __restrict__ npairs_d, int
     __syncthreads();
     int bc = base_c;
     for (int w = 0; w < warp; ++w) bc += warp_c[w];
-    if (pl < np) cbase[pair0 + pl] = bc + ic - kc;
+    if (pl < np) {
+      cbase[pair0 + pl] = bc + ic - kc;
+      for (int c = 0; c < kc; ++c) cpair[bc + ic - kc - chunk0 + c] = pair0 + pl;
+    }
     __syncthreads();
     if (tid == 0)
       for (int w = 0; w < 32; ++w) base_c += warp_c[w];
@@ -600,67 +605,70 @@ pair_phi_max(const double* __restrict__ ao, size_t stride_grid, const int* __res
   }
 }
 
-// The phi digit tiles of chunk c of pair pi: NSL planes of 128 rows (points:
-// rows 0-63 the lo tile, 64-127 the hi tile) x 32 bytes (union AOs
-// 32c .. 32c+31), 32-byte swizzled, at phisl + (cbase[pi] + c) * A_STAGE;
-// sigma[g] from pmax.  CTA (pair, chunk).
+// The phi digit tiles of every chunk of the batch (pair pi, chunk c): NSL
+// planes of 128 rows (points: rows 0-63 the lo tile, 64-127 the hi tile) x
+// 32 bytes (union AOs 32c .. 32c+31), 32-byte swizzled, at phisl + (cbase[pi]
+// + c) * A_STAGE; sigma[g] from pmax.  Persistent CTAs walk the batch's
+// chunks [chunk0, chunks_end) through the chunk -> pair map.
 template <int NSL>
 __global__ void __launch_bounds__(256)
 pair_phi_tiles(const double* __restrict__ ao, size_t stride_grid,
                const unsigned long long* __restrict__ pmax, const int4* __restrict__ pairs,
-               const int* __restrict__ npairs, int pair0, const int* __restrict__ ulist,
-               const uint8_t* __restrict__ uflag, const int* __restrict__ ucount,
-               const int* __restrict__ cbase, int nao, int ngrid, int blk, int gsub,
-               int* __restrict__ sigma, uint8_t* __restrict__ phisl) {
+               const int* __restrict__ cpair, int chunk0, const int* __restrict__ chunks_end,
+               const int* __restrict__ ulist, const uint8_t* __restrict__ uflag,
+               const int* __restrict__ ucount, const int* __restrict__ cbase, int nao, int ngrid,
+               int blk, int gsub, int* __restrict__ sigma, uint8_t* __restrict__ phisl) {
   using C = Cfg<NSL>;
-  const int pl = blockIdx.x, c = blockIdx.y;
-  if (pl >= npairs[0]) return;
-  const int pi = pair0 + pl;
-  const int nu = ucount[pi];
-  if (c * TK >= nu) return;
-  const int4 pr = pairs[pi];
   // staged digit words [plane][quad of 4 AOs][point], rows padded to 132 words
   __shared__ uint32_t stage[NSL][8][PT + 4];
-  const int* U = ulist + size_t(pi) * nao;
-  const uint8_t* F = uflag + size_t(pi) * nao;
-  {
-    const int v = threadIdx.x;
-    const int r = v & (PT - 1), hq = v >> 7;  // point row, half of the quads
-    const int h = r >> 6, j = r & (HT - 1);
-    const int tile = h ? pr.y : pr.x;
-    int g = -1;
-    if (tile >= 0) {
-      int g0, gend;
-      tile_points(tile, blk, gsub, ngrid, &g0, &gend);
-      if (g0 + j < gend) g = g0 + j;
-    }
-    const int e = g >= 0 ? exp_for(__longlong_as_double(static_cast<long long>(pmax[g]))) : 0;
-    if (c == 0 && hq == 0 && g >= 0) sigma[g] = e;
-#pragma unroll
-    for (int qq = 0; qq < 4; ++qq) {
-      const int q = hq * 4 + qq;
-      uint2 w[4];
-#pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        const int k = c * TK + q * 4 + t;
-        bool on = g >= 0 && k < nu && e != kBadExp;
-        if (on) on = ((F[k] >> h) & 1u) != 0;
-        w[t] = on ? digits_of<NSL>(ao[size_t(U[k]) * stride_grid + g], e) : make_uint2(0u, 0u);
+  const int nch = chunks_end[0] - chunk0;
+  for (int ci = blockIdx.x; ci < nch; ci += gridDim.x) {
+    const int pi = cpair[ci];
+    const int c = chunk0 + ci - cbase[pi];
+    const int nu = ucount[pi];
+    const int4 pr = pairs[pi];
+    const int* U = ulist + size_t(pi) * nao;
+    const uint8_t* F = uflag + size_t(pi) * nao;
+    {
+      const int r = threadIdx.x & (PT - 1), hq = threadIdx.x >> 7;  // point row, half of the quads
+      const int h = r >> 6;
+      const int tile = h ? pr.y : pr.x;
+      int g = -1;
+      if (tile >= 0) {
+        int g0, gend;
+        tile_points(tile, blk, gsub, ngrid, &g0, &gend);
+        if (g0 + (r & (HT - 1)) < gend) g = g0 + (r & (HT - 1));
       }
-      uint32_t o[8];
-      transpose4(w[0].x, w[1].x, w[2].x, w[3].x, o[0], o[1], o[2], o[3]);
-      transpose4(w[0].y, w[1].y, w[2].y, w[3].y, o[4], o[5], o[6], o[7]);
+      const int e = g >= 0 ? exp_for(__longlong_as_double(static_cast<long long>(pmax[g]))) : 0;
+      if (c == 0 && hq == 0 && g >= 0) sigma[g] = e;
 #pragma unroll
-      for (int pl2 = 0; pl2 < NSL; ++pl2) stage[pl2][q][r] = o[pl2];
+      for (int qq = 0; qq < 4; ++qq) {
+        const int q = hq * 4 + qq;
+        uint2 w[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const int k = c * TK + q * 4 + t;
+          const bool on = g >= 0 && k < nu && e != kBadExp && ((__ldg(F + k) >> h) & 1u);
+          w[t] = on ? digits_of<NSL>(ao[size_t(__ldg(U + k)) * stride_grid + g], e)
+                    : make_uint2(0u, 0u);
+        }
+        uint32_t o[8];
+        transpose4(w[0].x, w[1].x, w[2].x, w[3].x, o[0], o[1], o[2], o[3]);
+        transpose4(w[0].y, w[1].y, w[2].y, w[3].y, o[4], o[5], o[6], o[7]);
+#pragma unroll
+        for (int pl2 = 0; pl2 < NSL; ++pl2) stage[pl2][q][r] = o[pl2];
+      }
     }
-  }
-  __syncthreads();
-  uint8_t* tile0 = phisl + (size_t(cbase[pi]) + c) * C::A_STAGE;
-  for (int v = threadIdx.x; v < NSL * PT * 2; v += 256) {
-    const int hh = v & 1, r = (v >> 1) & (PT - 1), j = v >> 8;
-    const uint4 w = make_uint4(stage[j][4 * hh][r], stage[j][4 * hh + 1][r],
-                               stage[j][4 * hh + 2][r], stage[j][4 * hh + 3][r]);
-    *reinterpret_cast<uint4*>(tile0 + j * C::A_SLICE + tc::sw32_offset(uint32_t(r), uint32_t(hh))) = w;
+    __syncthreads();
+    uint8_t* tile0 = phisl + (size_t(cbase[pi]) + c) * C::A_STAGE;
+    for (int v = threadIdx.x; v < NSL * PT * 2; v += 256) {
+      const int hh = v & 1, r = (v >> 1) & (PT - 1), j = v >> 8;
+      const uint4 wv = make_uint4(stage[j][4 * hh][r], stage[j][4 * hh + 1][r],
+                                  stage[j][4 * hh + 2][r], stage[j][4 * hh + 3][r]);
+      *reinterpret_cast<uint4*>(tile0 + j * C::A_SLICE +
+                                tc::sw32_offset(uint32_t(r), uint32_t(hh))) = wv;
+    }
+    __syncthreads();
   }
 }
 
@@ -1281,8 +1289,8 @@ size_t a256(size_t v) { return (v + 255) / 256 * 256; }
 
 struct Layout {
   size_t lists, counts, bits, cnt, key, order, cand, ncand, partner, pos, choice, pairs, npairs,
-      ulist, uflag, ucount, cbase, items, total, dsl, tau, dhalf, sigma, pmax, phisl, partial,
-      bytes;
+      ulist, uflag, ucount, cbase, cpair, items, total, dsl, tau, dhalf, sigma, pmax, phisl,
+      partial, bytes;
 };
 
 Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk, int nsl) {
@@ -1312,7 +1320,8 @@ Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk, int nsl) {
   L.uflag = L.ulist + a256(nbg * nao * sizeof(int));
   L.ucount = L.uflag + a256(nbg * nao);
   L.cbase = L.ucount + a256(nbg * sizeof(int));
-  L.items = L.cbase + a256((nbg + 1) * sizeof(int));
+  L.cpair = L.cbase + a256((nbg + 1) * sizeof(int));
+  L.items = L.cpair + a256(nbg * max_kc * sizeof(int));
   L.total = L.items + a256(nbg * max_t * nset * sizeof(int4));
   L.dsl = L.total + 256;
   L.tau = L.dsl + a256(nset * nao * nao * 8);
@@ -1426,7 +1435,7 @@ cudaError_t split_pair_prepare_pairs(const PairPrep& q, cudaStream_t stream) {
                                         q.ulist, q.uflag, q.ucount);
   const size_t hist = size_t(d.max_kc + 2) * sizeof(int);
   pair_build<<<1, 1024, hist, stream>>>(q.ucount, q.npairs, q.pair0, q.nset, q.batch, d.tn,
-                                        d.max_kc, q.chunk0, q.cbase, q.items, q.total,
+                                        d.max_kc, q.chunk0, q.cbase, q.cpair, q.items, q.total,
                                         q.chunks_end);
   return cudaGetLastError();
 }
@@ -1445,15 +1454,23 @@ cudaError_t split_pair_prepare_scales(const PairPrep& q, cudaStream_t stream) {
 cudaError_t split_pair_prepare_tiles(const PairPrep& q, cudaStream_t stream) {
   const BatchDims d = batch_dims(q);
   if (d.nbg <= 0) return cudaSuccess;
-  const dim3 tg(d.nbg, d.max_kc);
+  int dev = 0, nsm = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err == cudaSuccess) err = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (err != cudaSuccess) return err;
+  // persistent: as many CTAs as fit beside one another (30 KB of shared memory each)
+  const unsigned grid = unsigned(std::min<long long>((long long)nsm * 6,
+                                                     (long long)d.nbg * d.max_kc));
   if (q.nsl == 6)
-    pair_phi_tiles<6><<<tg, 256, 0, stream>>>(q.ao_rhs, q.stride_grid, q.pmax, q.pairs, q.npairs,
-                                              q.pair0, q.ulist, q.uflag, q.ucount, q.cbase, q.nao,
-                                              q.ngrid, q.blk, d.gsub, q.sigma, q.phisl);
+    pair_phi_tiles<6><<<grid, 256, 0, stream>>>(q.ao_rhs, q.stride_grid, q.pmax, q.pairs, q.cpair,
+                                                q.chunk0, q.chunks_end, q.ulist, q.uflag,
+                                                q.ucount, q.cbase, q.nao, q.ngrid, q.blk, d.gsub,
+                                                q.sigma, q.phisl);
   else
-    pair_phi_tiles<7><<<tg, 256, 0, stream>>>(q.ao_rhs, q.stride_grid, q.pmax, q.pairs, q.npairs,
-                                              q.pair0, q.ulist, q.uflag, q.ucount, q.cbase, q.nao,
-                                              q.ngrid, q.blk, d.gsub, q.sigma, q.phisl);
+    pair_phi_tiles<7><<<grid, 256, 0, stream>>>(q.ao_rhs, q.stride_grid, q.pmax, q.pairs, q.cpair,
+                                                q.chunk0, q.chunks_end, q.ulist, q.uflag,
+                                                q.ucount, q.cbase, q.nao, q.ngrid, q.blk, d.gsub,
+                                                q.sigma, q.phisl);
   return cudaGetLastError();
 }
 
@@ -1510,6 +1527,7 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   q.uflag = static_cast<uint8_t*>(at(L.uflag));
   q.ucount = static_cast<int*>(at(L.ucount));
   q.cbase = static_cast<int*>(at(L.cbase));
+  q.cpair = static_cast<int*>(at(L.cpair));
   q.items = static_cast<int4*>(at(L.items));
   q.total = static_cast<int*>(at(L.total));
   q.chunks_end = q.total + 2;
