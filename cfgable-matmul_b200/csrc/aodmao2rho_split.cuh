@@ -157,7 +157,12 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
 // (from the block lists), pairing and work list (from the mask), phi tiles
 // (from both); prepare_batch runs the three in that order on one stream.
 cudaError_t split_pair_prepare_scales(const PairPrep& q, cudaStream_t stream);
-cudaError_t split_pair_prepare_pairs(const PairPrep& q, cudaStream_t stream);
+// signatures = false: pair_lists_and_signatures has made them (with the
+// block lists, from one read of the mask)
+cudaError_t split_pair_prepare_pairs(const PairPrep& q, cudaStream_t stream,
+                                     bool signatures = true);
+cudaError_t split_pair_lists_and_signatures(const PairPrep& q, int* lists, int* counts,
+                                            cudaStream_t stream);
 cudaError_t split_pair_prepare_tiles(const PairPrep& q, cudaStream_t stream);
 cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream);
 // D digits of every row (dsl, tau, and dhalf: the digits of D_uu / 2 for the

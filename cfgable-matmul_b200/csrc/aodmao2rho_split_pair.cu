@@ -263,6 +263,73 @@ pair_sig(const uint8_t* __restrict__ tab, size_t ldtab, int nao, int nbg, int gs
   }
 }
 
+// The block lists (as aodm_block_lists: ascending active AOs of block b,
+// counts[b]) and the signatures of the block's tiles (as pair_sig) from one
+// read of the mask column; CTA per block.
+__global__ void __launch_bounds__(256)
+pair_lists_sig(const uint8_t* __restrict__ tab, size_t ldtab, int nao, int nblk, int gsub,
+               int nwords, int* __restrict__ lists, int* __restrict__ counts,
+               uint32_t* __restrict__ bits, int* __restrict__ cnt,
+               unsigned long long* __restrict__ key) {
+  const int b = blockIdx.x;
+  if (b >= nblk) return;
+  __shared__ int warp_tot[8];
+  __shared__ int base_s;
+  __shared__ uint32_t s1[8], s2[8];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) base_s = 0;
+  __syncthreads();
+  int* out = lists + size_t(b) * nao;
+  uint32_t h1 = 0xffffffffu, h2 = 0xffffffffu;
+  for (int u0 = 0; u0 < nao; u0 += 256) {
+    const int u = u0 + tid;
+    const bool on = u < nao && tab[size_t(u) * ldtab + b] != 0;
+    const uint32_t bal = __ballot_sync(0xffffffffu, on);
+    const int wbase = u0 + (tid & ~31);
+    if (lane == 0 && wbase < nao)
+      for (int t = 0; t < gsub; ++t) bits[size_t(b * gsub + t) * nwords + wbase / 32] = bal;
+    if (on) {
+      h1 = min(h1, mix32(uint32_t(u), 0x2545F491u));
+      h2 = min(h2, mix32(uint32_t(u), 0x6C8E9CF5u));
+    }
+    if (lane == 0) warp_tot[warp] = __popc(bal);
+    __syncthreads();
+    int before = base_s;
+    for (int w = 0; w < warp; ++w) before += warp_tot[w];
+    if (on) out[before + __popc(bal & ((1u << lane) - 1u))] = u;
+    __syncthreads();
+    if (tid == 0) {
+      int t = 0;
+      for (int w = 0; w < 8; ++w) t += warp_tot[w];
+      base_s += t;
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    h1 = min(h1, __shfl_xor_sync(0xffffffffu, h1, o));
+    h2 = min(h2, __shfl_xor_sync(0xffffffffu, h2, o));
+  }
+  if (lane == 0) {
+    s1[warp] = h1;
+    s2[warp] = h2;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    uint32_t a = s1[0], c = s2[0];
+    for (int w = 1; w < 8; ++w) {
+      a = min(a, s1[w]);
+      c = min(c, s2[w]);
+    }
+    const int n = base_s;
+    counts[b] = n;
+    for (int t = 0; t < gsub; ++t) {
+      cnt[b * gsub + t] = n;
+      key[b * gsub + t] = n == 0 ? ~0ull : (static_cast<unsigned long long>(a) << 32) | c;
+    }
+  }
+}
+
 // order[q] = tile at sorted position q (keys ascending, ties by index); above
 // kSortMax tiles the caller's order.
 __global__ void __launch_bounds__(1024)
@@ -1409,15 +1476,26 @@ BatchDims batch_dims(const PairPrep& q) {
 
 }  // namespace
 
-cudaError_t split_pair_prepare_pairs(const PairPrep& q, cudaStream_t stream) {
+cudaError_t split_pair_lists_and_signatures(const PairPrep& q, int* lists, int* counts,
+                                            cudaStream_t stream) {
+  const BatchDims d = batch_dims(q);
+  if (d.nbg <= 0) return cudaSuccess;
+  const int nblk = d.nbg / d.gsub;
+  pair_lists_sig<<<nblk, 256, 0, stream>>>(q.tab, q.ldtab, q.nao, nblk, d.gsub, d.nwords, lists,
+                                           counts, q.bits, q.cnt, q.key);
+  return cudaGetLastError();
+}
+
+cudaError_t split_pair_prepare_pairs(const PairPrep& q, cudaStream_t stream, bool signatures) {
   const BatchDims d = batch_dims(q);
   if (d.nbg <= 0) return cudaSuccess;
   constexpr size_t sort_smem = size_t(kSortMax) * (sizeof(unsigned long long) + sizeof(int));
   static const cudaError_t sort_attr = cudaFuncSetAttribute(
       pair_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sort_smem));
   if (sort_attr != cudaSuccess) return sort_attr;
-  pair_sig<<<d.nbg, 256, 0, stream>>>(q.tab, q.ldtab, q.nao, d.nbg, d.gsub, d.nwords, q.bits,
-                                      q.cnt, q.key);
+  if (signatures)
+    pair_sig<<<d.nbg, 256, 0, stream>>>(q.tab, q.ldtab, q.nao, d.nbg, d.gsub, d.nwords, q.bits,
+                                        q.cnt, q.key);
   pair_sort<<<1, 1024, sort_smem, stream>>>(q.key, d.nbg, q.order);
   pair_scores<<<d.nbg, 2 * kWin, 0, stream>>>(q.bits, q.cnt, q.order, d.nbg, d.nwords, q.cand,
                                               q.ncand);
@@ -1555,13 +1633,12 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   if ((err = split_pair_prepare_d(dms, stride_ao, nao, nset, nsl, dsl, tau, dhalf, asym,
                                   stream)) != cudaSuccess)
     return err;
-  if ((err = aodm_block_lists_launch(tab, ldtab, nao, nblk, lists, counts, sp)) != cudaSuccess)
-    return err;
+  if ((err = split_pair_lists_and_signatures(q, lists, counts, sp)) != cudaSuccess) return err;
   const SideStream* ss = side_stream(true);
   const bool split_streams = sp != stream && ss;
   if (split_streams && (err = side_join(ss, stream)) != cudaSuccess) return err;  // lists -> scales
   if ((err = split_pair_prepare_scales(q, stream)) != cudaSuccess) return err;
-  if ((err = split_pair_prepare_pairs(q, sp)) != cudaSuccess) return err;
+  if ((err = split_pair_prepare_pairs(q, sp, false)) != cudaSuccess) return err;
   if (split_streams && (err = side_fork(ss, stream)) != cudaSuccess) return err;  // scales -> tiles
   if ((err = split_pair_prepare_tiles(q, sp)) != cudaSuccess) return err;
   if ((err = side.join()) != cudaSuccess) return err;
