@@ -1620,26 +1620,27 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   int* asym = aodm_sym_enabled() && ao_lhs == ao_rhs ? q.total + 1 : nullptr;
   cudaError_t err = cudaMemsetAsync(q.total, 0, 4 * sizeof(int), stream);
   if (err != cudaSuccess) return err;
-  // Two chains: the pairing chain (block lists, signatures, sort, scores,
-  // matching, unions, work list, then the phi tiles) on a high-priority side
-  // stream, so that its small kernels are not held back behind the CTAs of
-  // the D chain (symmetry check, D digits, then the point scales) on the
-  // caller's stream.  The point scales wait for the block lists, the phi
-  // tiles for the point scales; the side stream joins back before the main
-  // kernel.
+  // Two chains.  On a high-priority side stream the pairing chain (block lists
+  // with the tile signatures, sort, scores, matching, unions, work list,
+  // then the phi tiles); on the caller's stream the point scales (after the
+  // block lists) and then the D preparation (digits and symmetry check), which
+  // only the main kernel needs.  The phi tiles wait for the point scales
+  // alone; the side stream joins back before the main kernel.
   SideScope side(side_stream(true), stream);
   if ((err = side.fork()) != cudaSuccess) return err;
   const cudaStream_t sp = side.stream();
+  const SideStream* ss = side_stream(true);
+  const bool split_streams = sp != stream && ss;
+  if ((err = split_pair_lists_and_signatures(q, lists, counts, sp)) != cudaSuccess) return err;
+  if (split_streams && (err = side_join(ss, stream)) != cudaSuccess) return err;  // lists -> scales
+  if ((err = split_pair_prepare_scales(q, stream)) != cudaSuccess) return err;
+  if (split_streams && (err = cudaEventRecord(ss->fork, stream)) != cudaSuccess) return err;
   if ((err = split_pair_prepare_d(dms, stride_ao, nao, nset, nsl, dsl, tau, dhalf, asym,
                                   stream)) != cudaSuccess)
     return err;
-  if ((err = split_pair_lists_and_signatures(q, lists, counts, sp)) != cudaSuccess) return err;
-  const SideStream* ss = side_stream(true);
-  const bool split_streams = sp != stream && ss;
-  if (split_streams && (err = side_join(ss, stream)) != cudaSuccess) return err;  // lists -> scales
-  if ((err = split_pair_prepare_scales(q, stream)) != cudaSuccess) return err;
   if ((err = split_pair_prepare_pairs(q, sp, false)) != cudaSuccess) return err;
-  if (split_streams && (err = side_fork(ss, stream)) != cudaSuccess) return err;  // scales -> tiles
+  // the tiles wait for the scales (the fork event recorded after them above)
+  if (split_streams && (err = cudaStreamWaitEvent(sp, ss->fork, 0)) != cudaSuccess) return err;
   if ((err = split_pair_prepare_tiles(q, sp)) != cudaSuccess) return err;
   if ((err = side.join()) != cudaSuccess) return err;
 
