@@ -1622,28 +1622,25 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   if (err != cudaSuccess) return err;
   // Two chains.  On a high-priority side stream the pairing chain (block lists
   // with the tile signatures, sort, scores, matching, unions, work list,
-  // then the phi tiles); on the caller's stream the point scales (after the
-  // block lists, beside the pairing kernels) and the D preparation (digits
-  // and symmetry check, only the main kernel needs them) after the pairing
-  // kernels, beside the phi tiles: the small, latency-bound pairing kernels
-  // run without the D preparation's memory traffic.  The side stream joins
-  // back before the main kernel.
+  // then the phi tiles); on the caller's stream the D preparation (digits and
+  // symmetry check) and then the point scales (after the block lists).  The
+  // phi tiles wait for the scales; the side stream joins back before the
+  // main kernel.  (The D preparation after the pairing kernels, or after the
+  // scales, measured slower: the preparation as a whole is bound by memory
+  // traffic and latency, about 0.22 ms at taxol size.)
   SideScope side(side_stream(true), stream);
   if ((err = side.fork()) != cudaSuccess) return err;
   const cudaStream_t sp = side.stream();
   const SideStream* ss = side_stream(true);
   const bool split_streams = sp != stream && ss;
-  if ((err = split_pair_lists_and_signatures(q, lists, counts, sp)) != cudaSuccess) return err;
-  if (split_streams && (err = side_join(ss, stream)) != cudaSuccess) return err;  // lists -> scales
-  if ((err = split_pair_prepare_scales(q, stream)) != cudaSuccess) return err;
-  if (split_streams && (err = cudaEventRecord(ss->fork, stream)) != cudaSuccess) return err;
-  if ((err = split_pair_prepare_pairs(q, sp, false)) != cudaSuccess) return err;
-  if (split_streams && (err = side_join(ss, stream)) != cudaSuccess) return err;  // pairs -> D
   if ((err = split_pair_prepare_d(dms, stride_ao, nao, nset, nsl, dsl, tau, dhalf, asym,
                                   stream)) != cudaSuccess)
     return err;
-  // the tiles wait for the scales (the fork event recorded after them above)
-  if (split_streams && (err = cudaStreamWaitEvent(sp, ss->fork, 0)) != cudaSuccess) return err;
+  if ((err = split_pair_lists_and_signatures(q, lists, counts, sp)) != cudaSuccess) return err;
+  if (split_streams && (err = side_join(ss, stream)) != cudaSuccess) return err;  // lists -> scales
+  if ((err = split_pair_prepare_scales(q, stream)) != cudaSuccess) return err;
+  if ((err = split_pair_prepare_pairs(q, sp, false)) != cudaSuccess) return err;
+  if (split_streams && (err = side_fork(ss, stream)) != cudaSuccess) return err;  // scales -> tiles
   if ((err = split_pair_prepare_tiles(q, sp)) != cudaSuccess) return err;
   if ((err = side.join()) != cudaSuccess) return err;
 
