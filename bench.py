@@ -542,7 +542,9 @@ def serving_section(args, cm, wl):
                 "latency_ms": st["latency_ms"], "warm_latency_ms": st["warm_latency_ms"],
                 "molecule_load_ms": st["load_ms"], "plan_build_ms": st["plan_ms"],
                 "queue_ms": st["queue_ms"], "device_ms": st["device_ms"],
-                "gpu_busy": st["device_ms_total"] / (wall * 1e3),
+                # the requests' device spans (events on their slot streams) summed over
+                # the wall time: above 1 when requests of different molecules overlap
+                "device_spans_over_wall": st["device_ms_total"] / (wall * 1e3),
                 "max_inflight": st["max_inflight"],
                 "peak_bytes": st["peak_bytes"], "evictions": st["evictions"],
                 "admitted_molecules": st["admitted_molecules"]}
@@ -795,9 +797,11 @@ def run_ours(args, ranks: Ranks):
             k: {"host_dm": serving[k]["throughput"]["value"],
                 "device_dm": serving[k]["throughput_device_dm"]["value"],
                 "plan_build_max_ms": serving[k]["throughput_device_dm"]["plan_build_ms"]["max"],
-                "gpu_busy": serving[k]["throughput_device_dm"]["gpu_busy"],
+                "device_spans_over_wall":
+                    serving[k]["throughput_device_dm"]["device_spans_over_wall"],
                 "latency_p99_ms": serving[k]["latency"]["latency_ms"]["p99"],
-                "latency_gpu_busy": serving[k]["latency"]["gpu_busy"]}
+                "latency_device_spans_over_wall":
+                    serving[k]["latency"]["device_spans_over_wall"]}
             for k in ("fp64", "split")}
         targets["serving_saturated_gflops"]["target"] = ">= 10000 (FP64), split >= FP64"
     out = {
