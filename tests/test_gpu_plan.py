@@ -132,13 +132,15 @@ def test_autotune_cache(cm, wl, tmp_path, monkeypatch):
     p2.close()
 
 
+@pytest.mark.parametrize("form", ["row", "pair"])
 @pytest.mark.parametrize("graph,tune", [(True, True), (False, False)])
-def test_split_plan_equals_single_split_calls(cm, wl, tmp_path, monkeypatch, graph, tune):
+def test_split_plan_equals_single_split_calls(cm, wl, tmp_path, monkeypatch, graph, tune, form):
     """The split plan keeps phi digits from creation and rebuilds D digits per
     run; its arithmetic is the single call's, so results match bit for bit,
     and stay within 1e-12 of FP64."""
     import torch
     monkeypatch.setenv("CFGMM_AUTOTUNE_CACHE", str(tmp_path / "tune.txt"))
+    monkeypatch.setenv("CFGMM_SPLIT_FORM", form)
     bs, dms = _batches(wl, torch, 11, 17)
     dev, ddms = _device(torch, bs, dms)
     plan = cm.AodmPlan(dev, ddms, blksize=64, precision=cm.PREC_OZAKI_INT8, graph=graph, tune=tune)

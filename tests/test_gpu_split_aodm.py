@@ -11,6 +11,15 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
 
+@pytest.fixture(autouse=True, params=["row", "pair"])
+def split_form(request, monkeypatch):
+    """Every test runs both forms of the split kernel: the row form (one
+    block tile per item) and the pair form (two paired block tiles per item,
+    the default from 1024 AOs and 8192 points on)."""
+    monkeypatch.setenv("CFGMM_SPLIT_FORM", request.param)
+    return request.param
+
+
 def split(cm, rho, dms, lhs, rhs, strides, shape, nset, tab, ldtab, blk):
     cm.aodmao2rho_ex(rho, dms, lhs, rhs, strides, shape, nset, tab, ldtab, blk,
                      precision=cm.PREC_OZAKI_INT8)
