@@ -440,6 +440,8 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
   const size_t nwords = (nao + 31) / 32;
   const size_t a_stage = size_t(nsl) * PT * TK;
   size_t nbg_tot = 0, nbg_max = 0, ngrid_max = 0, sg_n = 0, chunk_bound = 0, item_bound = 0;
+  size_t row_bound = 0;  // partial row tiles of all pairs, at most
+  double work = 0.0;     // the autotune key's work: sum over the block tiles of |I|^2
   std::vector<size_t> sg_off(nbatch);
   for (size_t i = 0; i < nbatch; ++i) {
     const size_t nbg = nblk[i] * gsub;
@@ -453,6 +455,8 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
       // |U| <= |I_a| + |I_b|: a pair's chunks and row tiles are bounded by its tiles'
       chunk_bound += gsub * ((nb + TK - 1) / TK);
       item_bound += gsub * ((nb + tn - 1) / tn) * batches[i].nset;
+      row_bound += gsub * ((nb + tn - 1) / tn);
+      work += double(gsub) * double(nb) * double(nb);
     }
   }
   // ---- device memory (the partial sums follow once the pairs are known) ----
@@ -527,60 +531,81 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
     q.pmax = static_cast<unsigned long long*>(at(o_pmax));
     q.phisl = static_cast<uint8_t*>(at(o_phisl));
     err = cfgmm::split_pair_prepare_batch(q, s);
-    int got[2] = {0, 0};
-    if (err == cudaSuccess) err = cudaMemcpyAsync(&got[0], d_np + 1, 4, cudaMemcpyDeviceToHost, s);
-    if (err == cudaSuccess)
-      err = cudaMemcpyAsync(&got[1], d_total + 2, 4, cudaMemcpyDeviceToHost, s);
-    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
-    pair0 += got[0];
-    chunk0 = got[1];
+    if (nbatch > 1) {  // the next batch's pairs and chunks follow this one's
+      int got[2] = {0, 0};
+      if (err == cudaSuccess)
+        err = cudaMemcpyAsync(&got[0], d_np + 1, 4, cudaMemcpyDeviceToHost, s);
+      if (err == cudaSuccess)
+        err = cudaMemcpyAsync(&got[1], d_total + 2, 4, cudaMemcpyDeviceToHost, s);
+      if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+      pair0 += got[0];
+      chunk0 = got[1];
+    }
     hb[i] = cfgmm::PairBatch{b.ao_lhs, b.rhos, q.sigma, b.stride_grid, int(b.ngrid), int(b.nset)};
   }
   if (err != cudaSuccess) return cuda_fail(err, "split plan setup");
-  const int P = pair0;
-  if (size_t(chunk0) > chunk_bound) return fail(CFGMM_ERR_CUDA, "split plan: chunk bound exceeded");
-  // ---- work list: pair-major (a pair's phi tiles and D rows shared in L2 by
-  // the CTAs running at one time), heaviest pairs first ----
-  int nitems = 0;
-  err = cudaMemcpyAsync(&nitems, d_total, 4, cudaMemcpyDeviceToHost, s);
-  if (err == cudaSuccess) err = cudaStreamSynchronize(s);
-  if (err != cudaSuccess) return cuda_fail(err, "split plan work list");
-  if (size_t(nitems) > item_bound) return fail(CFGMM_ERR_CUDA, "split plan: item bound exceeded");
-  std::vector<int4> items(size_t(std::max(nitems, 0)));
-  std::vector<int> ucount(size_t(std::max(P, 1)));
-  if (err == cudaSuccess && nitems > 0)
-    err = cudaMemcpyAsync(items.data(), at(o_items), size_t(nitems) * sizeof(int4),
-                          cudaMemcpyDeviceToHost, s);
-  if (err == cudaSuccess && P > 0)
-    err = cudaMemcpyAsync(ucount.data(), at(o_ucount), size_t(P) * 4, cudaMemcpyDeviceToHost, s);
-  if (err == cudaSuccess) err = cudaStreamSynchronize(s);
-  if (err != cudaSuccess) return cuda_fail(err, "split plan work list");
-  std::stable_sort(items.begin(), items.end(), [&](const int4& x, const int4& y) {
-    const int kx = (ucount[x.x] + TK - 1) / TK, ky = (ucount[y.x] + TK - 1) / TK;
-    if (kx != ky) return kx > ky;
-    if (x.x != y.x) return x.x < y.x;
-    if (x.y != y.y) return x.y < y.y;
-    return x.z < y.z;
-  });
-  // partial row tiles: exact, from the unions
-  std::vector<int> poff(size_t(P) + 1, 0);
-  for (int q = 0; q < P; ++q) poff[q + 1] = poff[q] + (ucount[q] + tn - 1) / tn;
-  const size_t part_bytes =
-      size_t(poff[P]) * nset_max * cfgmm::split_pair_partial_points() * sizeof(double);
-  err = cudaMallocAsync(&plan->mem3, std::max<size_t>(part_bytes, 256), s);
-  if (err != cudaSuccess) return cuda_fail(err, "cudaMalloc(split plan partials)");
-  const int np_all = P;
-  if (nitems > 0)
-    err = cudaMemcpyAsync(at(o_items), items.data(), size_t(nitems) * sizeof(int4),
-                          cudaMemcpyHostToDevice, s);
-  if (err == cudaSuccess)
-    err = cudaMemcpyAsync(at(o_poff), poff.data(), poff.size() * 4, cudaMemcpyHostToDevice, s);
-  if (err == cudaSuccess) err = cudaMemcpyAsync(d_np, &np_all, 4, cudaMemcpyHostToDevice, s);
-  if (err == cudaSuccess)
-    err = cudaMemcpyAsync(at(o_batch), hb.data(), nbatch * sizeof(cfgmm::PairBatch),
-                          cudaMemcpyHostToDevice, s);
-  if (err == cudaSuccess) err = cudaStreamSynchronize(s);  // host vectors die on return
-  if (err != cudaSuccess) return cuda_fail(err, "split plan upload");
+  int P = pair0, nitems = 0;
+  if (nbatch == 1) {
+    // One batch (a server molecule): the work list stays in the device's
+    // order (pair-major, heaviest pairs first by chunk count), the partial
+    // offsets come from a device scan and the partial sums from the host
+    // bound -- no host round trip, so a plan builds without waiting for the
+    // device.  Counts reported below are bounds.
+    P = int(nbg_tot);
+    nitems = int(item_bound);
+    const size_t part_bytes =
+        row_bound * nset_max * cfgmm::split_pair_partial_points() * sizeof(double);
+    err = cudaMallocAsync(&plan->mem3, std::max<size_t>(part_bytes, 256), s);
+    if (err != cudaSuccess) return cuda_fail(err, "cudaMalloc(split plan partials)");
+    err = cudaMemcpyAsync(d_np, d_np + 1, 4, cudaMemcpyDeviceToDevice, s);
+    if (err == cudaSuccess)
+      err = cfgmm::split_pair_partial_offsets(static_cast<const int*>(at(o_ucount)), d_np, tn,
+                                              static_cast<int*>(at(o_poff)), s);
+    if (err != cudaSuccess) return cuda_fail(err, "split plan work list");
+  } else {
+    if (size_t(chunk0) > chunk_bound) return fail(CFGMM_ERR_CUDA, "split plan: chunk bound exceeded");
+    // ---- work list: pair-major (a pair's phi tiles and D rows shared in L2 by
+    // the CTAs running at one time), heaviest pairs first ----
+    err = cudaMemcpyAsync(&nitems, d_total, 4, cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) return cuda_fail(err, "split plan work list");
+    if (size_t(nitems) > item_bound) return fail(CFGMM_ERR_CUDA, "split plan: item bound exceeded");
+    std::vector<int4> items(size_t(std::max(nitems, 0)));
+    std::vector<int> ucount(size_t(std::max(P, 1)));
+    if (err == cudaSuccess && nitems > 0)
+      err = cudaMemcpyAsync(items.data(), at(o_items), size_t(nitems) * sizeof(int4),
+                            cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess && P > 0)
+      err = cudaMemcpyAsync(ucount.data(), at(o_ucount), size_t(P) * 4, cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) return cuda_fail(err, "split plan work list");
+    std::stable_sort(items.begin(), items.end(), [&](const int4& x, const int4& y) {
+      const int kx = (ucount[x.x] + TK - 1) / TK, ky = (ucount[y.x] + TK - 1) / TK;
+      if (kx != ky) return kx > ky;
+      if (x.x != y.x) return x.x < y.x;
+      if (x.y != y.y) return x.y < y.y;
+      return x.z < y.z;
+    });
+    // partial row tiles: exact, from the unions
+    std::vector<int> poff(size_t(P) + 1, 0);
+    for (int q = 0; q < P; ++q) poff[q + 1] = poff[q] + (ucount[q] + tn - 1) / tn;
+    const size_t part_bytes =
+        size_t(poff[P]) * nset_max * cfgmm::split_pair_partial_points() * sizeof(double);
+    err = cudaMallocAsync(&plan->mem3, std::max<size_t>(part_bytes, 256), s);
+    if (err != cudaSuccess) return cuda_fail(err, "cudaMalloc(split plan partials)");
+    const int np_all = P;
+    if (nitems > 0)
+      err = cudaMemcpyAsync(at(o_items), items.data(), size_t(nitems) * sizeof(int4),
+                            cudaMemcpyHostToDevice, s);
+    if (err == cudaSuccess)
+      err = cudaMemcpyAsync(at(o_poff), poff.data(), poff.size() * 4, cudaMemcpyHostToDevice, s);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(d_np, &np_all, 4, cudaMemcpyHostToDevice, s);
+    if (err == cudaSuccess)
+      err = cudaMemcpyAsync(at(o_batch), hb.data(), nbatch * sizeof(cfgmm::PairBatch),
+                            cudaMemcpyHostToDevice, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);  // host vectors die on return
+    if (err != cudaSuccess) return cuda_fail(err, "split plan upload");
+  }
 
   plan->split = true;
   plan->pair = true;
@@ -604,7 +629,8 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
   a.ulist = static_cast<const int*>(at(o_ulist));
   a.uflag = static_cast<const uint8_t*>(at(o_uflag));
   a.cbase = static_cast<const int*>(at(o_cbase));
-  a.batches = static_cast<const cfgmm::PairBatch*>(at(o_batch));
+  a.batches = nbatch == 1 ? nullptr : static_cast<const cfgmm::PairBatch*>(at(o_batch));
+  a.one = hb[0];
   a.partial = static_cast<double*>(plan->mem3);
   a.poff = static_cast<const int*>(at(o_poff));
   a.nao = int(nao);
@@ -621,8 +647,6 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
   // ---- autotuning: pipeline depth of the persistent kernel ----
   std::string tune = "default";
   char key[256];
-  double work = 0.0;
-  for (int q = 0; q < P; ++q) work += double(ucount[q]) * ucount[q];
   std::snprintf(key, sizeof(key), "aodm_split_pair%d:nao%d:work%d:items%d:nset%zu:blk%zu", nsl,
                 bucket(double(nao)), bucket(work), bucket(double(nitems)), nset_max, blksize);
   plan->stages = 0;
@@ -680,9 +704,10 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
   std::snprintf(buf, sizeof(buf),
                 "{\"precision\":\"split\",\"form\":\"pair\",\"digits\":%d,\"batches\":%zu,"
                 "\"items\":%d,\"block_tiles\":%zu,\"pairs\":%d,\"phi_chunks\":%d,"
-                "\"flops\":%.6e,\"config\":{\"row_tile\":%d,\"stages\":%d},\"graph\":%s,"
-                "\"tuning\":",
-                nsl, nbatch, nitems, nbg_tot, P, chunk0, plan->flops, tn, plan->stages,
+                "\"counts\":\"%s\",\"flops\":%.6e,\"config\":{\"row_tile\":%d,\"stages\":%d},"
+                "\"graph\":%s,\"tuning\":",
+                nsl, nbatch, nitems, nbg_tot, P, nbatch == 1 ? int(chunk_bound) : chunk0,
+                nbatch == 1 ? "bounds" : "exact", plan->flops, tn, plan->stages,
                 plan->exec ? "true" : "false");
   plan->info = std::string(buf) + (tune[0] == '[' ? tune : "\"" + tune + "\"") + ",\"key\":\"" +
                key + "\"}";

@@ -165,6 +165,10 @@ cudaError_t split_pair_lists_and_signatures(const PairPrep& q, int* lists, int* 
                                             cudaStream_t stream);
 cudaError_t split_pair_prepare_tiles(const PairPrep& q, cudaStream_t stream);
 cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream);
+// poff[pi]: the first partial row of pair pi (pairs from 0, npairs on the
+// device), poff[npairs] their total; one launch, no host round trip.
+cudaError_t split_pair_partial_offsets(const int* ucount, const int* npairs, int tn, int* poff,
+                                       cudaStream_t stream);
 // D digits of every row (dsl, tau, and dhalf: the digits of D_uu / 2 for the
 // symmetric mode's diagonal) and, when asym is non-null (zeroed by the
 // caller), the bitwise symmetry check of every D, in one launch.

@@ -1552,6 +1552,49 @@ cudaError_t split_pair_prepare_tiles(const PairPrep& q, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
+namespace {
+
+// poff[pi] = sum over the pairs before pi of their row tiles (ceil(ucount/tn)),
+// poff[npairs] the total: the partial sums' offsets.  One CTA.
+__global__ void __launch_bounds__(1024)
+pair_partial_offsets(const int* __restrict__ ucount, const int* __restrict__ npairs_d, int tn,
+                     int* __restrict__ poff) {
+  __shared__ int warp_c[32];
+  __shared__ int base_s;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int np = npairs_d[0];
+  if (tid == 0) base_s = 0;
+  __syncthreads();
+  for (int p0 = 0; p0 < np; p0 += 1024) {
+    const int pl = p0 + tid;
+    const int nt = pl < np ? (ucount[pl] + tn - 1) / tn : 0;
+    int ic = nt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, ic, o);
+      if (lane >= o) ic += t;
+    }
+    if (lane == 31) warp_c[warp] = ic;
+    __syncthreads();
+    int bc = base_s;
+    for (int w = 0; w < warp; ++w) bc += warp_c[w];
+    if (pl < np) poff[pl] = bc + ic - nt;
+    __syncthreads();
+    if (tid == 0)
+      for (int w = 0; w < 32; ++w) base_s += warp_c[w];
+    __syncthreads();
+  }
+  if (tid == 0) poff[np] = base_s;
+}
+
+}  // namespace
+
+cudaError_t split_pair_partial_offsets(const int* ucount, const int* npairs, int tn, int* poff,
+                                       cudaStream_t stream) {
+  pair_partial_offsets<<<1, 1024, 0, stream>>>(ucount, npairs, tn, poff);
+  return cudaGetLastError();
+}
+
 cudaError_t split_pair_prepare_batch(const PairPrep& q, cudaStream_t stream) {
   cudaError_t err = split_pair_prepare_scales(q, stream);
   if (err == cudaSuccess) err = split_pair_prepare_pairs(q, stream);
