@@ -128,6 +128,15 @@ struct Molecule {
   bool loading = false;  // being put on the device by the loader thread
   int pending = 0;  // requests queued or on the GPU
   uint64_t last_use = 0;
+  // recorded after the device work that puts the molecule and its plans on
+  // the device; every request's slot stream waits for it (no host wait)
+  cudaEvent_t ready = nullptr;
+  Molecule() = default;
+  Molecule(const Molecule&) = delete;
+  Molecule& operator=(const Molecule&) = delete;
+  ~Molecule() {
+    if (ready) cudaEventDestroy(ready);
+  }
 };
 
 struct Request {
@@ -268,6 +277,8 @@ size_t molecule_cost(const Molecule& m, int precision, size_t blksize) {
 
 // Frees a resident, idle molecule's device state (lock held).
 void release(cfgmm_server* s, Molecule& m) {
+  // the frees on the admin stream come after the molecule's load and plan work
+  if (m.ready) cudaStreamWaitEvent(s->admin, m.ready, 0);
   for (auto& kv : m.plans) cfgmm::aodm_plan_release_idle(kv.second, s->admin);
   m.plans.clear();
   if (m.mem) cudaFreeAsync(m.mem, s->admin);
@@ -276,9 +287,9 @@ void release(cfgmm_server* s, Molecule& m) {
   s->used -= m.cost;
 }
 
-// Puts the molecule's phi, mask and buffers on the device (worker thread,
-// without the lock: the molecule is reserved; the GPU work is on the admin
-// stream and finished on return).
+// Puts the molecule's phi, mask and buffers on the device (a loader thread,
+// without the lock: the molecule is reserved; the GPU work is enqueued on the
+// loader's stream `st`).
 int materialize(cfgmm_server* s, Molecule& m, cudaStream_t st, std::string* err) {
   const size_t phi = m.nao * m.ngrid * sizeof(double);
   const size_t nblk = (m.ngrid + s->blksize - 1) / s->blksize;
@@ -461,19 +472,32 @@ bool make_room(cfgmm_server* s, size_t need, uint64_t keep) {
 // molecule and the slot are reserved).  Returns a status and message.
 int launch(cfgmm_server* s, Request& r, Molecule& m, Slot& sl, std::string* err) {
   int rc = CFGMM_OK;
+  const bool built = m.plans.count(r.nset) == 0;
   cfgmm_aodm_plan* plan = plan_for(s, m, r.nset, s->admin, &rc);
   if (!plan) {
     *err = std::string("plan: ") + cfgmm_last_error();
     return rc;
   }
+  // a plan built here (a request with another nset): its device work on the
+  // admin stream, after what the event stood for, comes before the request's
+  if (built) {
+    cudaError_t e = cudaSuccess;
+    if (m.ready) e = cudaStreamWaitEvent(s->admin, m.ready, 0);
+    else e = cudaEventCreateWithFlags(&m.ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(m.ready, s->admin);
+    if (e != cudaSuccess) {
+      *err = cuda_msg(e, "plan");
+      return CFGMM_ERR_CUDA;
+    }
+  }
   r.flops = cfgmm::aodm_plan_flops(plan);
   r.t_launch = Clock::now();
-  cudaError_t e = cudaSuccess;
-  if (r.on_device) {
+  cudaError_t e = m.ready ? cudaStreamWaitEvent(sl.stream, m.ready, 0) : cudaSuccess;
+  if (e == cudaSuccess && r.on_device) {
     e = cudaStreamWaitEvent(sl.stream, r.ready, 0);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(m.d_dms, r.dev_d, r.d_bytes, cudaMemcpyDeviceToDevice, sl.stream);
-  } else {
+  } else if (e == cudaSuccess) {
     e = cudaMemcpyAsync(m.d_dms, r.pin_d, r.d_bytes, cudaMemcpyHostToDevice, sl.stream);
   }
   if (e == cudaSuccess) e = cudaMemsetAsync(m.d_rho, 0, r.rho_bytes, sl.stream);
@@ -573,8 +597,10 @@ void loader_loop(cfgmm_server* s, cudaStream_t st) {
     const Clock::time_point t1 = Clock::now();
     if (rc == CFGMM_OK && !plan_for(s, m, r.nset, st, &rc))
       err = std::string("plan: ") + cfgmm_last_error();
-    if (rc == CFGMM_OK) {  // the worker's streams use the molecule after this
-      const cudaError_t e = cudaStreamSynchronize(st);
+    if (rc == CFGMM_OK) {  // the requests' slot streams wait for this point of st
+      cudaError_t e = m.ready ? cudaSuccess
+                              : cudaEventCreateWithFlags(&m.ready, cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventRecord(m.ready, st);
       if (e != cudaSuccess) {
         rc = CFGMM_ERR_CUDA;
         err = cuda_msg(e, "molecule load");
