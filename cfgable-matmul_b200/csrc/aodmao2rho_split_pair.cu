@@ -675,8 +675,8 @@ pair_phi_max(const double* __restrict__ ao, size_t stride_grid, const int* __res
 // The phi digit tiles of every chunk of the batch (pair pi, chunk c): NSL
 // planes of 128 rows (points: rows 0-63 the lo tile, 64-127 the hi tile) x
 // 32 bytes (union AOs 32c .. 32c+31), 32-byte swizzled, at phisl + (cbase[pi]
-// + c) * A_STAGE; sigma[g] from pmax.  Persistent CTAs walk the batch's
-// chunks [chunk0, chunks_end) through the chunk -> pair map.
+// + c) * A_STAGE; sigma[g] from pmax.  Persistent CTAs take contiguous runs
+// of the batch's chunks [chunk0, chunks_end) through the chunk -> pair map.
 template <int NSL>
 __global__ void __launch_bounds__(256)
 pair_phi_tiles(const double* __restrict__ ao, size_t stride_grid,
@@ -689,7 +689,11 @@ pair_phi_tiles(const double* __restrict__ ao, size_t stride_grid,
   // staged digit words [plane][quad of 4 AOs][point], rows padded to 132 words
   __shared__ uint32_t stage[NSL][8][PT + 4];
   const int nch = chunks_end[0] - chunk0;
-  for (int ci = blockIdx.x; ci < nch; ci += gridDim.x) {
+  // a contiguous run of chunks per CTA: mostly one pair's, whose union list,
+  // flags and offsets stay in L1 from one chunk to the next
+  const int per = (nch + int(gridDim.x) - 1) / int(gridDim.x);
+  const int ci0 = int(blockIdx.x) * per, ci1 = min(nch, ci0 + per);
+  for (int ci = ci0; ci < ci1; ++ci) {
     const int pi = cpair[ci];
     const int c = chunk0 + ci - cbase[pi];
     const int nu = ucount[pi];
