@@ -169,6 +169,38 @@ def test_split_plan_equals_single_split_calls(cm, wl, tmp_path, monkeypatch, gra
     plan.close()
 
 
+@pytest.mark.parametrize("form", ["row", "pair"])
+@pytest.mark.parametrize("graph", [True, False])
+def test_split_plan_of_one_batch(cm, wl, tmp_path, monkeypatch, form, graph):
+    """A plan of one batch (the server's plans; the pair form builds it with
+    no host round trip: the device's work list, partial offsets from a device
+    scan): bit for bit the single split call, on two runs."""
+    import torch
+    monkeypatch.setenv("CFGMM_AUTOTUNE_CACHE", str(tmp_path / "tune.txt"))
+    monkeypatch.setenv("CFGMM_SPLIT_FORM", form)
+    rng = np.random.default_rng(41)
+    nao, ngrid, blk, nset = 300, 3000, 64, 2
+    nblk = -(-ngrid // blk)
+    tab = (rng.random((nao, nblk)) < 0.35).astype(np.uint8)
+    phi = rng.standard_normal((nao, ngrid))
+    phi[~wl.expand_mask(tab, ngrid, blk)] = 0.0
+    dms = wl.sym_dms(rng, nset, nao)
+    b = dict(lhs=phi, rhs=phi, tab=tab, nset=nset, rho0=rng.standard_normal((nset, ngrid)),
+             ngrid=ngrid)
+    dev, ddms = _device(torch, [b], dms)
+    plan = cm.AodmPlan(dev, ddms, blksize=blk, precision=cm.PREC_OZAKI_INT8, graph=graph)
+    plan.run()
+    torch.cuda.synchronize()
+    want = _single(cm, torch, b, dms, blk, cm.PREC_OZAKI_INT8)
+    assert np.array_equal(dev[0][0].cpu().numpy(), want)
+    dev[0][0].copy_(torch.from_numpy(b["rho0"]))
+    plan.run()
+    torch.cuda.synchronize()
+    assert np.array_equal(dev[0][0].cpu().numpy(), want)
+    assert normwise(want, _single(cm, torch, b, dms, blk)) < 1e-12
+    plan.close()
+
+
 def test_plan_rejections(cm, wl):
     import torch
     bs, dms = _batches(wl, torch, 4, 2, nset_max=2)
