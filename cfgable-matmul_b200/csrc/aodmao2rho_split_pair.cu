@@ -1313,8 +1313,12 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
         const int kc = (nu + TK - 1) / TK;
         const int kc0 = sym ? (it.y * TN) / TK : 0;
         const uint8_t* src = p.phisl + size_t(p.cbase[it.x]) * C::A_STAGE;
+        // the chunks' plane masks, loaded a chunk ahead (beside the stage wait)
         const uint8_t* cm = p.cmask + p.cbase[it.x];
+        uint32_t mnext = kc0 < kc ? cm[kc0] : 0u;
         for (int c = kc0; c < kc; ++c, ++seq) {
+          const uint32_t mcur = mnext;
+          if (c + 1 < kc) mnext = cm[c + 1];
           const int stg = int(seq % STAGES);
           const uint32_t use = seq / STAGES;
           if (use > 0 && !tc::mbar_wait(&empty[stg], (use - 1) & 1, err, 37, false, lim)) {
@@ -1324,7 +1328,7 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
           // test hook: the first stage is never published, so the MMA warp's
           // bounded wait runs out and the call reports a timeout
           if (p.inject && seq == 0) continue;
-          pmask[stg] = cm[c];
+          pmask[stg] = uint8_t(mcur);
           tc::mbar_arrive_expect_tx(&full_phi[stg], C::A_STAGE);
           tc::bulk_load(smem + stg * C::STAGE, src + size_t(c) * C::A_STAGE, C::A_STAGE,
                         &full_phi[stg]);

@@ -174,7 +174,8 @@ def test_split_plan_equals_single_split_calls(cm, wl, tmp_path, monkeypatch, gra
 def test_split_plan_of_one_batch(cm, wl, tmp_path, monkeypatch, form, graph):
     """A plan of one batch (the server's plans; the pair form builds it with
     no host round trip: the device's work list, partial offsets from a device
-    scan): bit for bit the single split call, on two runs."""
+    scan): bit for bit the single split call on two runs with a general D;
+    with a symmetric D (the half contraction) within 1e-12 of FP64."""
     import torch
     monkeypatch.setenv("CFGMM_AUTOTUNE_CACHE", str(tmp_path / "tune.txt"))
     monkeypatch.setenv("CFGMM_SPLIT_FORM", form)
@@ -184,7 +185,7 @@ def test_split_plan_of_one_batch(cm, wl, tmp_path, monkeypatch, form, graph):
     tab = (rng.random((nao, nblk)) < 0.35).astype(np.uint8)
     phi = rng.standard_normal((nao, ngrid))
     phi[~wl.expand_mask(tab, ngrid, blk)] = 0.0
-    dms = wl.sym_dms(rng, nset, nao)
+    dms = rng.uniform(-1, 1, (nset, nao, nao))  # general: no half contraction
     b = dict(lhs=phi, rhs=phi, tab=tab, nset=nset, rho0=rng.standard_normal((nset, ngrid)),
              ngrid=ngrid)
     dev, ddms = _device(torch, [b], dms)
@@ -198,6 +199,13 @@ def test_split_plan_of_one_batch(cm, wl, tmp_path, monkeypatch, form, graph):
     torch.cuda.synchronize()
     assert np.array_equal(dev[0][0].cpu().numpy(), want)
     assert normwise(want, _single(cm, torch, b, dms, blk)) < 1e-12
+    plan.close()
+    sdms = wl.sym_dms(rng, nset, nao)  # symmetric: the half contraction
+    dev, ddms = _device(torch, [b], sdms)
+    plan = cm.AodmPlan(dev, ddms, blksize=blk, precision=cm.PREC_OZAKI_INT8, graph=graph)
+    plan.run()
+    torch.cuda.synchronize()
+    assert normwise(dev[0][0].cpu().numpy(), _single(cm, torch, b, sdms, blk)) < 1e-12
     plan.close()
 
 
