@@ -480,7 +480,7 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
                o_dsl = take(nset_max * nao * nao * 8), o_tau = take(nset_max * nao * 4),
                o_dhalf = take(nset_max * nao * 8),
                o_batch = take(nbatch * sizeof(cfgmm::PairBatch)),
-               o_phisl = take(chunk_bound * a_stage), o_cmask = take(chunk_bound);
+               o_phisl = take(chunk_bound * a_stage);
   cudaError_t err = cudaMallocAsync(&plan->mem2, o, s);
   if (err != cudaSuccess) return cuda_fail(err, "cudaMalloc(split plan)");
   char* base = static_cast<char*>(plan->mem2);
@@ -530,7 +530,6 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
     q.sigma = static_cast<int*>(at(o_sigma)) + sg_off[i];
     q.pmax = static_cast<unsigned long long*>(at(o_pmax));
     q.phisl = static_cast<uint8_t*>(at(o_phisl));
-    q.cmask = static_cast<uint8_t*>(at(o_cmask));
     err = cfgmm::split_pair_prepare_batch(q, s);
     if (nbatch > 1) {  // the next batch's pairs and chunks follow this one's
       int got[2] = {0, 0};
@@ -623,7 +622,6 @@ int build_split_pair(cfgmm_aodm_plan* plan, const cfgmm_aodm_batch* batches, siz
   a.tau = static_cast<const int*>(at(o_tau));
   a.dhalf = static_cast<const uint2*>(at(o_dhalf));
   a.phisl = static_cast<const uint8_t*>(at(o_phisl));
-  a.cmask = static_cast<const uint8_t*>(at(o_cmask));
   a.items = static_cast<const int4*>(at(o_items));
   a.total = d_total;
   a.pairs = static_cast<const int4*>(at(o_pairs));

@@ -97,7 +97,6 @@ struct PairArgs {
   const int* tau;         // row scales [s][u]
   const uint2* dhalf;     // digits of D_uu / 2 [s][u] (the symmetric mode's diagonal)
   const uint8_t* phisl;   // phi digit tiles [chunk][NSL][128 x 32]
-  const uint8_t* cmask;   // [chunk] bit j: phi digit plane j holds a nonzero digit
   const int4* items;      // (pair, row tile, s, batch)
   const int* total;       // [0] items
   const int4* pairs;      // (lo tile, hi tile or -1, batch, 0), tiles local to the batch
@@ -143,7 +142,6 @@ struct PairPrep {
   int* sigma;             // out: [ngrid]
   unsigned long long* pmax;  // scratch [ngrid]
   uint8_t* phisl;         // out: phi tiles from chunk0
-  uint8_t* cmask;         // out: [chunk] nonzero phi digit planes, from chunk0
 };
 
 size_t aodmao2rho_split_pair_workspace(size_t nao, size_t ngrid, size_t nset, size_t blk,

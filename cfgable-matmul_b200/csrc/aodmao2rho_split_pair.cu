@@ -105,12 +105,11 @@ struct Cfg {
   static constexpr int STEPS = WROWS / 4;  // four rows per step
   static constexpr int OCTETS = TN / 8;    // TMEM column octets of one level
   static constexpr int MAXQ = 2 * ((OCTETS + NG - 1) / NG);  // epilogue quartets per group
-  // shared memory of a launch: stages, a zero digit plane, barriers, the item
-  // ring, the stages' phi plane masks and the epilogue's phi_lhs values
-  // ([warp][column][lane])
+  // shared memory of a launch: stages, barriers, the item ring and the
+  // epilogue's phi_lhs values ([warp][column][lane])
   template <int STAGES>
   static constexpr size_t smem_bytes() {
-    return size_t(STAGES) * STAGE + A_SLICE + 1024 + 256 + kRing * (16 + 4) + 16 +
+    return size_t(STAGES) * STAGE + 1024 + 256 + kRing * (16 + 4) +
            size_t(GW) * 4 * MAXQ * 32 * 8;
   }
   static_assert(NSL * TN <= 512, "level accumulators exceed the TMEM columns");
@@ -685,14 +684,10 @@ pair_phi_tiles(const double* __restrict__ ao, size_t stride_grid,
                const int* __restrict__ cpair, int chunk0, const int* __restrict__ chunks_end,
                const int* __restrict__ ulist, const uint8_t* __restrict__ uflag,
                const int* __restrict__ ucount, const int* __restrict__ cbase, int nao, int ngrid,
-               int blk, int gsub, int* __restrict__ sigma, uint8_t* __restrict__ phisl,
-               uint8_t* __restrict__ cmask) {
+               int blk, int gsub, int* __restrict__ sigma, uint8_t* __restrict__ phisl) {
   using C = Cfg<NSL>;
   // staged digit words [plane][quad of 4 AOs][point], rows padded to 132 words
   __shared__ uint32_t stage[NSL][8][PT + 4];
-  __shared__ uint32_t planes;  // the chunk's planes holding a nonzero digit
-  if (threadIdx.x == 0) planes = 0;
-  __syncthreads();
   const int nch = chunks_end[0] - chunk0;
   // a contiguous run of chunks per CTA: mostly one pair's, whose union list,
   // flags and offsets stay in L1 from one chunk to the next
@@ -717,7 +712,6 @@ pair_phi_tiles(const double* __restrict__ ao, size_t stride_grid,
       }
       const int e = g >= 0 ? exp_for(__longlong_as_double(static_cast<long long>(pmax[g]))) : 0;
       if (c == 0 && hq == 0 && g >= 0) sigma[g] = e;
-      uint32_t nz = 0;
 #pragma unroll
       for (int qq = 0; qq < 4; ++qq) {
         const int q = hq * 4 + qq;
@@ -733,19 +727,10 @@ pair_phi_tiles(const double* __restrict__ ao, size_t stride_grid,
         transpose4(w[0].x, w[1].x, w[2].x, w[3].x, o[0], o[1], o[2], o[3]);
         transpose4(w[0].y, w[1].y, w[2].y, w[3].y, o[4], o[5], o[6], o[7]);
 #pragma unroll
-        for (int pl2 = 0; pl2 < NSL; ++pl2) {
-          stage[pl2][q][r] = o[pl2];
-          nz |= uint32_t(o[pl2] != 0u) << pl2;
-        }
+        for (int pl2 = 0; pl2 < NSL; ++pl2) stage[pl2][q][r] = o[pl2];
       }
-      nz = __reduce_or_sync(0xffffffffu, nz);
-      if ((threadIdx.x & 31) == 0 && nz) atomicOr(&planes, nz);
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      cmask[size_t(cbase[pi]) + c] = uint8_t(planes);
-      planes = 0;  // the next chunk's, after the barrier below
-    }
     uint8_t* tile0 = phisl + (size_t(cbase[pi]) + c) * C::A_STAGE;
     for (int v = threadIdx.x; v < NSL * PT * 2; v += 256) {
       const int hh = v & 1, r = (v >> 1) & (PT - 1), j = v >> 8;
@@ -871,10 +856,7 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                              ~uintptr_t(1023));
-  // an all-zero digit plane: the operands that clear a level no MMA of an
-  // item wrote
-  uint8_t* zplane = smem + STAGES * C::STAGE;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(zplane + C::A_SLICE);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * C::STAGE);
   uint64_t* full_phi = bars;            // phi tile landed (bulk copy)
   uint64_t* full_d = bars + STAGES;     // D digits stored (4 gather warps)
   uint64_t* empty = bars + 2 * STAGES;  // the stage's MMAs completed
@@ -885,13 +867,10 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
   // the work-item ring: the loader thread draws items from the global counter
   // (dynamic scheduling: the list is pair-major, heaviest pairs first) and
   // every role reads them from here in the same order
-  uint64_t* ifull = bars + 32;  // [kRing], 256 bytes after the barriers
+  uint64_t* ifull = reinterpret_cast<uint64_t*>(smem + STAGES * C::STAGE + 256);  // [kRing]
   uint64_t* iempty = ifull + kRing;                                   // [kRing]
   int* ring = reinterpret_cast<int*>(iempty + kRing);                 // [kRing]
-  // bit j of pmask[stage]: the stage's phi digit plane j holds a nonzero digit
-  // (written by the loader before it arms the stage's barrier)
-  uint8_t* pmask = reinterpret_cast<uint8_t*>(ring + kRing);          // [STAGES <= 16]
-  double* phl_all = reinterpret_cast<double*>(pmask + 16);            // [GW][4 MAXQ][32]
+  double* phl_all = reinterpret_cast<double*>(ring + kRing);          // [GW][4 MAXQ][32]
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int* err = &g_pair_error;
@@ -911,9 +890,6 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
     }
     tc::mbar_fence_init();
   }
-  for (uint32_t i = threadIdx.x; i < C::A_SLICE / 16; i += THREADS)
-    reinterpret_cast<uint4*>(zplane)[i] = make_uint4(0u, 0u, 0u, 0u);
-  tc::fence_proxy_async_smem();  // the zero plane is read by the tensor cores
   if (warp == GW) {
     tc::tmem_alloc(tmem_slot, 512);
     tc::tmem_relinquish();
@@ -1223,7 +1199,6 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
         const int kc0 = sym ? (it.y * TN) / TK : 0;
         if (nitem > 0 && !tc::mbar_wait(acc_empty, (nitem - 1) & 1, err, 33, false, lim)) break;
         tc::fence_after_sync();
-        uint32_t written = 0;  // levels an MMA of this item has written
         for (int c = kc0; c < kc; ++c, ++seq) {
           const int stg = int(seq % STAGES);
           const uint32_t par = (seq / STAGES) & 1;
@@ -1235,20 +1210,15 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
           tc::fence_after_sync();
           const uint32_t a0 = tc::smem_u32(smem + stg * C::STAGE);
           const uint32_t b0 = a0 + C::A_STAGE;
-          const uint32_t planes = pmask[stg];
           // phi digit j (the A operand) meets D digits 0 .. NSL-1-j (levels
           // j .. NSL-1) in consecutive MMAs: its plane is read from shared
-          // memory once and held in the collector buffer for the rest.  A
-          // plane without a nonzero digit adds nothing: its MMAs are skipped,
-          // and a level's first MMA in the item overwrites it.
+          // memory once and held in the collector buffer for the rest
 #pragma unroll
           for (int j = 0; j < NSL; ++j) {
-            if (!((planes >> j) & 1u)) continue;
             const uint64_t ad = tc::smem_desc_k32(a0 + j * C::A_SLICE);
+            const bool acc = c > kc0 || j > 0;
 #pragma unroll
             for (int i = 0; i + j < NSL; ++i) {
-              const bool acc = (written >> (i + j)) & 1u;
-              written |= 1u << (i + j);
               const uint32_t d = tmem + uint32_t((i + j) * TN);
               const uint64_t bd = tc::smem_desc_k32(b0 + i * C::B_SLICE);
               if (j == NSL - 1)
@@ -1264,11 +1234,6 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
           tc::mma_commit(&empty[stg]);
         }
         if (!ok) break;
-        // levels no MMA wrote still hold the last item's sums: zero products
-        const uint64_t zd = tc::smem_desc_k32(tc::smem_u32(zplane));
-#pragma unroll
-        for (int L = 0; L < NSL; ++L)
-          if (!((written >> L) & 1u)) tc::mma_i8(tmem + uint32_t(L * TN), zd, zd, idesc, false);
         tc::mma_commit(acc_full);
       }
       tc::mma_commit(drain);
@@ -1313,12 +1278,7 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
         const int kc = (nu + TK - 1) / TK;
         const int kc0 = sym ? (it.y * TN) / TK : 0;
         const uint8_t* src = p.phisl + size_t(p.cbase[it.x]) * C::A_STAGE;
-        // the chunks' plane masks, loaded a chunk ahead (beside the stage wait)
-        const uint8_t* cm = p.cmask + p.cbase[it.x];
-        uint32_t mnext = kc0 < kc ? cm[kc0] : 0u;
         for (int c = kc0; c < kc; ++c, ++seq) {
-          const uint32_t mcur = mnext;
-          if (c + 1 < kc) mnext = cm[c + 1];
           const int stg = int(seq % STAGES);
           const uint32_t use = seq / STAGES;
           if (use > 0 && !tc::mbar_wait(&empty[stg], (use - 1) & 1, err, 37, false, lim)) {
@@ -1328,7 +1288,6 @@ __global__ void __launch_bounds__(THREADS, 1) pair_main(PairArgs p) {
           // test hook: the first stage is never published, so the MMA warp's
           // bounded wait runs out and the call reports a timeout
           if (p.inject && seq == 0) continue;
-          pmask[stg] = uint8_t(mcur);
           tc::mbar_arrive_expect_tx(&full_phi[stg], C::A_STAGE);
           tc::bulk_load(smem + stg * C::STAGE, src + size_t(c) * C::A_STAGE, C::A_STAGE,
                         &full_phi[stg]);
@@ -1402,7 +1361,7 @@ size_t a256(size_t v) { return (v + 255) / 256 * 256; }
 struct Layout {
   size_t lists, counts, bits, cnt, key, order, cand, ncand, partner, pos, choice, pairs, npairs,
       ulist, uflag, ucount, cbase, cpair, items, total, dsl, tau, dhalf, sigma, pmax, phisl,
-      cmask, partial, bytes;
+      partial, bytes;
 };
 
 Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk, int nsl) {
@@ -1441,8 +1400,7 @@ Layout layout(size_t nao, size_t ngrid, size_t nset, size_t blk, int nsl) {
   L.sigma = L.dhalf + a256(nset * nao * 8);
   L.pmax = L.sigma + a256(ngrid * sizeof(int));
   L.phisl = L.pmax + a256(ngrid * sizeof(unsigned long long));
-  L.cmask = L.phisl + a256(nbg * max_kc * a_stage);
-  L.partial = L.cmask + a256(nbg * max_kc);
+  L.partial = L.phisl + a256(nbg * max_kc * a_stage);
   L.bytes = L.partial + nbg * max_t * nset * NG * PT * sizeof(double);
   return L;
 }
@@ -1589,12 +1547,12 @@ cudaError_t split_pair_prepare_tiles(const PairPrep& q, cudaStream_t stream) {
     pair_phi_tiles<6><<<grid, 256, 0, stream>>>(q.ao_rhs, q.stride_grid, q.pmax, q.pairs, q.cpair,
                                                 q.chunk0, q.chunks_end, q.ulist, q.uflag,
                                                 q.ucount, q.cbase, q.nao, q.ngrid, q.blk, d.gsub,
-                                                q.sigma, q.phisl, q.cmask);
+                                                q.sigma, q.phisl);
   else
     pair_phi_tiles<7><<<grid, 256, 0, stream>>>(q.ao_rhs, q.stride_grid, q.pmax, q.pairs, q.cpair,
                                                 q.chunk0, q.chunks_end, q.ulist, q.uflag,
                                                 q.ucount, q.cbase, q.nao, q.ngrid, q.blk, d.gsub,
-                                                q.sigma, q.phisl, q.cmask);
+                                                q.sigma, q.phisl);
   return cudaGetLastError();
 }
 
@@ -1701,7 +1659,6 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   q.sigma = static_cast<int*>(at(L.sigma));
   q.pmax = static_cast<unsigned long long*>(at(L.pmax));
   q.phisl = static_cast<uint8_t*>(at(L.phisl));
-  q.cmask = static_cast<uint8_t*>(at(L.cmask));
   uint2* dsl = static_cast<uint2*>(at(L.dsl));
   int* tau = static_cast<int*>(at(L.tau));
   uint2* dhalf = static_cast<uint2*>(at(L.dhalf));
@@ -1739,7 +1696,6 @@ cudaError_t aodmao2rho_split_pair(double* rhos, const double* dms, const double*
   a.tau = tau;
   a.dhalf = dhalf;
   a.phisl = q.phisl;
-  a.cmask = q.cmask;
   a.items = q.items;
   a.total = q.total;
   a.pairs = q.pairs;
