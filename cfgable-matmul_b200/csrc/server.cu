@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>
@@ -157,7 +158,9 @@ struct Request {
   double flops = 0.0;
   int slot = -1;
   bool cold = false;         // its molecule was put on the device for it
-  bool device_done = false;  // set by the host callback
+  // set by the host callback, which takes no lock: a host function must not
+  // wait on a thread that may itself be inside a CUDA call
+  std::atomic<bool> device_done{false};
   bool finished = false;     // set by the worker
   int status = CFGMM_OK;
   std::string error;
@@ -396,10 +399,10 @@ void CUDART_CB on_device_done(void* arg) {
   Request* r = static_cast<Request*>(arg);
   if (!r->on_device) std::memcpy(r->user_rho, r->pin_rho, r->rho_bytes);
   cfgmm_server* s = r->srv;
-  {
-    std::lock_guard<std::mutex> lk(s->mu);
-    r->device_done = true;
-  }
+  // r may be gone once the flag is up; the server outlives its slot streams'
+  // callbacks (destroy synchronises them).  A wakeup lost to the unlocked
+  // notify costs the worker at most its 5 ms poll.
+  r->device_done.store(true, std::memory_order_release);
   s->cv_work.notify_one();
 }
 
@@ -635,7 +638,7 @@ void worker_loop(cfgmm_server* s) {
   for (;;) {
     // completions
     for (Slot& sl : s->slots) {
-      if (sl.req && sl.req->device_done) {
+      if (sl.req && sl.req->device_done.load(std::memory_order_acquire)) {
         Request& r = *sl.req;
         cudaEventElapsedTime(&r.device_ms, sl.e0, sl.e1);
         sl.req = nullptr;
@@ -779,6 +782,7 @@ int cfgmm_server_destroy(cfgmm_server* s) {
     if (kv.second->resident) release(s, *kv.second);
   cudaStreamSynchronize(s->admin);
   for (Slot& sl : s->slots) {
+    cudaStreamSynchronize(sl.stream);  // the last host callbacks have returned
     cudaStreamDestroy(sl.stream);
     cudaEventDestroy(sl.e0);
     cudaEventDestroy(sl.e1);
