@@ -507,17 +507,25 @@ def serving_section(args, cm, wl):
     def one_pass(precision, arrivals, device_dm=False):
         import torch
         srv = cm.Server(budget, nslots=args.serve_slots, precision=precision)
-        t_start = time.perf_counter()
+        # the clock starts once every client thread is up (and, for the device
+        # SCF loop, holds its D, its update and its rho on the device already)
+        t0 = [0.0]
+        ready = threading.Barrier(len(mols) + 1, action=lambda: t0.__setitem__(0, time.perf_counter()))
 
         def client(k):
             mol, pts, nset, d0, noise = mols[k]
-            time.sleep(max(0.0, t_start + arrivals[k] - time.perf_counter()))
-            mid = srv.open_shells(pts, mol.shell_xyz, mol.shell_l, mol.alpha, mol.norm, 0.3, nset)
             if device_dm:  # the SCF loop on the GPU: D updated and rho read on the device
-                with torch.cuda.stream(torch.cuda.Stream()):
+                st = torch.cuda.Stream()
+                with torch.cuda.stream(st):
                     rho = torch.zeros(nset, len(pts), dtype=torch.float64, device="cuda")
                     d = torch.from_numpy(d0).cuda()
                     dn = torch.from_numpy(noise).cuda()
+                st.synchronize()
+            ready.wait(300.0)  # a client that failed to start breaks it for all
+            time.sleep(max(0.0, t0[0] + arrivals[k] - time.perf_counter()))
+            mid = srv.open_shells(pts, mol.shell_xyz, mol.shell_l, mol.alpha, mol.norm, 0.3, nset)
+            if device_dm:
+                with torch.cuda.stream(st):
                     for step in range(10):
                         srv.wait(srv.submit(mid, d, rho), 600.0)
                         d += dn
@@ -532,9 +540,10 @@ def serving_section(args, cm, wl):
         th = [threading.Thread(target=client, args=(k,)) for k in range(len(mols))]
         for t in th:
             t.start()
+        ready.wait(300.0)
         for t in th:
             t.join()
-        wall = time.perf_counter() - t_start
+        wall = time.perf_counter() - t0[0]
         st = srv.stats()
         srv.shutdown()
         return {"value": st["flops_completed"] / wall / 1e9, "unit": "GFLOP/s",
