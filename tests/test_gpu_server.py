@@ -177,6 +177,58 @@ def test_server_device_resident_requests(cm, wl, precision):
             srv2.shutdown()
 
 
+@pytest.mark.timeout(900)
+@pytest.mark.parametrize("form", ["row", "pair"])
+def test_server_saturated_device_scf(cm, wl, monkeypatch, form):
+    """Every molecule's SCF loop at once with D and rho on the device, each
+    client on its own thread and stream (the serving bench's saturated device
+    pass), in split precision with the given form forced: every request
+    completes, none fails, and each result matches the FP64 single call
+    within 1e-12.  The server's completion callback takes no lock; one that
+    waited on the server mutex deadlocked this pattern against the worker's
+    CUDA calls."""
+    import threading
+    import torch
+    monkeypatch.setenv("CFGMM_SPLIT_FORM", form)
+    mols = _molecules(wl, 31, 8)
+    srv = cm.Server(8 << 30, nslots=8, precision=1)
+    results, errors = [None] * len(mols), []
+
+    def client(k):
+        try:
+            m = mols[k]
+            i = srv.open(m["ao"], m["tab"], m["nset"])
+            side = torch.cuda.Stream()
+            outs = []
+            with torch.cuda.stream(side):
+                for step in range(3):
+                    d = torch.from_numpy(m["dms"][step]).cuda()
+                    rho = torch.full((m["nset"], m["ao"].shape[1]), float("nan"),
+                                     dtype=torch.float64, device="cuda")
+                    srv.wait(srv.submit(i, d, rho), WAIT)
+                    outs.append(rho)
+            side.synchronize()
+            srv.close(i)
+            results[k] = [o.cpu().numpy() for o in outs]
+        except Exception as e:  # reported below, on the test's thread
+            errors.append(e)
+
+    try:
+        th = [threading.Thread(target=client, args=(k,)) for k in range(len(mols))]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        st = srv.stats()
+    finally:
+        srv.shutdown()
+    assert not errors, errors
+    assert st["failed"] == 0 and st["completed"] == 3 * len(mols), st
+    for m, outs in zip(mols, results):
+        for step in range(3):
+            assert normwise(outs[step], _single(cm, m, m["dms"][step])) < 1e-12
+
+
 def test_server_budget_admission(cm, wl):
     """A budget that holds about one molecule: every request still completes,
     molecules are admitted one after another, and the server never holds more
