@@ -29,12 +29,23 @@ constexpr int THREADS = 256;   // 8 warps: 4 along rows (16 each) x 2 along colu
 constexpr int TILE = FT * FT;  // doubles per staged tile
 
 // Offset (doubles) of element (row, point k) of a 64 x 64 tile: the 16-byte slot
-// 4(k/8) + k%4 of a row holds points k and k+4 -- one m16n8k8 fragment pair of A
-// (rows = u) and of B (rows = v) -- and the slots of a row are XOR-swizzled by
-// swz_key(row), so a fragment load's phases of 8 lanes meet 8 distinct slots.
+// k/2 of a row holds points k and k+1, contiguous in phi, so one 16-byte copy
+// fills it; the slots of a row are XOR-swizzled by swz_key(row), so a fragment
+// load's phases of 8 lanes meet 8 distinct slots.  A k step of 8 points gives
+// the m16n8k8 index j (0..3) the points 2j and 2j+1 as its k = j and k = j + 4,
+// on both operands alike: the products summed are the same, and a fragment
+// pair (a0, a2) of A (rows = u) or (b0, b1) of B (rows = v) is one 16-byte load.
 __device__ __forceinline__ int f_off(int r, int k) {
-  const int slot = ((k >> 3) << 2) | (k & 3);
-  return r * FT + ((slot ^ swz_key(r)) << 1) + ((k >> 2) & 1);
+  return r * FT + (((k >> 1) ^ swz_key(r)) << 1) + (k & 1);
+}
+
+// 16-byte asynchronous copy of which the first `bytes` (0, 8 or 16) are read
+// from `src`; the rest of the destination is zero-filled.
+__device__ __forceinline__ void cp_async_16_n(void* smem_dst, const void* gmem_src, int bytes) {
+  const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(gmem_src),
+               "r"(bytes)
+               : "memory");
 }
 
 struct FockArgs {
@@ -48,6 +59,7 @@ struct FockArgs {
   const int* counts;
   int nao, ngrid, blk, gsub;
   int sym;  // ao_lhs == ao_rhs: chunks from the row tile's own on, mirrored
+  int vec;  // phi rows and w 16-byte aligned at every tile: pairs of points per copy
   const int4* items;
   int* counters;  // [nset] work counters, [nset] = item total
 };
@@ -83,22 +95,52 @@ fock_compact_kernel(const __grid_constant__ FockArgs p) {
     const int gw = min(min((b + 1) * p.blk, p.ngrid), g0 + FT) - g0;
 
     // A = phi_lhs[I[u0 + r]][g0 + k] * w[g0 + k], zero past the rows and points
-    for (int e = tid; e < TILE; e += THREADS) {
-      const int r = e >> 6, k = e & 63;
-      double x = 0.0;
-      if (r < mu && k < gw)
-        x = p.ao_lhs[size_t(I[u0 + r]) * p.stride_grid + g0 + k] * w[g0 + k];
-      As[f_off(r, k)] = x;
+    if (p.vec) {
+      // pairs of points (k even): the partner of the tile's last point lies
+      // inside the row (stride_grid is even, so ngrid < stride_grid when odd)
+      for (int e = tid; e < TILE / 2; e += THREADS) {
+        const int r = e >> 5, k = 2 * (e & 31);
+        double2 x = make_double2(0.0, 0.0);
+        if (r < mu && k < gw) {
+          const double2 f = *reinterpret_cast<const double2*>(
+              p.ao_lhs + size_t(I[u0 + r]) * p.stride_grid + g0 + k);
+          const double2 ww = *reinterpret_cast<const double2*>(w + g0 + k);
+          x.x = f.x * ww.x;
+          if (k + 1 < gw) x.y = f.y * ww.y;
+        }
+        *reinterpret_cast<double2*>(As + f_off(r, k)) = x;
+      }
+    } else {
+      for (int e = tid; e < TILE; e += THREADS) {
+        const int r = e >> 6, k = e & 63;
+        double x = 0.0;
+        if (r < mu && k < gw)
+          x = p.ao_lhs[size_t(I[u0 + r]) * p.stride_grid + g0 + k] * w[g0 + k];
+        As[f_off(r, k)] = x;
+      }
     }
     auto issue = [&](int ch) {
       double* B = Bs + (ch & 1) * TILE;
       const int c0 = ch * FT;
-      for (int e = tid; e < TILE; e += THREADS) {
-        const int c = e >> 6, k = e & 63;
-        const bool valid = c0 + c < nb && g0 + k < p.ngrid;
-        const double* src =
-            valid ? p.ao_rhs + size_t(I[c0 + c]) * p.stride_grid + g0 + k : p.ao_rhs;
-        cp_async_8(B + f_off(c, k), src, valid);
+      if (p.vec) {
+        // one 16-byte copy per pair of points; a pair past ngrid is zero-filled
+        // (one of its points, or both)
+        for (int e = tid; e < TILE / 2; e += THREADS) {
+          const int c = e >> 5, k = 2 * (e & 31);
+          const int left = p.ngrid - (g0 + k);
+          const int bytes = c0 + c < nb ? (left >= 2 ? 16 : (left == 1 ? 8 : 0)) : 0;
+          const double* src =
+              bytes ? p.ao_rhs + size_t(I[c0 + c]) * p.stride_grid + g0 + k : p.ao_rhs;
+          cp_async_16_n(B + f_off(c, k), src, bytes);
+        }
+      } else {
+        for (int e = tid; e < TILE; e += THREADS) {
+          const int c = e >> 6, k = e & 63;
+          const bool valid = c0 + c < nb && g0 + k < p.ngrid;
+          const double* src =
+              valid ? p.ao_rhs + size_t(I[c0 + c]) * p.stride_grid + g0 + k : p.ao_rhs;
+          cp_async_8(B + f_off(c, k), src, valid);
+        }
       }
       cp_async_commit();
     };
@@ -218,6 +260,10 @@ cudaError_t fock_compact_fp64(double* vs, const double* ws, const double* ao_lhs
   a.blk = blk;
   a.gsub = gsub;
   a.sym = ao_lhs == ao_rhs;
+  // 16-byte copies need every tile's first point (b * blk + 64 t) 16-byte
+  // aligned in phi and w: an even BLKSIZE and row stride, aligned bases
+  auto al16 = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
+  a.vec = blk % 2 == 0 && stride_grid % 2 == 0 && al16(ao_lhs) && al16(ao_rhs) && al16(ws);
   a.items = items;
   a.counters = counters;
   const size_t dyn = 2 * TILE * sizeof(double);
