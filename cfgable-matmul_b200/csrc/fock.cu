@@ -94,10 +94,41 @@ fock_compact_kernel(const __grid_constant__ FockArgs p) {
     const int g0 = b * p.blk + gt * FT;
     const int gw = min(min((b + 1) * p.blk, p.ngrid), g0 + FT) - g0;
 
+    auto issue = [&](int ch) {
+      double* B = Bs + (ch & 1) * TILE;
+      const int c0 = ch * FT;
+      if (p.vec) {
+        // one 16-byte copy per pair of points; a pair past ngrid is zero-filled
+        // (one of its points, or both)
+#pragma unroll
+        for (int e = tid; e < TILE / 2; e += THREADS) {
+          const int c = e >> 5, k = 2 * (e & 31);
+          const int left = p.ngrid - (g0 + k);
+          const int bytes = c0 + c < nb ? (left >= 2 ? 16 : (left == 1 ? 8 : 0)) : 0;
+          const double* src =
+              bytes ? p.ao_rhs + size_t(I[c0 + c]) * p.stride_grid + g0 + k : p.ao_rhs;
+          cp_async_16_n(B + f_off(c, k), src, bytes);
+        }
+      } else {
+#pragma unroll 4
+        for (int e = tid; e < TILE; e += THREADS) {
+          const int c = e >> 6, k = e & 63;
+          const bool valid = c0 + c < nb && g0 + k < p.ngrid;
+          const double* src =
+              valid ? p.ao_rhs + size_t(I[c0 + c]) * p.stride_grid + g0 + k : p.ao_rhs;
+          cp_async_8(B + f_off(c, k), src, valid);
+        }
+      }
+      cp_async_commit();
+    };
+    const int nch = (nb + FT - 1) / FT;
+    const int ch0 = p.sym ? a : 0;
+    issue(ch0);  // the first chunk's copies fly while A is staged
     // A = phi_lhs[I[u0 + r]][g0 + k] * w[g0 + k], zero past the rows and points
     if (p.vec) {
       // pairs of points (k even): the partner of the tile's last point lies
       // inside the row (stride_grid is even, so ngrid < stride_grid when odd)
+#pragma unroll
       for (int e = tid; e < TILE / 2; e += THREADS) {
         const int r = e >> 5, k = 2 * (e & 31);
         double2 x = make_double2(0.0, 0.0);
@@ -111,6 +142,7 @@ fock_compact_kernel(const __grid_constant__ FockArgs p) {
         *reinterpret_cast<double2*>(As + f_off(r, k)) = x;
       }
     } else {
+#pragma unroll 4
       for (int e = tid; e < TILE; e += THREADS) {
         const int r = e >> 6, k = e & 63;
         double x = 0.0;
@@ -119,34 +151,6 @@ fock_compact_kernel(const __grid_constant__ FockArgs p) {
         As[f_off(r, k)] = x;
       }
     }
-    auto issue = [&](int ch) {
-      double* B = Bs + (ch & 1) * TILE;
-      const int c0 = ch * FT;
-      if (p.vec) {
-        // one 16-byte copy per pair of points; a pair past ngrid is zero-filled
-        // (one of its points, or both)
-        for (int e = tid; e < TILE / 2; e += THREADS) {
-          const int c = e >> 5, k = 2 * (e & 31);
-          const int left = p.ngrid - (g0 + k);
-          const int bytes = c0 + c < nb ? (left >= 2 ? 16 : (left == 1 ? 8 : 0)) : 0;
-          const double* src =
-              bytes ? p.ao_rhs + size_t(I[c0 + c]) * p.stride_grid + g0 + k : p.ao_rhs;
-          cp_async_16_n(B + f_off(c, k), src, bytes);
-        }
-      } else {
-        for (int e = tid; e < TILE; e += THREADS) {
-          const int c = e >> 6, k = e & 63;
-          const bool valid = c0 + c < nb && g0 + k < p.ngrid;
-          const double* src =
-              valid ? p.ao_rhs + size_t(I[c0 + c]) * p.stride_grid + g0 + k : p.ao_rhs;
-          cp_async_8(B + f_off(c, k), src, valid);
-        }
-      }
-      cp_async_commit();
-    };
-    const int nch = (nb + FT - 1) / FT;
-    const int ch0 = p.sym ? a : 0;
-    issue(ch0);
     const int r_lo = wm * 16 + g, r_hi = r_lo + 8;
     const int u_lo = r_lo < mu ? I[u0 + r_lo] : -1;
     const int u_hi = r_hi < mu ? I[u0 + r_hi] : -1;
