@@ -25,6 +25,7 @@
 #include "dgemm_fp64.cuh"
 #include "f32.cuh"
 #include "fock.cuh"
+#include "server.cuh"
 #include "gemm_i8.cuh"
 #include "ozaki.cuh"
 
@@ -1272,6 +1273,7 @@ int cfgmm_release_workspace(void) {
   if (st->buf) CFGMM_CUDA(cudaFree(st->buf));
   st->buf = nullptr;
   st->cap = 0;
+  cfgmm::release_pinned_staging();
   return CFGMM_OK;
 }
 

@@ -41,6 +41,7 @@
 #include "ao_eval.cuh"
 #include "aodmao2rho_fp64.cuh"
 #include "aodmao2rho_split.cuh"
+#include "server.cuh"
 
 namespace cfgmm {
 void set_last_error(const std::string& msg);
@@ -60,6 +61,10 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
 size_t a256(size_t v) { return (v + 255) / 256 * 256; }
 
 // ---- pinned host staging, reused by size class ----------------------------
+// One pool for the process (portable pinned memory, usable from every
+// device): a buffer outlives the server that pinned it, so a later server, or
+// a later request of the same size class, gets it without pinning host memory
+// while other requests run.  cfgmm_release_workspace frees the idle ones.
 class PinnedPool {
  public:
   void* get(size_t bytes) {
@@ -74,7 +79,7 @@ class PinnedPool {
       }
     }
     void* p = nullptr;
-    if (cudaHostAlloc(&p, cls, cudaHostAllocDefault) != cudaSuccess) {
+    if (cudaHostAlloc(&p, cls, cudaHostAllocPortable) != cudaSuccess) {
       cudaGetLastError();
       return nullptr;
     }
@@ -87,8 +92,15 @@ class PinnedPool {
     std::lock_guard<std::mutex> lk(mu_);
     free_[size_of_[p]].push_back(p);
   }
-  ~PinnedPool() {
-    for (auto& kv : size_of_) cudaFreeHost(kv.first);
+  // Frees the buffers no request holds.
+  void trim() {
+    std::lock_guard<std::mutex> lk(mu_);
+    for (auto& kv : free_)
+      for (void* p : kv.second) {
+        cudaFreeHost(p);
+        size_of_.erase(p);
+      }
+    free_.clear();
   }
 
  private:
@@ -101,6 +113,13 @@ class PinnedPool {
   std::map<size_t, std::vector<void*>> free_;
   std::unordered_map<void*, size_t> size_of_;
 };
+
+// Never destroyed: freeing pinned memory from a static destructor would race
+// the CUDA runtime's own teardown at exit.
+PinnedPool& pinned_pool() {
+  static PinnedPool* pool = new PinnedPool();
+  return *pool;
+}
 
 enum Kind { kHost = 0, kDevice = 1, kShells = 2 };
 
@@ -175,6 +194,10 @@ struct Slot {
 
 }  // namespace
 
+namespace cfgmm {
+void release_pinned_staging() { pinned_pool().trim(); }
+}  // namespace cfgmm
+
 struct cfgmm_server {
   int dev = 0;
   size_t budget = 0;
@@ -182,7 +205,6 @@ struct cfgmm_server {
   size_t blksize = 64;
   std::vector<Slot> slots;
   cudaStream_t admin = nullptr;
-  PinnedPool pinned;
 
   std::mutex mu;
   std::condition_variable cv_work;  // worker: new requests, completions, stop
@@ -411,8 +433,8 @@ void finish(cfgmm_server* s, Request& r, int status, const std::string& err) {
   r.error = err;
   r.finished = true;
   r.t_done = Clock::now();
-  s->pinned.put(r.pin_d);
-  s->pinned.put(r.pin_rho);
+  pinned_pool().put(r.pin_d);
+  pinned_pool().put(r.pin_rho);
   r.pin_d = r.pin_rho = nullptr;
   if (r.ready) cudaEventDestroy(r.ready);
   r.ready = nullptr;
@@ -906,11 +928,11 @@ int submit_common(cfgmm_server* s, uint64_t molecule, const double* dms, size_t 
       return fail(CFGMM_ERR_CUDA, cuda_msg(e, "submit"));
     }
   } else {
-    r->pin_d = s->pinned.get(r->d_bytes);
-    r->pin_rho = s->pinned.get(r->rho_bytes);
+    r->pin_d = pinned_pool().get(r->d_bytes);
+    r->pin_rho = pinned_pool().get(r->rho_bytes);
     if (!r->pin_d || !r->pin_rho) {
-      s->pinned.put(r->pin_d);
-      s->pinned.put(r->pin_rho);
+      pinned_pool().put(r->pin_d);
+      pinned_pool().put(r->pin_rho);
       return fail(CFGMM_ERR_OUT_OF_MEMORY, "pinned staging");
     }
     std::memcpy(r->pin_d, dms, r->d_bytes);
@@ -921,8 +943,8 @@ int submit_common(cfgmm_server* s, uint64_t molecule, const double* dms, size_t 
     std::lock_guard<std::mutex> lk(s->mu);
     auto it = s->mols.find(molecule);
     if (it == s->mols.end() || it->second->closed) {
-      s->pinned.put(r->pin_d);
-      s->pinned.put(r->pin_rho);
+      pinned_pool().put(r->pin_d);
+      pinned_pool().put(r->pin_rho);
       if (r->ready) cudaEventDestroy(r->ready);
       return fail(CFGMM_ERR_INVALID_ARGUMENT, "molecule closed during submit");
     }

@@ -337,7 +337,9 @@ int cfgmm_mask_ao_dev(double* ao, size_t stride_grid, size_t ngrid, const int* s
                       double threshold, uint8_t* tab, size_t ldtab, size_t blksize, void* stream);
 
 /* Releases the calling device's cached workspaces (they are otherwise kept
- * and reused across calls until process exit). */
+ * and reused across calls until process exit), and the servers' idle pinned
+ * host staging buffers, which are kept for the process and reused across
+ * servers. */
 int cfgmm_release_workspace(void);
 
 /* ---- serving: density requests from many molecules, continuous batching ----
