@@ -258,6 +258,28 @@ def test_server_budget_admission(cm, wl):
     srv.shutdown()
 
 
+def test_server_staging_outlives_servers(cm, wl):
+    """The pinned host staging of D and rho is one process-wide pool: a later
+    server reuses the buffers of an earlier one, and cfgmm_release_workspace
+    frees the idle ones.  Three servers in turn, with the release between the
+    second and the third, give the same results bit for bit."""
+    mols = _molecules(wl, 41, 3)
+    outs = []
+    for k in range(3):
+        if k == 2:
+            assert cm.lib().cfgmm_release_workspace() == 0
+        srv = cm.Server(8 << 30, nslots=4)
+        try:
+            outs.append(_serve(cm, srv, mols, concurrent=True))
+            assert srv.stats()["failed"] == 0
+        finally:
+            srv.shutdown()
+    for k in (1, 2):
+        for a, b in zip(outs[0], outs[k]):
+            for step in range(3):
+                assert np.array_equal(a[step], b[step])
+
+
 def test_server_device_molecule_and_eviction(cm, wl):
     """Caller-owned device phi used in place; LRU eviction under a small
     budget brings a molecule back for its later requests."""
