@@ -91,8 +91,11 @@ OzakiPlan ozaki_plan(int k, int nmod, int min_bits) {
   const int logM = bit_length(M) - 1;  // floor(log2 M)
   const int P = logM - 3 - ceil_log2(k > 1 ? k : 2);
   // at most 52 bits each: the FP32 residue computation is exact up to 2^52
-  p.alpha = std::min(P / 2, kOzakiMaxBits);
-  p.beta = std::min(P - P / 2, kOzakiMaxBits);
+  // op(B) takes the smaller half when P is odd: in a host call it is split once
+  // for every row block of A, and at 47 bits or fewer its residues take the
+  // three-digit form (the headline shape has the larger B)
+  p.beta = std::min(P / 2, kOzakiMaxBits);
+  p.alpha = std::min(P - P / 2, kOzakiMaxBits);
   // split point T: sum_l |r_l| hi_l + |q| H < 2^53 with |r_l| <= 128, |q| <= 128 N
   const int T = std::max(0, logM + 1 + 7 + ceil_log2(nmod + 1) + 1 - 52);
   p.two_T = std::ldexp(1.0, T);
@@ -215,6 +218,7 @@ using f32x2 = unsigned long long;  // two FP32 lanes in a 64-bit register
 struct ResidueArgs {
   int nmod;
   f32x2 c14[kMaxModuli], c28[kMaxModuli], c42[kMaxModuli], inv[kMaxModuli], nm[kMaxModuli];
+  f32x2 c16[kMaxModuli], c32[kMaxModuli];  // the 16-bit digit form's 2^16, 2^32 mods m
 };
 
 __device__ __forceinline__ f32x2 pack2(float lo, float hi) {
@@ -251,29 +255,46 @@ constexpr long long kDigitBias = 8192LL * (1 + (1LL << 14) + (1LL << 28));
 // [2^52, 2^53), where the spacing of doubles is 1, so its mantissa field holds
 // w + 2^51 (w = v + kDigitBias) and the rounding that forms it is rint(v).
 constexpr double kRoundBias = 6755399441055744.0 + double(kDigitBias);
+// The 16-bit digit form, for |v| <= 2^47: w = v + kDigitBias16 in [0, 2^49),
+// v = sum_{t<3} (u_t - 2^15) 2^16t with u_t = (w >> 16t) & 0xffff (t < 2) and
+// u_2 = w >> 32, every balanced digit within [-2^15, 2^15]; then
+//   s = b_0 + b_1 c_16 + b_2 c_32,  |s| <= 2^15 (1 + 2 * 127) < 2^23,
+// two FMAs per modulus, exact, and |s| < 2^23 is what the quotient needs
+// (|s| 2^-24 / m, the error of s * fl(1/m), stays below 1/(2m)).
+constexpr long long kDigitBias16 = 32768LL * (1 + (1LL << 16) + (1LL << 32));
+constexpr double kRoundBias16 = 6755399441055744.0 + double(kDigitBias16);
+
+// Digit forms of write_residues8: plain (integers up to 2^52, four 14-bit
+// digits), biased (up to 2^50, four 14-bit digits read off the double's bits)
+// and biased16 (up to 2^47, three 16-bit digits).
+enum : int { kPlain = 0, kBiased14 = 1, kBiased16 = 2 };
 
 // The operand element x(r, p) 2^e as the input of write_residues8: rint(x 2^e)
-// (the plain form), or that integer plus kRoundBias, rounded once by the FMA
-// (the biased form, for |x 2^e| < 2^50).  e = kNonFinite gives 0.
-template <bool kBiased>
+// (the plain form), or that integer plus the form's round bias, rounded once by
+// the FMA (the biased forms).  e = kNonFinite gives 0.
+template <int kForm>
 __device__ __forceinline__ double scaled(double x, int e) {
-  if constexpr (kBiased) {
-    if (e == kNonFinite) return kRoundBias;
+  if constexpr (kForm != kPlain) {
+    constexpr double bias = kForm == kBiased16 ? kRoundBias16 : kRoundBias;
+    if (e == kNonFinite) return bias;
     if (e >= -1022 && e <= 1023)
-      return fma(x, __longlong_as_double(static_cast<long long>(e + 1023) << 52), kRoundBias);
-    return rint(ldexp(x, e)) + kRoundBias;
+      return fma(x, __longlong_as_double(static_cast<long long>(e + 1023) << 52), bias);
+    return rint(ldexp(x, e)) + bias;
   } else {
     return scaled_int(x, e);
   }
 }
-template <bool kBiased>
-__device__ __forceinline__ double scaled_zero() { return kBiased ? kRoundBias : 0.0; }
+template <int kForm>
+__device__ __forceinline__ double scaled_zero() {
+  return kForm == kBiased16 ? kRoundBias16 : (kForm == kBiased14 ? kRoundBias : 0.0);
+}
 
 // The residues of 8 consecutive elements for every modulus, 8 bytes per modulus
 // plane at Y + l * plane + off (8-byte aligned).  v[] holds integers |v| <= 2^52
-// (plain form) or |v| <= 2^50 plus kRoundBias (biased form: the digits are bit
-// fields of the double, with no conversion to a 64-bit integer).
-template <bool kBiased>
+// (plain form) or |v| <= 2^50 (2^47) plus the form's round bias (biased forms:
+// the digits are bit fields of the double, with no conversion to a 64-bit
+// integer).  The low byte of w is v's (both digit biases are multiples of 256).
+template <int kForm>
 __device__ __forceinline__ void write_residues8(const ResidueArgs& a, int8_t* Y, size_t plane,
                                                 size_t off, const double (&v)[8]) {
   constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23
@@ -284,7 +305,15 @@ __device__ __forceinline__ void write_residues8(const ResidueArgs& a, int8_t* Y,
     float u[2][4];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      if constexpr (kBiased) {
+      if constexpr (kForm == kBiased16) {
+        // mantissa field = w + 2^51: bits 0..31 are w's, bits 32..51 are (w >> 32) + 2^19
+        const uint32_t lo = __double2loint(v[j + h]), hi = __double2hiint(v[j + h]);
+        lowb[(j + h) >> 2] |= (lo & 0xffu) << (8 * ((j + h) & 3));  // modulus 256
+        u[h][0] = float(int(lo & 0xffffu) - 32768);
+        u[h][1] = float(int(lo >> 16) - 32768);
+        u[h][2] = float(int(hi & 0xfffffu) - (1 << 19) - 32768);
+        u[h][3] = 0.0f;
+      } else if constexpr (kForm == kBiased14) {
         // mantissa field = w + 2^51: bits 0..41 are w's, bits 42..51 are (w >> 42) + 2^9
         const uint32_t lo = __double2loint(v[j + h]), hi = __double2hiint(v[j + h]);
         lowb[(j + h) >> 2] |= (lo & 0xffu) << (8 * ((j + h) & 3));  // modulus 256
@@ -313,13 +342,19 @@ __device__ __forceinline__ void write_residues8(const ResidueArgs& a, int8_t* Y,
 #pragma unroll
   for (int l = 1; l < kMaxModuli; ++l) {
     if (l >= a.nmod) break;
-    const f32x2 C14 = a.c14[l], C28 = a.c28[l], C42 = a.c42[l], INV = a.inv[l], NM = a.nm[l];
+    const f32x2 INV = a.inv[l], NM = a.nm[l];
     uint32_t bits[8];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      f32x2 S = fma2(P1[q], C14, P0[q]);
-      S = fma2(P2[q], C28, S);
-      S = fma2(P3[q], C42, S);                      // s, exact
+      f32x2 S;
+      if constexpr (kForm == kBiased16) {
+        S = fma2(P1[q], a.c16[l], P0[q]);
+        S = fma2(P2[q], a.c32[l], S);                 // s, exact
+      } else {
+        S = fma2(P1[q], a.c14[l], P0[q]);
+        S = fma2(P2[q], a.c28[l], S);
+        S = fma2(P3[q], a.c42[l], S);                 // s, exact
+      }
       const f32x2 Q = add2(fma2(S, INV, MAG), NMAG);  // rint(s / m), exact
       const f32x2 R = add2(fma2(NM, Q, S), MAG);      // (s - m q) + MAGIC
       unpack2(R, bits[2 * q], bits[2 * q + 1]);
@@ -333,7 +368,7 @@ __device__ __forceinline__ void write_residues8(const ResidueArgs& a, int8_t* Y,
 }
 
 // element (r, p) at x[r*ld + p]: CTA per row, thread per 8 consecutive p
-template <bool kBiased>
+template <int kForm>
 __global__ void __launch_bounds__(256, 5)
 residues_rows(const double* __restrict__ x, size_t ld, int rows, int k, size_t kpad,
               const int* __restrict__ e, int8_t* __restrict__ Y, ResidueArgs a) {
@@ -346,8 +381,8 @@ residues_rows(const double* __restrict__ x, size_t ld, int rows, int k, size_t k
     double v[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j)
-      v[j] = (p + j < k) ? scaled<kBiased>(row[p + j], er) : scaled_zero<kBiased>();
-    write_residues8<kBiased>(a, Y, plane, size_t(r) * kpad + p, v);
+      v[j] = (p + j < k) ? scaled<kForm>(row[p + j], er) : scaled_zero<kForm>();
+    write_residues8<kForm>(a, Y, plane, size_t(r) * kpad + p, v);
   }
 }
 
@@ -357,7 +392,7 @@ residues_rows(const double* __restrict__ x, size_t ld, int rows, int k, size_t k
 // read side (two r, eight groups of p) meets 16 distinct 8-byte bank pairs.
 __device__ __forceinline__ int tile_col(int p, int r) { return r ^ ((p >> 2) & 14); }
 
-template <bool kBiased>
+template <int kForm>
 __global__ void __launch_bounds__(256, 5)
 residues_cols(const double* __restrict__ x, size_t ld, int rows, int k, size_t kpad,
               const int* __restrict__ e, int8_t* __restrict__ Y, ResidueArgs a, Mask mask) {
@@ -380,9 +415,9 @@ residues_cols(const double* __restrict__ x, size_t ld, int rows, int k, size_t k
   double v[8];
 #pragma unroll
   for (int j = 0; j < 8; ++j)
-    v[j] = (p + j < k) ? scaled<kBiased>(tile[pg + j][tile_col(pg + j, rr)], er)
-                       : scaled_zero<kBiased>();
-  write_residues8<kBiased>(a, Y, plane, size_t(r) * kpad + p, v);
+    v[j] = (p + j < k) ? scaled<kForm>(tile[pg + j][tile_col(pg + j, rr)], er)
+                       : scaled_zero<kForm>();
+  write_residues8<kForm>(a, Y, plane, size_t(r) * kpad + p, v);
 }
 
 // ---------------------------------------------------------------------------
@@ -539,6 +574,8 @@ ResidueArgs residue_args(const OzakiPlan& p) {
     a.c14[l] = splat2(float(mods_host(1LL << 14, p.mod[l])));
     a.c28[l] = splat2(float(mods_host(1LL << 28, p.mod[l])));
     a.c42[l] = splat2(float(mods_host(1LL << 42, p.mod[l])));
+    a.c16[l] = splat2(float(mods_host(1LL << 16, p.mod[l])));
+    a.c32[l] = splat2(float(mods_host(1LL << 32, p.mod[l])));
   }
   return a;
 }
@@ -557,15 +594,20 @@ cudaError_t prepare(const double* x, size_t ld, bool rows_contig, int rows, int 
                                                                          mask);
   }
   finalize_exps<<<rb, 256, 0, s>>>(emax, rows, bits, e);
-  // scaled elements below 2^50 take the biased form of the digit split
-  const bool biased = bits <= 50;
+  // scaled elements up to 2^47 take three 16-bit digits, up to 2^50 the
+  // biased form of four 14-bit digits, the rest the plain form
+  const int form = bits <= 47 ? kBiased16 : (bits <= 50 ? kBiased14 : kPlain);
   if (rows_contig) {
-    (biased ? residues_rows<true> : residues_rows<false>)<<<rows, 256, 0, s>>>(
-        x, ld, rows, k, kpad, e, Y, ra);
+    auto kern = form == kBiased16 ? residues_rows<kBiased16>
+                                  : (form == kBiased14 ? residues_rows<kBiased14>
+                                                       : residues_rows<kPlain>);
+    kern<<<rows, 256, 0, s>>>(x, ld, rows, k, kpad, e, Y, ra);
   } else {
     dim3 grid((rows + 31) / 32, (k + 63) / 64);
-    (biased ? residues_cols<true> : residues_cols<false>)<<<grid, 256, 0, s>>>(
-        x, ld, rows, k, kpad, e, Y, ra, mask);
+    auto kern = form == kBiased16 ? residues_cols<kBiased16>
+                                  : (form == kBiased14 ? residues_cols<kBiased14>
+                                                       : residues_cols<kPlain>);
+    kern<<<grid, 256, 0, s>>>(x, ld, rows, k, kpad, e, Y, ra, mask);
   }
   return cudaGetLastError();
 }
