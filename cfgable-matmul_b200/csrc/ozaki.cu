@@ -109,12 +109,13 @@ OzakiPlan ozaki_plan(int k, int nmod, int min_bits) {
     p.mod[l] = int(m);
     p.inv_f[l] = 1.0f / float(m);
     p.inv_d[l] = 1.0 / double(m);
-    p.w_frac[l] = double(w) / Md;
     p.w_hi[l] = double(w >> T);
     p.w_lo[l] = double(w & lo_mask);
   }
   p.M_hi = double(M >> T);
   p.M_lo = double(M & lo_mask);
+  p.t_x = std::ldexp(1.0, T) / Md;
+  p.t_y = 1.0 / Md;
   return p;
 }
 
@@ -426,18 +427,19 @@ residues_cols(const double* __restrict__ x, size_t ld, int rows, int k, size_t k
 struct ReconArgs {
   int nmod;
   double w_hi[kMaxModuli], w_lo[kMaxModuli];
-  double w_frac[kMaxModuli];  // w_l / M (for the quotient only)
   double M_hi, M_lo, two_T;
+  double t_x, t_y;  // 2^T / M and 1 / M (the quotient estimate)
 };
 
 // A thread rebuilds 4 consecutive C[i][j]: its residue loads (4 bytes per
 // modulus plane) are all issued before the arithmetic.  A residue byte becomes
 // an exact double without a conversion instruction: with its sign bit flipped
 // it is r + 128 in [0, 255], placed in the low word of 2^52 and the 2^52 + 128
-// subtracted again.  t = sum_l r_l w_l / M in FP64 is within 2^-40 of the
-// exact value, and |C'| <= M/8 keeps the exact value within 1/8 of the
-// integer q, so q = rint(t) is the one of exact arithmetic; the hi / lo sums
-// are exact (every partial sum < 2^53).
+// subtracted again.  X = sum_l r_l w_hi[l] is exact (every partial sum is
+// below 2^53) and Y = sum_l r_l w_lo[l] rounded, so t = X 2^T / M + Y / M, two
+// operations, is within ~1e-12 of sum_l r_l w_l / M (|X 2^T / M| <= 128 N);
+// |C'| <= M/8 keeps that exact value within 1/8 of the integer q, so
+// q = rint(t) is the one of exact arithmetic.
 __global__ void __launch_bounds__(256)
 reconstruct(double* __restrict__ c, size_t ldc, int m, int n, const int8_t* __restrict__ R,
             size_t ldr, const int* __restrict__ ea, const int* __restrict__ eb, ReconArgs a) {
@@ -463,9 +465,9 @@ reconstruct(double* __restrict__ c, size_t ldc, int m, int n, const int8_t* __re
     fj[u] = in ? __ldg(eb + j0 + u) : 0;
   }
   constexpr double kBias = 4503599627370624.0;  // 2^52 + 128
-  double t[4], X[4], Y[4];
+  double X[4], Y[4];
 #pragma unroll
-  for (int u = 0; u < 4; ++u) t[u] = X[u] = Y[u] = 0.0;
+  for (int u = 0; u < 4; ++u) X[u] = Y[u] = 0.0;
 #pragma unroll
   for (int l = 0; l < kMaxModuli; ++l) {
     if (l >= a.nmod) break;
@@ -473,7 +475,6 @@ reconstruct(double* __restrict__ c, size_t ldc, int m, int n, const int8_t* __re
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const double r = __hiloint2double(0x43300000, int(__byte_perm(wb, 0u, 0x4440u + u))) - kBias;
-      t[u] = fma(r, a.w_frac[l], t[u]);
       X[u] = fma(r, a.w_hi[l], X[u]);  // exact
       Y[u] = fma(r, a.w_lo[l], Y[u]);
     }
@@ -483,7 +484,7 @@ reconstruct(double* __restrict__ c, size_t ldc, int m, int n, const int8_t* __re
   for (int u = 0; u < 4; ++u) {
     const int j = j0 + u;
     if (j >= n) break;
-    const double q = rint(t[u]);
+    const double q = rint(fma(X[u], a.t_x, Y[u] * a.t_y));
     const double hi = fma(-q, a.M_hi, X[u]);  // exact
     const double lo = fma(-q, a.M_lo, Y[u]);
     const double cp = fma(hi, a.two_T, lo);   // C' with one rounding
@@ -724,13 +725,14 @@ cudaError_t ozaki_dgemm(double* c, const double* a, const double* b, int m, int 
   ReconArgs rc{};
   rc.nmod = plan.nmod;
   for (int l = 0; l < plan.nmod; ++l) {
-    rc.w_frac[l] = plan.w_frac[l];
     rc.w_hi[l] = plan.w_hi[l];
     rc.w_lo[l] = plan.w_lo[l];
   }
   rc.M_hi = plan.M_hi;
   rc.M_lo = plan.M_lo;
   rc.two_T = plan.two_T;
+  rc.t_x = plan.t_x;
+  rc.t_y = plan.t_y;
   const long long rgrid = (long long)((n + 1023) / 1024) * m;
   if (rgrid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
   if (c_ready && (err = cudaStreamWaitEvent(stream, c_ready, 0)) != cudaSuccess) return err;

@@ -23,10 +23,10 @@ struct OzakiPlan {
   float inv_f[kMaxModuli];
   double inv_d[kMaxModuli];
   // CRT weights w_l (sum_l r_l w_l = C' mod M), split at 2^T:
-  double w_frac[kMaxModuli];  // w_l / M
   double w_hi[kMaxModuli];    // w_l >> T (exact)
   double w_lo[kMaxModuli];    // w_l mod 2^T (rounded)
   double M_hi, M_lo, two_T;   // M >> T, M mod 2^T, 2^T
+  double t_x, t_y;            // 2^T / M, 1 / M: the quotient from the hi / lo sums
 };
 
 // Plan for contraction length k with `nmod` moduli (<= 0: the fewest moduli
