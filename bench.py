@@ -515,13 +515,17 @@ def serving_section(args, cm, wl):
         def client(k):
             mol, pts, nset, d0, noise = mols[k]
             if device_dm:  # the SCF loop on the GPU: D updated and rho read on the device
-                st = torch.cuda.Stream()
-                with torch.cuda.stream(st):
-                    rho = torch.zeros(nset, len(pts), dtype=torch.float64, device="cuda")
-                    d = torch.from_numpy(d0).cuda()
-                    dn = torch.from_numpy(noise).cuda()
-                st.synchronize()
-            ready.wait(300.0)  # a client that failed to start breaks it for all
+                try:
+                    st = torch.cuda.Stream()
+                    with torch.cuda.stream(st):
+                        rho = torch.zeros(nset, len(pts), dtype=torch.float64, device="cuda")
+                        d = torch.from_numpy(d0).cuda()
+                        dn = torch.from_numpy(noise).cuda()
+                    st.synchronize()
+                except BaseException:
+                    ready.abort()  # the other clients and the timer stop waiting now
+                    raise
+            ready.wait(300.0)
             time.sleep(max(0.0, t0[0] + arrivals[k] - time.perf_counter()))
             mid = srv.open_shells(pts, mol.shell_xyz, mol.shell_l, mol.alpha, mol.norm, 0.3, nset)
             if device_dm:
